@@ -1,0 +1,348 @@
+"""Throughput of the WaterSim FLIP/MAC substep on B200.
+
+Workload (the 128^3 planet of the headline metric): 128^3 MAC grid, unit
+cells, sea-level radius 52 and ocean depth 8 (core radius 44), seeded
+value-noise terrain (seed 20260114), 8 particles per fluid cell (~2M), FLIP
+with pic 0.05, red-black SOR (omega 1.7) to a 1e-5 relative residual checked
+every 10 iterations, speed clamp 3.2 m/s, full planet gravity, thermal cycle
+off, and the seeded Gaussian stir kick (sigma 4 cells, 2 m/s peak) every 50
+substeps. One bench step = one substep of dt = 0.01 (the reference's
+step(1/60) runs two such substeps).
+
+Arms
+  default            the CUDA library through the C ABI (watersim-v1_b200)
+  --impl reference   the reference's CPU algorithm: the C restatement of
+                     js/solver.js in oracle/ (no JavaScript engine exists on
+                     the machine), reference order (lexicographic SOR),
+                     single-threaded like solver.js, same workload.
+
+Multi-GPU: the substep does not shard, so N GPUs run N independent replicas
+(weak scaling); value = substeps completed by all ranks / max-rank time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "watersim-v1_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+WORKLOAD = dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, per_cell=8.0)
+PARAMS = dict(pic=0.05, omega=1.7, maxSpeed=3.2, cfl=3.0, viscosity=5e-4, thermalOn=0,
+              sorTol=1e-5, sorCheckEvery=10, sorMaxIters=5000, pressureIters=40)
+DT = 0.01
+STIR_EVERY, STIR_SIGMA, STIR_PEAK = 50, 4.0, 2.0
+METRIC = "substeps/s @128^3/2M particles (plain red-black SOR to 1e-5 relative divergence residual)"
+E2E_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pflag")
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) > 7 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 7 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 7 for i in range(4)
+                          if r[4 + i].lower() in ("active", "1")})
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def make_solver(device, rank=0):
+    """The 128^3 planet through the library's own terrain generator and fill."""
+    from fluid_solver import FluidSolver
+    W = WORKLOAD
+    coreR = W["R"] - W["depth"]
+    depthW = W["depth"]
+    Rlo = max(coreR * 0.55, W["R"] - 1.8889 * depthW)
+    cap = int(4 / 3 * math.pi * (W["R"] ** 3 - Rlo ** 3) * W["per_cell"]) + 8192
+    fs = FluidSolver(nx=W["n"], ny=W["n"], nz=W["n"], dx=1.0, coreR=coreR, terrainSeed=W["seed"],
+                     capacity=cap, device=device)
+    fs.generateTerrain(W["seed"], W["R"])
+    vw = fs.water_volume(W["depth"])
+    fs.set_scalars(targetParticles=float(round(vw * W["per_cell"])))
+    fs.resetWater(W["depth"])
+    fs.set_params(**PARAMS)
+    fs.set_scalars(gRamp=1.5)
+    return fs
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    fs = make_solver(local_rank, rank)
+    nP = fs.scalars.nP
+    stream = torch.cuda.ExternalStream(fs.stream())
+    count = [0]
+
+    def one_step():
+        if count[0] % STIR_EVERY == 0:
+            fs.stir_gaussian(STIR_SIGMA, STIR_PEAK)
+        fs._substep(DT)
+        count[0] += 1
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        one_step()
+    # ---- device-resident timed region (inputs already in HBM)
+    barrier()
+    clk = Clocks(local_rank)
+    clk.start()
+    l0 = fs.launch_count()
+    iters0 = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        one_step()
+        iters0.append(fs.scalars.sorIters)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    clocks = clk.stop()
+    launches = fs.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = args.steps * world / (ms / 1000.0)
+    # ---- end to end through the public API with pinned host buffers
+    host = {k: torch.empty(nP, dtype=torch.uint8 if k == "pflag" else torch.float32).pin_memory().numpy()
+            for k in E2E_FIELDS}
+    for k in E2E_FIELDS:
+        host[k][:] = fs.download(k)
+    e2e_steps = max(1, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for k in E2E_FIELDS:
+            fs.upload(k, host[k])
+        one_step()
+        for k in E2E_FIELDS:
+            host[k][:] = fs.download(k, nP)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    bytes_io = sum(host[k].nbytes for k in E2E_FIELDS)
+    # ---- roofline of the dominant kernel, timed live on the library stream
+    roof = roofline(fs, ms / args.steps, iters0)
+    out = None
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)",
+               "config": {"workload": "planet128: 128^3 MAC grid, R=52, depth 8, %d particles" % nP,
+                          "particles": nP, "parallelism": "replicas x%d" % world,
+                          "sor": "red-black to 1e-5 (check every 10), mean iterations %.1f"
+                                 % (sum(iters0) / max(1, len(iters0))),
+                          "particle_substeps_per_s": value * nP,
+                          "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP)},
+               "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
+                       "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
+               "gpu_launches": int(launches),
+               "roofline": roof,
+               "clocks": clocks}
+    return out, fs
+
+
+def state_mb(fs, nP):
+    n = fs.nx
+    F = 3 * (n + 1) * n * n
+    return int((nP * 55 + F * 21 + n ** 3 * 16) / 1e6)
+
+
+def roofline(fs, ms_step, iters):
+    """Dominant kernel by time share per substep; achieved = algorithmic
+    bytes per launch / measured launch time (CUDA events, library stream)."""
+    peak, kind = _peaks()
+    n = fs.nx
+    N = n ** 3
+    F = 3 * (n + 1) * n * n
+    nP = fs.scalars.nP
+    it = sum(iters) / max(1, len(iters))
+    us_sor = fs.time_kernel(0, 40)          # per colour launch
+    us_p2g = fs.time_kernel(1, 5)
+    us_g2p = fs.time_kernel(2, 5)
+    share_sor = 2 * it * us_sor / (ms_step * 1000)
+    share_p2g = us_p2g / (ms_step * 1000)
+    share_g2p = us_g2p / (ms_step * 1000)
+    # algorithmic bytes: SOR 13 B per cell per iteration (q read + rhs + stencil + q write),
+    # half per colour launch; P2G 25 B/particle in + 8 B per face accumulator (read+write);
+    # G2P+advect 52 B/particle + 8 B/face (u, uO)
+    cand = {"k_sor_color": (share_sor, 6.5 * N, us_sor),
+            "k_p2g": (share_p2g, 25 * nP + 16 * F, us_p2g),
+            "k_g2p_advect": (share_g2p, 52 * nP + 8 * F, us_g2p)}
+    name = max(cand, key=lambda k: cand[k][0])
+    share, nbytes, us = cand[name]
+    achieved = nbytes / (us * 1e-6) / 1e9
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": kind, "traffic": None,
+            "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": share,
+            "others": {k: {"us_per_launch": v[2], "time_share": v[0],
+                           "GB_s": v[1] / (v[2] * 1e-6) / 1e9} for k, v in cand.items()}}
+
+
+def cpu_baseline(fs, seconds=20.0):
+    """The oracle (CPU restatement, reference order) on this exact planet, one
+    core, a bounded sample of whole substeps."""
+    from oracle.oracle import Oracle
+    import numpy as np
+    s = fs.scalars
+    nP = s.nP
+    t = fs.terrain()
+    W = WORKLOAD
+    coreR = W["R"] - W["depth"]
+    o = Oracle(fs.nx, fs.ny, fs.nz, 1.0, coreR=coreR, terrainSeed=W["seed"], targetParticles=s.targetParticles)
+    depthW = W["depth"]
+    Rlo = max(coreR * 0.55, W["R"] - 1.8889 * depthW)
+    o.load_terrain({"n": t["n"], "dv": 0.5, "solid": t["solid"], "R": t["R"], "Rsl": W["R"],
+                    "Rlo": Rlo, "Rhi": W["R"] + 0.7778 * depthW, "landFrac": t["landFrac"]})
+    o.alloc_particles(nP + 8192)
+    for k in ("px", "py", "pz", "pvx", "pvy", "pvz", "pT", "pAir", "pflag", "pcool"):
+        o.arr(k)[:nP] = fs.download(k)
+    o.arr("q")[:] = fs.q
+    o.set_scalars(nP=nP, oceanR=s.oceanR, spacing=s.spacing, particleVolume=s.particleVolume,
+                  gRamp=1.5, dtLast=DT, umax=s.umax)
+    o.L.or_build_planet_gravity(o.h)
+    o.set(**{k: v for k, v in PARAMS.items()}, sorRedBlack=0, viscJacobi=0, extrapJacobi=0)
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.substep(DT)
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or done >= 20:
+            break
+    return {"value": done / el, "unit": "substeps/s", "cores": 1, "kind": "port",
+            "sample": "%d whole substep(s) of the 128^3 planet (%d particles) in %.1f s, oracle "
+                      "(C restatement of js/solver.js, lexicographic SOR) on 1 host core" % (done, nP, el)}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU algorithm of js/solver.js (oracle port), one core."""
+    if rank != 0:
+        return None
+    from oracle.oracle import make_planet
+    W = WORKLOAD
+    o = make_planet(W["n"], R=W["R"], depth=W["depth"], seed=W["seed"], per_cell=W["per_cell"])
+    o.set(**PARAMS, sorRedBlack=0, viscJacobi=0, extrapJacobi=0)
+    o.set_scalars(gRamp=1.5)
+    nP = o.nP
+    warm = min(args.warmup, 1)
+    steps = max(1, min(args.steps, 3))
+    count = 0
+    for _ in range(warm):
+        if count % STIR_EVERY == 0:
+            o.stir_gaussian(STIR_SIGMA, STIR_PEAK)
+        o.substep(DT)
+        count += 1
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        if count % STIR_EVERY == 0:
+            o.stir_gaussian(STIR_SIGMA, STIR_PEAK)
+        o.substep(DT)
+        count += 1
+    el = time.perf_counter() - t0
+    v = steps / el
+    sample = ("%d substep(s) of the 128^3 planet (%d particles) after %d warm-up; C restatement of "
+              "js/solver.js (reference order), 1 core — no JavaScript engine on the host" % (steps, nP, warm))
+    return {"metric": METRIC, "value": v, "unit": "substeps/s", "n_gpus": world, "steps": steps,
+            "warmup": warm, "ms_per_step": 1000 * el / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic / f32 storage",
+            "data": "synthetic seeded planet", "impl": "reference",
+            "config": {"workload": "planet128: 128^3 MAC grid, R=52, depth 8, %d particles" % nP},
+            "cpu_baseline": {"value": v, "unit": "substeps/s", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    import torch
+    import datetime
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out, fs = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(fs, args.cpu_seconds)
+        print(json.dumps(out))
+    fs.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,219 @@
+/*
+ * watersim.h — C ABI of libwatersim.so, the B200 (sm_100a) implementation of
+ * WaterSim's FLIP/MAC substep.
+ *
+ * The boundary replaces the FluidSolver object of the reference
+ * (js/solver.js): its constructor options, public knobs, typed-array fields,
+ * step()/_substep() drivers and interaction helpers. Each entry point below
+ * names the reference interface it stands in for.
+ *
+ * Conventions
+ *  - Every call returns a ws_status: 0 = OK, negative = error. The message of
+ *    the last error on a handle is available from ws_last_error(). Nothing
+ *    aborts or traps; device-side faults (NaN, index out of range, a bounded
+ *    wait that ran out) are latched in a device status word and reported by
+ *    the next call that synchronises.
+ *  - Host pointers are owned by the caller and read or written only during
+ *    the call. Device memory is owned by the handle.
+ *  - One CUDA stream per handle; calls on one handle must be serialised by
+ *    the caller. There is no global mutable state, so different handles may
+ *    be used from different threads.
+ *  - Storage is float32 for particle and grid fields, uint8 for flags and
+ *    cell types — the layouts of the reference's typed arrays.
+ *  - Only the sphere-planet world (mode 'sphere' with voxel terrain) of the
+ *    reference is implemented; balls and subsurface currents are not.
+ */
+#ifndef WATERSIM_H
+#define WATERSIM_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t ws_status;
+#define WS_OK            0
+#define WS_ERR_INVALID  -1   /* bad argument or handle */
+#define WS_ERR_CUDA     -2   /* a CUDA runtime call failed */
+#define WS_ERR_NOMEM    -3   /* device or host allocation failed */
+#define WS_ERR_STATE    -4   /* call out of order (e.g. no terrain yet) */
+#define WS_ERR_DEVICE   -5   /* a kernel latched a fault (NaN, out of range) */
+#define WS_ERR_TIMEOUT  -6   /* a bounded device-side wait ran out */
+#define WS_ERR_RANGE    -7   /* size beyond a documented maximum */
+
+typedef struct ws_handle ws_handle;
+
+/* Grid and capacity — the FluidSolver constructor options nx, ny, nz, dx
+ * (js/solver.js:45-53) plus the particle capacity (_allocParticles,
+ * js/solver.js:218-231) and the CUDA device ordinal. */
+typedef struct {
+  int32_t nx, ny, nz;
+  int32_t capacity;       /* particle capacity */
+  double dx;
+  double coreR;           /* opts.coreR (js/solver.js:81) */
+  double bumpiness;       /* opts.bumpiness (js/solver.js:138) */
+  double targetParticles; /* opts.targetParticles (js/solver.js:75) */
+  uint32_t terrainSeed;   /* opts.terrainSeed (js/solver.js:137) */
+  int32_t device;
+} ws_config;
+
+/* Public knobs of FluidSolver (js/solver.js:55-193), copied on every
+ * ws_set_params. The last block selects solver strategy:
+ *   sorRedBlack  must be 1 (red-black SOR is the device order);
+ *   sorTol > 0   iterates to ||b - A q|| / ||b|| <= sorTol, FP64 residual
+ *                checked every sorCheckEvery iterations, at most sorMaxIters;
+ *                sorTol <= 0 runs pressureIters iterations like the reference;
+ *   viscJacobi / extrapJacobi must be 1 (the device order of the two
+ *                in-place passes of the reference). */
+typedef struct {
+  int32_t substeps;
+  int32_t pressureIters;
+  double cfl, pic, gravity, viscosity, omega, maxSpeed;
+  double vorticity, currents, shadeCool;
+  double sunActivity, evapIntensity, atmosphereH;
+  int32_t ceilReflect;     /* 0 'linear', 1 'quadratic', 2 'exponential' */
+  int32_t hasSun;          /* sunPos != null */
+  double sunPos[3];
+  double heatK, Tamb, cloudT, cloudP, rainT, rainLiftAge, snowT, meltT;
+  int32_t spinOn;
+  int32_t thermalOn;       /* run the ~25 Hz thermal tick and frame passes in ws_step */
+  int32_t sorRedBlack;
+  int32_t sorCheckEvery;
+  double sorTol;
+  int32_t sorMaxIters;
+  int32_t viscJacobi;
+  int32_t extrapJacobi;
+} ws_params;
+
+/* Scalar state and counters of FluidSolver (js/solver.js:81-214, RNG states
+ * :151-153), plus solve diagnostics. */
+typedef struct {
+  double coreR, oceanR, spacing, particleVolume, iso, waterTopY;
+  double umax, dtLast, simTime, gRamp, heatAcc;
+  double targetParticles, landFrac, bumpiness;
+  double sorRelRes;        /* FP64 relative residual after the last solve */
+  uint32_t evS, cfS, bfS, stirS;
+  uint32_t terrainSeed;
+  int32_t nP, capacity;
+  int32_t airborneCount, vaporCount, nightVaporCount, evapCount, substepsLast, nFluid;
+  int32_t sorIters;        /* iterations run by the last solve */
+  int32_t pad_;
+} ws_scalars;
+
+/* Named fields — the typed arrays of FluidSolver (js/solver.js:94-129). */
+typedef enum {
+  WS_F_PX = 0, WS_F_PY, WS_F_PZ, WS_F_PVX, WS_F_PVY, WS_F_PVZ,      /* float32, capacity */
+  WS_F_PT, WS_F_PAIR, WS_F_PLIGHT, WS_F_PWX, WS_F_PWY, WS_F_PWZ, WS_F_PPH,
+  WS_F_PFLAG, WS_F_PCOOL, WS_F_PDEPTH,                               /* uint8, capacity */
+  WS_F_CELLTYPE,                                                     /* uint8, nCells */
+  WS_F_Q,                                                            /* float32, nCells (cellPhi == q) */
+  WS_F_RHS,                                                          /* float32, nCells */
+  WS_F_U, WS_F_V, WS_F_W,                                            /* float32, uN / vN / wN */
+  WS_F_UO, WS_F_VO, WS_F_WO,                                         /* float32 snapshot */
+  WS_F_UW, WS_F_VW, WS_F_WW,                                         /* float32 P2G weights */
+  WS_F_VALIDU, WS_F_VALIDV, WS_F_VALIDW,                             /* uint8 */
+  WS_F_DENS,                                                         /* float32, (nx+1)(ny+1)(nz+1) */
+  WS_F_COUNT
+} ws_field;
+
+/* Terrain (the `terrain` object of generateTerrain, js/solver.js:499-504):
+ * voxel rock mask and radius field on an n^3 lattice of spacing dv. */
+typedef struct {
+  int32_t n;
+  double dv, Rsl, Rlo, Rhi, landFrac;
+  const uint8_t* solid;    /* n^3 */
+  const float* R;          /* n^3 */
+} ws_terrain;
+
+/* ---- lifetime: new FluidSolver(opts) (js/solver.js:45-216) */
+ws_status ws_create(const ws_config* cfg, ws_handle** out);
+ws_status ws_destroy(ws_handle* h);
+const char* ws_last_error(const ws_handle* h);
+const char* ws_version(void);
+
+/* ---- knobs: assignments to the public fields (js/solver.js:55-193) */
+ws_status ws_set_params(ws_handle* h, const ws_params* p);
+ws_status ws_get_params(const ws_handle* h, ws_params* p);
+ws_status ws_default_params(ws_params* p);
+ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s);
+ws_status ws_get_scalars(ws_handle* h, ws_scalars* s);
+
+/* ---- world setup: generateTerrain (js/solver.js:272-508) and
+ *      resetWater/_resetWaterSphere (js/solver.js:611-731); terrain can also
+ *      be supplied (the same `s.terrain` assignment the reference tests use) */
+ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double seaLevel);
+ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t);
+ws_status ws_download_terrain(ws_handle* h, uint8_t* solid, float* R, double meta[4]);
+ws_status ws_water_volume(ws_handle* h, double depth, double* volume);
+ws_status ws_reset_water(ws_handle* h, double depth);
+
+/* ---- field transfer: the typed arrays (js/solver.js:94-129). count is the
+ *      element count to copy from element 0; ws_set_nparticles sets nP. */
+ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host, int64_t count);
+ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count);
+ws_status ws_field_info(const ws_handle* h, ws_field f, int64_t* count, int32_t* elem_bytes);
+ws_status ws_set_nparticles(ws_handle* h, int32_t nP);
+
+/* ---- drivers: step(dtFrame) == _stepSync (js/solver.js:2663-2700) and
+ *      _substep(dt) (js/solver.js:2568-2624) */
+ws_status ws_step(ws_handle* h, double dtFrame);
+ws_status ws_substep(ws_handle* h, double dt);
+
+/* ---- single stages, for tests (the private methods the reference tests
+ *      call one at a time, test/phase.test.js, test/optimization.test.js).
+ *      Stage ids follow the substep order. */
+typedef enum {
+  WS_STAGE_CLEAR_RASTER = 0,  /* u..wW.fill(0) + _rasterizeStatic      :2569-2572, :865 */
+  WS_STAGE_MARK_FLUID,        /* _markFluidCells                        :945 */
+  WS_STAGE_P2G,               /* _p2g + _p2gNormalizeFace + _applyBC + snapshot  :1030-1171, :2579 */
+  WS_STAGE_FORCES,            /* _viscosity + _applyPlanetGravity + _applyBC     :1259, :2656, :1130 */
+  WS_STAGE_PRESSURE,          /* _pressureSolve                         :1312 */
+  WS_STAGE_PROJECT,           /* _project                               :1417 */
+  WS_STAGE_VORTICITY,         /* _vorticityConfinement                  :1454 */
+  WS_STAGE_CLAMP,             /* _clampUmSlice -> umax                  :2629 */
+  WS_STAGE_EXTRAPOLATE,       /* _extrapolate                           :1562 */
+  WS_STAGE_G2P_ADVECT,        /* _g2p + _advect                         :1639-2292 */
+  WS_STAGE_HEAT,              /* _updateHeat                            :2715 */
+  WS_STAGE_EVAPORATION,       /* _updateEvaporation                     :3008 */
+  WS_STAGE_PHASE,             /* _updatePhaseChanges                    :3152 */
+  WS_STAGE_PUSH_SURFACE,      /* _pushSurfaceParticles                  :3486 */
+  WS_STAGE_SPLAT,             /* splatDensity                           :3785 */
+  WS_STAGE_VAPOR_COLLISIONS,  /* _vaporCollisions                       :3345 */
+  WS_STAGE_ICE_CONTACTS,      /* _iceContacts                           :3290 */
+  WS_STAGE_COUNT
+} ws_stage_id;
+ws_status ws_stage(ws_handle* h, int32_t stage, double dt);
+
+/* ---- reductions (FP64 on the device) */
+ws_status ws_residual(ws_handle* h, double* relres);               /* ||b-Aq||/||b|| over fluid cells */
+ws_status ws_mt_volume(ws_handle* h, double iso, double* volume, int64_t* vertexCount);
+                                                                    /* MarchingTetrahedra.build volume, js/surface.js:66-177 */
+ws_status ws_autotune_iso(ws_handle* h, double* iso);              /* autotuneIso, js/solver.js:3838 */
+ws_status ws_census(ws_handle* h, double fractions[3]);            /* earthCensus, js/main.js:176 */
+ws_status ws_kinetic_energy(ws_handle* h, double* ke);             /* kineticEnergy, js/solver.js:3914 */
+
+/* ---- interactions (js/solver.js:3852-3908) and the seeded Gaussian stir
+ *      kick of the 128^3 planet workload (no reference counterpart) */
+ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy, double cz, double R,
+                                  double fx, double fy, double fz);
+ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, double vx, double vy,
+                     double vz, double R, double dt);
+ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak);
+
+/* ---- timing / synchronisation helpers */
+/* Times `reps` back-to-back launches of one kernel group on the handle's
+ * stream with CUDA events and returns the mean duration of one launch in
+ * microseconds. Runs on the current state (timing only; the state advances
+ * as if the kernels ran). kernel: 0 one red-black SOR iteration (two
+ * launches, reported per launch), 1 P2G scatter, 2 fused G2P + advection,
+ * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection. */
+ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us_per_launch);
+ws_status ws_synchronize(ws_handle* h);
+ws_status ws_get_stream(ws_handle* h, void** cuda_stream);
+ws_status ws_launch_count(ws_handle* h, int64_t* launches);        /* kernels this handle launched */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

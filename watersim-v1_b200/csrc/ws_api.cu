@@ -1,0 +1,862 @@
+// ws_api.cu — the C ABI of libwatersim (include/watersim.h): handle
+// lifetime, device memory, the substep and frame drivers, field transfer and
+// world setup. One CUDA stream per handle; no global mutable state.
+#include "ws_kernels.cuh"
+#include "ws_terrain.h"
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <new>
+
+struct ws_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Dims d{};
+  ws_params P{};
+  ws_scalars S{};
+  std::string err;
+  int capacity = 0;
+  long long launches = 0;
+  // grid
+  uint8_t *type = nullptr, *staticTypes = nullptr, *valid = nullptr, *diag8 = nullptr;
+  float *vel = nullptr, *velO = nullptr, *gvel = nullptr, *q = nullptr, *rhs = nullptr, *pw = nullptr;
+  float *vort = nullptr, *dens = nullptr;
+  float2* acc = nullptr;
+  // particles
+  PartsDev parts{};
+  // terrain
+  uint8_t* tsolid = nullptr;
+  float* tR = nullptr;
+  TerrainDev terr{};
+  wsterrain::Terrain hostTerrain;
+  bool hasTerrain = false;
+  // status, reductions, scratch
+  DevStatus* st = nullptr;
+  DevStatus* stHost = nullptr;          // pinned
+  double2* partials = nullptr;
+  int partialsCap = 0;
+  double* red = nullptr;                // device reduction outputs
+  double* redHost = nullptr;            // pinned
+  uint32_t* rng = nullptr;              // device: cfS, bfS, evS
+  int *blockCounts = nullptr, *list = nullptr, *listCount = nullptr;
+  uint8_t* cand = nullptr;
+  int* cellCnt = nullptr;
+  double *cellSum = nullptr, *cellChange = nullptr;
+  void* contactScratch = nullptr;       // allocated on first contact pass
+  bool vaporPossible = false;
+  double oceanRGeom = -1;               // oceanR the gravity geometry was built for
+};
+
+static float bits_to_float(unsigned u) { float f; std::memcpy(&f, &u, sizeof(f)); return f; }
+
+#define WS_TRY(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return fail_cuda(h, e_, #call); } while (0)
+
+static ws_status fail(ws_handle* h, ws_status code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+static ws_status fail_cuda(ws_handle* h, cudaError_t e, const char* what) {
+  return fail(h, WS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+static ws_status check_launch(ws_handle* h, int n) {
+  h->launches += n;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail_cuda(h, e, "kernel launch");
+  return WS_OK;
+}
+
+static GridDev grid_of(ws_handle* h) {
+  GridDev g;
+  g.type = h->type; g.staticTypes = h->staticTypes; g.vel = h->vel; g.velO = h->velO; g.acc = h->acc;
+  g.valid = h->valid; g.gvel = h->gvel; g.q = h->q; g.rhs = h->rhs; g.pw = h->pw;
+  long long N = h->d.nCells;
+  g.vfx = h->vort; g.vfy = h->vort + N; g.vfz = h->vort + 2 * N; g.omg = h->vort + 3 * N;
+  g.omx = h->vort + 4 * N; g.omy = h->vort + 5 * N; g.omz = h->vort + 6 * N;
+  g.dens = h->dens;
+  return g;
+}
+static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; return P; }
+
+extern "C" const char* ws_version(void) { return "watersim-b200 0.1 (sm_100a)"; }
+
+extern "C" const char* ws_last_error(const ws_handle* h) {
+  if (!h) return "null handle";
+  return h->err.c_str();
+}
+
+extern "C" ws_status ws_default_params(ws_params* p) {
+  if (!p) return WS_ERR_INVALID;
+  std::memset(p, 0, sizeof(*p));
+  // library defaults of FluidSolver, js/solver.js:56-193
+  p->substeps = 1; p->cfl = 3.0; p->pic = 0.15; p->gravity = 9.81; p->viscosity = 5e-4;
+  p->pressureIters = 20; p->omega = 1.55; p->maxSpeed = 3.2;
+  p->vorticity = 0; p->currents = 0; p->shadeCool = 0.035;
+  p->sunActivity = 0; p->evapIntensity = 0.05; p->atmosphereH = 0.35; p->ceilReflect = 0;
+  p->hasSun = 0; p->heatK = 0.6; p->Tamb = 0.32;
+  p->cloudT = 0.34; p->cloudP = 0.35; p->rainT = 0.22; p->rainLiftAge = 0.4; p->snowT = 0.10;
+  p->meltT = 0.10 * 1.05; p->spinOn = 0; p->thermalOn = 1;
+  // device order of the order-dependent passes
+  p->sorRedBlack = 1; p->sorCheckEvery = 10; p->sorTol = 0; p->sorMaxIters = 10000;
+  p->viscJacobi = 1; p->extrapJacobi = 1;
+  return WS_OK;
+}
+
+static void free_all(ws_handle* h) {
+  void* bufs[] = { h->type, h->staticTypes, h->valid, h->diag8, h->vel, h->velO, h->gvel, h->q, h->rhs, h->pw,
+                   h->vort, h->dens, h->acc, h->tsolid, h->tR, h->st, h->partials, h->red, h->rng,
+                   h->blockCounts, h->list, h->listCount, h->cand, h->cellCnt, h->cellSum, h->cellChange,
+                   h->parts.px, h->parts.py, h->parts.pz, h->parts.pvx, h->parts.pvy, h->parts.pvz, h->parts.pT,
+                   h->parts.pAir, h->parts.pLight, h->parts.pWx, h->parts.pWy, h->parts.pWz, h->parts.pPh,
+                   h->parts.pflag, h->parts.pcool, h->parts.pDepth };
+  for (void* b : bufs) if (b) cudaFree(b);
+  if (h->contactScratch) cudaFree(h->contactScratch);
+  if (h->stHost) cudaFreeHost(h->stHost);
+  if (h->redHost) cudaFreeHost(h->redHost);
+  if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+  if (e == cudaSuccess) e = cudaMemset(*p, 0, sizeof(T) * (count ? count : 1));
+  return e;
+}
+
+extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
+  if (!cfg || !out) return WS_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->nx < 4 || cfg->ny < 4 || cfg->nz < 4 || !(cfg->dx > 0) || cfg->capacity < 1) return WS_ERR_INVALID;
+  if ((long long)cfg->nx * cfg->ny * cfg->nz > (1LL << 31) / 4) return WS_ERR_RANGE;
+  ws_handle* h = new (std::nothrow) ws_handle();
+  if (!h) return WS_ERR_NOMEM;
+  h->device = cfg->device;
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaSetDevice"); delete h; return r; }
+  e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaStreamCreate"); delete h; return r; }
+  Dims& d = h->d;
+  d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.dx = cfg->dx;
+  d.W = d.nx * d.dx; d.H = d.ny * d.dx; d.D = d.nz * d.dx;
+  d.cx = d.W / 2; d.cy = d.H / 2; d.cz = d.D / 2;
+  d.domainR = 0.5 * std::min(std::min(d.W, d.H), d.D) - d.dx;
+  d.nCells = (long long)d.nx * d.ny * d.nz;
+  d.uN = (long long)(d.nx + 1) * d.ny * d.nz; d.vN = (long long)d.nx * (d.ny + 1) * d.nz;
+  d.wN = (long long)d.nx * d.ny * (d.nz + 1); d.F = d.uN + d.vN + d.wN;
+  h->capacity = cfg->capacity;
+  ws_default_params(&h->P);
+  ws_scalars& S = h->S;
+  S.coreR = cfg->coreR; S.spacing = d.dx * 0.5; S.particleVolume = S.spacing * S.spacing * S.spacing;
+  S.iso = 1.8; S.waterTopY = d.dx + 1; S.gRamp = 1e9;
+  S.evS = 0x51ab3c77u; S.cfS = 0x2f6e2b1u; S.bfS = 0x7f4a7c15u; S.stirS = 0x2545f491u;
+  S.terrainSeed = cfg->terrainSeed ? cfg->terrainSeed : 20260114u;
+  S.bumpiness = cfg->bumpiness < 0 ? 0 : (cfg->bumpiness > 2.5 ? 2.5 : cfg->bumpiness);
+  S.targetParticles = cfg->targetParticles > 0 ? cfg->targetParticles : 110000;
+  S.capacity = cfg->capacity;
+  long long N = d.nCells, F = d.F, P = cfg->capacity;
+  long long ND = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+#define AL(ptr, n) if ((e = dalloc(&(ptr), (size_t)(n))) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
+  AL(h->type, N) AL(h->staticTypes, N) AL(h->diag8, N) AL(h->valid, F)
+  AL(h->vel, F) AL(h->velO, F) AL(h->gvel, F) AL(h->acc, F)
+  AL(h->q, N) AL(h->rhs, N) AL(h->pw, N) AL(h->vort, 7 * N) AL(h->dens, ND)
+  AL(h->st, 1) AL(h->red, 8) AL(h->rng, 4)
+  AL(h->cellCnt, N) AL(h->cellSum, N) AL(h->cellChange, N)
+  PartsDev& pp = h->parts;
+  AL(pp.px, P) AL(pp.py, P) AL(pp.pz, P) AL(pp.pvx, P) AL(pp.pvy, P) AL(pp.pvz, P)
+  AL(pp.pT, P) AL(pp.pAir, P) AL(pp.pLight, P) AL(pp.pWx, P) AL(pp.pWy, P) AL(pp.pWz, P) AL(pp.pPh, P)
+  AL(pp.pflag, P) AL(pp.pcool, P) AL(pp.pDepth, P)
+  long long nb = (P + 255) / 256 + 1;
+  AL(h->blockCounts, nb) AL(h->list, P) AL(h->listCount, 1) AL(h->cand, P)
+  long long partN = std::max((long long)grid_for(N, 128) + 1, (long long)(3 * nb));
+  AL(h->partials, partN)
+  h->partialsCap = (int)partN;
+#undef AL
+  if ((e = cudaMallocHost(&h->stHost, sizeof(DevStatus))) != cudaSuccess ||
+      (e = cudaMallocHost(&h->redHost, sizeof(double) * 8)) != cudaSuccess) {
+    ws_status r = fail_cuda(h, e, "cudaMallocHost"); free_all(h); delete h; return r;
+  }
+  std::memset(h->stHost, 0, sizeof(DevStatus));
+  uint32_t rng0[4] = { S.cfS, S.bfS, S.evS, 0 };
+  cudaMemcpy(h->rng, rng0, sizeof(rng0), cudaMemcpyHostToDevice);
+  // static types without terrain (the shell only) until a terrain arrives
+  h->terr = TerrainDev{}; h->terr.has = 0;
+  launch_static_types(d, h->terr, S.coreR, h->staticTypes, h->stream);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) { ws_status r = fail_cuda(h, e, "init"); free_all(h); delete h; return r; }
+  *out = h;
+  return WS_OK;
+}
+
+extern "C" ws_status ws_destroy(ws_handle* h) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return WS_OK;
+}
+
+extern "C" ws_status ws_set_params(ws_handle* h, const ws_params* p) {
+  if (!h || !p) return WS_ERR_INVALID;
+  if (!p->sorRedBlack || !p->viscJacobi || !p->extrapJacobi)
+    return fail(h, WS_ERR_INVALID, "the device path runs red-black SOR and Jacobi viscosity/extrapolation "
+                                   "(sorRedBlack, viscJacobi and extrapJacobi must be 1)");
+  if (p->currents > 0) return fail(h, WS_ERR_INVALID, "subsurface currents are not implemented (currents must be 0)");
+  h->P = *p;
+  return WS_OK;
+}
+extern "C" ws_status ws_get_params(const ws_handle* h, ws_params* p) {
+  if (!h || !p) return WS_ERR_INVALID;
+  *p = h->P;
+  return WS_OK;
+}
+
+static ws_status sync_status(ws_handle* h) {
+  WS_TRY(cudaMemcpyAsync(h->stHost, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (h->stHost->err) {
+    int ebits = h->stHost->err;
+    cudaMemsetAsync(&h->st->err, 0, sizeof(int), h->stream);
+    if (ebits & WS_DERR_TIMEOUT) return fail(h, WS_ERR_TIMEOUT, "a bounded device wait ran out");
+    return fail(h, WS_ERR_DEVICE, "device fault latched (NaN or index out of range)");
+  }
+  return WS_OK;
+}
+
+static ws_status ensure_gravity(ws_handle* h) {
+  if (h->oceanRGeom != h->S.oceanR) {
+    launch_gravity_geometry(h->d, h->S.oceanR, h->gvel, h->stream);
+    h->oceanRGeom = h->S.oceanR;
+    return check_launch(h, 1);
+  }
+  return WS_OK;
+}
+
+extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
+  if (!h || !s) return WS_ERR_INVALID;
+  uint32_t rng[4];
+  WS_TRY(cudaMemcpyAsync(rng, h->rng, sizeof(rng), cudaMemcpyDeviceToHost, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  h->S.cfS = rng[0]; h->S.bfS = rng[1]; h->S.evS = rng[2];
+  *s = h->S;
+  return WS_OK;
+}
+extern "C" ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s) {
+  if (!h || !s) return WS_ERR_INVALID;
+  if (s->nP < 0 || s->nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
+  int cap = h->capacity;
+  h->S = *s;
+  h->S.capacity = cap;
+  uint32_t rng[4] = { s->cfS, s->bfS, s->evS, 0 };
+  WS_TRY(cudaMemcpyAsync(h->rng, rng, sizeof(rng), cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return ensure_gravity(h);
+}
+extern "C" ws_status ws_set_nparticles(ws_handle* h, int32_t nP) {
+  if (!h) return WS_ERR_INVALID;
+  if (nP < 0 || nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
+  h->S.nP = nP;
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ fields
+struct FieldRef { void* ptr; long long count; int elem; int kind; };   // kind 1: weights view, 2: valid view
+static bool field_ref(ws_handle* h, ws_field f, FieldRef& r) {
+  const Dims& d = h->d; PartsDev& p = h->parts; long long P = h->capacity;
+  long long ND = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  r.kind = 0;
+  switch (f) {
+    case WS_F_PX: r = {p.px, P, 4, 0}; return true;
+    case WS_F_PY: r = {p.py, P, 4, 0}; return true;
+    case WS_F_PZ: r = {p.pz, P, 4, 0}; return true;
+    case WS_F_PVX: r = {p.pvx, P, 4, 0}; return true;
+    case WS_F_PVY: r = {p.pvy, P, 4, 0}; return true;
+    case WS_F_PVZ: r = {p.pvz, P, 4, 0}; return true;
+    case WS_F_PT: r = {p.pT, P, 4, 0}; return true;
+    case WS_F_PAIR: r = {p.pAir, P, 4, 0}; return true;
+    case WS_F_PLIGHT: r = {p.pLight, P, 4, 0}; return true;
+    case WS_F_PWX: r = {p.pWx, P, 4, 0}; return true;
+    case WS_F_PWY: r = {p.pWy, P, 4, 0}; return true;
+    case WS_F_PWZ: r = {p.pWz, P, 4, 0}; return true;
+    case WS_F_PPH: r = {p.pPh, P, 4, 0}; return true;
+    case WS_F_PFLAG: r = {p.pflag, P, 1, 0}; return true;
+    case WS_F_PCOOL: r = {p.pcool, P, 1, 0}; return true;
+    case WS_F_PDEPTH: r = {p.pDepth, P, 1, 0}; return true;
+    case WS_F_CELLTYPE: r = {h->type, d.nCells, 1, 0}; return true;
+    case WS_F_Q: r = {h->q, d.nCells, 4, 0}; return true;
+    case WS_F_RHS: r = {h->rhs, d.nCells, 4, 0}; return true;
+    case WS_F_U: r = {h->vel, d.uN, 4, 0}; return true;
+    case WS_F_V: r = {h->vel + d.uN, d.vN, 4, 0}; return true;
+    case WS_F_W: r = {h->vel + d.uN + d.vN, d.wN, 4, 0}; return true;
+    case WS_F_UO: r = {h->velO, d.uN, 4, 0}; return true;
+    case WS_F_VO: r = {h->velO + d.uN, d.vN, 4, 0}; return true;
+    case WS_F_WO: r = {h->velO + d.uN + d.vN, d.wN, 4, 0}; return true;
+    case WS_F_UW: r = {(void*)0, d.uN, 4, 1}; return true;
+    case WS_F_VW: r = {(void*)d.uN, d.vN, 4, 1}; return true;
+    case WS_F_WW: r = {(void*)(d.uN + d.vN), d.wN, 4, 1}; return true;
+    case WS_F_VALIDU: r = {h->valid, d.uN, 1, 2}; return true;
+    case WS_F_VALIDV: r = {h->valid + d.uN, d.vN, 1, 2}; return true;
+    case WS_F_VALIDW: r = {h->valid + d.uN + d.vN, d.wN, 1, 2}; return true;
+    case WS_F_DENS: r = {h->dens, ND, 4, 0}; return true;
+    default: return false;
+  }
+}
+extern "C" ws_status ws_field_info(const ws_handle* hc, ws_field f, int64_t* count, int32_t* elem) {
+  ws_handle* h = const_cast<ws_handle*>(hc);
+  if (!h) return WS_ERR_INVALID;
+  FieldRef r;
+  if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
+  if (count) *count = r.count;
+  if (elem) *elem = r.elem;
+  return WS_OK;
+}
+extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host, int64_t count) {
+  if (!h || (!host && count)) return WS_ERR_INVALID;
+  FieldRef r;
+  if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
+  if (count < 0 || count > r.count) return fail(h, WS_ERR_RANGE, "count exceeds the field size");
+  if (r.kind != 0) return fail(h, WS_ERR_INVALID, "derived field is read-only");
+  WS_TRY(cudaMemcpyAsync(r.ptr, host, (size_t)count * r.elem, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (f == WS_F_PFLAG) {
+    const uint8_t* fl = (const uint8_t*)host;
+    for (int64_t i = 0; i < count; i++) if (fl[i] == 2 || fl[i] == 3) { h->vaporPossible = true; break; }
+  }
+  return WS_OK;
+}
+extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count) {
+  if (!h || (!host && count)) return WS_ERR_INVALID;
+  FieldRef r;
+  if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
+  if (count < 0 || count > r.count) return fail(h, WS_ERR_RANGE, "count exceeds the field size");
+  if (r.kind == 1) {
+    float* tmp = (float*)h->cellChange;                   // 8 N bytes >= 4 * (component face count)
+    if ((long long)count * 4 > h->d.nCells * 8) return fail(h, WS_ERR_RANGE, "weights view too large");
+    launch_extract_weight(h->d, h->acc, tmp, (long long)(size_t)r.ptr, count, h->stream);
+    ws_status s = check_launch(h, 1); if (s) return s;
+    WS_TRY(cudaMemcpyAsync(host, tmp, (size_t)count * 4, cudaMemcpyDeviceToHost, h->stream));
+  } else {
+    WS_TRY(cudaMemcpyAsync(host, r.ptr, (size_t)count * r.elem, cudaMemcpyDeviceToHost, h->stream));
+  }
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (r.kind == 2) { uint8_t* v = (uint8_t*)host; for (int64_t i = 0; i < count; i++) if (v[i] == 2) v[i] = 1; }
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ terrain + fill
+static ws_status terrain_to_device(ws_handle* h) {
+  const wsterrain::Terrain& T = h->hostTerrain;
+  long long n3 = (long long)T.n * T.n * T.n;
+  if (h->tsolid) { cudaFree(h->tsolid); h->tsolid = nullptr; }
+  if (h->tR) { cudaFree(h->tR); h->tR = nullptr; }
+  WS_TRY(cudaMalloc(&h->tsolid, (size_t)n3));
+  WS_TRY(cudaMalloc(&h->tR, sizeof(float) * (size_t)n3));
+  WS_TRY(cudaMemcpyAsync(h->tsolid, T.solid.data(), (size_t)n3, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaMemcpyAsync(h->tR, T.R.data(), sizeof(float) * (size_t)n3, cudaMemcpyHostToDevice, h->stream));
+  TerrainDev& t = h->terr;
+  t.n = T.n; t.has = 1; t.dv = T.dv; t.Rsl = T.Rsl; t.Rlo = T.Rlo; t.Rhi = T.Rhi;
+  t.Rlo2 = T.Rlo * T.Rlo; t.Rhi2 = T.Rhi * T.Rhi; t.solid = h->tsolid; t.R = h->tR;
+  h->S.landFrac = T.landFrac;
+  h->hasTerrain = true;
+  launch_static_types(h->d, t, h->S.coreR, h->staticTypes, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}
+
+extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double seaLevel) {
+  if (!h) return WS_ERR_INVALID;
+  wsterrain::GenInput in{seed, h->S.coreR, seaLevel, h->S.bumpiness, h->d.dx, h->d.cx, h->d.cy, h->d.cz, h->d.nx, h->stream};
+  int r = wsterrain::generate(in, h->hostTerrain, h->err);
+  if (r) return r;
+  h->launches += 1;
+  return terrain_to_device(h);
+}
+
+extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
+  if (!h || !t || t->n < 2 || !t->solid || !t->R) return WS_ERR_INVALID;
+  wsterrain::Terrain& T = h->hostTerrain;
+  long long n3 = (long long)t->n * t->n * t->n;
+  T.n = t->n; T.dv = t->dv; T.Rsl = t->Rsl; T.Rlo = t->Rlo; T.Rhi = t->Rhi; T.landFrac = t->landFrac;
+  T.solid.assign(t->solid, t->solid + n3);
+  T.R.assign(t->R, t->R + n3);
+  return terrain_to_device(h);
+}
+
+extern "C" ws_status ws_download_terrain(ws_handle* h, uint8_t* solid, float* R, double meta[4]) {
+  if (!h) return WS_ERR_INVALID;
+  if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
+  const wsterrain::Terrain& T = h->hostTerrain;
+  size_t n3 = (size_t)T.n * T.n * T.n;
+  if (solid) std::memcpy(solid, T.solid.data(), n3);
+  if (R) std::memcpy(R, T.R.data(), n3 * sizeof(float));
+  if (meta) { meta[0] = T.n; meta[1] = T.Rlo; meta[2] = T.Rhi; meta[3] = T.landFrac; }
+  return WS_OK;
+}
+
+static wsterrain::FillInput fill_input(ws_handle* h, double depth) {
+  wsterrain::FillInput in;
+  in.seed = h->S.terrainSeed; in.nx = h->d.nx; in.ny = h->d.ny; in.nz = h->d.nz;
+  in.dx = h->d.dx; in.cx = h->d.cx; in.cy = h->d.cy; in.cz = h->d.cz;
+  in.coreR = h->S.coreR; in.depth = depth; in.targetParticles = h->S.targetParticles; in.capacity = h->capacity;
+  return in;
+}
+
+extern "C" ws_status ws_water_volume(ws_handle* h, double depth, double* volume) {
+  if (!h || !volume) return WS_ERR_INVALID;
+  if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
+  *volume = wsterrain::water_volume(h->hostTerrain, fill_input(h, depth));
+  return WS_OK;
+}
+
+static ws_status splat_and_iso(ws_handle* h);
+
+// _resetWaterSphere, js/solver.js:651-731
+extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
+  if (!h) return WS_ERR_INVALID;
+  double R2 = h->S.coreR + depth;
+  h->S.oceanR = R2;
+  if (!h->hasTerrain) { ws_status s = ws_generate_terrain(h, h->S.terrainSeed, R2); if (s) return s; }
+  wsterrain::FillOutput fo;
+  wsterrain::fill(h->hostTerrain, fill_input(h, depth), fo);
+  int n = (int)fo.px.size();
+  h->S.spacing = fo.spacing; h->S.particleVolume = fo.spacing * fo.spacing * fo.spacing;
+  PartsDev& p = h->parts;
+  size_t P = (size_t)h->capacity;
+  WS_TRY(cudaMemcpyAsync(p.px, fo.px.data(), sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaMemcpyAsync(p.py, fo.py.data(), sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaMemcpyAsync(p.pz, fo.pz.data(), sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pvx, 0, sizeof(float) * n, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pvy, 0, sizeof(float) * n, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pvz, 0, sizeof(float) * n, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pflag, 0, (size_t)n, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pcool, 0, (size_t)n, h->stream));
+  WS_TRY(cudaMemsetAsync(p.pAir, 0, sizeof(float) * P, h->stream));
+  std::vector<float> tamb((size_t)n, (float)h->P.Tamb);
+  WS_TRY(cudaMemcpyAsync(p.pT, tamb.data(), sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaMemsetAsync(h->q, 0, sizeof(float) * h->d.nCells, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  h->S.nP = n;
+  h->S.heatAcc = 0; h->S.vaporCount = h->S.nightVaporCount = 0;
+  h->S.waterTopY = h->d.cy + R2;
+  h->vaporPossible = false;
+  ws_status s = ensure_gravity(h); if (s) return s;
+  h->S.gRamp = 0;
+  s = splat_and_iso(h); if (s) return s;
+  h->S.umax = 0; h->S.airborneCount = 0;
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ reductions
+static ws_status mt_volume(ws_handle* h, double iso, double* vol, int64_t* cnt) {
+  if ((long long)grid_for(h->d.nCells, 128) > h->partialsCap) return fail(h, WS_ERR_RANGE, "partials too small");
+  launch_mt_volume(h->d, h->dens, iso, h->partials, h->red, h->stream);
+  ws_status s = check_launch(h, 2); if (s) return s;
+  WS_TRY(cudaMemcpyAsync(h->redHost, h->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (vol) *vol = std::fabs(h->redHost[0]);
+  if (cnt) *cnt = (int64_t)llround(h->redHost[1]);
+  return WS_OK;
+}
+extern "C" ws_status ws_mt_volume(ws_handle* h, double iso, double* volume, int64_t* vertexCount) {
+  if (!h) return WS_ERR_INVALID;
+  return mt_volume(h, iso, volume, vertexCount);
+}
+// autotuneIso, js/solver.js:3838-3849
+static ws_status autotune(ws_handle* h, double* iso) {
+  double Vt = h->S.nP * h->S.particleVolume, lo = 0.3, hi = 3.0;
+  for (int it = 0; it < 8; it++) {
+    double mid = 0.5 * (lo + hi), vol; int64_t cnt;
+    ws_status s = mt_volume(h, mid, &vol, &cnt); if (s) return s;
+    if (cnt > 900000 || vol > Vt) lo = mid; else hi = mid;
+  }
+  *iso = 0.5 * (lo + hi);
+  return WS_OK;
+}
+extern "C" ws_status ws_autotune_iso(ws_handle* h, double* iso) {
+  if (!h || !iso) return WS_ERR_INVALID;
+  return autotune(h, iso);
+}
+static ws_status splat_and_iso(ws_handle* h) {
+  launch_splat(h->d, grid_of(h), parts_of(h), h->S.spacing, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  double iso;
+  s = autotune(h, &iso); if (s) return s;
+  h->S.iso = iso;
+  return WS_OK;
+}
+static ws_status particle_reduce(ws_handle* h, int mode, double mp, double out[3]) {
+  launch_particle_reduce(parts_of(h), mode, mp, (double*)h->partials, h->red, h->stream);
+  ws_status s = check_launch(h, 2); if (s) return s;
+  WS_TRY(cudaMemcpyAsync(h->redHost, h->red, sizeof(double) * 3, cudaMemcpyDeviceToHost, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  out[0] = h->redHost[0]; out[1] = h->redHost[1]; out[2] = h->redHost[2];
+  return WS_OK;
+}
+extern "C" ws_status ws_kinetic_energy(ws_handle* h, double* ke) {
+  if (!h || !ke) return WS_ERR_INVALID;
+  double o[3];
+  ws_status s = particle_reduce(h, 0, 1000 * h->S.particleVolume, o); if (s) return s;
+  *ke = o[0];
+  return WS_OK;
+}
+// earthCensus, js/main.js:176-186: counts are exact, fractions in FP64
+extern "C" ws_status ws_census(ws_handle* h, double fr[3]) {
+  if (!h || !fr) return WS_ERR_INVALID;
+  double o[3];
+  ws_status s = particle_reduce(h, 1, 0, o); if (s) return s;
+  double tot = o[0] + o[1] + o[2];
+  if (tot > 0) { fr[0] = o[0] / tot; fr[1] = o[1] / tot; fr[2] = o[2] / tot; } else fr[0] = fr[1] = fr[2] = 0;
+  return WS_OK;
+}
+extern "C" ws_status ws_residual(ws_handle* h, double* relres) {
+  if (!h || !relres) return WS_ERR_INVALID;
+  launch_residual(h->d, grid_of(h), h->diag8, h->partials, h->st, nullptr, h->stream);
+  ws_status s = check_launch(h, 2); if (s) return s;
+  s = sync_status(h); if (s) return s;
+  *relres = h->stHost->relres;
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ substep stages
+static AdvectParams advect_params(ws_handle* h, double dt) {
+  AdvectParams a;
+  a.dt = dt; a.dtLast = h->S.dtLast; a.pic = h->P.pic; a.maxSpeed = h->P.maxSpeed; a.gravity = h->P.gravity;
+  a.oceanR = h->S.oceanR; a.coreR = h->S.coreR; a.atmosphereH = h->P.atmosphereH;
+  double rainTe = std::min(h->P.rainT, h->P.cloudT - 0.02); if (rainTe < 0) rainTe = 0;
+  a.rainTe = rainTe; a.rainLiftAge = h->P.rainLiftAge; a.ceilReflect = h->P.ceilReflect;
+  a.windS[0] = 1; a.windS[1] = 0; a.windS[2] = 0;
+  if (h->P.hasSun) {
+    double sx = h->P.sunPos[0] - h->d.cx, sy = h->P.sunPos[1] - h->d.cy, sz = h->P.sunPos[2] - h->d.cz;
+    double L = std::sqrt(sx * sx + sy * sy + sz * sz); if (L == 0) L = 1;
+    a.windS[0] = sx / L; a.windS[1] = sy / L; a.windS[2] = sz / L;
+  }
+  return a;
+}
+
+static ws_status stage_clear_raster(ws_handle* h) {
+  launch_clear_raster(h->d, grid_of(h), h->st, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_mark(ws_handle* h) {
+  launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_p2g(ws_handle* h) {
+  launch_p2g(h->d, grid_of(h), parts_of(h), h->stream);
+  launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
+  return check_launch(h, 2);
+}
+static ws_status stage_forces(ws_handle* h, double dt) {
+  ws_status s = ensure_gravity(h); if (s) return s;
+  double nu = h->P.viscosity;
+  double coef = std::min(nu * dt / (h->d.dx * h->d.dx), 0.24);
+  int viscOn = nu > 1e-6;
+  // planet gravity ramp, js/solver.js:2656-2662
+  double gs = h->S.gRamp / 1.5; if (gs > 1) gs = 1;
+  h->S.gRamp += dt;
+  double gsA = gs > 0 ? gs * h->P.gravity : 0;
+  launch_faces_forces(h->d, grid_of(h), coef, viscOn, dt, gsA, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_pressure(ws_handle* h) {
+  GridDev g = grid_of(h);
+  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  double om1 = 1 - h->P.omega;
+  bool tolMode = h->P.sorTol > 0;
+  int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
+  int check = h->P.sorCheckEvery > 0 ? h->P.sorCheckEvery : 1;
+  int it = 0;
+  for (it = 0; it < iters; ) {
+    launch_sor_color(h->d, g, 0, om1, h->stream);
+    launch_sor_color(h->d, g, 1, om1, h->stream);
+    it++;
+    s = check_launch(h, 2); if (s) return s;
+    if (tolMode && it % check == 0) {
+      launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
+      s = check_launch(h, 2); if (s) return s;
+      s = sync_status(h); if (s) return s;
+      if (h->stHost->relres <= h->P.sorTol) break;
+    }
+  }
+  h->S.sorIters = it;
+  launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
+  s = check_launch(h, 2); if (s) return s;
+  s = sync_status(h); if (s) return s;
+  h->S.sorRelRes = h->stHost->relres;
+  h->S.nFluid = h->stHost->nFluid;
+  return WS_OK;
+}
+static ws_status stage_project(ws_handle* h, bool clampToo) {
+  launch_project(h->d, grid_of(h), clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_vorticity(ws_handle* h, double dt) {
+  if (!(h->P.vorticity > 0)) return WS_OK;
+  launch_vorticity(h->d, grid_of(h), h->P.vorticity, dt, h->stream);
+  return check_launch(h, 3);
+}
+static ws_status stage_clamp(ws_handle* h) {
+  launch_clamp_umax(h->d, grid_of(h), h->P.maxSpeed, h->st, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_extrapolate(ws_handle* h) {
+  launch_extrapolate(h->d, grid_of(h), h->stream);
+  return check_launch(h, 1);
+}
+static ws_status stage_g2p_advect(ws_handle* h, double dt) {
+  AdvectParams ap = advect_params(h, dt);
+  launch_g2p_advect(h->d, grid_of(h), parts_of(h), h->terr, ap, h->st, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  if (h->vaporPossible && h->S.nP > 0) {
+    launch_compact(h->parts.pflag, h->S.nP, 0, h->blockCounts, h->list, h->listCount, h->stream);
+    launch_vapor_advect(h->d, grid_of(h), parts_of(h), h->terr, ap, h->list, h->listCount, h->rng, h->st, h->stream);
+    s = check_launch(h, 4); if (s) return s;
+  }
+  return WS_OK;
+}
+
+// _substep, js/solver.js:2568-2624
+static ws_status substep(ws_handle* h, double dt) {
+  ws_status s;
+  if ((s = stage_clear_raster(h))) return s;
+  if ((s = stage_mark(h))) return s;
+  if ((s = stage_p2g(h))) return s;
+  if ((s = stage_forces(h, dt))) return s;
+  if ((s = stage_pressure(h))) return s;
+  bool vort = h->P.vorticity > 0;
+  if ((s = stage_project(h, !vort))) return s;
+  if (vort) { if ((s = stage_vorticity(h, dt))) return s; if ((s = stage_clamp(h))) return s; }
+  if ((s = stage_extrapolate(h))) return s;
+  if ((s = stage_g2p_advect(h, dt))) return s;
+  if ((s = sync_status(h))) return s;
+  h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
+  h->S.airborneCount = h->stHost->airborne;
+  h->S.dtLast = dt;
+  return WS_OK;
+}
+
+extern "C" ws_status ws_substep(ws_handle* h, double dt) {
+  if (!h || !(dt > 0)) return WS_ERR_INVALID;
+  if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain: call ws_generate_terrain or ws_upload_terrain");
+  cudaSetDevice(h->device);
+  return substep(h, dt);
+}
+
+// ------------------------------------------------------------ frame passes
+static ws_status heat(ws_handle* h, double dt) {
+  HeatParams hp;
+  hp.hasSun = h->P.hasSun; hp.sun[0] = h->P.sunPos[0]; hp.sun[1] = h->P.sunPos[1]; hp.sun[2] = h->P.sunPos[2];
+  hp.sunActivity = h->P.sunActivity; hp.Tamb = h->P.Tamb; hp.shadeCool = h->P.shadeCool; hp.heatK = h->P.heatK;
+  hp.coreR = h->S.coreR;
+  launch_heat(h->d, grid_of(h), parts_of(h), h->terr, hp, dt, h->cellCnt, h->cellSum, h->cellChange, h->stream);
+  return check_launch(h, hp.heatK > 0 ? 5 : 2);
+}
+static ws_status evaporation(ws_handle* h, double dt) {
+  if (h->P.sunActivity <= 0 || h->P.evapIntensity <= 0) return WS_OK;
+  double freezeT = std::max(h->P.meltT, h->P.snowT * 1.05);
+  double rate = h->P.sunActivity * h->P.evapIntensity;
+  launch_evaporation(h->d, grid_of(h), parts_of(h), freezeT, rate, dt, h->cand, h->blockCounts, h->list,
+                     h->listCount, h->rng + 2, h->st, h->stream);
+  ws_status s = check_launch(h, 5); if (s) return s;
+  s = sync_status(h); if (s) return s;
+  h->S.evapCount = h->stHost->evapCount;
+  if (h->S.evapCount > 0) h->vaporPossible = true;
+  return WS_OK;
+}
+static ws_status phase(ws_handle* h, double dt) {
+  PhaseParams pp;
+  double cloudT = h->P.cloudT;
+  double rainT = std::min(h->P.rainT, cloudT - 0.02); if (rainT < 0) rainT = 0;
+  double snowT = std::min(h->P.snowT, rainT - 0.02); if (snowT < 0) snowT = 0;
+  pp.cloudT = cloudT; pp.cloudP = h->P.cloudP; pp.rainT = rainT; pp.snowT = snowT;
+  pp.meltT = h->P.meltT > snowT * 1.05 ? h->P.meltT : snowT * 1.05;
+  pp.rainLiftAge = h->P.rainLiftAge; pp.cloudBase = h->S.oceanR + 0.3 * h->P.atmosphereH;
+  pp.dt = dt; pp.spinOn = h->P.spinOn; pp.tick = (uint32_t)(int)(h->S.simTime * 60);
+  launch_phase(h->d, grid_of(h), parts_of(h), pp, h->cellCnt, h->stream);
+  return check_launch(h, pp.spinOn && dt > 0 ? 3 : 2);
+}
+static ws_status push_surface(ws_handle* h) {
+  launch_push_surface(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->P.atmosphereH, h->stream);
+  return check_launch(h, 1);
+}
+static ws_status contact_scratch(ws_handle* h) {
+  if (h->contactScratch) return WS_OK;
+  WS_TRY(cudaMalloc(&h->contactScratch, contacts_scratch_bytes(h->capacity)));
+  return WS_OK;
+}
+static ws_status vapor_collisions(ws_handle* h) {
+  double sunRel[3] = { h->P.sunPos[0] - h->d.cx, h->P.sunPos[1] - h->d.cy, h->P.sunPos[2] - h->d.cz };
+  ws_status s0 = contact_scratch(h); if (s0) return s0;
+  launch_vapor_collisions(h->d, parts_of(h), h->S.spacing, h->S.oceanR, h->P.spinOn, h->P.hasSun, sunRel,
+                          h->contactScratch, contacts_scratch_bytes(h->capacity), h->st, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  s = sync_status(h); if (s) return s;
+  h->S.vaporCount = h->stHost->vaporCount; h->S.nightVaporCount = h->stHost->nightVapor;
+  return WS_OK;
+}
+static ws_status ice_contacts(ws_handle* h) {
+  ws_status s0 = contact_scratch(h); if (s0) return s0;
+  launch_ice_contacts(parts_of(h), h->S.spacing, h->contactScratch, contacts_scratch_bytes(h->capacity), h->stream);
+  return check_launch(h, 1);
+}
+
+// _stepSync, js/solver.js:2670-2700
+extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
+  if (!h || !(dtFrame > 0)) return WS_ERR_INVALID;
+  if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
+  cudaSetDevice(h->device);
+  ws_status s;
+  h->S.simTime += dtFrame;
+  if (h->P.thermalOn && h->capacity > 1) {
+    h->S.heatAcc = h->S.heatAcc + dtFrame;
+    if (h->S.heatAcc >= 1.0 / 25) {
+      double dtTick = std::min(h->S.heatAcc, 1.0 / 12);
+      if ((s = heat(h, dtTick))) return s;
+      if (h->P.sunActivity > 0) { if ((s = evaporation(h, dtTick))) return s; }
+      h->S.heatAcc = 0;
+    }
+  }
+  double remaining = dtFrame; int guard = 0, nSub = 0;
+  double base = dtFrame / std::max(1, h->P.substeps);
+  while (remaining > 1e-6 && guard < 10) {
+    double dt = std::min(std::min(base, (h->P.cfl * h->d.dx) / std::max(h->S.umax, 0.08)), 1.0 / 100);
+    if (dt < 1e-5) dt = 1e-5;
+    if ((s = substep(h, dt))) return s;
+    remaining -= dt; guard++; nSub++;
+  }
+  h->S.substepsLast = nSub;
+  if (h->P.thermalOn) {
+    if ((s = vapor_collisions(h))) return s;
+    if ((s = phase(h, dtFrame))) return s;
+    if ((s = ice_contacts(h))) return s;
+  }
+  if ((s = push_surface(h))) return s;
+  return sync_status(h);
+}
+
+extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = WS_OK;
+  switch (stage) {
+    case WS_STAGE_CLEAR_RASTER: s = stage_clear_raster(h); break;
+    case WS_STAGE_MARK_FLUID: s = stage_mark(h); break;
+    case WS_STAGE_P2G: s = stage_p2g(h); break;
+    case WS_STAGE_FORCES: s = stage_forces(h, dt); break;
+    case WS_STAGE_PRESSURE: s = stage_pressure(h); break;
+    case WS_STAGE_PROJECT: s = stage_project(h, false); break;
+    case WS_STAGE_VORTICITY: s = stage_vorticity(h, dt); break;
+    case WS_STAGE_CLAMP:
+      s = stage_clamp(h); if (s) return s;
+      s = sync_status(h); if (s) return s;
+      h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
+      return WS_OK;
+    case WS_STAGE_EXTRAPOLATE: s = stage_extrapolate(h); break;
+    case WS_STAGE_G2P_ADVECT:
+      s = stage_g2p_advect(h, dt); if (s) return s;
+      s = sync_status(h); if (s) return s;
+      h->S.airborneCount = h->stHost->airborne; h->S.dtLast = dt;
+      return WS_OK;
+    case WS_STAGE_HEAT: s = heat(h, dt); break;
+    case WS_STAGE_EVAPORATION: s = evaporation(h, dt); break;
+    case WS_STAGE_PHASE: s = phase(h, dt); break;
+    case WS_STAGE_PUSH_SURFACE: s = push_surface(h); break;
+    case WS_STAGE_SPLAT:
+      launch_splat(h->d, grid_of(h), parts_of(h), h->S.spacing, h->stream);
+      s = check_launch(h, 1); break;
+    case WS_STAGE_VAPOR_COLLISIONS: s = vapor_collisions(h); break;
+    case WS_STAGE_ICE_CONTACTS: s = ice_contacts(h); break;
+    default: return fail(h, WS_ERR_INVALID, "unknown stage");
+  }
+  if (s) return s;
+  return sync_status(h);
+}
+
+// ------------------------------------------------------------ interactions
+extern "C" ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy, double cz, double R,
+                                             double fx, double fy, double fz) {
+  if (!h) return WS_ERR_INVALID;
+  launch_impulse_sphere(parts_of(h), cx, cy, cz, R, fx, fy, fz, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  return sync_status(h);
+}
+extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, double vx, double vy,
+                                double vz, double R, double dt) {
+  if (!h) return WS_ERR_INVALID;
+  launch_stir_at(parts_of(h), cx, cy, cz, vx, vy, vz, R, dt, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  return sync_status(h);
+}
+// Seeded Gaussian stir kick: the draw order (u1, theta, phi from stirS) and
+// the tangent construction are part of the workload definition.
+extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
+  if (!h || !(sigma > 0)) return WS_ERR_INVALID;
+  uint32_t st = h->S.stirS;
+  st = lcg_next(st); double u1 = st / 4294967296.0 * 2 - 1;
+  st = lcg_next(st); double th = st / 4294967296.0 * 6.283185307179586;
+  st = lcg_next(st); double ph = st / 4294967296.0 * 6.283185307179586;
+  h->S.stirS = st;
+  double sq = std::sqrt(1 - u1 * u1);
+  double dxn = sq * std::cos(th), dyn = u1, dzn = sq * std::sin(th);
+  double ax = 0, ay = 1, az = 0;
+  if (std::fabs(dyn) > 0.9) { ax = 1; ay = 0; }
+  double e1x = dyn * az - dzn * ay, e1y = dzn * ax - dxn * az, e1z = dxn * ay - dyn * ax;
+  double e1l = std::sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+  e1x /= e1l; e1y /= e1l; e1z /= e1l;
+  double e2x = dyn * e1z - dzn * e1y, e2y = dzn * e1x - dxn * e1z, e2z = dxn * e1y - dyn * e1x;
+  double cph = std::cos(ph), sph = std::sin(ph);
+  double tx = cph * e1x + sph * e2x, ty = cph * e1y + sph * e2y, tz = cph * e1z + sph * e2z;
+  double R = h->S.oceanR;
+  launch_stir_gaussian(parts_of(h), h->d.cx + dxn * R, h->d.cy + dyn * R, h->d.cz + dzn * R, tx, ty, tz, sigma, peak, h->stream);
+  return check_launch(h, 1);
+}
+
+extern "C" ws_status ws_synchronize(ws_handle* h) {
+  if (!h) return WS_ERR_INVALID;
+  return sync_status(h);
+}
+extern "C" ws_status ws_get_stream(ws_handle* h, void** s) {
+  if (!h || !s) return WS_ERR_INVALID;
+  *s = (void*)h->stream;
+  return WS_OK;
+}
+extern "C" ws_status ws_launch_count(ws_handle* h, int64_t* n) {
+  if (!h || !n) return WS_ERR_INVALID;
+  *n = h->launches;
+  return WS_OK;
+}
+
+extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us) {
+  if (!h || !us || reps < 1) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  cudaEvent_t e0, e1;
+  WS_TRY(cudaEventCreate(&e0));
+  WS_TRY(cudaEventCreate(&e1));
+  GridDev g = grid_of(h);
+  int perRep = 1;
+  WS_TRY(cudaEventRecord(e0, h->stream));
+  for (int r = 0; r < reps; r++) {
+    switch (kernel) {
+      case 0: launch_sor_color(h->d, g, 0, 1 - h->P.omega, h->stream);
+              launch_sor_color(h->d, g, 1, 1 - h->P.omega, h->stream); perRep = 2; break;
+      case 1: launch_p2g(h->d, g, parts_of(h), h->stream); break;
+      case 2: { AdvectParams ap = advect_params(h, h->S.dtLast > 0 ? h->S.dtLast : 0.01);
+                launch_g2p_advect(h->d, g, parts_of(h), h->terr, ap, h->st, h->stream); } break;
+      case 3: launch_faces_normalize_bc(h->d, g, h->stream); break;
+      case 4: launch_faces_forces(h->d, g, 5e-6, 1, 0.01, 9.81, h->stream); break;
+      case 5: launch_project(h->d, g, 1, h->P.maxSpeed, h->st, h->stream); break;
+      default: cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(h, WS_ERR_INVALID, "unknown kernel id");
+    }
+  }
+  WS_TRY(cudaEventRecord(e1, h->stream));
+  ws_status s = check_launch(h, reps * perRep); if (s) return s;
+  WS_TRY(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  *us = 1000.0 * ms / (reps * perRep);
+  return sync_status(h);
+}

@@ -1,0 +1,640 @@
+// ws_frame.cu — per-frame passes: thermal tick (js/solver.js:2715-2994),
+// evaporation (:3008-3125), phase changes (:3145-3281), frame-end rescue
+// (:3496-3587), density splat (:3785-3820) and the FP64 reductions
+// (marching-tets volume js/surface.js:66-177, census js/main.js:176-186,
+// kinetic energy js/solver.js:3914-3921).
+#include "ws_kernels.cuh"
+
+// ------------------------------------------------------------ thermal: shadows + heating
+// _heatShadowChunk, js/solver.js:2773-2918 — independent per particle.
+__global__ void k_heat_shadow(Dims d, GridDev g, PartsDev P, TerrainDev t, HeatParams hp, double dt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  const double dx = d.dx, cx = d.cx, cy = d.cy, cz = d.cz;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const uint8_t* type = g.type;
+  double lit = hp.hasSun ? 1 : 0;
+  double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
+  double dwx = PX - cx, dwy = PY - cy, dwz = PZ - cz;
+  double dwl = sqrt(dwx * dwx + dwy * dwy + dwz * dwz); if (dwl == 0) dwl = 1e-9;
+  double stpU = dx / dwl; int above = 0;
+  for (int stU = 1; stU <= 4; stU++) {
+    double qx = PX + dwx * stpU * stU, qy = PY + dwy * stpU * stU, qz = PZ + dwz * stpU * stU;
+    int qi = jtrunc(qx / dx), qj = jtrunc(qy / dx), qk = jtrunc(qz / dx);
+    if (qi < 0 || qj < 0 || qk < 0 || qi >= nx || qj >= ny || qk >= nz) break;
+    if (type[((long long)qk * ny + qj) * nx + qi] != WS_FLUID) break;
+    above++;
+  }
+  P.pDepth[p] = (uint8_t)above;
+  if (hp.hasSun) {
+    if (above >= 4) lit = 0;
+    else {
+      double lx = hp.sun[0] - PX, ly = hp.sun[1] - PY, lz = hp.sun[2] - PZ;
+      double ld = sqrt(lx * lx + ly * ly + lz * lz); if (ld == 0) ld = 1e-9;
+      double dxn = lx / ld, dyn = ly / ld, dzn = lz / ld;
+      double ex = cx - PX, ey = cy - PY, ez = cz - PZ;
+      double b = ex * dxn + ey * dyn + ez * dzn;
+      if (t.has) {
+        double d2c = ex * ex + ey * ey + ez * ez - b * b;
+        if (b > 0 && d2c < t.Rlo2 * 0.96) lit = 0;
+        else if (b > 0 || d2c < t.Rhi2 * 1.1) {
+          double stp = dx * 1.5, mx = PX, my = PY, mz = PZ;
+          double esc2 = (t.Rhi + 0.1) * (t.Rhi + 0.1);
+          for (int st2 = 0; st2 < 26; st2++) {
+            mx += dxn * stp; my += dyn * stp; mz += dzn * stp;
+            double rex = mx - cx, rey = my - cy, rez = mz - cz;
+            if (rex * rex + rey * rey + rez * rez > esc2) break;
+            int ivx = jtrunc(mx / t.dv); if (ivx < 0 || ivx >= t.n) break;
+            int ivy = jtrunc(my / t.dv); if (ivy < 0 || ivy >= t.n) break;
+            int ivz = jtrunc(mz / t.dv); if (ivz < 0 || ivz >= t.n) break;
+            if (t.solid[((long long)ivz * t.n + ivy) * t.n + ivx]) { lit = 0; break; }
+          }
+        }
+      } else if (b > 0) {
+        double d2c2 = ex * ex + ey * ey + ez * ez - b * b;
+        if (d2c2 < hp.coreR * hp.coreR) lit = 0;
+      }
+      if (lit != 0) {
+        double od = 0, sx = PX, sy = PY, sz = PZ, half = dx;
+        long long sj = nx + 1, sk = (long long)(ny + 1) * sj;
+        for (int st = 0; st < 6 && st * half < 0.55; st++) {
+          sx += dxn * half; sy += dyn * half; sz += dzn * half;
+          int i0 = jtrunc(sx / dx), j0 = jtrunc(sy / dx), k0 = jtrunc(sz / dx);
+          if (i0 < 0 || j0 < 0 || k0 < 0 || i0 >= nx || j0 >= ny || k0 >= nz) break;
+          double vv = g.dens[k0 * sk + j0 * sj + i0];
+          od += vv * half * 1.1;
+          if (od > 3.5) break;
+        }
+        lit = od < 3.5 ? exp(-od) : 0;
+      }
+    }
+  }
+  P.pLight[p] = (float)lit;
+  double T, pT = P.pT[p], Tamb = hp.Tamb, sunPow = hp.sunActivity / 3;
+  int f = P.pflag[p];
+  if (f == 2) {
+    double amb = lit > 0.05 ? Tamb + 0.18 : 0.06, K = hp.hasSun ? 0.16 + (1 - lit) * 0.20 : 1.2;
+    T = pT + (amb - pT) * K * dt; if (lit > 0) T += sunPow * 0.6 * lit * dt;
+  } else if (f == 3) {
+    double amb = lit > 0.05 ? Tamb + 0.18 : 0.06, K = hp.hasSun ? 0.10 + (1 - lit) * 0.12 : 0.9;
+    T = pT + (amb - pT) * K * dt; if (lit > 0) T += sunPow * 0.35 * lit * dt;
+  } else if (f == 4) {
+    double amb = lit > 0.05 ? Tamb + 0.18 : 0.06, K = hp.hasSun ? 0.14 + (1 - lit) * 0.16 : 1.0;
+    T = pT + (amb - pT) * K * dt; if (lit > 0) T += sunPow * 0.45 * lit * dt;
+  } else {
+    double amb = lit > 0.05 ? Tamb : 0;
+    T = pT + (amb - pT) * (0.045 + (1 - lit) * hp.shadeCool) * dt; if (lit > 0) T += sunPow * lit * dt;
+  }
+  if (T > 1.15) T = 1.15; else if (T < 0) T = 0;
+  P.pT[p] = (float)T;
+}
+
+// ------------------------------------------------------------ thermal: conduction
+// Cell aggregates of _heatMeansSlice/_heatConductFlux/_heatApplySlice
+// (:2921-2979) without a particle sort: counts and FP64 temperature sums per
+// cell, then each cell gathers its six edge energies in the reference's
+// accumulation order, then each particle applies its cell's update.
+__device__ __forceinline__ long long heat_cell(const Dims& d, double x, double y, double z) {
+  int gx = jtrunc(x / d.dx); if (gx < 0) gx = 0; else if (gx >= d.nx) gx = d.nx - 1;
+  int gy = jtrunc(y / d.dx); if (gy < 0) gy = 0; else if (gy >= d.ny) gy = d.ny - 1;
+  int gz = jtrunc(z / d.dx); if (gz < 0) gz = 0; else if (gz >= d.nz) gz = d.nz - 1;
+  return ((long long)gz * d.ny + gy) * d.nx + gx;
+}
+__global__ void k_heat_bin(Dims d, PartsDev P, int* __restrict__ cnt, double* __restrict__ sumT) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  long long c = heat_cell(d, P.px[p], P.py[p], P.pz[p]);
+  atomicAdd(&cnt[c], 1);
+  atomicAdd(&sumT[c], (double)P.pT[p]);
+}
+__global__ void k_heat_means(Dims d, const int* __restrict__ cnt, double* __restrict__ sumT) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  sumT[c] = cnt[c] ? sumT[c] / cnt[c] : 0.0;        // in place: sum -> mean
+}
+__global__ void k_heat_flux(Dims d, const int* __restrict__ cnt, const double* __restrict__ mean,
+                            double* __restrict__ change, double alpha) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  int nc = cnt[c];
+  if (!nc) return;
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  double ch = 0;
+  // contributions as the neighbour of an earlier cell (:2961 "-="): c-nxy, c-nx, c-1
+  if (k > 0 && cnt[c - nxy]) { int a = cnt[c - nxy]; ch -= alpha * (double)(a < nc ? a : nc) * (mean[c] - mean[c - nxy]); }
+  if (j > 0 && cnt[c - nx]) { int a = cnt[c - nx]; ch -= alpha * (double)(a < nc ? a : nc) * (mean[c] - mean[c - nx]); }
+  if (i > 0 && cnt[c - 1]) { int a = cnt[c - 1]; ch -= alpha * (double)(a < nc ? a : nc) * (mean[c] - mean[c - 1]); }
+  // own edges along +x, +y, +z (:2961 "+=")
+  if (i < nx - 1 && cnt[c + 1]) { int a = cnt[c + 1]; ch += alpha * (double)(nc < a ? nc : a) * (mean[c + 1] - mean[c]); }
+  if (j < ny - 1 && cnt[c + nx]) { int a = cnt[c + nx]; ch += alpha * (double)(nc < a ? nc : a) * (mean[c + nx] - mean[c]); }
+  if (k < nz - 1 && cnt[c + nxy]) { int a = cnt[c + nxy]; ch += alpha * (double)(nc < a ? nc : a) * (mean[c + nxy] - mean[c]); }
+  change[c] = ch;
+}
+__global__ void k_heat_apply_convect(Dims d, PartsDev P, const int* __restrict__ cnt, const double* __restrict__ mean,
+                                     const double* __restrict__ change, double alphaA, int conduct, double Tamb, double dt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  double x = P.px[p], y = P.py[p], z = P.pz[p];
+  float T = P.pT[p];
+  if (conduct) {
+    long long c = heat_cell(d, x, y, z);
+    double deltaT = change[c] / cnt[c];
+    T = (float)((double)T + alphaA * (mean[c] - (double)T) + deltaT);
+    P.pT[p] = T;
+  }
+  if (P.pflag[p] != 0) return;                       // _heatConvectChunk :2982-2994
+  double rx = x - d.cx, ry = y - d.cy, rz = z - d.cz;
+  double rl = sqrt(rx * rx + ry * ry + rz * rz); if (rl == 0) rl = 1e-9;
+  double ab = 3.0 * ((double)T - Tamb) * dt / rl;
+  P.pvx[p] = (float)((double)P.pvx[p] + rx * ab);
+  P.pvy[p] = (float)((double)P.pvy[p] + ry * ab);
+  P.pvz[p] = (float)((double)P.pvz[p] + rz * ab);
+}
+void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t, const HeatParams& hp,
+                 double dt, int* cnt, double* sumT, double* change, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  unsigned gp = grid_for(P.nP, 256), gc = grid_for(d.nCells, 256);
+  k_heat_shadow<<<gp, 256, 0, s>>>(d, g, P, t, hp, dt);
+  int conduct = hp.heatK > 0;
+  if (conduct) {
+    cudaMemsetAsync(cnt, 0, sizeof(int) * d.nCells, s);
+    cudaMemsetAsync(sumT, 0, sizeof(double) * d.nCells, s);
+    k_heat_bin<<<gp, 256, 0, s>>>(d, P, cnt, sumT);
+    k_heat_means<<<gc, 256, 0, s>>>(d, cnt, sumT);
+    double alpha = hp.heatK * dt * 0.15; if (alpha > 0.14) alpha = 0.14;
+    k_heat_flux<<<gc, 256, 0, s>>>(d, cnt, sumT, change, alpha);
+    k_heat_apply_convect<<<gp, 256, 0, s>>>(d, P, cnt, sumT, change, alpha, 1, hp.Tamb, dt);
+  } else {
+    k_heat_apply_convect<<<gp, 256, 0, s>>>(d, P, cnt, sumT, change, 0, 0, hp.Tamb, dt);
+  }
+}
+
+// ------------------------------------------------------------ evaporation
+// _evapChunk, js/solver.js:3028-3116. Candidates (surface-top liquid above
+// the freezing point) are compacted in index order; one CTA then walks them
+// reproducing the reference's single _evS stream: every lane evaluates its
+// draw assuming no ejection before it (lcg_jump), the first ejecting lane
+// runs its six Box-Muller draws (with the u1 < 1e-9 retry) serially, and the
+// walk restarts after it.
+__device__ __forceinline__ bool evap_candidate(const Dims& d, const GridDev& g, const PartsDev& P, int p,
+                                               double freezeT, int& ci, int& cj, int& ck) {
+  if (P.pflag[p] != 0) return false;
+  double T = P.pT[p];
+  if (T <= freezeT) return false;
+  double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
+  int i = jtrunc(PX / d.dx), j = jtrunc(PY / d.dx), k = jtrunc(PZ / d.dx);
+  if (i < 1) i = 1; else if (i > d.nx - 2) i = d.nx - 2;
+  if (j < 1) j = 1; else if (j > d.ny - 2) j = d.ny - 2;
+  if (k < 1) k = 1; else if (k > d.nz - 2) k = d.nz - 2;
+  if (g.type[((long long)k * d.ny + j) * d.nx + i] != WS_FLUID) return false;
+  double ex = PX - d.cx, ey = PY - d.cy, ez = PZ - d.cz;
+  double el = sqrt(ex * ex + ey * ey + ez * ez); if (el == 0) el = 1e-9;
+  int ui = jtrunc((PX + ex / el * d.dx) / d.dx), uj = jtrunc((PY + ey / el * d.dx) / d.dx), uk = jtrunc((PZ + ez / el * d.dx) / d.dx);
+  if (ui < 0 || uj < 0 || uk < 0 || ui >= d.nx || uj >= d.ny || uk >= d.nz) return false;
+  if (g.type[((long long)uk * d.ny + uj) * d.nx + ui] == WS_FLUID) return false;
+  ci = i; cj = j; ck = k;
+  return true;
+}
+__global__ void k_evap_flags(Dims d, GridDev g, PartsDev P, double freezeT, uint8_t* __restrict__ cand) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  int i, j, k;
+  cand[p] = evap_candidate(d, g, P, p, freezeT, i, j, k) ? 1 : 0;
+}
+__device__ __forceinline__ double ev_gauss(uint32_t& s) {
+  double u1;
+  do { s = lcg_next(s); u1 = s / 4294967296.0; } while (u1 < 1e-9);
+  s = lcg_next(s);
+  return sqrt(-2 * log(u1)) * cos(6.283185306 * (s / 4294967296.0));
+}
+__global__ void __launch_bounds__(1024) k_evap_walk(Dims d, GridDev g, PartsDev P, double freezeT, double rate, double dt,
+                                                    const int* __restrict__ list, const int* __restrict__ nCp,
+                                                    uint32_t* __restrict__ evS, DevStatus* st) {
+  __shared__ int firstLane;
+  __shared__ uint32_t sNext;
+  const int nC = *nCp;
+  uint32_t s = *evS;
+  int base = 0, ejections = 0;
+  const double C = 3.5, T_CAP = 1.15;
+  while (base < nC) {
+    int idx = base + (int)threadIdx.x;
+    bool act = idx < nC;
+    int p = act ? list[idx] : 0;
+    double T = act ? (double)P.pT[p] : 0;
+    bool ej = false;
+    if (act) {
+      double prob = rate * dt * exp(C * (T - freezeT));
+      if (prob > 1) prob = 1;
+      uint32_t sl = lcg_jump(s, threadIdx.x + 1u);
+      ej = !(sl / 4294967296.0 > prob);
+    }
+    if (threadIdx.x == 0) firstLane = 1 << 30;
+    __syncthreads();
+    if (ej) atomicMin(&firstLane, (int)threadIdx.x);
+    __syncthreads();
+    int L = firstLane;
+    int remaining = nC - base; if (remaining > (int)blockDim.x) remaining = blockDim.x;
+    if (L >= remaining) {                              // no ejection in this window
+      s = lcg_jump(s, (uint32_t)remaining);
+      base += remaining;
+      __syncthreads();
+      continue;
+    }
+    if ((int)threadIdx.x == L) {                       // the first ejector, :3083-3113
+      uint32_t sl = lcg_jump(s, (uint32_t)L + 1u);
+      int i, j, k;
+      evap_candidate(d, g, P, p, freezeT, i, j, k);
+      P.pflag[p] = 2; P.pAir[p] = 0.f;
+      double tau = (T - freezeT) / (T_CAP - freezeT);
+      if (tau < 0) tau = 0; else if (tau > 1) tau = 1;
+      double sig = 0.30 + 0.32 * sqrt(tau);
+      double kx = sig * ev_gauss(sl); double ky = sig * ev_gauss(sl); double kz = sig * ev_gauss(sl);
+      double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
+      double ex2 = PX - d.cx, ey2 = PY - d.cy, ez2 = PZ - d.cz;
+      double el2 = ex2 * ex2 + ey2 * ey2 + ez2 * ez2;
+      double elL = sqrt(el2); if (elL == 0) elL = 1e-9;
+      double kUp = (kx * ex2 + ky * ey2 + kz * ez2) / el2;
+      if (kUp < 0) { kx -= 2 * kUp * ex2 / elL; ky -= 2 * kUp * ey2 / elL; kz -= 2 * kUp * ez2 / elL; }
+      int nx = d.nx, ny = d.ny;
+      double guS = g.vel[((long long)k * ny + j) * (nx + 1) + i];
+      double gvS = g.vel[d.uN + ((long long)k * (ny + 1) + j) * nx + i];
+      double gwS = g.vel[d.uN + d.vN + ((long long)k * ny + j) * nx + i];
+      double nl2 = 1 / el2;
+      double vN = ((double)P.pvx[p] * ex2 + (double)P.pvy[p] * ey2 + (double)P.pvz[p] * ez2) * nl2;
+      double gN = (guS * ex2 + gvS * ey2 + gwS * ez2) * nl2;
+      P.pvx[p] = (float)(vN * ex2 + (guS - gN * ex2) + kx);
+      P.pvy[p] = (float)(vN * ey2 + (gvS - gN * ey2) + ky);
+      P.pvz[p] = (float)(vN * ez2 + (gwS - gN * ez2) + kz);
+      sNext = sl;
+    }
+    __syncthreads();
+    s = sNext;
+    base += L + 1;
+    ejections++;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { *evS = s; st->evapCount = ejections; }
+}
+void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
+                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, DevStatus* st, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  k_evap_flags<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, freezeT, cand);
+  launch_compact(cand, P.nP, 2, blockCounts, list, nC, s);
+  k_evap_walk<<<1, 1024, 0, s>>>(d, g, P, freezeT, rate, dt, list, nC, evS, st);
+}
+
+// ------------------------------------------------------------ phase changes
+// _updatePhaseChanges, js/solver.js:3152-3281: steam counts per cell
+// (integer atomics, exact), then independent per-particle transitions.
+__device__ __forceinline__ long long clamp_cell(const Dims& d, double x, double y, double z, int& i, int& j, int& k) {
+  i = jtrunc(x / d.dx); j = jtrunc(y / d.dx); k = jtrunc(z / d.dx);
+  if (i < 0) i = 0; else if (i >= d.nx) i = d.nx - 1;
+  if (j < 0) j = 0; else if (j >= d.ny) j = d.ny - 1;
+  if (k < 0) k = 0; else if (k >= d.nz) k = d.nz - 1;
+  return ((long long)k * d.ny + j) * d.nx + i;
+}
+__global__ void k_steam_count(Dims d, PartsDev P, int* __restrict__ cnt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP || P.pflag[p] != 2) return;
+  int i, j, k;
+  atomicAdd(&cnt[clamp_cell(d, P.px[p], P.py[p], P.pz[p], i, j, k)], 1);
+}
+__device__ __forceinline__ uint32_t js_mul_u32(double a, double b) {
+  double m = fmod(a * b, 4294967296.0); if (m < 0) m += 4294967296.0;
+  return (uint32_t)m;
+}
+__device__ __forceinline__ uint32_t spin_hash(uint32_t a, uint32_t b, uint32_t c) {   // :3145-3150
+  uint32_t s = a ^ js_mul_u32(b, 2654435769.0) ^ js_mul_u32(c, 2246822507.0) ^ js_mul_u32(1370176631.0, 3266489909.0);
+  s = lcg_next(s);
+  s ^= s >> 13; s = js_mul_u32(s, 1540483477.0); s ^= s >> 15;
+  return s;
+}
+__global__ void k_phase_update(Dims d, GridDev g, PartsDev P, PhaseParams pp, const int* __restrict__ cnt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  const uint8_t* type = g.type;
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int f = P.pflag[p], i, j, k;
+  double T = P.pT[p];
+  if (f == 0) {
+    if (T <= pp.snowT && T > 1e-3) {
+      long long cB = clamp_cell(d, P.px[p], P.py[p], P.pz[p], i, j, k);
+      bool atSurf = (k > 0 && type[cB - nxy] != WS_FLUID) || (k < nz - 1 && type[cB + nxy] != WS_FLUID) ||
+                    (j > 0 && type[cB - nx] != WS_FLUID) || (j < ny - 1 && type[cB + nx] != WS_FLUID) ||
+                    (i > 0 && type[cB - 1] != WS_FLUID) || (i < nx - 1 && type[cB + 1] != WS_FLUID);
+      if (atSurf) { P.pflag[p] = 5; P.pvx[p] = P.pvy[p] = P.pvz[p] = 0.f; P.pAir[p] = 1.f; }
+    }
+  } else if (f == 5) {
+    if (T >= pp.meltT) {
+      long long c = clamp_cell(d, P.px[p], P.py[p], P.pz[p], i, j, k);
+      P.pflag[p] = type[c] == WS_FLUID ? 0 : 4;
+      P.pAir[p] = 0.f; P.pWx[p] = P.pWy[p] = P.pWz[p] = 0.f;
+    }
+  } else if (T > 1e-3) {
+    if (f == 2) {
+      if (T <= pp.rainT && (double)P.pAir[p] >= pp.rainLiftAge) {
+        P.pflag[p] = 4; P.pAir[p] = 0.f; P.pvx[p] = P.pvy[p] = P.pvz[p] = 0.f; P.pWx[p] = P.pWy[p] = P.pWz[p] = 0.f;
+        f = 4;
+      } else if (T <= pp.cloudT) {
+        double rx = (double)P.px[p] - d.cx, ry = (double)P.py[p] - d.cy, rz = (double)P.pz[p] - d.cz;
+        if (sqrt(rx * rx + ry * ry + rz * rz) >= pp.cloudBase) {
+          i = jtrunc(P.px[p] / d.dx); j = jtrunc(P.py[p] / d.dx); k = jtrunc(P.pz[p] / d.dx);
+          int i0 = i > 0 ? i - 1 : 0, i1 = i < nx - 1 ? i + 1 : nx - 1;
+          int j0 = j > 0 ? j - 1 : 0, j1 = j < ny - 1 ? j + 1 : ny - 1;
+          int k0 = k > 0 ? k - 1 : 0, k1 = k < nz - 1 ? k + 1 : nz - 1;
+          double sum = 0;
+          for (int kk = k0; kk <= k1; kk++) for (int jj = j0; jj <= j1; jj++) {
+            long long row = ((long long)kk * ny + jj) * nx;
+            for (int ii = i0; ii <= i1; ii++) sum += cnt[row + ii];
+          }
+          if (sum / 27 >= pp.cloudP) { P.pflag[p] = 3; P.pAir[p] = 0.f; f = 3; }
+        }
+      }
+    } else if (f == 3) {
+      if (T >= pp.cloudT + 0.05) { P.pflag[p] = 2; f = 2; }
+    } else if ((f == 1 || f == 4) && T <= pp.snowT) {   // spray and rain freeze (:3253)
+      P.pflag[p] = 5; P.pvx[p] = P.pvy[p] = P.pvz[p] = 0.f; P.pAir[p] = 0.f; P.pWx[p] = P.pWy[p] = P.pWz[p] = 0.f;
+    }
+  }
+}
+// spin bookkeeping (:3259-3280), a separate pass over the final flags
+__global__ void k_phase_spin(PartsDev P, uint32_t tick, double dt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  int f = P.pflag[p];
+  if (f != 2 && f != 3) return;
+  float wx = P.pWx[p], wy = P.pWy[p], wz = P.pWz[p];
+  if (f == 2 && P.pAir[p] <= 1e-6f && wx == 0.f && wy == 0.f && wz == 0.f) {
+    uint32_t sd = 0x51ab3c77u;
+    double h1 = spin_hash(sd, (uint32_t)p, tick) / 4294967296.0;
+    double h2 = spin_hash(sd + 1, (uint32_t)p, tick) / 4294967296.0;
+    double h3 = spin_hash(sd + 2, (uint32_t)p, tick) / 4294967296.0;
+    double zz = 2 * h2 - 1, rr = sqrt(dmax(0, 1 - zz * zz)), th = 6.283185306 * h1;
+    double Tp = P.pT[p]; if (!(Tp > 0.05)) Tp = 0.05; else if (Tp > 1.15) Tp = 1.15;
+    double wSpd = 3.0 * sqrt(Tp) * (0.5 + h3);
+    wx = (float)(rr * cos(th) * wSpd); wy = (float)(zz * wSpd); wz = (float)(rr * sin(th) * wSpd);
+  }
+  double wm = sqrt((double)wx * wx + (double)wy * wy + (double)wz * wz);
+  if (wm > 1e-6) P.pPh[p] = (float)((double)P.pPh[p] + wm * dt);
+  double damp = dmax(0, 1 - 0.12 * dt);
+  P.pWx[p] = (float)(wx * damp); P.pWy[p] = (float)(wy * damp); P.pWz[p] = (float)(wz * damp);
+}
+void launch_phase(const Dims& d, const GridDev& g, const PartsDev& P, const PhaseParams& pp, int* cnt, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  cudaMemsetAsync(cnt, 0, sizeof(int) * d.nCells, s);
+  unsigned gp = grid_for(P.nP, 256);
+  k_steam_count<<<gp, 256, 0, s>>>(d, P, cnt);
+  k_phase_update<<<gp, 256, 0, s>>>(d, g, P, pp, cnt);
+  if (pp.spinOn && pp.dt > 0) k_phase_spin<<<gp, 256, 0, s>>>(P, pp.tick, pp.dt);
+}
+
+// ------------------------------------------------------------ frame-end rescue
+// _pushSurfaceChunk, js/solver.js:3496-3587 — independent per particle.
+__global__ void k_push_surface(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR, double atmosphereH) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP || !t.has) return;
+  const double cx = d.cx, cy = d.cy, cz = d.cz, dx = d.dx;
+  double x = P.px[p], y = P.py[p], z = P.pz[p];
+  float fvx = P.pvx[p], fvy = P.pvy[p], fvz = P.pvz[p];
+  double ex = x - cx, ey = y - cy, ez = z - cz;
+  double er = sqrt(ex * ex + ey * ey + ez * ez); if (er == 0) er = 1e-9;
+  bool fixed = false, rockFixed = false, velChanged = false;
+  double outer = d.domainR - dx * 0.02;
+  double skyHi = oceanR + atmosphereH - 1e-3 * dx;
+  if (er > skyHi) {
+    x = cx + ex / er * skyHi; y = cy + ey / er * skyHi; z = cz + ez / er * skyHi;
+    double outward = ((double)fvx * ex + (double)fvy * ey + (double)fvz * ez) / er;
+    if (outward > 0) { fvx = (float)(fvx - ex / er * outward); fvy = (float)(fvy - ey / er * outward); fvz = (float)(fvz - ez / er * outward); velChanged = true; }
+    ex = x - cx; ey = y - cy; ez = z - cz; er = skyHi;
+    fixed = true;
+  }
+  if (er <= d.domainR && rock_cell_at(d, g.staticTypes, x, y, z)) {
+    rockFixed = true;
+    int tries = 0;
+    while (rock_cell_at(d, g.staticTypes, x, y, z) && tries < d.nx * 2) {
+      x += ex / er * dx * 0.5; y += ey / er * dx * 0.5; z += ez / er * dx * 0.5; tries++;
+    }
+    double exR = x - cx, eyR = y - cy, ezR = z - cz;
+    double erR = sqrt(exR * exR + eyR * eyR + ezR * ezR); if (erR == 0) erR = 1e-9;
+    double wantR = terrain_radius_at(t, coreR, x, y, z) + dx * 0.06;
+    if (erR > wantR) { x = cx + exR / erR * wantR; y = cy + eyR / erR * wantR; z = cz + ezR / erR * wantR; }
+    int kR = 0;
+    while (rock_cell_at(d, g.staticTypes, x, y, z) && kR < 4) {
+      x += exR / erR * dx * 0.5; y += eyR / erR * dx * 0.5; z += ezR / erR * dx * 0.5; kR++;
+    }
+    fixed = true;
+  } else if (P.pflag[p] == 0 && er <= d.domainR) {
+    double Rt = terrain_radius_at(t, coreR, x, y, z);
+    if (er < Rt - dx * 0.5) {
+      rockFixed = true;
+      x = cx + ex / er * (Rt + dx * 0.05); y = cy + ey / er * (Rt + dx * 0.05); z = cz + ez / er * (Rt + dx * 0.05);
+      int t2 = 0;
+      while (rock_cell_at(d, g.staticTypes, x, y, z) && t2 < 8) {
+        x += ex / er * dx * 0.5; y += ey / er * dx * 0.5; z += ez / er * dx * 0.5; t2++;
+      }
+      fixed = true;
+    }
+  }
+  double finalR = sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz));
+  double capR = P.pflag[p] == 0 ? outer : skyHi;
+  if (finalR > capR) {
+    x = cx + (x - cx) * capR / finalR; y = cy + (y - cy) * capR / finalR; z = cz + (z - cz) * capR / finalR;
+    fixed = true;
+  }
+  if (fixed) {
+    P.px[p] = (float)x; P.py[p] = (float)y; P.pz[p] = (float)z;
+    double vr = ((double)fvx * ex + (double)fvy * ey + (double)fvz * ez) / er;
+    if (rockFixed && vr < 0) { fvx = (float)(fvx - ex / er * vr); fvy = (float)(fvy - ey / er * vr); fvz = (float)(fvz - ez / er * vr); velChanged = true; }
+  }
+  if (velChanged) { P.pvx[p] = fvx; P.pvy[p] = fvy; P.pvz[p] = fvz; }
+}
+void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
+                         double oceanR, double coreR, double atmosphereH, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  k_push_surface<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, atmosphereH);
+}
+
+// ------------------------------------------------------------ density splat
+// _splatInto, js/solver.js:3792-3820 (float atomics on the corner lattice)
+__global__ void k_splat(Dims d, GridDev g, PartsDev P, double spacing) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP || P.pflag[p] != 0) return;
+  double dx = d.dx, r = 1.6 * spacing, r2 = r * r;
+  long long sj = d.nx + 1, sk = (long long)(d.ny + 1) * sj;
+  double X = P.px[p], Y = P.py[p], Z = P.pz[p];
+  double fi = floor(X / dx), fj = floor(Y / dx), fk = floor(Z / dx);
+  int i0 = fi < 0 ? 0 : (fi > d.nx - 1 ? d.nx - 1 : (int)fi);
+  int j0 = fj < 0 ? 0 : (fj > d.ny - 1 ? d.ny - 1 : (int)fj);
+  int k0 = fk < 0 ? 0 : (fk > d.nz - 1 ? d.nz - 1 : (int)fk);
+  double fx = X - i0 * dx, fy = Y - j0 * dx, fz = Z - k0 * dx;
+  for (int kk = 0; kk < 2; kk++) {
+    double czz = kk == 0 ? fz : fz - dx;
+    for (int jj = 0; jj < 2; jj++) {
+      double cyy = jj == 0 ? fy : fy - dx;
+      for (int ii = 0; ii < 2; ii++) {
+        double cxx = ii == 0 ? fx : fx - dx;
+        double d2 = cxx * cxx + cyy * cyy + czz * czz;
+        if (d2 >= r2) continue;
+        double ww = 1 - d2 / r2; ww = ww * ww;
+        atomicAdd(&g.dens[(k0 + kk) * sk + (j0 + jj) * sj + (i0 + ii)], (float)ww);
+      }
+    }
+  }
+}
+void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spacing, cudaStream_t s) {
+  long long nd = (long long)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+  cudaMemsetAsync(g.dens, 0, sizeof(float) * nd, s);
+  if (P.nP <= 0) return;
+  k_splat<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, spacing);
+}
+
+// ------------------------------------------------------------ marching-tets volume (FP64)
+__constant__ int c_corners[8][3] = { {0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1} };
+__constant__ int c_tets[6][4] = { {0,5,1,6},{0,1,2,6},{0,2,3,6},{0,3,7,6},{0,7,4,6},{0,4,5,6} };
+__constant__ int c_edges[6][2] = { {0,1},{1,2},{2,0},{0,3},{1,3},{2,3} };
+__constant__ int c_ntri[16] = { 0,1,1,2,1,2,2,1,1,2,2,1,2,1,1,0 };
+__constant__ int c_cases[16][2][3] = {
+  {{0,0,0},{0,0,0}}, {{0,2,3},{0,0,0}}, {{0,1,4},{0,0,0}}, {{2,3,4},{2,4,1}},
+  {{2,1,5},{0,0,0}}, {{0,3,5},{0,5,1}}, {{0,4,5},{0,5,2}}, {{3,5,4},{0,0,0}},
+  {{3,4,5},{0,0,0}}, {{0,2,5},{0,5,4}}, {{0,1,5},{0,5,3}}, {{2,1,5},{0,0,0}},
+  {{2,1,4},{2,4,3}}, {{0,1,4},{0,0,0}}, {{0,2,3},{0,0,0}}, {{0,0,0},{0,0,0}} };
+// One cell's signed tet-mesh volume contribution and vertex count (the
+// per-cell body of MarchingTetrahedra.build, js/surface.js:80-171).
+__device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz, double dx, double iso,
+                          int i, int j, int k, int& verts) {
+  long long sj = nx + 1, sk = (long long)(ny + 1) * sj;
+  double cv[8], gx[8], gy[8], gz[8], minv = 1e300, maxv = -1e300;
+  verts = 0;
+  for (int c = 0; c < 8; c++) {
+    double val = dens[(k + c_corners[c][2]) * sk + (j + c_corners[c][1]) * sj + (i + c_corners[c][0])];
+    cv[c] = val; if (val < minv) minv = val; if (val > maxv) maxv = val;
+  }
+  if (maxv < iso || minv > iso) return 0;
+  for (int c = 0; c < 8; c++) {
+    int ci = i + c_corners[c][0], cj = j + c_corners[c][1], ck = k + c_corners[c][2];
+    int ip = ci + 1 < nx ? ci + 1 : nx, im = ci - 1 > 0 ? ci - 1 : 0;
+    int jp = cj + 1 < ny ? cj + 1 : ny, jm = cj - 1 > 0 ? cj - 1 : 0;
+    int kp = ck + 1 < nz ? ck + 1 : nz, km = ck - 1 > 0 ? ck - 1 : 0;
+    gx[c] = ((double)dens[ck * sk + cj * sj + ip] - (double)dens[ck * sk + cj * sj + im]) / (2 * dx);
+    gy[c] = ((double)dens[ck * sk + jp * sj + ci] - (double)dens[ck * sk + jm * sj + ci]) / (2 * dx);
+    gz[c] = ((double)dens[kp * sk + cj * sj + ci] - (double)dens[km * sk + cj * sj + ci]) / (2 * dx);
+  }
+  double vol = 0;
+  for (int t = 0; t < 6; t++) {
+    int code = 0;
+    for (int c = 0; c < 4; c++) if (cv[c_tets[t][c]] > iso) code |= 1 << c;
+    int ntri = c_ntri[code];
+    for (int e = 0; e < ntri; e++) {
+      double P3[3][3], N3[3][3];
+      for (int vi = 0; vi < 3; vi++) {
+        int ed = c_cases[code][e][vi];
+        int a = c_tets[t][c_edges[ed][0]], b = c_tets[t][c_edges[ed][1]];
+        double va = cv[a], vb = cv[b], den = vb - va;
+        double tt = den != 0 ? (iso - va) / den : 0.5;
+        if (tt < 0) tt = 0; else if (tt > 1) tt = 1;
+        P3[vi][0] = ((i + c_corners[a][0]) + (c_corners[b][0] - c_corners[a][0]) * tt) * dx;
+        P3[vi][1] = ((j + c_corners[a][1]) + (c_corners[b][1] - c_corners[a][1]) * tt) * dx;
+        P3[vi][2] = ((k + c_corners[a][2]) + (c_corners[b][2] - c_corners[a][2]) * tt) * dx;
+        double nxx = -(gx[a] + (gx[b] - gx[a]) * tt), nyy = -(gy[a] + (gy[b] - gy[a]) * tt), nzz = -(gz[a] + (gz[b] - gz[a]) * tt);
+        double nl = sqrt(nxx * nxx + nyy * nyy + nzz * nzz); if (nl == 0) nl = 1;
+        N3[vi][0] = nxx / nl; N3[vi][1] = nyy / nl; N3[vi][2] = nzz / nl;
+      }
+      double ux = P3[1][0] - P3[0][0], uy = P3[1][1] - P3[0][1], uz = P3[1][2] - P3[0][2];
+      double vx = P3[2][0] - P3[0][0], vy = P3[2][1] - P3[0][1], vz = P3[2][2] - P3[0][2];
+      double fnx = uy * vz - uz * vy, fny = uz * vx - ux * vz, fnz = ux * vy - uy * vx;
+      double cgx = N3[0][0] + N3[1][0] + N3[2][0], cgy = N3[0][1] + N3[1][1] + N3[2][1], cgz = N3[0][2] + N3[1][2] + N3[2][2];
+      if (fnx * cgx + fny * cgy + fnz * cgz < 0) {
+        for (int q = 0; q < 3; q++) { double tmp = P3[2][q]; P3[2][q] = P3[1][q]; P3[1][q] = tmp; }
+      }
+      vol += (P3[0][0] * (P3[1][1] * P3[2][2] - P3[2][1] * P3[1][2]) -
+              P3[0][1] * (P3[1][0] * P3[2][2] - P3[2][0] * P3[1][2]) +
+              P3[0][2] * (P3[1][0] * P3[2][1] - P3[2][0] * P3[1][1])) / 6;
+      verts += 3;
+    }
+  }
+  return vol;
+}
+// Block partial sums of the signed volume (FP64) and the vertex count.
+__global__ void k_mt_partial(Dims d, const float* __restrict__ dens, double iso, double2* __restrict__ partials) {
+  __shared__ double sv[32], sc[32];
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double vol = 0, cnt = 0;
+  if (c < d.nCells) {
+    int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+    int v;
+    vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v);
+    cnt = v;
+  }
+  vol = warp_sum(vol); cnt = warp_sum(cnt);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sv[wid] = vol; sc[wid] = cnt; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    vol = lane < nw ? sv[lane] : 0; cnt = lane < nw ? sc[lane] : 0;
+    vol = warp_sum(vol); cnt = warp_sum(cnt);
+    if (lane == 0) partials[blockIdx.x] = make_double2(vol, cnt);
+  }
+}
+// Fixed-order final reduction of double2 partials into out[0..1].
+__global__ void k_reduce_pairs(const double2* __restrict__ partials, int n, double* __restrict__ out) {
+  __shared__ double sa[32], sb[32];
+  double a = 0, b = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { a += partials[i].x; b += partials[i].y; }
+  a = warp_sum(a); b = warp_sum(b);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sa[wid] = a; sb[wid] = b; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    a = lane < nw ? sa[lane] : 0; b = lane < nw ? sb[lane] : 0;
+    a = warp_sum(a); b = warp_sum(b);
+    if (lane == 0) { out[0] = a; out[1] = b; }
+  }
+}
+void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s) {
+  int nb = (int)grid_for(d.nCells, 128);
+  k_mt_partial<<<nb, 128, 0, s>>>(d, dens, iso, partials);
+  k_reduce_pairs<<<1, 1024, 0, s>>>(partials, nb, out);
+}
+
+// ------------------------------------------------------------ particle reductions
+// mode 0: kinetic energy sum of 0.5 mp v^2 (FP64); mode 1: census counts
+// (liquid 0/1/4, ice 5, vapour 2/3) as exact FP64 integers.
+__global__ void k_particle_reduce(PartsDev P, int mode, double mp, double* __restrict__ partials) {
+  __shared__ double s0[32], s1[32], s2[32];
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  double a = 0, b = 0, c = 0;
+  if (p < P.nP) {
+    if (mode == 0) {
+      double vx = P.pvx[p], vy = P.pvy[p], vz = P.pvz[p];
+      a = 0.5 * mp * (vx * vx + vy * vy + vz * vz);
+    } else {
+      int f = P.pflag[p];
+      if (f == 0 || f == 1 || f == 4) a = 1; else if (f == 5) b = 1; else if (f == 2 || f == 3) c = 1;
+    }
+  }
+  a = warp_sum(a); b = warp_sum(b); c = warp_sum(c);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { s0[wid] = a; s1[wid] = b; s2[wid] = c; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    a = lane < nw ? s0[lane] : 0; b = lane < nw ? s1[lane] : 0; c = lane < nw ? s2[lane] : 0;
+    a = warp_sum(a); b = warp_sum(b); c = warp_sum(c);
+    if (lane == 0) { partials[3 * blockIdx.x] = a; partials[3 * blockIdx.x + 1] = b; partials[3 * blockIdx.x + 2] = c; }
+  }
+}
+__global__ void k_reduce_triples(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0, c = 0;
+    for (int i = 0; i < n; i++) { a += partials[3 * i]; b += partials[3 * i + 1]; c += partials[3 * i + 2]; }
+    out[0] = a; out[1] = b; out[2] = c;
+  }
+}
+void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s) {
+  int nb = (int)grid_for(P.nP > 0 ? P.nP : 1, 256);
+  k_particle_reduce<<<nb, 256, 0, s>>>(P, mode, mp, partials);
+  k_reduce_triples<<<1, 32, 0, s>>>(partials, nb, out);
+}

@@ -1,0 +1,506 @@
+// ws_grid.cu — grid-side kernels of the substep (js/solver.js:865-1636, 2629-2653).
+//
+// Each kernel cites the reference lines it restates. Grid kernels are
+// HBM-bound streaming passes; their algorithmic bytes per element are listed
+// next to each launcher and used for the roofline report.
+#include "ws_kernels.cuh"
+
+// ------------------------------------------------------------ face decoding
+struct FaceIJK { int comp, i, j, k; long long local; };
+__device__ __forceinline__ FaceIJK decode_face(const Dims& d, long long f) {
+  FaceIJK r;
+  int nx = d.nx, ny = d.ny;
+  if (f < d.uN) {
+    r.comp = 0; r.local = f;
+    r.i = (int)(f % (nx + 1)); long long t = f / (nx + 1); r.j = (int)(t % ny); r.k = (int)(t / ny);
+  } else if (f < d.uN + d.vN) {
+    r.comp = 1; long long g = f - d.uN; r.local = g;
+    r.i = (int)(g % nx); long long t = g / nx; r.j = (int)(t % (ny + 1)); r.k = (int)(t / (ny + 1));
+  } else {
+    r.comp = 2; long long g = f - d.uN - d.vN; r.local = g;
+    r.i = (int)(g % nx); long long t = g / nx; r.j = (int)(t % ny); r.k = (int)(t / ny);
+  }
+  return r;
+}
+// the two cells a face separates; boundary=true for the domain planes
+__device__ __forceinline__ bool face_cells(const Dims& d, const FaceIJK& F, long long& cL, long long& cR) {
+  long long nx = d.nx, ny = d.ny;
+  if (F.comp == 0) {
+    if (F.i == 0 || F.i == d.nx) return true;
+    cR = ((long long)F.k * ny + F.j) * nx + F.i; cL = cR - 1;
+  } else if (F.comp == 1) {
+    if (F.j == 0 || F.j == d.ny) return true;
+    cR = ((long long)F.k * ny + F.j) * nx + F.i; cL = cR - nx;
+  } else {
+    if (F.k == 0 || F.k == d.nz) return true;
+    cR = ((long long)F.k * ny + F.j) * nx + F.i; cL = cR - nx * ny;
+  }
+  return false;
+}
+
+// ------------------------------------------------------------ static types
+// _rasterizeStatic static part, js/solver.js:872-900: terrain voxel at the
+// cell centre, plus the closed domain shell.
+__global__ void k_static_types(Dims d, TerrainDev t, double coreR, uint8_t* __restrict__ st) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+  bool shell = (j == 0 || j == d.ny - 1 || k == 0 || k == d.nz - 1 || i == 0 || i == d.nx - 1);
+  bool rock;
+  if (t.has) {
+    int vx = jtrunc((i + 0.5) * d.dx / t.dv), vy = jtrunc((j + 0.5) * d.dx / t.dv), vz = jtrunc((k + 0.5) * d.dx / t.dv);
+    if (vx < 0) vx = 0; else if (vx >= t.n) vx = t.n - 1;
+    if (vy < 0) vy = 0; else if (vy >= t.n) vy = t.n - 1;
+    if (vz < 0) vz = 0; else if (vz >= t.n) vz = t.n - 1;
+    rock = t.solid[((long long)vz * t.n + vy) * t.n + vx] == 1;
+  } else {
+    double dx2 = (i + 0.5) * d.dx - d.cx, dy2 = (j + 0.5) * d.dx - d.cy, dz2 = (k + 0.5) * d.dx - d.cz;
+    rock = dx2 * dx2 + dy2 * dy2 + dz2 * dz2 < coreR * coreR;
+  }
+  st[c] = (shell || rock) ? WS_SOLID : WS_AIR;
+}
+void launch_static_types(const Dims& d, const TerrainDev& t, double coreR, uint8_t* st, cudaStream_t s) {
+  k_static_types<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, t, coreR, st);
+}
+
+// _buildPlanetGravity, js/solver.js:1177-1210: unit-g radial geometry per face
+__global__ void k_gravity_geometry(Dims d, double oceanR, float* __restrict__ g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  FaceIJK F = decode_face(d, f);
+  double g0 = oceanR * oceanR, ex, ey, ez, e;
+  if (F.comp == 0) { ex = F.i * d.dx - d.cx; ey = (F.j + 0.5) * d.dx - d.cy; ez = (F.k + 0.5) * d.dx - d.cz; e = ex; }
+  else if (F.comp == 1) { ex = (F.i + 0.5) * d.dx - d.cx; ey = F.j * d.dx - d.cy; ez = (F.k + 0.5) * d.dx - d.cz; e = ey; }
+  else { ex = (F.i + 0.5) * d.dx - d.cx; ey = (F.j + 0.5) * d.dx - d.cy; ez = F.k * d.dx - d.cz; e = ez; }
+  double r3 = pow(ex * ex + ey * ey + ez * ez, 1.5);
+  if (r3 == 0) r3 = 1e-9;
+  g[f] = (float)(-g0 * e / r3);
+}
+void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_t s) {
+  k_gravity_geometry<<<grid_for(d.F, 256), 256, 0, s>>>(d, oceanR, g);
+}
+
+// ------------------------------------------------------------ 1. clear + raster
+// u..wW.fill(0) (js/solver.js:2569-2570) and cellType <- static types
+// (:865-871). Bytes: 8F (acc) + 2N.
+__global__ void k_clear_raster(Dims d, GridDev g, DevStatus* st) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < d.F) g.acc[t] = make_float2(0.f, 0.f);
+  if (t < d.nCells) g.type[t] = g.staticTypes[t];
+  if (t == 0) { st->umaxBits = 0u; st->airborne = 0; st->nFluid = 0; }
+}
+void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s) {
+  long long n = d.F > d.nCells ? d.F : d.nCells;
+  k_clear_raster<<<grid_for(n, 256), 256, 0, s>>>(d, g, st);
+}
+
+// ------------------------------------------------------------ 2. mark fluid
+// _markFluidCells, js/solver.js:945-1000 (sphere). Bytes: 13P + N.
+__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  if (P.pflag[p] != 0) return;
+  double X = P.px[p], Y = P.py[p], Z = P.pz[p];
+  double rx = X - d.cx, ry = Y - d.cy, rz = Z - d.cz;
+  double radius2 = rx * rx + ry * ry + rz * rz;
+  double skyAlt = 2 * d.dx > 0.3 ? 2 * d.dx : 0.3;
+  if (radius2 > (oceanR + 0.3) * (oceanR + 0.3) &&
+      sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > skyAlt &&
+      !(t.has && rock_cell_at(d, g.staticTypes, X, Y, Z))) {
+    P.pflag[p] = 1; return;
+  }
+  int i = jfloor_clamp(X / d.dx, 0, d.nx - 1);
+  int j = jfloor_clamp(Y / d.dx, 0, d.ny - 1);
+  int k = jfloor_clamp(Z / d.dx, 0, d.nz - 1);
+  if (j >= d.ny - 2) {
+    if (sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > 0.3) { P.pflag[p] = 1; return; }
+  }
+  long long idx = ((long long)k * d.ny + j) * d.nx + i;
+  if (g.type[idx] == WS_AIR) g.type[idx] = WS_FLUID;   // idempotent byte store
+}
+void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
+                       double oceanR, double coreR, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  k_mark_fluid<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR);
+}
+
+// ------------------------------------------------------------ 3. P2G scatter
+// _p2gInto, js/solver.js:1035-1105: trilinear momentum + weight per face,
+// one float2 vector atomic per face (momentum, weight).
+__device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc, int comp,
+                                         double x, double y, double z, double vel) {
+  int i0, j0, k0; double tx, ty, tz; long long idx, sj, sk;
+  face_coords(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
+  face_strides(d, comp, i0, j0, k0, idx, sj, sk);
+  double s0 = 1 - tx, s1 = tx, t0 = 1 - ty, t1 = ty, r0 = 1 - tz, r1 = tz;
+  double wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
+  double w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
+  long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj, idx + sk + sj + 1 };
+#pragma unroll
+  for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2((float)(w8[q] * vel), (float)w8[q]));
+}
+__global__ void k_p2g(Dims d, GridDev g, PartsDev P) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP) return;
+  if (P.pflag[p] != 0) return;
+  double x = P.px[p], y = P.py[p], z = P.pz[p];
+  p2g_comp(d, g.acc, 0, x, y, z, P.pvx[p]);
+  p2g_comp(d, g.acc, 1, x, y, z, P.pvy[p]);
+  p2g_comp(d, g.acc, 2, x, y, z, P.pvz[p]);
+}
+void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s) {
+  if (P.nP <= 0) return;
+  k_p2g<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P);
+}
+
+// ------------------------------------------------------------ 4. faces pass 1
+// _p2gNormalizeFace (:1109-1120) + _applyBC (:1130-1171, no moving solids)
+// + FLIP snapshot (:2579) + the extrapolation valid mark (:1578-1611).
+// Bytes: 8F read + 4F vel + 4F velO + 1F valid + 2 type reads per face.
+__global__ void k_faces_normalize_bc(Dims d, GridDev g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  float2 a = g.acc[f];
+  float u = a.x;
+  if ((double)a.y > 1e-8) u = (float)((double)a.x / (double)a.y);
+  FaceIJK F = decode_face(d, f);
+  long long cL = 0, cR = 0;
+  bool solidAdj = face_cells(d, F, cL, cR);
+  if (!solidAdj) solidAdj = g.type[cL] == WS_SOLID || g.type[cR] == WS_SOLID;
+  if (solidAdj) u = 0.f;
+  g.vel[f] = u;
+  g.velO[f] = u;
+  g.valid[f] = ((double)a.y > 1e-8 || solidAdj) ? 1 : 0;
+}
+void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s) {
+  k_faces_normalize_bc<<<grid_for(d.F, 256), 256, 0, s>>>(d, g);
+}
+
+// ------------------------------------------------------------ 5. forces
+// _viscosity (:1259-1304, Jacobi: neighbours from the snapshot, which equals
+// the post-BC field on entry), planet gravity (:1229-1256 with the ramp of
+// :2656-2662 applied by the caller in gs) and the BC again (:2598).
+__global__ void k_faces_forces(Dims d, GridDev g, double coef, int viscOn, double dt, double gs) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  FaceIJK F = decode_face(d, f);
+  long long cL = 0, cR = 0;
+  if (face_cells(d, F, cL, cR)) { g.vel[f] = 0.f; return; }
+  int tL = g.type[cL], tR = g.type[cR];
+  if (tL == WS_SOLID || tR == WS_SOLID) { g.vel[f] = 0.f; return; }
+  const float* __restrict__ o = g.velO;
+  float u = o[f];
+  if (viscOn && tL == WS_FLUID && tR == WS_FLUID) {
+    int nx = d.nx, ny = d.ny, nz = d.nz;
+    long long sI = 1, sJ, sK; int iLo, iHi, jLo, jHi, kLo, kHi;
+    if (F.comp == 0) { sJ = nx + 1; sK = (long long)ny * (nx + 1);
+      iLo = F.i - 1 >= 0; iHi = F.i + 1 <= nx; jLo = F.j - 1 >= 0; jHi = F.j + 1 < ny; kLo = F.k - 1 >= 0; kHi = F.k + 1 < nz; }
+    else if (F.comp == 1) { sJ = nx; sK = (long long)(ny + 1) * nx;
+      iLo = F.i - 1 >= 0; iHi = F.i + 1 < nx; jLo = F.j - 1 >= 0; jHi = F.j + 1 <= ny; kLo = F.k - 1 >= 0; kHi = F.k + 1 < nz; }
+    else { sJ = nx; sK = (long long)ny * nx;
+      iLo = F.i - 1 >= 0; iHi = F.i + 1 < nx; jLo = F.j - 1 >= 0; jHi = F.j + 1 < ny; kLo = F.k - 1 >= 0; kHi = F.k + 1 <= nz; }
+    double c0 = o[f];
+    double val = c0 * 6;
+    val -= iLo ? (double)o[f - sI] : c0;
+    val -= iHi ? (double)o[f + sI] : c0;
+    val -= jLo ? (double)o[f - sJ] : c0;
+    val -= jHi ? (double)o[f + sJ] : c0;
+    val -= kLo ? (double)o[f - sK] : c0;
+    val -= kHi ? (double)o[f + sK] : c0;
+    u = (float)(c0 + coef * val);
+  }
+  if (gs > 0 && (tL == WS_FLUID || tR == WS_FLUID)) u = (float)((double)u + (double)g.gvel[f] * dt * gs);
+  g.vel[f] = u;
+}
+void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s) {
+  k_faces_forces<<<grid_for(d.F, 256), 256, 0, s>>>(d, g, coef, viscOn, dt, gs);
+}
+
+// ------------------------------------------------------------ 6. pressure setup
+// _pressureSolve passes 1-2, js/solver.js:1321-1366: q = 0 off the fluid,
+// diag = Nf + Na, rhs = -dx^2 div, relaxation weight pw = omega/diag
+// (float32, as the reference's pW). pw < 0 marks a non-fluid cell.
+__global__ void k_pressure_setup(Dims d, GridDev g, uint8_t* __restrict__ diag8, double omega, DevStatus* st) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  const uint8_t* type = g.type;
+  if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; return; }
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
+                       j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
+  int cnt = 0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) if (nbr[q] >= 0 && type[nbr[q]] != WS_SOLID) cnt++;
+  const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
+  double div = ((double)u[((long long)k * ny + j) * (nx + 1) + i + 1] - (double)u[((long long)k * ny + j) * (nx + 1) + i] +
+                (double)v[((long long)k * (ny + 1) + j + 1) * nx + i] - (double)v[((long long)k * (ny + 1) + j) * nx + i] +
+                (double)w[((long long)(k + 1) * ny + j) * nx + i] - (double)w[((long long)k * ny + j) * nx + i]) / d.dx;
+  g.rhs[c] = (float)(-d.dx * d.dx * div);
+  g.pw[c] = (float)(cnt > 0 ? omega / (double)cnt : 0.0);
+  diag8[c] = (uint8_t)cnt;
+  atomicAdd(&st->nFluid, 1);
+}
+void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, cudaStream_t s) {
+  k_pressure_setup<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, g, diag8, omega, st);
+}
+
+// ------------------------------------------------------------ 7. red-black SOR
+// One colour of the SOR sweep, js/solver.js:1397-1404 in red-black order:
+// q <- q (1 - omega) + pw (rhs + sum of the six neighbour q), FP64 arithmetic
+// rounded to float32 as the reference's Float32Array store. q is zero on
+// every non-fluid cell, so summing all six neighbours in the reference's
+// order (-x, +x, -y, +y, -z, +z) equals its sum over fluid neighbours.
+// The thread layout packs the cells of one colour: thread t -> row r, slot s,
+// i = 2 s + ((j + k + colour) & 1). Bytes per full iteration: 13 per cell.
+__global__ void k_sor_color(Dims d, float* __restrict__ q, const float* __restrict__ rhs,
+                            const float* __restrict__ pw, int color, double om1) {
+  int nx = d.nx, ny = d.ny, nz = d.nz;
+  int half = (nx + 1) >> 1;
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long rows = (long long)ny * nz;
+  if (t >= rows * half) return;
+  int sl = (int)(t % half); long long r = t / half;
+  int j = (int)(r % ny), k = (int)(r / ny);
+  int i = 2 * sl + ((j + k + color) & 1);
+  if (i >= nx) return;
+  long long c = r * nx + i;
+  float w = pw[c];
+  if (w < 0.f) return;
+  if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2 || k < 1 || k > nz - 2) return;
+  long long nxy = (long long)nx * ny;
+  double sum = (double)q[c - 1];
+  sum += (double)q[c + 1];
+  sum += (double)q[c - nx];
+  sum += (double)q[c + nx];
+  sum += (double)q[c - nxy];
+  sum += (double)q[c + nxy];
+  q[c] = (float)((double)q[c] * om1 + (double)w * ((double)rhs[c] + sum));
+}
+void launch_sor_color(const Dims& d, const GridDev& g, int color, double om1, cudaStream_t s) {
+  long long n = (long long)d.ny * d.nz * ((d.nx + 1) >> 1);
+  k_sor_color<<<grid_for(n, 256), 256, 0, s>>>(d, g.q, g.rhs, g.pw, color, om1);
+}
+
+// ------------------------------------------------------------ 8. FP64 residual
+// ||b - A q||_2 / ||b||_2 over fluid cells with A, b the reference assembly
+// (js/solver.js:1361-1365): r = rhs + sum_fluid q_n - diag q. Block partials
+// in FP64, combined in a fixed order by k_residual_final (deterministic).
+__global__ void k_residual_partial(Dims d, const float* __restrict__ q, const float* __restrict__ rhs,
+                                   const float* __restrict__ pw, const uint8_t* __restrict__ diag8,
+                                   double2* __restrict__ partials) {
+  __shared__ double srr[32], sbb[32];
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double rr = 0, bb = 0;
+  bool interior = false;
+  if (c < d.nCells) {
+    int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+    interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
+  }
+  if (interior && pw[c] >= 0.f) {
+    int nx = d.nx; long long nxy = (long long)nx * d.ny;
+    double sum = (double)q[c - 1];
+    sum += (double)q[c + 1]; sum += (double)q[c - nx]; sum += (double)q[c + nx];
+    sum += (double)q[c - nxy]; sum += (double)q[c + nxy];
+    double b = rhs[c];
+    double r = b + sum - (double)diag8[c] * (double)q[c];
+    rr = r * r; bb = b * b;
+  }
+  rr = warp_sum(rr); bb = warp_sum(bb);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { srr[wid] = rr; sbb[wid] = bb; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    rr = lane < nw ? srr[lane] : 0; bb = lane < nw ? sbb[lane] : 0;
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    if (lane == 0) partials[blockIdx.x] = make_double2(rr, bb);
+  }
+}
+__global__ void k_residual_final(const double2* __restrict__ partials, int n, DevStatus* st, double* hostMirror) {
+  __shared__ double srr[32], sbb[32];
+  double rr = 0, bb = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) { rr += partials[i].x; bb += partials[i].y; }
+  rr = warp_sum(rr); bb = warp_sum(bb);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { srr[wid] = rr; sbb[wid] = bb; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    rr = lane < nw ? srr[lane] : 0; bb = lane < nw ? sbb[lane] : 0;
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    if (lane == 0) {
+      double rel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
+      st->rr = rr; st->bb = bb; st->relres = rel;
+      if (hostMirror) *hostMirror = rel;
+    }
+  }
+}
+int residual_blocks(const Dims& d) { return (int)grid_for(d.nCells, 256); }
+void launch_residual(const Dims& d, const GridDev& g, const uint8_t* diag8, double2* partials,
+                     DevStatus* st, double* hostMirror, cudaStream_t s) {
+  int nb = residual_blocks(d);
+  k_residual_partial<<<nb, 256, 0, s>>>(d, g.q, g.rhs, g.pw, diag8, partials);
+  k_residual_final<<<1, 1024, 0, s>>>(partials, nb, st, hostMirror);
+}
+
+// ------------------------------------------------------------ 9. project (+clamp)
+// _projectSlice (:1417-1443) and, fused when vorticity is off,
+// _clampUmSlice (:2629-2653) with the max |u| reduction (exact: max of
+// non-negative float bit patterns).
+__device__ __forceinline__ void umax_reduce(float a, DevStatus* st) {
+  unsigned bits = __float_as_uint(fabsf(a));
+  bits = warp_max_u(bits);
+  if ((threadIdx.x & 31) == 0) atomicMax(&st->umaxBits, bits);
+}
+__global__ void k_project(Dims d, GridDev g, int doClamp, float vcap, DevStatus* st) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float u = 0.f;
+  if (f < d.F) {
+    u = g.vel[f];
+    FaceIJK F = decode_face(d, f);
+    long long cL = 0, cR = 0;
+    if (!face_cells(d, F, cL, cR)) {
+      int tL = g.type[cL], tR = g.type[cR];
+      if (tL != WS_SOLID && tR != WS_SOLID) {
+        double pL = tL == WS_FLUID ? (double)g.q[cL] : 0.0, pR = tR == WS_FLUID ? (double)g.q[cR] : 0.0;
+        u = (float)((double)u - (pR - pL) * (1.0 / d.dx));
+      }
+    }
+    if (doClamp) { if (u > vcap) u = vcap; else if (u < -vcap) u = -vcap; }
+    g.vel[f] = u;
+  }
+  if (doClamp) umax_reduce(u, st);
+}
+void launch_project(const Dims& d, const GridDev& g, int doClamp, double maxSpeed, DevStatus* st, cudaStream_t s) {
+  k_project<<<grid_for(d.F, 256), 256, 0, s>>>(d, g, doClamp, (float)(maxSpeed * 1.1), st);
+}
+__global__ void k_clamp_umax(Dims d, float* __restrict__ vel, float vcap, DevStatus* st) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float u = 0.f;
+  if (f < d.F) {
+    u = vel[f];
+    if (u > vcap) { u = vcap; vel[f] = u; } else if (u < -vcap) { u = -vcap; vel[f] = u; }
+  }
+  umax_reduce(u, st);
+}
+void launch_clamp_umax(const Dims& d, const GridDev& g, double maxSpeed, DevStatus* st, cudaStream_t s) {
+  k_clamp_umax<<<grid_for(d.F, 256), 256, 0, s>>>(d, g.vel, (float)(maxSpeed * 1.1), st);
+}
+
+// ------------------------------------------------------------ 10. vorticity
+// _vorticityConfinement, js/solver.js:1454-1559. (a) omega per cell from the
+// float32 cell-centred velocities (recomputed from the faces, rounded as the
+// reference stores them), (b) the gated confinement force per fluid cell,
+// (c) the splat onto faces between two fluid cells.
+__device__ __forceinline__ float ccx(const Dims& d, const float* u, long long c) {
+  long long nx = d.nx; long long row = c / nx, i = c % nx;
+  long long ui = row * (nx + 1) + i;
+  return (float)(0.5 * ((double)u[ui] + (double)u[ui + 1]));
+}
+__device__ __forceinline__ float ccy(const Dims& d, const float* v, long long c) {
+  long long nx = d.nx, ny = d.ny; long long i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+  long long vi = (k * (ny + 1) + j) * nx + i;
+  return (float)(0.5 * ((double)v[vi] + (double)v[vi + nx]));
+}
+__device__ __forceinline__ float ccz(const Dims& d, const float* w, long long c) {
+  long long nxy = (long long)d.nx * d.ny;
+  return (float)(0.5 * ((double)w[c] + (double)w[c + nxy]));
+}
+__global__ void k_vort_omega(Dims d, GridDev g) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
+  long long im = i > 0 ? c - 1 : c, ip = i < nx - 1 ? c + 1 : c;
+  long long jm = j > 0 ? c - nx : c, jp = j < ny - 1 ? c + nx : c;
+  long long km = k > 0 ? c - nxy : c, kp = k < nz - 1 ? c + nxy : c;
+  double inv2 = 0.5 / d.dx;
+  double wx = ((double)ccz(d, w, jp) - (double)ccz(d, w, jm) - ((double)ccy(d, v, kp) - (double)ccy(d, v, km))) * inv2;
+  double wy = ((double)ccx(d, u, kp) - (double)ccx(d, u, km) - ((double)ccz(d, w, ip) - (double)ccz(d, w, im))) * inv2;
+  double wz = ((double)ccy(d, v, ip) - (double)ccy(d, v, im) - ((double)ccx(d, u, jp) - (double)ccx(d, u, jm))) * inv2;
+  g.omx[c] = (float)wx; g.omy[c] = (float)wy; g.omz[c] = (float)wz;
+  g.omg[c] = (float)sqrt(wx * wx + wy * wy + wz * wz);
+}
+__global__ void k_vort_force(Dims d, GridDev g, double eps, double dt) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  const uint8_t* type = g.type;
+  if (type[c] != WS_FLUID) return;
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  const float* omg = g.omg;
+  if (omg[c] < 0.35f ||
+      (i > 0 && type[c - 1] != WS_FLUID) || (i < nx - 1 && type[c + 1] != WS_FLUID) ||
+      (j > 0 && type[c - nx] != WS_FLUID) || (j < ny - 1 && type[c + nx] != WS_FLUID) ||
+      (k > 0 && type[c - nxy] != WS_FLUID) || (k < nz - 1 && type[c + nxy] != WS_FLUID)) {
+    g.vfx[c] = 0.f; g.vfy[c] = 0.f; g.vfz[c] = 0.f; return;
+  }
+  double gx = (double)omg[i < nx - 1 ? c + 1 : c] - (double)omg[i > 0 ? c - 1 : c];
+  double gy = (double)omg[j < ny - 1 ? c + nx : c] - (double)omg[j > 0 ? c - nx : c];
+  double gz = (double)omg[k < nz - 1 ? c + nxy : c] - (double)omg[k > 0 ? c - nxy : c];
+  double g2 = gx * gx + gy * gy + gz * gz;
+  if (g2 < 1e-12) { g.vfx[c] = 0.f; g.vfy[c] = 0.f; g.vfz[c] = 0.f; return; }
+  double inv = 1 / sqrt(g2);
+  double Nx = gx * inv, Ny = gy * inv, Nz = gz * inv;
+  double ox = g.omx[c], oy = g.omy[c], oz = g.omz[c];
+  double fx = eps * (Ny * oz - Nz * oy), fy = eps * (Nz * ox - Nx * oz), fz = eps * (Nx * oy - Ny * ox);
+  double f2 = fx * fx + fy * fy + fz * fz, fCap = 6.0;
+  if (f2 > fCap * fCap) { double fs = fCap / sqrt(f2); fx *= fs; fy *= fs; fz *= fs; }
+  g.vfx[c] = (float)(fx * dt); g.vfy[c] = (float)(fy * dt); g.vfz[c] = (float)(fz * dt);
+}
+__global__ void k_vort_splat(Dims d, GridDev g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  FaceIJK F = decode_face(d, f);
+  long long cL = 0, cR = 0;
+  if (face_cells(d, F, cL, cR)) return;
+  if (g.type[cL] != WS_FLUID || g.type[cR] != WS_FLUID) return;
+  const float* fv = F.comp == 0 ? g.vfx : (F.comp == 1 ? g.vfy : g.vfz);
+  g.vel[f] = (float)((double)g.vel[f] + 0.5 * ((double)fv[cL] + (double)fv[cR]));
+}
+void launch_vorticity(const Dims& d, const GridDev& g, double eps, double dt, cudaStream_t s) {
+  k_vort_omega<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, g);
+  k_vort_force<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, g, eps, dt);
+  k_vort_splat<<<grid_for(d.F, 256), 256, 0, s>>>(d, g);
+}
+
+// ------------------------------------------------------------ 11. extrapolate
+// _extrapolate, js/solver.js:1562-1636 in Jacobi order: an invalid face takes
+// the mean of the neighbours (same component grid) that were valid before
+// the pass, summed in the reference's order -i, +i, -j, +j, -k, +k. Filled
+// faces are marked 2 so no thread reads a value written in this pass.
+__global__ void k_extrapolate(Dims d, GridDev g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  const uint8_t* valid = g.valid;
+  if (valid[f] != 0) return;
+  FaceIJK F = decode_face(d, f);
+  int d0, d1, d2;
+  if (F.comp == 0) { d0 = d.nx + 1; d1 = d.ny; d2 = d.nz; }
+  else if (F.comp == 1) { d0 = d.nx; d1 = d.ny + 1; d2 = d.nz; }
+  else { d0 = d.nx; d1 = d.ny; d2 = d.nz + 1; }
+  long long sK = (long long)d0 * d1;
+  const float* a = g.vel;
+  double sum = 0; int cnt = 0;
+  if (F.i > 0 && valid[f - 1] == 1) { sum += a[f - 1]; cnt++; }
+  if (F.i < d0 - 1 && valid[f + 1] == 1) { sum += a[f + 1]; cnt++; }
+  if (F.j > 0 && valid[f - d0] == 1) { sum += a[f - d0]; cnt++; }
+  if (F.j < d1 - 1 && valid[f + d0] == 1) { sum += a[f + d0]; cnt++; }
+  if (F.k > 0 && valid[f - sK] == 1) { sum += a[f - sK]; cnt++; }
+  if (F.k < d2 - 1 && valid[f + sK] == 1) { sum += a[f + sK]; cnt++; }
+  if (cnt > 0) { g.vel[f] = (float)(sum / cnt); g.valid[f] = 2; }
+}
+void launch_extrapolate(const Dims& d, const GridDev& g, cudaStream_t s) {
+  k_extrapolate<<<grid_for(d.F, 256), 256, 0, s>>>(d, g);
+}
+
+// ------------------------------------------------------------ field helpers
+__global__ void k_extract_weight(Dims d, const float2* __restrict__ acc, float* __restrict__ out, long long off, long long n) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n) out[t] = acc[off + t].y;
+}
+void launch_extract_weight(const Dims& d, const float2* acc, float* out, long long off, long long n, cudaStream_t s) {
+  k_extract_weight<<<grid_for(n, 256), 256, 0, s>>>(d, acc, out, off, n);
+}

@@ -1,0 +1,189 @@
+// ws_internal.cuh — device state and shared device helpers of libwatersim.
+//
+// Memory layout in HBM (one handle):
+//   particles  SoA, float32 px..pPh, uint8 pflag/pcool/pDepth, capacity each;
+//              kept in reference index order so the serial RNG streams of
+//              the reference (_evS, _cfS, _bfS) are consumed in its order.
+//   faces      vel = u | v | w contiguous (F = uN + vN + wN floats); the same
+//              for the snapshot velO, the gravity geometry gvel and the P2G
+//              accumulator acc (float2 momentum, weight per face).
+//              Index formulas of the reference (js/solver.js:88-113):
+//              u (k*ny+j)*(nx+1)+i, v (k*(ny+1)+j)*nx+i, w (k*ny+j)*nx+i.
+//   cells      cellType u8, q/rhs/pw float32, cell (k*ny+j)*nx+i.
+//
+// Arithmetic: kernels evaluate in FP64 and store FP32, mirroring the
+// reference (JavaScript doubles over Float32Array storage); the library is
+// built with -fmad=false because JavaScript never fuses a multiply-add.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+#include "../../include/watersim.h"
+
+#define WS_AIR 0
+#define WS_FLUID 1
+#define WS_SOLID 2
+
+// device error bits latched in DevStatus::err
+#define WS_DERR_NAN 1
+#define WS_DERR_RANGE 2
+#define WS_DERR_TIMEOUT 4
+
+struct Dims {
+  int nx, ny, nz;
+  double dx, W, H, D, cx, cy, cz, domainR;
+  long long nCells, uN, vN, wN, F;
+};
+
+struct TerrainDev {
+  int n, has;
+  double dv, Rsl, Rlo, Rhi, Rlo2, Rhi2;
+  const uint8_t* __restrict__ solid;
+  const float* __restrict__ R;
+};
+
+struct PartsDev {
+  float *px, *py, *pz, *pvx, *pvy, *pvz, *pT, *pAir, *pLight, *pWx, *pWy, *pWz, *pPh;
+  uint8_t *pflag, *pcool, *pDepth;
+  int nP;
+};
+
+// per-substep device counters (zeroed by the raster kernel)
+struct DevStatus {
+  unsigned int umaxBits;   // max |u| as float bits (non-negative floats order as ints)
+  int airborne;
+  int nFluid;
+  int err;
+  int vaporCount, nightVapor, evapCount, pad;
+  int cfA, bfB;            // draws consumed by the vapour pass (diagnostic)
+  double relres;
+  double rr, bb;
+};
+
+struct GridDev {
+  uint8_t* type;
+  const uint8_t* staticTypes;
+  float* vel;
+  float* velO;
+  float2* acc;
+  uint8_t* valid;
+  const float* gvel;
+  float *q, *rhs, *pw;
+  float *vfx, *vfy, *vfz, *omg, *omx, *omy, *omz;
+  float* dens;
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ int jtrunc(double v) { return (int)v; }
+__device__ __forceinline__ int jfloor_clamp(double v, int a, int b) {
+  double f = floor(v);
+  if (f < a) return a;
+  if (f > b) return b;
+  return (int)f;
+}
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ uint32_t lcg_next(uint32_t s) { return s * 1664525u + 1013904223u; }
+
+// LCG jump-ahead: the affine map s -> a s + c composed k times, by square
+// and multiply (mod 2^32 arithmetic is exact in uint32).
+__host__ __device__ __forceinline__ uint32_t lcg_jump(uint32_t s, uint32_t k) {
+  uint32_t A = 1u, Cc = 0u, a = 1664525u, c = 1013904223u;
+  while (k) {
+    if (k & 1u) { A = A * a; Cc = Cc * a + c; }
+    c = c * (a + 1u); a = a * a;
+    k >>= 1;
+  }
+  return A * s + Cc;
+}
+
+// terrainRadiusAt, js/solver.js:512-535
+__device__ __forceinline__ double terrain_radius_at(const TerrainDev& t, double coreR, double x, double y, double z) {
+  if (!t.has) return coreR;
+  int n = t.n; double dv = t.dv;
+  double gx = x / dv - 0.5, gy = y / dv - 0.5, gz = z / dv - 0.5;
+  int i = jtrunc(gx), j = jtrunc(gy), k = jtrunc(gz);
+  if (i < 0) i = 0; else if (i > n - 2) i = n - 2;
+  if (j < 0) j = 0; else if (j > n - 2) j = n - 2;
+  if (k < 0) k = 0; else if (k > n - 2) k = n - 2;
+  double fx = gx - i, fy = gy - j, fz = gz - k;
+  if (fx < 0) fx = 0; else if (fx > 1) fx = 1;
+  if (fy < 0) fy = 0; else if (fy > 1) fy = 1;
+  if (fz < 0) fz = 0; else if (fz > 1) fz = 1;
+  long long b000 = ((long long)k * n + j) * n + i, s7 = (long long)n * n;
+  const float* R = t.R;
+  double v000 = R[b000], v100 = R[b000 + 1];
+  double v010 = R[b000 + n], v110 = R[b000 + n + 1];
+  double v001 = R[b000 + s7], v101 = R[b000 + s7 + 1];
+  double v011 = R[b000 + s7 + n], v111 = R[b000 + s7 + n + 1];
+  double a0 = v000 + (v100 - v000) * fx, a1 = v010 + (v110 - v010) * fx;
+  double a2 = v001 + (v101 - v001) * fx, a3 = v011 + (v111 - v011) * fx;
+  double b0 = a0 + (a1 - a0) * fy, b1 = a2 + (a3 - a2) * fy;
+  return b0 + (b1 - b0) * fz;
+}
+
+// _rockCellAt, js/solver.js:542-559: the static cell type at the clamped
+// cell equals the voxel at the cell centre (rock) for interior cells.
+__device__ __forceinline__ bool rock_cell_at(const Dims& d, const uint8_t* __restrict__ staticTypes,
+                                             double x, double y, double z) {
+  int i = jtrunc(x / d.dx), j = jtrunc(y / d.dx), k = jtrunc(z / d.dx);
+  if (i < 1) i = 1; else if (i > d.nx - 2) i = d.nx - 2;
+  if (j < 1) j = 1; else if (j > d.ny - 2) j = d.ny - 2;
+  if (k < 1) k = 1; else if (k > d.nz - 2) k = d.nz - 2;
+  return staticTypes[((long long)k * d.ny + j) * d.nx + i] == WS_SOLID;
+}
+
+// Face-grid coordinates of component comp, js/solver.js:737-748
+__device__ __forceinline__ void face_coords(const Dims& d, int comp, double x, double y, double z,
+                                            int& i0, int& j0, int& k0, double& tx, double& ty, double& tz) {
+  double a, b, c, dx = d.dx;
+  if (comp == 0) { a = x / dx; b = y / dx - 0.5; c = z / dx - 0.5; }
+  else if (comp == 1) { a = x / dx - 0.5; b = y / dx; c = z / dx - 0.5; }
+  else { a = x / dx - 0.5; b = y / dx - 0.5; c = z / dx; }
+  double fi = floor(a), fj = floor(b), fk = floor(c);
+  if (fi < 0) { i0 = 0; tx = 0; } else if (fi > d.nx - 1) { i0 = d.nx - 1; tx = 1; } else { i0 = (int)fi; tx = a - fi; }
+  if (fj < 0) { j0 = 0; ty = 0; } else if (fj > d.ny - 2) { j0 = d.ny - 2; ty = 1; } else { j0 = (int)fj; ty = b - fj; }
+  if (fk < 0) { k0 = 0; tz = 0; } else if (fk > d.nz - 2) { k0 = d.nz - 2; tz = 1; } else { k0 = (int)fk; tz = c - fk; }
+}
+// flat offset into vel (u|v|w) and the j/k strides of component comp
+__device__ __forceinline__ void face_strides(const Dims& d, int comp, int i0, int j0, int k0,
+                                             long long& idx, long long& sj, long long& sk) {
+  int nx = d.nx, ny = d.ny;
+  if (comp == 0) { sj = nx + 1; sk = (long long)ny * (nx + 1); idx = ((long long)k0 * ny + j0) * (nx + 1) + i0; }
+  else if (comp == 1) { sj = nx; sk = (long long)(ny + 1) * nx; idx = d.uN + ((long long)k0 * (ny + 1) + j0) * nx + i0; }
+  else { sj = nx; sk = (long long)ny * nx; idx = d.uN + d.vN + ((long long)k0 * ny + j0) * nx + i0; }
+}
+__device__ __forceinline__ double tri_sample(const float* __restrict__ a, long long idx, long long sj, long long sk,
+                                             double tx, double ty, double tz) {
+  double s0 = 1 - tx, s1 = tx, t0 = 1 - ty, t1 = ty, r0 = 1 - tz, r1 = tz;
+  long long o1 = idx + sj, o2 = idx + sk, o3 = o2 + sj;
+  return (((double)a[idx] * s0 + (double)a[idx + 1] * s1) * t0 + ((double)a[o1] * s0 + (double)a[o1 + 1] * s1) * t1) * r0
+       + (((double)a[o2] * s0 + (double)a[o2 + 1] * s1) * t0 + ((double)a[o3] * s0 + (double)a[o3 + 1] * s1) * t1) * r1;
+}
+// _sampleVel3, js/solver.js:820-854
+__device__ __forceinline__ void sample_vel3(const Dims& d, const float* __restrict__ vel, double x, double y, double z,
+                                            double& ox, double& oy, double& oz) {
+  int i0, j0, k0; double tx, ty, tz; long long idx, sj, sk;
+  face_coords(d, 0, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
+  ox = tri_sample(vel, idx, sj, sk, tx, ty, tz);
+  face_coords(d, 1, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
+  oy = tri_sample(vel, idx, sj, sk, tx, ty, tz);
+  face_coords(d, 2, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
+  oz = tri_sample(vel, idx, sj, sk, tx, ty, tz);
+}
+
+// block-wide helpers
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ unsigned warp_max_u(unsigned v) {
+  for (int o = 16; o > 0; o >>= 1) { unsigned t = __shfl_down_sync(0xffffffffu, v, o); v = t > v ? t : v; }
+  return v;
+}
+
+static inline unsigned grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  return (unsigned)(g < 1 ? 1 : g);
+}

@@ -1,0 +1,72 @@
+// ws_kernels.cuh — kernel parameter blocks and launcher declarations.
+#pragma once
+#include "ws_internal.cuh"
+
+struct AdvectParams {
+  double dt, dtLast, pic, maxSpeed, gravity, oceanR, coreR, atmosphereH;
+  double rainTe, rainLiftAge;
+  double windS[3];
+  int ceilReflect;
+};
+
+struct HeatParams {
+  int hasSun;
+  double sun[3];
+  double sunActivity, Tamb, shadeCool, heatK, coreR;
+};
+
+struct PhaseParams {
+  double cloudT, cloudP, rainT, snowT, meltT, rainLiftAge, cloudBase, dt;
+  int spinOn;
+  uint32_t tick;
+};
+
+// ---- ws_grid.cu
+void launch_static_types(const Dims& d, const TerrainDev& t, double coreR, uint8_t* st, cudaStream_t s);
+void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_t s);
+void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s);
+void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
+                       double oceanR, double coreR, cudaStream_t s);
+void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s);
+void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s);
+void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s);
+void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, cudaStream_t s);
+void launch_sor_color(const Dims& d, const GridDev& g, int color, double om1, cudaStream_t s);
+int residual_blocks(const Dims& d);
+void launch_residual(const Dims& d, const GridDev& g, const uint8_t* diag8, double2* partials,
+                     DevStatus* st, double* hostMirror, cudaStream_t s);
+void launch_project(const Dims& d, const GridDev& g, int doClamp, double maxSpeed, DevStatus* st, cudaStream_t s);
+void launch_clamp_umax(const Dims& d, const GridDev& g, double maxSpeed, DevStatus* st, cudaStream_t s);
+void launch_vorticity(const Dims& d, const GridDev& g, double eps, double dt, cudaStream_t s);
+void launch_extrapolate(const Dims& d, const GridDev& g, cudaStream_t s);
+void launch_extract_weight(const Dims& d, const float2* acc, float* out, long long off, long long n, cudaStream_t s);
+
+// ---- ws_particles.cu
+void launch_g2p_advect(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
+                       const AdvectParams& ap, DevStatus* st, cudaStream_t s);
+void launch_compact(const uint8_t* fl, int nP, int mode, int* blockCounts, int* out, int* total, cudaStream_t s);
+void launch_vapor_advect(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t, const AdvectParams& ap,
+                         const int* vIdx, const int* nV, uint32_t* rng, DevStatus* st, cudaStream_t s);
+void launch_impulse_sphere(const PartsDev& P, double cx, double cy, double cz, double R, double fx, double fy, double fz, cudaStream_t s);
+void launch_stir_at(const PartsDev& P, double cx, double cy, double cz, double vx, double vy, double vz, double R, double dt, cudaStream_t s);
+void launch_stir_gaussian(const PartsDev& P, double pcx, double pcy, double pcz, double tx, double ty, double tz,
+                          double sigma, double peak, cudaStream_t s);
+
+// ---- ws_frame.cu
+void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t, const HeatParams& hp,
+                 double dt, int* cnt, double* sumT, double* change, cudaStream_t s);
+void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
+                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, DevStatus* st, cudaStream_t s);
+void launch_phase(const Dims& d, const GridDev& g, const PartsDev& P, const PhaseParams& pp, int* cnt, cudaStream_t s);
+void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
+                         double oceanR, double coreR, double atmosphereH, cudaStream_t s);
+void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spacing, cudaStream_t s);
+void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s);
+void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);
+
+// ---- ws_contacts.cu
+void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,
+                             int hasSun, const double* sunRel, void* scratch, size_t scratchBytes,
+                             DevStatus* st, cudaStream_t s);
+void launch_ice_contacts(const PartsDev& P, double spacing, void* scratch, size_t scratchBytes, cudaStream_t s);
+size_t contacts_scratch_bytes(int capacity);

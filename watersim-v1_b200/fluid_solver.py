@@ -1,0 +1,389 @@
+"""Host-side mirror of WaterSim's FluidSolver (js/solver.js) over libwatersim.
+
+The reference's host code is JavaScript; this module stands in for it with
+the same surface: constructor options, public knobs as attributes, the
+typed-array fields, step(dtFrame) / _substep(dt), resetWater(depth),
+generateTerrain(seed, seaLevel), splatDensity(), autotuneIso(), the
+interaction helpers and kineticEnergy(). Everything computes on the GPU
+through the C ABI of include/watersim.h; there is no CPU fallback — the
+constructor raises if the CUDA library cannot be loaded or no device exists.
+
+Differences from the reference object, all documented at the attribute:
+  * typed-array fields are snapshots (numpy copies downloaded on access);
+    assigning a numpy array to a field uploads it;
+  * only the sphere-planet world is implemented (mode 'sphere');
+  * pressure uses red-black SOR, viscosity and extrapolation Jacobi order.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libwatersim.so")
+_lib = None
+
+
+class WsError(RuntimeError):
+    """A ws_status < 0 from the library, with ws_last_error()'s message."""
+
+    def __init__(self, code, msg):
+        super().__init__("watersim error %d: %s" % (code, msg))
+        self.code = code
+
+
+class WsConfig(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("capacity", C.c_int32),
+                ("dx", C.c_double), ("coreR", C.c_double), ("bumpiness", C.c_double),
+                ("targetParticles", C.c_double), ("terrainSeed", C.c_uint32), ("device", C.c_int32)]
+
+
+class WsParams(C.Structure):
+    _fields_ = [
+        ("substeps", C.c_int32), ("pressureIters", C.c_int32),
+        ("cfl", C.c_double), ("pic", C.c_double), ("gravity", C.c_double),
+        ("viscosity", C.c_double), ("omega", C.c_double), ("maxSpeed", C.c_double),
+        ("vorticity", C.c_double), ("currents", C.c_double), ("shadeCool", C.c_double),
+        ("sunActivity", C.c_double), ("evapIntensity", C.c_double), ("atmosphereH", C.c_double),
+        ("ceilReflect", C.c_int32), ("hasSun", C.c_int32), ("sunPos", C.c_double * 3),
+        ("heatK", C.c_double), ("Tamb", C.c_double), ("cloudT", C.c_double),
+        ("cloudP", C.c_double), ("rainT", C.c_double), ("rainLiftAge", C.c_double),
+        ("snowT", C.c_double), ("meltT", C.c_double),
+        ("spinOn", C.c_int32), ("thermalOn", C.c_int32),
+        ("sorRedBlack", C.c_int32), ("sorCheckEvery", C.c_int32),
+        ("sorTol", C.c_double), ("sorMaxIters", C.c_int32),
+        ("viscJacobi", C.c_int32), ("extrapJacobi", C.c_int32),
+    ]
+
+
+class WsScalars(C.Structure):
+    _fields_ = [
+        ("coreR", C.c_double), ("oceanR", C.c_double), ("spacing", C.c_double),
+        ("particleVolume", C.c_double), ("iso", C.c_double), ("waterTopY", C.c_double),
+        ("umax", C.c_double), ("dtLast", C.c_double), ("simTime", C.c_double),
+        ("gRamp", C.c_double), ("heatAcc", C.c_double),
+        ("targetParticles", C.c_double), ("landFrac", C.c_double), ("bumpiness", C.c_double),
+        ("sorRelRes", C.c_double),
+        ("evS", C.c_uint32), ("cfS", C.c_uint32), ("bfS", C.c_uint32), ("stirS", C.c_uint32),
+        ("terrainSeed", C.c_uint32),
+        ("nP", C.c_int32), ("capacity", C.c_int32),
+        ("airborneCount", C.c_int32), ("vaporCount", C.c_int32), ("nightVaporCount", C.c_int32),
+        ("evapCount", C.c_int32), ("substepsLast", C.c_int32), ("nFluid", C.c_int32),
+        ("sorIters", C.c_int32), ("pad_", C.c_int32),
+    ]
+
+
+class WsTerrain(C.Structure):
+    _fields_ = [("n", C.c_int32), ("dv", C.c_double), ("Rsl", C.c_double), ("Rlo", C.c_double),
+                ("Rhi", C.c_double), ("landFrac", C.c_double),
+                ("solid", C.c_void_p), ("R", C.c_void_p)]
+
+
+# field ids of include/watersim.h (ws_field), with element dtype
+FIELDS = {
+    "px": (0, np.float32), "py": (1, np.float32), "pz": (2, np.float32),
+    "pvx": (3, np.float32), "pvy": (4, np.float32), "pvz": (5, np.float32),
+    "pT": (6, np.float32), "pAir": (7, np.float32), "pLight": (8, np.float32),
+    "pWx": (9, np.float32), "pWy": (10, np.float32), "pWz": (11, np.float32), "pPh": (12, np.float32),
+    "pflag": (13, np.uint8), "pcool": (14, np.uint8), "pDepth": (15, np.uint8),
+    "cellType": (16, np.uint8), "q": (17, np.float32), "rhs": (18, np.float32),
+    "u": (19, np.float32), "v": (20, np.float32), "w": (21, np.float32),
+    "uO": (22, np.float32), "vO": (23, np.float32), "wO": (24, np.float32),
+    "uW": (25, np.float32), "vW": (26, np.float32), "wW": (27, np.float32),
+    "validU": (28, np.uint8), "validV": (29, np.uint8), "validW": (30, np.uint8),
+    "dens": (31, np.float32),
+}
+PARTICLE_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pT", "pAir", "pLight", "pWx", "pWy",
+                   "pWz", "pPh", "pflag", "pcool", "pDepth")
+STAGES = ["CLEAR_RASTER", "MARK_FLUID", "P2G", "FORCES", "PRESSURE", "PROJECT", "VORTICITY", "CLAMP",
+          "EXTRAPOLATE", "G2P_ADVECT", "HEAT", "EVAPORATION", "PHASE", "PUSH_SURFACE", "SPLAT",
+          "VAPOR_COLLISIONS", "ICE_CONTACTS"]
+CEIL = {"linear": 0, "quadratic": 1, "exponential": 2}
+
+# exported entry points of include/watersim.h
+SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_params", "ws_get_params",
+           "ws_default_params", "ws_set_scalars", "ws_get_scalars", "ws_generate_terrain",
+           "ws_upload_terrain", "ws_download_terrain", "ws_water_volume", "ws_reset_water",
+           "ws_upload_field", "ws_download_field", "ws_field_info", "ws_set_nparticles", "ws_step",
+           "ws_substep", "ws_stage", "ws_residual", "ws_mt_volume", "ws_autotune_iso", "ws_census",
+           "ws_kinetic_energy", "ws_apply_impulse_sphere", "ws_stir_at", "ws_stir_gaussian",
+           "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel"]
+
+
+def load_library(path=None):
+    """Load libwatersim.so and declare its signatures (raises if missing)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or _LIB_PATH
+    if not os.path.exists(p):
+        raise OSError("libwatersim.so not built (%s); run watersim-v1_b200/build.py" % p)
+    L = C.CDLL(p)
+    h, vp, d, i32, u32, i64 = C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_uint32, C.c_int64
+    sig = {
+        "ws_create": [C.POINTER(WsConfig), C.POINTER(C.c_void_p)],
+        "ws_destroy": [h], "ws_set_params": [h, C.POINTER(WsParams)],
+        "ws_get_params": [h, C.POINTER(WsParams)], "ws_default_params": [C.POINTER(WsParams)],
+        "ws_set_scalars": [h, C.POINTER(WsScalars)], "ws_get_scalars": [h, C.POINTER(WsScalars)],
+        "ws_generate_terrain": [h, u32, d], "ws_upload_terrain": [h, C.POINTER(WsTerrain)],
+        "ws_download_terrain": [h, vp, vp, C.POINTER(C.c_double)],
+        "ws_water_volume": [h, d, C.POINTER(C.c_double)], "ws_reset_water": [h, d],
+        "ws_upload_field": [h, i32, vp, i64], "ws_download_field": [h, i32, vp, i64],
+        "ws_field_info": [h, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int32)],
+        "ws_set_nparticles": [h, i32], "ws_step": [h, d], "ws_substep": [h, d],
+        "ws_stage": [h, i32, d], "ws_residual": [h, C.POINTER(C.c_double)],
+        "ws_mt_volume": [h, d, C.POINTER(C.c_double), C.POINTER(C.c_int64)],
+        "ws_autotune_iso": [h, C.POINTER(C.c_double)], "ws_census": [h, C.POINTER(C.c_double)],
+        "ws_kinetic_energy": [h, C.POINTER(C.c_double)],
+        "ws_apply_impulse_sphere": [h, d, d, d, d, d, d, d],
+        "ws_stir_at": [h, d, d, d, d, d, d, d, d], "ws_stir_gaussian": [h, d, d],
+        "ws_synchronize": [h], "ws_get_stream": [h, C.POINTER(C.c_void_p)],
+        "ws_launch_count": [h, C.POINTER(C.c_int64)],
+        "ws_time_kernel": [h, i32, i32, C.POINTER(C.c_double)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int32
+    L.ws_last_error.argtypes = [h]
+    L.ws_last_error.restype = C.c_char_p
+    L.ws_version.argtypes = []
+    L.ws_version.restype = C.c_char_p
+    if path is None:
+        _lib = L
+    return L
+
+
+class FluidSolver:
+    """The FluidSolver of js/solver.js:45-216 on a B200, sphere mode only.
+
+    opts: nx, ny, nz, dx, coreR, terrainSeed, bumpiness, targetParticles,
+    capacity (particle capacity; default targetParticles + 8192), device.
+    """
+
+    _KNOBS = {f[0] for f in WsParams._fields_} - {"sunPos", "hasSun", "ceilReflect"}
+
+    def __init__(self, **opts):
+        object.__setattr__(self, "_h", None)
+        L = load_library()
+        object.__setattr__(self, "_L", L)
+        tp = float(opts.get("targetParticles", 110000))
+        cfg = WsConfig(nx=int(opts["nx"]), ny=int(opts["ny"]), nz=int(opts["nz"]),
+                       capacity=int(opts.get("capacity", tp + 8192)), dx=float(opts["dx"]),
+                       coreR=float(opts.get("coreR", 0.0)), bumpiness=float(opts.get("bumpiness", 1.0)),
+                       targetParticles=tp, terrainSeed=int(opts.get("terrainSeed", 20260114)),
+                       device=int(opts.get("device", 0)))
+        hh = C.c_void_p()
+        rc = L.ws_create(C.byref(cfg), C.byref(hh))
+        if rc:
+            raise WsError(rc, "ws_create failed (no CUDA device or bad options)")
+        object.__setattr__(self, "_h", hh)
+        object.__setattr__(self, "nx", cfg.nx)
+        object.__setattr__(self, "ny", cfg.ny)
+        object.__setattr__(self, "nz", cfg.nz)
+        object.__setattr__(self, "dx", cfg.dx)
+        object.__setattr__(self, "mode", "sphere")
+        p = WsParams()
+        self._check(L.ws_get_params(hh, C.byref(p)))
+        object.__setattr__(self, "_p", p)
+        if "vorticity" in opts:
+            self.vorticity = opts["vorticity"]
+
+    # ---- lifetime
+    def close(self):
+        if self._h:
+            self._L.ws_destroy(self._h)
+            object.__setattr__(self, "_h", None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise WsError(rc, self._L.ws_last_error(self._h).decode(errors="replace"))
+
+    # ---- knobs: attribute writes go straight to ws_set_params
+    def __setattr__(self, k, v):
+        if k in FluidSolver._KNOBS:
+            setattr(self._p, k, v)
+            self._check(self._L.ws_set_params(self._h, C.byref(self._p)))
+        elif k == "sunPos":
+            if v is None:
+                self._p.hasSun = 0
+            else:
+                self._p.hasSun = 1
+                for i in range(3):
+                    self._p.sunPos[i] = float(v[i])
+            self._check(self._L.ws_set_params(self._h, C.byref(self._p)))
+        elif k == "ceilReflect":
+            self._p.ceilReflect = CEIL[v] if isinstance(v, str) else int(v)
+            self._check(self._L.ws_set_params(self._h, C.byref(self._p)))
+        elif k in FIELDS:
+            self.upload(k, v)
+        elif k in {f[0] for f in WsScalars._fields_}:
+            self.set_scalars(**{k: v})
+        else:
+            object.__setattr__(self, k, v)
+
+    def __getattr__(self, k):
+        if k.startswith("_"):
+            raise AttributeError(k)
+        if k in FluidSolver._KNOBS:
+            return getattr(self._p, k)
+        if k == "sunPos":
+            return list(self._p.sunPos) if self._p.hasSun else None
+        if k in FIELDS:
+            return self.download(k)
+        if k in {f[0] for f in WsScalars._fields_}:
+            return getattr(self.scalars, k)
+        raise AttributeError(k)
+
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            if k == "sunPos":
+                if v is None:
+                    self._p.hasSun = 0
+                else:
+                    self._p.hasSun = 1
+                    for i in range(3):
+                        self._p.sunPos[i] = float(v[i])
+            elif k == "ceilReflect":
+                self._p.ceilReflect = CEIL[v] if isinstance(v, str) else int(v)
+            else:
+                setattr(self._p, k, v)
+        self._check(self._L.ws_set_params(self._h, C.byref(self._p)))
+
+    @property
+    def scalars(self):
+        s = WsScalars()
+        self._check(self._L.ws_get_scalars(self._h, C.byref(s)))
+        return s
+
+    def set_scalars(self, **kw):
+        s = self.scalars
+        for k, v in kw.items():
+            setattr(s, k, v)
+        self._check(self._L.ws_set_scalars(self._h, C.byref(s)))
+
+    # ---- fields
+    def field_size(self, name):
+        cnt, elem = C.c_int64(), C.c_int32()
+        self._check(self._L.ws_field_info(self._h, FIELDS[name][0], C.byref(cnt), C.byref(elem)))
+        return cnt.value
+
+    def download(self, name, count=None):
+        fid, dt = FIELDS[name]
+        if count is None:
+            count = self.scalars.nP if name in PARTICLE_FIELDS else self.field_size(name)
+        out = np.empty(count, dt)
+        self._check(self._L.ws_download_field(self._h, fid, out.ctypes.data, count))
+        return out
+
+    def upload(self, name, arr):
+        fid, dt = FIELDS[name]
+        a = np.ascontiguousarray(arr, dt)
+        self._check(self._L.ws_upload_field(self._h, fid, a.ctypes.data, a.size))
+
+    def set_nparticles(self, n):
+        self._check(self._L.ws_set_nparticles(self._h, int(n)))
+
+    # ---- world setup
+    def generateTerrain(self, seed, seaLevel):
+        self._check(self._L.ws_generate_terrain(self._h, int(seed), float(seaLevel)))
+
+    def upload_terrain(self, t):
+        solid = np.ascontiguousarray(t["solid"], np.uint8)
+        R = np.ascontiguousarray(t["R"], np.float32)
+        wt = WsTerrain(n=int(t["n"]), dv=float(t["dv"]), Rsl=float(t["Rsl"]), Rlo=float(t["Rlo"]),
+                       Rhi=float(t["Rhi"]), landFrac=float(t["landFrac"]),
+                       solid=solid.ctypes.data, R=R.ctypes.data)
+        self._check(self._L.ws_upload_terrain(self._h, C.byref(wt)))
+
+    def terrain(self):
+        meta = (C.c_double * 4)()
+        self._check(self._L.ws_download_terrain(self._h, None, None, meta))
+        n = int(meta[0])
+        solid = np.empty(n ** 3, np.uint8)
+        R = np.empty(n ** 3, np.float32)
+        self._check(self._L.ws_download_terrain(self._h, solid.ctypes.data, R.ctypes.data, meta))
+        return {"n": n, "solid": solid, "R": R, "Rlo": meta[1], "Rhi": meta[2], "landFrac": meta[3]}
+
+    def water_volume(self, depth):
+        v = C.c_double()
+        self._check(self._L.ws_water_volume(self._h, float(depth), C.byref(v)))
+        return v.value
+
+    def resetWater(self, depth):
+        self._check(self._L.ws_reset_water(self._h, float(depth)))
+
+    # ---- drivers
+    def step(self, dtFrame):
+        self._check(self._L.ws_step(self._h, float(dtFrame)))
+
+    def _substep(self, dt):
+        self._check(self._L.ws_substep(self._h, float(dt)))
+
+    substep = _substep
+
+    def stage(self, name, dt=0.0):
+        self._check(self._L.ws_stage(self._h, STAGES.index(name), float(dt)))
+
+    # ---- reductions and helpers
+    def residual(self):
+        r = C.c_double()
+        self._check(self._L.ws_residual(self._h, C.byref(r)))
+        return r.value
+
+    def splatDensity(self):
+        self.stage("SPLAT")
+
+    def mt_volume(self, iso):
+        v, n = C.c_double(), C.c_int64()
+        self._check(self._L.ws_mt_volume(self._h, float(iso), C.byref(v), C.byref(n)))
+        return v.value, n.value
+
+    def autotuneIso(self):
+        v = C.c_double()
+        self._check(self._L.ws_autotune_iso(self._h, C.byref(v)))
+        return v.value
+
+    def census(self):
+        out = (C.c_double * 3)()
+        self._check(self._L.ws_census(self._h, out))
+        return tuple(out)
+
+    def kineticEnergy(self):
+        v = C.c_double()
+        self._check(self._L.ws_kinetic_energy(self._h, C.byref(v)))
+        return v.value
+
+    def applyImpulseSphere(self, cx, cy, cz, R, fx, fy, fz):
+        self._check(self._L.ws_apply_impulse_sphere(self._h, cx, cy, cz, R, fx, fy, fz))
+
+    def stirAt(self, cx, cy, cz, vx, vy, vz, R, dt):
+        self._check(self._L.ws_stir_at(self._h, cx, cy, cz, vx, vy, vz, R, dt))
+
+    def stir_gaussian(self, sigma, peak):
+        self._check(self._L.ws_stir_gaussian(self._h, float(sigma), float(peak)))
+
+    def synchronize(self):
+        self._check(self._L.ws_synchronize(self._h))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._check(self._L.ws_get_stream(self._h, C.byref(s)))
+        return s.value
+
+    def launch_count(self):
+        n = C.c_int64()
+        self._check(self._L.ws_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def time_kernel(self, kernel, reps=20):
+        """Mean microseconds per launch of one kernel group (ws_time_kernel)."""
+        us = C.c_double()
+        self._check(self._L.ws_time_kernel(self._h, int(kernel), int(reps), C.byref(us)))
+        return us.value
