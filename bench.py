@@ -2,7 +2,8 @@
 
 Workload (the 128^3 planet of the headline metric): 128^3 MAC grid, unit
 cells, sea-level radius 52 and ocean depth 8 (core radius 44), seeded
-value-noise terrain (seed 20260114), 8 particles per fluid cell (~2M), FLIP
+value-noise terrain (seed 20260114), targetParticles 2,000,000 (the
+reference's fill knob; ~24 per water cell with this terrain), FLIP
 with pic 0.05, red-black SOR (omega 1.7) to a 1e-5 relative residual checked
 every 10 iterations, speed clamp 3.2 m/s, full planet gravity, thermal cycle
 off, and the seeded Gaussian stir kick (sigma 4 cells, 2 m/s peak) every 50
@@ -34,7 +35,7 @@ for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-WORKLOAD = dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, per_cell=8.0)
+WORKLOAD = dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000)
 PARAMS = dict(pic=0.05, omega=1.7, maxSpeed=3.2, cfl=3.0, viscosity=5e-4, thermalOn=0,
               sorTol=1e-5, sorCheckEvery=10, sorMaxIters=5000, pressureIters=40)
 DT = 0.01
@@ -97,14 +98,9 @@ def make_solver(device, rank=0):
     from fluid_solver import FluidSolver
     W = WORKLOAD
     coreR = W["R"] - W["depth"]
-    depthW = W["depth"]
-    Rlo = max(coreR * 0.55, W["R"] - 1.8889 * depthW)
-    cap = int(4 / 3 * math.pi * (W["R"] ** 3 - Rlo ** 3) * W["per_cell"]) + 8192
     fs = FluidSolver(nx=W["n"], ny=W["n"], nz=W["n"], dx=1.0, coreR=coreR, terrainSeed=W["seed"],
-                     capacity=cap, device=device)
+                     targetParticles=float(W["particles"]), capacity=W["particles"] + 8192, device=device)
     fs.generateTerrain(W["seed"], W["R"])
-    vw = fs.water_volume(W["depth"])
-    fs.set_scalars(targetParticles=float(round(vw * W["per_cell"])))
     fs.resetWater(W["depth"])
     fs.set_params(**PARAMS)
     fs.set_scalars(gRamp=1.5)
@@ -138,6 +134,7 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     clk = Clocks(local_rank)
     clk.start()
+    time.sleep(0.5)                      # first samples land before the timed region
     l0 = fs.launch_count()
     iters0 = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -189,6 +186,7 @@ def run_ours(args, rank, world, local_rank):
                           "particles": nP, "parallelism": "replicas x%d" % world,
                           "sor": "red-black to 1e-5 (check every 10), mean iterations %.1f"
                                  % (sum(iters0) / max(1, len(iters0))),
+                          "fluid_cells": fs.scalars.nFluid,
                           "particle_substeps_per_s": value * nP,
                           "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP)},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
@@ -206,34 +204,45 @@ def state_mb(fs, nP):
 
 
 def roofline(fs, ms_step, iters):
-    """Dominant kernel by time share per substep; achieved = algorithmic
-    bytes per launch / measured launch time (CUDA events, library stream)."""
+    """Dominant kernel by measured time share per substep; achieved =
+    algorithmic bytes per launch / live launch time (CUDA events on the
+    library's stream, ws_time_kernel)."""
     peak, kind = _peaks()
     n = fs.nx
     N = n ** 3
     F = 3 * (n + 1) * n * n
-    nP = fs.scalars.nP
-    it = sum(iters) / max(1, len(iters))
-    us_sor = fs.time_kernel(0, 40)          # per colour launch
+    s = fs.scalars
+    nP, nF = s.nP, s.nFluid
+    it = max(1, int(round(sum(iters) / max(1, len(iters)))))
+    keep = fs.pressureIters
+    fs.pressureIters = it
+    us_sor = fs.time_kernel(6, 5)                 # whole solve of `it` iterations
+    fs.pressureIters = keep
     us_p2g = fs.time_kernel(1, 5)
     us_g2p = fs.time_kernel(2, 5)
-    share_sor = 2 * it * us_sor / (ms_step * 1000)
-    share_p2g = us_p2g / (ms_step * 1000)
-    share_g2p = us_g2p / (ms_step * 1000)
-    # algorithmic bytes: SOR 13 B per cell per iteration (q read + rhs + stencil + q write),
-    # half per colour launch; P2G 25 B/particle in + 8 B per face accumulator (read+write);
-    # G2P+advect 52 B/particle + 8 B/face (u, uO)
-    cand = {"k_sor_color": (share_sor, 6.5 * N, us_sor),
-            "k_p2g": (share_p2g, 25 * nP + 16 * F, us_p2g),
-            "k_g2p_advect": (share_g2p, 52 * nP + 8 * F, us_g2p)}
+    us_f1 = fs.time_kernel(3, 5)
+    us_f2 = fs.time_kernel(4, 5)
+    us_pr = fs.time_kernel(5, 5)
+    step_us = ms_step * 1000
+    # algorithmic bytes per launch (each input read once, each output written once):
+    #  SOR solve     13 B per fluid cell per iteration (q read, rhs, stencil byte, q write)
+    #  P2G           25 B per particle in + 8 B per face accumulator
+    #  G2P+advect    52 B per particle + 8 B per face (u and uO)
+    #  faces pass 1  8 B acc + 9 B out per face; forces 12 B per face; project 8 B per face
+    cand = {"k_sor_persistent": (us_sor, 13.0 * nF * it),
+            "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
+            "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),
+            "k_faces_normalize_bc": (us_f1, 17.0 * F),
+            "k_faces_forces": (us_f2, 12.0 * F),
+            "k_project": (us_pr, 8.0 * F)}
     name = max(cand, key=lambda k: cand[k][0])
-    share, nbytes, us = cand[name]
+    us, nbytes = cand[name]
     achieved = nbytes / (us * 1e-6) / 1e9
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": kind, "traffic": None,
-            "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": share,
-            "others": {k: {"us_per_launch": v[2], "time_share": v[0],
-                           "GB_s": v[1] / (v[2] * 1e-6) / 1e9} for k, v in cand.items()}}
+            "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": us / step_us,
+            "others": {k: {"us_per_launch": v[0], "time_share": v[0] / step_us,
+                           "GB_s": v[1] / (v[0] * 1e-6) / 1e9} for k, v in cand.items()}}
 
 
 def cpu_baseline(fs, seconds=20.0):
@@ -277,7 +286,7 @@ def run_reference(args, rank, world):
         return None
     from oracle.oracle import make_planet
     W = WORKLOAD
-    o = make_planet(W["n"], R=W["R"], depth=W["depth"], seed=W["seed"], per_cell=W["per_cell"])
+    o = make_planet(W["n"], R=W["R"], depth=W["depth"], seed=W["seed"], particles=W["particles"])
     o.set(**PARAMS, sorRedBlack=0, viscJacobi=0, extrapJacobi=0)
     o.set_scalars(gRamp=1.5)
     nP = o.nP
@@ -311,7 +320,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)

@@ -207,7 +207,9 @@ ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak);
  * microseconds. Runs on the current state (timing only; the state advances
  * as if the kernels ran). kernel: 0 one red-black SOR iteration (two
  * launches, reported per launch), 1 P2G scatter, 2 fused G2P + advection,
- * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection. */
+ * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection,
+ * 6 one whole persistent SOR solve of pressureIters iterations (list build +
+ * cooperative kernel, reported per solve). */
 ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us_per_launch);
 ws_status ws_synchronize(ws_handle* h);
 ws_status ws_get_stream(ws_handle* h, void** cuda_stream);

@@ -300,28 +300,30 @@ def mt_volume_field(dens, nx, ny, nz, dx, iso):
     return v, cnt.value
 
 
-# Planet workloads (sea-level radius R, ocean depth, grid n): coreR = R - depth,
-# unit cells, 8 particles per fluid cell (spacing dx/2).
+# Planet workloads (grid n, sea-level radius R, ocean depth): coreR = R - depth,
+# unit cells. "particles" is the reference's targetParticles knob; None fills
+# at 8 particles per water cell (spacing dx/2).
 PLANETS = {
-    "planet32": dict(n=32, R=12.0, depth=3.0),
-    "planet64": dict(n=64, R=26.0, depth=5.0),
-    "planet128": dict(n=128, R=52.0, depth=8.0),
-    "planet256": dict(n=256, R=110.0, depth=12.0),
+    "planet32": dict(n=32, R=12.0, depth=3.0, particles=None),          # ~10k at 8 per cell
+    "planet64": dict(n=64, R=26.0, depth=5.0, particles=220000),
+    "planet128": dict(n=128, R=52.0, depth=8.0, particles=2000000),
+    "planet256": dict(n=256, R=110.0, depth=12.0, particles=16000000),
 }
 
 
-def make_planet(name_or_n, R=None, depth=None, seed=20260114, fp64=False, per_cell=8.0):
+def make_planet(name_or_n, R=None, depth=None, seed=20260114, fp64=False, per_cell=8.0, particles=None):
     """Build the seeded planet fixture: terrain, then the jittered lattice fill
-    with targetParticles chosen so the spacing is dx/2 (8 particles per cell)."""
+    with targetParticles = particles (or 8 per water cell)."""
     if isinstance(name_or_n, str):
         cfg = PLANETS[name_or_n]
-        n, R, depth = cfg["n"], cfg["R"], cfg["depth"]
+        n, R, depth, particles = cfg["n"], cfg["R"], cfg["depth"], cfg["particles"]
     else:
         n = name_or_n
     coreR = R - depth
     o = Oracle(n, n, n, 1.0, coreR=coreR, terrainSeed=seed, fp64=fp64)
     o.generate_terrain(seed, R)
-    Vw = o.water_volume_mc(depth)
-    o.set_scalars(targetParticles=float(round(Vw * per_cell)))
+    if particles is None:
+        particles = float(round(o.water_volume_mc(depth) * per_cell))
+    o.set_scalars(targetParticles=float(particles))
     o.reset_water(depth)
     return o

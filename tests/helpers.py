@@ -63,8 +63,9 @@ def restore(snap, fp64=False):
     return o
 
 
-def to_device(o, capacity=None):
-    """A FluidSolver on cuda:0 holding exactly the oracle's state and knobs."""
+def to_device(o, capacity=None, with_grid=False):
+    """A FluidSolver on cuda:0 holding exactly the oracle's state and knobs
+    (with_grid: also the cell types and face velocities of the last substep)."""
     from fluid_solver import FluidSolver
     s = o.scalars
     nP = s.nP
@@ -82,6 +83,9 @@ def to_device(o, capacity=None):
     fs.upload("q", o.arr("q"))
     fs.upload("dens", o.arr("dens"))
     fs.set_scalars(**{k: getattr(s, k) for k in SCALARS}, nFluid=s.nFluid)
+    if with_grid:
+        for k in ("cellType", "u", "v", "w", "uO", "vO", "wO"):
+            fs.upload(k, o.arr(k))
     return fs
 
 

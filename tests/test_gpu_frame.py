@@ -1,0 +1,202 @@
+"""Parity of the per-frame passes (thermal tick, evaporation, phases,
+rescue, density splat, FP64 reductions, impulses) and of the vapour branch
+of advection against the oracle, on the 64^3 planet with the sun on.
+
+Exactness: flags, depths, RNG states and counts are bit-exact; temperatures
+and exposures within 1e-6 absolute (FP64 conduction sums are accumulated in a
+different order, transcendental functions differ in the last ulp); the
+marching-tets volume and the census in FP64 to 1e-9 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import planet, to_device, rel_err, DEVICE_ORDER
+
+pytestmark = pytest.mark.gpu
+
+THERMAL64 = dict(pic=0.05, omega=1.7, maxSpeed=3.2, thermalOn=1, vorticity=0.05, sunActivity=0.6,
+                 evapIntensity=0.05, sorTol=1e-5, sorCheckEvery=10, sorMaxIters=3000)
+TILT = math.radians(23.4)
+
+
+def _sun(o, dist=3.0):
+    c = o.nx / 2
+    R = o.scalars.oceanR * dist
+    return [c + R * math.cos(TILT), c + R * math.sin(TILT), c]
+
+
+def _state64():
+    o = planet("planet64", **THERMAL64)
+    o.set(sunPos=_sun(o))
+    o.set_scalars(gRamp=1.5)
+    o.substep(0.01)
+    o.substep(0.01)
+    o.stage("splat_density")
+    return o
+
+
+def test_heat_tick_parity():
+    o = _state64()
+    fs = to_device(o, with_grid=True)
+    o.stage("update_heat", 1 / 12)
+    fs.stage("HEAT", 1 / 12)
+    nP = o.nP
+    assert np.array_equal(fs.pDepth, o.pDepth[:nP])
+    assert np.max(np.abs(fs.pLight.astype(np.float64) - o.pLight[:nP])) <= 1e-6
+    assert np.max(np.abs(fs.pT.astype(np.float64) - o.pT[:nP])) <= 1e-6
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
+
+
+def test_evaporation_parity():
+    o = _state64()
+    o.set(sunActivity=2.0, evapIntensity=1.0)
+    nP = o.nP
+    rng = np.random.default_rng(7)
+    o.pT[:nP] = rng.uniform(0.2, 1.0, nP).astype(np.float32)
+    fs = to_device(o, with_grid=True)
+    o.stage("update_evaporation", 1 / 12)
+    fs.stage("EVAPORATION", 1 / 12)
+    so, sg = o.scalars, fs.scalars
+    assert sg.evapCount == so.evapCount and so.evapCount > 10
+    assert sg.evS == so.evS
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
+
+
+def test_phase_parity():
+    o = _state64()
+    nP = o.nP
+    rng = np.random.default_rng(11)
+    fl = rng.choice([0, 0, 0, 1, 2, 3, 4, 5], nP).astype(np.uint8)
+    o.pflag[:nP] = fl
+    o.pT[:nP] = rng.uniform(0.0, 0.6, nP).astype(np.float32)
+    o.pAir[:nP] = rng.uniform(0.0, 1.0, nP).astype(np.float32)
+    fs = to_device(o, with_grid=True)
+    o.stage("update_phase", 1 / 60)
+    fs.stage("PHASE", 1 / 60)
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    assert np.array_equal(fs.pAir, o.pAir[:nP])
+    for k in ("pvx", "pvy", "pvz"):
+        assert np.array_equal(fs.download(k), o.arr(k)[:nP]), k
+
+
+def test_vapor_advection_exact_streams():
+    """Vapour parcels consume the serial _cfS/_bfS streams: the device pass
+    reproduces every draw (states bit-exact after the substep)."""
+    o = _state64()
+    nP = o.nP
+    rng = np.random.default_rng(3)
+    c = o.nx / 2
+    R = o.scalars.oceanR
+    sel = rng.choice(nP, 3000, replace=False)
+    d = rng.normal(size=(3000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    r = R + rng.uniform(-0.1, 0.4, 3000)
+    o.px[sel] = c + d[:, 0] * r; o.py[sel] = c + d[:, 1] * r; o.pz[sel] = c + d[:, 2] * r
+    o.pvx[sel] = rng.normal(0, 0.5, 3000); o.pvy[sel] = rng.normal(0, 0.5, 3000); o.pvz[sel] = rng.normal(0, 0.5, 3000)
+    o.pflag[sel] = rng.choice([2, 3], 3000)
+    o.pT[sel] = rng.uniform(0.1, 0.5, 3000)
+    o.pAir[sel] = rng.uniform(0, 1, 3000)
+    fs = to_device(o)
+    o.substep(0.01)
+    fs._substep(0.01)
+    so, sg = o.scalars, fs.scalars
+    assert (sg.cfS, sg.bfS) == (so.cfS, so.bfS)
+    assert so.cfS != 0x2f6e2b1 and so.bfS != 0x7f4a7c15   # the streams were consumed
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    W = o.nx
+    for k in ("px", "py", "pz"):
+        assert np.max(np.abs(fs.download(k)[sel].astype(np.float64) - o.arr(k)[sel])) <= 1e-5 * W, k
+
+
+def test_push_surface_parity():
+    o = _state64()
+    nP = o.nP
+    rng = np.random.default_rng(5)
+    sel = rng.choice(nP, 5000, replace=False)
+    c = o.nx / 2
+    for a in ("px", "py", "pz"):
+        o.arr(a)[sel] = c + (o.arr(a)[sel] - c) * rng.uniform(0.7, 1.2, 5000)
+    fs = to_device(o, with_grid=True)
+    o.stage("push_surface")
+    fs.stage("PUSH_SURFACE")
+    W = o.nx
+    for k in ("px", "py", "pz"):
+        assert np.max(np.abs(fs.download(k).astype(np.float64) - o.arr(k)[:nP])) <= 1e-6 * W, k
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
+
+
+def test_splat_volume_census_ke():
+    o = _state64()
+    fs = to_device(o, with_grid=True)
+    o.stage("splat_density")
+    fs.stage("SPLAT")
+    assert rel_err(fs.dens, o.dens) <= 1e-6
+    for iso in (0.8, 1.6):
+        vg, ng = fs.mt_volume(iso)
+        vo, no = o.mt_volume(iso)
+        assert abs(vg - vo) <= 1e-6 * vo and abs(ng - no) <= max(3, 1e-4 * no)
+    nP = o.nP
+    fl = np.random.default_rng(2).choice([0, 1, 2, 3, 4, 5], nP).astype(np.uint8)
+    o.pflag[:nP] = fl
+    fs.upload("pflag", fl)
+    assert np.allclose(fs.census(), o.census(), rtol=0, atol=1e-15)
+    assert abs(fs.kineticEnergy() - o.kinetic_energy()) <= 1e-9 * o.kinetic_energy()
+
+
+def test_impulses_parity():
+    o = _state64()
+    fs = to_device(o)
+    c = o.nx / 2
+    R = o.scalars.oceanR
+    o.apply_impulse_sphere(c + R, c, c, 4.0, 0.5, -0.2, 0.1)
+    fs.applyImpulseSphere(c + R, c, c, 4.0, 0.5, -0.2, 0.1)
+    o.stir_at(c, c + R, c, 0.3, 0.0, -0.4, 5.0, 0.01)
+    fs.stirAt(c, c + R, c, 0.3, 0.0, -0.4, 5.0, 0.01)
+    o.stir_gaussian(4.0, 2.0)
+    fs.stir_gaussian(4.0, 2.0)
+    nP = o.nP
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-7, k
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    assert fs.scalars.stirS == o.scalars.stirS
+
+
+def test_thermal_substep_parity_with_vorticity():
+    o = planet("planet64", **THERMAL64)
+    o.set(sunPos=_sun(o))
+    o.set_scalars(gRamp=1.5)
+    fs = to_device(o)
+    o.substep(0.01)
+    fs._substep(0.01)
+    nP = o.nP
+    assert np.array_equal(fs.cellType, o.cellType)
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    assert fs.scalars.sorIters == o.scalars.sorIters
+    assert rel_err(fs.q, o.q) <= 1e-5
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-5, k
+
+
+def test_frames_with_thermal_cycle():
+    """Whole frames (thermal tick, evaporation, substeps, contacts, phases,
+    rescue): counts and energy track the oracle. Vapour contacts are resolved
+    in Jacobi order on the device, so this compares run-level observables."""
+    o = planet("planet64", **THERMAL64)
+    o.set(sunPos=_sun(o, 2.0), sunActivity=1.2, evapIntensity=0.5)
+    o.set_scalars(gRamp=1.5)
+    fs = to_device(o)
+    for _ in range(6):
+        o.step(1 / 60)
+        fs.step(1 / 60)
+    so, sg = o.scalars, fs.scalars
+    assert sg.substepsLast == so.substepsLast
+    assert abs(sg.evapCount - so.evapCount) <= max(2, 0.05 * so.evapCount)
+    assert abs(sg.vaporCount - so.vaporCount) <= max(3, 0.05 * so.vaporCount)
+    ko, kg = o.kinetic_energy(), fs.kineticEnergy()
+    assert abs(kg - ko) <= 0.02 * ko

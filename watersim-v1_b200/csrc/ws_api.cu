@@ -45,6 +45,7 @@ struct ws_handle {
   int* cellCnt = nullptr;
   double *cellSum = nullptr, *cellChange = nullptr;
   void* contactScratch = nullptr;       // allocated on first contact pass
+  void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
 };
@@ -112,6 +113,7 @@ static void free_all(ws_handle* h) {
                    h->parts.pflag, h->parts.pcool, h->parts.pDepth };
   for (void* b : bufs) if (b) cudaFree(b);
   if (h->contactScratch) cudaFree(h->contactScratch);
+  if (h->sor) sor_free(h->sor);
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -170,6 +172,7 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   AL(h->blockCounts, nb) AL(h->list, P) AL(h->listCount, 1) AL(h->cand, P)
   long long partN = std::max((long long)grid_for(N, 128) + 1, (long long)(3 * nb));
   AL(h->partials, partN)
+  if ((e = sor_init(&h->sor, N, cfg->device)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "SOR state"); free_all(h); delete h; return r; }
   h->partialsCap = (int)partN;
 #undef AL
   if ((e = cudaMallocHost(&h->stHost, sizeof(DevStatus))) != cudaSuccess ||
@@ -560,34 +563,30 @@ static ws_status stage_forces(ws_handle* h, double dt) {
   launch_faces_forces(h->d, grid_of(h), coef, viscOn, dt, gsA, h->stream);
   return check_launch(h, 1);
 }
+// _pressureSolve: setup (diag, rhs, q = 0 off the fluid) then the whole SOR
+// solve in one persistent cooperative launch (ws_sor.cu). Iteration count and
+// FP64 residual land in the status word and are read at the next sync.
 static ws_status stage_pressure(ws_handle* h) {
   GridDev g = grid_of(h);
   launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
-  double om1 = 1 - h->P.omega;
   bool tolMode = h->P.sorTol > 0;
   int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
-  int check = h->P.sorCheckEvery > 0 ? h->P.sorCheckEvery : 1;
-  int it = 0;
-  for (it = 0; it < iters; ) {
-    launch_sor_color(h->d, g, 0, om1, h->stream);
-    launch_sor_color(h->d, g, 1, om1, h->stream);
-    it++;
-    s = check_launch(h, 2); if (s) return s;
-    if (tolMode && it % check == 0) {
-      launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
-      s = check_launch(h, 2); if (s) return s;
-      s = sync_status(h); if (s) return s;
-      if (h->stHost->relres <= h->P.sorTol) break;
-    }
-  }
-  h->S.sorIters = it;
-  launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
-  s = check_launch(h, 2); if (s) return s;
-  s = sync_status(h); if (s) return s;
+  int check = tolMode ? (h->P.sorCheckEvery > 0 ? h->P.sorCheckEvery : 1) : 0;
+  int* dIters = nullptr; double* dRel = nullptr;
+  cudaError_t e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
+                                   &h->st->err, &dIters, &dRel, h->stream);
+  if (e != cudaSuccess) return fail_cuda(h, e, "SOR solve launch");
+  s = check_launch(h, 4); if (s) return s;
+  WS_TRY(cudaMemcpyAsync(&h->st->sorIters, dIters, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+  WS_TRY(cudaMemcpyAsync(&h->st->relres, dRel, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  return WS_OK;
+}
+// solve diagnostics, valid after a sync_status that followed stage_pressure
+static void pressure_diagnostics(ws_handle* h) {
+  h->S.sorIters = h->stHost->sorIters;
   h->S.sorRelRes = h->stHost->relres;
   h->S.nFluid = h->stHost->nFluid;
-  return WS_OK;
 }
 static ws_status stage_project(ws_handle* h, bool clampToo) {
   launch_project(h->d, grid_of(h), clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
@@ -632,6 +631,7 @@ static ws_status substep(ws_handle* h, double dt) {
   if ((s = stage_extrapolate(h))) return s;
   if ((s = stage_g2p_advect(h, dt))) return s;
   if ((s = sync_status(h))) return s;
+  pressure_diagnostics(h);
   h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
   h->S.airborneCount = h->stHost->airborne;
   h->S.dtLast = dt;
@@ -746,7 +746,11 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
     case WS_STAGE_MARK_FLUID: s = stage_mark(h); break;
     case WS_STAGE_P2G: s = stage_p2g(h); break;
     case WS_STAGE_FORCES: s = stage_forces(h, dt); break;
-    case WS_STAGE_PRESSURE: s = stage_pressure(h); break;
+    case WS_STAGE_PRESSURE:
+      s = stage_pressure(h); if (s) return s;
+      s = sync_status(h); if (s) return s;
+      pressure_diagnostics(h);
+      return WS_OK;
     case WS_STAGE_PROJECT: s = stage_project(h, false); break;
     case WS_STAGE_VORTICITY: s = stage_vorticity(h, dt); break;
     case WS_STAGE_CLAMP:
@@ -848,6 +852,11 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
       case 3: launch_faces_normalize_bc(h->d, g, h->stream); break;
       case 4: launch_faces_forces(h->d, g, 5e-6, 1, 0.01, 9.81, h->stream); break;
       case 5: launch_project(h->d, g, 1, h->P.maxSpeed, h->st, h->stream); break;
+      case 6: { int* di; double* dr;
+                cudaError_t e6 = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
+                                                  &h->st->err, &di, &dr, h->stream);
+                if (e6 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e6, "SOR solve"); }
+                h->launches += 3; } break;                     // list build; timed per whole solve
       default: cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(h, WS_ERR_INVALID, "unknown kernel id");
     }
   }

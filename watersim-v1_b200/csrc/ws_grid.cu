@@ -7,20 +7,25 @@
 
 // ------------------------------------------------------------ face decoding
 struct FaceIJK { int comp, i, j, k; long long local; };
-__device__ __forceinline__ FaceIJK decode_face(const Dims& d, long long f) {
+// 32-bit index arithmetic: face counts stay below 2^32 for grids up to 1000^3
+__device__ __forceinline__ FaceIJK decode_face(const Dims& d, long long f64) {
   FaceIJK r;
-  int nx = d.nx, ny = d.ny;
-  if (f < d.uN) {
+  unsigned f = (unsigned)f64, nx = d.nx, ny = d.ny, uN = (unsigned)d.uN, vN = (unsigned)d.vN;
+  if (f < uN) {
     r.comp = 0; r.local = f;
-    r.i = (int)(f % (nx + 1)); long long t = f / (nx + 1); r.j = (int)(t % ny); r.k = (int)(t / ny);
-  } else if (f < d.uN + d.vN) {
-    r.comp = 1; long long g = f - d.uN; r.local = g;
-    r.i = (int)(g % nx); long long t = g / nx; r.j = (int)(t % (ny + 1)); r.k = (int)(t / (ny + 1));
+    unsigned t = f / (nx + 1); r.i = (int)(f - t * (nx + 1)); unsigned k = t / ny; r.j = (int)(t - k * ny); r.k = (int)k;
+  } else if (f < uN + vN) {
+    unsigned g = f - uN; r.comp = 1; r.local = g;
+    unsigned t = g / nx; r.i = (int)(g - t * nx); unsigned k = t / (ny + 1); r.j = (int)(t - k * (ny + 1)); r.k = (int)k;
   } else {
-    r.comp = 2; long long g = f - d.uN - d.vN; r.local = g;
-    r.i = (int)(g % nx); long long t = g / nx; r.j = (int)(t % ny); r.k = (int)(t / ny);
+    unsigned g = f - uN - vN; r.comp = 2; r.local = g;
+    unsigned t = g / nx; r.i = (int)(g - t * nx); unsigned k = t / ny; r.j = (int)(t - k * ny); r.k = (int)k;
   }
   return r;
+}
+__device__ __forceinline__ void decode_cell(const Dims& d, long long c64, int& i, int& j, int& k) {
+  unsigned c = (unsigned)c64, nx = d.nx, ny = d.ny;
+  unsigned t = c / nx; i = (int)(c - t * nx); unsigned kk = t / ny; j = (int)(t - kk * ny); k = (int)kk;
 }
 // the two cells a face separates; boundary=true for the domain planes
 __device__ __forceinline__ bool face_cells(const Dims& d, const FaceIJK& F, long long& cL, long long& cR) {
@@ -44,7 +49,7 @@ __device__ __forceinline__ bool face_cells(const Dims& d, const FaceIJK& F, long
 __global__ void k_static_types(Dims d, TerrainDev t, double coreR, uint8_t* __restrict__ st) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= d.nCells) return;
-  int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+  int i, j, k; decode_cell(d, c, i, j, k);
   bool shell = (j == 0 || j == d.ny - 1 || k == 0 || k == d.nz - 1 || i == 0 || i == d.nx - 1);
   bool rock;
   if (t.has) {
@@ -226,7 +231,7 @@ __global__ void k_pressure_setup(Dims d, GridDev g, uint8_t* __restrict__ diag8,
   const uint8_t* type = g.type;
   if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; return; }
   int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  int i, j, k; decode_cell(d, c, i, j, k);
   long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
                        j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
   int cnt = 0;
@@ -294,7 +299,7 @@ __global__ void k_residual_partial(Dims d, const float* __restrict__ q, const fl
   double rr = 0, bb = 0;
   bool interior = false;
   if (c < d.nCells) {
-    int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+    int i, j, k; decode_cell(d, c, i, j, k);
     interior = i > 0 && i < d.nx - 1 && j > 0 && j < d.ny - 1 && k > 0 && k < d.nz - 1;
   }
   if (interior && pw[c] >= 0.f) {
@@ -348,10 +353,19 @@ void launch_residual(const Dims& d, const GridDev& g, const uint8_t* diag8, doub
 // _projectSlice (:1417-1443) and, fused when vorticity is off,
 // _clampUmSlice (:2629-2653) with the max |u| reduction (exact: max of
 // non-negative float bit patterns).
+// block-level max, then one atomic per block (every thread of the block must call)
 __device__ __forceinline__ void umax_reduce(float a, DevStatus* st) {
+  __shared__ unsigned sm[32];
   unsigned bits = __float_as_uint(fabsf(a));
   bits = warp_max_u(bits);
-  if ((threadIdx.x & 31) == 0) atomicMax(&st->umaxBits, bits);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sm[wid] = bits;
+  __syncthreads();
+  if (wid == 0) {
+    bits = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0u;
+    bits = warp_max_u(bits);
+    if (lane == 0 && bits) atomicMax(&st->umaxBits, bits);
+  }
 }
 __global__ void k_project(Dims d, GridDev g, int doClamp, float vcap, DevStatus* st) {
   long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -411,7 +425,7 @@ __global__ void k_vort_omega(Dims d, GridDev g) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= d.nCells) return;
   int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  int i, j, k; decode_cell(d, c, i, j, k);
   const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
   long long im = i > 0 ? c - 1 : c, ip = i < nx - 1 ? c + 1 : c;
   long long jm = j > 0 ? c - nx : c, jp = j < ny - 1 ? c + nx : c;
@@ -429,7 +443,7 @@ __global__ void k_vort_force(Dims d, GridDev g, double eps, double dt) {
   const uint8_t* type = g.type;
   if (type[c] != WS_FLUID) return;
   int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  int i, j, k; decode_cell(d, c, i, j, k);
   const float* omg = g.omg;
   if (omg[c] < 0.35f ||
       (i > 0 && type[c - 1] != WS_FLUID) || (i < nx - 1 && type[c + 1] != WS_FLUID) ||

@@ -56,6 +56,7 @@ struct DevStatus {
   int err;
   int vaporCount, nightVapor, evapCount, pad;
   int cfA, bfB;            // draws consumed by the vapour pass (diagnostic)
+  int sorIters, pad2;
   double relres;
   double rr, bb;
 };

@@ -64,6 +64,13 @@ void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spa
 void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s);
 void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);
 
+// ---- ws_sor.cu
+cudaError_t sor_init(void** statePtr, long long nCells, int device);
+void sor_free(void* statePtr);
+cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                             int iters, int check, double tol, int* err, int** outIters, double** outRel,
+                             cudaStream_t s);
+
 // ---- ws_contacts.cu
 void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,
                              int hasSun, const double* sunRel, void* scratch, size_t scratchBytes,

@@ -1,0 +1,361 @@
+// ws_sor.cu — the pressure solve of _pressureSolve (js/solver.js:1368-1404)
+// as one persistent cooperative kernel.
+//
+// The fluid cells (about 5% of the 128^3 box) are compacted per red-black
+// colour into lists in cell order (rhs, omega/diag and diag copied beside
+// each index). One kernel then runs every sweep of the solve: each block
+// strides over the colour lists, and a software grid barrier separates the
+// half-sweeps, so no launch and no host round trip sits between them. The
+// FP64 residual check (||b - A q|| / ||b||, every sorCheckEvery iterations)
+// is reduced in the kernel: block partials are summed in block order by
+// every block, so all blocks take the same stop decision and the value is
+// deterministic. q neighbours are read with ld.global.cg (L2) because other
+// SMs wrote them in the previous half-sweep.
+//
+// Every barrier wait is bounded: after kSpinLimit polls the block latches
+// WS_DERR_TIMEOUT in the status word and the solve ends early; the host
+// reports WS_ERR_TIMEOUT. The cooperative launch guarantees co-residency,
+// so a healthy run never reaches the limit.
+#include "ws_kernels.cuh"
+#include <cooperative_groups.h>
+
+static const long long kSpinLimit = 4000000LL;
+
+struct SorLists {
+  int* idx[2];
+  float* rhs[2];
+  float* pw[2];
+  uint8_t* dg[2];
+  int* count;          // [2] list lengths (device)
+};
+
+// ---------------------------------------------------------------- list build
+// colour of an interior fluid cell (pw >= 0 marks fluid), -1 otherwise; fluid
+// never touches the solid domain shell, and the interior test keeps every
+// stencil read inside the grid whatever state a caller uploads
+__device__ __forceinline__ int sor_colour(const Dims& d, const float* __restrict__ pw, unsigned c) {
+  if (c >= (unsigned)d.nCells || pw[c] < 0.f) return -1;
+  unsigned nx = d.nx, ny = d.ny;
+  unsigned t = c / nx, i = c - t * nx, k = t / ny, j = t - k * ny;
+  if (i < 1 || j < 1 || k < 1 || i + 2 > nx || j + 2 > ny || (int)k + 2 > d.nz) return -1;
+  return (int)((i + j + k) & 1u);
+}
+__global__ void k_sor_count(Dims d, const float* __restrict__ pw, int* __restrict__ blockCounts) {
+  __shared__ int s0, s1;
+  if (threadIdx.x == 0) { s0 = 0; s1 = 0; }
+  __syncthreads();
+  unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+  int col = sor_colour(d, pw, c);
+  if (col == 1) atomicAdd(&s1, 1); else if (col == 0) atomicAdd(&s0, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) { blockCounts[2 * blockIdx.x] = s0; blockCounts[2 * blockIdx.x + 1] = s1; }
+}
+// exclusive scan of the (colour 0, colour 1) block counts, one block
+__global__ void k_sor_scan(int* __restrict__ blockCounts, int nb, int* __restrict__ total) {
+  __shared__ int w0[32], w1[32];
+  __shared__ int carry0, carry1;
+  if (threadIdx.x == 0) { carry0 = 0; carry1 = 0; }
+  __syncthreads();
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v0 = i < nb ? blockCounts[2 * i] : 0, v1 = i < nb ? blockCounts[2 * i + 1] : 0;
+    int x0 = v0, x1 = v1;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+      if (lane >= o) { x0 += y0; x1 += y1; }
+    }
+    if (lane == 31) { w0[wid] = x0; w1[wid] = x1; }
+    __syncthreads();
+    if (wid == 0) {
+      int a = lane < nw ? w0[lane] : 0, b = lane < nw ? w1[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        int ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
+        if (lane >= o) { a += ya; b += yb; }
+      }
+      w0[lane] = a; w1[lane] = b;
+    }
+    __syncthreads();
+    int e0 = x0 - v0 + (wid > 0 ? w0[wid - 1] : 0) + carry0;
+    int e1 = x1 - v1 + (wid > 0 ? w1[wid - 1] : 0) + carry1;
+    if (i < nb) { blockCounts[2 * i] = e0; blockCounts[2 * i + 1] = e1; }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) { carry0 = e0 + v0; carry1 = e1 + v1; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { total[0] = carry0; total[1] = carry1; }
+}
+__global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float* __restrict__ rhs,
+                              const uint8_t* __restrict__ diag8, const int* __restrict__ offs, SorLists L) {
+  __shared__ int wt0[32], wt1[32];
+  unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+  int col = sor_colour(d, pw, c);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned m0 = __ballot_sync(0xffffffffu, col == 0), m1 = __ballot_sync(0xffffffffu, col == 1);
+  if (lane == 0) { wt0[wid] = __popc(m0); wt1[wid] = __popc(m1); }
+  __syncthreads();
+  if (col >= 0) {
+    unsigned m = col ? m1 : m0;
+    int rank = __popc(m & ((1u << lane) - 1u));
+    int off = offs[2 * blockIdx.x + col];
+    for (int w = 0; w < wid; w++) off += col ? wt1[w] : wt0[w];
+    int e = off + rank;
+    L.idx[col][e] = (int)c; L.rhs[col][e] = rhs[c]; L.pw[col][e] = pw[c]; L.dg[col][e] = diag8[c];
+  }
+}
+
+// ---------------------------------------------------------------- grid barrier
+struct GridBar { unsigned count; unsigned gen; };
+
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* err) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = &bar->gen;
+    unsigned g = *vgen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      long long n = 0;
+      while (*vgen == g) {
+        if (++n > kSpinLimit) { atomicOr(err, WS_DERR_TIMEOUT); ok = 0; break; }
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)err & WS_DERR_TIMEOUT) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ---------------------------------------------------------------- solve
+struct SorArgs {
+  Dims d;
+  float* q;
+  SorLists L;
+  double om1;
+  int iters;           // fixed iteration count, or the cap in tolerance mode
+  int check;           // residual cadence in tolerance mode (0: fixed mode)
+  double tol;
+  GridBar* bar;
+  double2* partials;   // gridDim.x
+  int* err;            // DevStatus::err
+  int* outIters;
+  double* outRel;
+};
+
+__device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned tid, unsigned T) {
+  const int n = a.L.count[col];
+  const int* __restrict__ idx = a.L.idx[col];
+  const float* __restrict__ rhs = a.L.rhs[col];
+  const float* __restrict__ pw = a.L.pw[col];
+  float* q = a.q;
+  const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
+  for (unsigned e = tid; e < (unsigned)n; e += T) {
+    long long c = idx[e];
+    double sum = (double)__ldcg(q + c - 1);
+    sum += (double)__ldcg(q + c + 1);
+    sum += (double)__ldcg(q + c - nx);
+    sum += (double)__ldcg(q + c + nx);
+    sum += (double)__ldcg(q + c - nxy);
+    sum += (double)__ldcg(q + c + nxy);
+    double qc = (double)__ldcg(q + c);
+    __stcg(q + c, (float)(qc * a.om1 + (double)pw[e] * ((double)rhs[e] + sum)));
+  }
+}
+
+// residual partial of this block (both colours) -> partials[blockIdx.x]
+__device__ void residual_block(const SorArgs& a, unsigned tid, unsigned T) {
+  __shared__ double srr[32], sbb[32];
+  double rr = 0, bb = 0;
+  const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
+  const float* q = a.q;
+  for (int col = 0; col < 2; col++) {
+    const int n = a.L.count[col];
+    for (unsigned e = tid; e < (unsigned)n; e += T) {
+      long long c = a.L.idx[col][e];
+      double sum = (double)__ldcg(q + c - 1);
+      sum += (double)__ldcg(q + c + 1); sum += (double)__ldcg(q + c - nx); sum += (double)__ldcg(q + c + nx);
+      sum += (double)__ldcg(q + c - nxy); sum += (double)__ldcg(q + c + nxy);
+      double b = a.L.rhs[col][e];
+      double r = b + sum - (double)a.L.dg[col][e] * (double)__ldcg(q + c);
+      rr += r * r; bb += b * b;
+    }
+  }
+  rr = warp_sum(rr); bb = warp_sum(bb);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { srr[wid] = rr; sbb[wid] = bb; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    rr = lane < nw ? srr[lane] : 0; bb = lane < nw ? sbb[lane] : 0;
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    if (lane == 0) __stcg(&a.partials[blockIdx.x], make_double2(rr, bb));
+  }
+}
+// every block sums the partials in block order: identical value everywhere
+__device__ double residual_total(const SorArgs& a) {
+  __shared__ double s_rel;
+  if (threadIdx.x < 32) {
+    double rr = 0, bb = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += 32) { double2 p = __ldcg(&a.partials[b]); rr += p.x; bb += p.y; }
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    if (threadIdx.x == 0) s_rel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
+  }
+  __syncthreads();
+  return s_rel;
+}
+
+// One list entry held in registers for the whole solve: cell index, rhs,
+// omega/diag, diag and the cell's own q (only its owner thread writes it).
+struct Entry { long long c; float rhs, pw, q; uint8_t dg; };
+
+__device__ __forceinline__ void entry_relax(Entry& e, const float* q, long long nx, long long nxy, double om1) {
+  if (e.c < 0) return;
+  double sum = (double)__ldcg(q + e.c - 1);
+  sum += (double)__ldcg(q + e.c + 1);
+  sum += (double)__ldcg(q + e.c - nx);
+  sum += (double)__ldcg(q + e.c + nx);
+  sum += (double)__ldcg(q + e.c - nxy);
+  sum += (double)__ldcg(q + e.c + nxy);
+  e.q = (float)((double)e.q * om1 + (double)e.pw * ((double)e.rhs + sum));
+  __stcg(const_cast<float*>(q) + e.c, e.q);
+}
+__device__ __forceinline__ void entry_residual(const Entry& e, const float* q, long long nx, long long nxy,
+                                               double& rr, double& bb) {
+  if (e.c < 0) return;
+  double sum = (double)__ldcg(q + e.c - 1);
+  sum += (double)__ldcg(q + e.c + 1); sum += (double)__ldcg(q + e.c - nx); sum += (double)__ldcg(q + e.c + nx);
+  sum += (double)__ldcg(q + e.c - nxy); sum += (double)__ldcg(q + e.c + nxy);
+  double b = e.rhs;
+  double r = b + sum - (double)e.dg * (double)e.q;
+  rr += r * r; bb += b * b;
+}
+__device__ __forceinline__ void block_partial(const SorArgs& a, double rr, double bb) {
+  __shared__ double srr[32], sbb[32];
+  rr = warp_sum(rr); bb = warp_sum(bb);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { srr[wid] = rr; sbb[wid] = bb; }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    rr = lane < nw ? srr[lane] : 0; bb = lane < nw ? sbb[lane] : 0;
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    if (lane == 0) __stcg(&a.partials[blockIdx.x], make_double2(rr, bb));
+  }
+}
+
+__global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
+  const unsigned T = gridDim.x * blockDim.x;
+  const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n0 = a.L.count[0], n1 = a.L.count[1];
+  // register-resident path when every thread owns at most one cell per colour
+  const bool cached = (unsigned)n0 <= T && (unsigned)n1 <= T;
+  const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
+  Entry e0, e1;
+  e0.c = -1; e1.c = -1;
+  if (cached) {
+    if (tid < (unsigned)n0) { e0.c = a.L.idx[0][tid]; e0.rhs = a.L.rhs[0][tid]; e0.pw = a.L.pw[0][tid]; e0.dg = a.L.dg[0][tid]; e0.q = __ldcg(a.q + e0.c); }
+    if (tid < (unsigned)n1) { e1.c = a.L.idx[1][tid]; e1.rhs = a.L.rhs[1][tid]; e1.pw = a.L.pw[1][tid]; e1.dg = a.L.dg[1][tid]; e1.q = __ldcg(a.q + e1.c); }
+  }
+  int it = 0;
+  bool ok = true;
+  double rel = -1;
+  for (it = 0; it < a.iters && ok; ) {
+    if (cached) entry_relax(e0, a.q, nx, nxy, a.om1); else sor_half(a, 0, tid, T);
+    if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+    if (cached) entry_relax(e1, a.q, nx, nxy, a.om1); else sor_half(a, 1, tid, T);
+    if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+    it++;
+    if (a.check > 0 && it % a.check == 0) {
+      if (cached) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
+      else residual_block(a, tid, T);
+      if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+      rel = residual_total(a);
+      if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;   // partials reusable
+      if (rel <= a.tol) break;
+    }
+  }
+  if (ok) {
+    if (cached) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
+    else residual_block(a, tid, T);
+    ok = grid_barrier(a.bar, gridDim.x, a.err);
+    if (ok) rel = residual_total(a);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; }
+}
+
+// ---------------------------------------------------------------- host side
+struct SorState {
+  SorLists L{};
+  int* blockCounts = nullptr;
+  GridBar* bar = nullptr;
+  double2* partials = nullptr;
+  int* outIters = nullptr;
+  double* outRel = nullptr;
+  int grid = 0, block = 1024;
+  long long cap = 0;
+};
+
+cudaError_t sor_init(void** statePtr, long long nCells, int device) {
+  SorState* S = new SorState();
+  *statePtr = S;
+  cudaError_t e;
+  int smCount = 0, perSM = 0;
+  cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sor_persistent, S->block, 0)) != cudaSuccess) return e;
+  if (perSM < 1) return cudaErrorLaunchOutOfResources;
+  S->grid = smCount * (perSM > 1 ? 1 : perSM);
+  long long half = nCells / 2 + 2;
+  S->cap = half;
+  for (int c = 0; c < 2; c++) {
+    if ((e = cudaMalloc(&S->L.idx[c], sizeof(int) * half)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&S->L.rhs[c], sizeof(float) * half)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&S->L.pw[c], sizeof(float) * half)) != cudaSuccess) return e;
+    if ((e = cudaMalloc(&S->L.dg[c], half)) != cudaSuccess) return e;
+  }
+  long long nb = (nCells + 255) / 256 + 1;
+  if ((e = cudaMalloc(&S->L.count, sizeof(int) * 2)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->blockCounts, sizeof(int) * 2 * nb)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->bar, sizeof(GridBar))) != cudaSuccess) return e;
+  if ((e = cudaMemset(S->bar, 0, sizeof(GridBar))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->partials, sizeof(double2) * (S->grid + 1))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->outIters, sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->outRel, sizeof(double))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+void sor_free(void* statePtr) {
+  SorState* S = (SorState*)statePtr;
+  if (!S) return;
+  for (int c = 0; c < 2; c++) { cudaFree(S->L.idx[c]); cudaFree(S->L.rhs[c]); cudaFree(S->L.pw[c]); cudaFree(S->L.dg[c]); }
+  cudaFree(S->L.count); cudaFree(S->blockCounts); cudaFree(S->bar); cudaFree(S->partials);
+  cudaFree(S->outIters); cudaFree(S->outRel);
+  delete S;
+}
+
+// Builds the colour lists from the pressure setup (pw, rhs, diag8) and runs
+// the whole solve. Results land in device memory (iterations, residual);
+// the caller reads them with its next status synchronisation.
+cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                             int iters, int check, double tol, int* err, int** outIters, double** outRel,
+                             cudaStream_t s) {
+  SorState* S = (SorState*)statePtr;
+  int nb = (int)grid_for(d.nCells, 256);
+  k_sor_count<<<nb, 256, 0, s>>>(d, g.pw, S->blockCounts);
+  k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->L.count);
+  k_sor_scatter<<<nb, 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockCounts, S->L);
+  cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
+  SorArgs a;
+  a.d = d; a.q = g.q; a.L = S->L; a.om1 = 1 - omega; a.iters = iters; a.check = check; a.tol = tol;
+  a.bar = S->bar; a.partials = S->partials; a.err = err; a.outIters = S->outIters; a.outRel = S->outRel;
+  void* args[] = { &a };
+  cudaError_t e = cudaLaunchCooperativeKernel((void*)k_sor_persistent, dim3(S->grid), dim3(S->block), args, 0, s);
+  *outIters = S->outIters; *outRel = S->outRel;
+  return e;
+}
