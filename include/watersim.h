@@ -215,6 +215,22 @@ ws_status ws_synchronize(ws_handle* h);
 ws_status ws_get_stream(ws_handle* h, void** cuda_stream);
 ws_status ws_launch_count(ws_handle* h, int64_t* launches);        /* kernels this handle launched */
 
+/* ---- allocation-free FP64 residual (no counterpart in the reference)
+ * For callers that cannot let a library allocate device memory: a host that
+ * owns every GPU buffer through its own allocator, or a frame loop where a
+ * cudaMalloc/cudaFree would synchronise the device. Needs no handle (creating
+ * one allocates): computes ||b - A q||_2 / ||b||_2 over the interior fluid
+ * cells of the caller's own device buffers q, rhs (float32, nx*ny*nz) and
+ * cellType (uint8), with A, b the pressure system of _pressureSolve, and
+ * writes the double to the caller's device pointer relres, on `stream`
+ * (a cudaStream_t, or NULL). Calls no cudaMalloc/cudaFree: its scratch is a
+ * fixed 128 KB device array in the library, so grids above 128^3 cells
+ * (2,097,152) return WS_ERR_RANGE. All calls on a device share that array;
+ * calls that overlap on the GPU race. The first call on a device looks the
+ * array up (cudaGetSymbolAddress) and should come before any stream capture. */
+ws_status ws_residual_noalloc(int32_t nx, int32_t ny, int32_t nz, const float* q, const float* rhs,
+                              const uint8_t* cellType, double* relres, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

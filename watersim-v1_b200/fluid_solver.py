@@ -107,7 +107,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_upload_field", "ws_download_field", "ws_field_info", "ws_set_nparticles", "ws_step",
            "ws_substep", "ws_stage", "ws_residual", "ws_mt_volume", "ws_autotune_iso", "ws_census",
            "ws_kinetic_energy", "ws_apply_impulse_sphere", "ws_stir_at", "ws_stir_gaussian",
-           "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel"]
+           "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel",
+           "ws_residual_noalloc"]
 
 
 def load_library(path=None):
@@ -147,6 +148,8 @@ def load_library(path=None):
         f.restype = C.c_int32
     L.ws_last_error.argtypes = [h]
     L.ws_last_error.restype = C.c_char_p
+    L.ws_residual_noalloc.argtypes = [i32, i32, i32, vp, vp, vp, vp, vp]
+    L.ws_residual_noalloc.restype = C.c_int32
     L.ws_version.argtypes = []
     L.ws_version.restype = C.c_char_p
     if path is None:
