@@ -98,7 +98,7 @@ typedef struct {
   int32_t nP, capacity;
   int32_t airborneCount, vaporCount, nightVaporCount, evapCount, substepsLast, nFluid;
   int32_t sorIters;        /* iterations run by the last solve */
-  int32_t pad_;
+  int32_t sorPath;         /* 1 grid-wide persistent solve, 2 cluster-resident solve */
 } ws_scalars;
 
 /* Named fields — the typed arrays of FluidSolver (js/solver.js:94-129). */

@@ -52,7 +52,7 @@ class OrScalars(C.Structure):
         ("nP", C.c_int32), ("capacity", C.c_int32),
         ("airborneCount", C.c_int32), ("vaporCount", C.c_int32), ("nightVaporCount", C.c_int32),
         ("evapCount", C.c_int32), ("substepsLast", C.c_int32), ("nFluid", C.c_int32),
-        ("sorIters", C.c_int32), ("pad_", C.c_int32),
+        ("sorIters", C.c_int32), ("sorPath", C.c_int32),
     ]
 
 

@@ -62,7 +62,7 @@ typedef struct {
   int32_t nP, capacity;
   int32_t airborneCount, vaporCount, nightVaporCount, evapCount, substepsLast, nFluid;
   int32_t sorIters;             /* iterations run by the last solve */
-  int32_t pad_;
+  int32_t sorPath;              /* always 0 on the CPU */
 } or_scalars;
 
 typedef struct or_solver or_solver;

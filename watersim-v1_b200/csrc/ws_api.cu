@@ -46,6 +46,13 @@ struct ws_handle {
   double *cellSum = nullptr, *cellChange = nullptr;
   void* contactScratch = nullptr;       // allocated on first contact pass
   void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
+  // substep graph: the kernel sequence of one substep captured once and
+  // replayed while its launch parameters stay the same
+  cudaGraphExec_t gexec = nullptr;
+  bool graphDisabled = false;
+  long long graphLaunches = 0;
+  struct { double dt, gsA; int vapor, nP; ws_params P; } gsig{};
+  bool substepPending = false;          // status of an asynchronous substep not yet pulled
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
 };
@@ -114,6 +121,7 @@ static void free_all(ws_handle* h) {
   for (void* b : bufs) if (b) cudaFree(b);
   if (h->contactScratch) cudaFree(h->contactScratch);
   if (h->sor) sor_free(h->sor);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -215,9 +223,11 @@ extern "C" ws_status ws_get_params(const ws_handle* h, ws_params* p) {
   return WS_OK;
 }
 
+static void pull_substep(ws_handle* h);
 static ws_status sync_status(ws_handle* h) {
   WS_TRY(cudaMemcpyAsync(h->stHost, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
+  if (h->substepPending) { pull_substep(h); h->substepPending = false; }
   if (h->stHost->err) {
     int ebits = h->stHost->err;
     cudaMemsetAsync(&h->st->err, 0, sizeof(int), h->stream);
@@ -238,6 +248,7 @@ static ws_status ensure_gravity(ws_handle* h) {
 
 extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
   if (!h || !s) return WS_ERR_INVALID;
+  ws_status st0 = sync_status(h); if (st0) return st0;
   uint32_t rng[4];
   WS_TRY(cudaMemcpyAsync(rng, h->rng, sizeof(rng), cudaMemcpyDeviceToHost, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
@@ -551,15 +562,17 @@ static ws_status stage_p2g(ws_handle* h) {
   launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
   return check_launch(h, 2);
 }
-static ws_status stage_forces(ws_handle* h, double dt) {
-  ws_status s = ensure_gravity(h); if (s) return s;
+// planet gravity ramp, js/solver.js:2656-2662: the applied scale of this
+// substep (0 = no gravity), advancing the ramp timer
+static double gravity_scale(ws_handle* h, double dt) {
+  double gs = h->S.gRamp / 1.5; if (gs > 1) gs = 1;
+  h->S.gRamp += dt;
+  return gs > 0 ? gs * h->P.gravity : 0;
+}
+static ws_status stage_forces(ws_handle* h, double dt, double gsA) {
   double nu = h->P.viscosity;
   double coef = std::min(nu * dt / (h->d.dx * h->d.dx), 0.24);
   int viscOn = nu > 1e-6;
-  // planet gravity ramp, js/solver.js:2656-2662
-  double gs = h->S.gRamp / 1.5; if (gs > 1) gs = 1;
-  h->S.gRamp += dt;
-  double gsA = gs > 0 ? gs * h->P.gravity : 0;
   launch_faces_forces(h->d, grid_of(h), coef, viscOn, dt, gsA, h->stream);
   return check_launch(h, 1);
 }
@@ -573,13 +586,14 @@ static ws_status stage_pressure(ws_handle* h) {
   bool tolMode = h->P.sorTol > 0;
   int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
   int check = tolMode ? (h->P.sorCheckEvery > 0 ? h->P.sorCheckEvery : 1) : 0;
-  int* dIters = nullptr; double* dRel = nullptr;
+  int* dIters = nullptr; double* dRel = nullptr; int* dPath = nullptr;
   cudaError_t e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
-                                   &h->st->err, &dIters, &dRel, h->stream);
+                                   &h->st->err, &dIters, &dRel, &dPath, h->stream);
   if (e != cudaSuccess) return fail_cuda(h, e, "SOR solve launch");
   s = check_launch(h, 4); if (s) return s;
   WS_TRY(cudaMemcpyAsync(&h->st->sorIters, dIters, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(&h->st->relres, dRel, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  WS_TRY(cudaMemcpyAsync(&h->st->pad2, dPath, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   return WS_OK;
 }
 // solve diagnostics, valid after a sync_status that followed stage_pressure
@@ -587,6 +601,13 @@ static void pressure_diagnostics(ws_handle* h) {
   h->S.sorIters = h->stHost->sorIters;
   h->S.sorRelRes = h->stHost->relres;
   h->S.nFluid = h->stHost->nFluid;
+  h->S.sorPath = h->stHost->pad2;
+}
+// counters of the last substep (umax, airborne, solve diagnostics)
+static void pull_substep(ws_handle* h) {
+  pressure_diagnostics(h);
+  h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
+  h->S.airborneCount = h->stHost->airborne;
 }
 static ws_status stage_project(ws_handle* h, bool clampToo) {
   launch_project(h->d, grid_of(h), clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
@@ -618,23 +639,62 @@ static ws_status stage_g2p_advect(ws_handle* h, double dt) {
 }
 
 // _substep, js/solver.js:2568-2624
-static ws_status substep(ws_handle* h, double dt) {
+// _substep, js/solver.js:2568-2624: the kernels of one substep, enqueued
+// without any host synchronisation (capturable into a CUDA graph)
+static ws_status enqueue_substep(ws_handle* h, double dt, double gsA) {
   ws_status s;
   if ((s = stage_clear_raster(h))) return s;
   if ((s = stage_mark(h))) return s;
   if ((s = stage_p2g(h))) return s;
-  if ((s = stage_forces(h, dt))) return s;
+  if ((s = stage_forces(h, dt, gsA))) return s;
   if ((s = stage_pressure(h))) return s;
   bool vort = h->P.vorticity > 0;
   if ((s = stage_project(h, !vort))) return s;
   if (vort) { if ((s = stage_vorticity(h, dt))) return s; if ((s = stage_clamp(h))) return s; }
   if ((s = stage_extrapolate(h))) return s;
   if ((s = stage_g2p_advect(h, dt))) return s;
-  if ((s = sync_status(h))) return s;
-  pressure_diagnostics(h);
-  h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
-  h->S.airborneCount = h->stHost->airborne;
+  return WS_OK;
+}
+// Captures the substep into a graph; on any capture failure the handle
+// falls back to direct launches for good (same kernels, same order).
+static bool capture_substep(ws_handle* h, double dt, double gsA) {
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  long long l0 = h->launches;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError(); h->graphDisabled = true; return false;
+  }
+  ws_status s = enqueue_substep(h, dt, gsA);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (s != WS_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError(); h->graphDisabled = true; h->launches = l0; return false;
+  }
+  e = cudaGraphInstantiate(&h->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { cudaGetLastError(); h->gexec = nullptr; h->graphDisabled = true; h->launches = l0; return false; }
+  h->graphLaunches = h->launches - l0;
+  h->launches = l0;
+  return true;
+}
+static ws_status substep(ws_handle* h, double dt) {
+  ws_status s = ensure_gravity(h); if (s) return s;
+  double gsA = gravity_scale(h, dt);
+  bool vapor = h->vaporPossible && h->S.nP > 0;
+  bool same = h->gexec && h->gsig.dt == dt && h->gsig.gsA == gsA && h->gsig.vapor == (int)vapor &&
+              h->gsig.nP == h->S.nP && std::memcmp(&h->gsig.P, &h->P, sizeof(ws_params)) == 0;
+  if (!same && !h->graphDisabled && capture_substep(h, dt, gsA)) {
+    h->gsig.dt = dt; h->gsig.gsA = gsA; h->gsig.vapor = (int)vapor; h->gsig.nP = h->S.nP; h->gsig.P = h->P;
+    same = true;
+  }
+  if (same) {
+    WS_TRY(cudaGraphLaunch(h->gexec, h->stream));
+    h->launches += h->graphLaunches;
+  } else {
+    if ((s = enqueue_substep(h, dt, gsA))) return s;
+  }
   h->S.dtLast = dt;
+  h->substepPending = true;           // umax, counts and solve diagnostics are pulled at the next sync
   return WS_OK;
 }
 
@@ -721,7 +781,11 @@ extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
   }
   double remaining = dtFrame; int guard = 0, nSub = 0;
   double base = dtFrame / std::max(1, h->P.substeps);
+  // the grid clamp keeps umax <= 1.1 maxSpeed, so when even that speed leaves
+  // the CFL term above min(base, 1/100) the substep dt needs no readback
+  bool cflFree = (h->P.cfl * h->d.dx) / std::max(1.1 * h->P.maxSpeed, 0.08) >= std::min(base, 1.0 / 100);
   while (remaining > 1e-6 && guard < 10) {
+    if (!cflFree && h->substepPending) { if ((s = sync_status(h))) return s; }
     double dt = std::min(std::min(base, (h->P.cfl * h->d.dx) / std::max(h->S.umax, 0.08)), 1.0 / 100);
     if (dt < 1e-5) dt = 1e-5;
     if ((s = substep(h, dt))) return s;
@@ -745,7 +809,9 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
     case WS_STAGE_CLEAR_RASTER: s = stage_clear_raster(h); break;
     case WS_STAGE_MARK_FLUID: s = stage_mark(h); break;
     case WS_STAGE_P2G: s = stage_p2g(h); break;
-    case WS_STAGE_FORCES: s = stage_forces(h, dt); break;
+    case WS_STAGE_FORCES:
+      s = ensure_gravity(h); if (s) return s;
+      s = stage_forces(h, dt, gravity_scale(h, dt)); break;
     case WS_STAGE_PRESSURE:
       s = stage_pressure(h); if (s) return s;
       s = sync_status(h); if (s) return s;
@@ -852,9 +918,9 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
       case 3: launch_faces_normalize_bc(h->d, g, h->stream); break;
       case 4: launch_faces_forces(h->d, g, 5e-6, 1, 0.01, 9.81, h->stream); break;
       case 5: launch_project(h->d, g, 1, h->P.maxSpeed, h->st, h->stream); break;
-      case 6: { int* di; double* dr;
+      case 6: { int* di; double* dr; int* dp;
                 cudaError_t e6 = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
-                                                  &h->st->err, &di, &dr, h->stream);
+                                                  &h->st->err, &di, &dr, &dp, h->stream);
                 if (e6 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e6, "SOR solve"); }
                 h->launches += 3; } break;                     // list build; timed per whole solve
       default: cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(h, WS_ERR_INVALID, "unknown kernel id");

@@ -69,7 +69,7 @@ cudaError_t sor_init(void** statePtr, long long nCells, int device);
 void sor_free(void* statePtr);
 cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
                              int iters, int check, double tol, int* err, int** outIters, double** outRel,
-                             cudaStream_t s);
+                             int** outPath, cudaStream_t s);
 
 // ---- ws_contacts.cu
 void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,

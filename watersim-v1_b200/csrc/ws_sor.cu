@@ -26,8 +26,16 @@ struct SorLists {
   float* rhs[2];
   float* pw[2];
   uint8_t* dg[2];
+  uint16_t* code[2];   // 6 neighbour codes per entry for the cluster solve
+  int* pos;            // dense: list position of each listed cell
   int* count;          // [2] list lengths (device)
 };
+
+// Cluster-resident solve: one cluster of kClusterMax CTAs holds every fluid
+// cell. A CTA owns at most kSmax cells per colour; a neighbour code packs the
+// owner's rank (4 bits) and slot (12 bits); slot kSmax is a zero (non-fluid).
+#define kClusterMax 16
+#define kSmax 4095
 
 // ---------------------------------------------------------------- list build
 // colour of an interior fluid cell (pw >= 0 marks fluid), -1 otherwise; fluid
@@ -101,6 +109,29 @@ __global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float*
     for (int w = 0; w < wid; w++) off += col ? wt1[w] : wt0[w];
     int e = off + rank;
     L.idx[col][e] = (int)c; L.rhs[col][e] = rhs[c]; L.pw[col][e] = pw[c]; L.dg[col][e] = diag8[c];
+    L.pos[c] = e;
+  }
+}
+// neighbour codes (-x, +x, -y, +y, -z, +z) for the cluster solve: the owner
+// rank and slot of each fluid neighbour (always of the other colour)
+__global__ void k_sor_codes(Dims d, const float* __restrict__ pw, SorLists L, int C) {
+  int col = blockIdx.y;
+  int n = L.count[col], nOther = L.count[1 - col];
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || n > C * kSmax || nOther > C * kSmax) return;
+  int S = (nOther + C - 1) / C, Sown = (n + C - 1) / C;
+  // a non-fluid neighbour reads the owner CTA's own zero slot (no remote traffic)
+  const uint16_t zeroCode = (uint16_t)(((e / Sown) << 12) | kSmax);
+  long long c = L.idx[col][e], nx = d.nx, nxy = (long long)d.nx * d.ny;
+  long long nb[6] = { c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy };
+  for (int q = 0; q < 6; q++) {
+    uint16_t code = zeroCode;
+    if (sor_colour(d, pw, (unsigned)nb[q]) >= 0) {
+      int e2 = L.pos[nb[q]];
+      int r = e2 / S, slot = e2 - r * S;
+      code = (uint16_t)((r << 12) | slot);
+    }
+    L.code[col][6 * (long long)e + q] = code;
   }
 }
 
@@ -147,6 +178,8 @@ struct SorArgs {
   int* err;            // DevStatus::err
   int* outIters;
   double* outRel;
+  int* outPath;
+  int clusterCap;      // lists up to this size per colour were solved by k_sor_cluster
 };
 
 __device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned tid, unsigned T) {
@@ -254,6 +287,7 @@ __global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
   const unsigned T = gridDim.x * blockDim.x;
   const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n0 = a.L.count[0], n1 = a.L.count[1];
+  if (n0 <= a.clusterCap && n1 <= a.clusterCap) return;      // the cluster solve ran
   // register-resident path when every thread owns at most one cell per colour
   const bool cached = (unsigned)n0 <= T && (unsigned)n1 <= T;
   const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
@@ -287,8 +321,152 @@ __global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
     ok = grid_barrier(a.bar, gridDim.x, a.err);
     if (ok) rel = residual_total(a);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; }
+  if (blockIdx.x == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; *a.outPath = 1; }
 }
+
+
+// ---------------------------------------------------------------- cluster solve
+// The whole solve inside one thread-block cluster: each CTA keeps its share
+// of the fluid cells (q, rhs, omega/diag, diag, neighbour codes) in shared
+// memory, reads neighbour q from the other CTAs through distributed shared
+// memory, and separates half-sweeps with the hardware cluster barrier.
+// Same per-cell arithmetic and order as the reference's sweep
+// (js/solver.js:1397-1404, red-black order), so results match
+// k_sor_persistent bit for bit.
+struct ClusterArgs {
+  Dims d;
+  float* q;
+  SorLists L;
+  double om1;
+  int iters, check;
+  double tol;
+  int* outIters;
+  double* outRel;
+  int* outPath;
+};
+extern __shared__ __align__(16) unsigned char sor_smem[];
+
+// Non-fluid neighbours are coded to slot kSmax of the owner CTA's own table,
+// which holds 0.0f: all six loads of a cell are unconditional and
+// independent, and adding +0.0 leaves the sum of the fluid neighbours
+// unchanged (the reference adds only fluid neighbours).
+__device__ __forceinline__ float cl_load(float* const* rq, uint16_t code) {
+  return rq[code >> 12][code & 4095u];
+}
+// relax (or measure) up to two cells per call with all twelve loads in flight
+__device__ __forceinline__ void cl_sums(const uint16_t* cd, float* const* rq, int e0, int e1, int m,
+                                        double& s0, double& s1) {
+  float v[2][6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    v[0][q] = e0 < m ? cl_load(rq, cd[6 * e0 + q]) : 0.f;
+    v[1][q] = e1 < m ? cl_load(rq, cd[6 * e1 + q]) : 0.f;
+  }
+  s0 = (double)v[0][0]; s1 = (double)v[1][0];
+#pragma unroll
+  for (int q = 1; q < 6; q++) { s0 += (double)v[0][q]; s1 += (double)v[1][q]; }
+}
+
+__global__ void __launch_bounds__(1024, 1) k_sor_cluster(ClusterArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int C = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int n0 = a.L.count[0], n1 = a.L.count[1];
+  if (n0 > C * kSmax || n1 > C * kSmax) return;         // uniform: the grid solve takes it
+  const int S0 = (n0 + C - 1) / C, S1 = (n1 + C - 1) / C;
+  const int QS = kSmax + 1;                              // slot kSmax holds 0.0f
+  float* qs[2]; float* rh[2]; float* pw[2]; uint16_t* cd[2]; uint8_t* dg[2];
+  qs[0] = (float*)sor_smem; qs[1] = qs[0] + QS;
+  rh[0] = qs[1] + QS; rh[1] = rh[0] + kSmax;
+  pw[0] = rh[1] + kSmax; pw[1] = pw[0] + kSmax;
+  cd[0] = (uint16_t*)(pw[1] + kSmax); cd[1] = cd[0] + 6 * kSmax;
+  dg[0] = (uint8_t*)(cd[1] + 6 * kSmax); dg[1] = dg[0] + kSmax;
+  __shared__ float* rq[2][kClusterMax];
+  __shared__ double2 mypart;
+  __shared__ double srr[32], sbb[32];
+  __shared__ double s_rel;
+  const int base[2] = { rank * S0, rank * S1 };
+  const int m[2] = { max(0, min(S0, n0 - base[0])), max(0, min(S1, n1 - base[1])) };
+  for (int col = 0; col < 2; col++) {
+    for (int e = threadIdx.x; e < m[col]; e += blockDim.x) {
+      int g = base[col] + e;
+      qs[col][e] = __ldcg(a.q + a.L.idx[col][g]);
+      rh[col][e] = a.L.rhs[col][g]; pw[col][e] = a.L.pw[col][g]; dg[col][e] = a.L.dg[col][g];
+#pragma unroll
+      for (int q = 0; q < 6; q++) cd[col][6 * e + q] = a.L.code[col][6 * (long long)g + q];
+    }
+  }
+  if (threadIdx.x == 0) { qs[0][kSmax] = 0.f; qs[1][kSmax] = 0.f; }
+  if (threadIdx.x < kClusterMax) {
+    int r = (int)threadIdx.x;
+    // own rank: plain shared-memory pointer; other ranks: the distributed-shared-memory window
+    rq[0][r] = (r < C && r != rank) ? cl.map_shared_rank(qs[0], r) : qs[0];
+    rq[1][r] = (r < C && r != rank) ? cl.map_shared_rank(qs[1], r) : qs[1];
+  }
+  cl.sync();
+  const double om1 = a.om1;
+  const int B = blockDim.x;
+  auto residual = [&]() -> double {
+    double rr = 0, bb = 0;
+    for (int col = 0; col < 2; col++)
+      for (int e = threadIdx.x; e < m[col]; e += 2 * B) {
+        int e1 = e + B;
+        double s0, s1;
+        cl_sums(cd[col], rq[1 - col], e, e1, m[col], s0, s1);
+        double b = rh[col][e];
+        double r = b + s0 - (double)dg[col][e] * (double)qs[col][e];
+        rr += r * r; bb += b * b;
+        if (e1 < m[col]) {
+          b = rh[col][e1];
+          r = b + s1 - (double)dg[col][e1] * (double)qs[col][e1];
+          rr += r * r; bb += b * b;
+        }
+      }
+    rr = warp_sum(rr); bb = warp_sum(bb);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { srr[wid] = rr; sbb[wid] = bb; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      rr = lane < (int)(blockDim.x >> 5) ? srr[lane] : 0; bb = lane < (int)(blockDim.x >> 5) ? sbb[lane] : 0;
+      rr = warp_sum(rr); bb = warp_sum(bb);
+      if (lane == 0) mypart = make_double2(rr, bb);
+    }
+    cl.sync();                                               // every CTA's partial is in place
+    if (threadIdx.x == 0) {
+      double R = 0, Bb = 0;
+      for (int r = 0; r < C; r++) { double2 p = *cl.map_shared_rank(&mypart, r); R += p.x; Bb += p.y; }
+      s_rel = Bb > 0 ? sqrt(R) / sqrt(Bb) : sqrt(R);
+    }
+    cl.sync();                                               // partials may be rewritten after this
+    return s_rel;
+  };
+  int it = 0;
+  double rel = -1;
+  for (it = 0; it < a.iters; ) {
+    for (int col = 0; col < 2; col++) {
+      for (int e = threadIdx.x; e < m[col]; e += 2 * B) {
+        int e1 = e + B;
+        double s0, s1;
+        cl_sums(cd[col], rq[1 - col], e, e1, m[col], s0, s1);
+        qs[col][e] = (float)((double)qs[col][e] * om1 + (double)pw[col][e] * ((double)rh[col][e] + s0));
+        if (e1 < m[col])
+          qs[col][e1] = (float)((double)qs[col][e1] * om1 + (double)pw[col][e1] * ((double)rh[col][e1] + s1));
+      }
+      cl.sync();
+    }
+    it++;
+    if (a.check > 0 && it % a.check == 0) {
+      rel = residual();
+      if (rel <= a.tol) break;
+    }
+  }
+  rel = residual();
+  for (int col = 0; col < 2; col++)
+    for (int e = threadIdx.x; e < m[col]; e += blockDim.x) a.q[a.L.idx[col][base[col] + e]] = qs[col][e];
+  if (rank == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; *a.outPath = 2; }
+}
+static size_t cluster_smem_bytes() { return (size_t)(kSmax + 1) * 2 * 4 + (size_t)kSmax * (2 * 4 * 2 + 2 * 6 * 2 + 2); }
 
 // ---------------------------------------------------------------- host side
 struct SorState {
@@ -298,8 +476,10 @@ struct SorState {
   double2* partials = nullptr;
   int* outIters = nullptr;
   double* outRel = nullptr;
+  int* outPath = nullptr;
   int grid = 0, block = 1024;
   long long cap = 0;
+  int clusterSize = 0;       // 0: cluster path unavailable on this device
 };
 
 cudaError_t sor_init(void** statePtr, long long nCells, int device) {
@@ -320,22 +500,44 @@ cudaError_t sor_init(void** statePtr, long long nCells, int device) {
     if ((e = cudaMalloc(&S->L.dg[c], half)) != cudaSuccess) return e;
   }
   long long nb = (nCells + 255) / 256 + 1;
+  for (int c = 0; c < 2; c++)
+    if ((e = cudaMalloc(&S->L.code[c], sizeof(uint16_t) * 6 * half)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->L.pos, sizeof(int) * nCells)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->L.count, sizeof(int) * 2)) != cudaSuccess) return e;
+  // the largest cluster this device co-schedules with the solve's shared memory
+  size_t smem = cluster_smem_bytes();
+  if (cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess) {
+    cudaFuncSetAttribute(k_sor_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int C = kClusterMax; C >= 8 && !S->clusterSize; C /= 2) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = C; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(C); cfg.blockDim = dim3(1024); cfg.dynamicSmemBytes = smem;
+      cfg.attrs = attr; cfg.numAttrs = 1;
+      int nClusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nClusters, k_sor_cluster, &cfg) == cudaSuccess && nClusters >= 1)
+        S->clusterSize = C;
+    }
+  }
+  cudaGetLastError();                                   // a refused probe is not an error
   if ((e = cudaMalloc(&S->blockCounts, sizeof(int) * 2 * nb)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->bar, sizeof(GridBar))) != cudaSuccess) return e;
   if ((e = cudaMemset(S->bar, 0, sizeof(GridBar))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->partials, sizeof(double2) * (S->grid + 1))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->outIters, sizeof(int))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->outRel, sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->outPath, sizeof(int))) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
 void sor_free(void* statePtr) {
   SorState* S = (SorState*)statePtr;
   if (!S) return;
-  for (int c = 0; c < 2; c++) { cudaFree(S->L.idx[c]); cudaFree(S->L.rhs[c]); cudaFree(S->L.pw[c]); cudaFree(S->L.dg[c]); }
+  for (int c = 0; c < 2; c++) { cudaFree(S->L.idx[c]); cudaFree(S->L.rhs[c]); cudaFree(S->L.pw[c]); cudaFree(S->L.dg[c]); cudaFree(S->L.code[c]); }
+  cudaFree(S->L.pos);
   cudaFree(S->L.count); cudaFree(S->blockCounts); cudaFree(S->bar); cudaFree(S->partials);
-  cudaFree(S->outIters); cudaFree(S->outRel);
+  cudaFree(S->outIters); cudaFree(S->outRel); cudaFree(S->outPath);
   delete S;
 }
 
@@ -344,16 +546,34 @@ void sor_free(void* statePtr) {
 // the caller reads them with its next status synchronisation.
 cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
                              int iters, int check, double tol, int* err, int** outIters, double** outRel,
-                             cudaStream_t s) {
+                             int** outPath, cudaStream_t s) {
   SorState* S = (SorState*)statePtr;
+  *outPath = S->outPath;
   int nb = (int)grid_for(d.nCells, 256);
   k_sor_count<<<nb, 256, 0, s>>>(d, g.pw, S->blockCounts);
   k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->L.count);
   k_sor_scatter<<<nb, 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockCounts, S->L);
   cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
+  int C = S->clusterSize;
+  if (C) {
+    k_sor_codes<<<dim3((unsigned)grid_for(S->cap, 256), 2), 256, 0, s>>>(d, g.pw, S->L, C);
+    ClusterArgs ca;
+    ca.d = d; ca.q = g.q; ca.L = S->L; ca.om1 = 1 - omega; ca.iters = iters; ca.check = check; ca.tol = tol;
+    ca.outIters = S->outIters; ca.outRel = S->outRel; ca.outPath = S->outPath;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(C); cfg.blockDim = dim3(1024); cfg.dynamicSmemBytes = cluster_smem_bytes();
+    cfg.stream = s; cfg.attrs = attr; cfg.numAttrs = 1;
+    cudaError_t ec = cudaLaunchKernelEx(&cfg, k_sor_cluster, ca);
+    if (ec != cudaSuccess) return ec;
+  }
   SorArgs a;
   a.d = d; a.q = g.q; a.L = S->L; a.om1 = 1 - omega; a.iters = iters; a.check = check; a.tol = tol;
   a.bar = S->bar; a.partials = S->partials; a.err = err; a.outIters = S->outIters; a.outRel = S->outRel;
+  a.outPath = S->outPath;
+  a.clusterCap = C ? C * kSmax : -1;
   void* args[] = { &a };
   cudaError_t e = cudaLaunchCooperativeKernel((void*)k_sor_persistent, dim3(S->grid), dim3(S->block), args, 0, s);
   *outIters = S->outIters; *outRel = S->outRel;
