@@ -159,17 +159,14 @@ def run_ours(args, rank, world, local_rank):
     # ---- end to end through the public API with pinned host buffers
     host = {k: torch.empty(nP, dtype=torch.uint8 if k == "pflag" else torch.float32).pin_memory().numpy()
             for k in E2E_FIELDS}
-    for k in E2E_FIELDS:
-        host[k][:] = fs.download(k)
-    e2e_steps = max(1, min(args.steps, 10))
+    fs.download_state(host, nP)
+    e2e_steps = max(1, min(args.steps, 20))
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for k in E2E_FIELDS:
-            fs.upload(k, host[k])
+        fs.upload_state(host, nP)        # this step's particle state from pinned host buffers
         one_step()
-        for k in E2E_FIELDS:
-            host[k][:] = fs.download(k, nP)
+        fs.download_state(host, nP)      # and the stepped state back into them
     barrier()
     e2e_s = time.perf_counter() - t0
     if world > 1:

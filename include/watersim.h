@@ -155,6 +155,21 @@ ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count)
 ws_status ws_field_info(const ws_handle* h, ws_field f, int64_t* count, int32_t* elem_bytes);
 ws_status ws_set_nparticles(ws_handle* h, int32_t nP);
 
+/* ---- particle state in one call: the readback/upload GpuSim does around a
+ *      frame (js/gpu/gpusim.js:568-650). field[f] is the host buffer of
+ *      particle field f (WS_F_PX..WS_F_PDEPTH, element type as listed
+ *      above) or NULL to skip it; count elements from element 0 move per
+ *      field. All copies are queued on the handle's stream and the call
+ *      returns after one synchronisation, so the buffers are only read (or
+ *      written) during the call. Pinned buffers copy at full link speed. */
+#define WS_NUM_PARTICLE_FIELDS 16
+typedef struct {
+  int64_t count;
+  void* field[WS_NUM_PARTICLE_FIELDS];
+} ws_host_arrays;
+ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a);
+ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a);
+
 /* ---- drivers: step(dtFrame) == _stepSync (js/solver.js:2663-2700) and
  *      _substep(dt) (js/solver.js:2568-2624) */
 ws_status ws_step(ws_handle* h, double dtFrame);

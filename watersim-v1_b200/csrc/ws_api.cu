@@ -275,6 +275,21 @@ extern "C" ws_status ws_set_nparticles(ws_handle* h, int32_t nP) {
 }
 
 // ------------------------------------------------------------ fields
+// true if any byte is a steam (2) or cloud (3) flag: eight bytes per test,
+// (b & 0xFE) == 2 <=> b in {2, 3}, with the classic has-zero-byte trick
+static bool any_vapor_flag(const uint8_t* fl, int64_t n) {
+  const uint64_t ones = 0x0101010101010101ull, highs = 0x8080808080808080ull;
+  const uint64_t mask = 0xFEFEFEFEFEFEFEFEull, two = 0x0202020202020202ull;
+  int64_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t x; std::memcpy(&x, fl + i, 8);
+    uint64_t y = (x & mask) ^ two;
+    if ((y - ones) & ~y & highs) return true;
+  }
+  for (; i < n; i++) if ((fl[i] & 0xFE) == 2) return true;
+  return false;
+}
+
 struct FieldRef { void* ptr; long long count; int elem; int kind; };   // kind 1: weights view, 2: valid view
 static bool field_ref(ws_handle* h, ws_field f, FieldRef& r) {
   const Dims& d = h->d; PartsDev& p = h->parts; long long P = h->capacity;
@@ -333,10 +348,8 @@ extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host,
   if (r.kind != 0) return fail(h, WS_ERR_INVALID, "derived field is read-only");
   WS_TRY(cudaMemcpyAsync(r.ptr, host, (size_t)count * r.elem, cudaMemcpyHostToDevice, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
-  if (f == WS_F_PFLAG) {
-    const uint8_t* fl = (const uint8_t*)host;
-    for (int64_t i = 0; i < count; i++) if (fl[i] == 2 || fl[i] == 3) { h->vaporPossible = true; break; }
-  }
+  if (f == WS_F_PFLAG && !h->vaporPossible && any_vapor_flag((const uint8_t*)host, count))
+    h->vaporPossible = true;
   return WS_OK;
 }
 extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count) {
@@ -356,6 +369,29 @@ extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int
   WS_TRY(cudaStreamSynchronize(h->stream));
   if (r.kind == 2) { uint8_t* v = (uint8_t*)host; for (int64_t i = 0; i < count; i++) if (v[i] == 2) v[i] = 1; }
   return WS_OK;
+}
+
+// one queued copy per particle field, one synchronisation for all of them
+static ws_status state_copy(ws_handle* h, const ws_host_arrays* a, bool up) {
+  if (!h || !a) return WS_ERR_INVALID;
+  if (a->count < 0 || a->count > h->capacity) return fail(h, WS_ERR_RANGE, "count exceeds the particle capacity");
+  for (int f = 0; f < WS_NUM_PARTICLE_FIELDS; f++) {
+    if (!a->field[f]) continue;
+    FieldRef r;
+    field_ref(h, (ws_field)f, r);
+    size_t bytes = (size_t)a->count * r.elem;
+    if (up) WS_TRY(cudaMemcpyAsync(r.ptr, a->field[f], bytes, cudaMemcpyHostToDevice, h->stream));
+    else WS_TRY(cudaMemcpyAsync(a->field[f], r.ptr, bytes, cudaMemcpyDeviceToHost, h->stream));
+  }
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (up && a->field[WS_F_PFLAG] && !h->vaporPossible &&
+      any_vapor_flag((const uint8_t*)a->field[WS_F_PFLAG], a->count))
+    h->vaporPossible = true;
+  return WS_OK;
+}
+extern "C" ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a) { return state_copy(h, a, true); }
+extern "C" ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a) {
+  return state_copy(h, a, false);
 }
 
 // ------------------------------------------------------------ terrain + fill

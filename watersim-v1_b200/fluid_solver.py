@@ -73,6 +73,11 @@ class WsScalars(C.Structure):
     ]
 
 
+class WsHostArrays(C.Structure):
+    """ws_host_arrays: count plus one host pointer per particle field (NULL skips it)."""
+    _fields_ = [("count", C.c_int64), ("field", C.c_void_p * 16)]
+
+
 class WsTerrain(C.Structure):
     _fields_ = [("n", C.c_int32), ("dv", C.c_double), ("Rsl", C.c_double), ("Rlo", C.c_double),
                 ("Rhi", C.c_double), ("landFrac", C.c_double),
@@ -108,7 +113,7 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_substep", "ws_stage", "ws_residual", "ws_mt_volume", "ws_autotune_iso", "ws_census",
            "ws_kinetic_energy", "ws_apply_impulse_sphere", "ws_stir_at", "ws_stir_gaussian",
            "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel",
-           "ws_residual_noalloc"]
+           "ws_residual_noalloc", "ws_upload_state", "ws_download_state"]
 
 
 def load_library(path=None):
@@ -141,6 +146,7 @@ def load_library(path=None):
         "ws_synchronize": [h], "ws_get_stream": [h, C.POINTER(C.c_void_p)],
         "ws_launch_count": [h, C.POINTER(C.c_int64)],
         "ws_time_kernel": [h, i32, i32, C.POINTER(C.c_double)],
+        "ws_upload_state": [h, C.POINTER(WsHostArrays)], "ws_download_state": [h, C.POINTER(WsHostArrays)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -289,6 +295,34 @@ class FluidSolver:
         fid, dt = FIELDS[name]
         a = np.ascontiguousarray(arr, dt)
         self._check(self._L.ws_upload_field(self._h, fid, a.ctypes.data, a.size))
+
+    def _host_arrays(self, arrays, count):
+        a = WsHostArrays()
+        a.count = int(count)
+        keep = []
+        for name, arr in arrays.items():
+            fid, dt = FIELDS[name]
+            if name not in PARTICLE_FIELDS:
+                raise ValueError("%s is not a particle field" % name)
+            if arr.dtype != dt or not arr.flags.c_contiguous or arr.size < count:
+                raise ValueError("%s: need a contiguous %s array of >= %d elements" % (name, np.dtype(dt), count))
+            a.field[fid] = arr.ctypes.data
+            keep.append(arr)
+        return a, keep
+
+    def upload_state(self, arrays, count=None):
+        """Copy several particle fields host -> device in one call (one synchronisation).
+        arrays maps field name -> contiguous array of that field's dtype; pinned
+        buffers copy at full link speed."""
+        count = self.scalars.nP if count is None else count
+        a, _keep = self._host_arrays(arrays, count)
+        self._check(self._L.ws_upload_state(self._h, C.byref(a)))
+
+    def download_state(self, arrays, count=None):
+        """Copy several particle fields device -> host into the given arrays (one synchronisation)."""
+        count = self.scalars.nP if count is None else count
+        a, _keep = self._host_arrays(arrays, count)
+        self._check(self._L.ws_download_state(self._h, C.byref(a)))
 
     def set_nparticles(self, n):
         self._check(self._L.ws_set_nparticles(self._h, int(n)))
