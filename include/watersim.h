@@ -246,6 +246,60 @@ ws_status ws_launch_count(ws_handle* h, int64_t* launches);        /* kernels th
 ws_status ws_residual_noalloc(int32_t nx, int32_t ny, int32_t nz, const float* q, const float* rhs,
                               const uint8_t* cellType, double* relres, void* stream);
 
+/* ---- learned warm start of the pressure solve. No counterpart in the
+ *      reference: its _pressureSolve (js/solver.js:1312-1410) starts SOR
+ *      from the previous substep's q. A 3-level 3D U-Net (16/32/64
+ *      channels, 3x3x3 convolutions, BF16 weights and activations, FP32
+ *      accumulation on the tensor cores) maps the residual of the previous
+ *      q, r0 = b - A q_prev scaled by its RMS sigma, and the cell types to
+ *      the change of q over the solve; with the warm start on, every solve
+ *      starts from q_prev + sigma * G * net(...) at fluid cells and SOR
+ *      continues to the same tolerance, so the network only changes how
+ *      many iterations the solve takes. Training pairs (input, converged
+ *      q - q_prev) come from the plain solver's own solves. */
+typedef struct {
+  int32_t pairs_stored, pairs_capacity;  /* pairs recorded so far; ring size */
+  int64_t train_steps;                   /* Adam steps taken */
+  int64_t num_weights;                   /* FP32 parameters (weights, biases, head) */
+  double gain;                           /* output scale G (0 until set) */
+  double last_loss;                      /* mean loss of the last ws_unet_train call */
+  int32_t enabled, collecting;
+} ws_unet_info;
+/* allocate the network on first use and (re)initialise its weights (He
+ * normal from seed, zero biases) and Adam state */
+ws_status ws_unet_init(ws_handle* h, uint32_t seed);
+/* capacity > 0: record one pair per solve into a ring of that many pairs
+ * (about 9 bytes per cell each); 0: stop recording (pairs are kept) */
+ws_status ws_unet_collect(ws_handle* h, int32_t capacity);
+/* on != 0: every solve starts from the network's prediction */
+ws_status ws_unet_enable(ws_handle* h, int32_t on);
+/* steps Adam steps (beta 0.9/0.999) of batch pairs drawn from the ring with
+ * a seeded generator; mean squared error over fluid cells of the target
+ * scaled by 1/G. The first call sets G to the RMS of the stored targets. */
+ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, double lr, uint32_t seed,
+                        double* mean_loss);
+ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out);
+/* the FP32 parameters, flat: per layer W[cout][cin][27] then b[cout], in
+ * the order e0a e0b e1a e1b ba bb d1a d1b d0a d0b, then head w[16], b */
+ws_status ws_unet_get_weights(ws_handle* h, float* host, int64_t count);
+ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_t count);
+ws_status ws_unet_set_gain(ws_handle* h, double gain);
+/* one stored pair: r0 / sigma (float), cell types (uint8), target
+ * (q - q_prev) / sigma (float), each nx*ny*nz; any pointer may be NULL */
+ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uint8_t* types, float* target);
+ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint8_t* types, const float* target);
+/* network output (before the gain) at every cell of pair idx, 0 outside
+ * active tiles; and the loss gradient of one pair, flat like the weights */
+ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out);
+ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, double* loss);
+/* after the forces stage: sets up the pressure system and returns the
+ * relative residual of the previous q and of the predicted q (q is left
+ * at the prediction) */
+ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* relres_pred);
+/* mean device time in ms of `what`: 0 the prediction (writes q), 1 one
+ * training step of batch 1 at learning rate 0 */
+ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,7 +2,9 @@
 
 Compiles every csrc/*.cu with nvcc into one shared library in this folder.
 -fmad=false: the reference computes in JavaScript doubles and never fuses a
-multiply-add, so neither does the device arithmetic that mirrors it.
+multiply-add, so neither does the device arithmetic that mirrors it. The
+learned warm start (ws_unet*.cu) has no reference arithmetic to mirror and
+is built with contraction on.
 """
 import os
 import subprocess
@@ -39,7 +41,10 @@ def build(verbose=False, force=False, jobs=8):
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        flags = FLAGS
+        if os.path.basename(src).startswith("ws_unet"):
+            flags = ["-fmad=true" if f == "-fmad=false" else f for f in FLAGS]
+        cmd = [NVCC, *ARCH, *flags, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

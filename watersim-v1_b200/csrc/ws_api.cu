@@ -3,6 +3,7 @@
 // world setup. One CUDA stream per handle; no global mutable state.
 #include "ws_kernels.cuh"
 #include "ws_terrain.h"
+#include "ws_unet.cuh"
 #include <cstdio>
 #include <cstring>
 #include <cmath>
@@ -51,10 +52,14 @@ struct ws_handle {
   cudaGraphExec_t gexec = nullptr;
   bool graphDisabled = false;
   long long graphLaunches = 0;
-  struct { double dt, gsA; int vapor, nP; ws_params P; } gsig{};
+  struct { double dt, gsA; int vapor, nP, unet; ws_params P; } gsig{};
   bool substepPending = false;          // status of an asynchronous substep not yet pulled
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
+  // learned warm start of the pressure solve (ws_unet.cu)
+  unet::Net* net = nullptr;
+  bool unetOn = false;                  // predict q before every solve
+  bool unetCollect = false;             // store (input, converged q) pairs from every solve
 };
 
 static float bits_to_float(unsigned u) { float f; std::memcpy(&f, &u, sizeof(f)); return f; }
@@ -122,6 +127,7 @@ static void free_all(ws_handle* h) {
   if (h->contactScratch) cudaFree(h->contactScratch);
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->net) { h->net->destroy(); delete h->net; }
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -623,13 +629,26 @@ static ws_status stage_pressure(ws_handle* h) {
   int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
   int check = tolMode ? (h->P.sorCheckEvery > 0 ? h->P.sorCheckEvery : 1) : 0;
   int* dIters = nullptr; double* dRel = nullptr; int* dPath = nullptr;
-  cudaError_t e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
+  cudaError_t e;
+  if (h->net && h->unetCollect) {
+    if ((e = h->net->collect_pre(h->q, h->rhs, h->diag8, h->type, h->stream)) != cudaSuccess)
+      return fail_cuda(h, e, "warm-start pair (before the solve)");
+  }
+  if (h->net && h->unetOn) {
+    if ((e = h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream)) != cudaSuccess)
+      return fail_cuda(h, e, "learned warm start");
+    h->launches += 24;
+  }
+  e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
                                    &h->st->err, &dIters, &dRel, &dPath, h->stream);
   if (e != cudaSuccess) return fail_cuda(h, e, "SOR solve launch");
   s = check_launch(h, 4); if (s) return s;
   WS_TRY(cudaMemcpyAsync(&h->st->sorIters, dIters, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(&h->st->relres, dRel, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(&h->st->pad2, dPath, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+  if (h->net && h->unetCollect) {
+    if ((e = h->net->collect_post(h->q, h->stream)) != cudaSuccess) return fail_cuda(h, e, "warm-start pair (after the solve)");
+  }
   return WS_OK;
 }
 // solve diagnostics, valid after a sync_status that followed stage_pressure
@@ -717,10 +736,14 @@ static ws_status substep(ws_handle* h, double dt) {
   ws_status s = ensure_gravity(h); if (s) return s;
   double gsA = gravity_scale(h, dt);
   bool vapor = h->vaporPossible && h->S.nP > 0;
-  bool same = h->gexec && h->gsig.dt == dt && h->gsig.gsA == gsA && h->gsig.vapor == (int)vapor &&
-              h->gsig.nP == h->S.nP && std::memcmp(&h->gsig.P, &h->P, sizeof(ws_params)) == 0;
-  if (!same && !h->graphDisabled && capture_substep(h, dt, gsA)) {
+  // pair collection writes a new slot each substep: those substeps run uncaptured
+  const bool collect = h->net && h->unetCollect;
+  bool same = !collect && h->gexec && h->gsig.dt == dt && h->gsig.gsA == gsA && h->gsig.vapor == (int)vapor &&
+              h->gsig.nP == h->S.nP && h->gsig.unet == (int)h->unetOn &&
+              std::memcmp(&h->gsig.P, &h->P, sizeof(ws_params)) == 0;
+  if (!same && !collect && !h->graphDisabled && capture_substep(h, dt, gsA)) {
     h->gsig.dt = dt; h->gsig.gsA = gsA; h->gsig.vapor = (int)vapor; h->gsig.nP = h->S.nP; h->gsig.P = h->P;
+    h->gsig.unet = (int)h->unetOn;
     same = true;
   }
   if (same) {
@@ -970,4 +993,163 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
   cudaEventDestroy(e0); cudaEventDestroy(e1);
   *us = 1000.0 * ms / (reps * perRep);
   return sync_status(h);
+}
+
+// ------------------------------------------------------------ learned warm start
+static ws_status net_ready(ws_handle* h) {
+  if (!h) return WS_ERR_INVALID;
+  if (!h->net) return fail(h, WS_ERR_STATE, "warm-start network not initialised: call ws_unet_init");
+  cudaSetDevice(h->device);
+  return sync_status(h);
+}
+extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  if (!h->net) {
+    h->net = new (std::nothrow) unet::Net();
+    if (!h->net) return fail(h, WS_ERR_NOMEM, "warm-start network");
+    cudaError_t e = h->net->create(h->d);
+    if (e != cudaSuccess) { h->net->destroy(); delete h->net; h->net = nullptr; return fail_cuda(h, e, "warm-start network buffers"); }
+  }
+  WS_TRY(h->net->init_weights(seed, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (capacity < 0) return fail(h, WS_ERR_RANGE, "negative pair capacity");
+  if (capacity > 0) {
+    cudaError_t e = h->net->reserve_pairs(capacity);
+    if (e != cudaSuccess) return fail_cuda(h, e, "pair store");
+  }
+  h->unetCollect = capacity > 0;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_enable(ws_handle* h, int32_t on) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (on && !(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain: train it or call ws_unet_set_gain");
+  h->unetOn = on != 0;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, double lr, uint32_t seed,
+                                   double* mean_loss) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
+  if (steps < 0 || batch < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad training arguments");
+  cudaError_t e = h->net->train(steps, batch, lr, seed, mean_loss, h->stream);
+  if (e != cudaSuccess) return fail_cuda(h, e, "warm-start training");
+  int derr = 0;
+  WS_TRY(cudaMemcpy(&derr, h->net->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) return fail(h, WS_ERR_TIMEOUT, "tensor-core convolution timed out");
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out) {
+  if (!h || !out) return WS_ERR_INVALID;
+  std::memset(out, 0, sizeof(*out));
+  if (!h->net) return WS_OK;
+  out->pairs_stored = h->net->pairsStored; out->pairs_capacity = h->net->pairCap;
+  out->train_steps = h->net->trainSteps; out->num_weights = h->net->nparams;
+  out->gain = h->net->gain; out->last_loss = h->net->lastLoss;
+  out->enabled = h->unetOn; out->collecting = h->unetCollect;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_get_weights(ws_handle* h, float* host, int64_t count) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
+  WS_TRY(cudaMemcpy(host, h->net->params, sizeof(float) * count, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_t count) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
+  WS_TRY(h->net->set_weights(host, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_set_gain(ws_handle* h, double gain) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!(gain > 0)) return fail(h, WS_ERR_INVALID, "gain must be positive");
+  WS_TRY(h->net->set_gain(gain, h->stream));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uint8_t* types, float* target) {
+  ws_status s = net_ready(h); if (s) return s;
+  unet::Net& n = *h->net;
+  if (idx < 0 || idx >= std::min(n.pairsStored, n.pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
+  long long N = h->d.nCells;
+  if (r0n) WS_TRY(cudaMemcpy(r0n, n.pr0n + N * idx, sizeof(float) * N, cudaMemcpyDeviceToHost));
+  if (types) WS_TRY(cudaMemcpy(types, n.ptype + N * idx, (size_t)N, cudaMemcpyDeviceToHost));
+  if (target) WS_TRY(cudaMemcpy(target, n.ptarget + N * idx, sizeof(float) * N, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint8_t* types, const float* target) {
+  ws_status s = net_ready(h); if (s) return s;
+  unet::Net& n = *h->net;
+  if (!r0n || !types || !target) return WS_ERR_INVALID;
+  if (n.pairCap <= 0) { cudaError_t e = n.reserve_pairs(1); if (e != cudaSuccess) return fail_cuda(h, e, "pair store"); }
+  long long N = h->d.nCells;
+  int slot = n.pairsStored % n.pairCap;
+  double t2 = 0;
+  for (long long c = 0; c < N; c++) if (types[c] == 1) t2 += (double)target[c] * target[c];
+  double sc[2] = { 1.0, t2 };
+  WS_TRY(cudaMemcpy(n.pr0n + N * slot, r0n, sizeof(float) * N, cudaMemcpyHostToDevice));
+  WS_TRY(cudaMemcpy(n.ptype + N * slot, types, (size_t)N, cudaMemcpyHostToDevice));
+  WS_TRY(cudaMemcpy(n.ptarget + N * slot, target, sizeof(float) * N, cudaMemcpyHostToDevice));
+  WS_TRY(cudaMemcpy(n.pscal + 2 * slot, sc, sizeof(sc), cudaMemcpyHostToDevice));
+  n.pairsStored++;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!out || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
+  WS_TRY(h->net->forward_pair(idx, out, h->stream));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, double* loss) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!grads || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
+  WS_TRY(h->net->grad_pair(idx, grads, loss, h->stream));
+  return WS_OK;
+}
+// relative residual of q before and after the prediction, on the pressure
+// system of the current face velocities (call after the forces stage)
+extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* relres_pred) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain");
+  GridDev g = grid_of(h);
+  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, h->stream);
+  if ((s = check_launch(h, 1))) return s;
+  launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
+  if ((s = check_launch(h, 2))) return s;
+  if ((s = sync_status(h))) return s;
+  if (relres_prev) *relres_prev = h->stHost->relres;
+  WS_TRY(h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream));
+  launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
+  if ((s = check_launch(h, 2))) return s;
+  if ((s = sync_status(h))) return s;
+  if (relres_pred) *relres_pred = h->stHost->relres;
+  return WS_OK;
+}
+// device time of `what`: 0 the prediction on the current pressure system
+// (writes q), 1 one training step on a stored pair (batch 1, learning rate 0)
+extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!ms || reps < 1 || what < 0 || what > 1) return WS_ERR_INVALID;
+  if (what == 1 && h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
+  cudaEvent_t a, b;
+  WS_TRY(cudaEventCreate(&a)); WS_TRY(cudaEventCreate(&b));
+  WS_TRY(cudaEventRecord(a, h->stream));
+  for (int r = 0; r < reps; r++) {
+    cudaError_t e = what == 0 ? h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream)
+                              : h->net->train(1, 1, 0.0, 7u + r, nullptr, h->stream);
+    if (e != cudaSuccess) { cudaEventDestroy(a); cudaEventDestroy(b); return fail_cuda(h, e, "warm-start timing"); }
+  }
+  WS_TRY(cudaEventRecord(b, h->stream));
+  WS_TRY(cudaEventSynchronize(b));
+  float t = 0;
+  cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a); cudaEventDestroy(b);
+  *ms = t / reps;
+  return WS_OK;
 }

@@ -1,0 +1,268 @@
+// ws_unet_conv.cu — 3x3x3 convolution of the warm-start U-Net as an
+// implicit GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// One CTA computes a sub-tile of 8 (x) x 16 (y) x ZT (z) output voxels of one
+// active tile. For each 16-channel slice of the input it stages, in shared
+// memory, the (8+2) x (16+2) x (ZT+2) halo of that slice (two 8-channel
+// chunks, voxel-major, 16 bytes per voxel per chunk) and the slice's weights
+// for all 27 taps. One elected thread then issues, for every output plane z
+// and tap (dz, dy, dx), one tcgen05.mma of M = 128 (the 8 x 16 voxels of the
+// plane), N = cout, K = 16 (the channel slice), BF16 inputs, FP32
+// accumulator in tensor memory. The A operand of a tap is the halo shifted by
+// (dz, dy, dx): with the no-swizzle K-major layout each 8-row core matrix is
+// the 8 x-consecutive voxels of one y-row (128 contiguous bytes), the stride
+// between core matrices along M is one halo row (160 bytes) and the stride
+// between the two K chunks is one halo chunk, so a shift only moves the
+// descriptor's start address. Inactive neighbour tiles and voxels outside
+// the grid are staged as zeros. The epilogue reads the accumulators with
+// tcgen05.ld (each warp its 32-lane quarter), adds bias and ReLU (forward)
+// or applies a ReLU mask (backward data), and stores BF16 NDHWC.
+//
+// Every mbarrier wait is bounded; on a timeout the CTA latches
+// WS_DERR_TIMEOUT, waits once more (bounded) for its MMAs, frees its tensor
+// memory and returns.
+#include "ws_unet.cuh"
+
+namespace unet {
+
+static constexpr long long kWaitLimit = 1LL << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle: start, leading (K-chunk) and
+// stride (8-row group) byte offsets in 16-byte units, descriptor version 1
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+// instruction descriptor of kind::f16: D f32, A bf16, B bf16, both K-major, M = 128
+__host__ __device__ constexpr uint32_t idesc_bf16_m128(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+               :: "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long long n = 0; n < kWaitLimit; n++)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int COUT> struct ConvShape {
+  static constexpr int ZT = COUT <= 32 ? 8 : COUT <= 64 ? 4 : 2;
+  static constexpr int HX = kTX + 2, HY = kTY + 2, HZ = ZT + 2;
+  static constexpr int HV = HX * HY * HZ;           // halo voxels
+  static constexpr int KSTR = HV * 16;              // bytes of one 8-channel halo chunk
+  static constexpr int WCH = 27 * 2 * COUT * 16;    // bytes of one 16-channel weight slice
+  static constexpr int NCOL = ZT * COUT;
+  static constexpr int TCOLS = NCOL <= 32 ? 32 : NCOL <= 64 ? 64 : NCOL <= 128 ? 128 : NCOL <= 256 ? 256 : 512;
+  // shared memory per CTA, padded so that the CTAs one SM can hold never
+  // ask for more than the 512 tensor-memory columns together (233472 bytes
+  // of shared memory per SM, 1 KB of it reserved per CTA)
+  static constexpr int MAXCTA = 512 / TCOLS;
+  static constexpr int SMEM_MIN = 233472 / (MAXCTA + 1) + 1;
+  static constexpr int SMEM = 2 * KSTR + WCH > SMEM_MIN ? 2 * KSTR + WCH : SMEM_MIN;
+};
+
+template <int COUT>
+__global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
+  using S = ConvShape<COUT>;
+  constexpr int ZT = S::ZT, HX = S::HX, HY = S::HY, HV = S::HV, KSTR = S::KSTR, WCH = S::WCH;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* halo = smem;                       // [2][HV][16 B]
+  unsigned char* wsm = smem + 2 * KSTR;             // [27][2][COUT][16 B]
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+
+  constexpr int sub = kTZ / ZT;
+  const int nT = *a.nTiles;
+  if ((int)blockIdx.x >= nT * sub) return;          // uniform over the CTA
+  const int tile = a.tiles[blockIdx.x / sub];
+  const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
+  const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ + (int)(blockIdx.x % sub) * ZT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&s_tmem)), "r"((uint32_t)S::TCOLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) { mbar_init(&mbar, 1); s_abort = 0; }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+
+  const int cin = a.c0 + a.c1;
+  const int nslices = cin >> 4;
+  constexpr uint32_t idesc = idesc_bf16_m128(COUT);
+  uint32_t phase = 0;
+  bool pending = false;
+  for (int kk = 0; kk < nslices; kk++) {
+    // ---- stage the halo of input channels [16 kk, 16 kk + 16) and their weights
+    for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
+      const int j = i & 1, hv = i >> 1;
+      const int hx = hv % HX, t2 = hv / HX, hy = t2 % HY, hz = t2 / HY;
+      const int gx = X0 - 1 + hx, gy = Y0 - 1 + hy, gz = Z0 - 1 + hz;
+      uint4 val = make_uint4(0u, 0u, 0u, 0u);
+      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
+          a.active[((gz / kTZ) * a.nty + gy / kTY) * a.ntx + gx / kTX]) {
+        const int c = kk * 16 + j * 8;
+        const bf16* p;
+        if (c < a.c0) {
+          if (a.up0) {
+            const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
+            p = a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c;
+          } else {
+            p = a.src0 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c0 + c;
+          }
+        } else {
+          p = a.src1 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c1 + (c - a.c0);
+        }
+        val = __ldg(reinterpret_cast<const uint4*>(p));
+      }
+      *reinterpret_cast<uint4*>(halo + j * KSTR + hv * 16) = val;
+    }
+    const uint4* wsrc = reinterpret_cast<const uint4*>(a.w) + (size_t)kk * (WCH / 16);
+    for (int i = threadIdx.x; i < WCH / 16; i += blockDim.x) reinterpret_cast<uint4*>(wsm)[i] = __ldg(wsrc + i);
+    fence_proxy_async();                             // generic-proxy stores -> tensor-core reads
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      fence_after();
+      const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
+      for (int z = 0; z < ZT; z++) {
+#pragma unroll 1
+        for (int t = 0; t < 27; t++) {
+          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+          const uint64_t ad = smem_desc(hbase + (uint32_t)((((z + dz) * HY + dy) * HX + dx) * 16), KSTR, HX * 16);
+          const uint64_t bd = smem_desc(wbase + (uint32_t)(t * 2 * COUT * 16), COUT * 16, 128);
+          mma_bf16(tmem + (uint32_t)(z * COUT), ad, bd, idesc, (kk | t) != 0);
+        }
+      }
+      mma_commit(&mbar);
+    }
+    pending = true;
+    // the next slice overwrites the staged operands: wait for the MMAs that read them
+    const bool ok = mbar_wait(&mbar, phase);
+    if (!ok) { s_abort = 1; atomicOr(a.err, WS_DERR_TIMEOUT); }
+    __syncthreads();
+    if (s_abort) break;
+    pending = false;
+    phase ^= 1u;
+  }
+  if (s_abort && pending) mbar_wait(&mbar, phase);    // bounded: let the issued MMAs drain
+  fence_after();
+  if (!s_abort) {
+    const int q = warp & 3;                          // tensor-memory lane quarter of this warp
+    const int m = q * 32 + lane;                     // accumulator row = voxel of the plane
+    const int gx = X0 + (m & 7), gy = Y0 + (m >> 3);
+    for (int z = warp >> 2; z < ZT; z += 2) {
+      const int gz = Z0 + z;
+      const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
+      const size_t vox = ((size_t)gz * a.ny + gy) * a.nx + gx;
+#pragma unroll 1
+      for (int cg = 0; cg < COUT / 16; cg++) {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(z * COUT + cg * 16), r);
+        if (!in) continue;
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+        const int c = cg * 16;
+        if (a.mode == 0) {
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + __ldg(a.bias + c + i), 0.f);
+        } else if (a.mask) {
+          const uint4* mp = reinterpret_cast<const uint4*>(a.mask + vox * COUT + c);
+          uint4 mk[2] = { __ldg(mp), __ldg(mp + 1) };
+          const bf16* mb = reinterpret_cast<const bf16*>(mk);
+#pragma unroll
+          for (int i = 0; i < 16; i++) if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
+        }
+        uint4 o[2];
+        __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+        for (int i = 0; i < 8; i++) ob[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        uint4* dst = c < a.split
+            ? reinterpret_cast<uint4*>(a.out0 + vox * a.split + c)
+            : reinterpret_cast<uint4*>(a.out1 + vox * (COUT - a.split) + (c - a.split));
+        dst[0] = o[0]; dst[1] = o[1];
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"((uint32_t)S::TCOLS) : "memory");
+}
+
+template <int COUT> static cudaError_t set_smem() {
+  return cudaFuncSetAttribute(k_conv3<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ConvShape<COUT>::SMEM);
+}
+cudaError_t conv3_init() {
+  cudaError_t e;
+  if ((e = set_smem<16>()) != cudaSuccess) return e;
+  if ((e = set_smem<32>()) != cudaSuccess) return e;
+  if ((e = set_smem<48>()) != cudaSuccess) return e;
+  if ((e = set_smem<64>()) != cudaSuccess) return e;
+  return set_smem<96>();
+}
+int conv3_zt(int cout) {
+  switch (cout) {
+    case 16: return ConvShape<16>::ZT; case 32: return ConvShape<32>::ZT; case 48: return ConvShape<48>::ZT;
+    case 64: return ConvShape<64>::ZT; case 96: return ConvShape<96>::ZT; default: return 0;
+  }
+}
+size_t conv3_smem_bytes(int cout) {
+  switch (cout) {
+    case 16: return ConvShape<16>::SMEM; case 32: return ConvShape<32>::SMEM; case 48: return ConvShape<48>::SMEM;
+    case 64: return ConvShape<64>::SMEM; case 96: return ConvShape<96>::SMEM; default: return 0;
+  }
+}
+cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t s) {
+  if (((a.c0 + a.c1) & 15) || (a.c0 & 7) || (a.c1 & 7) || a.c0 + a.c1 <= 0 || (a.split & 15)) return cudaErrorInvalidValue;
+  const int zt = conv3_zt(cout);
+  if (!zt) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)(maxTiles * (kTZ / zt)));
+  if (grid.x == 0) return cudaSuccess;
+  const size_t sm = conv3_smem_bytes(cout);
+  switch (cout) {
+    case 16: k_conv3<16><<<grid, 256, sm, s>>>(a); break;
+    case 32: k_conv3<32><<<grid, 256, sm, s>>>(a); break;
+    case 48: k_conv3<48><<<grid, 256, sm, s>>>(a); break;
+    case 64: k_conv3<64><<<grid, 256, sm, s>>>(a); break;
+    case 96: k_conv3<96><<<grid, 256, sm, s>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace unet

@@ -78,6 +78,12 @@ class WsHostArrays(C.Structure):
     _fields_ = [("count", C.c_int64), ("field", C.c_void_p * 16)]
 
 
+class WsUnetInfo(C.Structure):
+    _fields_ = [("pairs_stored", C.c_int32), ("pairs_capacity", C.c_int32), ("train_steps", C.c_int64),
+                ("num_weights", C.c_int64), ("gain", C.c_double), ("last_loss", C.c_double),
+                ("enabled", C.c_int32), ("collecting", C.c_int32)]
+
+
 class WsTerrain(C.Structure):
     _fields_ = [("n", C.c_int32), ("dv", C.c_double), ("Rsl", C.c_double), ("Rlo", C.c_double),
                 ("Rhi", C.c_double), ("landFrac", C.c_double),
@@ -113,7 +119,10 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_substep", "ws_stage", "ws_residual", "ws_mt_volume", "ws_autotune_iso", "ws_census",
            "ws_kinetic_energy", "ws_apply_impulse_sphere", "ws_stir_at", "ws_stir_gaussian",
            "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel",
-           "ws_residual_noalloc", "ws_upload_state", "ws_download_state"]
+           "ws_residual_noalloc", "ws_upload_state", "ws_download_state",
+           "ws_unet_init", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
+           "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
+           "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time"]
 
 
 def load_library(path=None):
@@ -147,6 +156,14 @@ def load_library(path=None):
         "ws_launch_count": [h, C.POINTER(C.c_int64)],
         "ws_time_kernel": [h, i32, i32, C.POINTER(C.c_double)],
         "ws_upload_state": [h, C.POINTER(WsHostArrays)], "ws_download_state": [h, C.POINTER(WsHostArrays)],
+        "ws_unet_init": [h, u32], "ws_unet_collect": [h, i32], "ws_unet_enable": [h, i32],
+        "ws_unet_train": [h, i32, i32, d, u32, C.POINTER(C.c_double)],
+        "ws_unet_get_info": [h, C.POINTER(WsUnetInfo)],
+        "ws_unet_get_weights": [h, vp, i64], "ws_unet_set_weights": [h, vp, i64], "ws_unet_set_gain": [h, d],
+        "ws_unet_get_pair": [h, i32, vp, vp, vp], "ws_unet_put_pair": [h, vp, vp, vp],
+        "ws_unet_forward_pair": [h, i32, vp], "ws_unet_grad_pair": [h, i32, vp, C.POINTER(C.c_double)],
+        "ws_unet_probe": [h, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+        "ws_unet_time": [h, i32, i32, C.POINTER(C.c_double)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -323,6 +340,73 @@ class FluidSolver:
         count = self.scalars.nP if count is None else count
         a, _keep = self._host_arrays(arrays, count)
         self._check(self._L.ws_download_state(self._h, C.byref(a)))
+
+    # ---- learned warm start of the pressure solve (no reference counterpart)
+    def unet_init(self, seed=1):
+        self._check(self._L.ws_unet_init(self._h, int(seed)))
+
+    def unet_collect(self, capacity):
+        self._check(self._L.ws_unet_collect(self._h, int(capacity)))
+
+    def unet_enable(self, on=True):
+        self._check(self._L.ws_unet_enable(self._h, 1 if on else 0))
+
+    def unet_train(self, steps, batch=4, lr=1e-3, seed=1):
+        loss = C.c_double()
+        self._check(self._L.ws_unet_train(self._h, int(steps), int(batch), float(lr), int(seed), C.byref(loss)))
+        return loss.value
+
+    def unet_info(self):
+        i = WsUnetInfo()
+        self._check(self._L.ws_unet_get_info(self._h, C.byref(i)))
+        return {f[0]: getattr(i, f[0]) for f in i._fields_}
+
+    def unet_weights(self):
+        n = self.unet_info()["num_weights"]
+        w = np.empty(n, np.float32)
+        self._check(self._L.ws_unet_get_weights(self._h, w.ctypes.data, n))
+        return w
+
+    def unet_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self._L.ws_unet_set_weights(self._h, w.ctypes.data, w.size))
+
+    def unet_set_gain(self, g):
+        self._check(self._L.ws_unet_set_gain(self._h, float(g)))
+
+    def unet_pair(self, idx):
+        N = self.nx * self.ny * self.nz
+        r0n, types, target = np.empty(N, np.float32), np.empty(N, np.uint8), np.empty(N, np.float32)
+        self._check(self._L.ws_unet_get_pair(self._h, int(idx), r0n.ctypes.data, types.ctypes.data,
+                                             target.ctypes.data))
+        return r0n, types, target
+
+    def unet_put_pair(self, r0n, types, target):
+        r0n = np.ascontiguousarray(r0n, np.float32)
+        types = np.ascontiguousarray(types, np.uint8)
+        target = np.ascontiguousarray(target, np.float32)
+        self._check(self._L.ws_unet_put_pair(self._h, r0n.ctypes.data, types.ctypes.data, target.ctypes.data))
+
+    def unet_forward_pair(self, idx):
+        out = np.empty(self.nx * self.ny * self.nz, np.float32)
+        self._check(self._L.ws_unet_forward_pair(self._h, int(idx), out.ctypes.data))
+        return out
+
+    def unet_grad_pair(self, idx):
+        g = np.empty(self.unet_info()["num_weights"], np.float32)
+        loss = C.c_double()
+        self._check(self._L.ws_unet_grad_pair(self._h, int(idx), g.ctypes.data, C.byref(loss)))
+        return g, loss.value
+
+    def unet_probe(self):
+        a, b = C.c_double(), C.c_double()
+        self._check(self._L.ws_unet_probe(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def unet_time(self, what, reps=10):
+        ms = C.c_double()
+        self._check(self._L.ws_unet_time(self._h, int(what), int(reps), C.byref(ms)))
+        return ms.value
 
     def set_nparticles(self, n):
         self._check(self._L.ws_set_nparticles(self._h, int(n)))
