@@ -1,0 +1,116 @@
+"""The warm-start network on the GPU: forward output and loss gradients of
+the tensor-core kernels against the CPU oracle (oracle/ws_unet_oracle.c,
+itself pinned by finite differences), and what a trained network gains
+over the plain previous-q start on the same pressure system.
+
+Tolerances: BF16 activations (8-bit mantissa) are rounded at the same
+points on both sides; the GPU accumulates in FP32 in another order, so a
+value near a rounding boundary can land one BF16 ulp (2^-8 relative) apart
+and propagate. Outputs must agree to 3% (relative L2 over fluid cells),
+gradients to 6% per layer, the loss to 2%."""
+import numpy as np
+import pytest
+
+from helpers import planet, to_device, PLAIN32
+from oracle import unet_oracle as U
+
+pytestmark = pytest.mark.gpu
+
+SOLVE = dict(sorTol=1e-5, sorCheckEvery=10, sorMaxIters=4000)
+DIMS = (32, 32, 32)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def _solver(pairs, stir_every=0, seed=5):
+    o = planet("planet32", **PLAIN32)
+    fs = to_device(o)
+    fs.set_params(**SOLVE)
+    fs.unet_init(seed)
+    fs.unet_collect(pairs)
+    for i in range(pairs):
+        if stir_every and i % stir_every == 0:
+            fs.stir_gaussian(2.0, 1.5)
+        fs._substep(0.01)
+    fs.unet_collect(0)
+    assert fs.unet_info()["pairs_stored"] == pairs
+    return fs
+
+
+@pytest.fixture(scope="module")
+def two_pairs():
+    return _solver(2)
+
+
+def test_pair_contents(two_pairs):
+    fs = two_pairs
+    r0n, types, target = fs.unet_pair(1)
+    fl = types == 1
+    assert fl.sum() > 1000
+    assert np.all(r0n[~fl] == 0) and np.all(target[~fl] == 0)
+    # r0 / sigma has unit RMS over fluid cells by construction
+    assert abs(np.sqrt(np.mean(r0n[fl].astype(np.float64) ** 2)) - 1.0) < 1e-3
+    assert np.abs(target[fl]).max() > 0
+
+
+def test_forward_matches_oracle(two_pairs):
+    fs = two_pairs
+    w = fs.unet_weights()
+    for p in range(2):
+        r0n, types, target = fs.unet_pair(p)
+        gpu = fs.unet_forward_pair(p)
+        cpu = U.forward(DIMS, w, r0n, types, rounding=True)
+        fl = types == 1
+        assert np.all(gpu[cpu == 0] == 0)
+        assert _rel(gpu[fl], cpu[fl]) < 3e-2, p
+
+
+def test_gradients_match_oracle(two_pairs):
+    fs = two_pairs
+    w = fs.unet_weights()
+    r0n, types, target = fs.unet_pair(1)
+    fl = types == 1
+    gain = float(np.sqrt(np.mean(target[fl].astype(np.float64) ** 2)))
+    fs.unet_set_gain(gain)
+    g_gpu, loss_gpu = fs.unet_grad_pair(1)
+    loss_cpu, g_cpu = U.loss_grad(DIMS, w, r0n, types, target / np.float32(gain), rounding=True)
+    assert abs(loss_gpu - loss_cpu) <= 2e-2 * loss_cpu
+    sl = U.slices()
+    for name, (ws, bs) in sl.items():
+        assert _rel(g_gpu[ws], g_cpu[ws]) < 6e-2, name + " weights"
+        assert _rel(g_gpu[bs], g_cpu[bs]) < 6e-2, name + " biases"
+
+
+def test_trained_network_saves_iterations():
+    """Train on pairs from the plain solver's own solves, then on fresh
+    pressure systems compare the SOR iterations to 1e-5 from the previous q
+    and from the prediction, and the residual each start leaves."""
+    fs = _solver(64, stir_every=8)
+    l0 = fs.unet_train(20, batch=4, lr=1e-3, seed=1)
+    l1 = fs.unet_train(400, batch=4, lr=1e-3, seed=2)
+    assert l1 < 0.5 * l0, (l0, l1)
+    rows = []
+    for k in range(6):
+        if k % 3 == 0:
+            fs.stir_gaussian(2.0, 1.5)
+        for st in ("CLEAR_RASTER", "MARK_FLUID", "P2G", "FORCES"):
+            fs.stage(st, 0.01)
+        qprev = fs.download("q")
+        rel0, rel1 = fs.unet_probe()
+        fs.stage("PRESSURE", 0.01)
+        it_learned = fs.scalars.sorIters
+        fs.upload("q", qprev)
+        fs.stage("PRESSURE", 0.01)
+        it_plain = fs.scalars.sorIters
+        rows.append((it_plain, it_learned, rel0, rel1))
+        fs.stage("PROJECT", 0.01)
+        fs.stage("EXTRAPOLATE", 0.01)
+        fs.stage("G2P_ADVECT", 0.01)
+    plain = sum(r[0] for r in rows)
+    learned = sum(r[1] for r in rows)
+    print("iterations plain %d learned %d; residual prev-q %.3g predicted %.3g"
+          % (plain, learned, np.mean([r[2] for r in rows]), np.mean([r[3] for r in rows])))
+    assert np.mean([r[3] for r in rows]) < np.mean([r[2] for r in rows])
+    assert learned < plain
