@@ -10,6 +10,15 @@ off, and the seeded Gaussian stir kick (sigma 4 cells, 2 m/s peak) every 50
 substeps. One bench step = one substep of dt = 0.01 (the reference's
 step(1/60) runs two such substeps).
 
+Learned warm start (the metric's comparison): after the plain solver's
+timed run, the same planet keeps running while every solve stores its
+(input, converged pressure) pair (2000 pairs), the 3-level U-Net is trained
+on them with Adam (lr 1e-3, batch 4), and the same substep is timed again
+with every solve starting from the network's prediction. Both arms solve to
+the same 1e-5 relative residual. `value` is the learned arm's substeps/s;
+the plain arm's figure, SOR iterations of both, the residual left by the
+prediction and the training and inference times are reported beside it.
+
 Arms
   default            the CUDA library through the C ABI (watersim-v1_b200)
   --impl reference   the reference's CPU algorithm: the C restatement of
@@ -40,7 +49,8 @@ PARAMS = dict(pic=0.05, omega=1.7, maxSpeed=3.2, cfl=3.0, viscosity=5e-4, therma
               sorTol=1e-5, sorCheckEvery=10, sorMaxIters=5000, pressureIters=40)
 DT = 0.01
 STIR_EVERY, STIR_SIGMA, STIR_PEAK = 50, 4.0, 2.0
-METRIC = "substeps/s @128^3/2M particles (plain red-black SOR to 1e-5 relative divergence residual)"
+METRIC = "substeps/s @128^3/2M particles: learned warm-start vs plain SOR at equal \u2016\u2207\u00b7u\u2016"
+METRIC_PLAIN = "substeps/s @128^3/2M particles (plain red-black SOR to 1e-5 relative divergence residual)"
 E2E_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pflag")
 
 
@@ -128,34 +138,55 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def timed_region():
+        """K substeps with inputs in HBM, device-timed on the library stream,
+        max over ranks; nvidia-smi clocks sampled during the region."""
+        barrier()
+        clk = Clocks(local_rank)
+        clk.start()
+        time.sleep(0.5)                  # first samples land before the timed region
+        l0 = fs.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            one_step()                   # asynchronous: no host sync inside the timed region
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        clocks = clk.stop()
+        launches = fs.launch_count() - l0
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        its = []                         # SOR iterations per substep, read back afterwards
+        for _ in range(min(20, args.steps)):
+            one_step()
+            its.append(fs.scalars.sorIters)
+        return ms, clocks, launches, its
+
     for _ in range(args.warmup):
         one_step()
-    # ---- device-resident timed region (inputs already in HBM)
-    barrier()
-    clk = Clocks(local_rank)
-    clk.start()
-    time.sleep(0.5)                      # first samples land before the timed region
-    l0 = fs.launch_count()
-    iters0 = []
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        one_step()                       # asynchronous: no host sync inside the timed region
-    e1.record(stream)
-    e1.synchronize()
-    barrier()
-    clocks = clk.stop()
-    launches = fs.launch_count() - l0
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    # ---- plain SOR arm
+    ms, clocks, launches, iters0 = timed_region()
+    plain = {"substeps_per_s": args.steps * world / (ms / 1000.0), "ms_per_step": ms / args.steps,
+             "sor_iterations": sum(iters0) / len(iters0), "clocks": clocks}
+    ms_plain = ms
+    # ---- learned warm-start arm
+    learned = None
+    if not args.no_learned:
+        learned = learned_arm(fs, one_step, args)
+        for _ in range(args.warmup):
+            one_step()
+        ms, clocks, launches, iters1 = timed_region()
+        learned["sor_iterations"] = sum(iters1) / len(iters1)
+        learned["substeps_per_s"] = args.steps * world / (ms / 1000.0)
+        learned["ms_per_step"] = ms / args.steps
+        qsave = fs.download("q")
+        learned["inference_ms"] = fs.unet_time(0, 10)   # applies the prediction repeatedly: restore q after
+        fs.upload("q", qsave)
     value = args.steps * world / (ms / 1000.0)
-    # SOR iterations per substep, read back after the timed region
-    for _ in range(min(20, args.steps)):
-        one_step()
-        iters0.append(fs.scalars.sorIters)
     # ---- end to end through the public API with pinned host buffers
     host = {k: torch.empty(nP, dtype=torch.uint8 if k == "pflag" else torch.float32).pin_memory().numpy()
             for k in E2E_FIELDS}
@@ -175,21 +206,28 @@ def run_ours(args, rank, world, local_rank):
         e2e_s = float(t.item())
     bytes_io = sum(host[k].nbytes for k in E2E_FIELDS)
     # ---- roofline of the dominant kernel, timed live on the library stream
-    roof = roofline(fs, ms / args.steps, iters0)
+    roof = roofline(fs, ms_plain / args.steps, iters0)
     out = None
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": "substeps/s", "n_gpus": world,
+        cfg_learned = {}
+        if learned:
+            cfg_learned = {"plain_substeps_per_s": plain["substeps_per_s"],
+                           "learned_vs_plain": learned["substeps_per_s"] / plain["substeps_per_s"],
+                           "warm_start": learned, "plain": plain}
+        out = {"metric": METRIC if learned else METRIC_PLAIN, "value": value, "unit": "substeps/s", "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)",
                "config": {"workload": "planet128: 128^3 MAC grid, R=52, depth 8, %d particles" % nP,
                           "particles": nP, "parallelism": "replicas x%d" % world,
+                          "arm": "learned warm start" if learned else "plain SOR",
                           "sor": "red-black to 1e-5 (check every 10), mean iterations %.1f"
-                                 % (sum(iters0) / max(1, len(iters0))),
+                                 % ((learned or plain)["sor_iterations"]),
                           "fluid_cells": fs.scalars.nFluid,
                           "sor_path": {0: "none", 1: "grid-wide persistent", 2: "cluster-resident (DSMEM)"}[fs.scalars.sorPath],
                           "particle_substeps_per_s": value * nP,
-                          "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP)},
+                          "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP),
+                          **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
                "gpu_launches": int(launches),
@@ -202,6 +240,53 @@ def state_mb(fs, nP):
     n = fs.nx
     F = 3 * (n + 1) * n * n
     return int((nP * 55 + F * 21 + n ** 3 * 16) / 1e6)
+
+
+def learned_arm(fs, one_step, args):
+    """Record (input, converged q) pairs from the plain solves, train the
+    U-Net on them, and measure what its prediction leaves for SOR on fresh
+    pressure systems. Leaves the warm start enabled."""
+    fs.unet_init(7)
+    fs.unet_collect(args.pairs)
+    t0 = time.perf_counter()
+    for _ in range(args.pairs):
+        one_step()
+    fs.synchronize()
+    collect_s = time.perf_counter() - t0
+    fs.unet_collect(0)
+    t0 = time.perf_counter()
+    loss0 = fs.unet_train(10, 4, 1e-3, 1)
+    loss1 = fs.unet_train(args.train_steps, 4, 1e-3, 2)
+    fs.synchronize()
+    train_s = time.perf_counter() - t0
+    # fresh pressure systems: iterations from the previous q and from the
+    # prediction (check every iteration), and the residual each start leaves
+    keep = (fs.sorCheckEvery,)
+    fs.sorCheckEvery = 1
+    rows = []
+    for k in range(8):
+        for st in ("CLEAR_RASTER", "MARK_FLUID", "P2G", "FORCES"):
+            fs.stage(st, DT)
+        qprev = fs.download("q")
+        r0, r1 = fs.unet_probe()
+        fs.stage("PRESSURE", DT)
+        it_l = fs.scalars.sorIters
+        fs.upload("q", qprev)
+        fs.stage("PRESSURE", DT)
+        it_p = fs.scalars.sorIters
+        rows.append((it_p, it_l, r0, r1))
+        for st in ("PROJECT", "EXTRAPOLATE", "G2P_ADVECT"):
+            fs.stage(st, DT)
+    fs.sorCheckEvery = keep[0]
+    fs.unet_enable(True)
+    n = len(rows)
+    return {"pairs": args.pairs, "collect_s": collect_s, "train_steps": args.train_steps + 10, "batch": 4,
+            "lr": 1e-3, "train_s": train_s, "loss_first": loss0, "loss_last": loss1,
+            "train_ms_per_sample": fs.unet_time(1, 3),
+            "probe_iterations_plain": sum(r[0] for r in rows) / n,
+            "probe_iterations_learned": sum(r[1] for r in rows) / n,
+            "probe_relres_previous_q": sum(r[2] for r in rows) / n,
+            "probe_relres_predicted": sum(r[3] for r in rows) / n}
 
 
 def roofline(fs, ms_step, iters):
@@ -326,6 +411,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="plain SOR arm only")
+    ap.add_argument("--pairs", type=int, default=2000, help="training pairs recorded from plain solves")
+    ap.add_argument("--train-steps", type=int, default=1000, help="Adam steps of batch 4")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

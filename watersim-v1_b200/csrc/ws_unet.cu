@@ -154,9 +154,10 @@ __global__ void k_scale(float* __restrict__ r0, long long n, const double* sigma
 // network input at the voxels of active level-0 tiles
 __global__ void k_input(Level L, const int* tiles, const int* count, const float* __restrict__ r0n,
                         const uint8_t* __restrict__ type, bf16* __restrict__ x) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   int X, Y, Z; long long v;
-  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) return;
+  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) continue;
   uint8_t t = type[v];
   bf16 ch[16];
 #pragma unroll
@@ -168,17 +169,19 @@ __global__ void k_input(Level L, const int* tiles, const int* count, const float
   uint4* dst = reinterpret_cast<uint4*>(x + v * 16);
   const uint4* s = reinterpret_cast<const uint4*>(ch);
   dst[0] = s[0]; dst[1] = s[1];
+  }
 }
 
 // ------------------------------------------------------------ pooling
 // coarse voxel = mean of its 8 fine voxels (inactive / outside read as 0)
 __global__ void k_pool(Level C, const int* tiles, const int* count, Level F, const uint8_t* __restrict__ factive,
                        const bf16* __restrict__ fine, bf16* __restrict__ coarse, int ch) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024 * (ch / 8);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   long long task = i / (ch / 8);
   int c8 = (int)(i % (ch / 8)) * 8;
   int X, Y, Z; long long v;
-  if (!tile_voxel(C, tiles, *count, task, X, Y, Z, v)) return;
+  if (!tile_voxel(C, tiles, *count, task, X, Y, Z, v)) continue;
   float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int k = 0; k < 8; k++) {
     int fx = 2 * X + (k & 1), fy = 2 * Y + ((k >> 1) & 1), fz = 2 * Z + (k >> 2);
@@ -193,17 +196,19 @@ __global__ void k_pool(Level C, const int* tiles, const int* count, Level F, con
 #pragma unroll
   for (int e = 0; e < 4; e++) ob[e] = __floats2bfloat162_rn(acc[2 * e] * 0.125f, acc[2 * e + 1] * 0.125f);
   *reinterpret_cast<uint4*>(coarse + v * ch + c8) = o;
+  }
 }
 // backward of pool, added to the skip gradient and masked by the ReLU of s:
 // ds(v) = (dskip(v) + dpool(parent) / 8) * (s(v) > 0)
 __global__ void k_pool_bwd_add(Level F, const int* tiles, const int* count, Level C,
                                const bf16* __restrict__ dskip, const bf16* __restrict__ dpool,
                                const bf16* __restrict__ s, bf16* __restrict__ ds, int ch) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024 * (ch / 8);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   long long task = i / (ch / 8);
   int c8 = (int)(i % (ch / 8)) * 8;
   int X, Y, Z; long long v;
-  if (!tile_voxel(F, tiles, *count, task, X, Y, Z, v)) return;
+  if (!tile_voxel(F, tiles, *count, task, X, Y, Z, v)) continue;
   long long pv = ((long long)(Z >> 1) * C.ny + (Y >> 1)) * C.nx + (X >> 1);
   uint4 a = __ldg(reinterpret_cast<const uint4*>(dskip + v * ch + c8));
   uint4 b = __ldg(reinterpret_cast<const uint4*>(dpool + pv * ch + c8));
@@ -218,16 +223,18 @@ __global__ void k_pool_bwd_add(Level F, const int* tiles, const int* count, Leve
 #pragma unroll
   for (int e = 0; e < 4; e++) ob[e] = __floats2bfloat162_rn(r[2 * e], r[2 * e + 1]);
   *reinterpret_cast<uint4*>(ds + v * ch + c8) = o;
+  }
 }
 // backward of the nearest upsampling: coarse gradient = sum over the 8 fine
 // children (inactive / outside read as 0), masked by the ReLU of act
 __global__ void k_up_bwd(Level C, const int* tiles, const int* count, Level F, const uint8_t* __restrict__ factive,
                          const bf16* __restrict__ dup, const bf16* __restrict__ act, bf16* __restrict__ dc, int ch) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024 * (ch / 8);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   long long task = i / (ch / 8);
   int c8 = (int)(i % (ch / 8)) * 8;
   int X, Y, Z; long long v;
-  if (!tile_voxel(C, tiles, *count, task, X, Y, Z, v)) return;
+  if (!tile_voxel(C, tiles, *count, task, X, Y, Z, v)) continue;
   float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int k = 0; k < 8; k++) {
     int fx = 2 * X + (k & 1), fy = 2 * Y + ((k >> 1) & 1), fz = 2 * Z + (k >> 2);
@@ -246,6 +253,7 @@ __global__ void k_up_bwd(Level C, const int* tiles, const int* count, Level F, c
     ob[e] = __floats2bfloat162_rn(__bfloat162float(pm[2 * e]) > 0.f ? acc[2 * e] : 0.f,
                                   __bfloat162float(pm[2 * e + 1]) > 0.f ? acc[2 * e + 1] : 0.f);
   *reinterpret_cast<uint4*>(dc + v * ch + c8) = o;
+  }
 }
 
 // ------------------------------------------------------------ output head
@@ -253,27 +261,31 @@ __global__ void k_up_bwd(Level C, const int* tiles, const int* count, Level F, c
 __global__ void k_head_apply(Level L, const int* tiles, const int* count, const bf16* __restrict__ h,
                              const float* __restrict__ head, const uint8_t* __restrict__ type,
                              const double* sigma, const double* gain, float* __restrict__ q) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   int X, Y, Z; long long v;
-  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) return;
-  if (type[v] != WS_FLUID) return;
+  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) continue;
+  if (type[v] != WS_FLUID) continue;
   uint4 u[2] = { __ldg(reinterpret_cast<const uint4*>(h + v * 16)), __ldg(reinterpret_cast<const uint4*>(h + v * 16) + 1) };
   const bf16* b = reinterpret_cast<const bf16*>(u);
   float o = head[16];
 #pragma unroll
   for (int c = 0; c < 16; c++) o += head[c] * __bfloat162float(b[c]);
   q[v] = (float)((double)q[v] + *sigma * *gain * (double)o);
+  }
 }
 // network output at every active voxel (testing) -> out (fp32, dense)
 __global__ void k_head_out(Level L, const int* tiles, const int* count, const bf16* __restrict__ h,
                            const float* __restrict__ head, float* __restrict__ out) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)*count * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   int X, Y, Z; long long v;
-  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) return;
+  if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) continue;
   const bf16* b = h + v * 16;
   float o = head[16];
   for (int c = 0; c < 16; c++) o += head[c] * __bfloat162float(b[c]);
   out[v] = o;
+  }
 }
 // training head: loss = sum_fluid (out - t)^2 / nFluid, its gradients for
 // wh, bh (grad[0..16]) and dh = dloss/dout * wh * (h > 0) at every active voxel
@@ -283,13 +295,14 @@ __global__ void k_head_train(Level L, const int* tiles, const int* count, const 
                              bf16* __restrict__ dh, float* __restrict__ ghead, double* loss) {
   __shared__ float sg[17][8];
   __shared__ double sl[8];
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   int X, Y, Z; long long v;
   float g[17];
 #pragma unroll
   for (int c = 0; c < 17; c++) g[c] = 0.f;
   double l = 0;
-  if (tile_voxel(L, tiles, *count, i, X, Y, Z, v)) {
+  const long long n = (long long)*count * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if (!tile_voxel(L, tiles, *count, i, X, Y, Z, v)) continue;
     const bf16* b = h + v * 16;
     float hv[16];
     float o = head[16];
@@ -298,13 +311,13 @@ __global__ void k_head_train(Level L, const int* tiles, const int* count, const 
     float dout = 0.f;
     if (type[v] == WS_FLUID) {
       float diff = o - target[v];
-      l = (double)diff * diff;
+      l += (double)diff * diff;
       dout = 2.f * diff / (float)max(*nFluid, 1);
     }
     bf16 od[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) { od[c] = __float2bfloat16_rn(hv[c] > 0.f ? dout * head[c] : 0.f); g[c] = dout * hv[c]; }
-    g[16] = dout;
+    for (int c = 0; c < 16; c++) { od[c] = __float2bfloat16_rn(hv[c] > 0.f ? dout * head[c] : 0.f); g[c] += dout * hv[c]; }
+    g[16] += dout;
     uint4* dst = reinterpret_cast<uint4*>(dh + v * 16);
     dst[0] = reinterpret_cast<uint4*>(od)[0]; dst[1] = reinterpret_cast<uint4*>(od)[1];
   }
@@ -342,12 +355,13 @@ __global__ void __launch_bounds__(kDwThreads) k_dw(DwArgs a) {
   bf16* halo = reinterpret_cast<bf16*>(dsm);                                // [HV][16]
   float* pl = reinterpret_cast<float*>(dsm + HV * 32);                      // [128][16]
   const int cin = a.c0 + a.c1, nsl = cin >> 4, nog = a.cout >> 4;
-  const int nT = *a.nTiles;
-  int b = blockIdx.x;
+  const int nItems = *a.nTiles * nsl * nog;
+  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
+  int b = item;
   const int og = b % nog; b /= nog;
   const int kk = b % nsl; b /= nsl;
-  if (b >= nT) return;
   const int tile = a.tiles[b];
+  __syncthreads();                                   // the previous item is done with the halo
   const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
   const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ;
   for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
@@ -434,6 +448,7 @@ __global__ void __launch_bounds__(kDwThreads) k_dw(DwArgs a) {
         atomicAdd(a.dw + ((size_t)co * cin + ci) * 27 + gt[r], acc[r][p * 4 + q]);
       }
   if (kk == 0 && threadIdx.x < 16) atomicAdd(a.db + og * 16 + threadIdx.x, bsum);
+  }
 }
 static size_t dw_smem_bytes() { return (size_t)(kTX + 2) * (kTY + 2) * (kTZ + 2) * 32 + 128 * 16 * 4; }
 
@@ -500,6 +515,8 @@ __global__ void k_scale_copy(const float* __restrict__ a, float* __restrict__ b,
 
 // ------------------------------------------------------------ host driver
 static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
+// grid of a grid-stride kernel over at most n items: a few waves of the device
+static inline unsigned gridv(long long n, int b) { return (unsigned)std::min<long long>(grid1(n, b), 148LL * 8); }
 
 // He-normal initial weights from a seeded LCG and Box-Muller (host)
 struct HostRng {
@@ -671,14 +688,15 @@ cudaError_t Net::dw(int l, const bf16* src0, const bf16* src1, const bf16* dz, c
   const int cin = S.c0 + S.c1;
   static bool attr = false;
   if (!attr) { cudaFuncSetAttribute(k_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dw_smem_bytes()); attr = true; }
-  k_dw<<<(unsigned)(L.ntiles * (cin / 16) * (S.cout / 16)), kDwThreads, dw_smem_bytes(), s>>>(a);
+  const long long items = (long long)L.ntiles * (cin / 16) * (S.cout / 16);
+  k_dw<<<(unsigned)std::min<long long>(items, 148LL * 3), kDwThreads, dw_smem_bytes(), s>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t Net::pool(int fineLevel, const bf16* fine, bf16* coarse, int ch, cudaStream_t s) {
   const Level& C = lv[fineLevel + 1];
   long long n = (long long)C.ntiles * 1024 * (ch / 8);
-  k_pool<<<grid1(n, 256), 256, 0, s>>>(C, tiles[fineLevel + 1], counts + fineLevel + 1, lv[fineLevel], act[fineLevel],
+  k_pool<<<gridv(n, 256), 256, 0, s>>>(C, tiles[fineLevel + 1], counts + fineLevel + 1, lv[fineLevel], act[fineLevel],
                                        fine, coarse, ch);
   return cudaGetLastError();
 }
@@ -706,14 +724,14 @@ cudaError_t Net::backward(cudaStream_t s) {
   auto upb = [&](int coarseLevel, const bf16* dup, const bf16* a, bf16* out, int ch) {
     const Level& C = lv[coarseLevel];
     long long n = (long long)C.ntiles * 1024 * (ch / 8);
-    k_up_bwd<<<grid1(n, 256), 256, 0, s>>>(C, tiles[coarseLevel], counts + coarseLevel, lv[coarseLevel - 1],
+    k_up_bwd<<<gridv(n, 256), 256, 0, s>>>(C, tiles[coarseLevel], counts + coarseLevel, lv[coarseLevel - 1],
                                            act[coarseLevel - 1], dup, a, out, ch);
     return cudaGetLastError();
   };
   auto pba = [&](int fineLevel, const bf16* dskip, const bf16* dpool, const bf16* sAct, bf16* out, int ch) {
     const Level& F = lv[fineLevel];
     long long n = (long long)F.ntiles * 1024 * (ch / 8);
-    k_pool_bwd_add<<<grid1(n, 256), 256, 0, s>>>(F, tiles[fineLevel], counts + fineLevel, lv[fineLevel + 1],
+    k_pool_bwd_add<<<gridv(n, 256), 256, 0, s>>>(F, tiles[fineLevel], counts + fineLevel, lv[fineLevel + 1],
                                                  dskip, dpool, sAct, out, ch);
     return cudaGetLastError();
   };
@@ -747,7 +765,7 @@ cudaError_t Net::prepare(const float* r0nIn, const uint8_t* type, cudaStream_t s
   cudaError_t e;
   if ((e = activity(type, s)) != cudaSuccess) return e;
   long long n = (long long)lv[0].ntiles * 1024;
-  k_input<<<grid1(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0nIn, type, x);
+  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0nIn, type, x);
   return cudaGetLastError();
 }
 // r0 / sigma of the current pressure setup into dst, sigma into sig
@@ -766,9 +784,9 @@ cudaError_t Net::predict(float* q, const float* rhs, const uint8_t* diag8, const
   if ((e = activity(type, s)) != cudaSuccess) return e;          // also the fluid count sigma divides by
   if ((e = residual(q, rhs, diag8, type, r0n, scal + 0, s)) != cudaSuccess) return e;
   long long n = (long long)lv[0].ntiles * 1024;
-  k_input<<<grid1(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, type, x);
+  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, type, x);
   if ((e = forward(s)) != cudaSuccess) return e;
-  k_head_apply<<<grid1(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, type, scal + 0, scal + 1, q);
+  k_head_apply<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, type, scal + 0, scal + 1, q);
   return cudaGetLastError();
 }
 
@@ -853,7 +871,7 @@ cudaError_t Net::sample_grad(int p, cudaStream_t s) {
   if ((e = forward(s)) != cudaSuccess) return e;
   k_scale_copy<<<grid1(N, 256), 256, 0, s>>>(ptarget + N * p, tscaled, N, (float)(1.0 / gain));
   long long n = (long long)lv[0].ntiles * 1024;
-  k_head_train<<<grid1(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, ptype + N * p, tscaled,
+  k_head_train<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, ptype + N * p, tscaled,
                                              counts + 3, gh, grads + headOff, scal + 2);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return backward(s);
@@ -892,7 +910,7 @@ cudaError_t Net::forward_pair(int p, float* outHost, cudaStream_t s) {
   if ((e = forward(s)) != cudaSuccess) return e;
   cudaMemsetAsync(outbuf, 0, sizeof(float) * N, s);
   long long n = (long long)lv[0].ntiles * 1024;
-  k_head_out<<<grid1(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, outbuf);
+  k_head_out<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, outbuf);
   if ((e = cudaMemcpyAsync(outHost, outbuf, sizeof(float) * N, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   return cudaStreamSynchronize(s);
 }

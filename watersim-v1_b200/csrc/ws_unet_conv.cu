@@ -22,6 +22,7 @@
 // WS_DERR_TIMEOUT, waits once more (bounded) for its MMAs, frees its tensor
 // memory and returns.
 #include "ws_unet.cuh"
+#include <algorithm>
 
 namespace unet {
 
@@ -92,24 +93,67 @@ template <int COUT> struct ConvShape {
   static constexpr int SMEM = 2 * KSTR + WCH > SMEM_MIN ? 2 * KSTR + WCH : SMEM_MIN;
 };
 
+// 16-byte asynchronous global -> shared copy; src_size 0 writes zeros
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_size) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(dst), "l"(src), "r"(src_size) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// queue the copies of one 16-channel slice of the halo of sub-tile (X0, Y0, Z0)
+template <int COUT>
+__device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, int Z0, int kk, uint32_t hbase) {
+  using S = ConvShape<COUT>;
+  constexpr int HX = S::HX, HY = S::HY, HV = S::HV, KSTR = S::KSTR;
+  const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
+  for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
+    const int j = i & 1, hv = i >> 1;
+    const int hx = hv % HX, t2 = hv / HX, hy = t2 % HY, hz = t2 / HY;
+    const int gx = X0 - 1 + hx, gy = Y0 - 1 + hy, gz = Z0 - 1 + hz;
+    const bf16* p = a.src1 ? a.src1 : a.src0;             // any valid address when nothing is read
+    uint32_t n = 0;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
+        a.active[((gz / kTZ) * a.nty + gy / kTY) * a.ntx + gx / kTX]) {
+      const int c = kk * 16 + j * 8;
+      if (c < a.c0) {
+        p = a.up0 ? a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c
+                  : a.src0 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c0 + c;
+      } else {
+        p = a.src1 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c1 + (c - a.c0);
+      }
+      n = 16;
+    }
+    cp_async16(hbase + (uint32_t)(j * KSTR + hv * 16), p, n);
+  }
+}
+template <int COUT>
+__device__ __forceinline__ void stage_weights(const ConvArgs& a, int kk, uint32_t wbase) {
+  constexpr int WCH = ConvShape<COUT>::WCH;
+  const char* src = reinterpret_cast<const char*>(a.w) + (size_t)kk * WCH;
+  for (int i = threadIdx.x; i < WCH / 16; i += blockDim.x) cp_async16(wbase + (uint32_t)(i * 16), src + (size_t)i * 16, 16);
+}
+
+// Persistent over the work items (active tile x z sub-tile): tensor memory
+// is allocated once per CTA; weights stay resident when the input has a
+// single 16-channel slice; the next item's first slice is fetched while
+// the current item's accumulators are drained.
 template <int COUT>
 __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   using S = ConvShape<COUT>;
-  constexpr int ZT = S::ZT, HX = S::HX, HY = S::HY, HV = S::HV, KSTR = S::KSTR, WCH = S::WCH;
+  constexpr int ZT = S::ZT, HX = S::HX, HY = S::HY, KSTR = S::KSTR;
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char* halo = smem;                       // [2][HV][16 B]
-  unsigned char* wsm = smem + 2 * KSTR;             // [27][2][COUT][16 B]
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
 
   constexpr int sub = kTZ / ZT;
-  const int nT = *a.nTiles;
-  if ((int)blockIdx.x >= nT * sub) return;          // uniform over the CTA
-  const int tile = a.tiles[blockIdx.x / sub];
-  const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
-  const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ + (int)(blockIdx.x % sub) * ZT;
+  const int nItems = *a.nTiles * sub;
+  if ((int)blockIdx.x >= nItems) return;            // uniform over the CTA
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t hbase = smem_u32(smem), wbase = hbase + 2 * KSTR;
+  const int cin = a.c0 + a.c1, nslices = cin >> 4;
+  const bool wres = nslices == 1;                   // weights loaded once
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -121,104 +165,105 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
-
-  const int cin = a.c0 + a.c1;
-  const int nslices = cin >> 4;
   constexpr uint32_t idesc = idesc_bf16_m128(COUT);
   uint32_t phase = 0;
   bool pending = false;
-  for (int kk = 0; kk < nslices; kk++) {
-    // ---- stage the halo of input channels [16 kk, 16 kk + 16) and their weights
-    for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
-      const int j = i & 1, hv = i >> 1;
-      const int hx = hv % HX, t2 = hv / HX, hy = t2 % HY, hz = t2 / HY;
-      const int gx = X0 - 1 + hx, gy = Y0 - 1 + hy, gz = Z0 - 1 + hz;
-      uint4 val = make_uint4(0u, 0u, 0u, 0u);
-      if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
-          a.active[((gz / kTZ) * a.nty + gy / kTY) * a.ntx + gx / kTX]) {
-        const int c = kk * 16 + j * 8;
-        const bf16* p;
-        if (c < a.c0) {
-          if (a.up0) {
-            const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
-            p = a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c;
-          } else {
-            p = a.src0 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c0 + c;
-          }
-        } else {
-          p = a.src1 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c1 + (c - a.c0);
-        }
-        val = __ldg(reinterpret_cast<const uint4*>(p));
-      }
-      *reinterpret_cast<uint4*>(halo + j * KSTR + hv * 16) = val;
-    }
-    const uint4* wsrc = reinterpret_cast<const uint4*>(a.w) + (size_t)kk * (WCH / 16);
-    for (int i = threadIdx.x; i < WCH / 16; i += blockDim.x) reinterpret_cast<uint4*>(wsm)[i] = __ldg(wsrc + i);
-    fence_proxy_async();                             // generic-proxy stores -> tensor-core reads
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      fence_after();
-      const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
-      for (int z = 0; z < ZT; z++) {
+
+  auto origin = [&](int item, int& X0, int& Y0, int& Z0) {
+    const int tile = a.tiles[item / sub];
+    const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
+    X0 = tx * kTX; Y0 = ty * kTY; Z0 = tz * kTZ + (item % sub) * ZT;
+  };
+  int X0, Y0, Z0;
+  origin(blockIdx.x, X0, Y0, Z0);
+  stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase);
+  stage_weights<COUT>(a, 0, wbase);
+  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
+    for (int kk = 0; kk < nslices; kk++) {
+      cp_async_wait_all();
+      fence_proxy_async();                           // generic-proxy writes -> tensor-core reads
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        fence_after();
+        // taps outer, planes inner: consecutive MMAs go to different
+        // accumulators, so ZT of them are in flight instead of a chain of
+        // read-modify-writes of one accumulator
 #pragma unroll 1
         for (int t = 0; t < 27; t++) {
           const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint64_t ad = smem_desc(hbase + (uint32_t)((((z + dz) * HY + dy) * HX + dx) * 16), KSTR, HX * 16);
           const uint64_t bd = smem_desc(wbase + (uint32_t)(t * 2 * COUT * 16), COUT * 16, 128);
-          mma_bf16(tmem + (uint32_t)(z * COUT), ad, bd, idesc, (kk | t) != 0);
+#pragma unroll
+          for (int z = 0; z < ZT; z++) {
+            const uint64_t ad = smem_desc(hbase + (uint32_t)((((z + dz) * HY + dy) * HX + dx) * 16), KSTR, HX * 16);
+            mma_bf16(tmem + (uint32_t)(z * COUT), ad, bd, idesc, (kk | t) != 0);
+          }
+        }
+        mma_commit(&mbar);
+      }
+      pending = true;
+      const bool ok = mbar_wait(&mbar, phase);       // the staged operands are free again
+      if (!ok) { s_abort = 1; atomicOr(a.err, WS_DERR_TIMEOUT); }
+      __syncthreads();
+      if (s_abort) break;
+      pending = false;
+      phase ^= 1u;
+      if (kk + 1 < nslices) {
+        stage_halo<COUT>(a, X0, Y0, Z0, kk + 1, hbase);
+        stage_weights<COUT>(a, kk + 1, wbase);
+      }
+    }
+    if (s_abort) break;
+    // fetch the next item's first slice while this item's accumulators drain
+    const int cX = X0, cY = Y0, cZ = Z0;
+    const int next = item + gridDim.x;
+    if (next < nItems) {
+      origin(next, X0, Y0, Z0);
+      stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase);
+      if (!wres) stage_weights<COUT>(a, 0, wbase);
+    }
+    fence_after();
+    {
+      const int q = warp & 3;                        // tensor-memory lane quarter of this warp
+      const int m = q * 32 + lane;                   // accumulator row = voxel of the plane
+      const int gx = cX + (m & 7), gy = cY + (m >> 3);
+      for (int z = warp >> 2; z < ZT; z += 2) {
+        const int gz = cZ + z;
+        const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
+        const size_t vox = ((size_t)gz * a.ny + gy) * a.nx + gx;
+#pragma unroll 1
+        for (int cg = 0; cg < COUT / 16; cg++) {
+          uint32_t r[16];
+          tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(z * COUT + cg * 16), r);
+          if (!in) continue;
+          float v[16];
+#pragma unroll
+          for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+          const int c = cg * 16;
+          if (a.mode == 0) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + __ldg(a.bias + c + i), 0.f);
+          } else if (a.mask) {
+            const uint4* mp = reinterpret_cast<const uint4*>(a.mask + vox * COUT + c);
+            uint4 mk[2] = { __ldg(mp), __ldg(mp + 1) };
+            const bf16* mb = reinterpret_cast<const bf16*>(mk);
+#pragma unroll
+            for (int i = 0; i < 16; i++) if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
+          }
+          uint4 o[2];
+          __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+          for (int i = 0; i < 8; i++) ob[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+          uint4* dst = c < a.split
+              ? reinterpret_cast<uint4*>(a.out0 + vox * a.split + c)
+              : reinterpret_cast<uint4*>(a.out1 + vox * (COUT - a.split) + (c - a.split));
+          dst[0] = o[0]; dst[1] = o[1];
         }
       }
-      mma_commit(&mbar);
     }
-    pending = true;
-    // the next slice overwrites the staged operands: wait for the MMAs that read them
-    const bool ok = mbar_wait(&mbar, phase);
-    if (!ok) { s_abort = 1; atomicOr(a.err, WS_DERR_TIMEOUT); }
-    __syncthreads();
-    if (s_abort) break;
-    pending = false;
-    phase ^= 1u;
+    fence_before();                                  // accumulators read before the next item's MMAs
   }
   if (s_abort && pending) mbar_wait(&mbar, phase);    // bounded: let the issued MMAs drain
-  fence_after();
-  if (!s_abort) {
-    const int q = warp & 3;                          // tensor-memory lane quarter of this warp
-    const int m = q * 32 + lane;                     // accumulator row = voxel of the plane
-    const int gx = X0 + (m & 7), gy = Y0 + (m >> 3);
-    for (int z = warp >> 2; z < ZT; z += 2) {
-      const int gz = Z0 + z;
-      const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
-      const size_t vox = ((size_t)gz * a.ny + gy) * a.nx + gx;
-#pragma unroll 1
-      for (int cg = 0; cg < COUT / 16; cg++) {
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(z * COUT + cg * 16), r);
-        if (!in) continue;
-        float v[16];
-#pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-        const int c = cg * 16;
-        if (a.mode == 0) {
-#pragma unroll
-          for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + __ldg(a.bias + c + i), 0.f);
-        } else if (a.mask) {
-          const uint4* mp = reinterpret_cast<const uint4*>(a.mask + vox * COUT + c);
-          uint4 mk[2] = { __ldg(mp), __ldg(mp + 1) };
-          const bf16* mb = reinterpret_cast<const bf16*>(mk);
-#pragma unroll
-          for (int i = 0; i < 16; i++) if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
-        }
-        uint4 o[2];
-        __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
-#pragma unroll
-        for (int i = 0; i < 8; i++) ob[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-        uint4* dst = c < a.split
-            ? reinterpret_cast<uint4*>(a.out0 + vox * a.split + c)
-            : reinterpret_cast<uint4*>(a.out1 + vox * (COUT - a.split) + (c - a.split));
-        dst[0] = o[0]; dst[1] = o[1];
-      }
-    }
-  }
+  cp_async_wait_all();
   fence_before();
   __syncthreads();
   if (warp == 0)
@@ -252,7 +297,13 @@ cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t
   if (((a.c0 + a.c1) & 15) || (a.c0 & 7) || (a.c1 & 7) || a.c0 + a.c1 <= 0 || (a.split & 15)) return cudaErrorInvalidValue;
   const int zt = conv3_zt(cout);
   if (!zt) return cudaErrorInvalidValue;
-  const dim3 grid((unsigned)(maxTiles * (kTZ / zt)));
+  // persistent: at most the CTAs the device holds at once, never more than the work items
+  static int smCount = 0;
+  if (!smCount) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev); }
+  const size_t smb = conv3_smem_bytes(cout);
+  const int perSM = (int)(233472 / (smb + 1024 + 256));
+  const long long items = (long long)maxTiles * (kTZ / zt);
+  const dim3 grid((unsigned)std::min<long long>(items, (long long)smCount * std::max(perSM, 1)));
   if (grid.x == 0) return cudaSuccess;
   const size_t sm = conv3_smem_bytes(cout);
   switch (cout) {
