@@ -103,6 +103,15 @@ class Clocks:
                 "reasons": reasons, "samples": len(sm)}
 
 
+def reduce_max(value, device):
+    """Max of a per-rank float over all ranks (the device-time rule for N > 1)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_solver(device, rank=0):
     """The 128^3 planet through the library's own terrain generator and fill."""
     from fluid_solver import FluidSolver
@@ -157,9 +166,7 @@ def run_ours(args, rank, world, local_rank):
         launches = fs.launch_count() - l0
         ms = e0.elapsed_time(e1)
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = reduce_max(ms, "cuda")
         its = []                         # SOR iterations per substep, read back afterwards
         for _ in range(min(20, args.steps)):
             one_step()
@@ -176,7 +183,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- learned warm-start arm
     learned = None
     if not args.no_learned:
-        learned = learned_arm(fs, one_step, args)
+        learned = learned_arm(fs, one_step, args, world)
         for _ in range(args.warmup):
             one_step()
         ms, clocks, launches, iters1 = timed_region()
@@ -201,9 +208,7 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = reduce_max(e2e_s, "cuda")
     bytes_io = sum(host[k].nbytes for k in E2E_FIELDS)
     # ---- roofline of the dominant kernel, timed live on the library stream
     roof = roofline(fs, ms_plain / args.steps, iters0)
@@ -242,7 +247,7 @@ def state_mb(fs, nP):
     return int((nP * 55 + F * 21 + n ** 3 * 16) / 1e6)
 
 
-def learned_arm(fs, one_step, args):
+def learned_arm(fs, one_step, args, world=1):
     """Record (input, converged q) pairs from the plain solves, train the
     U-Net on them, and measure what its prediction leaves for SOR on fresh
     pressure systems. Leaves the warm start enabled."""
@@ -255,8 +260,15 @@ def learned_arm(fs, one_step, args):
     collect_s = time.perf_counter() - t0
     fs.unet_collect(0)
     t0 = time.perf_counter()
-    loss0 = fs.unet_train(10, 4, 1e-3, 1)
-    loss1 = fs.unet_train(args.train_steps, 4, 1e-3, 2)
+    if world > 1:
+        # one network for all replicas: gradients summed over the ranks each step
+        import dp_train
+        dp_train.agree_gain(fs)
+        loss0 = dp_train.train_data_parallel(fs, 10, 4, 1e-3, 1)
+        loss1 = dp_train.train_data_parallel(fs, args.train_steps, 4, 1e-3, 2)
+    else:
+        loss0 = fs.unet_train(10, 4, 1e-3, 1)
+        loss1 = fs.unet_train(args.train_steps, 4, 1e-3, 2)
     fs.synchronize()
     train_s = time.perf_counter() - t0
     # fresh pressure systems: iterations from the previous q and from the
@@ -280,7 +292,8 @@ def learned_arm(fs, one_step, args):
     fs.sorCheckEvery = keep[0]
     fs.unet_enable(True)
     n = len(rows)
-    return {"pairs": args.pairs, "collect_s": collect_s, "train_steps": args.train_steps + 10, "batch": 4,
+    return {"pairs": args.pairs, "collect_s": collect_s, "train_steps": args.train_steps + 10, "batch": 4 * world,
+            "training": "data-parallel over %d ranks (gradients all-reduced)" % world if world > 1 else "one GPU",
             "lr": 1e-3, "train_s": train_s, "loss_first": loss0, "loss_last": loss1,
             "train_ms_per_sample": fs.unet_time(1, 3),
             "probe_iterations_plain": sum(r[0] for r in rows) / n,

@@ -299,6 +299,16 @@ ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* relres_pred);
 /* mean device time in ms of `what`: 0 the prediction (writes q), 1 one
  * training step of batch 1 at learning rate 0 */
 ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms);
+/* data-parallel training across processes (one per GPU): accumulate the
+ * gradients of `samples` stored pairs drawn with `seed` (no update; returns
+ * the loss summed over them), expose the FP32 gradient buffer (device
+ * pointer, num_weights floats, owned by the handle) so the caller can sum it
+ * over the ranks in place, then apply one Adam step with the summed
+ * gradients divided by total_samples (the batch of all ranks). Ranks that
+ * start from the same ws_unet_init seed and the same gain stay identical. */
+ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t seed, double* loss_sum);
+ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* count);
+ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_samples);
 
 #ifdef __cplusplus
 }

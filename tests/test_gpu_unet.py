@@ -114,3 +114,38 @@ def test_trained_network_saves_iterations():
           % (plain, learned, np.mean([r[2] for r in rows]), np.mean([r[3] for r in rows])))
     assert np.mean([r[3] for r in rows]) < np.mean([r[2] for r in rows])
     assert learned < plain
+
+
+def test_data_parallel_pieces():
+    """ws_unet_accumulate / ws_unet_grads / ws_unet_apply: the accumulated
+    gradient of the single stored pair equals ws_unet_grad_pair's, the
+    gradient view shares the library's buffer, and the data-parallel driver
+    runs over a one-rank NCCL group."""
+    import socket
+    import torch
+    import torch.distributed as dist
+    import dp_train
+    fs = _solver(1)
+    fs.unet_set_gain(0.5)
+    g_ref, loss_ref = fs.unet_grad_pair(0)
+    loss = fs.unet_accumulate(1, 3)
+    g = fs.unet_grads()
+    assert g.is_cuda and g.numel() == g_ref.size
+    assert abs(loss - loss_ref) <= 1e-6 * abs(loss_ref)
+    assert _rel(g.cpu().numpy(), g_ref.astype(np.float64)) < 1e-4    # atomics: summation order only
+    w0 = fs.unet_weights()
+    fs.unet_apply(1e-3, 1)
+    w1 = fs.unet_weights()
+    assert np.abs(w1 - w0).max() > 0
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        G = dp_train.agree_gain(fs)
+        assert G > 0
+        L = dp_train.train_data_parallel(fs, steps=3, batch=2, lr=1e-3, seed=4)
+        assert np.isfinite(L) and L > 0
+    finally:
+        dist.destroy_process_group()
+    assert fs.unet_info()["train_steps"] == 4

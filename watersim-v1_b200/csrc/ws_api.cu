@@ -1153,3 +1153,31 @@ extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, doub
   *ms = t / reps;
   return WS_OK;
 }
+
+// ---- data-parallel training: each rank accumulates the gradients of its own
+// samples, the caller sums the FP32 gradient buffer over the ranks (an
+// all-reduce on its communicator), then every rank applies the same step
+extern "C" ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t seed, double* loss_sum) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
+  if (samples < 1) return fail(h, WS_ERR_INVALID, "samples must be positive");
+  WS_TRY(h->net->accumulate(samples, seed, h->stream));
+  double L = 0;
+  WS_TRY(h->net->loss_sum(&L, h->stream));
+  if (loss_sum) *loss_sum = L;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* count) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!device_ptr || !count) return WS_ERR_INVALID;
+  *device_ptr = h->net->grads;
+  *count = h->net->nparams;
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_samples) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (total_samples < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad learning rate or sample count");
+  WS_TRY(h->net->apply(lr, total_samples, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}

@@ -876,30 +876,54 @@ cudaError_t Net::sample_grad(int p, cudaStream_t s) {
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return backward(s);
 }
+// zero the gradients and the loss, then add the gradients of `samples`
+// pairs drawn with a seeded generator (no parameter update)
+cudaError_t Net::accumulate(int samples, uint32_t seed, cudaStream_t s) {
+  int n = std::min(pairsStored, pairCap);
+  if (n <= 0 || samples < 0) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (!(gain > 0)) { if ((e = set_gain_from_pairs(s)) != cudaSuccess) return e; }
+  HostRng rng(seed ? seed : 1u);
+  cudaMemsetAsync(grads, 0, sizeof(float) * nparams, s);
+  cudaMemsetAsync(scal + 2, 0, sizeof(double), s);
+  for (int b = 0; b < samples; b++)
+    if ((e = sample_grad((int)(rng.next() % (uint32_t)n), s)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+// one Adam step with the accumulated gradients divided by `total` samples
+cudaError_t Net::apply(double lr, int total, cudaStream_t s) {
+  if (total < 1) return cudaErrorInvalidValue;
+  adamStep++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  float c1 = 1.f - std::pow(b1, (float)adamStep), c2 = 1.f - std::pow(b2, (float)adamStep);
+  k_adam<<<grid1(nparams, 256), 256, 0, s>>>(params, grads, adm, adv, nparams, (float)lr, b1, b2, 1e-8f, c1, c2,
+                                           1.f / total);
+  cudaError_t e = pack(s);
+  if (e == cudaSuccess) trainSteps++;
+  return e;
+}
+cudaError_t Net::loss_sum(double* out, cudaStream_t s) {
+  cudaError_t e = cudaMemcpyAsync(out, scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
 cudaError_t Net::train(int steps, int batch, double lr, uint32_t seed, double* meanLoss, cudaStream_t s) {
   int n = std::min(pairsStored, pairCap);
   if (n <= 0 || steps < 0 || batch < 1) return cudaErrorInvalidValue;
   cudaError_t e;
   if (!(gain > 0)) { if ((e = set_gain_from_pairs(s)) != cudaSuccess) return e; }
   HostRng rng(seed ? seed : 1u);
-  cudaMemsetAsync(scal + 2, 0, sizeof(double), s);
+  double total = 0;
   for (int it = 0; it < steps; it++) {
-    cudaMemsetAsync(grads, 0, sizeof(float) * nparams, s);
-    for (int b = 0; b < batch; b++)
-      if ((e = sample_grad((int)(rng.next() % (uint32_t)n), s)) != cudaSuccess) return e;
-    adamStep++;
-    const float b1 = 0.9f, b2 = 0.999f;
-    float c1 = 1.f - std::pow(b1, (float)adamStep), c2 = 1.f - std::pow(b2, (float)adamStep);
-    k_adam<<<grid1(nparams, 256), 256, 0, s>>>(params, grads, adm, adv, nparams, (float)lr, b1, b2, 1e-8f, c1, c2,
-                                             1.f / batch);
-    if ((e = pack(s)) != cudaSuccess) return e;
-    trainSteps++;
+    if ((e = accumulate(batch, rng.next() | 1u, s)) != cudaSuccess) return e;
+    if ((e = apply(lr, batch, s)) != cudaSuccess) return e;
+    double L = 0;
+    if ((e = loss_sum(&L, s)) != cudaSuccess) return e;
+    total += L;
   }
-  double L = 0;
-  if ((e = cudaMemcpyAsync(&L, scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-  if (meanLoss) *meanLoss = steps > 0 ? L / ((double)steps * batch) : 0.0;
-  lastLoss = meanLoss ? *meanLoss : 0.0;
+  if (meanLoss) *meanLoss = steps > 0 ? total / ((double)steps * batch) : 0.0;
+  lastLoss = steps > 0 ? total / ((double)steps * batch) : lastLoss;
   return cudaSuccess;
 }
 // network output (un-scaled by G) at every cell of pair p

@@ -82,6 +82,9 @@ class Net {
   cudaError_t collect_pre(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type, cudaStream_t s);
   cudaError_t collect_post(const float* q, cudaStream_t s);
   cudaError_t train(int steps, int batch, double lr, uint32_t seed, double* meanLoss, cudaStream_t s);
+  cudaError_t accumulate(int samples, uint32_t seed, cudaStream_t s);
+  cudaError_t apply(double lr, int total, cudaStream_t s);
+  cudaError_t loss_sum(double* out, cudaStream_t s);
   cudaError_t forward_pair(int p, float* outHost, cudaStream_t s);
   cudaError_t grad_pair(int p, float* gradHost, double* loss, cudaStream_t s);
   static long long layer_weights(int l);

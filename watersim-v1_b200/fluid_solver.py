@@ -122,7 +122,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_residual_noalloc", "ws_upload_state", "ws_download_state",
            "ws_unet_init", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
-           "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time"]
+           "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
+           "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply"]
 
 
 def load_library(path=None):
@@ -164,6 +165,9 @@ def load_library(path=None):
         "ws_unet_forward_pair": [h, i32, vp], "ws_unet_grad_pair": [h, i32, vp, C.POINTER(C.c_double)],
         "ws_unet_probe": [h, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         "ws_unet_time": [h, i32, i32, C.POINTER(C.c_double)],
+        "ws_unet_accumulate": [h, i32, u32, C.POINTER(C.c_double)],
+        "ws_unet_grads": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_unet_apply": [h, d, i32],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -209,6 +213,7 @@ class FluidSolver:
         object.__setattr__(self, "nz", cfg.nz)
         object.__setattr__(self, "dx", cfg.dx)
         object.__setattr__(self, "mode", "sphere")
+        object.__setattr__(self, "device", cfg.device)
         p = WsParams()
         self._check(L.ws_get_params(hh, C.byref(p)))
         object.__setattr__(self, "_p", p)
@@ -407,6 +412,26 @@ class FluidSolver:
         ms = C.c_double()
         self._check(self._L.ws_unet_time(self._h, int(what), int(reps), C.byref(ms)))
         return ms.value
+
+    # data-parallel training pieces (watersim-v1_b200/dp_train.py drives them)
+    def unet_accumulate(self, samples, seed):
+        loss = C.c_double()
+        self._check(self._L.ws_unet_accumulate(self._h, int(samples), int(seed) & 0xffffffff, C.byref(loss)))
+        return loss.value
+
+    def unet_grads(self):
+        """The FP32 gradient buffer as a CUDA tensor sharing the library's memory."""
+        import torch
+        ptr, n = C.c_void_p(), C.c_int64()
+        self._check(self._L.ws_unet_grads(self._h, C.byref(ptr), C.byref(n)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n.value,), "typestr": "<f4", "data": (ptr.value, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device="cuda:%d" % self.device)
+
+    def unet_apply(self, lr, total_samples):
+        self._check(self._L.ws_unet_apply(self._h, float(lr), int(total_samples)))
 
     def set_nparticles(self, n):
         self._check(self._L.ws_set_nparticles(self._h, int(n)))
