@@ -101,11 +101,21 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// queue the copies of one 16-channel slice of the halo of sub-tile (X0, Y0, Z0)
+// queue the copies of one 16-channel slice of the halo of sub-tile (X0, Y0, Z0).
+// The activity of the (up to) 3x3x3 tiles the halo touches is read once into
+// shared memory, so no copy waits on a global load of its own.
 template <int COUT>
-__device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, int Z0, int kk, uint32_t hbase) {
+__device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, int Z0, int kk, uint32_t hbase,
+                                           uint8_t* s_act) {
   using S = ConvShape<COUT>;
   constexpr int HX = S::HX, HY = S::HY, HV = S::HV, KSTR = S::KSTR;
+  const int tx0 = X0 / kTX - 1, ty0 = Y0 / kTY - 1, tz0 = (Z0 + kTZ - 1) / kTZ - 1;   // tile of the halo's low corner
+  if (threadIdx.x < 27) {
+    const int t = threadIdx.x, tx = tx0 + t % 3, ty = ty0 + (t / 3) % 3, tz = tz0 + t / 9;
+    s_act[t] = (tx >= 0 && ty >= 0 && tz >= 0 && tx < a.ntx && ty < a.nty && tz < a.ntz)
+                   ? a.active[(tz * a.nty + ty) * a.ntx + tx] : (uint8_t)0;
+  }
+  __syncthreads();
   const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
   for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
     const int j = i & 1, hv = i >> 1;
@@ -114,7 +124,7 @@ __device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, in
     const bf16* p = a.src1 ? a.src1 : a.src0;             // any valid address when nothing is read
     uint32_t n = 0;
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
-        a.active[((gz / kTZ) * a.nty + gy / kTY) * a.ntx + gx / kTX]) {
+        s_act[((gz / kTZ - tz0) * 3 + (gy / kTY - ty0)) * 3 + (gx / kTX - tx0)]) {
       const int c = kk * 16 + j * 8;
       if (c < a.c0) {
         p = a.up0 ? a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c
@@ -146,6 +156,7 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
+  __shared__ uint8_t s_act[27];
 
   constexpr int sub = kTZ / ZT;
   const int nItems = *a.nTiles * sub;
@@ -176,7 +187,7 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   };
   int X0, Y0, Z0;
   origin(blockIdx.x, X0, Y0, Z0);
-  stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase);
+  stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase, s_act);
   stage_weights<COUT>(a, 0, wbase);
   for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
     for (int kk = 0; kk < nslices; kk++) {
@@ -208,7 +219,7 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
       pending = false;
       phase ^= 1u;
       if (kk + 1 < nslices) {
-        stage_halo<COUT>(a, X0, Y0, Z0, kk + 1, hbase);
+        stage_halo<COUT>(a, X0, Y0, Z0, kk + 1, hbase, s_act);
         stage_weights<COUT>(a, kk + 1, wbase);
       }
     }
@@ -218,7 +229,7 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
     const int next = item + gridDim.x;
     if (next < nItems) {
       origin(next, X0, Y0, Z0);
-      stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase);
+      stage_halo<COUT>(a, X0, Y0, Z0, 0, hbase, s_act);
       if (!wres) stage_weights<COUT>(a, 0, wbase);
     }
     fence_after();
