@@ -335,123 +335,6 @@ __global__ void k_head_train(Level L, const int* tiles, const int* count, const 
   if (threadIdx.x == 32) { double s = 0; for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sl[k]; if (s != 0) atomicAdd(loss, s / max(*nFluid, 1)); }
 }
 
-// ------------------------------------------------------------ weight gradient
-// dW[co][ci][t] += sum_v X(v + off_t)[ci] dZ(v)[co] and db[co] += sum_v dZ(v)[co]
-// over the voxels of active tiles. CTA = (active tile, 16-channel input
-// slice, 16-channel output group); 216 threads, each owning two
-// (tap, 4 inputs, 4 outputs) blocks of 16 FP32 accumulators. The input
-// halo slice is staged once per CTA, the output gradient one plane at a time.
-struct DwArgs {
-  int nx, ny, nz, ntx, nty, ntz;
-  const int* tiles; const int* nTiles; const uint8_t* active;
-  const bf16* src0; int c0; int up0; const bf16* src1; int c1;
-  const bf16* dz; int cout;
-  float* dw; float* db;
-};
-constexpr int kDwThreads = 216;
-__global__ void __launch_bounds__(kDwThreads) k_dw(DwArgs a) {
-  constexpr int HX = kTX + 2, HY = kTY + 2, HZ = kTZ + 2, HV = HX * HY * HZ;
-  extern __shared__ __align__(16) unsigned char dsm[];
-  bf16* halo = reinterpret_cast<bf16*>(dsm);                                // [HV][16]
-  float* pl = reinterpret_cast<float*>(dsm + HV * 32);                      // [128][16]
-  const int cin = a.c0 + a.c1, nsl = cin >> 4, nog = a.cout >> 4;
-  const int nItems = *a.nTiles * nsl * nog;
-  for (int item = blockIdx.x; item < nItems; item += gridDim.x) {
-  int b = item;
-  const int og = b % nog; b /= nog;
-  const int kk = b % nsl; b /= nsl;
-  const int tile = a.tiles[b];
-  __syncthreads();                                   // the previous item is done with the halo
-  const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
-  const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ;
-  for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
-    const int j = i & 1, hv = i >> 1;
-    const int hx = hv % HX, t2 = hv / HX, hy = t2 % HY, hz = t2 / HY;
-    const int gx = X0 - 1 + hx, gy = Y0 - 1 + hy, gz = Z0 - 1 + hz;
-    uint4 val = make_uint4(0u, 0u, 0u, 0u);
-    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
-        a.active[((gz / kTZ) * a.nty + gy / kTY) * a.ntx + gx / kTX]) {
-      const int c = kk * 16 + j * 8;
-      const bf16* p;
-      if (c < a.c0) {
-        if (a.up0) {
-          const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
-          p = a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c;
-        } else {
-          p = a.src0 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c0 + c;
-        }
-      } else {
-        p = a.src1 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c1 + (c - a.c0);
-      }
-      val = __ldg(reinterpret_cast<const uint4*>(p));
-    }
-    reinterpret_cast<uint4*>(halo)[hv * 2 + j] = val;
-  }
-  // two blocks per thread: g = threadIdx.x and threadIdx.x + 216 over 432 = 27 taps x 4 x 4
-  int gt[2], gci[2], gco[2], goff[2];
-#pragma unroll
-  for (int r = 0; r < 2; r++) {
-    int g = threadIdx.x + r * kDwThreads;
-    gt[r] = g >> 4; gci[r] = ((g >> 2) & 3) * 4; gco[r] = (g & 3) * 4;
-    int t = gt[r], dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-    goff[r] = (dz * HY + dy) * HX + dx;
-  }
-  float acc[2][16];
-#pragma unroll
-  for (int r = 0; r < 2; r++)
-#pragma unroll
-    for (int e = 0; e < 16; e++) acc[r][e] = 0.f;
-  float bsum = 0.f;
-  for (int z = 0; z < kTZ; z++) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < 128 * 2; i += blockDim.x) {
-      const int m = i >> 1, j = i & 1;
-      const int gx = X0 + (m & 7), gy = Y0 + (m >> 3), gz = Z0 + z;
-      float f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (gx < a.nx && gy < a.ny && gz < a.nz) {
-        uint4 u = __ldg(reinterpret_cast<const uint4*>(a.dz + (((size_t)gz * a.ny + gy) * a.nx + gx) * a.cout + og * 16 + j * 8));
-        const bf16* bb = reinterpret_cast<const bf16*>(&u);
-#pragma unroll
-        for (int e = 0; e < 8; e++) f[e] = __bfloat162float(bb[e]);
-      }
-#pragma unroll
-      for (int e = 0; e < 8; e++) pl[m * 16 + j * 8 + e] = f[e];
-    }
-    __syncthreads();
-    if (kk == 0 && threadIdx.x < 16)
-      for (int m = 0; m < 128; m++) bsum += pl[m * 16 + threadIdx.x];
-#pragma unroll
-    for (int r = 0; r < 2; r++) {
-      const int base = z * HY * HX + goff[r];
-#pragma unroll 4
-      for (int m = 0; m < 128; m++) {
-        const int hv = base + (m >> 3) * HX + (m & 7);
-        const uint2 xr = *reinterpret_cast<const uint2*>(halo + hv * 16 + gci[r]);
-        const __nv_bfloat162* x2 = reinterpret_cast<const __nv_bfloat162*>(&xr);
-        const float2 xa = __bfloat1622float2(x2[0]), xb = __bfloat1622float2(x2[1]);
-        const float4 d = *reinterpret_cast<const float4*>(pl + m * 16 + gco[r]);
-        const float xv[4] = { xa.x, xa.y, xb.x, xb.y }, dv[4] = { d.x, d.y, d.z, d.w };
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[r][p * 4 + q] = fmaf(xv[p], dv[q], acc[r][p * 4 + q]);
-      }
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < 2; r++)
-#pragma unroll
-    for (int p = 0; p < 4; p++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int ci = kk * 16 + gci[r] + p, co = og * 16 + gco[r] + q;
-        atomicAdd(a.dw + ((size_t)co * cin + ci) * 27 + gt[r], acc[r][p * 4 + q]);
-      }
-  if (kk == 0 && threadIdx.x < 16) atomicAdd(a.db + og * 16 + threadIdx.x, bsum);
-  }
-}
-static size_t dw_smem_bytes() { return (size_t)(kTX + 2) * (kTY + 2) * (kTZ + 2) * 32 + 128 * 16 * 4; }
-
 // ------------------------------------------------------------ weights
 // FP32 master W[co][ci][27] -> the packed BF16 operand of the forward conv,
 // [ci/16][27][2][co][8], and of the backward-data conv (cin' = co, cout' =
@@ -680,17 +563,12 @@ cudaError_t Net::conv_bwd(int l, const bf16* dz, const bf16* mask, bf16* out0, b
 cudaError_t Net::dw(int l, const bf16* src0, const bf16* src1, const bf16* dz, cudaStream_t s) {
   const LayerSpec& S = kLayers[l];
   const Level& L = lv[S.level];
-  DwArgs a{};
+  ConvArgs a{};
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.ntx = L.ntx; a.nty = L.nty; a.ntz = L.ntz;
   a.tiles = tiles[S.level]; a.nTiles = counts + S.level; a.active = act[S.level];
-  a.src0 = src0; a.c0 = S.c0; a.up0 = S.c0 > 0; a.src1 = src1; a.c1 = S.c1;
-  a.dz = dz; a.cout = S.cout; a.dw = grads + woff[l]; a.db = grads + boff[l];
+  a.src0 = src0; a.c0 = S.c0; a.up0 = S.c0 > 0; a.src1 = src1; a.c1 = S.c1; a.err = err;
   const int cin = S.c0 + S.c1;
-  static bool attr = false;
-  if (!attr) { cudaFuncSetAttribute(k_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dw_smem_bytes()); attr = true; }
-  const long long items = (long long)L.ntiles * (cin / 16) * (S.cout / 16);
-  k_dw<<<(unsigned)std::min<long long>(items, 148LL * 3), kDwThreads, dw_smem_bytes(), s>>>(a);
-  return cudaGetLastError();
+  return launch_dw_tc(a, dz, S.cout, grads + woff[l], grads + boff[l], L.ntiles * (cin / 16), s);
 }
 
 cudaError_t Net::pool(int fineLevel, const bf16* fine, bf16* coarse, int ch, cudaStream_t s) {

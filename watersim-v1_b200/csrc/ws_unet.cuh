@@ -52,6 +52,10 @@ cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t
 size_t conv3_smem_bytes(int cout);
 int conv3_zt(int cout);
 cudaError_t conv3_init();
+// tcgen05 weight and bias gradients of one convolution (ws_unet_conv.cu);
+// src describes the convolution's input as for launch_conv3, cout <= 128
+cudaError_t launch_dw_tc(const ConvArgs& src, const bf16* dz, int cout, float* dw, float* db, int maxItems,
+                         cudaStream_t s);
 
 }  // namespace unet
 

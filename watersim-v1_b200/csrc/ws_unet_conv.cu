@@ -198,16 +198,17 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
         fence_after();
         // taps outer, planes inner: consecutive MMAs go to different
         // accumulators, so ZT of them are in flight instead of a chain of
-        // read-modify-writes of one accumulator
+        // read-modify-writes of one accumulator. Descriptors are base
+        // descriptors plus 16-byte offsets in the start-address field.
+        const uint64_t ad0 = smem_desc(hbase, KSTR, HX * 16), bd0 = smem_desc(wbase, COUT * 16, 128);
 #pragma unroll 1
         for (int t = 0; t < 27; t++) {
           const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint64_t bd = smem_desc(wbase + (uint32_t)(t * 2 * COUT * 16), COUT * 16, 128);
+          const uint64_t bd = bd0 + (uint64_t)(t * 2 * COUT);
+          const uint64_t at = ad0 + (uint64_t)((dz * HY + dy) * HX + dx);
 #pragma unroll
-          for (int z = 0; z < ZT; z++) {
-            const uint64_t ad = smem_desc(hbase + (uint32_t)((((z + dz) * HY + dy) * HX + dx) * 16), KSTR, HX * 16);
-            mma_bf16(tmem + (uint32_t)(z * COUT), ad, bd, idesc, (kk | t) != 0);
-          }
+          for (int z = 0; z < ZT; z++)
+            mma_bf16(tmem + (uint32_t)(z * COUT), at + (uint64_t)(z * HY * HX), bd, idesc, (kk | t) != 0);
         }
         mma_commit(&mbar);
       }
@@ -281,6 +282,140 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"((uint32_t)S::TCOLS) : "memory");
 }
 
+// ------------------------------------------------------------ weight gradient
+// dW[co][ci][t] += sum_v X(v + off_t)[ci] dZ(v)[co] over the voxels of
+// active tiles, on the tensor cores. One CTA per (active tile, 16-channel
+// input slice), persistent, one per SM. Per tap t the GEMM is D[co][ci] =
+// sum over voxels: A = dZ (M = 64 rows, cout <= 64 real), B = the input halo
+// shifted by the tap (N = 16 channels), K = 16 voxels (two x-rows of a plane)
+// per MMA. Both operands are MN-major: a core matrix is 8 channels (16
+// bytes) by 8 consecutive voxels; K groups are 128 bytes apart in the staged
+// dZ and one halo row (160 bytes) apart in the halo. The whole tile's dZ and
+// halo are staged once; the 8 planes x 8 K steps x 27 taps = 1728 MMAs are
+// issued back to back (taps innermost: 27 independent accumulators of 16
+// columns) with descriptors formed by adding 16-byte offsets to two base
+// descriptors, and drained once per item.
+struct DwTcArgs { ConvArgs src; const bf16* dz; int cout; float* dw; float* db; };
+constexpr int kDzPlane = 128 * 16;                // bytes of one plane of one 8-channel chunk of dZ
+constexpr int kDzChunk = kTZ * kDzPlane;          // one 8-channel chunk of the tile's dZ
+constexpr int kDwTcSmem = 2 * ConvShape<16>::KSTR + 8 * kDzChunk;
+static_assert(kDwTcSmem + 1024 <= 232448, "halo and dZ of a tile fit one CTA's shared memory");
+// instruction descriptor: D f32, A and B bf16, both MN-major, M = 64, N = 16.
+// With M = 64 the accumulator rows 16q..16q+15 sit in tensor-memory lanes
+// 32q..32q+15 (the lower half of each 32-lane subpartition).
+constexpr uint32_t kIdescDw = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                              ((uint32_t)(16 >> 3) << 17) | ((uint32_t)(64 >> 4) << 24);
+
+__global__ void __launch_bounds__(256, 1) k_dw_tc(DwTcArgs A) {
+  const ConvArgs& a = A.src;
+  using S = ConvShape<16>;                          // ZT = 8: the whole tile's halo of one slice
+  constexpr int HX = S::HX, HY = S::HY, KSTR = S::KSTR;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_abort;
+  __shared__ uint8_t s_act[27];
+  const int cin = a.c0 + a.c1, nsl = cin >> 4, cout = A.cout;
+  const int nItems = *a.nTiles * nsl;
+  if ((int)blockIdx.x >= nItems) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t hbase = smem_u32(smem), zbase = hbase + 2 * KSTR;
+  unsigned char* zbuf = smem + 2 * KSTR;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(&s_tmem)), "r"(512u) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) { mbar_init(&mbar, 1); s_abort = 0; }
+  // rows co >= cout of the A operand read zeros
+  for (int i = threadIdx.x; i < 8 * kDzChunk / 16; i += blockDim.x) reinterpret_cast<uint4*>(zbuf)[i] = make_uint4(0u, 0u, 0u, 0u);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint64_t adesc0 = smem_desc(zbase, 128, kDzChunk), bdesc0 = smem_desc(hbase, HX * 16, KSTR);
+  uint32_t phase = 0;
+  bool pending = false;
+  for (int item = blockIdx.x; item < nItems && !s_abort; item += gridDim.x) {
+    const int tile = a.tiles[item / nsl], kk = item % nsl;
+    const int tx = tile % a.ntx, ty = (tile / a.ntx) % a.nty, tz = tile / (a.ntx * a.nty);
+    const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ;
+    stage_halo<16>(a, X0, Y0, Z0, kk, hbase, s_act);
+    for (int i = threadIdx.x; i < (cout >> 3) * kTZ * 128; i += blockDim.x) {
+      const int c = i / (kTZ * 128), r = i - c * (kTZ * 128), z = r >> 7, m = r & 127;
+      const int gx = X0 + (m & 7), gy = Y0 + (m >> 3), gz = Z0 + z;
+      const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
+      const bf16* src = in ? A.dz + (((size_t)gz * a.ny + gy) * a.nx + gx) * cout + c * 8 : A.dz;
+      cp_async16(zbase + (uint32_t)(c * kDzChunk + z * kDzPlane + m * 16), src, in ? 16u : 0u);
+    }
+    cp_async_wait_all();
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      fence_after();
+#pragma unroll 1
+      for (int z = 0; z < kTZ; z++) {
+#pragma unroll 1
+        for (int ks = 0; ks < 8; ks++) {
+          const uint64_t ad = adesc0 + (uint64_t)((z * kDzPlane + ks * 256) >> 4);
+          const uint32_t rowb = (uint32_t)(z * HY + 2 * ks) * HX;       // halo row of tap (0, 0, 0), 16-byte units
+#pragma unroll
+          for (int t = 0; t < 27; t++) {
+            const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+            const uint64_t bd = bdesc0 + (uint64_t)(rowb + (uint32_t)((dz * HY + dy) * HX + dx));
+            mma_bf16(tmem + (uint32_t)(t * 16), ad, bd, kIdescDw, (z | ks) != 0);
+          }
+        }
+      }
+      mma_commit(&mbar);
+    }
+    pending = true;
+    float bsum = 0.f;                                // bias gradient while the MMAs run
+    if (kk == 0 && (int)threadIdx.x < cout) {
+      const bf16* col = reinterpret_cast<const bf16*>(zbuf + (threadIdx.x >> 3) * kDzChunk) + (threadIdx.x & 7);
+      for (int m = 0; m < kTZ * 128; m++) bsum += __bfloat162float(col[m * 8]);
+    }
+    const bool ok = mbar_wait(&mbar, phase);
+    if (!ok) { s_abort = 1; atomicOr(a.err, WS_DERR_TIMEOUT); }
+    __syncthreads();
+    if (s_abort) break;
+    pending = false;
+    phase ^= 1u;
+    fence_after();
+    {
+      const int q = warp & 3, co = lane < 16 ? q * 16 + lane : 1 << 20;   // accumulator row of this lane
+      for (int t = warp >> 2; t < 27; t += 2) {
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(t * 16), r);
+        if (co < cout) {
+#pragma unroll
+          for (int i = 0; i < 16; i++)
+            atomicAdd(A.dw + ((size_t)co * cin + kk * 16 + i) * 27 + t, __uint_as_float(r[i]));
+        }
+      }
+    }
+    if (kk == 0 && (int)threadIdx.x < cout) atomicAdd(A.db + threadIdx.x, bsum);
+    fence_before();
+    __syncthreads();                                 // accumulators and staged operands free for the next item
+  }
+  if (s_abort && pending) mbar_wait(&mbar, phase);
+  cp_async_wait_all();
+  fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(512u) : "memory");
+}
+cudaError_t launch_dw_tc(const ConvArgs& src, const bf16* dz, int cout, float* dw, float* db, int maxItems,
+                         cudaStream_t s) {
+  if (((src.c0 + src.c1) & 15) || (cout & 7) || cout > 64) return cudaErrorInvalidValue;
+  static int smCount = 0;
+  if (!smCount) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev); }
+  DwTcArgs A{src, dz, cout, dw, db};
+  const unsigned grid = (unsigned)std::min(maxItems, smCount);     // one CTA per SM: 512 TMEM columns each
+  if (grid == 0) return cudaSuccess;
+  k_dw_tc<<<grid, 256, kDwTcSmem, s>>>(A);
+  return cudaGetLastError();
+}
+
 template <int COUT> static cudaError_t set_smem() {
   return cudaFuncSetAttribute(k_conv3<COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ConvShape<COUT>::SMEM);
 }
@@ -290,7 +425,9 @@ cudaError_t conv3_init() {
   if ((e = set_smem<32>()) != cudaSuccess) return e;
   if ((e = set_smem<48>()) != cudaSuccess) return e;
   if ((e = set_smem<64>()) != cudaSuccess) return e;
-  return set_smem<96>();
+  if ((e = set_smem<96>()) != cudaSuccess) return e;
+  // the weight-gradient kernel holds more than half an SM's shared memory: one CTA per SM
+  return cudaFuncSetAttribute(k_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDwTcSmem);
 }
 int conv3_zt(int cout) {
   switch (cout) {
