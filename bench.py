@@ -44,7 +44,12 @@ for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-WORKLOAD = dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000)
+WORKLOADS = {
+    "planet128": dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000),
+    # the large planet: 256^3, radius 110, ocean 12 deep, ~16M particles (plain arm only)
+    "planet256": dict(name="planet256", n=256, R=110.0, depth=12.0, seed=20260114, particles=16000000),
+}
+WORKLOAD = WORKLOADS["planet128"]
 PARAMS = dict(pic=0.05, omega=1.7, maxSpeed=3.2, cfl=3.0, viscosity=5e-4, thermalOn=0,
               sorTol=1e-5, sorCheckEvery=10, sorMaxIters=5000, pressureIters=40)
 DT = 0.01
@@ -113,7 +118,8 @@ def reduce_max(value, device):
 
 
 def make_solver(device, rank=0):
-    """The 128^3 planet through the library's own terrain generator and fill."""
+    """The bench planet through the library's own terrain generator and fill.
+    Replicas (rank > 0) draw their stir kicks from their own seed."""
     from fluid_solver import FluidSolver
     W = WORKLOAD
     coreR = W["R"] - W["depth"]
@@ -123,6 +129,8 @@ def make_solver(device, rank=0):
     fs.resetWater(W["depth"])
     fs.set_params(**PARAMS)
     fs.set_scalars(gRamp=1.5)
+    if rank > 0:
+        fs.set_scalars(stirS=(0x2545f491 + 7919 * rank) & 0xffffffff)
     return fs
 
 
@@ -223,7 +231,8 @@ def run_ours(args, rank, world, local_rank):
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)",
-               "config": {"workload": "planet128: 128^3 MAC grid, R=52, depth 8, %d particles" % nP,
+               "config": {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles"
+                                      % (WORKLOAD["name"], WORKLOAD["n"], WORKLOAD["R"], WORKLOAD["depth"], nP),
                           "particles": nP, "parallelism": "replicas x%d" % world,
                           "arm": "learned warm start" if learned else "plain SOR",
                           "sor": "red-black to 1e-5 (check every 10), mean iterations %.1f"
@@ -375,8 +384,8 @@ def cpu_baseline(fs, seconds=20.0):
         if el >= seconds or done >= 20:
             break
     return {"value": done / el, "unit": "substeps/s", "cores": 1, "kind": "port",
-            "sample": "%d whole substep(s) of the 128^3 planet (%d particles) in %.1f s, oracle "
-                      "(C restatement of js/solver.js, lexicographic SOR) on 1 host core" % (done, nP, el)}
+            "sample": ("%d whole substep(s) of the %d^3 planet (%d particles) in %.1f s, oracle "
+                       "(C restatement of js/solver.js, lexicographic SOR) on 1 host core" % (done, W["n"], nP, el))}
 
 
 def run_reference(args, rank, world):
@@ -405,13 +414,14 @@ def run_reference(args, rank, world):
         count += 1
     el = time.perf_counter() - t0
     v = steps / el
-    sample = ("%d substep(s) of the 128^3 planet (%d particles) after %d warm-up; C restatement of "
-              "js/solver.js (reference order), 1 core — no JavaScript engine on the host" % (steps, nP, warm))
+    sample = ("%d substep(s) of the %d^3 planet (%d particles) after %d warm-up; C restatement of "
+              "js/solver.js (reference order), 1 core — no JavaScript engine on the host" % (steps, W["n"], nP, warm))
     return {"metric": METRIC, "value": v, "unit": "substeps/s", "n_gpus": world, "steps": steps,
             "warmup": warm, "ms_per_step": 1000 * el / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic / f32 storage",
             "data": "synthetic seeded planet", "impl": "reference",
-            "config": {"workload": "planet128: 128^3 MAC grid, R=52, depth 8, %d particles" % nP},
+            "config": {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles"
+                                   % (W["name"], W["n"], W["R"], W["depth"], nP)},
             "cpu_baseline": {"value": v, "unit": "substeps/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -427,7 +437,15 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="plain SOR arm only")
     ap.add_argument("--pairs", type=int, default=2000, help="training pairs recorded from plain solves")
     ap.add_argument("--train-steps", type=int, default=1000, help="Adam steps of batch 4")
+    ap.add_argument("--workload", default="planet128", choices=sorted(WORKLOADS),
+                    help="planet256 (256^3, ~16M particles) runs the plain arm only")
     args = ap.parse_args()
+    global WORKLOAD, METRIC_PLAIN
+    WORKLOAD = WORKLOADS[args.workload]
+    if args.workload != "planet128":
+        args.no_learned = True
+        METRIC_PLAIN = ("substeps/s @%d^3/%dM particles (plain red-black SOR to 1e-5 relative divergence residual)"
+                        % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000))
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
