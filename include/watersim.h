@@ -170,6 +170,16 @@ typedef struct {
 ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a);
 ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a);
 
+/* ---- snapshot / restore of the whole solver state (resume, or shipping
+ *      state between processes). A versioned host blob: knobs, scalars and
+ *      RNG streams, the particle fields (nP each), the pressure warm start q
+ *      and the terrain; grid fields are rebuilt by the next substep. Call with
+ *      buf == NULL to get the size. Restore needs a handle of the same grid
+ *      and a capacity of at least the stored nP. No reference counterpart
+ *      beyond the typed arrays themselves (js/solver.js:94-129). */
+ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int64_t* size);
+ws_status ws_restore(ws_handle* h, const void* buf, int64_t size);
+
 /* ---- drivers: step(dtFrame) == _stepSync (js/solver.js:2663-2700) and
  *      _substep(dt) (js/solver.js:2568-2624) */
 ws_status ws_step(ws_handle* h, double dtFrame);
@@ -309,6 +319,10 @@ ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms);
 ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t seed, double* loss_sum);
 ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* count);
 ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_samples);
+/* the network's FP32 weights, output gain and Adam state as a host blob
+ * (buf == NULL: size query), and back (same layout; ws_unet_init first) */
+ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int64_t* size);
+ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size);
 
 #ifdef __cplusplus
 }

@@ -1181,3 +1181,144 @@ extern "C" ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_sample
   WS_TRY(cudaStreamSynchronize(h->stream));
   return WS_OK;
 }
+
+// ------------------------------------------------------------ snapshot / restore
+// A self-describing host blob of the whole solver state: header, knobs,
+// scalars (RNG streams included), the 16 particle fields (nP each), the
+// pressure q (the next solve's warm start) and the terrain. Grid fields are
+// rebuilt from the particles by the next substep, so they are not stored.
+namespace {
+constexpr char kSnapMagic[8] = { 'W', 'S', 'S', 'N', 'A', 'P', '0', '1' };
+struct SnapHeader {
+  char magic[8];
+  uint32_t version, headerBytes;
+  int32_t nx, ny, nz, nP, terrainN, pad;
+  double dx;
+  int64_t totalBytes;
+  double Rsl, Rlo, Rhi, landFrac, dv;
+};
+int64_t snap_bytes(const ws_handle* h, int terrainN) {
+  const int64_t nP = h->S.nP, N = h->d.nCells, n3 = (int64_t)terrainN * terrainN * terrainN;
+  return (int64_t)sizeof(SnapHeader) + (int64_t)sizeof(ws_params) + (int64_t)sizeof(ws_scalars) +
+         nP * (13 * 4 + 3) + N * 4 + n3 * 5;
+}
+}  // namespace
+
+extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
+  if (!h || !size) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  const int tn = h->hasTerrain ? h->hostTerrain.n : 0;
+  const int64_t need = snap_bytes(h, tn);
+  *size = need;
+  if (!buf) return WS_OK;                              // size query
+  if (capacity < need) return fail(h, WS_ERR_RANGE, "snapshot buffer too small");
+  unsigned char* p = (unsigned char*)buf;
+  SnapHeader hd{};
+  std::memcpy(hd.magic, kSnapMagic, 8);
+  hd.version = 1; hd.headerBytes = sizeof(SnapHeader);
+  hd.nx = h->d.nx; hd.ny = h->d.ny; hd.nz = h->d.nz; hd.nP = h->S.nP; hd.terrainN = tn; hd.dx = h->d.dx;
+  hd.totalBytes = need;
+  if (tn) { const auto& T = h->hostTerrain; hd.Rsl = T.Rsl; hd.Rlo = T.Rlo; hd.Rhi = T.Rhi; hd.landFrac = T.landFrac; hd.dv = T.dv; }
+  std::memcpy(p, &hd, sizeof hd); p += sizeof hd;
+  std::memcpy(p, &h->P, sizeof(ws_params)); p += sizeof(ws_params);
+  std::memcpy(p, &h->S, sizeof(ws_scalars)); p += sizeof(ws_scalars);
+  const int64_t nP = h->S.nP;
+  for (int f = WS_F_PX; f <= WS_F_PDEPTH; f++) {
+    FieldRef r; field_ref(h, (ws_field)f, r);
+    WS_TRY(cudaMemcpyAsync(p, r.ptr, (size_t)(nP * r.elem), cudaMemcpyDeviceToHost, h->stream));
+    p += nP * r.elem;
+  }
+  WS_TRY(cudaMemcpyAsync(p, h->q, sizeof(float) * (size_t)h->d.nCells, cudaMemcpyDeviceToHost, h->stream));
+  p += 4 * h->d.nCells;
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  if (tn) {
+    const auto& T = h->hostTerrain;
+    const size_t n3 = (size_t)tn * tn * tn;
+    std::memcpy(p, T.solid.data(), n3); p += n3;
+    std::memcpy(p, T.R.data(), 4 * n3); p += 4 * n3;
+  }
+  return WS_OK;
+}
+
+extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
+  if (!h || !buf) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  if (size < (int64_t)sizeof(SnapHeader)) return fail(h, WS_ERR_INVALID, "not a snapshot");
+  SnapHeader hd;
+  std::memcpy(&hd, buf, sizeof hd);
+  if (std::memcmp(hd.magic, kSnapMagic, 8) != 0 || hd.version != 1 || hd.headerBytes != sizeof(SnapHeader))
+    return fail(h, WS_ERR_INVALID, "not a version-1 snapshot");
+  if (hd.nx != h->d.nx || hd.ny != h->d.ny || hd.nz != h->d.nz || hd.dx != h->d.dx)
+    return fail(h, WS_ERR_INVALID, "snapshot grid differs from this handle's");
+  if (hd.nP < 0 || hd.nP > h->capacity) return fail(h, WS_ERR_RANGE, "snapshot holds more particles than the capacity");
+  if (hd.terrainN < 0 || hd.terrainN > 4096) return fail(h, WS_ERR_INVALID, "bad terrain size");
+  ws_scalars S;
+  std::memcpy(&S, (const unsigned char*)buf + sizeof hd + sizeof(ws_params), sizeof S);
+  const int64_t nP = hd.nP, N = h->d.nCells, n3 = (int64_t)hd.terrainN * hd.terrainN * hd.terrainN;
+  const int64_t need = (int64_t)sizeof hd + (int64_t)sizeof(ws_params) + (int64_t)sizeof(ws_scalars) +
+                       nP * (13 * 4 + 3) + N * 4 + n3 * 5;
+  if (size != need || hd.totalBytes != need || S.nP != hd.nP) return fail(h, WS_ERR_INVALID, "snapshot size mismatch");
+  const unsigned char* p = (const unsigned char*)buf + sizeof hd;
+  const unsigned char* fields = p + sizeof(ws_params) + sizeof(ws_scalars);
+  const unsigned char* qp = fields + nP * (13 * 4 + 3);
+  if (hd.terrainN) {
+    ws_terrain t;
+    t.n = hd.terrainN; t.dv = hd.dv; t.Rsl = hd.Rsl; t.Rlo = hd.Rlo; t.Rhi = hd.Rhi; t.landFrac = hd.landFrac;
+    t.solid = qp + 4 * N;
+    t.R = (const float*)(qp + 4 * N + n3);
+    if ((s = ws_upload_terrain(h, &t))) return s;
+  }
+  if ((s = ws_set_params(h, (const ws_params*)p))) return s;
+  if ((s = ws_set_scalars(h, &S))) return s;
+  ws_host_arrays a{};
+  a.count = nP;
+  const unsigned char* f = fields;
+  for (int k = WS_F_PX; k <= WS_F_PDEPTH; k++) {
+    a.field[k] = const_cast<unsigned char*>(f);
+    f += nP * (k <= WS_F_PPH ? 4 : 1);
+  }
+  if ((s = ws_upload_state(h, &a))) return s;
+  WS_TRY(cudaMemcpyAsync(h->q, qp, sizeof(float) * (size_t)N, cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}
+
+// network blob: header, gain, Adam step count, then params, Adam m and v (FP32)
+extern "C" ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!size) return WS_ERR_INVALID;
+  const int64_t n = h->net->nparams, need = 8 + 8 + 8 + 8 + 3 * 4 * n;
+  *size = need;
+  if (!buf) return WS_OK;
+  if (capacity < need) return fail(h, WS_ERR_RANGE, "network buffer too small");
+  unsigned char* p = (unsigned char*)buf;
+  std::memcpy(p, "WSUNET01", 8); p += 8;
+  std::memcpy(p, &n, 8); p += 8;
+  std::memcpy(p, &h->net->gain, 8); p += 8;
+  const int64_t steps = h->net->adamStep;
+  std::memcpy(p, &steps, 8); p += 8;
+  WS_TRY(cudaMemcpy(p, h->net->params, 4 * n, cudaMemcpyDeviceToHost)); p += 4 * n;
+  WS_TRY(cudaMemcpy(p, h->net->adm, 4 * n, cudaMemcpyDeviceToHost)); p += 4 * n;
+  WS_TRY(cudaMemcpy(p, h->net->adv, 4 * n, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
+  ws_status s = net_ready(h); if (s) return s;
+  if (!buf) return WS_ERR_INVALID;
+  const int64_t n = h->net->nparams;
+  if (size != 32 + 12 * n || std::memcmp(buf, "WSUNET01", 8) != 0) return fail(h, WS_ERR_INVALID, "not a network of this layout");
+  const unsigned char* p = (const unsigned char*)buf + 8;
+  int64_t n2, steps; double gain;
+  std::memcpy(&n2, p, 8); std::memcpy(&gain, p + 8, 8); std::memcpy(&steps, p + 16, 8);
+  if (n2 != n) return fail(h, WS_ERR_INVALID, "parameter count differs");
+  p += 24;
+  WS_TRY(cudaMemcpy(h->net->adm, p + 4 * n, 4 * n, cudaMemcpyHostToDevice));
+  WS_TRY(cudaMemcpy(h->net->adv, p + 8 * n, 4 * n, cudaMemcpyHostToDevice));
+  WS_TRY(h->net->set_weights((const float*)p, h->stream));
+  h->net->adamStep = (int)steps;
+  if (gain > 0) WS_TRY(h->net->set_gain(gain, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}

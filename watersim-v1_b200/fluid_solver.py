@@ -123,7 +123,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_init", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
            "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
-           "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply"]
+           "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
+           "ws_unet_save", "ws_unet_load"]
 
 
 def load_library(path=None):
@@ -168,6 +169,8 @@ def load_library(path=None):
         "ws_unet_accumulate": [h, i32, u32, C.POINTER(C.c_double)],
         "ws_unet_grads": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
         "ws_unet_apply": [h, d, i32],
+        "ws_snapshot": [h, vp, i64, C.POINTER(C.c_int64)], "ws_restore": [h, vp, i64],
+        "ws_unet_save": [h, vp, i64, C.POINTER(C.c_int64)], "ws_unet_load": [h, vp, i64],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -432,6 +435,29 @@ class FluidSolver:
 
     def unet_apply(self, lr, total_samples):
         self._check(self._L.ws_unet_apply(self._h, float(lr), int(total_samples)))
+
+    # ---- snapshot / restore (versioned host blobs)
+    def snapshot(self):
+        n = C.c_int64()
+        self._check(self._L.ws_snapshot(self._h, None, 0, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._check(self._L.ws_snapshot(self._h, buf.ctypes.data, buf.size, C.byref(n)))
+        return buf
+
+    def restore(self, blob):
+        blob = np.ascontiguousarray(blob, np.uint8)
+        self._check(self._L.ws_restore(self._h, blob.ctypes.data, blob.size))
+
+    def unet_save(self):
+        n = C.c_int64()
+        self._check(self._L.ws_unet_save(self._h, None, 0, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._check(self._L.ws_unet_save(self._h, buf.ctypes.data, buf.size, C.byref(n)))
+        return buf
+
+    def unet_load(self, blob):
+        blob = np.ascontiguousarray(blob, np.uint8)
+        self._check(self._L.ws_unet_load(self._h, blob.ctypes.data, blob.size))
 
     def set_nparticles(self, n):
         self._check(self._L.ws_set_nparticles(self._h, int(n)))
