@@ -220,6 +220,7 @@ def run_ours(args, rank, world, local_rank):
     bytes_io = sum(host[k].nbytes for k in E2E_FIELDS)
     # ---- roofline of the dominant kernel, timed live on the library stream
     roof = roofline(fs, ms_plain / args.steps, iters0)
+    surface = surface_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     out = None
     if rank == 0:
         cfg_learned = {}
@@ -241,6 +242,7 @@ def run_ours(args, rank, world, local_rank):
                           "sor_path": {0: "none", 1: "grid-wide persistent", 2: "cluster-resident (DSMEM)"}[fs.scalars.sorPath],
                           "particle_substeps_per_s": value * nP,
                           "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP),
+                          "surface_mesh": surface,
                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
@@ -351,6 +353,31 @@ def roofline(fs, ms_step, iters):
             "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": us / step_us,
             "others": {k: {"us_per_launch": v[0], "time_share": v[0] / step_us,
                            "GB_s": v[1] / (v[0] * 1e-6) / 1e9} for k, v in cand.items()}}
+
+
+def surface_timing(fs, cpu=True):
+    """MarchingTetrahedra.build of the splatted density (iso = the solver's
+    iso): device time through ws_surface_mesh (5 calls, the last timed alone
+    after warm-up), and the oracle's single-threaded CPU build of the same
+    field for comparison."""
+    import ctypes as C
+    fs.stage("SPLAT")
+    iso = fs.scalars.iso
+    n, vol = C.c_int64(), C.c_double()
+    for _ in range(2):
+        fs._check(fs._L.ws_surface_mesh(fs._h, float(iso), C.byref(n), C.byref(vol)))
+    t0 = time.perf_counter()
+    for _ in range(5):
+        fs._check(fs._L.ws_surface_mesh(fs._h, float(iso), C.byref(n), C.byref(vol)))
+    gpu_ms = (time.perf_counter() - t0) / 5 * 1000
+    out = {"iso": iso, "vertices": n.value, "volume": vol.value, "gpu_ms_per_build": gpu_ms}
+    if cpu:
+        from oracle.oracle import mt_mesh_field
+        dens = fs.download("dens")
+        t0 = time.perf_counter()
+        mt_mesh_field(dens, fs.nx, fs.ny, fs.nz, 1.0, iso)
+        out["cpu_oracle_ms_per_build"] = (time.perf_counter() - t0) * 1000
+    return out
 
 
 def cpu_baseline(fs, seconds=20.0):

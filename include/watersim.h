@@ -170,6 +170,18 @@ typedef struct {
 ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a);
 ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a);
 
+/* ---- surface mesh: MarchingTetrahedra.build (js/surface.js:66-177) of the
+ *      current density field (run ws_stage(WS_STAGE_SPLAT) first) at iso, into a
+ *      device buffer the handle owns: `vertices` vertices (a triangle per 3), each
+ *      with a float position and a float unit normal (3 floats each), in the
+ *      reference's emission order; volume is its FP64 signed-volume integral.
+ *      ws_surface_device returns the device pointers (valid until the next
+ *      ws_surface_mesh) for a consumer on the same GPU; ws_surface_download
+ *      copies them to host buffers of at least `vertices` vertices. */
+ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume);
+ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices);
+ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices);
+
 /* ---- snapshot / restore of the whole solver state (resume, or shipping
  *      state between processes). A versioned host blob: knobs, scalars and
  *      RNG streams, the particle fields (nP each), the pressure warm start q

@@ -102,6 +102,7 @@ def _lib(fp64):
         "or_stir_at": (None, [vp, d, d, d, d, d, d, d, d]),
         "or_stir_gaussian": (None, [vp, d, d]),
         "or_mt_volume_field": (d, [vp, i32, i32, i32, d, d, i64p]),
+        "or_mt_mesh_field": (d, [vp, i32, i32, i32, d, d, vp, vp, C.c_int64, i64p]),
     }
     for stage in ("clear_faces", "rasterize_static", "mark_fluid", "p2g", "apply_bc",
                   "snapshot_old", "pressure_solve", "project", "extrapolate",
@@ -298,6 +299,20 @@ def mt_volume_field(dens, nx, ny, nz, dx, iso):
     cnt = C.c_int64(0)
     v = L.or_mt_volume_field(d.ctypes.data, nx, ny, nz, dx, iso, C.byref(cnt))
     return v, cnt.value
+
+
+def mt_mesh_field(dens, nx, ny, nz, dx, iso):
+    """MarchingTetrahedra.build over an external float32 corner field: (volume,
+    positions (V,3) float32, normals (V,3) float32), vertices in build order."""
+    L = _lib(False)
+    d = np.ascontiguousarray(dens, np.float32)
+    cnt = C.c_int64(0)
+    L.or_mt_mesh_field(d.ctypes.data, nx, ny, nz, dx, iso, None, None, 0, C.byref(cnt))
+    n = cnt.value
+    pos = np.zeros((max(n, 1), 3), np.float32)
+    nrm = np.zeros((max(n, 1), 3), np.float32)
+    v = L.or_mt_mesh_field(d.ctypes.data, nx, ny, nz, dx, iso, pos.ctypes.data, nrm.ctypes.data, n, C.byref(cnt))
+    return v, pos[:n], nrm[:n]
 
 
 # Planet workloads (grid n, sea-level radius R, ocean depth): coreR = R - depth,

@@ -2085,8 +2085,10 @@ void or_splat_density(or_solver* s) {
   }
 }
 
-/* MarchingTetrahedra.build volume, js/surface.js:17-177 (triangle count and
- * signed-volume integral; vertex normals only orient the triangles) */
+/* MarchingTetrahedra.build, js/surface.js:17-177: triangle count, signed-
+ * volume integral and, when pos/nrm are given, the emitted vertices (float
+ * positions and gradient normals, 3 per vertex, in cell/tet/case order, at
+ * most maxVerts) */
 static const int MT_CORNERS[8][3] = { {0,0,0},{1,0,0},{1,1,0},{0,1,0},{0,0,1},{1,0,1},{1,1,1},{0,1,1} };
 static const int MT_TETS[6][4] = { {0,5,1,6},{0,1,2,6},{0,2,3,6},{0,3,7,6},{0,7,4,6},{0,4,5,6} };
 static const int MT_EDGES[6][2] = { {0,1},{1,2},{2,0},{0,3},{1,3},{2,3} };
@@ -2096,7 +2098,8 @@ static const int MT_CASES[16][2][3] = {
   {{2,1,5},{0,0,0}}, {{0,3,5},{0,5,1}}, {{0,4,5},{0,5,2}}, {{3,5,4},{0,0,0}},
   {{3,4,5},{0,0,0}}, {{0,2,5},{0,5,4}}, {{0,1,5},{0,5,3}}, {{2,1,5},{0,0,0}},
   {{2,1,4},{2,4,3}}, {{0,1,4},{0,0,0}}, {{0,2,3},{0,0,0}}, {{0,0,0},{0,0,0}} };
-static double mt_volume_impl(const st_t* dens, int nx, int ny, int nz, double dx, double iso, int64_t* triCount) {
+static double mt_volume_impl(const st_t* dens, int nx, int ny, int nz, double dx, double iso, int64_t* triCount,
+                             float* pos, float* nrm, int64_t maxVerts) {
   long sj = nx + 1, sk = (long)(ny + 1) * sj;
   double volume = 0; int64_t vcount = 0;
   double cv[8], gx[8], gy[8], gz[8], tv[4];
@@ -2146,11 +2149,17 @@ static double mt_volume_impl(const st_t* dens, int nx, int ny, int nz, double dx
         double cgy = N3[0][1] + N3[1][1] + N3[2][1];
         double cgz = N3[0][2] + N3[1][2] + N3[2][2];
         if (fnx * cgx + fny * cgy + fnz * cgz < 0) {
-          for (int d = 0; d < 3; d++) { double tmp = P3[2][d]; P3[2][d] = P3[1][d]; P3[1][d] = tmp; }
+          for (int d = 0; d < 3; d++) {
+            double tmp = P3[2][d]; P3[2][d] = P3[1][d]; P3[1][d] = tmp;
+            tmp = N3[2][d]; N3[2][d] = N3[1][d]; N3[1][d] = tmp;
+          }
         }
         volume += (P3[0][0] * (P3[1][1] * P3[2][2] - P3[2][1] * P3[1][2]) -
                    P3[0][1] * (P3[1][0] * P3[2][2] - P3[2][0] * P3[1][2]) +
                    P3[0][2] * (P3[1][0] * P3[2][1] - P3[2][0] * P3[1][1])) / 6;
+        if (pos && nrm && vcount + 3 <= maxVerts)
+          for (int vi = 0; vi < 3; vi++)
+            for (int d = 0; d < 3; d++) { pos[(vcount + vi) * 3 + d] = (float)P3[vi][d]; nrm[(vcount + vi) * 3 + d] = (float)N3[vi][d]; }
         vcount += 3;
       }
     }
@@ -2159,10 +2168,14 @@ static double mt_volume_impl(const st_t* dens, int nx, int ny, int nz, double dx
   return fabs(volume);
 }
 double or_mt_volume(or_solver* s, double iso, int64_t* triCount) {
-  return mt_volume_impl(s->dens, s->nx, s->ny, s->nz, s->dx, iso, triCount);
+  return mt_volume_impl(s->dens, s->nx, s->ny, s->nz, s->dx, iso, triCount, NULL, NULL, 0);
 }
 double or_mt_volume_field(const void* dens, int nx, int ny, int nz, double dx, double iso, int64_t* triCount) {
-  return mt_volume_impl((const st_t*)dens, nx, ny, nz, dx, iso, triCount);
+  return mt_volume_impl((const st_t*)dens, nx, ny, nz, dx, iso, triCount, NULL, NULL, 0);
+}
+double or_mt_mesh_field(const void* dens, int nx, int ny, int nz, double dx, double iso, float* pos, float* nrm,
+                        int64_t maxVerts, int64_t* vertCount) {
+  return mt_volume_impl((const st_t*)dens, nx, ny, nz, dx, iso, vertCount, pos, nrm, maxVerts);
 }
 /* autotuneIso, js/solver.js:3838-3849 */
 double or_autotune_iso(or_solver* s) {

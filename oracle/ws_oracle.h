@@ -133,6 +133,10 @@ void   or_stir_gaussian(or_solver*, double sigma, double peak);
 /* standalone marching-tets volume over an external corner field (js/surface.js:66-177) */
 double or_mt_volume_field(const void* dens, int nx, int ny, int nz, double dx, double iso,
                           int64_t* triCount);
+/* the same build with the emitted vertices: pos and nrm hold 3 floats per
+ * vertex (at most maxVerts vertices); returns the volume */
+double or_mt_mesh_field(const void* dens, int nx, int ny, int nz, double dx, double iso, float* pos, float* nrm,
+                        int64_t maxVerts, int64_t* vertCount);
 
 #ifdef __cplusplus
 }

@@ -56,6 +56,10 @@ struct ws_handle {
   bool substepPending = false;          // status of an asynchronous substep not yet pulled
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
+  // surface mesh (marching tets) in device memory, grown on demand
+  float *meshPos = nullptr, *meshNrm = nullptr;
+  long long* meshOffs = nullptr;
+  long long meshCap = 0, meshVerts = 0;
   // learned warm start of the pressure solve (ws_unet.cu)
   unet::Net* net = nullptr;
   bool unetOn = false;                  // predict q before every solve
@@ -128,6 +132,9 @@ static void free_all(ws_handle* h) {
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->net) { h->net->destroy(); delete h->net; }
+  if (h->meshPos) cudaFree(h->meshPos);
+  if (h->meshNrm) cudaFree(h->meshNrm);
+  if (h->meshOffs) cudaFree(h->meshOffs);
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1320,5 +1327,46 @@ extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
   h->net->adamStep = (int)steps;
   if (gain > 0) WS_TRY(h->net->set_gain(gain, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ surface mesh
+// MarchingTetrahedra.build (js/surface.js:66-177) on the current density
+// field (ws_stage SPLAT / splatDensity): vertices into a device buffer owned
+// by the handle, in the reference's emission order
+extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  double vol = 0; int64_t cnt = 0;
+  if ((s = mt_volume(h, iso, &vol, &cnt))) return s;        // also leaves the per-block counts
+  if (!h->meshOffs) WS_TRY(cudaMalloc(&h->meshOffs, sizeof(long long) * (size_t)(grid_for(h->d.nCells, 128) + 1)));
+  if (cnt > h->meshCap) {
+    long long cap = std::max<long long>(cnt + cnt / 4, 1 << 16);
+    if (h->meshPos) cudaFree(h->meshPos);
+    if (h->meshNrm) cudaFree(h->meshNrm);
+    h->meshPos = nullptr; h->meshNrm = nullptr; h->meshCap = 0;
+    WS_TRY(cudaMalloc(&h->meshPos, sizeof(float) * 3 * (size_t)cap));
+    WS_TRY(cudaMalloc(&h->meshNrm, sizeof(float) * 3 * (size_t)cap));
+    h->meshCap = cap;
+  }
+  launch_mt_mesh(h->d, h->dens, iso, h->partials, h->meshOffs, h->meshCap, h->meshPos, h->meshNrm, h->stream);
+  if ((s = check_launch(h, 2))) return s;
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  h->meshVerts = cnt;
+  if (vertices) *vertices = cnt;
+  if (volume) *volume = vol;
+  return WS_OK;
+}
+extern "C" ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
+  if (!h) return WS_ERR_INVALID;
+  if (max_vertices < h->meshVerts) return fail(h, WS_ERR_RANGE, "buffers hold fewer vertices than the mesh");
+  if (pos) WS_TRY(cudaMemcpy(pos, h->meshPos, sizeof(float) * 3 * (size_t)h->meshVerts, cudaMemcpyDeviceToHost));
+  if (nrm) WS_TRY(cudaMemcpy(nrm, h->meshNrm, sizeof(float) * 3 * (size_t)h->meshVerts, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
+  if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
+  *pos = h->meshPos; *nrm = h->meshNrm; *vertices = h->meshVerts;
   return WS_OK;
 }

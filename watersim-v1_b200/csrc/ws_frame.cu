@@ -501,8 +501,12 @@ __constant__ int c_cases[16][2][3] = {
   {{2,1,4},{2,4,3}}, {{0,1,4},{0,0,0}}, {{0,2,3},{0,0,0}}, {{0,0,0},{0,0,0}} };
 // One cell's signed tet-mesh volume contribution and vertex count (the
 // per-cell body of MarchingTetrahedra.build, js/surface.js:80-171).
+// one cell of MarchingTetrahedra.build (js/surface.js:66-177): its signed
+// volume, its vertex count and, when pos/nrm are given, its vertices
+// (positions and gradient normals as float, 3 per vertex) from index base
 __device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz, double dx, double iso,
-                          int i, int j, int k, int& verts) {
+                          int i, int j, int k, int& verts, float* pos = nullptr, float* nrm = nullptr,
+                          long long base = 0) {
   long long sj = nx + 1, sk = (long long)(ny + 1) * sj;
   double cv[8], gx[8], gy[8], gz[8], minv = 1e300, maxv = -1e300;
   verts = 0;
@@ -545,11 +549,20 @@ __device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz
       double fnx = uy * vz - uz * vy, fny = uz * vx - ux * vz, fnz = ux * vy - uy * vx;
       double cgx = N3[0][0] + N3[1][0] + N3[2][0], cgy = N3[0][1] + N3[1][1] + N3[2][1], cgz = N3[0][2] + N3[1][2] + N3[2][2];
       if (fnx * cgx + fny * cgy + fnz * cgz < 0) {
-        for (int q = 0; q < 3; q++) { double tmp = P3[2][q]; P3[2][q] = P3[1][q]; P3[1][q] = tmp; }
+        for (int q = 0; q < 3; q++) {
+          double tmp = P3[2][q]; P3[2][q] = P3[1][q]; P3[1][q] = tmp;
+          tmp = N3[2][q]; N3[2][q] = N3[1][q]; N3[1][q] = tmp;
+        }
       }
       vol += (P3[0][0] * (P3[1][1] * P3[2][2] - P3[2][1] * P3[1][2]) -
               P3[0][1] * (P3[1][0] * P3[2][2] - P3[2][0] * P3[1][2]) +
               P3[0][2] * (P3[1][0] * P3[2][1] - P3[2][0] * P3[1][1])) / 6;
+      if (pos) {
+        float* pp = pos + (base + verts) * 3;
+        float* nn = nrm + (base + verts) * 3;
+        for (int vi = 0; vi < 3; vi++)
+          for (int q = 0; q < 3; q++) { pp[vi * 3 + q] = (float)P3[vi][q]; nn[vi * 3 + q] = (float)N3[vi][q]; }
+      }
       verts += 3;
     }
   }
@@ -597,6 +610,62 @@ void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* par
   int nb = (int)grid_for(d.nCells, 128);
   k_mt_partial<<<nb, 128, 0, s>>>(d, dens, iso, partials);
   k_reduce_pairs<<<1, 1024, 0, s>>>(partials, nb, out);
+}
+
+// Mesh emission in the reference's order (cells in index order, then tets,
+// then case triangles): exclusive scan of the per-block vertex counts that
+// k_mt_partial left in partials[b].y, then each block places its cells'
+// vertices by a block scan of their counts.
+__global__ void k_mt_offsets(const double2* __restrict__ partials, int nb, long long* __restrict__ offs) {
+  __shared__ long long ws[32], carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    long long v = i < nb ? llround(partials[i].y) : 0, x = v;
+    for (int o = 1; o < 32; o <<= 1) { long long y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      long long a = lane < nw ? ws[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) { long long y = __shfl_up_sync(0xffffffffu, a, o); if (lane >= o) a += y; }
+      ws[lane] = a;
+    }
+    __syncthreads();
+    long long ex = x - v + (w > 0 ? ws[w - 1] : 0) + carry;
+    if (i < nb) offs[i] = ex;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = ex + v;
+    __syncthreads();
+  }
+}
+__global__ void k_mt_emit(Dims d, const float* __restrict__ dens, double iso, const long long* __restrict__ offs,
+                          long long maxVerts, float* __restrict__ pos, float* __restrict__ nrm) {
+  __shared__ int ws[4];
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int i = 0, j = 0, k = 0, v = 0;
+  if (c < d.nCells) {
+    i = (int)(c % d.nx); j = (int)((c / d.nx) % d.ny); k = (int)(c / ((long long)d.nx * d.ny));
+    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v);
+  }
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, x = v;
+  for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  int before = 0;
+  for (int q = 0; q < w; q++) before += ws[q];
+  const long long base = offs[blockIdx.x] + before + x - v;
+  if (v > 0 && base + v <= maxVerts) {
+    int v2;
+    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v2, pos, nrm, base);
+  }
+}
+void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
+                    long long maxVerts, float* pos, float* nrm, cudaStream_t s) {
+  int nb = (int)grid_for(d.nCells, 128);
+  k_mt_offsets<<<1, 1024, 0, s>>>(partials, nb, offs);
+  k_mt_emit<<<nb, 128, 0, s>>>(d, dens, iso, offs, maxVerts, pos, nrm);
 }
 
 // ------------------------------------------------------------ particle reductions

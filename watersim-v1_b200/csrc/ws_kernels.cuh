@@ -62,6 +62,10 @@ void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, con
                          double oceanR, double coreR, double atmosphereH, cudaStream_t s);
 void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spacing, cudaStream_t s);
 void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s);
+// the marching-tets mesh after launch_mt_volume at the same iso (which leaves
+// the per-block vertex counts in partials): vertices in build order
+void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
+                    long long maxVerts, float* pos, float* nrm, cudaStream_t s);
 void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);
 
 // ---- ws_sor.cu

@@ -124,7 +124,7 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
            "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
            "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
-           "ws_unet_save", "ws_unet_load"]
+           "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device"]
 
 
 def load_library(path=None):
@@ -171,6 +171,9 @@ def load_library(path=None):
         "ws_unet_apply": [h, d, i32],
         "ws_snapshot": [h, vp, i64, C.POINTER(C.c_int64)], "ws_restore": [h, vp, i64],
         "ws_unet_save": [h, vp, i64, C.POINTER(C.c_int64)], "ws_unet_load": [h, vp, i64],
+        "ws_surface_mesh": [h, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
+        "ws_surface_download": [h, vp, vp, i64],
+        "ws_surface_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -435,6 +438,18 @@ class FluidSolver:
 
     def unet_apply(self, lr, total_samples):
         self._check(self._L.ws_unet_apply(self._h, float(lr), int(total_samples)))
+
+    # ---- surface mesh (marching tets of the splatted density)
+    def surface_mesh(self, iso=None):
+        """(volume, positions (V,3), normals (V,3)) of the iso-surface of the
+        current density field (splat it first with stage('SPLAT'))."""
+        n, vol = C.c_int64(), C.c_double()
+        iso = self.scalars.iso if iso is None else iso
+        self._check(self._L.ws_surface_mesh(self._h, float(iso), C.byref(n), C.byref(vol)))
+        pos = np.empty((n.value, 3), np.float32)
+        nrm = np.empty((n.value, 3), np.float32)
+        self._check(self._L.ws_surface_download(self._h, pos.ctypes.data, nrm.ctypes.data, n.value))
+        return vol.value, pos, nrm
 
     # ---- snapshot / restore (versioned host blobs)
     def snapshot(self):
