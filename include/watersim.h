@@ -218,6 +218,7 @@ typedef enum {
   WS_STAGE_SPLAT,             /* splatDensity                           :3785 */
   WS_STAGE_VAPOR_COLLISIONS,  /* _vaporCollisions                       :3345 */
   WS_STAGE_ICE_CONTACTS,      /* _iceContacts                           :3290 */
+  WS_STAGE_CURRENTS,          /* _updateCurrents (uses the scalar simTime) :3658 */
   WS_STAGE_COUNT
 } ws_stage_id;
 ws_status ws_stage(ws_handle* h, int32_t stage, double dt);

@@ -109,7 +109,7 @@ def _lib(fp64):
                   "vapor_collisions", "ice_contacts", "push_surface", "splat_density"):
         sigs["or_" + stage] = (None, [vp])
     for stage in ("viscosity", "planet_gravity", "vorticity", "g2p", "advect", "update_heat",
-                  "update_evaporation", "update_phase"):
+                  "update_evaporation", "update_phase", "update_currents"):
         sigs["or_" + stage] = (None, [vp, d])
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

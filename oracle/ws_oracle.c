@@ -1480,6 +1480,93 @@ void or_substep(or_solver* s, double dt) {
   s->S.dtLast = dt;
 }
 
+/* ------------------------------------------------------------ currents
+ * Subsurface currents, js/solver.js:3624-3782: nine sum-of-sines waves of a
+ * vector potential (seeded LCG, _buildCurrWaves :3634-3656), its analytic curl
+ * sampled on a lattice of stride 4 cells (float storage, :3682-3722), and a
+ * capped relaxation of deep fluid particles toward the tangential part of the
+ * trilinearly sampled current (:3726-3782). */
+typedef struct { double kx, ky, kz, A, ph; } cwave_t;
+static void curr_waves(cwave_t w[3][3], double drift[3]) {
+  double seed = 1234567;
+  const double K[3] = { 1.5, 4.0, 9.0 }, amp[3] = { 0.10, 0.085, 0.05 }, dr[3] = { 0.021, 0.05, 0.11 };
+  for (int o = 0; o < 3; o++) {
+    for (int c = 0; c < 3; c++) {
+      double r3[3];
+      for (int q = 0; q < 3; q++) { seed = fmod(seed * 1664525 + 1013904223, 4294967296.0); r3[q] = seed / 4294967296.0 * 2 - 1; }
+      double L = sqrt(r3[0] * r3[0] + r3[1] * r3[1] + r3[2] * r3[2]); if (L == 0) L = 1;
+      w[o][c].kx = r3[0] / L * K[o]; w[o][c].ky = r3[1] / L * K[o]; w[o][c].kz = r3[2] / L * K[o];
+      w[o][c].A = amp[o] / K[o];
+      seed = fmod(seed * 1664525 + 1013904223, 4294967296.0);
+      w[o][c].ph = seed / 4294967296.0 * 6.283;
+    }
+    drift[o] = dr[o];
+  }
+}
+void or_update_currents(or_solver* s, double dt) {
+  double strength = s->P.currents, shell = s->S.oceanR - s->S.coreR;
+  if (!(strength > 0) || !(shell > 0)) return;
+  const int stride = 4;
+  int gnx = s->nx / stride + 2, gny = s->ny / stride + 2, gnz = s->nz / stride + 2;
+  long gN = (long)gnx * gny * gnz;
+  float* cfx = (float*)malloc(sizeof(float) * gN); float* cfy = (float*)malloc(sizeof(float) * gN);
+  float* cfz = (float*)malloc(sizeof(float) * gN);
+  cwave_t w[3][3]; double drift[3];
+  curr_waves(w, drift);
+  double sx = s->dx * stride, t = s->S.simTime, ampl = strength * 2;
+  for (int kk = 0; kk < gnz; kk++) for (int jj = 0; jj < gny; jj++) for (int ii = 0; ii < gnx; ii++) {
+    double wx2 = ii * sx, wy2 = jj * sx, wz2 = kk * sx, ux = 0, uy = 0, uz = 0;
+    for (int o = 0; o < 3; o++) {
+      double dph = drift[o] * t;
+      double thx = w[o][0].kx * wx2 + w[o][0].ky * wy2 + w[o][0].kz * wz2 + dph + w[o][0].ph;
+      double thy = w[o][1].kx * wx2 + w[o][1].ky * wy2 + w[o][1].kz * wz2 + dph + w[o][1].ph;
+      double thz = w[o][2].kx * wx2 + w[o][2].ky * wy2 + w[o][2].kz * wz2 + dph + w[o][2].ph;
+      ux += w[o][2].A * w[o][2].ky * cos(thz) - w[o][1].A * w[o][1].kz * cos(thy);
+      uy += w[o][0].A * w[o][0].kz * cos(thx) - w[o][2].A * w[o][2].kx * cos(thz);
+      uz += w[o][1].A * w[o][1].kx * cos(thy) - w[o][0].A * w[o][0].ky * cos(thx);
+    }
+    long gi = ((long)kk * gny + jj) * gnx + ii;
+    cfx[gi] = (float)(ux * ampl); cfy[gi] = (float)(uy * ampl); cfz[gi] = (float)(uz * ampl);
+  }
+  double relax = 2.2 * dt; if (relax > 0.35) relax = 0.35;
+  const double dvCap = 0.15, invS = 1 / (s->dx * stride);
+  long gxy = (long)gnx * gny;
+  int kmax = s->nz / stride;
+  for (int p = 0; p < s->S.nP; p++) {
+    if (s->pflag[p] != 0) continue;
+    double rx = s->px[p] - s->cx, ry = s->py[p] - s->cy, rz = s->pz[p] - s->cz;
+    double rl = sqrt(rx * rx + ry * ry + rz * rz); if (rl == 0) rl = 1e-9;
+    double dpt = (s->S.oceanR - rl) / shell;
+    double wgt = (dpt - 0.06) * 4.0;
+    if (wgt <= 0) continue;
+    if (wgt > 1) wgt = 1;
+    double qa = s->px[p] * invS, qb = s->py[p] * invS, qc = s->pz[p] * invS;
+    int i0 = jtrunc(qa), j0 = jtrunc(qb), k0 = jtrunc(qc);
+    if (i0 > gnx - 2) i0 = gnx - 2; else if (i0 < 0) i0 = 0;
+    if (j0 > gny - 2) j0 = gny - 2; else if (j0 < 0) j0 = 0;
+    if (k0 > kmax) k0 = kmax; else if (k0 < 0) k0 = 0;
+    double ta = qa - i0; if (ta > 1) ta = 1; else if (ta < 0) ta = 0;
+    double tb = qb - j0; if (tb > 1) tb = 1; else if (tb < 0) tb = 0;
+    double tc = qc - k0; if (tc > 1) tc = 1; else if (tc < 0) tc = 0;
+    long g = ((long)k0 * gny + j0) * gnx + i0;
+    double a0 = 1 - ta, a1 = ta, b0 = 1 - tb, b1 = tb, c0 = 1 - tc, c1 = tc;
+#define CSAMP(f) ((f[g] * a0 + f[g + 1] * a1) * b0 * c0 + (f[g + gnx] * a0 + f[g + gnx + 1] * a1) * b1 * c0 + \
+                  (f[g + gxy] * a0 + f[g + gxy + 1] * a1) * b0 * c1 + (f[g + gxy + gnx] * a0 + f[g + gxy + gnx + 1] * a1) * b1 * c1)
+    double Ux = CSAMP(cfx), Uy = CSAMP(cfy), Uz = CSAMP(cfz);
+#undef CSAMP
+    double ir = 1 / rl;
+    double Ur = (Ux * rx + Uy * ry + Uz * rz) * ir;
+    double Tx = (Ux - rx * ir * Ur) * wgt, Ty = (Uy - ry * ir * Ur) * wgt, Tz = (Uz - rz * ir * Ur) * wgt;
+    double vr = ((double)s->pvx[p] * rx + (double)s->pvy[p] * ry + (double)s->pvz[p] * rz) * ir;
+    double vx = s->pvx[p] - rx * ir * vr, vy = s->pvy[p] - ry * ir * vr, vz = s->pvz[p] - rz * ir * vr;
+    double ex = relax * (Tx - vx), ey = relax * (Ty - vy), ez = relax * (Tz - vz);
+    double e2 = ex * ex + ey * ey + ez * ez;
+    if (e2 > dvCap * dvCap) { double es = dvCap / sqrt(e2); ex *= es; ey *= es; ez *= es; }
+    s->pvx[p] = (st_t)(s->pvx[p] + ex); s->pvy[p] = (st_t)(s->pvy[p] + ey); s->pvz[p] = (st_t)(s->pvz[p] + ez);
+  }
+  free(cfx); free(cfy); free(cfz);
+}
+
 /* _stepSync, js/solver.js:2670-2700. thermalOn=0 skips the atmospheric
  * cycle (heat tick, evaporation, vapour collisions, phases, ice contacts). */
 void or_step(or_solver* s, double dtFrame) {
@@ -1490,6 +1577,7 @@ void or_step(or_solver* s, double dtFrame) {
       double dtTick = jmin(s->S.heatAcc, 1.0 / 12);
       or_update_heat(s, dtTick);
       if (s->P.sunActivity > 0) or_update_evaporation(s, dtTick);
+      if (s->P.currents > 0) or_update_currents(s, dtTick);
       s->S.heatAcc = 0;
     }
   }

@@ -110,6 +110,7 @@ void   or_g2p(or_solver*, double dt);
 void   or_advect(or_solver*, double dt);
 void   or_update_heat(or_solver*, double dt);
 void   or_update_evaporation(or_solver*, double dt);
+void   or_update_currents(or_solver*, double dt);
 void   or_update_phase(or_solver*, double dt);
 void   or_vapor_collisions(or_solver*);
 void   or_ice_contacts(or_solver*);

@@ -200,3 +200,20 @@ def test_frames_with_thermal_cycle():
     assert abs(sg.vaporCount - so.vaporCount) <= max(3, 0.05 * so.vaporCount)
     ko, kg = o.kinetic_energy(), fs.kineticEnergy()
     assert abs(kg - ko) <= 0.02 * ko
+
+
+def test_currents_parity():
+    """Subsurface currents (js/solver.js:3624-3782): the curl-noise lattice and
+    the relaxation of deep fluid particles. The lattice uses cos; the device's
+    and the host libm's may differ by an ulp, so velocities agree to 1e-6."""
+    o = _state64()
+    o.set(currents=0.6)
+    o.set_scalars(simTime=3.7)
+    fs = to_device(o)
+    nP = o.nP
+    before = o.arr("pvx")[:nP].copy()
+    o.stage("update_currents", 1 / 12)
+    fs.stage("CURRENTS", 1 / 12)
+    assert np.abs(o.arr("pvx")[:nP] - before).max() > 1e-3          # the pass acts
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k

@@ -56,6 +56,9 @@ struct ws_handle {
   bool substepPending = false;          // status of an asynchronous substep not yet pulled
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
+  // subsurface current lattice, allocated on first use
+  CurrField curr{};
+  double* currWaves = nullptr;
   // surface mesh (marching tets) in device memory, grown on demand
   float *meshPos = nullptr, *meshNrm = nullptr;
   long long* meshOffs = nullptr;
@@ -132,6 +135,8 @@ static void free_all(ws_handle* h) {
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->net) { h->net->destroy(); delete h->net; }
+  if (h->curr.cfx) { cudaFree(h->curr.cfx); cudaFree(h->curr.cfy); cudaFree(h->curr.cfz); }
+  if (h->currWaves) cudaFree(h->currWaves);
   if (h->meshPos) cudaFree(h->meshPos);
   if (h->meshNrm) cudaFree(h->meshNrm);
   if (h->meshOffs) cudaFree(h->meshOffs);
@@ -226,7 +231,6 @@ extern "C" ws_status ws_set_params(ws_handle* h, const ws_params* p) {
   if (!p->sorRedBlack || !p->viscJacobi || !p->extrapJacobi)
     return fail(h, WS_ERR_INVALID, "the device path runs red-black SOR and Jacobi viscosity/extrapolation "
                                    "(sorRedBlack, viscJacobi and extrapJacobi must be 1)");
-  if (p->currents > 0) return fail(h, WS_ERR_INVALID, "subsurface currents are not implemented (currents must be 0)");
   h->P = *p;
   return WS_OK;
 }
@@ -772,6 +776,39 @@ extern "C" ws_status ws_substep(ws_handle* h, double dt) {
 }
 
 // ------------------------------------------------------------ frame passes
+// _updateCurrents, js/solver.js:3658-3665: the nine waves of _buildCurrWaves
+// (:3634-3656, fixed seed 1234567, the LCG of the reference in doubles) are
+// built once; field and relaxation run on the device each tick
+static ws_status currents(ws_handle* h, double dt) {
+  if (!(h->P.currents > 0)) return WS_OK;
+  CurrField& F = h->curr;
+  if (!F.cfx) {
+    F.gnx = h->d.nx / 4 + 2; F.gny = h->d.ny / 4 + 2; F.gnz = h->d.nz / 4 + 2; F.sx = h->d.dx * 4;
+    const size_t gN = (size_t)F.gnx * F.gny * F.gnz;
+    WS_TRY(cudaMalloc(&F.cfx, sizeof(float) * gN));
+    WS_TRY(cudaMalloc(&F.cfy, sizeof(float) * gN));
+    WS_TRY(cudaMalloc(&F.cfz, sizeof(float) * gN));
+    double w[45], seed = 1234567;
+    const double K[3] = { 1.5, 4.0, 9.0 }, amp[3] = { 0.10, 0.085, 0.05 }, dr[3] = { 0.021, 0.05, 0.11 };
+    for (int o = 0; o < 3; o++) {
+      for (int c = 0; c < 3; c++) {
+        double r3[3];
+        for (int q = 0; q < 3; q++) { seed = std::fmod(seed * 1664525 + 1013904223, 4294967296.0); r3[q] = seed / 4294967296.0 * 2 - 1; }
+        double L = std::sqrt(r3[0] * r3[0] + r3[1] * r3[1] + r3[2] * r3[2]); if (L == 0) L = 1;
+        double* wv = w + (o * 3 + c) * 5;
+        wv[0] = r3[0] / L * K[o]; wv[1] = r3[1] / L * K[o]; wv[2] = r3[2] / L * K[o]; wv[3] = amp[o] / K[o];
+        seed = std::fmod(seed * 1664525 + 1013904223, 4294967296.0);
+        wv[4] = seed / 4294967296.0 * 6.283;
+      }
+      F.drift[o] = dr[o];
+    }
+    WS_TRY(cudaMalloc(&h->currWaves, sizeof(w)));
+    WS_TRY(cudaMemcpy(h->currWaves, w, sizeof(w), cudaMemcpyHostToDevice));
+    F.w = h->currWaves;
+  }
+  launch_currents(h->d, parts_of(h), F, h->S.simTime, h->P.currents, h->S.oceanR, h->S.coreR, dt, h->stream);
+  return check_launch(h, 2);
+}
 static ws_status heat(ws_handle* h, double dt) {
   HeatParams hp;
   hp.hasSun = h->P.hasSun; hp.sun[0] = h->P.sunPos[0]; hp.sun[1] = h->P.sunPos[1]; hp.sun[2] = h->P.sunPos[2];
@@ -842,6 +879,7 @@ extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
       double dtTick = std::min(h->S.heatAcc, 1.0 / 12);
       if ((s = heat(h, dtTick))) return s;
       if (h->P.sunActivity > 0) { if ((s = evaporation(h, dtTick))) return s; }
+      if (h->P.currents > 0) { if ((s = currents(h, dtTick))) return s; }
       h->S.heatAcc = 0;
     }
   }
@@ -905,6 +943,7 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
       s = check_launch(h, 1); break;
     case WS_STAGE_VAPOR_COLLISIONS: s = vapor_collisions(h); break;
     case WS_STAGE_ICE_CONTACTS: s = ice_contacts(h); break;
+    case WS_STAGE_CURRENTS: s = currents(h, dt); break;
     default: return fail(h, WS_ERR_INVALID, "unknown stage");
   }
   if (s) return s;

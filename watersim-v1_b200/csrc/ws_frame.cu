@@ -707,3 +707,75 @@ void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* part
   k_particle_reduce<<<nb, 256, 0, s>>>(P, mode, mp, partials);
   k_reduce_triples<<<1, 32, 0, s>>>(partials, nb, out);
 }
+
+// ------------------------------------------------------------ subsurface currents
+// js/solver.js:3624-3782. The curl of a drifting sum-of-sines vector
+// potential on a lattice of stride 4 cells (float storage), then a capped
+// relaxation of deep fluid particles toward its tangential part. The nine
+// waves come from the reference's fixed seeded LCG (host, CurrWaves).
+__global__ void k_curr_field(CurrField F, double t, double ampl) {
+  long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long gN = (long long)F.gnx * F.gny * F.gnz;
+  if (gi >= gN) return;
+  const int ii = (int)(gi % F.gnx), jj = (int)((gi / F.gnx) % F.gny), kk = (int)(gi / ((long long)F.gnx * F.gny));
+  const double wx2 = ii * F.sx, wy2 = jj * F.sx, wz2 = kk * F.sx;
+  double ux = 0, uy = 0, uz = 0;
+  for (int o = 0; o < 3; o++) {
+    const double* w0 = F.w + (o * 3 + 0) * 5;
+    const double* w1 = F.w + (o * 3 + 1) * 5;
+    const double* w2 = F.w + (o * 3 + 2) * 5;
+    const double dph = F.drift[o] * t;
+    const double thx = w0[0] * wx2 + w0[1] * wy2 + w0[2] * wz2 + dph + w0[4];
+    const double thy = w1[0] * wx2 + w1[1] * wy2 + w1[2] * wz2 + dph + w1[4];
+    const double thz = w2[0] * wx2 + w2[1] * wy2 + w2[2] * wz2 + dph + w2[4];
+    ux += w2[3] * w2[1] * cos(thz) - w1[3] * w1[2] * cos(thy);
+    uy += w0[3] * w0[2] * cos(thx) - w2[3] * w2[0] * cos(thz);
+    uz += w1[3] * w1[0] * cos(thy) - w0[3] * w0[1] * cos(thx);
+  }
+  F.cfx[gi] = (float)(ux * ampl); F.cfy[gi] = (float)(uy * ampl); F.cfz[gi] = (float)(uz * ampl);
+}
+__global__ void k_currents(Dims d, PartsDev P, CurrField F, double oceanR, double shell, double relax, int kmax) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP || P.pflag[p] != 0) return;
+  const double dvCap = 0.15, invS = 1 / F.sx;
+  double rx = P.px[p] - d.cx, ry = P.py[p] - d.cy, rz = P.pz[p] - d.cz;
+  double rl = sqrt(rx * rx + ry * ry + rz * rz); if (rl == 0) rl = 1e-9;
+  const double dpt = (oceanR - rl) / shell;
+  double wgt = (dpt - 0.06) * 4.0;
+  if (wgt <= 0) return;
+  if (wgt > 1) wgt = 1;
+  const double qa = P.px[p] * invS, qb = P.py[p] * invS, qc = P.pz[p] * invS;
+  int i0 = jtrunc(qa), j0 = jtrunc(qb), k0 = jtrunc(qc);
+  if (i0 > F.gnx - 2) i0 = F.gnx - 2; else if (i0 < 0) i0 = 0;
+  if (j0 > F.gny - 2) j0 = F.gny - 2; else if (j0 < 0) j0 = 0;
+  if (k0 > kmax) k0 = kmax; else if (k0 < 0) k0 = 0;
+  double ta = qa - i0; if (ta > 1) ta = 1; else if (ta < 0) ta = 0;
+  double tb = qb - j0; if (tb > 1) tb = 1; else if (tb < 0) tb = 0;
+  double tc = qc - k0; if (tc > 1) tc = 1; else if (tc < 0) tc = 0;
+  const long long gnx = F.gnx, gxy = (long long)F.gnx * F.gny, g = (k0 * (long long)F.gny + j0) * gnx + i0;
+  const double a0 = 1 - ta, a1 = ta, b0 = 1 - tb, b1 = tb, c0 = 1 - tc, c1 = tc;
+  auto samp = [&](const float* f) -> double {
+    return ((double)f[g] * a0 + (double)f[g + 1] * a1) * b0 * c0 + ((double)f[g + gnx] * a0 + (double)f[g + gnx + 1] * a1) * b1 * c0 +
+           ((double)f[g + gxy] * a0 + (double)f[g + gxy + 1] * a1) * b0 * c1 +
+           ((double)f[g + gxy + gnx] * a0 + (double)f[g + gxy + gnx + 1] * a1) * b1 * c1;
+  };
+  const double Ux = samp(F.cfx), Uy = samp(F.cfy), Uz = samp(F.cfz);
+  const double ir = 1 / rl;
+  const double Ur = (Ux * rx + Uy * ry + Uz * rz) * ir;
+  const double Tx = (Ux - rx * ir * Ur) * wgt, Ty = (Uy - ry * ir * Ur) * wgt, Tz = (Uz - rz * ir * Ur) * wgt;
+  const double vr = ((double)P.pvx[p] * rx + (double)P.pvy[p] * ry + (double)P.pvz[p] * rz) * ir;
+  const double vx = P.pvx[p] - rx * ir * vr, vy = P.pvy[p] - ry * ir * vr, vz = P.pvz[p] - rz * ir * vr;
+  double ex = relax * (Tx - vx), ey = relax * (Ty - vy), ez = relax * (Tz - vz);
+  const double e2 = ex * ex + ey * ey + ez * ez;
+  if (e2 > dvCap * dvCap) { const double es = dvCap / sqrt(e2); ex *= es; ey *= es; ez *= es; }
+  P.pvx[p] = (float)(P.pvx[p] + ex); P.pvy[p] = (float)(P.pvy[p] + ey); P.pvz[p] = (float)(P.pvz[p] + ez);
+}
+void launch_currents(const Dims& d, const PartsDev& P, const CurrField& F, double simTime, double strength,
+                     double oceanR, double coreR, double dt, cudaStream_t s) {
+  const double shell = oceanR - coreR;
+  if (!(strength > 0) || !(shell > 0)) return;
+  const long long gN = (long long)F.gnx * F.gny * F.gnz;
+  k_curr_field<<<grid_for(gN, 256), 256, 0, s>>>(F, simTime, strength * 2);
+  double relax = 2.2 * dt; if (relax > 0.35) relax = 0.35;
+  if (P.nP > 0) k_currents<<<grid_for(P.nP, 256), 256, 0, s>>>(d, P, F, oceanR, shell, relax, d.nz / 4);
+}

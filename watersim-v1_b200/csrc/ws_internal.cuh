@@ -48,6 +48,16 @@ struct PartsDev {
   int nP;
 };
 
+// subsurface current lattice (stride 4 cells) and its nine waves
+// (kx, ky, kz, A, ph per wave, 3 octaves x 3 potential components)
+struct CurrField {
+  int gnx, gny, gnz;
+  double sx;
+  float *cfx, *cfy, *cfz;
+  const double* w;          // device, 45 doubles
+  double drift[3];
+};
+
 // per-substep device counters (zeroed by the raster kernel)
 struct DevStatus {
   unsigned int umaxBits;   // max |u| as float bits (non-negative floats order as ints)

@@ -61,6 +61,8 @@ void launch_phase(const Dims& d, const GridDev& g, const PartsDev& P, const Phas
 void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                          double oceanR, double coreR, double atmosphereH, cudaStream_t s);
 void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spacing, cudaStream_t s);
+void launch_currents(const Dims& d, const PartsDev& P, const CurrField& F, double simTime, double strength,
+                     double oceanR, double coreR, double dt, cudaStream_t s);
 void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s);
 // the marching-tets mesh after launch_mt_volume at the same iso (which leaves
 // the per-block vertex counts in partials): vertices in build order

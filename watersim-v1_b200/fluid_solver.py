@@ -108,7 +108,7 @@ PARTICLE_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pT", "pAir", "pLight"
                    "pWz", "pPh", "pflag", "pcool", "pDepth")
 STAGES = ["CLEAR_RASTER", "MARK_FLUID", "P2G", "FORCES", "PRESSURE", "PROJECT", "VORTICITY", "CLAMP",
           "EXTRAPOLATE", "G2P_ADVECT", "HEAT", "EVAPORATION", "PHASE", "PUSH_SURFACE", "SPLAT",
-          "VAPOR_COLLISIONS", "ICE_CONTACTS"]
+          "VAPOR_COLLISIONS", "ICE_CONTACTS", "CURRENTS"]
 CEIL = {"linear": 0, "quadratic": 1, "exponential": 2}
 
 # exported entry points of include/watersim.h
