@@ -21,7 +21,7 @@
  *  - Storage is float32 for particle and grid fields, uint8 for flags and
  *    cell types — the layouts of the reference's typed arrays.
  *  - Only the sphere-planet world (mode 'sphere' with voxel terrain) of the
- *    reference is implemented; balls and subsurface currents are not.
+ *    reference is implemented; balls (addBall) are not.
  */
 #ifndef WATERSIM_H
 #define WATERSIM_H
