@@ -221,6 +221,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- roofline of the dominant kernel, timed live on the library stream
     roof = roofline(fs, ms_plain / args.steps, iters0)
     surface = surface_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
+    render = render_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     out = None
     if rank == 0:
         cfg_learned = {}
@@ -243,6 +244,7 @@ def run_ours(args, rank, world, local_rank):
                           "particle_substeps_per_s": value * nP,
                           "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP),
                           "surface_mesh": surface,
+                          "render_particles": render,
                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
@@ -377,6 +379,41 @@ def surface_timing(fs, cpu=True):
         t0 = time.perf_counter()
         mt_mesh_field(dens, fs.nx, fs.ny, fs.nz, 1.0, iso)
         out["cpu_oracle_ms_per_build"] = (time.perf_counter() - t0) * 1000
+    return out
+
+
+def render_timing(fs, cpu=True):
+    """WaterScene.updateParticles of the stepped particles (beads mode, lit
+    planet, camera two box widths out, so every class draws and the sort
+    spreads over all 64 buckets): time per ws_render_particles call (4 kernels
+    + the 20-byte count read-back, 5 calls after 2 warm-up), its algorithmic
+    bytes (26 read per particle: position, flag, temperature, exposure, depth,
+    spin phase; 36 written per drawn point) over that time against the
+    measured HBM peak, and the oracle's single-threaded CPU pass on the same
+    particles."""
+    from fluid_solver import render_opts
+    W = fs.nx * fs.dx
+    opts = render_opts(beadsMode=1, cam=(0.5 * W, 0.5 * W, -2.0 * W), sunDir=(0.6, 0.0, 0.8))
+    for _ in range(2):
+        counts, pts = fs.render_particles(opts, download=False)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        counts, pts = fs.render_particles(opts, download=False)
+    ms = (time.perf_counter() - t0) / 5 * 1000
+    nP = fs.scalars.nP
+    algo = 26 * nP + 36 * pts
+    peak, kind = _peaks()
+    out = {"particles": nP, "points": pts, "counts": counts, "gpu_ms_per_call": ms,
+           "algorithmic_bytes": algo, "achieved_gbs": algo / (ms * 1e6), "frac_of_hbm": algo / (ms * 1e6) / peak,
+           "peak_source": kind}
+    if cpu:
+        from oracle.render_oracle import render_particles
+        f = {k: fs.download(k, nP) for k in ("px", "py", "pz", "pflag", "pT", "pLight", "pDepth", "pPh",
+                                             "pWx", "pWy", "pWz")}
+        center = (0.5 * W, 0.5 * fs.ny * fs.dx, 0.5 * fs.nz * fs.dx)
+        t0 = time.perf_counter()
+        render_particles(opts, center, fs.scalars.spacing, fs._p.spinOn, f)
+        out["cpu_oracle_ms_per_call"] = (time.perf_counter() - t0) * 1000
     return out
 
 

@@ -182,6 +182,43 @@ ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* v
 ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices);
 ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices);
 
+/* ---- render-side particle prep: WaterScene.updateParticles
+ *      (js/scene.js:1595-1922) on the current particles. Each particle joins
+ *      one draw class (0 liquid beads, 1 spray/rain, 2 vapour, 3 cloud,
+ *      4 snow) or is culled, gets the scene's colour for it, and the draw list
+ *      is sorted far to near (64 buckets of squared camera distance, stable,
+ *      classes in the order above inside a bucket) into device buffers the
+ *      handle owns: per point a float position (3), colour (3), alpha, size
+ *      and sprite tile. counts[5] receives the class counts (the scene's
+ *      _classCounts), *points their sum. The solver side (spacing, spinOn,
+ *      the box centre) comes from the handle. ws_render_device returns the
+ *      device pointers (valid until the next ws_render_particles);
+ *      ws_render_download copies them to host buffers of max_points points
+ *      (NULL skips an attribute). */
+typedef struct ws_render_opts {
+  int32_t show;           /* updateParticles' show argument */
+  int32_t beadsMode;      /* liquid drawn as flat circles (setBeadsMode) */
+  int32_t metaballMode;   /* liquid drawn by the metaball skin instead */
+  int32_t spinColor;      /* colour = globally normalised spin velocity */
+  int32_t cloudSprite;    /* cloudSpriteMode and its image loaded: tile 5, else 3 */
+  int32_t planetLit;      /* day/night shading (scene oceanR > 0) */
+  int32_t sortOn;         /* camera known: sort far to near */
+  int32_t useLight;       /* solver exposure mirror present (else hemisphere) */
+  int32_t useDepth;       /* solver depth mirror present (night-side bead cull) */
+  int32_t useTemp;        /* temperature mirror present (else 0.32) */
+  double waterOpa;        /* water-surface opacity (beads) */
+  double pOpa;            /* spray/atmosphere opacity */
+  double wScale;          /* world scale of vapour/cloud sprites (0 = 1) */
+  double waterColor[3];   /* water hue, linear rgb */
+  double sunDir[3];       /* unit sun direction, planet-local frame */
+  double cam[3];          /* camera position, planet-local frame */
+} ws_render_opts;
+ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, int32_t counts[5], int64_t* points);
+ws_status ws_render_download(ws_handle* h, float* pos, float* col, float* alpha, float* size, float* sprite,
+                             int64_t max_points);
+ws_status ws_render_device(ws_handle* h, const float** pos, const float** col, const float** alpha,
+                           const float** size, const float** sprite, int64_t* points);
+
 /* ---- snapshot / restore of the whole solver state (resume, or shipping
  *      state between processes). A versioned host blob: knobs, scalars and
  *      RNG streams, the particle fields (nP each), the pressure warm start q

@@ -63,6 +63,10 @@ struct ws_handle {
   float *meshPos = nullptr, *meshNrm = nullptr;
   long long* meshOffs = nullptr;
   long long meshCap = 0, meshVerts = 0;
+  // render-side particle prep: sorted draw list + scratch, sized for capacity
+  RenderOut rdr{};
+  void* rdrScratch = nullptr;
+  long long rdrPoints = 0;
   // learned warm start of the pressure solve (ws_unet.cu)
   unet::Net* net = nullptr;
   bool unetOn = false;                  // predict q before every solve
@@ -140,6 +144,8 @@ static void free_all(ws_handle* h) {
   if (h->meshPos) cudaFree(h->meshPos);
   if (h->meshNrm) cudaFree(h->meshNrm);
   if (h->meshOffs) cudaFree(h->meshOffs);
+  for (float* b : { h->rdr.pos, h->rdr.col, h->rdr.alpha, h->rdr.size, h->rdr.sprite }) if (b) cudaFree(b);
+  if (h->rdrScratch) cudaFree(h->rdrScratch);
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1407,5 +1413,75 @@ extern "C" ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, i
 extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
   *pos = h->meshPos; *nrm = h->meshNrm; *vertices = h->meshVerts;
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ render prep
+// WaterScene.updateParticles (js/scene.js:1595-1922): scene flags and the
+// per-class size/alpha/sprite resolved here (js/scene.js:1601-1602,
+// 1783-1800), the per-particle work in ws_render.cu
+extern "C" ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, int32_t counts[5], int64_t* points) {
+  if (!h || !o) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  RenderCfg c{};
+  c.showBeads = o->show && o->beadsMode && o->waterOpa > 0.01 && !o->metaballMode;
+  c.showSpray = o->show && o->pOpa > 0.01;
+  c.planetLit = o->planetLit != 0; c.useLight = o->useLight != 0; c.useDepth = o->useDepth != 0;
+  c.useTemp = o->useTemp != 0; c.spinCue = h->P.spinOn != 0; c.spinCol = o->spinColor != 0;
+  c.sortOn = o->sortOn != 0;
+  c.center[0] = h->d.W * 0.5; c.center[1] = h->d.H * 0.5; c.center[2] = h->d.D * 0.5;
+  for (int i = 0; i < 3; i++) {
+    c.sun[i] = o->sunDir[i]; c.water[i] = o->waterColor[i];
+    c.cam[i] = c.sortOn ? o->cam[i] : c.center[i];            // unsorted: distance from the centre
+  }
+  double sp = h->S.spacing;
+  if (!(std::isfinite(sp) && sp > 0.02)) sp = 0.06;
+  const double wS = o->wScale ? o->wScale : 1;
+  const double size[5] = { sp * 3.4, sp * 3.4 / 3, std::max(0.18 * wS, std::min(0.4 * wS, sp * 5)),
+                           std::max(0.30 * wS, std::min(0.62 * wS, sp * 6.5)), sp * 3.4 };
+  const double alpha[5] = { std::min(1.0, std::max(0.0, o->waterOpa)), std::min(1.0, 0.95 * o->pOpa),
+                            0.23 * std::sqrt(o->pOpa), std::min(1.0, 0.88 * o->pOpa), 1 };
+  const double sprite[5] = { 0, 1, 2, o->cloudSprite ? 5.0 : 3.0, 4 };
+  for (int i = 0; i < 5; i++) { c.size[i] = (float)size[i]; c.alpha[i] = (float)alpha[i]; c.sprite[i] = (float)sprite[i]; }
+  if (!h->rdrScratch) {
+    size_t cap = (size_t)h->capacity;
+    WS_TRY(cudaMalloc(&h->rdrScratch, render_scratch_bytes(h->capacity)));
+    WS_TRY(cudaMalloc(&h->rdr.pos, sizeof(float) * 3 * cap));
+    WS_TRY(cudaMalloc(&h->rdr.col, sizeof(float) * 3 * cap));
+    WS_TRY(cudaMalloc(&h->rdr.alpha, sizeof(float) * cap));
+    WS_TRY(cudaMalloc(&h->rdr.size, sizeof(float) * cap));
+    WS_TRY(cudaMalloc(&h->rdr.sprite, sizeof(float) * cap));
+  }
+  h->rdrPoints = 0;
+  int32_t cnt[5] = { 0, 0, 0, 0, 0 };
+  if (c.showBeads || c.showSpray) {
+    launch_render_particles(c, parts_of(h), h->rdrScratch, h->rdr, h->stream);
+    if ((s = check_launch(h, h->S.nP ? 4 : 0))) return s;
+    WS_TRY(cudaMemcpyAsync(cnt, h->rdrScratch, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+    WS_TRY(cudaStreamSynchronize(h->stream));
+  }
+  for (int i = 0; i < 5; i++) h->rdrPoints += cnt[i];
+  if (counts) for (int i = 0; i < 5; i++) counts[i] = cnt[i];
+  if (points) *points = h->rdrPoints;
+  return WS_OK;
+}
+extern "C" ws_status ws_render_download(ws_handle* h, float* pos, float* col, float* alpha, float* size, float* sprite,
+                                        int64_t max_points) {
+  if (!h) return WS_ERR_INVALID;
+  if (max_points < h->rdrPoints) return fail(h, WS_ERR_RANGE, "buffers hold fewer points than the draw list");
+  const size_t n = (size_t)h->rdrPoints;
+  if (pos) WS_TRY(cudaMemcpy(pos, h->rdr.pos, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+  if (col) WS_TRY(cudaMemcpy(col, h->rdr.col, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost));
+  if (alpha) WS_TRY(cudaMemcpy(alpha, h->rdr.alpha, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (size) WS_TRY(cudaMemcpy(size, h->rdr.size, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  if (sprite) WS_TRY(cudaMemcpy(sprite, h->rdr.sprite, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_render_device(ws_handle* h, const float** pos, const float** col, const float** alpha,
+                                      const float** size, const float** sprite, int64_t* points) {
+  if (!h || !pos || !col || !alpha || !size || !sprite || !points) return WS_ERR_INVALID;
+  *pos = h->rdr.pos; *col = h->rdr.col; *alpha = h->rdr.alpha; *size = h->rdr.size; *sprite = h->rdr.sprite;
+  *points = h->rdrPoints;
   return WS_OK;
 }

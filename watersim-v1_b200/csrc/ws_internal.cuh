@@ -48,6 +48,16 @@ struct PartsDev {
   int nP;
 };
 
+// render-side particle prep (WaterScene.updateParticles): the scene state
+// resolved on the host, per-class alpha/size/sprite already float
+struct RenderCfg {
+  int showBeads, showSpray, planetLit, useLight, useDepth, useTemp, spinCue, spinCol, sortOn;
+  double center[3], sun[3], cam[3], water[3];
+  float alpha[5], size[5], sprite[5];
+};
+// sorted draw list, device buffers of capacity points
+struct RenderOut { float *pos, *col, *alpha, *size, *sprite; };
+
 // subsurface current lattice (stride 4 cells) and its nine waves
 // (kx, ky, kz, A, ph per wave, 3 octaves x 3 potential components)
 struct CurrField {

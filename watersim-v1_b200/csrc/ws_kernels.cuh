@@ -68,6 +68,10 @@ void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* par
 // the per-block vertex counts in partials): vertices in build order
 void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
                     long long maxVerts, float* pos, float* nrm, cudaStream_t s);
+// render-side particle prep: classify, bucket-sort far to near, emit the
+// draw list (ws_render.cu); counts land in the first five scratch words
+size_t render_scratch_bytes(long long capacity);
+void launch_render_particles(const RenderCfg& c, const PartsDev& P, void* scratch, RenderOut o, cudaStream_t s);
 void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);
 
 // ---- ws_sor.cu

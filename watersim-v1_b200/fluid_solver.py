@@ -84,6 +84,39 @@ class WsUnetInfo(C.Structure):
                 ("enabled", C.c_int32), ("collecting", C.c_int32)]
 
 
+class WsRenderOpts(C.Structure):
+    """ws_render_opts: the scene state WaterScene.updateParticles reads
+    (js/scene.js:1595-1922)."""
+    _fields_ = [("show", C.c_int32), ("beadsMode", C.c_int32), ("metaballMode", C.c_int32),
+                ("spinColor", C.c_int32), ("cloudSprite", C.c_int32), ("planetLit", C.c_int32),
+                ("sortOn", C.c_int32), ("useLight", C.c_int32), ("useDepth", C.c_int32),
+                ("useTemp", C.c_int32), ("waterOpa", C.c_double), ("pOpa", C.c_double),
+                ("wScale", C.c_double), ("waterColor", C.c_double * 3), ("sunDir", C.c_double * 3),
+                ("cam", C.c_double * 3)]
+
+
+RENDER_CLASSES = ("beads", "spray", "vapor", "cloud", "snow")
+
+
+def render_opts(**kw):
+    """A WsRenderOpts with the scene's defaults (js/scene.js:780, 849, 895-896,
+    981-983): liquid hidden (no beads mode), spray opacity 1, water opacity
+    0.25, water hue #9fd4ee, solver mirrors present, sorted, lit."""
+    o = WsRenderOpts()
+    o.show, o.beadsMode, o.metaballMode, o.spinColor, o.cloudSprite = 1, 0, 0, 0, 0
+    o.planetLit, o.sortOn, o.useLight, o.useDepth, o.useTemp = 1, 1, 1, 1, 1
+    o.waterOpa, o.pOpa, o.wScale = 0.25, 1.0, 1.0
+    o.waterColor[:] = (0x9f / 255, 0xd4 / 255, 0xee / 255)
+    o.sunDir[:] = (1.0, 0.0, 0.0)
+    o.cam[:] = (0.0, 0.0, 0.0)
+    for k, v in kw.items():
+        if k in ("waterColor", "sunDir", "cam"):
+            getattr(o, k)[:] = tuple(float(x) for x in v)
+        else:
+            setattr(o, k, v)
+    return o
+
+
 class WsTerrain(C.Structure):
     _fields_ = [("n", C.c_int32), ("dv", C.c_double), ("Rsl", C.c_double), ("Rlo", C.c_double),
                 ("Rhi", C.c_double), ("landFrac", C.c_double),
@@ -124,7 +157,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
            "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
            "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
-           "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device"]
+           "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device",
+           "ws_render_particles", "ws_render_download", "ws_render_device"]
 
 
 def load_library(path=None):
@@ -174,6 +208,9 @@ def load_library(path=None):
         "ws_surface_mesh": [h, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
         "ws_surface_download": [h, vp, vp, i64],
         "ws_surface_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_render_particles": [h, C.POINTER(WsRenderOpts), C.POINTER(C.c_int32), C.POINTER(C.c_int64)],
+        "ws_render_download": [h, vp, vp, vp, vp, vp, i64],
+        "ws_render_device": [h] + [C.POINTER(C.c_void_p)] * 5 + [C.POINTER(C.c_int64)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -450,6 +487,27 @@ class FluidSolver:
         nrm = np.empty((n.value, 3), np.float32)
         self._check(self._L.ws_surface_download(self._h, pos.ctypes.data, nrm.ctypes.data, n.value))
         return vol.value, pos, nrm
+
+    # ---- render-side particle prep (WaterScene.updateParticles)
+    def render_particles(self, opts=None, download=True, **kw):
+        """Classify, colour and sort the particles far to near into the
+        handle's draw list. Returns (counts dict by class, points) and, with
+        download, a dict of host arrays pos (P,3), col (P,3), alpha, size,
+        sprite. opts is a WsRenderOpts (render_opts(**kw) when None)."""
+        o = opts if opts is not None else render_opts(**kw)
+        cnt = (C.c_int32 * 5)()
+        pts = C.c_int64()
+        self._check(self._L.ws_render_particles(self._h, C.byref(o), cnt, C.byref(pts)))
+        counts = dict(zip(RENDER_CLASSES, list(cnt)))
+        if not download:
+            return counts, pts.value
+        n = pts.value
+        out = {"pos": np.empty((n, 3), np.float32), "col": np.empty((n, 3), np.float32),
+               "alpha": np.empty(n, np.float32), "size": np.empty(n, np.float32), "sprite": np.empty(n, np.float32)}
+        self._check(self._L.ws_render_download(self._h, out["pos"].ctypes.data, out["col"].ctypes.data,
+                                               out["alpha"].ctypes.data, out["size"].ctypes.data,
+                                               out["sprite"].ctypes.data, n))
+        return counts, n, out
 
     # ---- snapshot / restore (versioned host blobs)
     def snapshot(self):
