@@ -222,6 +222,7 @@ def run_ours(args, rank, world, local_rank):
     roof = roofline(fs, ms_plain / args.steps, iters0)
     surface = surface_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     render = render_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
+    metaballs = metaball_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     out = None
     if rank == 0:
         cfg_learned = {}
@@ -245,6 +246,7 @@ def run_ours(args, rank, world, local_rank):
                           "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP),
                           "surface_mesh": surface,
                           "render_particles": render,
+                          "metaballs": metaballs,
                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
@@ -378,6 +380,33 @@ def surface_timing(fs, cpu=True):
         dens = fs.download("dens")
         t0 = time.perf_counter()
         mt_mesh_field(dens, fs.nx, fs.ny, fs.nz, 1.0, iso)
+        out["cpu_oracle_ms_per_build"] = (time.perf_counter() - t0) * 1000
+    return out
+
+
+def metaball_timing(fs, cpu=True):
+    """Metaballs.build(solver, 0.5) of the stepped particles (the app's
+    default tension and detail): device time per ws_metaball_mesh call (field
+    splat, float rounding, marching-tets volume and emission; 5 calls after 2
+    warm-up), and the oracle's single-threaded field + mesh on the same
+    particles."""
+    import ctypes as C
+    n, vol = C.c_int64(), C.c_double()
+    for _ in range(2):
+        fs._check(fs._L.ws_metaball_mesh(fs._h, 0.5, float("nan"), C.byref(n), C.byref(vol)))
+    t0 = time.perf_counter()
+    for _ in range(5):
+        fs._check(fs._L.ws_metaball_mesh(fs._h, 0.5, float("nan"), C.byref(n), C.byref(vol)))
+    out = {"tension": 0.5, "vertices": n.value, "volume": vol.value,
+           "gpu_ms_per_build": (time.perf_counter() - t0) / 5 * 1000}
+    if cpu:
+        from oracle.oracle import metaball_field, mt_mesh_field
+        nP = fs.scalars.nP
+        f = {k: fs.download(k, nP) for k in ("px", "py", "pz", "pflag")}
+        t0 = time.perf_counter()
+        field, m, mdx, iso, _ = metaball_field(f["px"], f["py"], f["pz"], f["pflag"], fs.nx, fs.dx,
+                                               fs.scalars.spacing, 0.5)
+        mt_mesh_field(field, m, m, m, mdx, iso)
         out["cpu_oracle_ms_per_build"] = (time.perf_counter() - t0) * 1000
     return out
 

@@ -182,6 +182,21 @@ ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* v
 ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices);
 ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices);
 
+/* ---- metaball skin: Metaballs.build (js/surface.js:203-284). Every liquid
+ *      particle adds the kernel (1 - d²/R²)² to the corners of an (m+1)³ lattice
+ *      over the box, m = max(6, round(nx·detail)) (detail clamped to 0.5..1.6;
+ *      NaN or <= 0 means 1), R = (1.6 + 2.2·tension)·spacing in lattice cells
+ *      (tension clamped to 0..1, NaN means 0.5); the field is contoured at
+ *      1.5·((1.6 + 2.2·tension)/1.6)^1.5 by the marching-tets mesher into a
+ *      device buffer the handle owns (separate from the surface mesh). The
+ *      field accumulates in FP64 and is stored as float. ws_metaball_field
+ *      copies the last build's corner field (capacity >= (m+1)³ floats; NULL
+ *      field returns m only). */
+ws_status ws_metaball_mesh(ws_handle* h, double tension, double detail, int64_t* vertices, double* volume);
+ws_status ws_metaball_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices);
+ws_status ws_metaball_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices);
+ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capacity, int32_t* m);
+
 /* ---- render-side particle prep: WaterScene.updateParticles
  *      (js/scene.js:1595-1922) on the current particles. Each particle joins
  *      one draw class (0 liquid beads, 1 spray/rain, 2 vapour, 3 cloud,

@@ -103,6 +103,8 @@ def _lib(fp64):
         "or_stir_gaussian": (None, [vp, d, d]),
         "or_mt_volume_field": (d, [vp, i32, i32, i32, d, d, i64p]),
         "or_mt_mesh_field": (d, [vp, i32, i32, i32, d, d, vp, vp, C.c_int64, i64p]),
+        "or_metaball_field": (i32, [i32, vp, vp, vp, vp, i32, d, d, d, d, vp,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     }
     for stage in ("clear_faces", "rasterize_static", "mark_fluid", "p2g", "apply_bc",
                   "snapshot_old", "pressure_solve", "project", "extrapolate",
@@ -313,6 +315,23 @@ def mt_mesh_field(dens, nx, ny, nz, dx, iso):
     nrm = np.zeros((max(n, 1), 3), np.float32)
     v = L.or_mt_mesh_field(d.ctypes.data, nx, ny, nz, dx, iso, pos.ctypes.data, nrm.ctypes.data, n, C.byref(cnt))
     return v, pos[:n], nrm[:n]
+
+
+def metaball_field(px, py, pz, pflag, nx, dx, spacing, tension, detail=None):
+    """Metaballs.build's kernel field (js/surface.js:203-284) in the reference's
+    Float32Array accumulation order: (field (m+1)^3 float32, m, mdx, iso, R)."""
+    L = _lib(False)
+    n = len(px)
+    a = [np.ascontiguousarray(v, np.float32) for v in (px, py, pz)]
+    f = np.ascontiguousarray(pflag, np.uint8)
+    det = float("nan") if detail is None else float(detail)
+    mdx, iso, R = C.c_double(), C.c_double(), C.c_double()
+    m = L.or_metaball_field(n, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, f.ctypes.data, nx, dx, spacing,
+                            tension, det, None, C.byref(mdx), C.byref(iso), C.byref(R))
+    field = np.zeros((m + 1) ** 3, np.float32)
+    L.or_metaball_field(n, a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, f.ctypes.data, nx, dx, spacing,
+                        tension, det, field.ctypes.data, C.byref(mdx), C.byref(iso), C.byref(R))
+    return field, m, mdx.value, iso.value, R.value
 
 
 # Planet workloads (grid n, sea-level radius R, ocean depth): coreR = R - depth,

@@ -2265,6 +2265,59 @@ double or_mt_mesh_field(const void* dens, int nx, int ny, int nz, double dx, dou
                         int64_t maxVerts, int64_t* vertCount) {
   return mt_volume_impl((const st_t*)dens, nx, ny, nz, dx, iso, vertCount, pos, nrm, maxVerts);
 }
+/* Metaballs.build's kernel field (js/surface.js:203-284): every liquid
+ * particle adds (1 - d^2/R^2)^2 to the corners of its own (m+1)^3 lattice
+ * within the kernel radius R; Float32Array accumulation in particle order.
+ * Returns m; *mdx, *iso and *R give the lattice spacing, the contour level
+ * (metaballIso) and the kernel radius in lattice cells. field holds at least
+ * (m+1)^3 floats (pass NULL to get m only). */
+static double js_round(double x) { double r = floor(x); return (x - r >= 0.5) ? r + 1 : r; }
+int or_metaball_field(int nP, const float* px, const float* py, const float* pz, const uint8_t* fl, int nx, double dx,
+                      double spacing, double tension, double detail, float* field, double* mdx_out, double* iso_out,
+                      double* R_out) {
+  double f = 1;                                           /* js/surface.js:241-244 */
+  if (isfinite(detail) && detail > 0) f = detail < 0.5 ? 0.5 : (detail > 1.6 ? 1.6 : detail);
+  int m = (int)js_round(nx * f);
+  if (m < 6) m = 6;
+  double mdx = m == nx ? dx : (nx * dx) / m;
+  double t = isfinite(tension) ? tension : 0.5;            /* js/surface.js:211-224 */
+  t = t < 0 ? 0 : (t > 1 ? 1 : t);
+  double R = (1.6 + 2.2 * t) * spacing / mdx, R2 = R * R;
+  if (mdx_out) *mdx_out = mdx;
+  if (iso_out) *iso_out = 1.5 * pow((1.6 + 2.2 * t) / 1.6, 1.5);
+  if (R_out) *R_out = R;
+  if (!field) return m;
+  long long len = (long long)(m + 1) * (m + 1) * (m + 1);
+  memset(field, 0, sizeof(float) * (size_t)len);
+  int rad = (int)ceil(R); if (rad > 3) rad = 3;
+  long long sj = m + 1, sk = (long long)(m + 1) * sj;
+  for (int p = 0; p < nP; p++) {
+    if (fl[p] != 0) continue;
+    double gx = px[p] / mdx, gy = py[p] / mdx, gz = pz[p] / mdx;
+    /* outside (-8, m + 8) (or NaN) the reference's clamped ranges are empty */
+    if (!(gx > -8 && gx < m + 8 && gy > -8 && gy < m + 8 && gz > -8 && gz < m + 8)) continue;
+    int i0 = (int)js_round(gx), j0 = (int)js_round(gy), k0 = (int)js_round(gz);
+    int ia = i0 - rad > 0 ? i0 - rad : 0, ib = i0 + rad < m ? i0 + rad : m;
+    int ja = j0 - rad > 0 ? j0 - rad : 0, jb = j0 + rad < m ? j0 + rad : m;
+    int ka = k0 - rad > 0 ? k0 - rad : 0, kb = k0 + rad < m ? k0 + rad : m;
+    for (int k = ka; k <= kb; k++) {
+      double ez = k - gz, dz2 = ez * ez;
+      if (dz2 >= R2) continue;
+      for (int j = ja; j <= jb; j++) {
+        double ey = j - gy, dy2 = dz2 + ey * ey;
+        if (dy2 >= R2) continue;
+        long long base = k * sk + j * sj;
+        for (int i = ia; i <= ib; i++) {
+          double ex = i - gx, d2 = dy2 + ex * ex;
+          if (d2 >= R2) continue;
+          double u = 1 - d2 / R2;
+          field[base + i] = (float)(field[base + i] + u * u);
+        }
+      }
+    }
+  }
+  return m;
+}
 /* autotuneIso, js/solver.js:3838-3849 */
 double or_autotune_iso(or_solver* s) {
   double Vt = s->S.nP * s->S.particleVolume, lo = 0.3, hi = 3.0;

@@ -138,6 +138,9 @@ double or_mt_volume_field(const void* dens, int nx, int ny, int nz, double dx, d
  * vertex (at most maxVerts vertices); returns the volume */
 double or_mt_mesh_field(const void* dens, int nx, int ny, int nz, double dx, double iso, float* pos, float* nrm,
                         int64_t maxVerts, int64_t* vertCount);
+int or_metaball_field(int nP, const float* px, const float* py, const float* pz, const uint8_t* fl, int nx, double dx,
+                      double spacing, double tension, double detail, float* field, double* mdx_out, double* iso_out,
+                      double* R_out);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,14 @@
 #include <vector>
 #include <new>
 
+// a marching-tets mesh in device memory: vertices (pos, nrm: 3 floats each),
+// the per-block emission offsets, both grown on demand
+struct MeshBuf {
+  float *pos = nullptr, *nrm = nullptr;
+  long long* offs = nullptr;
+  long long cap = 0, offsCap = 0, verts = 0;
+};
+
 struct ws_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -59,10 +67,14 @@ struct ws_handle {
   // subsurface current lattice, allocated on first use
   CurrField curr{};
   double* currWaves = nullptr;
-  // surface mesh (marching tets) in device memory, grown on demand
-  float *meshPos = nullptr, *meshNrm = nullptr;
-  long long* meshOffs = nullptr;
-  long long meshCap = 0, meshVerts = 0;
+  // surface mesh and metaball skin (marching tets) in device memory, grown on demand
+  MeshBuf surf{}, mball{};
+  // metaball corner field: FP64 accumulator and its float copy, (m+1)^3 corners
+  double* mbAcc = nullptr;
+  float* mbField = nullptr;
+  double2* mbPartials = nullptr;
+  long long mbCorners = 0, mbCells = 0;
+  int mbM = 0;
   // render-side particle prep: sorted draw list + scratch, sized for capacity
   RenderOut rdr{};
   void* rdrScratch = nullptr;
@@ -141,9 +153,9 @@ static void free_all(ws_handle* h) {
   if (h->net) { h->net->destroy(); delete h->net; }
   if (h->curr.cfx) { cudaFree(h->curr.cfx); cudaFree(h->curr.cfy); cudaFree(h->curr.cfz); }
   if (h->currWaves) cudaFree(h->currWaves);
-  if (h->meshPos) cudaFree(h->meshPos);
-  if (h->meshNrm) cudaFree(h->meshNrm);
-  if (h->meshOffs) cudaFree(h->meshOffs);
+  for (MeshBuf* mb : { &h->surf, &h->mball })
+    for (void* b : { (void*)mb->pos, (void*)mb->nrm, (void*)mb->offs }) if (b) cudaFree(b);
+  for (void* b : { (void*)h->mbAcc, (void*)h->mbField, (void*)h->mbPartials }) if (b) cudaFree(b);
   for (float* b : { h->rdr.pos, h->rdr.col, h->rdr.alpha, h->rdr.size, h->rdr.sprite }) if (b) cudaFree(b);
   if (h->rdrScratch) cudaFree(h->rdrScratch);
   if (h->stHost) cudaFreeHost(h->stHost);
@@ -1376,43 +1388,123 @@ extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
 }
 
 // ------------------------------------------------------------ surface mesh
-// MarchingTetrahedra.build (js/surface.js:66-177) on the current density
-// field (ws_stage SPLAT / splatDensity): vertices into a device buffer owned
-// by the handle, in the reference's emission order
-extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume) {
-  if (!h) return WS_ERR_INVALID;
-  cudaSetDevice(h->device);
-  ws_status s = sync_status(h); if (s) return s;
-  double vol = 0; int64_t cnt = 0;
-  if ((s = mt_volume(h, iso, &vol, &cnt))) return s;        // also leaves the per-block counts
-  if (!h->meshOffs) WS_TRY(cudaMalloc(&h->meshOffs, sizeof(long long) * (size_t)(grid_for(h->d.nCells, 128) + 1)));
-  if (cnt > h->meshCap) {
-    long long cap = std::max<long long>(cnt + cnt / 4, 1 << 16);
-    if (h->meshPos) cudaFree(h->meshPos);
-    if (h->meshNrm) cudaFree(h->meshNrm);
-    h->meshPos = nullptr; h->meshNrm = nullptr; h->meshCap = 0;
-    WS_TRY(cudaMalloc(&h->meshPos, sizeof(float) * 3 * (size_t)cap));
-    WS_TRY(cudaMalloc(&h->meshNrm, sizeof(float) * 3 * (size_t)cap));
-    h->meshCap = cap;
+// MarchingTetrahedra.build (js/surface.js:66-177) of a corner field on the
+// lattice dd into mb, vertices in the reference's emission order. partials
+// holds grid_for(dd.nCells, 128) + 1 entries; the volume pass leaves the
+// per-block vertex counts there for the emission scan.
+static ws_status mt_build(ws_handle* h, const Dims& dd, const float* field, double iso, double2* partials, MeshBuf& mb,
+                          int64_t* vertices, double* volume) {
+  const long long nb = grid_for(dd.nCells, 128);
+  launch_mt_volume(dd, field, iso, partials, h->red, h->stream);
+  ws_status s = check_launch(h, 2); if (s) return s;
+  WS_TRY(cudaMemcpyAsync(h->redHost, h->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  const double vol = std::fabs(h->redHost[0]);
+  const long long cnt = llround(h->redHost[1]);
+  if (nb + 1 > mb.offsCap) {
+    if (mb.offs) cudaFree(mb.offs);
+    mb.offs = nullptr; mb.offsCap = 0;
+    WS_TRY(cudaMalloc(&mb.offs, sizeof(long long) * (size_t)(nb + 1)));
+    mb.offsCap = nb + 1;
   }
-  launch_mt_mesh(h->d, h->dens, iso, h->partials, h->meshOffs, h->meshCap, h->meshPos, h->meshNrm, h->stream);
+  if (cnt > mb.cap) {
+    long long cap = std::max<long long>(cnt + cnt / 4, 1 << 16);
+    if (mb.pos) cudaFree(mb.pos);
+    if (mb.nrm) cudaFree(mb.nrm);
+    mb.pos = nullptr; mb.nrm = nullptr; mb.cap = 0;
+    WS_TRY(cudaMalloc(&mb.pos, sizeof(float) * 3 * (size_t)cap));
+    WS_TRY(cudaMalloc(&mb.nrm, sizeof(float) * 3 * (size_t)cap));
+    mb.cap = cap;
+  }
+  launch_mt_mesh(dd, field, iso, partials, mb.offs, mb.cap, mb.pos, mb.nrm, h->stream);
   if ((s = check_launch(h, 2))) return s;
   WS_TRY(cudaStreamSynchronize(h->stream));
-  h->meshVerts = cnt;
+  mb.verts = cnt;
   if (vertices) *vertices = cnt;
   if (volume) *volume = vol;
   return WS_OK;
 }
+static ws_status mesh_download(ws_handle* h, const MeshBuf& mb, float* pos, float* nrm, int64_t max_vertices) {
+  if (max_vertices < mb.verts) return fail(h, WS_ERR_RANGE, "buffers hold fewer vertices than the mesh");
+  if (pos && mb.verts) WS_TRY(cudaMemcpy(pos, mb.pos, sizeof(float) * 3 * (size_t)mb.verts, cudaMemcpyDeviceToHost));
+  if (nrm && mb.verts) WS_TRY(cudaMemcpy(nrm, mb.nrm, sizeof(float) * 3 * (size_t)mb.verts, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+
+// the current density field (ws_stage SPLAT / splatDensity) at iso
+extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  if ((long long)grid_for(h->d.nCells, 128) + 1 > h->partialsCap) return fail(h, WS_ERR_RANGE, "partials too small");
+  return mt_build(h, h->d, h->dens, iso, h->partials, h->surf, vertices, volume);
+}
 extern "C" ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
   if (!h) return WS_ERR_INVALID;
-  if (max_vertices < h->meshVerts) return fail(h, WS_ERR_RANGE, "buffers hold fewer vertices than the mesh");
-  if (pos) WS_TRY(cudaMemcpy(pos, h->meshPos, sizeof(float) * 3 * (size_t)h->meshVerts, cudaMemcpyDeviceToHost));
-  if (nrm) WS_TRY(cudaMemcpy(nrm, h->meshNrm, sizeof(float) * 3 * (size_t)h->meshVerts, cudaMemcpyDeviceToHost));
-  return WS_OK;
+  return mesh_download(h, h->surf, pos, nrm, max_vertices);
 }
 extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
-  *pos = h->meshPos; *nrm = h->meshNrm; *vertices = h->meshVerts;
+  *pos = h->surf.pos; *nrm = h->surf.nrm; *vertices = h->surf.verts;
+  return WS_OK;
+}
+
+// ------------------------------------------------------------ metaballs
+// Metaballs.build (js/surface.js:203-284): lattice size, spacing, kernel
+// radius and contour level from tension and the detail factor, as
+// metaballKernelCells / metaballIso / buildMetaballs compute them
+static double js_round(double x) { double r = std::floor(x); return (x - r >= 0.5) ? r + 1 : r; }
+extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detail, int64_t* vertices, double* volume) {
+  if (!h) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  double f = 1;
+  if (std::isfinite(detail) && detail > 0) f = detail < 0.5 ? 0.5 : (detail > 1.6 ? 1.6 : detail);
+  const int nx = h->d.nx;
+  const int m = std::max(6, (int)js_round(nx * f));
+  const double mdx = m == nx ? h->d.dx : h->d.W / m;
+  double t = std::isfinite(tension) ? tension : 0.5;
+  t = t < 0 ? 0 : (t > 1 ? 1 : t);
+  const double R = (1.6 + 2.2 * t) * h->S.spacing / mdx;
+  const double iso = 1.5 * std::pow((1.6 + 2.2 * t) / 1.6, 1.5);
+  const int rad = std::min(3, (int)std::ceil(R));
+  const long long corners = (long long)(m + 1) * (m + 1) * (m + 1), cells = (long long)m * m * m;
+  if (corners > h->mbCorners) {
+    for (void* b : { (void*)h->mbAcc, (void*)h->mbField }) if (b) cudaFree(b);
+    h->mbAcc = nullptr; h->mbField = nullptr; h->mbCorners = 0;
+    WS_TRY(cudaMalloc(&h->mbAcc, sizeof(double) * (size_t)corners));
+    WS_TRY(cudaMalloc(&h->mbField, sizeof(float) * (size_t)corners));
+    h->mbCorners = corners;
+  }
+  if (cells > h->mbCells) {
+    if (h->mbPartials) cudaFree(h->mbPartials);
+    h->mbPartials = nullptr; h->mbCells = 0;
+    WS_TRY(cudaMalloc(&h->mbPartials, sizeof(double2) * (size_t)(grid_for(cells, 128) + 1)));
+    h->mbCells = cells;
+  }
+  h->mbM = m;
+  launch_metaball_field(parts_of(h), m, mdx, R * R, rad, h->mbAcc, h->mbField, h->stream);
+  if ((s = check_launch(h, h->S.nP ? 2 : 1))) return s;
+  Dims dd = h->d;
+  dd.nx = dd.ny = dd.nz = m; dd.dx = mdx; dd.nCells = cells;
+  return mt_build(h, dd, h->mbField, iso, h->mbPartials, h->mball, vertices, volume);
+}
+extern "C" ws_status ws_metaball_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
+  if (!h) return WS_ERR_INVALID;
+  return mesh_download(h, h->mball, pos, nrm, max_vertices);
+}
+extern "C" ws_status ws_metaball_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
+  if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
+  *pos = h->mball.pos; *nrm = h->mball.nrm; *vertices = h->mball.verts;
+  return WS_OK;
+}
+extern "C" ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capacity, int32_t* m) {
+  if (!h) return WS_ERR_INVALID;
+  const long long corners = (long long)(h->mbM + 1) * (h->mbM + 1) * (h->mbM + 1);
+  if (m) *m = h->mbM;
+  if (!h->mbM || !field) return WS_OK;
+  if (capacity < corners) return fail(h, WS_ERR_RANGE, "buffer holds fewer floats than the (m+1)^3 field");
+  WS_TRY(cudaMemcpy(field, h->mbField, sizeof(float) * (size_t)corners, cudaMemcpyDeviceToHost));
   return WS_OK;
 }
 

@@ -779,3 +779,50 @@ void launch_currents(const Dims& d, const PartsDev& P, const CurrField& F, doubl
   double relax = 2.2 * dt; if (relax > 0.35) relax = 0.35;
   if (P.nP > 0) k_currents<<<grid_for(P.nP, 256), 256, 0, s>>>(d, P, F, oceanR, shell, relax, d.nz / 4);
 }
+
+// ---------------------------------------------------------------- metaballs
+// Metaballs.build's kernel field (js/surface.js:248-283): every liquid
+// particle adds (1 - d^2/R^2)^2 to the corners of the (m+1)^3 lattice within
+// R (stencil +-rad around the rounded lattice position, clamped to the
+// lattice). The reference sums in Float32 in particle order; here each corner
+// accumulates in FP64 (any order) and is rounded to float once, so the field
+// is deterministic and within the reference's own float rounding of it.
+__device__ __forceinline__ double js_round(double x) { double r = floor(x); return (x - r >= 0.5) ? r + 1 : r; }
+__global__ void k_mb_splat(PartsDev P, int m, double mdx, double R2, int rad, double* __restrict__ acc) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P.nP || P.pflag[p] != 0) return;
+  const double gx = P.px[p] / mdx, gy = P.py[p] / mdx, gz = P.pz[p] / mdx;
+  // outside (-8, m + 8) (or NaN) the reference's clamped ranges are empty
+  if (!(gx > -8 && gx < m + 8 && gy > -8 && gy < m + 8 && gz > -8 && gz < m + 8)) return;
+  const int i0 = (int)js_round(gx), j0 = (int)js_round(gy), k0 = (int)js_round(gz);
+  const int ia = max(i0 - rad, 0), ib = min(i0 + rad, m);
+  const int ja = max(j0 - rad, 0), jb = min(j0 + rad, m);
+  const int ka = max(k0 - rad, 0), kb = min(k0 + rad, m);
+  const long long sj = m + 1, sk = (long long)(m + 1) * sj;
+  for (int k = ka; k <= kb; k++) {
+    const double ez = k - gz, dz2 = ez * ez;
+    if (dz2 >= R2) continue;
+    for (int j = ja; j <= jb; j++) {
+      const double ey = j - gy, dy2 = dz2 + ey * ey;
+      if (dy2 >= R2) continue;
+      const long long base = k * sk + j * sj;
+      for (int i = ia; i <= ib; i++) {
+        const double ex = i - gx, d2 = dy2 + ex * ex;
+        if (d2 >= R2) continue;
+        const double u = 1 - d2 / R2;
+        atomicAdd(acc + base + i, u * u);
+      }
+    }
+  }
+}
+__global__ void k_mb_round(const double* __restrict__ acc, float* __restrict__ field, long long n) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+    field[c] = (float)acc[c];
+}
+void launch_metaball_field(const PartsDev& P, int m, double mdx, double R2, int rad, double* acc, float* field,
+                           cudaStream_t s) {
+  const long long corners = (long long)(m + 1) * (m + 1) * (m + 1);
+  cudaMemsetAsync(acc, 0, sizeof(double) * (size_t)corners, s);
+  if (P.nP) k_mb_splat<<<grid_for(P.nP, 256), 256, 0, s>>>(P, m, mdx, R2, rad, acc);
+  k_mb_round<<<(int)std::min<long long>(grid_for(corners, 256), 148 * 16), 256, 0, s>>>(acc, field, corners);
+}

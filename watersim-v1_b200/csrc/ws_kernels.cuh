@@ -70,6 +70,10 @@ void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2*
                     long long maxVerts, float* pos, float* nrm, cudaStream_t s);
 // render-side particle prep: classify, bucket-sort far to near, emit the
 // draw list (ws_render.cu); counts land in the first five scratch words
+// Metaballs.build's corner field on an (m+1)^3 lattice of spacing mdx
+// (FP64 accumulation, float result); 1 or 2 launches
+void launch_metaball_field(const PartsDev& P, int m, double mdx, double R2, int rad, double* acc, float* field,
+                           cudaStream_t s);
 size_t render_scratch_bytes(long long capacity);
 void launch_render_particles(const RenderCfg& c, const PartsDev& P, void* scratch, RenderOut o, cudaStream_t s);
 void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);

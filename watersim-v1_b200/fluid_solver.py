@@ -158,7 +158,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
            "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
            "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device",
-           "ws_render_particles", "ws_render_download", "ws_render_device"]
+           "ws_render_particles", "ws_render_download", "ws_render_device",
+           "ws_metaball_mesh", "ws_metaball_download", "ws_metaball_device", "ws_metaball_field"]
 
 
 def load_library(path=None):
@@ -208,6 +209,10 @@ def load_library(path=None):
         "ws_surface_mesh": [h, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
         "ws_surface_download": [h, vp, vp, i64],
         "ws_surface_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_metaball_mesh": [h, d, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
+        "ws_metaball_download": [h, vp, vp, i64],
+        "ws_metaball_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_metaball_field": [h, vp, i64, C.POINTER(C.c_int32)],
         "ws_render_particles": [h, C.POINTER(WsRenderOpts), C.POINTER(C.c_int32), C.POINTER(C.c_int64)],
         "ws_render_download": [h, vp, vp, vp, vp, vp, i64],
         "ws_render_device": [h] + [C.POINTER(C.c_void_p)] * 5 + [C.POINTER(C.c_int64)],
@@ -487,6 +492,24 @@ class FluidSolver:
         nrm = np.empty((n.value, 3), np.float32)
         self._check(self._L.ws_surface_download(self._h, pos.ctypes.data, nrm.ctypes.data, n.value))
         return vol.value, pos, nrm
+
+    def metaballs(self, tension=0.5, detail=None, field=False):
+        """Metaballs.build(solver, tension, detail): (volume, positions (V,3),
+        normals (V,3)) of the metaball skin over the liquid particles; with
+        field, also the (m+1)^3 corner field and m."""
+        n, vol = C.c_int64(), C.c_double()
+        det = float("nan") if detail is None else float(detail)
+        self._check(self._L.ws_metaball_mesh(self._h, float(tension), det, C.byref(n), C.byref(vol)))
+        pos = np.empty((n.value, 3), np.float32)
+        nrm = np.empty((n.value, 3), np.float32)
+        self._check(self._L.ws_metaball_download(self._h, pos.ctypes.data, nrm.ctypes.data, n.value))
+        if not field:
+            return vol.value, pos, nrm
+        m = C.c_int32()
+        self._check(self._L.ws_metaball_field(self._h, None, 0, C.byref(m)))
+        f = np.empty((m.value + 1) ** 3, np.float32)
+        self._check(self._L.ws_metaball_field(self._h, f.ctypes.data, f.size, C.byref(m)))
+        return vol.value, pos, nrm, f, m.value
 
     # ---- render-side particle prep (WaterScene.updateParticles)
     def render_particles(self, opts=None, download=True, **kw):
