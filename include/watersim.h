@@ -8,7 +8,8 @@
  * names the reference interface it stands in for.
  *
  * Conventions
- *  - Every call returns a ws_status: 0 = OK, negative = error. The message of
+ *  - Every call returns a ws_status: 0 = OK, negative = error (and WS_BUSY,
+ *    positive, from ws_step_async). The message of
  *    the last error on a handle is available from ws_last_error(). Nothing
  *    aborts or traps; device-side faults (NaN, index out of range, a bounded
  *    wait that ran out) are latched in a device status word and reported by
@@ -16,8 +17,10 @@
  *  - Host pointers are owned by the caller and read or written only during
  *    the call. Device memory is owned by the handle.
  *  - One CUDA stream per handle; calls on one handle must be serialised by
- *    the caller. There is no global mutable state, so different handles may
- *    be used from different threads.
+ *    the caller (a frame started by ws_step_async holds the handle until it
+ *    is collected; other calls meanwhile return WS_ERR_BUSY). There is no
+ *    global mutable state, so different handles may be used from different
+ *    threads.
  *  - Storage is float32 for particle and grid fields, uint8 for flags and
  *    cell types — the layouts of the reference's typed arrays.
  *  - Only the sphere-planet world (mode 'sphere' with voxel terrain) of the
@@ -41,6 +44,8 @@ typedef int32_t ws_status;
 #define WS_ERR_DEVICE   -5   /* a kernel latched a fault (NaN, out of range) */
 #define WS_ERR_TIMEOUT  -6   /* a bounded device-side wait ran out */
 #define WS_ERR_RANGE    -7   /* size beyond a documented maximum */
+#define WS_ERR_BUSY     -8   /* an asynchronous step (ws_step_async) is in flight on the handle */
+#define WS_BUSY          1   /* ws_step_async: the previous frame is still running; nothing started */
 
 typedef struct ws_handle ws_handle;
 
@@ -247,6 +252,18 @@ ws_status ws_restore(ws_handle* h, const void* buf, int64_t size);
 /* ---- drivers: step(dtFrame) == _stepSync (js/solver.js:2663-2700) and
  *      _substep(dt) (js/solver.js:2568-2624) */
 ws_status ws_step(ws_handle* h, double dtFrame);
+
+/* ---- asynchronous frame step: GpuSim.step's non-blocking contract
+ *      (js/gpu/gpusim.js:328-339). ws_step_async starts ws_step(dtFrame) on a
+ *      worker thread the handle owns and returns at once: WS_OK when the frame
+ *      started, WS_BUSY (nothing started) while the previous frame still runs.
+ *      ws_step_poll sets *done and, once done, returns the frame's status;
+ *      ws_step_wait blocks until the frame ends and returns its status. While
+ *      a frame is in flight every other call on the handle returns
+ *      WS_ERR_BUSY; ws_destroy waits for the frame first. */
+ws_status ws_step_async(ws_handle* h, double dtFrame);
+ws_status ws_step_poll(ws_handle* h, int32_t* done);
+ws_status ws_step_wait(ws_handle* h);
 ws_status ws_substep(ws_handle* h, double dt);
 
 /* ---- single stages, for tests (the private methods the reference tests

@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 #include <new>
+#include <atomic>
+#include <thread>
 
 // a marching-tets mesh in device memory: vertices (pos, nrm: 3 floats each),
 // the per-block emission offsets, both grown on demand
@@ -68,6 +70,10 @@ struct ws_handle {
   CurrField curr{};
   double* currWaves = nullptr;
   // surface mesh and metaball skin (marching tets) in device memory, grown on demand
+  // asynchronous frame step (ws_step_async): worker thread, in-flight flag, result
+  std::thread asyncThread;
+  std::atomic<int> asyncRunning{0};
+  ws_status asyncResult = WS_OK;
   MeshBuf surf{}, mball{};
   // metaball corner field: FP64 accumulator and its float copy, (m+1)^3 corners
   double* mbAcc = nullptr;
@@ -96,6 +102,7 @@ static ws_status fail(ws_handle* h, ws_status code, const std::string& msg) {
 static ws_status fail_cuda(ws_handle* h, cudaError_t e, const char* what) {
   return fail(h, WS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+static void collect_async(ws_handle* h);
 static ws_status check_launch(ws_handle* h, int n) {
   h->launches += n;
   cudaError_t e = cudaGetLastError();
@@ -118,6 +125,7 @@ static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; 
 extern "C" const char* ws_version(void) { return "watersim-b200 0.1 (sm_100a)"; }
 
 extern "C" const char* ws_last_error(const ws_handle* h) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return "an asynchronous step is in flight";
   if (!h) return "null handle";
   return h->err.c_str();
 }
@@ -237,6 +245,7 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
 
 extern "C" ws_status ws_destroy(ws_handle* h) {
   if (!h) return WS_ERR_INVALID;
+  collect_async(h);
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   free_all(h);
@@ -245,6 +254,7 @@ extern "C" ws_status ws_destroy(ws_handle* h) {
 }
 
 extern "C" ws_status ws_set_params(ws_handle* h, const ws_params* p) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !p) return WS_ERR_INVALID;
   if (!p->sorRedBlack || !p->viscJacobi || !p->extrapJacobi)
     return fail(h, WS_ERR_INVALID, "the device path runs red-black SOR and Jacobi viscosity/extrapolation "
@@ -253,6 +263,7 @@ extern "C" ws_status ws_set_params(ws_handle* h, const ws_params* p) {
   return WS_OK;
 }
 extern "C" ws_status ws_get_params(const ws_handle* h, ws_params* p) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !p) return WS_ERR_INVALID;
   *p = h->P;
   return WS_OK;
@@ -282,6 +293,7 @@ static ws_status ensure_gravity(ws_handle* h) {
 }
 
 extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !s) return WS_ERR_INVALID;
   ws_status st0 = sync_status(h); if (st0) return st0;
   uint32_t rng[4];
@@ -292,6 +304,7 @@ extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
   return WS_OK;
 }
 extern "C" ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !s) return WS_ERR_INVALID;
   if (s->nP < 0 || s->nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
   int cap = h->capacity;
@@ -303,6 +316,7 @@ extern "C" ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s) {
   return ensure_gravity(h);
 }
 extern "C" ws_status ws_set_nparticles(ws_handle* h, int32_t nP) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   if (nP < 0 || nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
   h->S.nP = nP;
@@ -367,6 +381,7 @@ static bool field_ref(ws_handle* h, ws_field f, FieldRef& r) {
   }
 }
 extern "C" ws_status ws_field_info(const ws_handle* hc, ws_field f, int64_t* count, int32_t* elem) {
+  if (hc && hc->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_handle* h = const_cast<ws_handle*>(hc);
   if (!h) return WS_ERR_INVALID;
   FieldRef r;
@@ -376,6 +391,7 @@ extern "C" ws_status ws_field_info(const ws_handle* hc, ws_field f, int64_t* cou
   return WS_OK;
 }
 extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host, int64_t count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || (!host && count)) return WS_ERR_INVALID;
   FieldRef r;
   if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
@@ -388,6 +404,7 @@ extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host,
   return WS_OK;
 }
 extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || (!host && count)) return WS_ERR_INVALID;
   FieldRef r;
   if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
@@ -424,8 +441,10 @@ static ws_status state_copy(ws_handle* h, const ws_host_arrays* a, bool up) {
     h->vaporPossible = true;
   return WS_OK;
 }
-extern "C" ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a) { return state_copy(h, a, true); }
+extern "C" ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY; return state_copy(h, a, true); }
 extern "C" ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   return state_copy(h, a, false);
 }
 
@@ -451,6 +470,7 @@ static ws_status terrain_to_device(ws_handle* h) {
 }
 
 extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double seaLevel) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   wsterrain::GenInput in{seed, h->S.coreR, seaLevel, h->S.bumpiness, h->d.dx, h->d.cx, h->d.cy, h->d.cz, h->d.nx, h->stream};
   int r = wsterrain::generate(in, h->hostTerrain, h->err);
@@ -460,6 +480,7 @@ extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double sea
 }
 
 extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !t || t->n < 2 || !t->solid || !t->R) return WS_ERR_INVALID;
   wsterrain::Terrain& T = h->hostTerrain;
   long long n3 = (long long)t->n * t->n * t->n;
@@ -470,6 +491,7 @@ extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
 }
 
 extern "C" ws_status ws_download_terrain(ws_handle* h, uint8_t* solid, float* R, double meta[4]) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
   const wsterrain::Terrain& T = h->hostTerrain;
@@ -489,6 +511,7 @@ static wsterrain::FillInput fill_input(ws_handle* h, double depth) {
 }
 
 extern "C" ws_status ws_water_volume(ws_handle* h, double depth, double* volume) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !volume) return WS_ERR_INVALID;
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
   *volume = wsterrain::water_volume(h->hostTerrain, fill_input(h, depth));
@@ -499,6 +522,7 @@ static ws_status splat_and_iso(ws_handle* h);
 
 // _resetWaterSphere, js/solver.js:651-731
 extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   double R2 = h->S.coreR + depth;
   h->S.oceanR = R2;
@@ -545,6 +569,7 @@ static ws_status mt_volume(ws_handle* h, double iso, double* vol, int64_t* cnt) 
   return WS_OK;
 }
 extern "C" ws_status ws_mt_volume(ws_handle* h, double iso, double* volume, int64_t* vertexCount) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   return mt_volume(h, iso, volume, vertexCount);
 }
@@ -560,6 +585,7 @@ static ws_status autotune(ws_handle* h, double* iso) {
   return WS_OK;
 }
 extern "C" ws_status ws_autotune_iso(ws_handle* h, double* iso) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !iso) return WS_ERR_INVALID;
   return autotune(h, iso);
 }
@@ -580,6 +606,7 @@ static ws_status particle_reduce(ws_handle* h, int mode, double mp, double out[3
   return WS_OK;
 }
 extern "C" ws_status ws_kinetic_energy(ws_handle* h, double* ke) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !ke) return WS_ERR_INVALID;
   double o[3];
   ws_status s = particle_reduce(h, 0, 1000 * h->S.particleVolume, o); if (s) return s;
@@ -588,6 +615,7 @@ extern "C" ws_status ws_kinetic_energy(ws_handle* h, double* ke) {
 }
 // earthCensus, js/main.js:176-186: counts are exact, fractions in FP64
 extern "C" ws_status ws_census(ws_handle* h, double fr[3]) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !fr) return WS_ERR_INVALID;
   double o[3];
   ws_status s = particle_reduce(h, 1, 0, o); if (s) return s;
@@ -596,6 +624,7 @@ extern "C" ws_status ws_census(ws_handle* h, double fr[3]) {
   return WS_OK;
 }
 extern "C" ws_status ws_residual(ws_handle* h, double* relres) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !relres) return WS_ERR_INVALID;
   launch_residual(h->d, grid_of(h), h->diag8, h->partials, h->st, nullptr, h->stream);
   ws_status s = check_launch(h, 2); if (s) return s;
@@ -787,6 +816,7 @@ static ws_status substep(ws_handle* h, double dt) {
 }
 
 extern "C" ws_status ws_substep(ws_handle* h, double dt) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !(dt > 0)) return WS_ERR_INVALID;
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain: call ws_generate_terrain or ws_upload_terrain");
   cudaSetDevice(h->device);
@@ -885,8 +915,7 @@ static ws_status ice_contacts(ws_handle* h) {
 }
 
 // _stepSync, js/solver.js:2670-2700
-extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
-  if (!h || !(dtFrame > 0)) return WS_ERR_INVALID;
+static ws_status step_frame(ws_handle* h, double dtFrame) {
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
   cudaSetDevice(h->device);
   ws_status s;
@@ -922,8 +951,53 @@ extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
   if ((s = push_surface(h))) return s;
   return sync_status(h);
 }
+extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || !(dtFrame > 0)) return WS_ERR_INVALID;
+  return step_frame(h, dtFrame);
+}
+
+// GpuSim.step's non-blocking contract (js/gpu/gpusim.js:328-339): the frame
+// runs on a worker thread; a call while the previous frame is still running
+// starts nothing (WS_BUSY, as GpuSim returns while _busy). ws_step_poll and
+// ws_step_wait collect the frame's status; until then every other call on the
+// handle returns WS_ERR_BUSY.
+static void collect_async(ws_handle* h) {
+  if (h->asyncThread.joinable()) h->asyncThread.join();
+}
+extern "C" ws_status ws_step_async(ws_handle* h, double dtFrame) {
+  if (!h || !(dtFrame > 0)) return WS_ERR_INVALID;
+  if (h->asyncRunning.load(std::memory_order_acquire)) return WS_BUSY;
+  collect_async(h);
+  h->asyncResult = WS_OK;
+  h->asyncRunning.store(1, std::memory_order_release);
+  try {
+    h->asyncThread = std::thread([h, dtFrame] {
+      ws_status s = step_frame(h, dtFrame);
+      h->asyncResult = s;
+      h->asyncRunning.store(0, std::memory_order_release);
+    });
+  } catch (...) {
+    h->asyncRunning.store(0, std::memory_order_release);
+    return fail(h, WS_ERR_NOMEM, "cannot start the step thread");
+  }
+  return WS_OK;
+}
+extern "C" ws_status ws_step_poll(ws_handle* h, int32_t* done) {
+  if (!h || !done) return WS_ERR_INVALID;
+  if (h->asyncRunning.load(std::memory_order_acquire)) { *done = 0; return WS_OK; }
+  collect_async(h);
+  *done = 1;
+  return h->asyncResult;
+}
+extern "C" ws_status ws_step_wait(ws_handle* h) {
+  if (!h) return WS_ERR_INVALID;
+  collect_async(h);
+  return h->asyncResult;
+}
 
 extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = WS_OK;
@@ -971,6 +1045,7 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
 // ------------------------------------------------------------ interactions
 extern "C" ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy, double cz, double R,
                                              double fx, double fy, double fz) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   launch_impulse_sphere(parts_of(h), cx, cy, cz, R, fx, fy, fz, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
@@ -978,6 +1053,7 @@ extern "C" ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy,
 }
 extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, double vx, double vy,
                                 double vz, double R, double dt) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   launch_stir_at(parts_of(h), cx, cy, cz, vx, vy, vz, R, dt, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
@@ -986,6 +1062,7 @@ extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, d
 // Seeded Gaussian stir kick: the draw order (u1, theta, phi from stirS) and
 // the tangent construction are part of the workload definition.
 extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !(sigma > 0)) return WS_ERR_INVALID;
   uint32_t st = h->S.stirS;
   st = lcg_next(st); double u1 = st / 4294967296.0 * 2 - 1;
@@ -1008,21 +1085,25 @@ extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
 }
 
 extern "C" ws_status ws_synchronize(ws_handle* h) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   return sync_status(h);
 }
 extern "C" ws_status ws_get_stream(ws_handle* h, void** s) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !s) return WS_ERR_INVALID;
   *s = (void*)h->stream;
   return WS_OK;
 }
 extern "C" ws_status ws_launch_count(ws_handle* h, int64_t* n) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !n) return WS_ERR_INVALID;
   *n = h->launches;
   return WS_OK;
 }
 
 extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !us || reps < 1) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   cudaEvent_t e0, e1;
@@ -1067,6 +1148,7 @@ static ws_status net_ready(ws_handle* h) {
   return sync_status(h);
 }
 extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1081,6 +1163,7 @@ extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) {
   return WS_OK;
 }
 extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (capacity < 0) return fail(h, WS_ERR_RANGE, "negative pair capacity");
   if (capacity > 0) {
@@ -1091,6 +1174,7 @@ extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
   return WS_OK;
 }
 extern "C" ws_status ws_unet_enable(ws_handle* h, int32_t on) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (on && !(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain: train it or call ws_unet_set_gain");
   h->unetOn = on != 0;
@@ -1098,6 +1182,7 @@ extern "C" ws_status ws_unet_enable(ws_handle* h, int32_t on) {
 }
 extern "C" ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, double lr, uint32_t seed,
                                    double* mean_loss) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
   if (steps < 0 || batch < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad training arguments");
@@ -1109,6 +1194,7 @@ extern "C" ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, d
   return WS_OK;
 }
 extern "C" ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !out) return WS_ERR_INVALID;
   std::memset(out, 0, sizeof(*out));
   if (!h->net) return WS_OK;
@@ -1119,12 +1205,14 @@ extern "C" ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out) {
   return WS_OK;
 }
 extern "C" ws_status ws_unet_get_weights(ws_handle* h, float* host, int64_t count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
   WS_TRY(cudaMemcpy(host, h->net->params, sizeof(float) * count, cudaMemcpyDeviceToHost));
   return WS_OK;
 }
 extern "C" ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_t count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
   WS_TRY(h->net->set_weights(host, h->stream));
@@ -1132,12 +1220,14 @@ extern "C" ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_
   return WS_OK;
 }
 extern "C" ws_status ws_unet_set_gain(ws_handle* h, double gain) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!(gain > 0)) return fail(h, WS_ERR_INVALID, "gain must be positive");
   WS_TRY(h->net->set_gain(gain, h->stream));
   return WS_OK;
 }
 extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uint8_t* types, float* target) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
   if (idx < 0 || idx >= std::min(n.pairsStored, n.pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
@@ -1148,6 +1238,7 @@ extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uin
   return WS_OK;
 }
 extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint8_t* types, const float* target) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
   if (!r0n || !types || !target) return WS_ERR_INVALID;
@@ -1165,12 +1256,14 @@ extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint
   return WS_OK;
 }
 extern "C" ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!out || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
   WS_TRY(h->net->forward_pair(idx, out, h->stream));
   return WS_OK;
 }
 extern "C" ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, double* loss) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!grads || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
   WS_TRY(h->net->grad_pair(idx, grads, loss, h->stream));
@@ -1179,6 +1272,7 @@ extern "C" ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, 
 // relative residual of q before and after the prediction, on the pressure
 // system of the current face velocities (call after the forces stage)
 extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* relres_pred) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain");
   GridDev g = grid_of(h);
@@ -1198,6 +1292,7 @@ extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* re
 // device time of `what`: 0 the prediction on the current pressure system
 // (writes q), 1 one training step on a stored pair (batch 1, learning rate 0)
 extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!ms || reps < 1 || what < 0 || what > 1) return WS_ERR_INVALID;
   if (what == 1 && h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
@@ -1222,6 +1317,7 @@ extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, doub
 // samples, the caller sums the FP32 gradient buffer over the ranks (an
 // all-reduce on its communicator), then every rank applies the same step
 extern "C" ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t seed, double* loss_sum) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
   if (samples < 1) return fail(h, WS_ERR_INVALID, "samples must be positive");
@@ -1232,6 +1328,7 @@ extern "C" ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t 
   return WS_OK;
 }
 extern "C" ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!device_ptr || !count) return WS_ERR_INVALID;
   *device_ptr = h->net->grads;
@@ -1239,6 +1336,7 @@ extern "C" ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* cou
   return WS_OK;
 }
 extern "C" ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_samples) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (total_samples < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad learning rate or sample count");
   WS_TRY(h->net->apply(lr, total_samples, h->stream));
@@ -1269,6 +1367,7 @@ int64_t snap_bytes(const ws_handle* h, int terrainN) {
 }  // namespace
 
 extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !size) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1306,6 +1405,7 @@ extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int6
 }
 
 extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !buf) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1351,6 +1451,7 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
 
 // network blob: header, gain, Adam step count, then params, Adam m and v (FP32)
 extern "C" ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!size) return WS_ERR_INVALID;
   const int64_t n = h->net->nparams, need = 8 + 8 + 8 + 8 + 3 * 4 * n;
@@ -1369,6 +1470,7 @@ extern "C" ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int
   return WS_OK;
 }
 extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (!buf) return WS_ERR_INVALID;
   const int64_t n = h->net->nparams;
@@ -1433,6 +1535,7 @@ static ws_status mesh_download(ws_handle* h, const MeshBuf& mb, float* pos, floa
 
 // the current density field (ws_stage SPLAT / splatDensity) at iso
 extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1440,10 +1543,12 @@ extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices
   return mt_build(h, h->d, h->dens, iso, h->partials, h->surf, vertices, volume);
 }
 extern "C" ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   return mesh_download(h, h->surf, pos, nrm, max_vertices);
 }
 extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
   *pos = h->surf.pos; *nrm = h->surf.nrm; *vertices = h->surf.verts;
   return WS_OK;
@@ -1455,6 +1560,7 @@ extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const fl
 // metaballKernelCells / metaballIso / buildMetaballs compute them
 static double js_round(double x) { double r = std::floor(x); return (x - r >= 0.5) ? r + 1 : r; }
 extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detail, int64_t* vertices, double* volume) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1490,15 +1596,18 @@ extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detai
   return mt_build(h, dd, h->mbField, iso, h->mbPartials, h->mball, vertices, volume);
 }
 extern "C" ws_status ws_metaball_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   return mesh_download(h, h->mball, pos, nrm, max_vertices);
 }
 extern "C" ws_status ws_metaball_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
   *pos = h->mball.pos; *nrm = h->mball.nrm; *vertices = h->mball.verts;
   return WS_OK;
 }
 extern "C" ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capacity, int32_t* m) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   const long long corners = (long long)(h->mbM + 1) * (h->mbM + 1) * (h->mbM + 1);
   if (m) *m = h->mbM;
@@ -1513,6 +1622,7 @@ extern "C" ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capac
 // per-class size/alpha/sprite resolved here (js/scene.js:1601-1602,
 // 1783-1800), the per-particle work in ws_render.cu
 extern "C" ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, int32_t counts[5], int64_t* points) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !o) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1560,6 +1670,7 @@ extern "C" ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, 
 }
 extern "C" ws_status ws_render_download(ws_handle* h, float* pos, float* col, float* alpha, float* size, float* sprite,
                                         int64_t max_points) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
   if (max_points < h->rdrPoints) return fail(h, WS_ERR_RANGE, "buffers hold fewer points than the draw list");
   const size_t n = (size_t)h->rdrPoints;
@@ -1572,6 +1683,7 @@ extern "C" ws_status ws_render_download(ws_handle* h, float* pos, float* col, fl
 }
 extern "C" ws_status ws_render_device(ws_handle* h, const float** pos, const float** col, const float** alpha,
                                       const float** size, const float** sprite, int64_t* points) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !pos || !col || !alpha || !size || !sprite || !points) return WS_ERR_INVALID;
   *pos = h->rdr.pos; *col = h->rdr.col; *alpha = h->rdr.alpha; *size = h->rdr.size; *sprite = h->rdr.sprite;
   *points = h->rdrPoints;

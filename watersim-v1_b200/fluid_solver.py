@@ -24,6 +24,9 @@ _LIB_PATH = os.path.join(_HERE, "libwatersim.so")
 _lib = None
 
 
+WS_BUSY = 1          # ws_step_async: previous frame still running, nothing started
+
+
 class WsError(RuntimeError):
     """A ws_status < 0 from the library, with ws_last_error()'s message."""
 
@@ -159,7 +162,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
            "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device",
            "ws_render_particles", "ws_render_download", "ws_render_device",
-           "ws_metaball_mesh", "ws_metaball_download", "ws_metaball_device", "ws_metaball_field"]
+           "ws_metaball_mesh", "ws_metaball_download", "ws_metaball_device", "ws_metaball_field",
+           "ws_step_async", "ws_step_poll", "ws_step_wait"]
 
 
 def load_library(path=None):
@@ -209,6 +213,9 @@ def load_library(path=None):
         "ws_surface_mesh": [h, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
         "ws_surface_download": [h, vp, vp, i64],
         "ws_surface_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_step_async": [h, d],
+        "ws_step_poll": [h, C.POINTER(C.c_int32)],
+        "ws_step_wait": [h],
         "ws_metaball_mesh": [h, d, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
         "ws_metaball_download": [h, vp, vp, i64],
         "ws_metaball_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
@@ -279,6 +286,26 @@ class FluidSolver:
             self.close()
         except Exception:
             pass
+
+    def step_async(self, dtFrame):
+        """Start step(dtFrame) on the handle's worker thread; False (nothing
+        started) while the previous frame still runs, as GpuSim.step returns
+        while busy (js/gpu/gpusim.js:328-339)."""
+        rc = self._L.ws_step_async(self._h, float(dtFrame))
+        if rc == WS_BUSY:
+            return False
+        self._check(rc)
+        return True
+
+    def step_poll(self):
+        """True once the asynchronous frame has ended (raising its error, if any)."""
+        done = C.c_int32()
+        self._check(self._L.ws_step_poll(self._h, C.byref(done)))
+        return bool(done.value)
+
+    def step_wait(self):
+        """Block until the asynchronous frame ends; raises its error, if any."""
+        self._check(self._L.ws_step_wait(self._h))
 
     def _check(self, rc):
         if rc:
