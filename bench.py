@@ -223,6 +223,7 @@ def run_ours(args, rank, world, local_rank):
     surface = surface_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     render = render_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     metaballs = metaball_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
+    balls = ball_timing(fs, one_step)
     out = None
     if rank == 0:
         cfg_learned = {}
@@ -247,6 +248,7 @@ def run_ours(args, rank, world, local_rank):
                           "surface_mesh": surface,
                           "render_particles": render,
                           "metaballs": metaballs,
+                          "balls": balls,
                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
@@ -382,6 +384,43 @@ def surface_timing(fs, cpu=True):
         mt_mesh_field(dens, fs.nx, fs.ny, fs.nz, 1.0, iso)
         out["cpu_oracle_ms_per_build"] = (time.perf_counter() - t0) * 1000
     return out
+
+
+def ball_timing(fs, one_step, steps=50):
+    """The ball coupling's cost: substeps/s of the same planet with eight
+    balls (addBall; four light floaters at the sea surface, four heavy
+    sinkers) against the same number of substeps without, each run of n
+    substeps timed on the host between two stream synchronisations. Runs
+    last: the balls move particles."""
+    import numpy as np
+
+    def timed(n):
+        fs.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            one_step()
+        fs.synchronize()
+        return (time.perf_counter() - t0) / n * 1000
+
+    base = timed(steps)
+    iters_base = fs.scalars.sorIters
+    s = fs.scalars
+    c = fs.nx * fs.dx / 2
+    r = np.random.default_rng(9)
+    for i in range(8):
+        v = r.normal(size=3)
+        v /= np.linalg.norm(v)
+        R = s.oceanR if i < 4 else s.oceanR - 3.0
+        fs.add_ball(*(c + v * R), 2.0, 500.0 if i < 4 else 2500.0)
+    for _ in range(3):
+        one_step()
+    with_balls = timed(steps)
+    iters_balls = fs.scalars.sorIters
+    b = fs.balls
+    fs.set_balls(np.zeros((0, 9)))
+    return {"balls": 8, "ms_per_substep_without": base, "ms_per_substep_with": with_balls,
+            "overhead_ms": with_balls - base, "sor_iterations_last_without": iters_base,
+            "sor_iterations_last_with": iters_balls, "submerged": [round(float(x), 3) for x in b[:, 8]]}
 
 
 def metaball_timing(fs, cpu=True):

@@ -24,7 +24,7 @@
  *  - Storage is float32 for particle and grid fields, uint8 for flags and
  *    cell types — the layouts of the reference's typed arrays.
  *  - Only the sphere-planet world (mode 'sphere' with voxel terrain) of the
- *    reference is implemented; balls (addBall) are not.
+ *    reference is implemented.
  */
 #ifndef WATERSIM_H
 #define WATERSIM_H
@@ -241,13 +241,32 @@ ws_status ws_render_device(ws_handle* h, const float** pos, const float** col, c
 
 /* ---- snapshot / restore of the whole solver state (resume, or shipping
  *      state between processes). A versioned host blob: knobs, scalars and
- *      RNG streams, the particle fields (nP each), the pressure warm start q
- *      and the terrain; grid fields are rebuilt by the next substep. Call with
+ *      RNG streams, the particle fields (nP each), the pressure warm start q,
+ *      the terrain and the balls; grid fields are rebuilt by the next substep. Call with
  *      buf == NULL to get the size. Restore needs a handle of the same grid
  *      and a capacity of at least the stored nP. No reference counterpart
  *      beyond the typed arrays themselves (js/solver.js:94-129). */
 ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int64_t* size);
 ws_status ws_restore(ws_handle* h, const void* buf, int64_t size);
+
+/* ---- balls: addBall (js/solver.js:3910-3912). Each ball is a rigid sphere
+ *      coupled to the fluid every substep as the reference's _substep does
+ *      (:2568-2624): rasterised as a moving solid whose cells carry its
+ *      velocity (_rasterizeStatic :918-938, _applyBC :1153-1170), particles
+ *      pushed out of it after _markFluidCells and after advection
+ *      (_pushBallsChunk :1009-1026), then integrated (_updateBalls
+ *      :2344-2564: waterline from the surrounding liquid, Archimedes cap,
+ *      drag, added mass, terrain contact, domain shell, ball-ball contacts).
+ *      resetWater drops them. ws_get_balls copies up to max balls and sets
+ *      *count to the number held; ws_set_balls replaces the list (count 0
+ *      clears it). At most WS_MAX_BALLS. */
+#define WS_MAX_BALLS 64
+typedef struct {
+  double x, y, z, vx, vy, vz, r, rho, submerged;
+} ws_ball;
+ws_status ws_add_ball(ws_handle* h, double x, double y, double z, double r, double rho);
+ws_status ws_get_balls(ws_handle* h, ws_ball* out, int32_t max, int32_t* count);
+ws_status ws_set_balls(ws_handle* h, const ws_ball* in, int32_t count);
 
 /* ---- drivers: step(dtFrame) == _stepSync (js/solver.js:2663-2700) and
  *      _substep(dt) (js/solver.js:2568-2624) */

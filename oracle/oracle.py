@@ -100,6 +100,11 @@ def _lib(fp64):
         "or_rock_cell_at": (i32, [vp, d, d, d]),
         "or_apply_impulse_sphere": (None, [vp, d, d, d, d, d, d, d]),
         "or_stir_at": (None, [vp, d, d, d, d, d, d, d, d]),
+        "or_add_ball": (i32, [vp, d, d, d, d, d]),
+        "or_get_balls": (i32, [vp, vp, i32]),
+        "or_set_balls": (i32, [vp, vp, i32]),
+        "or_push_balls": (None, [vp]),
+        "or_update_balls": (None, [vp, d]),
         "or_stir_gaussian": (None, [vp, d, d]),
         "or_mt_volume_field": (d, [vp, i32, i32, i32, d, d, i64p]),
         "or_mt_mesh_field": (d, [vp, i32, i32, i32, d, d, vp, vp, C.c_int64, i64p]),
@@ -292,6 +297,23 @@ class Oracle:
 
     def stir_gaussian(self, sigma, peak):
         self.L.or_stir_gaussian(self.h, sigma, peak)
+
+    # balls: addBall (js/solver.js:3910); rows x y z vx vy vz r rho submerged
+    def add_ball(self, x, y, z, r, rho):
+        n = self.L.or_add_ball(self.h, x, y, z, r, rho)
+        if n < 0:
+            raise ValueError("too many balls")
+        return n
+
+    def balls(self):
+        out = np.zeros((64, 9))
+        n = self.L.or_get_balls(self.h, out.ctypes.data, 64)
+        return out[:n].copy()
+
+    def set_balls(self, rows):
+        a = np.ascontiguousarray(rows, np.float64).reshape(-1, 9)
+        if self.L.or_set_balls(self.h, a.ctypes.data, len(a)) < 0:
+            raise ValueError("too many balls")
 
 
 def mt_volume_field(dens, nx, ny, nz, dx, iso):

@@ -21,6 +21,8 @@
 typedef OR_ST st_t;
 
 enum { AIR = 0, FLUID = 1, SOLID = 2 };
+#define OR_MAX_BALLS 64
+enum { BX, BY, BZ, BVX, BVY, BVZ, BR, BRHO, BSUB };
 #define EVAP_STEEPNESS 3.5               /* js/solver.js:40 */
 
 struct or_solver {
@@ -49,6 +51,9 @@ struct or_solver {
   int32_t *pStart, *pAdj; st_t *pW; int pCap;
   int32_t *vIdx, *iceIdx; int idxCap;
   int gridSampleValid;
+  /* balls (addBall, js/solver.js:3910-3912): x y z vx vy vz r rho submerged */
+  double balls[OR_MAX_BALLS][9]; int nBalls; int hadSolidVelocity;
+  float surfY[OR_MAX_BALLS];
 };
 
 /* ------------------------------------------------------------ helpers */
@@ -60,6 +65,12 @@ static inline int jfloor_clamp(double v, int a, int b) {     /* clamp(Math.floor
   return (int)f;
 }
 static inline int jtrunc(double v) { return (int)v; }        /* v | 0 for |v| < 2^31 */
+static inline int jceil_clamp(double v, int a, int b) {      /* clamp(Math.ceil(v), a, b) */
+  double f = ceil(v);
+  if (f < a) return a;
+  if (f > b) return b;
+  return (int)f;
+}
 static inline uint32_t lcg(uint32_t s) { return s * 1664525u + 1013904223u; }
 static inline double jmin(double a, double b) { return a < b ? a : b; }
 static inline double jmax(double a, double b) { return a > b ? a : b; }
@@ -68,7 +79,7 @@ static void* xcalloc(size_t n, size_t sz) { void* p = calloc(n ? n : 1, sz); ret
 int or_storage_bytes(void) { return (int)sizeof(st_t); }
 
 /* ------------------------------------------------------------ construction
- * js/solver.js:45-216 (sphere mode; balls are not part of this build). */
+ * js/solver.js:45-216 (sphere mode). */
 or_solver* or_create(int nx, int ny, int nz, double dx, double coreR,
                      uint32_t terrainSeed, double bumpiness, double targetParticles) {
   or_solver* s = (or_solver*)xcalloc(1, sizeof(or_solver));
@@ -499,6 +510,7 @@ double or_water_volume_mc(or_solver* s, double depth) {
 /* _resetWaterSphere, js/solver.js:651-731 (the terrain must already exist
  * for (coreR, coreR+depth); or_generate_terrain is the generator). */
 void or_reset_water(or_solver* s, double depth) {
+  s->nBalls = 0;
   double R1 = s->S.coreR, R2 = R1 + depth;
   s->S.oceanR = R2;
   uint32_t seed = s->S.terrainSeed;
@@ -624,6 +636,30 @@ void or_rasterize_static(or_solver* s) {
     s->staticValid = 1;
   }
   memcpy(s->cellType, s->staticTypes, s->nCells);
+  /* balls become moving solids, js/solver.js:918-938 */
+  if (s->nBalls || s->hadSolidVelocity) {
+    memset(s->svx, 0, sizeof(st_t) * s->nCells); memset(s->svy, 0, sizeof(st_t) * s->nCells);
+    memset(s->svz, 0, sizeof(st_t) * s->nCells);
+  }
+  s->hadSolidVelocity = s->nBalls > 0;
+  double dx = s->dx;
+  for (int n = 0; n < s->nBalls; n++) {
+    const double* b = s->balls[n];
+    /* a non-finite ball covers no cell (NaN bounds, or an infinite distance) */
+    if (!isfinite(b[BX]) || !isfinite(b[BY]) || !isfinite(b[BZ]) || !isfinite(b[BR])) continue;
+    double r = b[BR], rr = (r + 0.4 * dx) * (r + 0.4 * dx);
+    int i0 = jfloor_clamp((b[BX] - r) / dx, 1, nx - 2), i1 = jceil_clamp((b[BX] + r) / dx, 1, nx - 2);
+    int j0 = jfloor_clamp((b[BY] - r) / dx, 1, ny - 2), j1 = jceil_clamp((b[BY] + r) / dx, 1, ny - 2);
+    int k0 = jfloor_clamp((b[BZ] - r) / dx, 1, nz - 2), k1 = jceil_clamp((b[BZ] + r) / dx, 1, nz - 2);
+    for (k = k0; k <= k1; k++) for (j = j0; j <= j1; j++) for (i = i0; i <= i1; i++) {
+      double cx = (i + 0.5) * dx - b[BX], cy = (j + 0.5) * dx - b[BY], cz = (k + 0.5) * dx - b[BZ];
+      if (cx * cx + cy * cy + cz * cz <= rr) {
+        long ci = ((long)k * ny + j) * nx + i;
+        s->cellType[ci] = SOLID;
+        s->svx[ci] = (st_t)b[BVX]; s->svy[ci] = (st_t)b[BVY]; s->svz[ci] = (st_t)b[BVZ];
+      }
+    }
+  }
 }
 
 /* _markFluidCells, js/solver.js:945-1000 */
@@ -1457,12 +1493,228 @@ void or_advect(or_solver* s, double dt) {
   s->gridSampleValid = 0;
 }
 
+/* ------------------------------------------------------------ balls
+ * addBall (js/solver.js:3910-3912), _pushBallsChunk (:1009-1026),
+ * _ballVsTerrain (:2299-2342) and _updateBalls (:2344-2564), sphere world. */
+int or_add_ball(or_solver* s, double x, double y, double z, double r, double rho) {
+  if (s->nBalls >= OR_MAX_BALLS) return -1;
+  double* b = s->balls[s->nBalls++];
+  b[BX] = x; b[BY] = y; b[BZ] = z; b[BVX] = b[BVY] = b[BVZ] = 0; b[BR] = r; b[BRHO] = rho; b[BSUB] = 0;
+  return s->nBalls;
+}
+int or_get_balls(or_solver* s, double* out, int max) {
+  for (int n = 0; n < s->nBalls && n < max; n++) memcpy(out + 9 * n, s->balls[n], sizeof(double) * 9);
+  return s->nBalls;
+}
+int or_set_balls(or_solver* s, const double* in, int count) {
+  if (count < 0 || count > OR_MAX_BALLS) return -1;
+  for (int n = 0; n < count; n++) memcpy(s->balls[n], in + 9 * n, sizeof(double) * 9);
+  s->nBalls = count;
+  return count;
+}
+void or_push_balls(or_solver* s) {
+  int nP = s->S.nP;
+  for (int n = 0; n < s->nBalls; n++) {
+    const double* b = s->balls[n];
+    double rr = b[BR] + 0.002;
+    for (int p = 0; p < nP; p++) {
+      double ex = s->px[p] - b[BX], ey = s->py[p] - b[BY], ez = s->pz[p] - b[BZ];
+      double d2 = ex * ex + ey * ey + ez * ez;
+      if (d2 < rr * rr) {
+        double d = sqrt(d2); if (!(d != 0)) d = 1e-9;
+        double inv = 1 / d, nxn = ex * inv, nyn = ey * inv, nzn = ez * inv;
+        s->px[p] = (st_t)(b[BX] + nxn * rr); s->py[p] = (st_t)(b[BY] + nyn * rr); s->pz[p] = (st_t)(b[BZ] + nzn * rr);
+        double rvx = s->pvx[p] - b[BVX], rvy = s->pvy[p] - b[BVY], rvz = s->pvz[p] - b[BVZ];
+        double vn = rvx * nxn + rvy * nyn + rvz * nzn;
+        if (vn < 0) {
+          s->pvx[p] = (st_t)(s->pvx[p] - nxn * vn); s->pvy[p] = (st_t)(s->pvy[p] - nyn * vn);
+          s->pvz[p] = (st_t)(s->pvz[p] - nzn * vn);
+        }
+      }
+    }
+  }
+}
+static void ball_vs_terrain(or_solver* s, double* b) {
+  int n = s->tn; double dv = s->tdv; const uint8_t* solid = s->tsolid;
+  int i0 = jtrunc((b[BX] - b[BR]) / dv), i1 = jtrunc((b[BX] + b[BR]) / dv);
+  int j0 = jtrunc((b[BY] - b[BR]) / dv), j1 = jtrunc((b[BY] + b[BR]) / dv);
+  int k0 = jtrunc((b[BZ] - b[BR]) / dv), k1 = jtrunc((b[BZ] + b[BR]) / dv);
+  if (i0 < 0) i0 = 0;
+  if (j0 < 0) j0 = 0;
+  if (k0 < 0) k0 = 0;
+  if (i1 > n - 1) i1 = n - 1;
+  if (j1 > n - 1) j1 = n - 1;
+  if (k1 > n - 1) k1 = n - 1;
+  double bestPen = 0, bpx = 0, bpy = 0, bpz = 0;
+  for (int k = k0; k <= k1; k++) for (int j = j0; j <= j1; j++) {
+    long rowB = ((long)k * n + j) * n;
+    for (int i = i0; i <= i1; i++) {
+      if (!solid[rowB + i]) continue;
+      double qx = b[BX], qy = b[BY], qz = b[BZ];
+      double vx0 = i * dv, vy0 = j * dv, vz0 = k * dv;
+      if (qx < vx0) qx = vx0; else if (qx > vx0 + dv) qx = vx0 + dv;
+      if (qy < vy0) qy = vy0; else if (qy > vy0 + dv) qy = vy0 + dv;
+      if (qz < vz0) qz = vz0; else if (qz > vz0 + dv) qz = vz0 + dv;
+      double ddx = b[BX] - qx, ddy = b[BY] - qy, ddz = b[BZ] - qz;
+      double dd = sqrt(ddx * ddx + ddy * ddy + ddz * ddz);
+      double pen = b[BR] - dd;
+      if (pen > bestPen) {
+        if (dd > 1e-6) { bestPen = pen; bpx = ddx / dd; bpy = ddy / dd; bpz = ddz / dd; }
+        else {
+          double rx = b[BX] - s->cx, ry = b[BY] - s->cy, rz = b[BZ] - s->cz;
+          double rl = sqrt(rx * rx + ry * ry + rz * rz); if (!(rl != 0)) rl = 1e-9;
+          bestPen = pen; bpx = rx / rl; bpy = ry / rl; bpz = rz / rl;
+        }
+      }
+    }
+  }
+  if (bestPen > 0) {
+    b[BX] += bpx * (bestPen + 0.002); b[BY] += bpy * (bestPen + 0.002); b[BZ] += bpz * (bestPen + 0.002);
+    double vn = b[BVX] * bpx + b[BVY] * bpy + b[BVZ] * bpz;
+    if (vn < 0) {
+      b[BVX] -= bpx * vn; b[BVY] -= bpy * vn; b[BVZ] -= bpz * vn;
+      b[BVX] *= 0.985; b[BVY] *= 0.985; b[BVZ] *= 0.985;
+    }
+  }
+}
+void or_update_balls(or_solver* s, double dt) {
+  const double rhoF = 1000, Cd = 0.5, PI = 3.141592653589793;
+  int nb = s->nBalls, nP = s->S.nP;
+  enum { HIST = 24 };
+  if (nb > 0) {
+    double hLo = s->S.coreR, hSpan = (s->S.oceanR - s->S.coreR) * 1.5;
+    float hist[OR_MAX_BALLS * HIST]; int32_t histC[OR_MAX_BALLS];
+    memset(hist, 0, sizeof(hist)); memset(histC, 0, sizeof(histC));
+    for (int p = 0; p < nP; p++) {
+      if (s->pflag[p] != 0) continue;
+      double ppx = s->px[p], ppy = s->py[p], ppz = s->pz[p];
+      double ldx = ppx - s->cx, ldy = ppy - s->cy, ldz = ppz - s->cz;
+      double level = sqrt(ldx * ldx + ldy * ldy + ldz * ldz);
+      for (int q = 0; q < nb; q++) {
+        const double* bb = s->balls[q];
+        double bdx = ppx - bb[BX], bdy = ppy - bb[BY], bdz = ppz - bb[BZ];
+        double dh2 = bdx * bdx + bdy * bdy + bdz * bdz;
+        double r1 = 2.2 * bb[BR], r2 = 3.2 * bb[BR];
+        if (dh2 < r1 * r1 || dh2 > r2 * r2) continue;
+        double bf = floor(((level - hLo) / hSpan) * HIST);
+        histC[q]++;
+        if (bf != bf) continue;                 /* NaN bucket: the reference's store is a no-op */
+        int bucket = bf < 0 ? 0 : (bf >= HIST ? HIST - 1 : (int)bf);
+        hist[q * HIST + bucket]++;
+      }
+    }
+    for (int q = 0; q < nb; q++) {
+      int total = histC[q]; double wl = -INFINITY;
+      if (total > 20) {
+        double acc = 0, target = total * 0.10;
+        for (int bkt = HIST - 1; bkt >= 0; bkt--) {
+          acc += hist[q * HIST + bkt];
+          if (acc >= target) { wl = hLo + (bkt + 0.5) / HIST * hSpan; break; }
+        }
+        if (wl == -INFINITY || total < 140) wl = s->S.oceanR;
+        double wlMax = s->S.oceanR + (s->S.oceanR - s->S.coreR) * 0.3;
+        if (wl > wlMax) wl = wlMax;
+        if (wl < s->S.coreR) wl = s->S.coreR;
+      } else {
+        wl = s->S.oceanR;
+      }
+      s->surfY[q] = (float)wl;
+    }
+  }
+  double g = s->P.gravity;
+  for (int n = 0; n < nb; n++) {
+    double* b = s->balls[n];
+    double m = b[BRHO] * 4 / 3 * PI * b[BR] * b[BR] * b[BR];
+    double area = PI * b[BR] * b[BR];
+    double surf = s->surfY[n];
+    double ex0 = b[BX] - s->cx, ey0 = b[BY] - s->cy, ez0 = b[BZ] - s->cz;
+    double bR = sqrt(ex0 * ex0 + ey0 * ey0 + ez0 * ez0);
+    double inner = bR - b[BR], h = surf - inner;
+    if (!(h > 0)) h = 0;
+    if (h > 2 * b[BR]) h = 2 * b[BR];
+    double Vs = PI * h * h * (3 * b[BR] - h) / 3;
+    b[BSUB] = Vs / (4.0 / 3 * PI * b[BR] * b[BR] * b[BR]);
+    double upx = 0, upy = 1, upz = 0, gEff = g;
+    if (bR > 1e-6) {
+      upx = (b[BX] - s->cx) / bR; upy = (b[BY] - s->cy) / bR; upz = (b[BZ] - s->cz) / bR;
+      gEff = g * (s->S.oceanR * s->S.oceanR) / (bR * bR);
+    }
+    double Fb = (rhoF * Vs - m) * gEff;
+    double tmp[3];
+    sample_vel3(s, b[BX], b[BY], b[BZ], tmp);
+    double rvx = b[BVX] - tmp[0], rvy = b[BVY] - tmp[1], rvz = b[BVZ] - tmp[2];
+    double vr = sqrt(rvx * rvx + rvy * rvy + rvz * rvz);
+    double kd = 0.5 * rhoF * Cd * area * vr;
+    double Fx = -kd * rvx + upx * Fb, Fz = -kd * rvz + upz * Fb, Fyd = -kd * rvy + upy * Fb;
+    double fdx = Fx - upx * Fb, fdy = Fyd - upy * Fb, fdz = Fz - upz * Fb;
+    double fdm = sqrt(fdx * fdx + fdy * fdy + fdz * fdz);
+    double fdmMax = 0.8 * m * g;
+    if (fdm > fdmMax) {
+      double fdc = fdmMax / fdm;
+      Fx = upx * Fb + fdx * fdc; Fyd = upy * Fb + fdy * fdc; Fz = upz * Fb + fdz * fdc;
+    }
+    double mEff = m + 0.5 * rhoF * Vs;
+    b[BVX] += (Fx / mEff) * dt;
+    b[BVZ] += (Fz / mEff) * dt;
+    b[BVY] += (Fyd / mEff) * dt;
+    b[BVX] *= 0.999; b[BVY] *= 0.999; b[BVZ] *= 0.999;
+    const double bvmax = 4;
+    if (b[BVX] > bvmax) b[BVX] = bvmax; else if (b[BVX] < -bvmax) b[BVX] = -bvmax;
+    if (b[BVZ] > bvmax) b[BVZ] = bvmax; else if (b[BVZ] < -bvmax) b[BVZ] = -bvmax;
+    if (b[BVY] > bvmax) b[BVY] = bvmax; else if (b[BVY] < -bvmax) b[BVY] = -bvmax;
+    b[BX] += b[BVX] * dt; b[BY] += b[BVY] * dt; b[BZ] += b[BVZ] * dt;
+    if (s->hasTerr) {
+      ball_vs_terrain(s, b);
+    } else {
+      double cbx = b[BX] - s->cx, cby = b[BY] - s->cy, cbz = b[BZ] - s->cz;
+      double cbr = sqrt(cbx * cbx + cby * cby + cbz * cbz); if (!(cbr != 0)) cbr = 1e-9;
+      if (cbr < s->S.coreR + b[BR]) {
+        double rnx0 = cbx / cbr, rny0 = cby / cbr, rnz0 = cbz / cbr, rr0 = s->S.coreR + b[BR];
+        b[BX] = s->cx + rnx0 * rr0; b[BY] = s->cy + rny0 * rr0; b[BZ] = s->cz + rnz0 * rr0;
+        double vn0 = b[BVX] * rnx0 + b[BVY] * rny0 + b[BVZ] * rnz0;
+        if (vn0 < 0) {
+          b[BVX] -= rnx0 * vn0 * 1.3; b[BVY] -= rny0 * vn0 * 1.3; b[BVZ] -= rnz0 * vn0 * 1.3;
+          b[BVX] *= 0.98; b[BVY] *= 0.98; b[BVZ] *= 0.98;
+        }
+      }
+    }
+    double sbx = b[BX] - s->cx, sby = b[BY] - s->cy, sbz = b[BZ] - s->cz;
+    double sbr = sqrt(sbx * sbx + sby * sby + sbz * sbz); if (!(sbr != 0)) sbr = 1e-9;
+    double rnx = sbx / sbr, rny = sby / sbr, rnz = sbz / sbr;
+    if (sbr > s->domainR - b[BR]) {
+      double rr1 = s->domainR - b[BR];
+      b[BX] = s->cx + rnx * rr1; b[BY] = s->cy + rny * rr1; b[BZ] = s->cz + rnz * rr1;
+      double vn1 = b[BVX] * rnx + b[BVY] * rny + b[BVZ] * rnz;
+      if (vn1 > 0) { b[BVX] -= rnx * vn1 * 1.3; b[BVY] -= rny * vn1 * 1.3; b[BVZ] -= rnz * vn1 * 1.3; }
+    }
+  }
+  for (int a = 0; a < nb; a++) for (int c = a + 1; c < nb; c++) {
+    double *A = s->balls[a], *B = s->balls[c];
+    double ex = B[BX] - A[BX], ey = B[BY] - A[BY], ez = B[BZ] - A[BZ];
+    double d2 = ex * ex + ey * ey + ez * ez, rSum = A[BR] + B[BR];
+    if (d2 > rSum * rSum || d2 < 1e-12) continue;
+    double d = sqrt(d2), nxn = ex / d, nyn = ey / d, nzn = ez / d;
+    double overlap = rSum - d;
+    double mA = A[BRHO] * A[BR] * A[BR] * A[BR], mB = B[BRHO] * B[BR] * B[BR] * B[BR];
+    double tA = mB / (mA + mB), tB = mA / (mA + mB);
+    A[BX] -= nxn * overlap * tA; A[BY] -= nyn * overlap * tA; A[BZ] -= nzn * overlap * tA;
+    B[BX] += nxn * overlap * tB; B[BY] += nyn * overlap * tB; B[BZ] += nzn * overlap * tB;
+    double rvn = (B[BVX] - A[BVX]) * nxn + (B[BVY] - A[BVY]) * nyn + (B[BVZ] - A[BVZ]) * nzn;
+    if (rvn < 0) {
+      double jimp = -(1 + 0.3) * rvn / (1 / mA + 1 / mB);
+      A[BVX] -= nxn * jimp / mA; A[BVY] -= nyn * jimp / mA; A[BVZ] -= nzn * jimp / mA;
+      B[BVX] += nxn * jimp / mB; B[BVY] += nyn * jimp / mB; B[BVZ] += nzn * jimp / mB;
+    }
+  }
+}
+
 /* ------------------------------------------------------------ substep
- * _substep, js/solver.js:2568-2624 (sphere mode, no balls) */
+ * _substep, js/solver.js:2568-2624 (sphere mode) */
 void or_substep(or_solver* s, double dt) {
   or_clear_faces(s);
   or_rasterize_static(s);
   or_mark_fluid(s);
+  if (s->nBalls) or_push_balls(s);
   or_p2g(s);
   or_apply_bc(s);
   or_snapshot_old(s);
@@ -1476,7 +1728,9 @@ void or_substep(or_solver* s, double dt) {
   or_extrapolate(s);
   or_g2p(s, dt);
   or_advect(s, dt);
+  if (s->nBalls) or_push_balls(s);
   s->gridSampleValid = 0;
+  if (s->nBalls) or_update_balls(s, dt);
   s->S.dtLast = dt;
 }
 

@@ -136,6 +136,12 @@ double or_mt_volume_field(const void* dens, int nx, int ny, int nz, double dx, d
                           int64_t* triCount);
 /* the same build with the emitted vertices: pos and nrm hold 3 floats per
  * vertex (at most maxVerts vertices); returns the volume */
+/* balls: each ball is 9 doubles x y z vx vy vz r rho submerged */
+int or_add_ball(or_solver* s, double x, double y, double z, double r, double rho);
+int or_get_balls(or_solver* s, double* out, int max);
+int or_set_balls(or_solver* s, const double* in, int count);
+void or_push_balls(or_solver* s);
+void or_update_balls(or_solver* s, double dt);
 double or_mt_mesh_field(const void* dens, int nx, int ny, int nz, double dx, double iso, float* pos, float* nrm,
                         int64_t maxVerts, int64_t* vertCount);
 int or_metaball_field(int nP, const float* px, const float* py, const float* pz, const uint8_t* fl, int nx, double dx,

@@ -62,7 +62,7 @@ struct ws_handle {
   cudaGraphExec_t gexec = nullptr;
   bool graphDisabled = false;
   long long graphLaunches = 0;
-  struct { double dt, gsA; int vapor, nP, unet; ws_params P; } gsig{};
+  struct { double dt, gsA, coreR, oceanR, spacing; int vapor, nP, unet, balls, clearSv; ws_params P; } gsig{};
   bool substepPending = false;          // status of an asynchronous substep not yet pulled
   bool vaporPossible = false;
   double oceanRGeom = -1;               // oceanR the gravity geometry was built for
@@ -70,6 +70,14 @@ struct ws_handle {
   CurrField curr{};
   double* currWaves = nullptr;
   // surface mesh and metaball skin (marching tets) in device memory, grown on demand
+  // balls (addBall): device state (9 doubles each), solid-velocity field
+  // (3 x nCells), histogram scratch and waterlines; allocated with the first ball
+  double* balls = nullptr;
+  float* sv = nullptr;
+  int* ballHist = nullptr;
+  float* ballSurf = nullptr;
+  int nBalls = 0;
+  bool hadSolidVelocity = false;
   // asynchronous frame step (ws_step_async): worker thread, in-flight flag, result
   std::thread asyncThread;
   std::atomic<int> asyncRunning{0};
@@ -103,6 +111,11 @@ static ws_status fail_cuda(ws_handle* h, cudaError_t e, const char* what) {
   return fail(h, WS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 static void collect_async(ws_handle* h);
+// A captured substep holds buffer pointers and scalars by value: state changes
+// that move either (terrain buffers, scalars, balls) drop it.
+static void drop_graph(ws_handle* h) {
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+}
 static ws_status check_launch(ws_handle* h, int n) {
   h->launches += n;
   cudaError_t e = cudaGetLastError();
@@ -118,6 +131,7 @@ static GridDev grid_of(ws_handle* h) {
   g.vfx = h->vort; g.vfy = h->vort + N; g.vfz = h->vort + 2 * N; g.omg = h->vort + 3 * N;
   g.omx = h->vort + 4 * N; g.omy = h->vort + 5 * N; g.omz = h->vort + 6 * N;
   g.dens = h->dens;
+  g.sv = h->sv;
   return g;
 }
 static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; return P; }
@@ -164,6 +178,7 @@ static void free_all(ws_handle* h) {
   for (MeshBuf* mb : { &h->surf, &h->mball })
     for (void* b : { (void*)mb->pos, (void*)mb->nrm, (void*)mb->offs }) if (b) cudaFree(b);
   for (void* b : { (void*)h->mbAcc, (void*)h->mbField, (void*)h->mbPartials }) if (b) cudaFree(b);
+  for (void* b : { (void*)h->balls, (void*)h->sv, (void*)h->ballHist, (void*)h->ballSurf }) if (b) cudaFree(b);
   for (float* b : { h->rdr.pos, h->rdr.col, h->rdr.alpha, h->rdr.size, h->rdr.sprite }) if (b) cudaFree(b);
   if (h->rdrScratch) cudaFree(h->rdrScratch);
   if (h->stHost) cudaFreeHost(h->stHost);
@@ -452,6 +467,7 @@ extern "C" ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a) {
 static ws_status terrain_to_device(ws_handle* h) {
   const wsterrain::Terrain& T = h->hostTerrain;
   long long n3 = (long long)T.n * T.n * T.n;
+  drop_graph(h);
   if (h->tsolid) { cudaFree(h->tsolid); h->tsolid = nullptr; }
   if (h->tR) { cudaFree(h->tR); h->tR = nullptr; }
   WS_TRY(cudaMalloc(&h->tsolid, (size_t)n3));
@@ -526,6 +542,7 @@ extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
   if (!h) return WS_ERR_INVALID;
   double R2 = h->S.coreR + depth;
   h->S.oceanR = R2;
+  h->nBalls = 0;                                 // resetWater drops the balls (js/solver.js:612, 652)
   if (!h->hasTerrain) { ws_status s = ws_generate_terrain(h, h->S.terrainSeed, R2); if (s) return s; }
   wsterrain::FillOutput fo;
   wsterrain::fill(h->hostTerrain, fill_input(h, depth), fo);
@@ -757,7 +774,15 @@ static ws_status stage_g2p_advect(ws_handle* h, double dt) {
 static ws_status enqueue_substep(ws_handle* h, double dt, double gsA) {
   ws_status s;
   if ((s = stage_clear_raster(h))) return s;
+  if (h->sv && (h->nBalls || h->hadSolidVelocity)) {      // balls become moving solids
+    launch_ball_raster(h->d, h->type, h->sv, true, h->balls, h->nBalls, h->stream);
+    if ((s = check_launch(h, h->nBalls ? 1 : 0))) return s;
+  }
   if ((s = stage_mark(h))) return s;
+  if (h->nBalls) {
+    launch_ball_push(parts_of(h), h->balls, h->nBalls, h->stream);
+    if ((s = check_launch(h, h->S.nP ? 1 : 0))) return s;
+  }
   if ((s = stage_p2g(h))) return s;
   if ((s = stage_forces(h, dt, gsA))) return s;
   if ((s = stage_pressure(h))) return s;
@@ -766,6 +791,13 @@ static ws_status enqueue_substep(ws_handle* h, double dt, double gsA) {
   if (vort) { if ((s = stage_vorticity(h, dt))) return s; if ((s = stage_clamp(h))) return s; }
   if ((s = stage_extrapolate(h))) return s;
   if ((s = stage_g2p_advect(h, dt))) return s;
+  if (h->nBalls) {                                        // _advect's push, then _updateBalls
+    launch_ball_push(parts_of(h), h->balls, h->nBalls, h->stream);
+    BallEnv env{ h->S.coreR, h->S.oceanR, h->P.gravity };
+    launch_ball_update(h->d, h->vel, h->terr, parts_of(h), h->balls, h->nBalls, h->ballHist, h->ballSurf, env, dt,
+                       h->stream);
+    if ((s = check_launch(h, (h->S.nP ? 3 : 1) + (h->nBalls > 1 ? 1 : 0)))) return s;
+  }
   return WS_OK;
 }
 // Captures the substep into a graph; on any capture failure the handle
@@ -796,12 +828,15 @@ static ws_status substep(ws_handle* h, double dt) {
   bool vapor = h->vaporPossible && h->S.nP > 0;
   // pair collection writes a new slot each substep: those substeps run uncaptured
   const bool collect = h->net && h->unetCollect;
+  const int clearSv = (h->sv && (h->nBalls || h->hadSolidVelocity)) ? 1 : 0;
   bool same = !collect && h->gexec && h->gsig.dt == dt && h->gsig.gsA == gsA && h->gsig.vapor == (int)vapor &&
-              h->gsig.nP == h->S.nP && h->gsig.unet == (int)h->unetOn &&
-              std::memcmp(&h->gsig.P, &h->P, sizeof(ws_params)) == 0;
+              h->gsig.nP == h->S.nP && h->gsig.unet == (int)h->unetOn && h->gsig.balls == h->nBalls &&
+              h->gsig.clearSv == clearSv && h->gsig.coreR == h->S.coreR && h->gsig.oceanR == h->S.oceanR &&
+              h->gsig.spacing == h->S.spacing && std::memcmp(&h->gsig.P, &h->P, sizeof(ws_params)) == 0;
   if (!same && !collect && !h->graphDisabled && capture_substep(h, dt, gsA)) {
     h->gsig.dt = dt; h->gsig.gsA = gsA; h->gsig.vapor = (int)vapor; h->gsig.nP = h->S.nP; h->gsig.P = h->P;
-    h->gsig.unet = (int)h->unetOn;
+    h->gsig.unet = (int)h->unetOn; h->gsig.balls = h->nBalls; h->gsig.clearSv = clearSv;
+    h->gsig.coreR = h->S.coreR; h->gsig.oceanR = h->S.oceanR; h->gsig.spacing = h->S.spacing;
     same = true;
   }
   if (same) {
@@ -811,6 +846,7 @@ static ws_status substep(ws_handle* h, double dt) {
     if ((s = enqueue_substep(h, dt, gsA))) return s;
   }
   h->S.dtLast = dt;
+  h->hadSolidVelocity = h->nBalls > 0;
   h->substepPending = true;           // umax, counts and solve diagnostics are pulled at the next sync
   return WS_OK;
 }
@@ -1040,6 +1076,61 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
   }
   if (s) return s;
   return sync_status(h);
+}
+
+// ------------------------------------------------------------ balls
+// addBall (js/solver.js:3910-3912) and the ball list the app reads back
+// (x y z vx vy vz r rho submerged, js/main.js:713 and the scene's ball meshes)
+static_assert(WS_MAX_BALLS == WS_MAX_BALLS_DEV && sizeof(ws_ball) == 9 * sizeof(double), "ball layout");
+static ws_status ensure_balls(ws_handle* h) {
+  if (h->balls) return WS_OK;
+  const size_t N = (size_t)h->d.nCells;
+  WS_TRY(cudaMalloc(&h->balls, sizeof(ws_ball) * WS_MAX_BALLS));
+  WS_TRY(cudaMalloc(&h->sv, sizeof(float) * 3 * N));
+  WS_TRY(cudaMalloc(&h->ballHist, sizeof(int) * (WS_MAX_BALLS * 24 + WS_MAX_BALLS)));
+  WS_TRY(cudaMalloc(&h->ballSurf, sizeof(float) * WS_MAX_BALLS));
+  WS_TRY(cudaMemsetAsync(h->sv, 0, sizeof(float) * 3 * N, h->stream));
+  WS_TRY(cudaMemsetAsync(h->ballHist, 0, sizeof(int) * (WS_MAX_BALLS * 24 + WS_MAX_BALLS), h->stream));
+  drop_graph(h);                                 // the BC kernels now read the solid-velocity field
+  return WS_OK;
+}
+extern "C" ws_status ws_add_ball(ws_handle* h, double x, double y, double z, double r, double rho) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h) return WS_ERR_INVALID;
+  if (!(r > 0) || !(rho > 0)) return fail(h, WS_ERR_INVALID, "ball radius and density must be positive");
+  if (h->nBalls >= WS_MAX_BALLS) return fail(h, WS_ERR_RANGE, "too many balls");
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  if ((s = ensure_balls(h))) return s;
+  ws_ball b{ x, y, z, 0, 0, 0, r, rho, 0 };
+  WS_TRY(cudaMemcpyAsync(h->balls + 9 * h->nBalls, &b, sizeof(b), cudaMemcpyHostToDevice, h->stream));
+  WS_TRY(cudaStreamSynchronize(h->stream));
+  h->nBalls++;
+  return WS_OK;
+}
+extern "C" ws_status ws_get_balls(ws_handle* h, ws_ball* out, int32_t max, int32_t* count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || !count || (max > 0 && !out)) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  *count = h->nBalls;
+  const int n = std::min(max, h->nBalls);
+  if (n > 0) WS_TRY(cudaMemcpy(out, h->balls, sizeof(ws_ball) * (size_t)n, cudaMemcpyDeviceToHost));
+  return WS_OK;
+}
+extern "C" ws_status ws_set_balls(ws_handle* h, const ws_ball* in, int32_t count) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || count < 0 || (count > 0 && !in)) return WS_ERR_INVALID;
+  if (count > WS_MAX_BALLS) return fail(h, WS_ERR_RANGE, "too many balls");
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  if (count > 0) {
+    if ((s = ensure_balls(h))) return s;
+    WS_TRY(cudaMemcpyAsync(h->balls, in, sizeof(ws_ball) * (size_t)count, cudaMemcpyHostToDevice, h->stream));
+    WS_TRY(cudaStreamSynchronize(h->stream));
+  }
+  h->nBalls = count;
+  return WS_OK;
 }
 
 // ------------------------------------------------------------ interactions
@@ -1354,7 +1445,7 @@ constexpr char kSnapMagic[8] = { 'W', 'S', 'S', 'N', 'A', 'P', '0', '1' };
 struct SnapHeader {
   char magic[8];
   uint32_t version, headerBytes;
-  int32_t nx, ny, nz, nP, terrainN, pad;
+  int32_t nx, ny, nz, nP, terrainN, nBalls;     // nBalls: 0 in version 1
   double dx;
   int64_t totalBytes;
   double Rsl, Rlo, Rhi, landFrac, dv;
@@ -1362,7 +1453,7 @@ struct SnapHeader {
 int64_t snap_bytes(const ws_handle* h, int terrainN) {
   const int64_t nP = h->S.nP, N = h->d.nCells, n3 = (int64_t)terrainN * terrainN * terrainN;
   return (int64_t)sizeof(SnapHeader) + (int64_t)sizeof(ws_params) + (int64_t)sizeof(ws_scalars) +
-         nP * (13 * 4 + 3) + N * 4 + n3 * 5;
+         nP * (13 * 4 + 3) + N * 4 + n3 * 5 + (int64_t)h->nBalls * (int64_t)sizeof(ws_ball);
 }
 }  // namespace
 
@@ -1379,8 +1470,9 @@ extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int6
   unsigned char* p = (unsigned char*)buf;
   SnapHeader hd{};
   std::memcpy(hd.magic, kSnapMagic, 8);
-  hd.version = 1; hd.headerBytes = sizeof(SnapHeader);
+  hd.version = 2; hd.headerBytes = sizeof(SnapHeader);
   hd.nx = h->d.nx; hd.ny = h->d.ny; hd.nz = h->d.nz; hd.nP = h->S.nP; hd.terrainN = tn; hd.dx = h->d.dx;
+  hd.nBalls = h->nBalls;
   hd.totalBytes = need;
   if (tn) { const auto& T = h->hostTerrain; hd.Rsl = T.Rsl; hd.Rlo = T.Rlo; hd.Rhi = T.Rhi; hd.landFrac = T.landFrac; hd.dv = T.dv; }
   std::memcpy(p, &hd, sizeof hd); p += sizeof hd;
@@ -1401,6 +1493,7 @@ extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int6
     std::memcpy(p, T.solid.data(), n3); p += n3;
     std::memcpy(p, T.R.data(), 4 * n3); p += 4 * n3;
   }
+  if (h->nBalls) WS_TRY(cudaMemcpy(p, h->balls, sizeof(ws_ball) * (size_t)h->nBalls, cudaMemcpyDeviceToHost));
   return WS_OK;
 }
 
@@ -1412,8 +1505,11 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
   if (size < (int64_t)sizeof(SnapHeader)) return fail(h, WS_ERR_INVALID, "not a snapshot");
   SnapHeader hd;
   std::memcpy(&hd, buf, sizeof hd);
-  if (std::memcmp(hd.magic, kSnapMagic, 8) != 0 || hd.version != 1 || hd.headerBytes != sizeof(SnapHeader))
-    return fail(h, WS_ERR_INVALID, "not a version-1 snapshot");
+  if (std::memcmp(hd.magic, kSnapMagic, 8) != 0 || (hd.version != 1 && hd.version != 2) ||
+      hd.headerBytes != sizeof(SnapHeader))
+    return fail(h, WS_ERR_INVALID, "not a version-1 or -2 snapshot");
+  if (hd.nBalls < 0 || hd.nBalls > WS_MAX_BALLS || (hd.version == 1 && hd.nBalls != 0))
+    return fail(h, WS_ERR_INVALID, "bad ball count");
   if (hd.nx != h->d.nx || hd.ny != h->d.ny || hd.nz != h->d.nz || hd.dx != h->d.dx)
     return fail(h, WS_ERR_INVALID, "snapshot grid differs from this handle's");
   if (hd.nP < 0 || hd.nP > h->capacity) return fail(h, WS_ERR_RANGE, "snapshot holds more particles than the capacity");
@@ -1422,7 +1518,7 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
   std::memcpy(&S, (const unsigned char*)buf + sizeof hd + sizeof(ws_params), sizeof S);
   const int64_t nP = hd.nP, N = h->d.nCells, n3 = (int64_t)hd.terrainN * hd.terrainN * hd.terrainN;
   const int64_t need = (int64_t)sizeof hd + (int64_t)sizeof(ws_params) + (int64_t)sizeof(ws_scalars) +
-                       nP * (13 * 4 + 3) + N * 4 + n3 * 5;
+                       nP * (13 * 4 + 3) + N * 4 + n3 * 5 + (int64_t)hd.nBalls * (int64_t)sizeof(ws_ball);
   if (size != need || hd.totalBytes != need || S.nP != hd.nP) return fail(h, WS_ERR_INVALID, "snapshot size mismatch");
   const unsigned char* p = (const unsigned char*)buf + sizeof hd;
   const unsigned char* fields = p + sizeof(ws_params) + sizeof(ws_scalars);
@@ -1446,7 +1542,9 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
   if ((s = ws_upload_state(h, &a))) return s;
   WS_TRY(cudaMemcpyAsync(h->q, qp, sizeof(float) * (size_t)N, cudaMemcpyHostToDevice, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
-  return WS_OK;
+  // the balls (version 2) follow the terrain; their solid cells are rebuilt
+  // by the next substep's raster
+  return ws_set_balls(h, (const ws_ball*)(qp + 4 * N + n3 * 5), hd.nBalls);
 }
 
 // network blob: header, gain, Adam step count, then params, Adam m and v (FP32)

@@ -158,8 +158,17 @@ void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t
   k_p2g<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P);
 }
 
+// Solid-adjacent interior face: the velocity of the solid cell beside it,
+// the left one first (_applyBCSlice, js/solver.js:1153-1170): 0 for rock and
+// the domain shell, the ball's velocity for a ball cell.
+__device__ __forceinline__ float solid_face_velocity(const Dims& d, const GridDev& g, int comp, long long cL, long long cR) {
+  if (!g.sv) return 0.f;
+  const long long c = g.type[cL] == WS_SOLID ? cL : cR;
+  return g.sv[comp * d.nCells + c];
+}
+
 // ------------------------------------------------------------ 4. faces pass 1
-// _p2gNormalizeFace (:1109-1120) + _applyBC (:1130-1171, no moving solids)
+// _p2gNormalizeFace (:1109-1120) + _applyBC (:1130-1171)
 // + FLIP snapshot (:2579) + the extrapolation valid mark (:1578-1611).
 // Bytes: 8F read + 4F vel + 4F velO + 1F valid + 2 type reads per face.
 __global__ void k_faces_normalize_bc(Dims d, GridDev g) {
@@ -171,8 +180,8 @@ __global__ void k_faces_normalize_bc(Dims d, GridDev g) {
   FaceIJK F = decode_face(d, f);
   long long cL = 0, cR = 0;
   bool solidAdj = face_cells(d, F, cL, cR);
-  if (!solidAdj) solidAdj = g.type[cL] == WS_SOLID || g.type[cR] == WS_SOLID;
-  if (solidAdj) u = 0.f;
+  if (solidAdj) u = 0.f;                                   // domain boundary plane
+  else if (g.type[cL] == WS_SOLID || g.type[cR] == WS_SOLID) { solidAdj = true; u = solid_face_velocity(d, g, F.comp, cL, cR); }
   g.vel[f] = u;
   g.velO[f] = u;
   g.valid[f] = ((double)a.y > 1e-8 || solidAdj) ? 1 : 0;
@@ -192,7 +201,7 @@ __global__ void k_faces_forces(Dims d, GridDev g, double coef, int viscOn, doubl
   long long cL = 0, cR = 0;
   if (face_cells(d, F, cL, cR)) { g.vel[f] = 0.f; return; }
   int tL = g.type[cL], tR = g.type[cR];
-  if (tL == WS_SOLID || tR == WS_SOLID) { g.vel[f] = 0.f; return; }
+  if (tL == WS_SOLID || tR == WS_SOLID) { g.vel[f] = solid_face_velocity(d, g, F.comp, cL, cR); return; }
   const float* __restrict__ o = g.velO;
   float u = o[f];
   if (viscOn && tL == WS_FLUID && tR == WS_FLUID) {

@@ -48,6 +48,10 @@ struct PartsDev {
   int nP;
 };
 
+// balls (addBall): capacity, and the scalars _updateBalls reads
+#define WS_MAX_BALLS_DEV 64
+struct BallEnv { double coreR, oceanR, gravity; };
+
 // render-side particle prep (WaterScene.updateParticles): the scene state
 // resolved on the host, per-class alpha/size/sprite already float
 struct RenderCfg {
@@ -92,6 +96,7 @@ struct GridDev {
   float *q, *rhs, *pw;
   float *vfx, *vfy, *vfz, *omg, *omx, *omy, *omz;
   float* dens;
+  const float* sv;          // solid velocity (3 x nCells: x, y, z) of moving solids, or null
 };
 
 // ---------------------------------------------------------------- helpers

@@ -70,6 +70,13 @@ void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2*
                     long long maxVerts, float* pos, float* nrm, cudaStream_t s);
 // render-side particle prep: classify, bucket-sort far to near, emit the
 // draw list (ws_render.cu); counts land in the first five scratch words
+// balls (ws_balls.cu): moving-solid raster (after the static raster),
+// particle push-out, and the per-substep histogram + integration
+void launch_ball_raster(const Dims& d, uint8_t* type, float* sv, bool clearSv, const double* balls, int nb,
+                        cudaStream_t s);
+void launch_ball_push(const PartsDev& P, const double* balls, int nb, cudaStream_t s);
+void launch_ball_update(const Dims& d, const float* vel, const TerrainDev& t, const PartsDev& P, double* balls, int nb,
+                        int* hist, float* surfY, const BallEnv& env, double dt, cudaStream_t s);
 // Metaballs.build's corner field on an (m+1)^3 lattice of spacing mdx
 // (FP64 accumulation, float result); 1 or 2 launches
 void launch_metaball_field(const PartsDev& P, int m, double mdx, double R2, int rad, double* acc, float* field,

@@ -163,7 +163,7 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_unet_save", "ws_unet_load", "ws_surface_mesh", "ws_surface_download", "ws_surface_device",
            "ws_render_particles", "ws_render_download", "ws_render_device",
            "ws_metaball_mesh", "ws_metaball_download", "ws_metaball_device", "ws_metaball_field",
-           "ws_step_async", "ws_step_poll", "ws_step_wait"]
+           "ws_step_async", "ws_step_poll", "ws_step_wait", "ws_add_ball", "ws_get_balls", "ws_set_balls"]
 
 
 def load_library(path=None):
@@ -213,6 +213,9 @@ def load_library(path=None):
         "ws_surface_mesh": [h, d, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
         "ws_surface_download": [h, vp, vp, i64],
         "ws_surface_device": [h, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_int64)],
+        "ws_add_ball": [h, d, d, d, d, d],
+        "ws_get_balls": [h, vp, i32, C.POINTER(C.c_int32)],
+        "ws_set_balls": [h, vp, i32],
         "ws_step_async": [h, d],
         "ws_step_poll": [h, C.POINTER(C.c_int32)],
         "ws_step_wait": [h],
@@ -286,6 +289,24 @@ class FluidSolver:
             self.close()
         except Exception:
             pass
+
+    # ---- balls: addBall (js/solver.js:3910); rows x y z vx vy vz r rho submerged
+    def addBall(self, x, y, z, r, rho):
+        self._check(self._L.ws_add_ball(self._h, float(x), float(y), float(z), float(r), float(rho)))
+
+    add_ball = addBall
+
+    @property
+    def balls(self):
+        """(n, 9) float64: x y z vx vy vz r rho submerged of every ball."""
+        cnt = C.c_int32()
+        out = np.zeros((64, 9))
+        self._check(self._L.ws_get_balls(self._h, out.ctypes.data, 64, C.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def set_balls(self, rows):
+        a = np.ascontiguousarray(rows, np.float64).reshape(-1, 9)
+        self._check(self._L.ws_set_balls(self._h, a.ctypes.data if len(a) else None, len(a)))
 
     def step_async(self, dtFrame):
         """Start step(dtFrame) on the handle's worker thread; False (nothing
