@@ -211,6 +211,7 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   d.cx = d.W / 2; d.cy = d.H / 2; d.cz = d.D / 2;
   d.domainR = 0.5 * std::min(std::min(d.W, d.H), d.D) - d.dx;
   d.nCells = (long long)d.nx * d.ny * d.nz;
+  dims_fastdiv(d);
   d.uN = (long long)(d.nx + 1) * d.ny * d.nz; d.vN = (long long)d.nx * (d.ny + 1) * d.nz;
   d.wN = (long long)d.nx * d.ny * (d.nz + 1); d.F = d.uN + d.vN + d.wN;
   h->capacity = cfg->capacity;
@@ -1691,6 +1692,7 @@ extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detai
   if ((s = check_launch(h, h->S.nP ? 2 : 1))) return s;
   Dims dd = h->d;
   dd.nx = dd.ny = dd.nz = m; dd.dx = mdx; dd.nCells = cells;
+  dims_fastdiv(dd);
   return mt_build(h, dd, h->mbField, iso, h->mbPartials, h->mball, vertices, volume);
 }
 extern "C" ws_status ws_metaball_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {

@@ -13,19 +13,23 @@ __device__ __forceinline__ FaceIJK decode_face(const Dims& d, long long f64) {
   unsigned f = (unsigned)f64, nx = d.nx, ny = d.ny, uN = (unsigned)d.uN, vN = (unsigned)d.vN;
   if (f < uN) {
     r.comp = 0; r.local = f;
-    unsigned t = f / (nx + 1); r.i = (int)(f - t * (nx + 1)); unsigned k = t / ny; r.j = (int)(t - k * ny); r.k = (int)k;
+    unsigned t = fastdiv(f, d.dnx1); r.i = (int)(f - t * (nx + 1));
+    unsigned k = fastdiv(t, d.dny); r.j = (int)(t - k * ny); r.k = (int)k;
   } else if (f < uN + vN) {
     unsigned g = f - uN; r.comp = 1; r.local = g;
-    unsigned t = g / nx; r.i = (int)(g - t * nx); unsigned k = t / (ny + 1); r.j = (int)(t - k * (ny + 1)); r.k = (int)k;
+    unsigned t = fastdiv(g, d.dnx); r.i = (int)(g - t * nx);
+    unsigned k = fastdiv(t, d.dny1); r.j = (int)(t - k * (ny + 1)); r.k = (int)k;
   } else {
     unsigned g = f - uN - vN; r.comp = 2; r.local = g;
-    unsigned t = g / nx; r.i = (int)(g - t * nx); unsigned k = t / ny; r.j = (int)(t - k * ny); r.k = (int)k;
+    unsigned t = fastdiv(g, d.dnx); r.i = (int)(g - t * nx);
+    unsigned k = fastdiv(t, d.dny); r.j = (int)(t - k * ny); r.k = (int)k;
   }
   return r;
 }
 __device__ __forceinline__ void decode_cell(const Dims& d, long long c64, int& i, int& j, int& k) {
   unsigned c = (unsigned)c64, nx = d.nx, ny = d.ny;
-  unsigned t = c / nx; i = (int)(c - t * nx); unsigned kk = t / ny; j = (int)(t - kk * ny); k = (int)kk;
+  unsigned t = fastdiv(c, d.dnx); i = (int)(c - t * nx);
+  unsigned kk = fastdiv(t, d.dny); j = (int)(t - kk * ny); k = (int)kk;
 }
 // the two cells a face separates; boundary=true for the domain planes
 __device__ __forceinline__ bool face_cells(const Dims& d, const FaceIJK& F, long long& cL, long long& cR) {

@@ -29,11 +29,34 @@
 #define WS_DERR_RANGE 2
 #define WS_DERR_TIMEOUT 4
 
+// Division by an invariant divisor for dividends below 2^31: q = n / d as a
+// multiply-high and a shift, m = ceil(2^(31 + l) / d) with l = ceil(log2 d)
+// (the error n (m - 2^(31+l)/d) / 2^(31+l) stays below 1/d, so the floor is
+// exact). Used to turn flat cell and face indices back into (i, j, k).
+struct FastDiv { unsigned m; int s; unsigned d; };
+inline FastDiv fastdiv_make(unsigned d) {
+  FastDiv f{ 0u, 0, d };
+  if (d <= 1) return f;
+  int l = 0;
+  while ((1ull << l) < d) l++;
+  f.m = (unsigned)(((1ull << (31 + l)) + d - 1) / d);
+  f.s = l - 1;
+  return f;
+}
+__device__ __forceinline__ unsigned fastdiv(unsigned n, const FastDiv& f) {
+  return f.d <= 1 ? n : (__umulhi(n, f.m) >> f.s);
+}
+
 struct Dims {
   int nx, ny, nz;
   double dx, W, H, D, cx, cy, cz, domainR;
   long long nCells, uN, vN, wN, F;
+  FastDiv dnx, dnx1, dny, dny1;   // nx, nx + 1, ny, ny + 1
 };
+inline void dims_fastdiv(Dims& d) {
+  d.dnx = fastdiv_make((unsigned)d.nx); d.dnx1 = fastdiv_make((unsigned)d.nx + 1);
+  d.dny = fastdiv_make((unsigned)d.ny); d.dny1 = fastdiv_make((unsigned)d.ny + 1);
+}
 
 struct TerrainDev {
   int n, has;

@@ -44,7 +44,7 @@ struct SorLists {
 __device__ __forceinline__ int sor_colour(const Dims& d, const float* __restrict__ pw, unsigned c) {
   if (c >= (unsigned)d.nCells || pw[c] < 0.f) return -1;
   unsigned nx = d.nx, ny = d.ny;
-  unsigned t = c / nx, i = c - t * nx, k = t / ny, j = t - k * ny;
+  unsigned t = fastdiv(c, d.dnx), i = c - t * nx, k = fastdiv(t, d.dny), j = t - k * ny;
   if (i < 1 || j < 1 || k < 1 || i + 2 > nx || j + 2 > ny || (int)k + 2 > d.nz) return -1;
   return (int)((i + j + k) & 1u);
 }
