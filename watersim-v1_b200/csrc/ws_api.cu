@@ -478,6 +478,7 @@ static ws_status terrain_to_device(ws_handle* h) {
   TerrainDev& t = h->terr;
   t.n = T.n; t.has = 1; t.dv = T.dv; t.Rsl = T.Rsl; t.Rlo = T.Rlo; t.Rhi = T.Rhi;
   t.Rlo2 = T.Rlo * T.Rlo; t.Rhi2 = T.Rhi * T.Rhi; t.solid = h->tsolid; t.R = h->tR;
+  t.rdv = 1.0 / T.dv; t.dvPow2 = is_pow2(T.dv) ? 1 : 0;
   h->S.landFrac = T.landFrac;
   h->hasTerrain = true;
   launch_static_types(h->d, t, h->S.coreR, h->staticTypes, h->stream);

@@ -118,9 +118,9 @@ __global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double
       !(t.has && rock_cell_at(d, g.staticTypes, X, Y, Z))) {
     P.pflag[p] = 1; return;
   }
-  int i = jfloor_clamp(X / d.dx, 0, d.nx - 1);
-  int j = jfloor_clamp(Y / d.dx, 0, d.ny - 1);
-  int k = jfloor_clamp(Z / d.dx, 0, d.nz - 1);
+  int i = jfloor_clamp(over_dx(d, X), 0, d.nx - 1);
+  int j = jfloor_clamp(over_dx(d, Y), 0, d.ny - 1);
+  int k = jfloor_clamp(over_dx(d, Z), 0, d.nz - 1);
   if (j >= d.ny - 2) {
     if (sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > 0.3) { P.pflag[p] = 1; return; }
   }

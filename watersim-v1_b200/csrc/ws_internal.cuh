@@ -15,6 +15,7 @@
 // reference (JavaScript doubles over Float32Array storage); the library is
 // built with -fmad=false because JavaScript never fuses a multiply-add.
 #pragma once
+#include <cmath>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
@@ -52,15 +53,24 @@ struct Dims {
   double dx, W, H, D, cx, cy, cz, domainR;
   long long nCells, uN, vN, wN, F;
   FastDiv dnx, dnx1, dny, dny1;   // nx, nx + 1, ny, ny + 1
+  double rdx; int dxPow2;         // 1 / dx, and whether dx is a power of two
 };
+// A power-of-two divisor b = 2^k: a / b and a * 2^-k are both the correctly
+// rounded value of the same real number, so the product is bit-identical to
+// the quotient (subnormal and overflowing results included).
+inline bool is_pow2(double b) { int e; return b > 0 && std::frexp(b, &e) == 0.5; }
 inline void dims_fastdiv(Dims& d) {
   d.dnx = fastdiv_make((unsigned)d.nx); d.dnx1 = fastdiv_make((unsigned)d.nx + 1);
   d.dny = fastdiv_make((unsigned)d.ny); d.dny1 = fastdiv_make((unsigned)d.ny + 1);
+  d.dxPow2 = is_pow2(d.dx) ? 1 : 0; d.rdx = 1.0 / d.dx;
 }
+// v / dx, exactly as the division rounds
+__device__ __forceinline__ double over_dx(const Dims& d, double v) { return d.dxPow2 ? v * d.rdx : v / d.dx; }
 
 struct TerrainDev {
   int n, has;
   double dv, Rsl, Rlo, Rhi, Rlo2, Rhi2;
+  double rdv; int dvPow2;         // 1 / dv and whether dv is a power of two (see is_pow2)
   const uint8_t* __restrict__ solid;
   const float* __restrict__ R;
 };
@@ -150,7 +160,9 @@ __host__ __device__ __forceinline__ uint32_t lcg_jump(uint32_t s, uint32_t k) {
 __device__ __forceinline__ double terrain_radius_at(const TerrainDev& t, double coreR, double x, double y, double z) {
   if (!t.has) return coreR;
   int n = t.n; double dv = t.dv;
-  double gx = x / dv - 0.5, gy = y / dv - 0.5, gz = z / dv - 0.5;
+  double gx, gy, gz;
+  if (t.dvPow2) { gx = x * t.rdv - 0.5; gy = y * t.rdv - 0.5; gz = z * t.rdv - 0.5; }
+  else { gx = x / dv - 0.5; gy = y / dv - 0.5; gz = z / dv - 0.5; }
   int i = jtrunc(gx), j = jtrunc(gy), k = jtrunc(gz);
   if (i < 0) i = 0; else if (i > n - 2) i = n - 2;
   if (j < 0) j = 0; else if (j > n - 2) j = n - 2;
@@ -175,7 +187,7 @@ __device__ __forceinline__ double terrain_radius_at(const TerrainDev& t, double 
 // cell equals the voxel at the cell centre (rock) for interior cells.
 __device__ __forceinline__ bool rock_cell_at(const Dims& d, const uint8_t* __restrict__ staticTypes,
                                              double x, double y, double z) {
-  int i = jtrunc(x / d.dx), j = jtrunc(y / d.dx), k = jtrunc(z / d.dx);
+  int i = jtrunc(over_dx(d, x)), j = jtrunc(over_dx(d, y)), k = jtrunc(over_dx(d, z));
   if (i < 1) i = 1; else if (i > d.nx - 2) i = d.nx - 2;
   if (j < 1) j = 1; else if (j > d.ny - 2) j = d.ny - 2;
   if (k < 1) k = 1; else if (k > d.nz - 2) k = d.nz - 2;
@@ -185,10 +197,11 @@ __device__ __forceinline__ bool rock_cell_at(const Dims& d, const uint8_t* __res
 // Face-grid coordinates of component comp, js/solver.js:737-748
 __device__ __forceinline__ void face_coords(const Dims& d, int comp, double x, double y, double z,
                                             int& i0, int& j0, int& k0, double& tx, double& ty, double& tz) {
-  double a, b, c, dx = d.dx;
-  if (comp == 0) { a = x / dx; b = y / dx - 0.5; c = z / dx - 0.5; }
-  else if (comp == 1) { a = x / dx - 0.5; b = y / dx; c = z / dx - 0.5; }
-  else { a = x / dx - 0.5; b = y / dx - 0.5; c = z / dx; }
+  double a, b, c;
+  const double X = over_dx(d, x), Y = over_dx(d, y), Z = over_dx(d, z);
+  if (comp == 0) { a = X; b = Y - 0.5; c = Z - 0.5; }
+  else if (comp == 1) { a = X - 0.5; b = Y; c = Z - 0.5; }
+  else { a = X - 0.5; b = Y - 0.5; c = Z; }
   double fi = floor(a), fj = floor(b), fk = floor(c);
   if (fi < 0) { i0 = 0; tx = 0; } else if (fi > d.nx - 1) { i0 = d.nx - 1; tx = 1; } else { i0 = (int)fi; tx = a - fi; }
   if (fj < 0) { j0 = 0; ty = 0; } else if (fj > d.ny - 2) { j0 = d.ny - 2; ty = 1; } else { j0 = (int)fj; ty = b - fj; }

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(256) k_g2p_advect(Dims d, GridDev g, PartsDev 
         double psc = maxSpeed / sqrt(pv2);
         fvx = (float)(fvx * psc); fvy = (float)(fvy * psc); fvz = (float)(fvz * psc);
       }
-      int ci = jfloor_clamp(x / dx, 0, d.nx - 1), cj = jfloor_clamp(y / dx, 0, d.ny - 1), ck = jfloor_clamp(z / dx, 0, d.nz - 1);
+      int ci = jfloor_clamp(over_dx(d, x), 0, d.nx - 1), cj = jfloor_clamp(over_dx(d, y), 0, d.ny - 1), ck = jfloor_clamp(over_dx(d, z), 0, d.nz - 1);
       long long c = ((long long)ck * d.ny + cj) * d.nx + ci; long long nxy = (long long)d.nx * d.ny;
       const uint8_t* type = g.type;
       if (type[c] == WS_AIR) {
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) k_g2p_advect(Dims d, GridDev g, PartsDev 
         if (rock_cell_at(d, g.staticTypes, x, y, z)) {
           P.pAir[p] = 1.f; fvx = fvy = fvz = 0.f;
         } else {
-          double ciF = floor(x / dx), cjF = floor(y / dx), ckF = floor(z / dx);
+          double ciF = floor(over_dx(d, x)), cjF = floor(over_dx(d, y)), ckF = floor(over_dx(d, z));
           if (ciF >= 0 && cjF >= 0 && ckF >= 0 && ciF < d.nx && cjF < d.ny && ckF < d.nz &&
               g.type[((long long)ckF * d.ny + (long long)cjF) * d.nx + (long long)ciF] == WS_FLUID) {
             double exF = x - cx, eyF = y - cy, ezF = z - cz;
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) k_g2p_advect(Dims d, GridDev g, PartsDev 
             double stepF = dx * 0.5;
             for (int mf = 0; mf < 12; mf++) {
               double qx = x + exF / elF * stepF, qy = y + eyF / elF * stepF, qz = z + ezF / elF * stepF;
-              double qi = floor(qx / dx), qj = floor(qy / dx), qk = floor(qz / dx);
+              double qi = floor(over_dx(d, qx)), qj = floor(over_dx(d, qy)), qk = floor(over_dx(d, qz));
               if (qi < 0 || qj < 0 || qk < 0 || qi >= d.nx || qj >= d.ny || qk >= d.nz) break;
               if (g.type[((long long)qk * d.ny + (long long)qj) * d.nx + (long long)qi] != WS_FLUID) break;
               x = qx; y = qy; z = qz;
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(256) k_g2p_advect(Dims d, GridDev g, PartsDev 
           fl = 0;
         }
       }
-      int ci = jfloor_clamp(x / dx, 0, d.nx - 1), cj = jfloor_clamp(y / dx, 0, d.ny - 1), ck = jfloor_clamp(z / dx, 0, d.nz - 1);
+      int ci = jfloor_clamp(over_dx(d, x), 0, d.nx - 1), cj = jfloor_clamp(over_dx(d, y), 0, d.ny - 1), ck = jfloor_clamp(over_dx(d, z), 0, d.nz - 1);
       if (g.type[((long long)ck * d.ny + cj) * d.nx + ci] == WS_FLUID) {
         fvx = (float)(fvx * 0.45); fvy = (float)(fvy * 0.45); fvz = (float)(fvz * 0.45);
         if (fvy > 0.5f) fvy = 0.5f;
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(1024) k_vapor_advect(Dims d, GridDev g, PartsD
         }
         fvx = (float)(fvx * 0.92); fvy = (float)(fvy * 0.92); fvz = (float)(fvz * 0.92);
       }
-      int ciV = jfloor_clamp(x / dx, 0, d.nx - 1), cjV = jfloor_clamp(y / dx, 0, d.ny - 1), ckV = jfloor_clamp(z / dx, 0, d.nz - 1);
+      int ciV = jfloor_clamp(over_dx(d, x), 0, d.nx - 1), cjV = jfloor_clamp(over_dx(d, y), 0, d.ny - 1), ckV = jfloor_clamp(over_dx(d, z), 0, d.nz - 1);
       bool backToSea = g.type[((long long)ckV * d.ny + cjV) * d.nx + ciV] == WS_FLUID;
       if (backToSea) {
         double bx2 = x - cx, by2 = y - cy, bz2 = z - cz;
