@@ -115,3 +115,22 @@ def test_tolerance_mode_sor():
     assert sg.sorIters == so.sorIters
     assert sg.sorRelRes <= 1e-5
     assert abs(sg.sorRelRes - so.sorRelRes) <= 1e-3 * so.sorRelRes
+
+
+def test_repeated_solves_on_one_system():
+    """The SOR list build reads the per-block colour counts the pressure setup
+    wrote and scans them into separate offsets, so the solve can run again on
+    the same system (ws_time_kernel repeats it) and the substep after it is
+    unchanged by that."""
+    o = planet("planet32", **PLAIN32)
+    o.set_scalars(gRamp=1.5)
+    a, b = to_device(o), to_device(o)
+    a._substep(0.01)
+    b._substep(0.01)
+    b.time_kernel(6, 4)                 # four more solves of the last system, no setup in between
+    assert np.all(np.isfinite(b.q))
+    a._substep(0.01)
+    b._substep(0.01)
+    assert np.array_equal(a.cellType, b.cellType)
+    assert a.scalars.nFluid == b.scalars.nFluid
+    assert rel_err(b.download("u"), a.download("u")) <= 1e-4

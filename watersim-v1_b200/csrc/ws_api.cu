@@ -700,7 +700,7 @@ static ws_status stage_forces(ws_handle* h, double dt, double gsA) {
 // FP64 residual land in the status word and are read at the next sync.
 static ws_status stage_pressure(ws_handle* h) {
   GridDev g = grid_of(h);
-  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, h->stream);
+  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, sor_block_counts(h->sor), h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
   bool tolMode = h->P.sorTol > 0;
   int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
@@ -719,7 +719,7 @@ static ws_status stage_pressure(ws_handle* h) {
   e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
                                    &h->st->err, &dIters, &dRel, &dPath, h->stream);
   if (e != cudaSuccess) return fail_cuda(h, e, "SOR solve launch");
-  s = check_launch(h, 4); if (s) return s;
+  s = check_launch(h, sor_solve_launches(h->sor)); if (s) return s;
   WS_TRY(cudaMemcpyAsync(&h->st->sorIters, dIters, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(&h->st->relres, dRel, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(&h->st->pad2, dPath, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
@@ -1219,7 +1219,7 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
                 cudaError_t e6 = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
                                                   &h->st->err, &di, &dr, &dp, h->stream);
                 if (e6 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e6, "SOR solve"); }
-                h->launches += 3; } break;                     // list build; timed per whole solve
+                h->launches += sor_solve_launches(h->sor) - 1; } break;   // list build; timed per whole solve
       default: cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(h, WS_ERR_INVALID, "unknown kernel id");
     }
   }
@@ -1369,7 +1369,7 @@ extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* re
   ws_status s = net_ready(h); if (s) return s;
   if (!(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain");
   GridDev g = grid_of(h);
-  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, h->stream);
+  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, sor_block_counts(h->sor), h->stream);
   if ((s = check_launch(h, 1))) return s;
   launch_residual(h->d, g, h->diag8, h->partials, h->st, nullptr, h->stream);
   if ((s = check_launch(h, 2))) return s;

@@ -237,30 +237,53 @@ void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscO
 // ------------------------------------------------------------ 6. pressure setup
 // _pressureSolve passes 1-2, js/solver.js:1321-1366: q = 0 off the fluid,
 // diag = Nf + Na, rhs = -dx^2 div, relaxation weight pw = omega/diag
-// (float32, as the reference's pW). pw < 0 marks a non-fluid cell.
-__global__ void k_pressure_setup(Dims d, GridDev g, uint8_t* __restrict__ diag8, double omega, DevStatus* st) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= d.nCells) return;
-  const uint8_t* type = g.type;
-  if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; return; }
-  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-  int i, j, k; decode_cell(d, c, i, j, k);
-  long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
-                       j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
-  int cnt = 0;
+// (float32, as the reference's pW). pw < 0 marks a non-fluid cell. Each
+// 256-cell block also counts its interior fluid cells per colour for the SOR
+// list build (sorCounts[2 b], [2 b + 1]; null skips) and adds its fluid
+// cells to the fluid count with one atomic.
+__global__ void __launch_bounds__(256) k_pressure_setup(Dims d, GridDev g, uint8_t* __restrict__ diag8, double omega,
+                                                        DevStatus* st, int* __restrict__ sorCounts) {
+  __shared__ int wc[3][8];                           // per warp: colour-0 and colour-1 list cells, fluid cells
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int col = -1, fluid = 0;
+  if (c < d.nCells) {
+    const uint8_t* type = g.type;
+    if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; }
+    else {
+      int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+      int i, j, k; decode_cell(d, c, i, j, k);
+      long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
+                           j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
+      int cnt = 0;
 #pragma unroll
-  for (int q = 0; q < 6; q++) if (nbr[q] >= 0 && type[nbr[q]] != WS_SOLID) cnt++;
-  const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
-  double div = ((double)u[((long long)k * ny + j) * (nx + 1) + i + 1] - (double)u[((long long)k * ny + j) * (nx + 1) + i] +
-                (double)v[((long long)k * (ny + 1) + j + 1) * nx + i] - (double)v[((long long)k * (ny + 1) + j) * nx + i] +
-                (double)w[((long long)(k + 1) * ny + j) * nx + i] - (double)w[((long long)k * ny + j) * nx + i]) / d.dx;
-  g.rhs[c] = (float)(-d.dx * d.dx * div);
-  g.pw[c] = (float)(cnt > 0 ? omega / (double)cnt : 0.0);
-  diag8[c] = (uint8_t)cnt;
-  atomicAdd(&st->nFluid, 1);
+      for (int q = 0; q < 6; q++) if (nbr[q] >= 0 && type[nbr[q]] != WS_SOLID) cnt++;
+      const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
+      double div = ((double)u[((long long)k * ny + j) * (nx + 1) + i + 1] - (double)u[((long long)k * ny + j) * (nx + 1) + i] +
+                    (double)v[((long long)k * (ny + 1) + j + 1) * nx + i] - (double)v[((long long)k * (ny + 1) + j) * nx + i] +
+                    (double)w[((long long)(k + 1) * ny + j) * nx + i] - (double)w[((long long)k * ny + j) * nx + i]) / d.dx;
+      g.rhs[c] = (float)(-d.dx * d.dx * div);
+      g.pw[c] = (float)(cnt > 0 ? omega / (double)cnt : 0.0);
+      diag8[c] = (uint8_t)cnt;
+      fluid = 1;
+      // membership of the SOR colour lists: interior fluid cells (sor_colour)
+      if (i >= 1 && j >= 1 && k >= 1 && i + 2 <= nx && j + 2 <= ny && k + 2 <= nz) col = (i + j + k) & 1;
+    }
+  }
+  const unsigned full = 0xffffffffu;
+  const unsigned m0 = __ballot_sync(full, col == 0), m1 = __ballot_sync(full, col == 1), mf = __ballot_sync(full, fluid);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { wc[0][wid] = __popc(m0); wc[1][wid] = __popc(m1); wc[2][wid] = __popc(mf); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int a = 0, b = 0, f = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a += wc[0][q]; b += wc[1][q]; f += wc[2][q]; }
+    if (sorCounts) { sorCounts[2 * blockIdx.x] = a; sorCounts[2 * blockIdx.x + 1] = b; }
+    if (f) atomicAdd(&st->nFluid, f);
+  }
 }
-void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, cudaStream_t s) {
-  k_pressure_setup<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, g, diag8, omega, st);
+void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, int* sorCounts,
+                           cudaStream_t s) {
+  k_pressure_setup<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, g, diag8, omega, st, sorCounts);
 }
 
 // ------------------------------------------------------------ 7. red-black SOR

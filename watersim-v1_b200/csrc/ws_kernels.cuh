@@ -30,7 +30,8 @@ void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s);
 void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s);
 void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s);
-void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, cudaStream_t s);
+void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, int* sorCounts,
+                           cudaStream_t s);
 void launch_sor_color(const Dims& d, const GridDev& g, int color, double om1, cudaStream_t s);
 int residual_blocks(const Dims& d);
 void launch_residual(const Dims& d, const GridDev& g, const uint8_t* diag8, double2* partials,
@@ -91,6 +92,9 @@ void sor_free(void* statePtr);
 cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
                              int iters, int check, double tol, int* err, int** outIters, double** outRel,
                              int** outPath, cudaStream_t s);
+// per-256-cell-block colour counts the pressure setup fills for the list build
+int* sor_block_counts(void* state);
+int sor_solve_launches(void* state);
 
 // ---- ws_contacts.cu
 void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,

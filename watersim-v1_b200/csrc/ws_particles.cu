@@ -12,7 +12,7 @@
 // streams _cfS/_bfS and are advanced by k_vapor_advect instead.
 // Float locals fvx/fvy/fvz hold the float32 array contents (every store of
 // the reference rounds to float32); positions are JS doubles until stored.
-__global__ void __launch_bounds__(256) k_g2p_advect(Dims d, GridDev g, PartsDev P, TerrainDev t,
+__global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsDev P, TerrainDev t,
                                                     AdvectParams ap, DevStatus* st) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   int air = 0;

@@ -48,50 +48,41 @@ __device__ __forceinline__ int sor_colour(const Dims& d, const float* __restrict
   if (i < 1 || j < 1 || k < 1 || i + 2 > nx || j + 2 > ny || (int)k + 2 > d.nz) return -1;
   return (int)((i + j + k) & 1u);
 }
-__global__ void k_sor_count(Dims d, const float* __restrict__ pw, int* __restrict__ blockCounts) {
-  __shared__ int s0, s1;
-  if (threadIdx.x == 0) { s0 = 0; s1 = 0; }
-  __syncthreads();
-  unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
-  int col = sor_colour(d, pw, c);
-  if (col == 1) atomicAdd(&s1, 1); else if (col == 0) atomicAdd(&s0, 1);
-  __syncthreads();
-  if (threadIdx.x == 0) { blockCounts[2 * blockIdx.x] = s0; blockCounts[2 * blockIdx.x + 1] = s1; }
-}
-// exclusive scan of the (colour 0, colour 1) block counts, one block
-__global__ void k_sor_scan(int* __restrict__ blockCounts, int nb, int* __restrict__ total) {
+// exclusive scan of the (colour 0, colour 1) block counts into offs, one
+// block: each thread sums a contiguous segment, the block scans the segment
+// sums, then each thread writes its segment's offsets; total = the two list
+// lengths. The counts stay as the pressure setup wrote them, so the solve can
+// be repeated on the same system.
+__global__ void __launch_bounds__(1024) k_sor_scan(const int* __restrict__ blockCounts, int nb, int* __restrict__ offs,
+                                                   int* __restrict__ total) {
   __shared__ int w0[32], w1[32];
-  __shared__ int carry0, carry1;
-  if (threadIdx.x == 0) { carry0 = 0; carry1 = 0; }
-  __syncthreads();
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int base = 0; base < nb; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    int v0 = i < nb ? blockCounts[2 * i] : 0, v1 = i < nb ? blockCounts[2 * i + 1] : 0;
-    int x0 = v0, x1 = v1;
-    for (int o = 1; o < 32; o <<= 1) {
-      int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
-      if (lane >= o) { x0 += y0; x1 += y1; }
-    }
-    if (lane == 31) { w0[wid] = x0; w1[wid] = x1; }
-    __syncthreads();
-    if (wid == 0) {
-      int a = lane < nw ? w0[lane] : 0, b = lane < nw ? w1[lane] : 0;
-      for (int o = 1; o < 32; o <<= 1) {
-        int ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
-        if (lane >= o) { a += ya; b += yb; }
-      }
-      w0[lane] = a; w1[lane] = b;
-    }
-    __syncthreads();
-    int e0 = x0 - v0 + (wid > 0 ? w0[wid - 1] : 0) + carry0;
-    int e1 = x1 - v1 + (wid > 0 ? w1[wid - 1] : 0) + carry1;
-    if (i < nb) { blockCounts[2 * i] = e0; blockCounts[2 * i + 1] = e1; }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) { carry0 = e0 + v0; carry1 = e1 + v1; }
-    __syncthreads();
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
+  const int per = (nb + blockDim.x - 1) / blockDim.x, lo = min(nb, t * per), hi = min(nb, lo + per);
+  int s0 = 0, s1 = 0;
+  for (int i = lo; i < hi; i++) { s0 += blockCounts[2 * i]; s1 += blockCounts[2 * i + 1]; }
+  int x0 = s0, x1 = s1;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+    if (lane >= o) { x0 += y0; x1 += y1; }
   }
-  if (threadIdx.x == 0) { total[0] = carry0; total[1] = carry1; }
+  if (lane == 31) { w0[wid] = x0; w1[wid] = x1; }
+  __syncthreads();
+  if (wid == 0) {
+    int a = lane < nw ? w0[lane] : 0, b = lane < nw ? w1[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int ya = __shfl_up_sync(0xffffffffu, a, o), yb = __shfl_up_sync(0xffffffffu, b, o);
+      if (lane >= o) { a += ya; b += yb; }
+    }
+    w0[lane] = a; w1[lane] = b;
+  }
+  __syncthreads();
+  int r0 = x0 - s0 + (wid > 0 ? w0[wid - 1] : 0), r1 = x1 - s1 + (wid > 0 ? w1[wid - 1] : 0);
+  for (int i = lo; i < hi; i++) {
+    const int c0 = blockCounts[2 * i], c1 = blockCounts[2 * i + 1];
+    offs[2 * i] = r0; offs[2 * i + 1] = r1;
+    r0 += c0; r1 += c1;
+  }
+  if (t == blockDim.x - 1) { total[0] = w0[nw - 1]; total[1] = w1[nw - 1]; }
 }
 __global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float* __restrict__ rhs,
                               const uint8_t* __restrict__ diag8, const int* __restrict__ offs, SorLists L) {
@@ -471,7 +462,8 @@ static size_t cluster_smem_bytes() { return (size_t)(kSmax + 1) * 2 * 4 + (size_
 // ---------------------------------------------------------------- host side
 struct SorState {
   SorLists L{};
-  int* blockCounts = nullptr;
+  int* blockCounts = nullptr;  // per 256-cell block: interior fluid cells of colour 0, 1 (pressure setup)
+  int* blockOffs = nullptr;    // their exclusive scan: each block's first list slot per colour
   GridBar* bar = nullptr;
   double2* partials = nullptr;
   int* outIters = nullptr;
@@ -522,6 +514,9 @@ cudaError_t sor_init(void** statePtr, long long nCells, int device) {
   }
   cudaGetLastError();                                   // a refused probe is not an error
   if ((e = cudaMalloc(&S->blockCounts, sizeof(int) * 2 * nb)) != cudaSuccess) return e;
+  // zero until the first pressure setup fills them: a solve before it lists no cell
+  if ((e = cudaMemset(S->blockCounts, 0, sizeof(int) * 2 * nb)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->blockOffs, sizeof(int) * 2 * nb)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->bar, sizeof(GridBar))) != cudaSuccess) return e;
   if ((e = cudaMemset(S->bar, 0, sizeof(GridBar))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->partials, sizeof(double2) * (S->grid + 1))) != cudaSuccess) return e;
@@ -531,12 +526,15 @@ cudaError_t sor_init(void** statePtr, long long nCells, int device) {
   return cudaSuccess;
 }
 
+int* sor_block_counts(void* statePtr) { return statePtr ? ((SorState*)statePtr)->blockCounts : nullptr; }
+// kernels one launch_sor_solve issues: scan, scatter, [codes, cluster solve,] grid solve
+int sor_solve_launches(void* statePtr) { return statePtr && ((SorState*)statePtr)->clusterSize ? 5 : 3; }
 void sor_free(void* statePtr) {
   SorState* S = (SorState*)statePtr;
   if (!S) return;
   for (int c = 0; c < 2; c++) { cudaFree(S->L.idx[c]); cudaFree(S->L.rhs[c]); cudaFree(S->L.pw[c]); cudaFree(S->L.dg[c]); cudaFree(S->L.code[c]); }
   cudaFree(S->L.pos);
-  cudaFree(S->L.count); cudaFree(S->blockCounts); cudaFree(S->bar); cudaFree(S->partials);
+  cudaFree(S->L.count); cudaFree(S->blockCounts); cudaFree(S->blockOffs); cudaFree(S->bar); cudaFree(S->partials);
   cudaFree(S->outIters); cudaFree(S->outRel); cudaFree(S->outPath);
   delete S;
 }
@@ -549,10 +547,10 @@ cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, co
                              int** outPath, cudaStream_t s) {
   SorState* S = (SorState*)statePtr;
   *outPath = S->outPath;
+  // the per-block colour counts come from the pressure setup (k_pressure_setup)
   int nb = (int)grid_for(d.nCells, 256);
-  k_sor_count<<<nb, 256, 0, s>>>(d, g.pw, S->blockCounts);
-  k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->L.count);
-  k_sor_scatter<<<nb, 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockCounts, S->L);
+  k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->blockOffs, S->L.count);
+  k_sor_scatter<<<nb, 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockOffs, S->L);
   cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
   int C = S->clusterSize;
   if (C) {
