@@ -569,7 +569,7 @@ __device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz
   return vol;
 }
 // Block partial sums of the signed volume (FP64) and the vertex count.
-__global__ void k_mt_partial(Dims d, const float* __restrict__ dens, double iso, double2* __restrict__ partials) {
+__global__ void __launch_bounds__(128, 8) k_mt_partial(Dims d, const float* __restrict__ dens, double iso, double2* __restrict__ partials) {
   __shared__ double sv[32], sc[32];
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double vol = 0, cnt = 0;
@@ -640,7 +640,7 @@ __global__ void k_mt_offsets(const double2* __restrict__ partials, int nb, long 
     __syncthreads();
   }
 }
-__global__ void k_mt_emit(Dims d, const float* __restrict__ dens, double iso, const long long* __restrict__ offs,
+__global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restrict__ dens, double iso, const long long* __restrict__ offs,
                           long long maxVerts, float* __restrict__ pos, float* __restrict__ nrm) {
   __shared__ int ws[4];
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
