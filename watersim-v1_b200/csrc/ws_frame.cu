@@ -504,8 +504,10 @@ __constant__ int c_cases[16][2][3] = {
 // one cell of MarchingTetrahedra.build (js/surface.js:66-177): its signed
 // volume, its vertex count and, when pos/nrm are given, its vertices
 // (positions and gradient normals as float, 3 per vertex) from index base
-__device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz, double dx, double iso,
-                          int i, int j, int k, int& verts, float* pos = nullptr, float* nrm = nullptr,
+// dxPow2: dx is a power of two, so the central differences' division by 2 dx
+// is the exact product with r2dx = 1 / (2 dx) (see is_pow2)
+__device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz, double dx, bool dxPow2, double r2dx,
+                          double iso, int i, int j, int k, int& verts, float* pos = nullptr, float* nrm = nullptr,
                           long long base = 0) {
   long long sj = nx + 1, sk = (long long)(ny + 1) * sj;
   double cv[8], gx[8], gy[8], gz[8], minv = 1e300, maxv = -1e300;
@@ -520,9 +522,11 @@ __device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz
     int ip = ci + 1 < nx ? ci + 1 : nx, im = ci - 1 > 0 ? ci - 1 : 0;
     int jp = cj + 1 < ny ? cj + 1 : ny, jm = cj - 1 > 0 ? cj - 1 : 0;
     int kp = ck + 1 < nz ? ck + 1 : nz, km = ck - 1 > 0 ? ck - 1 : 0;
-    gx[c] = ((double)dens[ck * sk + cj * sj + ip] - (double)dens[ck * sk + cj * sj + im]) / (2 * dx);
-    gy[c] = ((double)dens[ck * sk + jp * sj + ci] - (double)dens[ck * sk + jm * sj + ci]) / (2 * dx);
-    gz[c] = ((double)dens[kp * sk + cj * sj + ci] - (double)dens[km * sk + cj * sj + ci]) / (2 * dx);
+    const double ddx = (double)dens[ck * sk + cj * sj + ip] - (double)dens[ck * sk + cj * sj + im];
+    const double ddy = (double)dens[ck * sk + jp * sj + ci] - (double)dens[ck * sk + jm * sj + ci];
+    const double ddz = (double)dens[kp * sk + cj * sj + ci] - (double)dens[km * sk + cj * sj + ci];
+    if (dxPow2) { gx[c] = ddx * r2dx; gy[c] = ddy * r2dx; gz[c] = ddz * r2dx; }
+    else { gx[c] = ddx / (2 * dx); gy[c] = ddy / (2 * dx); gz[c] = ddz / (2 * dx); }
   }
   double vol = 0;
   for (int t = 0; t < 6; t++) {
@@ -576,7 +580,7 @@ __global__ void __launch_bounds__(128, 8) k_mt_partial(Dims d, const float* __re
   if (c < d.nCells) {
     int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
     int v;
-    vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v);
+    vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
     cnt = v;
   }
   vol = warp_sum(vol); cnt = warp_sum(cnt);
@@ -647,7 +651,7 @@ __global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restr
   int i = 0, j = 0, k = 0, v = 0;
   if (c < d.nCells) {
     i = (int)(c % d.nx); j = (int)((c / d.nx) % d.ny); k = (int)(c / ((long long)d.nx * d.ny));
-    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v);
+    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
   }
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5, x = v;
   for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
@@ -658,7 +662,7 @@ __global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restr
   const long long base = offs[blockIdx.x] + before + x - v;
   if (v > 0 && base + v <= maxVerts) {
     int v2;
-    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, iso, i, j, k, v2, pos, nrm, base);
+    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v2, pos, nrm, base);
   }
 }
 void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
