@@ -1,8 +1,8 @@
 """Parity of the CUDA substep against the oracle (the CPU restatement of
 js/solver.js), on the same seeded planet, through the C ABI.
 
-Tolerances (north_star: cell types and per-phase counts bit-exact;
-velocities, pressures and positions within 1e-5 relative in FP32):
+Tolerances (cell types and per-phase counts bit-exact; velocities,
+pressures and positions within 1e-5 relative in FP32):
   * cellType, pflag, pcool: bit-exact;
   * q, u/v/w, particle velocities: ||gpu - oracle||_inf / ||oracle||_inf <= 1e-5;
   * positions: max |gpu - oracle| <= 1e-5 * domain width.
