@@ -173,23 +173,47 @@ struct SorArgs {
   int clusterCap;      // lists up to this size per colour were solved by k_sor_cluster
 };
 
+// One colour's half-sweep over the lists in global memory, three cells per
+// thread at a time: every load of the three (list entry, six neighbours, own q)
+// is issued before any store, so a thread pays one list round trip and one q
+// round trip per batch instead of per cell. Cells of one colour never
+// neighbour each other, so the batch reads no value it writes.
+constexpr int kSorBatch = 3;
 __device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned tid, unsigned T) {
-  const int n = a.L.count[col];
+  const unsigned n = (unsigned)a.L.count[col];
   const int* __restrict__ idx = a.L.idx[col];
   const float* __restrict__ rhs = a.L.rhs[col];
   const float* __restrict__ pw = a.L.pw[col];
   float* q = a.q;
-  const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
-  for (unsigned e = tid; e < (unsigned)n; e += T) {
-    long long c = idx[e];
-    double sum = (double)__ldcg(q + c - 1);
-    sum += (double)__ldcg(q + c + 1);
-    sum += (double)__ldcg(q + c - nx);
-    sum += (double)__ldcg(q + c + nx);
-    sum += (double)__ldcg(q + c - nxy);
-    sum += (double)__ldcg(q + c + nxy);
-    double qc = (double)__ldcg(q + c);
-    __stcg(q + c, (float)(qc * a.om1 + (double)pw[e] * ((double)rhs[e] + sum)));
+  const int nx = a.d.nx, nxy = a.d.nx * a.d.ny;              // cell indices fit in 32 bits (list entries are int)
+  for (unsigned e0 = tid; e0 < n; e0 += kSorBatch * T) {
+    int c[kSorBatch];
+    float r[kSorBatch], w[kSorBatch], v[kSorBatch][7];
+#pragma unroll
+    for (int j = 0; j < kSorBatch; j++) {
+      const unsigned e = e0 + j * T;
+      c[j] = e < n ? idx[e] : -1;
+      r[j] = e < n ? rhs[e] : 0.f;
+      w[j] = e < n ? pw[e] : 0.f;
+    }
+#pragma unroll
+    for (int j = 0; j < kSorBatch; j++) {
+      if (c[j] < 0) continue;
+      const float* qc = q + c[j];
+      v[j][0] = __ldcg(qc - 1); v[j][1] = __ldcg(qc + 1); v[j][2] = __ldcg(qc - nx); v[j][3] = __ldcg(qc + nx);
+      v[j][4] = __ldcg(qc - nxy); v[j][5] = __ldcg(qc + nxy); v[j][6] = __ldcg(qc);
+    }
+#pragma unroll
+    for (int j = 0; j < kSorBatch; j++) {
+      if (c[j] < 0) continue;
+      double sum = (double)v[j][0];
+      sum += (double)v[j][1];
+      sum += (double)v[j][2];
+      sum += (double)v[j][3];
+      sum += (double)v[j][4];
+      sum += (double)v[j][5];
+      __stcg(q + c[j], (float)((double)v[j][6] * a.om1 + (double)w[j] * ((double)r[j] + sum)));
+    }
   }
 }
 
@@ -274,32 +298,33 @@ __device__ __forceinline__ void block_partial(const SorArgs& a, double rr, doubl
   }
 }
 
-__global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
-  const unsigned T = gridDim.x * blockDim.x;
-  const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+// The iteration loop, in two instantiations so that the register-resident
+// entries of the cached path are not live in the list-reading path.
+template <bool CACHED>
+__device__ __forceinline__ void persistent_loop(const SorArgs& a, unsigned tid, unsigned T) {
   const int n0 = a.L.count[0], n1 = a.L.count[1];
-  if (n0 <= a.clusterCap && n1 <= a.clusterCap) return;      // the cluster solve ran
-  // register-resident path when every thread owns at most one cell per colour
-  const bool cached = (unsigned)n0 <= T && (unsigned)n1 <= T;
   const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
   Entry e0, e1;
   e0.c = -1; e1.c = -1;
-  if (cached) {
+  if (CACHED) {
     if (tid < (unsigned)n0) { e0.c = a.L.idx[0][tid]; e0.rhs = a.L.rhs[0][tid]; e0.pw = a.L.pw[0][tid]; e0.dg = a.L.dg[0][tid]; e0.q = __ldcg(a.q + e0.c); }
     if (tid < (unsigned)n1) { e1.c = a.L.idx[1][tid]; e1.rhs = a.L.rhs[1][tid]; e1.pw = a.L.pw[1][tid]; e1.dg = a.L.dg[1][tid]; e1.q = __ldcg(a.q + e1.c); }
   }
+  auto partial = [&]() {
+    if (CACHED) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
+    else residual_block(a, tid, T);
+  };
   int it = 0;
   bool ok = true;
   double rel = -1;
   for (it = 0; it < a.iters && ok; ) {
-    if (cached) entry_relax(e0, a.q, nx, nxy, a.om1); else sor_half(a, 0, tid, T);
+    if (CACHED) entry_relax(e0, a.q, nx, nxy, a.om1); else sor_half(a, 0, tid, T);
     if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
-    if (cached) entry_relax(e1, a.q, nx, nxy, a.om1); else sor_half(a, 1, tid, T);
+    if (CACHED) entry_relax(e1, a.q, nx, nxy, a.om1); else sor_half(a, 1, tid, T);
     if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
     it++;
     if (a.check > 0 && it % a.check == 0) {
-      if (cached) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
-      else residual_block(a, tid, T);
+      partial();
       if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
       rel = residual_total(a);
       if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;   // partials reusable
@@ -307,12 +332,20 @@ __global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
     }
   }
   if (ok) {
-    if (cached) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
-    else residual_block(a, tid, T);
+    partial();
     ok = grid_barrier(a.bar, gridDim.x, a.err);
     if (ok) rel = residual_total(a);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; *a.outPath = 1; }
+}
+__global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
+  const unsigned T = gridDim.x * blockDim.x;
+  const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n0 = a.L.count[0], n1 = a.L.count[1];
+  if (n0 <= a.clusterCap && n1 <= a.clusterCap) return;      // the cluster solve ran
+  // register-resident path when every thread owns at most one cell per colour
+  if ((unsigned)n0 <= T && (unsigned)n1 <= T) persistent_loop<true>(a, tid, T);
+  else persistent_loop<false>(a, tid, T);
 }
 
 
