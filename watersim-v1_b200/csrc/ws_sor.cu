@@ -17,6 +17,7 @@
 // reports WS_ERR_TIMEOUT. The cooperative launch guarantees co-residency,
 // so a healthy run never reaches the limit.
 #include "ws_kernels.cuh"
+#include <algorithm>
 #include <cooperative_groups.h>
 
 static const long long kSpinLimit = 4000000LL;
@@ -49,23 +50,22 @@ __device__ __forceinline__ int sor_colour(const Dims& d, const float* __restrict
   return (int)((i + j + k) & 1u);
 }
 // exclusive scan of the (colour 0, colour 1) block counts into offs, one
-// block: each thread sums a contiguous segment, the block scans the segment
-// sums, then each thread writes its segment's offsets; total = the two list
-// lengths. The counts stay as the pressure setup wrote them, so the solve can
-// be repeated on the same system.
+// block of 32 warps: each warp owns a contiguous segment and reads it 32 pairs
+// at a time (coalesced); pass 1 sums the segments, the block scans the 32
+// sums, pass 2 rescans each segment from its carry and writes the offsets.
+// total = the two list lengths. The counts stay as the pressure setup wrote
+// them, so the solve can be repeated on the same system.
 __global__ void __launch_bounds__(1024) k_sor_scan(const int* __restrict__ blockCounts, int nb, int* __restrict__ offs,
                                                    int* __restrict__ total) {
   __shared__ int w0[32], w1[32];
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nw = blockDim.x >> 5;
-  const int per = (nb + blockDim.x - 1) / blockDim.x, lo = min(nb, t * per), hi = min(nb, lo + per);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int2* cnt = reinterpret_cast<const int2*>(blockCounts);
+  int2* out = reinterpret_cast<int2*>(offs);
+  const int seg = (nb + nw - 1) / nw, lo = min(nb, wid * seg), hi = min(nb, lo + seg);
   int s0 = 0, s1 = 0;
-  for (int i = lo; i < hi; i++) { s0 += blockCounts[2 * i]; s1 += blockCounts[2 * i + 1]; }
-  int x0 = s0, x1 = s1;
-  for (int o = 1; o < 32; o <<= 1) {
-    int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
-    if (lane >= o) { x0 += y0; x1 += y1; }
-  }
-  if (lane == 31) { w0[wid] = x0; w1[wid] = x1; }
+  for (int i = lo + lane; i < hi; i += 32) { int2 v = cnt[i]; s0 += v.x; s1 += v.y; }
+  s0 = __reduce_add_sync(0xffffffffu, s0); s1 = __reduce_add_sync(0xffffffffu, s1);
+  if (lane == 0) { w0[wid] = s0; w1[wid] = s1; }
   __syncthreads();
   if (wid == 0) {
     int a = lane < nw ? w0[lane] : 0, b = lane < nw ? w1[lane] : 0;
@@ -76,13 +76,19 @@ __global__ void __launch_bounds__(1024) k_sor_scan(const int* __restrict__ block
     w0[lane] = a; w1[lane] = b;
   }
   __syncthreads();
-  int r0 = x0 - s0 + (wid > 0 ? w0[wid - 1] : 0), r1 = x1 - s1 + (wid > 0 ? w1[wid - 1] : 0);
-  for (int i = lo; i < hi; i++) {
-    const int c0 = blockCounts[2 * i], c1 = blockCounts[2 * i + 1];
-    offs[2 * i] = r0; offs[2 * i + 1] = r1;
-    r0 += c0; r1 += c1;
+  int c0 = wid > 0 ? w0[wid - 1] : 0, c1 = wid > 0 ? w1[wid - 1] : 0;   // this segment's carry
+  for (int base = lo; base < hi; base += 32) {
+    const int i = base + lane;
+    int2 v = i < hi ? cnt[i] : make_int2(0, 0);
+    int x0 = v.x, x1 = v.y;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+      if (lane >= o) { x0 += y0; x1 += y1; }
+    }
+    if (i < hi) out[i] = make_int2(c0 + x0 - v.x, c1 + x1 - v.y);
+    c0 += __shfl_sync(0xffffffffu, x0, 31); c1 += __shfl_sync(0xffffffffu, x1, 31);
   }
-  if (t == blockDim.x - 1) { total[0] = w0[nw - 1]; total[1] = w1[nw - 1]; }
+  if (threadIdx.x == 0) { total[0] = w0[nw - 1]; total[1] = w1[nw - 1]; }
 }
 __global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float* __restrict__ rhs,
                               const uint8_t* __restrict__ diag8, const int* __restrict__ offs, SorLists L) {
@@ -104,25 +110,28 @@ __global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float*
   }
 }
 // neighbour codes (-x, +x, -y, +y, -z, +z) for the cluster solve: the owner
-// rank and slot of each fluid neighbour (always of the other colour)
+// rank and slot of each fluid neighbour (always of the other colour); one
+// thread per (list entry, direction), so the six lookups of a cell run in
+// parallel
 __global__ void k_sor_codes(Dims d, const float* __restrict__ pw, SorLists L, int C) {
-  int col = blockIdx.y;
-  int n = L.count[col], nOther = L.count[1 - col];
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n || n > C * kSmax || nOther > C * kSmax) return;
-  int S = (nOther + C - 1) / C, Sown = (n + C - 1) / C;
-  // a non-fluid neighbour reads the owner CTA's own zero slot (no remote traffic)
-  const uint16_t zeroCode = (uint16_t)(((e / Sown) << 12) | kSmax);
-  long long c = L.idx[col][e], nx = d.nx, nxy = (long long)d.nx * d.ny;
-  long long nb[6] = { c - 1, c + 1, c - nx, c + nx, c - nxy, c + nxy };
-  for (int q = 0; q < 6; q++) {
-    uint16_t code = zeroCode;
-    if (sor_colour(d, pw, (unsigned)nb[q]) >= 0) {
-      int e2 = L.pos[nb[q]];
-      int r = e2 / S, slot = e2 - r * S;
+  const int col = blockIdx.y;
+  const int n = L.count[col], nOther = L.count[1 - col];
+  if (n > C * kSmax || nOther > C * kSmax) return;
+  const int S = (nOther + C - 1) / C, Sown = (n + C - 1) / C;
+  const long long nx = d.nx, nxy = (long long)d.nx * d.ny;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6LL * n; t += stride) {
+    const int e = (int)(t / 6), q = (int)(t - (long long)e * 6);
+    const long long c = L.idx[col][e];
+    const long long nb = c + (q == 0 ? -1 : q == 1 ? 1 : q == 2 ? -nx : q == 3 ? nx : q == 4 ? -nxy : nxy);
+    // a non-fluid neighbour reads the owner CTA's own zero slot (no remote traffic)
+    uint16_t code = (uint16_t)(((e / Sown) << 12) | kSmax);
+    if (sor_colour(d, pw, (unsigned)nb) >= 0) {
+      const int e2 = L.pos[nb];
+      const int r = e2 / S, slot = e2 - r * S;
       code = (uint16_t)((r << 12) | slot);
     }
-    L.code[col][6 * (long long)e + q] = code;
+    L.code[col][t] = code;
   }
 }
 
@@ -587,7 +596,8 @@ cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, co
   cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
   int C = S->clusterSize;
   if (C) {
-    k_sor_codes<<<dim3((unsigned)grid_for(S->cap, 256), 2), 256, 0, s>>>(d, g.pw, S->L, C);
+    k_sor_codes<<<dim3((unsigned)std::min<long long>(grid_for(6 * S->cap, 256), 148 * 8), 2), 256, 0, s>>>(d, g.pw,
+                                                                                                      S->L, C);
     ClusterArgs ca;
     ca.d = d; ca.q = g.q; ca.L = S->L; ca.om1 = 1 - omega; ca.iters = iters; ca.check = check; ca.tol = tol;
     ca.outIters = S->outIters; ca.outRel = S->outRel; ca.outPath = S->outPath;
