@@ -714,7 +714,7 @@ static ws_status stage_pressure(ws_handle* h) {
   if (h->net && h->unetOn) {
     if ((e = h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream)) != cudaSuccess)
       return fail_cuda(h, e, "learned warm start");
-    h->launches += 24;
+    h->launches += 23;
   }
   e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
                                    &h->st->err, &dIters, &dRel, &dPath, h->stream);

@@ -152,8 +152,10 @@ __global__ void k_scale(float* __restrict__ r0, long long n, const double* sigma
   if (c < n) r0[c] = (float)((double)r0[c] / *sigma);
 }
 // network input at the voxels of active level-0 tiles
+// r0n: the residual already divided by sigma, or (sigma non-null) the raw
+// residual, divided here exactly as k_scale would: (float)(r0 / sigma)
 __global__ void k_input(Level L, const int* tiles, const int* count, const float* __restrict__ r0n,
-                        const uint8_t* __restrict__ type, bf16* __restrict__ x) {
+                        const uint8_t* __restrict__ type, bf16* __restrict__ x, const double* sigma) {
   const long long n = (long long)*count * 1024;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
   int X, Y, Z; long long v;
@@ -162,7 +164,7 @@ __global__ void k_input(Level L, const int* tiles, const int* count, const float
   bf16 ch[16];
 #pragma unroll
   for (int c = 0; c < 16; c++) ch[c] = __float2bfloat16_rn(0.f);
-  ch[0] = __float2bfloat16_rn(r0n[v]);
+  ch[0] = __float2bfloat16_rn(sigma ? (float)((double)r0n[v] / *sigma) : r0n[v]);
   ch[1] = __float2bfloat16_rn(t == WS_FLUID ? 1.f : 0.f);
   ch[2] = __float2bfloat16_rn(t == WS_SOLID ? 1.f : 0.f);
   ch[3] = __float2bfloat16_rn(t == WS_AIR ? 1.f : 0.f);
@@ -643,16 +645,16 @@ cudaError_t Net::prepare(const float* r0nIn, const uint8_t* type, cudaStream_t s
   cudaError_t e;
   if ((e = activity(type, s)) != cudaSuccess) return e;
   long long n = (long long)lv[0].ntiles * 1024;
-  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0nIn, type, x);
+  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0nIn, type, x, nullptr);
   return cudaGetLastError();
 }
 // r0 / sigma of the current pressure setup into dst, sigma into sig
 cudaError_t Net::residual(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type,
-                          float* dst, double* sig, cudaStream_t s) {
+                          float* dst, double* sig, cudaStream_t s, bool scale) {
   long long N = dims.nCells;
   k_residual0<<<nPartials, 256, 0, s>>>(dims, q, rhs, diag8, type, dst, partials);
   k_sigma<<<1, 1024, 0, s>>>(partials, nPartials, counts + 3, sig);
-  k_scale<<<grid1(N, 256), 256, 0, s>>>(dst, N, sig);
+  if (scale) k_scale<<<grid1(N, 256), 256, 0, s>>>(dst, N, sig);
   return cudaGetLastError();
 }
 
@@ -660,9 +662,10 @@ cudaError_t Net::residual(const float* q, const float* rhs, const uint8_t* diag8
 cudaError_t Net::predict(float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type, cudaStream_t s) {
   cudaError_t e;
   if ((e = activity(type, s)) != cudaSuccess) return e;          // also the fluid count sigma divides by
-  if ((e = residual(q, rhs, diag8, type, r0n, scal + 0, s)) != cudaSuccess) return e;
+  // raw residual; k_input divides by sigma at the active voxels only
+  if ((e = residual(q, rhs, diag8, type, r0n, scal + 0, s, false)) != cudaSuccess) return e;
   long long n = (long long)lv[0].ntiles * 1024;
-  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, type, x);
+  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, type, x, scal + 0);
   if ((e = forward(s)) != cudaSuccess) return e;
   k_head_apply<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, type, scal + 0, scal + 1, q);
   return cudaGetLastError();

@@ -110,7 +110,7 @@ class Net {
   cudaError_t pack(cudaStream_t s);
   cudaError_t activity(const uint8_t* type, cudaStream_t s);
   cudaError_t residual(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type, float* dst,
-                       double* sig, cudaStream_t s);
+                       double* sig, cudaStream_t s, bool scale = true);
   cudaError_t prepare(const float* r0nIn, const uint8_t* type, cudaStream_t s);
   cudaError_t conv(int l, const bf16* src0, const bf16* src1, bf16* out, cudaStream_t s);
   cudaError_t conv_bwd(int l, const bf16* dz, const bf16* mask, bf16* out0, bf16* out1, cudaStream_t s);
