@@ -223,6 +223,7 @@ def run_ours(args, rank, world, local_rank):
     surface = surface_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     render = render_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
     metaballs = metaball_timing(fs, cpu=(rank == 0 and not args.no_cpu_baseline))
+    fp64 = fp64_errors(fs) if (rank == 0 and not args.no_cpu_baseline) else None
     balls = ball_timing(fs, one_step)
     out = None
     if rank == 0:
@@ -248,6 +249,7 @@ def run_ours(args, rank, world, local_rank):
                           "surface_mesh": surface,
                           "render_particles": render,
                           "metaballs": metaballs,
+                          "fp64_field_errors": fp64,
                           "balls": balls,
                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
@@ -494,17 +496,17 @@ def render_timing(fs, cpu=True):
     return out
 
 
-def cpu_baseline(fs, seconds=20.0):
-    """The oracle (CPU restatement, reference order) on this exact planet, one
-    core, a bounded sample of whole substeps."""
+def oracle_from_device(fs, fp64=False):
+    """An oracle holding the device's current planet: terrain, particles, q and
+    scalars (fp64: the FP64-storage flavour)."""
     from oracle.oracle import Oracle
-    import numpy as np
     s = fs.scalars
     nP = s.nP
     t = fs.terrain()
     W = WORKLOAD
     coreR = W["R"] - W["depth"]
-    o = Oracle(fs.nx, fs.ny, fs.nz, 1.0, coreR=coreR, terrainSeed=W["seed"], targetParticles=s.targetParticles)
+    o = Oracle(fs.nx, fs.ny, fs.nz, 1.0, coreR=coreR, terrainSeed=W["seed"], targetParticles=s.targetParticles,
+               fp64=fp64)
     depthW = W["depth"]
     Rlo = max(coreR * 0.55, W["R"] - 1.8889 * depthW)
     o.load_terrain({"n": t["n"], "dv": 0.5, "solid": t["solid"], "R": t["R"], "Rsl": W["R"],
@@ -516,6 +518,60 @@ def cpu_baseline(fs, seconds=20.0):
     o.set_scalars(nP=nP, oceanR=s.oceanR, spacing=s.spacing, particleVolume=s.particleVolume,
                   gRamp=1.5, dtLast=DT, umax=s.umax)
     o.L.or_build_planet_gravity(o.h)
+    return o
+
+
+def fp64_errors(fs):
+    """Error of each field of one substep against the FP64 oracle of the same
+    substep: the device state is copied into the FP64-storage oracle (device
+    order: red-black SOR, Jacobi viscosity and extrapolation), both take one
+    substep of DT from it (warm start off), and each field's relative error is
+    reported as max |gpu - fp64| / max |fp64| and as the L2 ratio."""
+    import numpy as np
+    try:
+        warm = fs.unet_info()["enabled"]
+    except Exception:                     # no network on this handle (plain arm only)
+        warm = 0
+    if warm:
+        fs.unet_enable(0)
+    o = oracle_from_device(fs, fp64=True)
+    o.set(**{k: v for k, v in PARAMS.items()}, sorRedBlack=1, viscJacobi=1, extrapJacobi=1)
+    t0 = time.perf_counter()
+    o.substep(DT)
+    cpu_s = time.perf_counter() - t0
+    fs._substep(DT)
+    fs.synchronize()
+    nP = fs.scalars.nP
+    out = {"oracle": "FP64 storage and arithmetic, device order", "substep_dt": DT,
+           "sor_iterations": {"gpu": fs.scalars.sorIters, "fp64": o.scalars.sorIters}, "fp64_cpu_s": cpu_s}
+
+    def err(a, b):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        den = np.max(np.abs(b))
+        return {"linf_rel": float(np.max(np.abs(a - b)) / den) if den > 0 else 0.0,
+                "l2_rel": float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))}
+    out["q"] = err(fs.q, o.q)
+    for k in ("u", "v", "w"):
+        out[k] = err(fs.download(k), o.arr(k))
+    for k in ("pvx", "pvy", "pvz"):
+        out[k] = err(fs.download(k, nP), o.arr(k)[:nP])
+    W = fs.nx * fs.dx
+    out["positions_max_abs_over_width"] = float(max(
+        np.max(np.abs(fs.download(k, nP).astype(np.float64) - o.arr(k)[:nP])) for k in ("px", "py", "pz")) / W)
+    out["cell_types_differing"] = int(np.count_nonzero(fs.cellType != o.cellType))
+    if warm:
+        fs.unet_enable(1)
+    return out
+
+
+def cpu_baseline(fs, seconds=20.0):
+    """The oracle (CPU restatement, reference order) on this exact planet, one
+    core, a bounded sample of whole substeps."""
+    s = fs.scalars
+    nP = s.nP
+    W = WORKLOAD
+    o = oracle_from_device(fs)
     o.set(**{k: v for k, v in PARAMS.items()}, sorRedBlack=0, viscJacobi=0, extrapJacobi=0)
     done, t0 = 0, time.perf_counter()
     while True:
