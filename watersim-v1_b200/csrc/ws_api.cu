@@ -903,13 +903,20 @@ static ws_status heat(ws_handle* h, double dt) {
   launch_heat(h->d, grid_of(h), parts_of(h), h->terr, hp, dt, h->cellCnt, h->cellSum, h->cellChange, h->stream);
   return check_launch(h, hp.heatK > 0 ? 5 : 2);
 }
+static ws_status contact_scratch(ws_handle* h) {
+  if (h->contactScratch) return WS_OK;
+  WS_TRY(cudaMalloc(&h->contactScratch, contacts_scratch_bytes(h->capacity)));
+  return WS_OK;
+}
 static ws_status evaporation(ws_handle* h, double dt) {
   if (h->P.sunActivity <= 0 || h->P.evapIntensity <= 0) return WS_OK;
   double freezeT = std::max(h->P.meltT, h->P.snowT * 1.05);
   double rate = h->P.sunActivity * h->P.evapIntensity;
+  if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity)) return WS_ERR_STATE;
+  ws_status s0 = contact_scratch(h); if (s0) return s0;
   launch_evaporation(h->d, grid_of(h), parts_of(h), freezeT, rate, dt, h->cand, h->blockCounts, h->list,
-                     h->listCount, h->rng + 2, h->st, h->stream);
-  ws_status s = check_launch(h, 5); if (s) return s;
+                     h->listCount, h->rng + 2, h->contactScratch, h->capacity, h->st, h->stream);
+  ws_status s = check_launch(h, 7); if (s) return s;
   s = sync_status(h); if (s) return s;
   h->S.evapCount = h->stHost->evapCount;
   if (h->S.evapCount > 0) h->vaporPossible = true;
@@ -930,11 +937,6 @@ static ws_status phase(ws_handle* h, double dt) {
 static ws_status push_surface(ws_handle* h) {
   launch_push_surface(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->P.atmosphereH, h->stream);
   return check_launch(h, 1);
-}
-static ws_status contact_scratch(ws_handle* h) {
-  if (h->contactScratch) return WS_OK;
-  WS_TRY(cudaMalloc(&h->contactScratch, contacts_scratch_bytes(h->capacity)));
-  return WS_OK;
 }
 static ws_status vapor_collisions(ws_handle* h) {
   double sunRel[3] = { h->P.sunPos[0] - h->d.cx, h->P.sunPos[1] - h->d.cy, h->P.sunPos[2] - h->d.cz };

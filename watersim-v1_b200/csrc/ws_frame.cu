@@ -119,7 +119,7 @@ __global__ void k_heat_flux(Dims d, const int* __restrict__ cnt, const double* _
   int nc = cnt[c];
   if (!nc) return;
   int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-  int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / nxy);
+  int i, j, k; cell_ijk(d, c, i, j, k);
   double ch = 0;
   // contributions as the neighbour of an earlier cell (:2961 "-="): c-nxy, c-nx, c-1
   if (k > 0 && cnt[c - nxy]) { int a = cnt[c - nxy]; ch -= alpha * (double)(a < nc ? a : nc) * (mean[c] - mean[c - nxy]); }
@@ -172,11 +172,20 @@ void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const Terra
 
 // ------------------------------------------------------------ evaporation
 // _evapChunk, js/solver.js:3028-3116. Candidates (surface-top liquid above
-// the freezing point) are compacted in index order; one CTA then walks them
-// reproducing the reference's single _evS stream: every lane evaluates its
-// draw assuming no ejection before it (lcg_jump), the first ejecting lane
-// runs its six Box-Muller draws (with the u1 < 1e-9 retry) serially, and the
-// walk restarts after it.
+// the freezing point) are compacted in index order and walked as the
+// reference's single _evS stream. A candidate's draw sits at stream position
+// (its index + 1 + 6 x the ejections before it), each ejection taking six more
+// draws for its Box-Muller kick. Three passes:
+//  1. every candidate's ejection test as an integer threshold (parallel):
+//     rnd > prob with rnd = u / 2^32 is u > floor(prob 2^32), both sides exact;
+//  2. one CTA walks windows of 1024 candidates: each lane precomputes its
+//     decision for 0..63 earlier ejections in the window (a 64-bit mask), warp
+//     0 resolves the window in order by ballot, and every ejector records its
+//     particle and the stream state of its draw. A window holding 64 ejections,
+//     or a kick whose u1 < 1e-9 retry takes more than six draws (about one in
+//     10^9), ends the window early there;
+//  3. the kicks and velocity updates of all ejections (parallel): each touches
+//     only its own particle and reads the unchanged grid.
 __device__ __forceinline__ bool evap_candidate(const Dims& d, const GridDev& g, const PartsDev& P, int p,
                                                double freezeT, int& ci, int& cj, int& ck) {
   if (P.pflag[p] != 0) return false;
@@ -202,86 +211,162 @@ __global__ void k_evap_flags(Dims d, GridDev g, PartsDev P, double freezeT, uint
   int i, j, k;
   cand[p] = evap_candidate(d, g, P, p, freezeT, i, j, k) ? 1 : 0;
 }
-__device__ __forceinline__ double ev_gauss(uint32_t& s) {
+__device__ __forceinline__ double ev_gauss(uint32_t& s, int& draws) {
   double u1;
-  do { s = lcg_next(s); u1 = s / 4294967296.0; } while (u1 < 1e-9);
-  s = lcg_next(s);
+  do { s = lcg_next(s); u1 = s / 4294967296.0; draws++; } while (u1 < 1e-9);
+  s = lcg_next(s); draws++;
   return sqrt(-2 * log(u1)) * cos(6.283185306 * (s / 4294967296.0));
 }
-__global__ void __launch_bounds__(1024) k_evap_walk(Dims d, GridDev g, PartsDev P, double freezeT, double rate, double dt,
-                                                    const int* __restrict__ list, const int* __restrict__ nCp,
-                                                    uint32_t* __restrict__ evS, DevStatus* st) {
-  __shared__ int firstLane;
+// Six steps of the _evS generator (x -> 1664525 x + 1013904223 mod 2^32) as one affine map.
+constexpr uint32_t lcg_pow_a(int n) { return n == 0 ? 1u : 1664525u * lcg_pow_a(n - 1); }
+constexpr uint32_t lcg_pow_c(int n) { return n == 0 ? 0u : 1664525u * lcg_pow_c(n - 1) + 1013904223u; }
+constexpr uint32_t kLcg6A = lcg_pow_a(6), kLcg6C = lcg_pow_c(6);
+constexpr double kEvapC = 3.5, kEvapTCap = 1.15;   // EVAP_STEEPNESS and T_CAP, js/solver.js:3040-3041
+// The candidate ejects when its draw u satisfies u <= thr (thr = -1: never;
+// 2^32: always, prob >= 1 or NaN as in !(rnd > prob)).
+__global__ void k_evap_thr(const PartsDev P, double freezeT, double rate, double dt, const int* __restrict__ list,
+                           const int* __restrict__ nCp, long long* __restrict__ thr) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *nCp) return;
+  double prob = rate * dt * exp(kEvapC * ((double)P.pT[list[t]] - freezeT));
+  long long v;
+  if (!(prob < 1)) v = 4294967296ll;
+  else if (prob < 0) v = -1;
+  else v = (long long)floor(prob * 4294967296.0);
+  thr[t] = v;
+}
+__global__ void __launch_bounds__(1024) k_evap_walk(const int* __restrict__ list, const int* __restrict__ nCp,
+                                                    const long long* __restrict__ thr, uint32_t* __restrict__ evS,
+                                                    int* __restrict__ ejP, uint32_t* __restrict__ ejS,
+                                                    int* __restrict__ nEj, DevStatus* st) {
+  __shared__ unsigned long long smask[1024];
+  __shared__ unsigned short sE[1024];            // ejections before each resolved lane
+  __shared__ int sConsumed, sEtot, sFirstIrr;
   __shared__ uint32_t sNext;
   const int nC = *nCp;
+  const int t = (int)threadIdx.x;
   uint32_t s = *evS;
   int base = 0, ejections = 0;
-  const double C = 3.5, T_CAP = 1.15;
+  long long myThr = t < nC ? thr[t] : -1;
   while (base < nC) {
-    int idx = base + (int)threadIdx.x;
-    bool act = idx < nC;
-    int p = act ? list[idx] : 0;
-    double T = act ? (double)P.pT[p] : 0;
-    bool ej = false;
-    if (act) {
-      double prob = rate * dt * exp(C * (T - freezeT));
-      if (prob > 1) prob = 1;
-      uint32_t sl = lcg_jump(s, threadIdx.x + 1u);
-      ej = !(sl / 4294967296.0 > prob);
+    const int remaining = min(nC - base, (int)blockDim.x);
+    const bool act = t < remaining;
+    unsigned long long mask = 0;
+    if (act && myThr >= 0) {
+      uint32_t u = lcg_jump(s, (uint32_t)t + 1u);   // this lane's draw after m earlier ejections: + 6 m
+      for (int m = 0; m < 64; m++) {
+        if ((long long)u <= myThr) mask |= 1ull << m;
+        u = u * kLcg6A + kLcg6C;                     // six draws of the kick
+      }
     }
-    if (threadIdx.x == 0) firstLane = 1 << 30;
+    smask[t] = mask;
+    if (t == 0) sFirstIrr = 1 << 30;
     __syncthreads();
-    if (ej) atomicMin(&firstLane, (int)threadIdx.x);
-    __syncthreads();
-    int L = firstLane;
-    int remaining = nC - base; if (remaining > (int)blockDim.x) remaining = blockDim.x;
-    if (L >= remaining) {                              // no ejection in this window
-      s = lcg_jump(s, (uint32_t)remaining);
-      base += remaining;
-      __syncthreads();
-      continue;
-    }
-    if ((int)threadIdx.x == L) {                       // the first ejector, :3083-3113
-      uint32_t sl = lcg_jump(s, (uint32_t)L + 1u);
-      int i, j, k;
-      evap_candidate(d, g, P, p, freezeT, i, j, k);
-      P.pflag[p] = 2; P.pAir[p] = 0.f;
-      double tau = (T - freezeT) / (T_CAP - freezeT);
-      if (tau < 0) tau = 0; else if (tau > 1) tau = 1;
-      double sig = 0.30 + 0.32 * sqrt(tau);
-      double kx = sig * ev_gauss(sl); double ky = sig * ev_gauss(sl); double kz = sig * ev_gauss(sl);
-      double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
-      double ex2 = PX - d.cx, ey2 = PY - d.cy, ez2 = PZ - d.cz;
-      double el2 = ex2 * ex2 + ey2 * ey2 + ez2 * ez2;
-      double elL = sqrt(el2); if (elL == 0) elL = 1e-9;
-      double kUp = (kx * ex2 + ky * ey2 + kz * ez2) / el2;
-      if (kUp < 0) { kx -= 2 * kUp * ex2 / elL; ky -= 2 * kUp * ey2 / elL; kz -= 2 * kUp * ez2 / elL; }
-      int nx = d.nx, ny = d.ny;
-      double guS = g.vel[((long long)k * ny + j) * (nx + 1) + i];
-      double gvS = g.vel[d.uN + ((long long)k * (ny + 1) + j) * nx + i];
-      double gwS = g.vel[d.uN + d.vN + ((long long)k * ny + j) * nx + i];
-      double nl2 = 1 / el2;
-      double vN = ((double)P.pvx[p] * ex2 + (double)P.pvy[p] * ey2 + (double)P.pvz[p] * ez2) * nl2;
-      double gN = (guS * ex2 + gvS * ey2 + gwS * ez2) * nl2;
-      P.pvx[p] = (float)(vN * ex2 + (guS - gN * ex2) + kx);
-      P.pvy[p] = (float)(vN * ey2 + (gvS - gN * ey2) + ky);
-      P.pvz[p] = (float)(vN * ez2 + (gwS - gN * ez2) + kz);
-      sNext = sl;
+    if (t < 32) {                                 // the window in order: warp 0 finds each next ejector by ballot
+      int E = 0, i = 0;
+      while (i < remaining && E < 64) {
+        const int idx = i + t;
+        const bool hit = idx < remaining && ((smask[idx] >> E) & 1ull);
+        const unsigned b = __ballot_sync(0xffffffffu, hit);
+        const int f = b ? __ffs(b) - 1 : 31;
+        if (t <= f && idx < remaining) sE[idx] = (unsigned short)E;
+        if (b) E++;
+        i += f + 1;
+      }
+      if (t == 0) { sConsumed = min(i, remaining); sEtot = E; }
     }
     __syncthreads();
-    s = sNext;
-    base += L + 1;
-    ejections++;
+    const int consumed = sConsumed;
+    const bool ej = act && t < consumed && ((mask >> sE[t]) & 1ull);
+    uint32_t sl = 0;
+    if (ej) {
+      sl = lcg_jump(s, (uint32_t)(t + 1 + 6 * (int)sE[t]));
+      // Regular kick: its three u1 draws (1, 3 and 5 after the decision) are >= 1e-9, i.e. states >= 5.
+      uint32_t s1 = lcg_next(sl), s3 = lcg_next(lcg_next(s1)), s5 = lcg_next(lcg_next(s3));
+      if (s1 < 5u || s3 < 5u || s5 < 5u) atomicMin(&sFirstIrr, t);
+    }
+    // Prefetch the next window's thresholds (it starts at base + 1024 unless cut short).
+    const int nextBase = base + (int)blockDim.x;
+    const long long nextThr = nextBase + t < nC ? thr[nextBase + t] : -1;
     __syncthreads();
+    const int firstIrr = sFirstIrr;
+    if (ej && t <= firstIrr) {
+      ejP[ejections + sE[t]] = list[base + t];
+      ejS[ejections + sE[t]] = sl;
+      if (t == firstIrr) {                        // the stream after the irregular kick
+        uint32_t q = sl; int draws = 0;
+        ev_gauss(q, draws); ev_gauss(q, draws); ev_gauss(q, draws);
+        sNext = q;
+      }
+    }
+    __syncthreads();
+    int advance;
+    if (firstIrr < (1 << 30)) {
+      ejections += (int)sE[firstIrr] + 1;
+      s = sNext;
+      advance = firstIrr + 1;
+    } else {
+      ejections += sEtot;
+      s = lcg_jump(s, (uint32_t)(consumed + 6 * sEtot));
+      advance = consumed;
+    }
+    base += advance;
+    myThr = advance == (int)blockDim.x ? nextThr : (base + t < nC ? thr[base + t] : -1);
+    __syncthreads();                              // shared state is rewritten by the next window
   }
-  if (threadIdx.x == 0) { *evS = s; st->evapCount = ejections; }
+  if (t == 0) { *evS = s; *nEj = ejections; st->evapCount = ejections; }
+}
+// :3083-3113 for one ejection, its kick drawn from the recorded stream state.
+__global__ void k_evap_apply(Dims d, GridDev g, PartsDev P, double freezeT, const int* __restrict__ ejP,
+                             const uint32_t* __restrict__ ejS, const int* __restrict__ nEj) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *nEj) return;
+  const int p = ejP[e];
+  int i, j, k;
+  evap_candidate(d, g, P, p, freezeT, i, j, k);
+  const double T = P.pT[p];
+  double tau = (T - freezeT) / (kEvapTCap - freezeT);
+  if (tau < 0) tau = 0; else if (tau > 1) tau = 1;
+  const double sig = 0.30 + 0.32 * sqrt(tau);
+  uint32_t sl = ejS[e]; int draws = 0;
+  double kx = sig * ev_gauss(sl, draws); double ky = sig * ev_gauss(sl, draws); double kz = sig * ev_gauss(sl, draws);
+  P.pflag[p] = 2; P.pAir[p] = 0.f;
+  double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
+  double ex2 = PX - d.cx, ey2 = PY - d.cy, ez2 = PZ - d.cz;
+  double el2 = ex2 * ex2 + ey2 * ey2 + ez2 * ez2;
+  double elL = sqrt(el2); if (elL == 0) elL = 1e-9;
+  double kUp = (kx * ex2 + ky * ey2 + kz * ez2) / el2;
+  if (kUp < 0) { kx -= 2 * kUp * ex2 / elL; ky -= 2 * kUp * ey2 / elL; kz -= 2 * kUp * ez2 / elL; }
+  int nx = d.nx, ny = d.ny;
+  double guS = g.vel[((long long)k * ny + j) * (nx + 1) + i];
+  double gvS = g.vel[d.uN + ((long long)k * (ny + 1) + j) * nx + i];
+  double gwS = g.vel[d.uN + d.vN + ((long long)k * ny + j) * nx + i];
+  double nl2 = 1 / el2;
+  double vN = ((double)P.pvx[p] * ex2 + (double)P.pvy[p] * ey2 + (double)P.pvz[p] * ez2) * nl2;
+  double gN = (guS * ex2 + gvS * ey2 + gwS * ez2) * nl2;
+  P.pvx[p] = (float)(vN * ex2 + (guS - gN * ex2) + kx);
+  P.pvy[p] = (float)(vN * ey2 + (gvS - gN * ey2) + ky);
+  P.pvz[p] = (float)(vN * ez2 + (gwS - gN * ez2) + kz);
+}
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+size_t evaporation_scratch_bytes(int cap) {
+  return align256(8 * (size_t)cap) + 2 * align256(4 * (size_t)cap) + 256;
 }
 void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
-                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, DevStatus* st, cudaStream_t s) {
+                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, void* scratch, int cap,
+                        DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_evap_flags<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, freezeT, cand);
+  char* q = (char*)scratch;
+  long long* thr = (long long*)q; q += align256(8 * (size_t)cap);
+  int* ejP = (int*)q; q += align256(4 * (size_t)cap);
+  uint32_t* ejS = (uint32_t*)q; q += align256(4 * (size_t)cap);
+  int* nEj = (int*)q;
+  const int gp = grid_for(P.nP, 256);
+  k_evap_flags<<<gp, 256, 0, s>>>(d, g, P, freezeT, cand);
   launch_compact(cand, P.nP, 2, blockCounts, list, nC, s);
-  k_evap_walk<<<1, 1024, 0, s>>>(d, g, P, freezeT, rate, dt, list, nC, evS, st);
+  k_evap_thr<<<gp, 256, 0, s>>>(P, freezeT, rate, dt, list, nC, thr);
+  k_evap_walk<<<1, 1024, 0, s>>>(list, nC, thr, evS, ejP, ejS, nEj, st);
+  k_evap_apply<<<gp, 256, 0, s>>>(d, g, P, freezeT, ejP, ejS, nEj);
 }
 
 // ------------------------------------------------------------ phase changes
@@ -578,7 +663,7 @@ __global__ void __launch_bounds__(128, 8) k_mt_partial(Dims d, const float* __re
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double vol = 0, cnt = 0;
   if (c < d.nCells) {
-    int i = (int)(c % d.nx), j = (int)((c / d.nx) % d.ny), k = (int)(c / ((long long)d.nx * d.ny));
+    int i, j, k; cell_ijk(d, c, i, j, k);
     int v;
     vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
     cnt = v;
@@ -650,7 +735,7 @@ __global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restr
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   int i = 0, j = 0, k = 0, v = 0;
   if (c < d.nCells) {
-    i = (int)(c % d.nx); j = (int)((c / d.nx) % d.ny); k = (int)(c / ((long long)d.nx * d.ny));
+    cell_ijk(d, c, i, j, k);
     mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
   }
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5, x = v;

@@ -443,33 +443,37 @@ void launch_clamp_umax(const Dims& d, const GridDev& g, double maxSpeed, DevStat
 // float32 cell-centred velocities (recomputed from the faces, rounded as the
 // reference stores them), (b) the gated confinement force per fluid cell,
 // (c) the splat onto faces between two fluid cells.
-__device__ __forceinline__ float ccx(const Dims& d, const float* u, long long c) {
-  long long nx = d.nx; long long row = c / nx, i = c % nx;
-  long long ui = row * (nx + 1) + i;
+// cell-centred velocities of cell (i, j, k), as the reference's _vcx/_vcy/_vcz
+// (float stores of the two-face means)
+__device__ __forceinline__ float ccx(const Dims& d, const float* u, int i, int j, int k) {
+  const long long ui = ((long long)k * d.ny + j) * (d.nx + 1) + i;
   return (float)(0.5 * ((double)u[ui] + (double)u[ui + 1]));
 }
-__device__ __forceinline__ float ccy(const Dims& d, const float* v, long long c) {
-  long long nx = d.nx, ny = d.ny; long long i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
-  long long vi = (k * (ny + 1) + j) * nx + i;
-  return (float)(0.5 * ((double)v[vi] + (double)v[vi + nx]));
+__device__ __forceinline__ float ccy(const Dims& d, const float* v, int i, int j, int k) {
+  const long long vi = ((long long)k * (d.ny + 1) + j) * d.nx + i;
+  return (float)(0.5 * ((double)v[vi] + (double)v[vi + d.nx]));
 }
-__device__ __forceinline__ float ccz(const Dims& d, const float* w, long long c) {
-  long long nxy = (long long)d.nx * d.ny;
+__device__ __forceinline__ float ccz(const Dims& d, const float* w, int i, int j, int k) {
+  const long long c = ((long long)k * d.ny + j) * d.nx + i, nxy = (long long)d.nx * d.ny;
   return (float)(0.5 * ((double)w[c] + (double)w[c + nxy]));
 }
 __global__ void k_vort_omega(Dims d, GridDev g) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= d.nCells) return;
-  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  int nx = d.nx, ny = d.ny, nz = d.nz;
   int i, j, k; decode_cell(d, c, i, j, k);
   const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
-  long long im = i > 0 ? c - 1 : c, ip = i < nx - 1 ? c + 1 : c;
-  long long jm = j > 0 ? c - nx : c, jp = j < ny - 1 ? c + nx : c;
-  long long km = k > 0 ? c - nxy : c, kp = k < nz - 1 ? c + nxy : c;
+  // the clamped neighbours of the reference's central differences (a boundary cell uses itself)
+  const int im = i > 0 ? i - 1 : i, ip = i < nx - 1 ? i + 1 : i;
+  const int jm = j > 0 ? j - 1 : j, jp = j < ny - 1 ? j + 1 : j;
+  const int km = k > 0 ? k - 1 : k, kp = k < nz - 1 ? k + 1 : k;
   double inv2 = 0.5 / d.dx;
-  double wx = ((double)ccz(d, w, jp) - (double)ccz(d, w, jm) - ((double)ccy(d, v, kp) - (double)ccy(d, v, km))) * inv2;
-  double wy = ((double)ccx(d, u, kp) - (double)ccx(d, u, km) - ((double)ccz(d, w, ip) - (double)ccz(d, w, im))) * inv2;
-  double wz = ((double)ccy(d, v, ip) - (double)ccy(d, v, im) - ((double)ccx(d, u, jp) - (double)ccx(d, u, jm))) * inv2;
+  double wx = ((double)ccz(d, w, i, jp, k) - (double)ccz(d, w, i, jm, k) -
+               ((double)ccy(d, v, i, j, kp) - (double)ccy(d, v, i, j, km))) * inv2;
+  double wy = ((double)ccx(d, u, i, j, kp) - (double)ccx(d, u, i, j, km) -
+               ((double)ccz(d, w, ip, j, k) - (double)ccz(d, w, im, j, k))) * inv2;
+  double wz = ((double)ccy(d, v, ip, j, k) - (double)ccy(d, v, im, j, k) -
+               ((double)ccx(d, u, i, jp, k) - (double)ccx(d, u, i, jm, k))) * inv2;
   g.omx[c] = (float)wx; g.omy[c] = (float)wy; g.omz[c] = (float)wz;
   g.omg[c] = (float)sqrt(wx * wx + wy * wy + wz * wz);
 }

@@ -64,6 +64,11 @@ inline void dims_fastdiv(Dims& d) {
   d.dny = fastdiv_make((unsigned)d.ny); d.dny1 = fastdiv_make((unsigned)d.ny + 1);
   d.dxPow2 = is_pow2(d.dx) ? 1 : 0; d.rdx = 1.0 / d.dx;
 }
+// (i, j, k) of flat cell index c (c < 2^32) by the invariant-divisor multiply
+__device__ __forceinline__ void cell_ijk(const Dims& d, long long c64, int& i, int& j, int& k) {
+  const unsigned c = (unsigned)c64, t = fastdiv(c, d.dnx), kk = fastdiv(t, d.dny);
+  i = (int)(c - t * (unsigned)d.nx); j = (int)(t - kk * (unsigned)d.ny); k = (int)kk;
+}
 // v / dx, exactly as the division rounds
 __device__ __forceinline__ double over_dx(const Dims& d, double v) { return d.dxPow2 ? v * d.rdx : v / d.dx; }
 

@@ -57,7 +57,9 @@ void launch_stir_gaussian(const PartsDev& P, double pcx, double pcy, double pcz,
 void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t, const HeatParams& hp,
                  double dt, int* cnt, double* sumT, double* change, cudaStream_t s);
 void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
-                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, DevStatus* st, cudaStream_t s);
+                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, void* scratch, int cap,
+                        DevStatus* st, cudaStream_t s);
+size_t evaporation_scratch_bytes(int capacity);   // <= contacts_scratch_bytes: the two share one buffer
 void launch_phase(const Dims& d, const GridDev& g, const PartsDev& P, const PhaseParams& pp, int* cnt, cudaStream_t s);
 void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                          double oceanR, double coreR, double atmosphereH, cudaStream_t s);
