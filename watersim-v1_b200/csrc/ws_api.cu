@@ -913,13 +913,46 @@ static ws_status evaporation(ws_handle* h, double dt) {
   double freezeT = std::max(h->P.meltT, h->P.snowT * 1.05);
   double rate = h->P.sunActivity * h->P.evapIntensity;
   if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity)) return WS_ERR_STATE;
-  ws_status s0 = contact_scratch(h); if (s0) return s0;
-  launch_evaporation(h->d, grid_of(h), parts_of(h), freezeT, rate, dt, h->cand, h->blockCounts, h->list,
-                     h->listCount, h->rng + 2, h->contactScratch, h->capacity, h->st, h->stream);
-  ws_status s = check_launch(h, 7); if (s) return s;
-  s = sync_status(h); if (s) return s;
-  h->S.evapCount = h->stHost->evapCount;
-  if (h->S.evapCount > 0) h->vaporPossible = true;
+  ws_status s = contact_scratch(h); if (s) return s;
+  uint32_t* evS = h->rng + 2;
+  if (h->S.nP <= 0) { h->S.evapCount = 0; return WS_OK; }
+  const EvapScratch es = evap_carve(h->contactScratch, h->capacity);
+  launch_evap_prepare(h->d, grid_of(h), parts_of(h), freezeT, rate, dt, h->cand, h->blockCounts, h->list,
+                      h->listCount, es, h->stream);
+  s = check_launch(h, 5); if (s) return s;
+  // Passes: one, unless a kick's u1 retry shifted the stream (about one kick in 10^9).
+  int t0 = 0, eoff = 0, total = 0;
+  const uint32_t* sStart = evS;
+  for (;;) {
+    launch_evap_pass(h->S.nP, h->list, h->listCount, es, t0, eoff, sStart, h->st, h->stream);
+    s = check_launch(h, 5); if (s) return s;
+    s = sync_status(h); if (s) return s;
+    const DevStatus& hs = *h->stHost;
+    if (hs.evIrr == ~0ull) {
+      total = eoff + hs.evNEj;
+      WS_TRY(cudaMemcpyAsync(evS, &h->st->evSEnd, sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+      break;
+    }
+    const int e = (int)(hs.evIrr >> 32), tr = (int)(hs.evIrr & 0xffffffffu), nC = hs.evNC;
+    uint32_t q = 0;
+    WS_TRY(cudaMemcpyAsync(&q, es.ejS + eoff + e, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    WS_TRY(cudaStreamSynchronize(h->stream));
+    q = evap_kick_end(q);
+    eoff += e + 1; t0 += tr + 1;
+    if (t0 >= nC) {
+      total = eoff;
+      WS_TRY(cudaMemcpyAsync(evS, &q, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+      WS_TRY(cudaStreamSynchronize(h->stream));
+      break;
+    }
+    WS_TRY(cudaMemcpyAsync(&h->st->evSStart, &q, sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    WS_TRY(cudaStreamSynchronize(h->stream));
+    sStart = &h->st->evSStart;
+  }
+  launch_evap_apply(h->d, grid_of(h), parts_of(h), freezeT, es, total, h->stream);
+  s = check_launch(h, total > 0 ? 1 : 0); if (s) return s;
+  h->S.evapCount = total;
+  if (total > 0) h->vaporPossible = true;
   return WS_OK;
 }
 static ws_status phase(ws_handle* h, double dt) {

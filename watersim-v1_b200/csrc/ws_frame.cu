@@ -173,19 +173,20 @@ void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const Terra
 // ------------------------------------------------------------ evaporation
 // _evapChunk, js/solver.js:3028-3116. Candidates (surface-top liquid above
 // the freezing point) are compacted in index order and walked as the
-// reference's single _evS stream. A candidate's draw sits at stream position
-// (its index + 1 + 6 x the ejections before it), each ejection taking six more
-// draws for its Box-Muller kick. Three passes:
-//  1. every candidate's ejection test as an integer threshold (parallel):
-//     rnd > prob with rnd = u / 2^32 is u > floor(prob 2^32), both sides exact;
-//  2. one CTA walks windows of 1024 candidates: each lane precomputes its
-//     decision for 0..63 earlier ejections in the window (a 64-bit mask), warp
-//     0 resolves the window in order by ballot, and every ejector records its
-//     particle and the stream state of its draw. A window holding 64 ejections,
-//     or a kick whose u1 < 1e-9 retry takes more than six draws (about one in
-//     10^9), ends the window early there;
-//  3. the kicks and velocity updates of all ejections (parallel): each touches
-//     only its own particle and reads the unchanged grid.
+// reference's single _evS stream. With E ejections before it, candidate t
+// (counted from the walk's start state s0) draws the state T^(t+1+6E)(s0),
+// T the generator, each ejection taking six draws for its Box-Muller kick;
+// it ejects when that draw u has u / 2^32 <= prob, i.e. u <= floor(prob 2^32).
+// The walk is cut into windows of kEvW candidates. A window maps the
+// ejection count before it to the count after it, monotonically; each window
+// tabulates that map for a band of inputs around the expected count (the
+// prefix sum of the probabilities), one warp per input, all windows in
+// parallel; one warp then chains the windows through their tables (resolving
+// a window directly when the count falls outside its band), and every window
+// finally replays its own resolve to record its ejectors. A kick whose
+// u1 < 1e-9 retry takes more than six draws (about one in 10^9) shifts every
+// later position: the pass reports the first such ejection and the host starts
+// a new pass after it.
 __device__ __forceinline__ bool evap_candidate(const Dims& d, const GridDev& g, const PartsDev& P, int p,
                                                double freezeT, int& ci, int& cj, int& ck) {
   if (P.pflag[p] != 0) return false;
@@ -211,17 +212,31 @@ __global__ void k_evap_flags(Dims d, GridDev g, PartsDev P, double freezeT, uint
   int i, j, k;
   cand[p] = evap_candidate(d, g, P, p, freezeT, i, j, k) ? 1 : 0;
 }
-__device__ __forceinline__ double ev_gauss(uint32_t& s, int& draws) {
+__device__ __forceinline__ double ev_gauss(uint32_t& s) {
   double u1;
-  do { s = lcg_next(s); u1 = s / 4294967296.0; draws++; } while (u1 < 1e-9);
-  s = lcg_next(s); draws++;
+  do { s = lcg_next(s); u1 = s / 4294967296.0; } while (u1 < 1e-9);
+  s = lcg_next(s);
   return sqrt(-2 * log(u1)) * cos(6.283185306 * (s / 4294967296.0));
+}
+uint32_t evap_kick_end(uint32_t s) {             // the stream after a kick drawn from decision state s
+  for (int g = 0; g < 3; g++) {
+    do { s = lcg_next(s); } while (s < 5u);       // u1 = s / 2^32 < 1e-9 exactly when s < 5
+    s = lcg_next(s);
+  }
+  return s;
 }
 // Six steps of the _evS generator (x -> 1664525 x + 1013904223 mod 2^32) as one affine map.
 constexpr uint32_t lcg_pow_a(int n) { return n == 0 ? 1u : 1664525u * lcg_pow_a(n - 1); }
 constexpr uint32_t lcg_pow_c(int n) { return n == 0 ? 0u : 1664525u * lcg_pow_c(n - 1) + 1013904223u; }
 constexpr uint32_t kLcg6A = lcg_pow_a(6), kLcg6C = lcg_pow_c(6);
 constexpr double kEvapC = 3.5, kEvapTCap = 1.15;   // EVAP_STEEPNESS and T_CAP, js/solver.js:3040-3041
+constexpr int kEvW = 4096;                       // candidates per window
+constexpr int kEvKMax = 1024;                    // widest band of tabulated inputs per window
+__device__ __forceinline__ void lcg_affine(uint32_t k, uint32_t& A, uint32_t& C) {   // T^k(x) = A x + C
+  uint32_t a = 1664525u, c = 1013904223u;
+  A = 1u; C = 0u;
+  while (k) { if (k & 1u) { A = A * a; C = C * a + c; } c = c * (a + 1u); a = a * a; k >>= 1; }
+}
 // The candidate ejects when its draw u satisfies u <= thr (thr = -1: never;
 // 2^32: always, prob >= 1 or NaN as in !(rnd > prob)).
 __global__ void k_evap_thr(const PartsDev P, double freezeT, double rate, double dt, const int* __restrict__ list,
@@ -235,92 +250,162 @@ __global__ void k_evap_thr(const PartsDev P, double freezeT, double rate, double
   else v = (long long)floor(prob * 4294967296.0);
   thr[t] = v;
 }
-__global__ void __launch_bounds__(1024) k_evap_walk(const int* __restrict__ list, const int* __restrict__ nCp,
-                                                    const long long* __restrict__ thr, uint32_t* __restrict__ evS,
-                                                    int* __restrict__ ejP, uint32_t* __restrict__ ejS,
-                                                    int* __restrict__ nEj, DevStatus* st) {
-  __shared__ unsigned long long smask[1024];
-  __shared__ unsigned short sE[1024];            // ejections before each resolved lane
-  __shared__ int sConsumed, sEtot, sFirstIrr;
-  __shared__ uint32_t sNext;
-  const int nC = *nCp;
-  const int t = (int)threadIdx.x;
-  uint32_t s = *evS;
-  int base = 0, ejections = 0;
-  long long myThr = t < nC ? thr[t] : -1;
-  while (base < nC) {
-    const int remaining = min(nC - base, (int)blockDim.x);
-    const bool act = t < remaining;
-    unsigned long long mask = 0;
-    if (act && myThr >= 0) {
-      uint32_t u = lcg_jump(s, (uint32_t)t + 1u);   // this lane's draw after m earlier ejections: + 6 m
-      for (int m = 0; m < 64; m++) {
-        if ((long long)u <= myThr) mask |= 1ull << m;
-        u = u * kLcg6A + kLcg6C;                     // six draws of the kick
-      }
-    }
-    smask[t] = mask;
-    if (t == 0) sFirstIrr = 1 << 30;
-    __syncthreads();
-    if (t < 32) {                                 // the window in order: warp 0 finds each next ejector by ballot
-      int E = 0, i = 0;
-      while (i < remaining && E < 64) {
-        const int idx = i + t;
-        const bool hit = idx < remaining && ((smask[idx] >> E) & 1ull);
-        const unsigned b = __ballot_sync(0xffffffffu, hit);
-        const int f = b ? __ffs(b) - 1 : 31;
-        if (t <= f && idx < remaining) sE[idx] = (unsigned short)E;
-        if (b) E++;
-        i += f + 1;
-      }
-      if (t == 0) { sConsumed = min(i, remaining); sEtot = E; }
-    }
-    __syncthreads();
-    const int consumed = sConsumed;
-    const bool ej = act && t < consumed && ((mask >> sE[t]) & 1ull);
-    uint32_t sl = 0;
-    if (ej) {
-      sl = lcg_jump(s, (uint32_t)(t + 1 + 6 * (int)sE[t]));
-      // Regular kick: its three u1 draws (1, 3 and 5 after the decision) are >= 1e-9, i.e. states >= 5.
-      uint32_t s1 = lcg_next(sl), s3 = lcg_next(lcg_next(s1)), s5 = lcg_next(lcg_next(s3));
-      if (s1 < 5u || s3 < 5u || s5 < 5u) atomicMin(&sFirstIrr, t);
-    }
-    // Prefetch the next window's thresholds (it starts at base + 1024 unless cut short).
-    const int nextBase = base + (int)blockDim.x;
-    const long long nextThr = nextBase + t < nC ? thr[nextBase + t] : -1;
-    __syncthreads();
-    const int firstIrr = sFirstIrr;
-    if (ej && t <= firstIrr) {
-      ejP[ejections + sE[t]] = list[base + t];
-      ejS[ejections + sE[t]] = sl;
-      if (t == firstIrr) {                        // the stream after the irregular kick
-        uint32_t q = sl; int draws = 0;
-        ev_gauss(q, draws); ev_gauss(q, draws); ev_gauss(q, draws);
-        sNext = q;
-      }
-    }
-    __syncthreads();
-    int advance;
-    if (firstIrr < (1 << 30)) {
-      ejections += (int)sE[firstIrr] + 1;
-      s = sNext;
-      advance = firstIrr + 1;
-    } else {
-      ejections += sEtot;
-      s = lcg_jump(s, (uint32_t)(consumed + 6 * sEtot));
-      advance = consumed;
-    }
-    base += advance;
-    myThr = advance == (int)blockDim.x ? nextThr : (base + t < nC ? thr[base + t] : -1);
-    __syncthreads();                              // shared state is rewritten by the next window
+// One warp resolves a window of n candidates entering with Ein ejections:
+// b[j] = T^(j'+1)(s0) for the window's j-th candidate (j' its index in the
+// pass), so its draw after E ejections is T^(6E)(b[j]). Returns the count
+// after the window; emit(j, E, u) runs on the lane of each ejector.
+template <class Emit>
+__device__ __forceinline__ int ev_resolve(const uint32_t* b, const long long* thr, int n, int Ein, Emit emit) {
+  const int lane = threadIdx.x & 31;
+  uint32_t A, C;
+  lcg_affine(6u * (uint32_t)Ein, A, C);
+  int E = Ein, i = 0;
+  while (i < n) {
+    const int idx = i + lane;
+    uint32_t u = 0;
+    bool hit = false;
+    if (idx < n) { u = A * b[idx] + C; hit = (long long)u <= thr[idx]; }
+    const unsigned bal = __ballot_sync(0xffffffffu, hit);
+    if (!bal) { i += 32; continue; }
+    const int f = __ffs(bal) - 1;
+    if (lane == f) emit(idx, E, u);
+    E++; i += f + 1;
+    C = kLcg6A * C + kLcg6C; A = kLcg6A * A;
   }
-  if (t == 0) { *evS = s; *nEj = ejections; st->evapCount = ejections; }
+  return E;
+}
+__device__ __forceinline__ int ev_windows(int nC, int t0) { return nC > t0 ? (nC - t0 + kEvW - 1) / kEvW : 0; }
+__global__ void __launch_bounds__(256) k_evap_wsum(const long long* __restrict__ thr, const int* __restrict__ nCp,
+                                                   int t0, double* __restrict__ wsum) {
+  __shared__ double red[8];
+  const int nC = *nCp, w = blockIdx.x;
+  if (w >= ev_windows(nC, t0)) return;
+  const int lo = t0 + w * kEvW, hi = min(nC, lo + kEvW);
+  double acc = 0;
+  for (int t = lo + (int)threadIdx.x; t < hi; t += blockDim.x) {
+    const long long v = thr[t];
+    acc += v < 0 ? 0.0 : v >= 4294967296ll ? 1.0 : (double)v * (1.0 / 4294967296.0);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0;
+    for (int k = 0; k < 8; k++) tot += red[k];
+    wsum[w] = tot;
+  }
+}
+// Band origins: L[w] = floor(expected ejections before window w) - K/2, K set
+// from the expected total (eight standard deviations of a Poisson count, + 64).
+__global__ void __launch_bounds__(1024) k_evap_band(const double* __restrict__ wsum, const int* __restrict__ nCp,
+                                                    int t0, int* __restrict__ L, DevStatus* st) {
+  __shared__ double red[32];
+  __shared__ double sTot;
+  const int nW = ev_windows(*nCp, t0);
+  const int tid = (int)threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  double v = 0;
+  for (int w = tid; w < nW; w += 1024) v += wsum[w];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (tid == 0) { double tot = 0; for (int k = 0; k < 32; k++) tot += red[k]; sTot = tot; }
+  __syncthreads();
+  int keff = ((int)(8.0 * sqrt(sTot) + 64.0) + 31) & ~31;
+  keff = keff < 64 ? 64 : keff > kEvKMax ? kEvKMax : keff;
+  double carry = 0;
+  for (int c0 = 0; c0 < nW; c0 += 1024) {
+    __syncthreads();                              // red[] and sTot of the previous chunk are consumed
+    const int w = c0 + tid;
+    const double x = w < nW ? wsum[w] : 0.0;
+    double inc = x;
+    for (int o = 1; o < 32; o <<= 1) { double y = __shfl_up_sync(0xffffffffu, inc, o); if (lane >= o) inc += y; }
+    if (lane == 31) red[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      double r = red[lane], ri = r;
+      for (int o = 1; o < 32; o <<= 1) { double y = __shfl_up_sync(0xffffffffu, ri, o); if (lane >= o) ri += y; }
+      red[lane] = ri - r;                         // exclusive warp offsets
+      if (lane == 31) sTot = ri;
+    }
+    __syncthreads();
+    const double excl = carry + red[wid] + inc - x;
+    if (w < nW) { const int c = (int)floor(excl) - keff / 2; L[w] = c < 0 ? 0 : c; }
+    carry += sTot;
+  }
+  if (tid == 0) { st->evKeff = keff; st->evIrr = ~0ull; st->evNC = *nCp; }
+}
+// Each window: its candidates' base states and thresholds in shared memory,
+// then one warp per tabulated input.
+__global__ void __launch_bounds__(1024) k_evap_table(const long long* __restrict__ thr, const int* __restrict__ nCp,
+                                                     int t0, const uint32_t* __restrict__ sStart,
+                                                     const int* __restrict__ L, const DevStatus* __restrict__ st,
+                                                     uint32_t* __restrict__ bOut, unsigned short* __restrict__ table) {
+  __shared__ uint32_t sb[kEvW];
+  __shared__ long long sthr[kEvW];
+  const int nC = *nCp, w = blockIdx.x;
+  if (w >= ev_windows(nC, t0)) return;
+  const int lo = t0 + w * kEvW, n = min(kEvW, nC - lo);
+  const uint32_t s0 = *sStart;
+  for (int j = (int)threadIdx.x; j < n; j += blockDim.x) {
+    const uint32_t bj = lcg_jump(s0, (uint32_t)(lo - t0 + j + 1));
+    sb[j] = bj; bOut[lo + j] = bj;
+    sthr[j] = thr[lo + j];
+  }
+  __syncthreads();
+  const int keff = st->evKeff, Lw = L[w];
+  for (int k = (int)(threadIdx.x >> 5); k < keff; k += (int)(blockDim.x >> 5)) {
+    const int eo = ev_resolve(sb, sthr, n, Lw + k, [](int, int, uint32_t) {});
+    if ((threadIdx.x & 31) == 0) table[(size_t)w * kEvKMax + k] = (unsigned short)(eo - (Lw + k));
+  }
+}
+// One warp: the ejection count entering every window.
+__global__ void __launch_bounds__(32) k_evap_chain(const int* __restrict__ nCp, int t0, const int* __restrict__ L,
+                                                   const unsigned short* __restrict__ table,
+                                                   const uint32_t* __restrict__ b, const long long* __restrict__ thr,
+                                                   const uint32_t* __restrict__ sStart, int* __restrict__ Ew,
+                                                   DevStatus* st) {
+  const int nC = *nCp, nW = ev_windows(nC, t0), keff = st->evKeff;
+  int E = 0;
+  int Lnext = nW > 0 ? L[0] : 0;
+  for (int w = 0; w < nW; w++) {
+    const int Lw = Lnext;
+    if (w + 1 < nW) Lnext = L[w + 1];
+    if (threadIdx.x == 0) Ew[w] = E;
+    const int rel = E - Lw;
+    if (rel >= 0 && rel < keff) {
+      E += table[(size_t)w * kEvKMax + rel];
+    } else {
+      const int lo = t0 + w * kEvW;
+      E = ev_resolve(b + lo, thr + lo, min(kEvW, nC - lo), E, [](int, int, uint32_t) {});
+    }
+  }
+  if (threadIdx.x == 0) {
+    st->evNEj = E;
+    st->evSEnd = lcg_jump(*sStart, (uint32_t)(nC > t0 ? nC - t0 : 0) + 6u * (uint32_t)E);
+  }
+}
+// One warp per window: replay its resolve and record each ejector (particle and decision state).
+__global__ void k_evap_emit(const int* __restrict__ nCp, int t0, const uint32_t* __restrict__ b,
+                            const long long* __restrict__ thr, const int* __restrict__ Ew, const int* __restrict__ list,
+                            int eoff, int* __restrict__ ejP, uint32_t* __restrict__ ejS, DevStatus* st) {
+  const int nC = *nCp;
+  const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (w >= ev_windows(nC, t0)) return;          // uniform over the warp
+  const int lo = t0 + w * kEvW;
+  ev_resolve(b + lo, thr + lo, min(kEvW, nC - lo), Ew[w], [&](int j, int E, uint32_t u) {
+    ejP[eoff + E] = list[lo + j];
+    ejS[eoff + E] = u;
+    // Regular kick: its three u1 draws (1, 3 and 5 after the decision) have states >= 5.
+    const uint32_t s1 = lcg_next(u), s3 = lcg_next(lcg_next(s1)), s5 = lcg_next(lcg_next(s3));
+    if (s1 < 5u || s3 < 5u || s5 < 5u)
+      atomicMin(&st->evIrr, ((unsigned long long)(unsigned)E << 32) | (unsigned)(lo - t0 + j));
+  });
 }
 // :3083-3113 for one ejection, its kick drawn from the recorded stream state.
 __global__ void k_evap_apply(Dims d, GridDev g, PartsDev P, double freezeT, const int* __restrict__ ejP,
-                             const uint32_t* __restrict__ ejS, const int* __restrict__ nEj) {
+                             const uint32_t* __restrict__ ejS, int nEj) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= *nEj) return;
+  if (e >= nEj) return;
   const int p = ejP[e];
   int i, j, k;
   evap_candidate(d, g, P, p, freezeT, i, j, k);
@@ -328,8 +413,8 @@ __global__ void k_evap_apply(Dims d, GridDev g, PartsDev P, double freezeT, cons
   double tau = (T - freezeT) / (kEvapTCap - freezeT);
   if (tau < 0) tau = 0; else if (tau > 1) tau = 1;
   const double sig = 0.30 + 0.32 * sqrt(tau);
-  uint32_t sl = ejS[e]; int draws = 0;
-  double kx = sig * ev_gauss(sl, draws); double ky = sig * ev_gauss(sl, draws); double kz = sig * ev_gauss(sl, draws);
+  uint32_t sl = ejS[e];
+  double kx = sig * ev_gauss(sl); double ky = sig * ev_gauss(sl); double kz = sig * ev_gauss(sl);
   P.pflag[p] = 2; P.pAir[p] = 0.f;
   double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
   double ex2 = PX - d.cx, ey2 = PY - d.cy, ez2 = PZ - d.cz;
@@ -349,24 +434,44 @@ __global__ void k_evap_apply(Dims d, GridDev g, PartsDev P, double freezeT, cons
   P.pvz[p] = (float)(vN * ez2 + (gwS - gN * ez2) + kz);
 }
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+static size_t ev_max_windows(int cap) { return (size_t)(cap + kEvW - 1) / kEvW + 1; }
 size_t evaporation_scratch_bytes(int cap) {
-  return align256(8 * (size_t)cap) + 2 * align256(4 * (size_t)cap) + 256;
+  const size_t c = (size_t)cap, nw = ev_max_windows(cap);
+  return align256(8 * c) + 4 * align256(4 * c) + align256(8 * nw) + 2 * align256(4 * nw) + align256(2 * kEvKMax * nw);
 }
-void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
-                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, void* scratch, int cap,
-                        DevStatus* st, cudaStream_t s) {
-  if (P.nP <= 0) return;
-  char* q = (char*)scratch;
-  long long* thr = (long long*)q; q += align256(8 * (size_t)cap);
-  int* ejP = (int*)q; q += align256(4 * (size_t)cap);
-  uint32_t* ejS = (uint32_t*)q; q += align256(4 * (size_t)cap);
-  int* nEj = (int*)q;
+EvapScratch evap_carve(void* base, int cap) {
+  const size_t c = (size_t)cap, nw = ev_max_windows(cap);
+  char* q = (char*)base; EvapScratch e;
+  e.thr = (long long*)q; q += align256(8 * c);
+  e.b = (uint32_t*)q; q += align256(4 * c);
+  e.ejP = (int*)q; q += align256(4 * c);
+  e.ejS = (uint32_t*)q; q += align256(4 * c);
+  q += align256(4 * c);                           // reserved
+  e.wsum = (double*)q; q += align256(8 * nw);
+  e.L = (int*)q; q += align256(4 * nw);
+  e.Ew = (int*)q; q += align256(4 * nw);
+  e.table = (unsigned short*)q;
+  return e;
+}
+void launch_evap_prepare(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
+                         uint8_t* cand, int* blockCounts, int* list, int* nC, const EvapScratch& es, cudaStream_t s) {
   const int gp = grid_for(P.nP, 256);
   k_evap_flags<<<gp, 256, 0, s>>>(d, g, P, freezeT, cand);
   launch_compact(cand, P.nP, 2, blockCounts, list, nC, s);
-  k_evap_thr<<<gp, 256, 0, s>>>(P, freezeT, rate, dt, list, nC, thr);
-  k_evap_walk<<<1, 1024, 0, s>>>(list, nC, thr, evS, ejP, ejS, nEj, st);
-  k_evap_apply<<<gp, 256, 0, s>>>(d, g, P, freezeT, ejP, ejS, nEj);
+  k_evap_thr<<<gp, 256, 0, s>>>(P, freezeT, rate, dt, list, nC, es.thr);
+}
+void launch_evap_pass(int nP, const int* list, const int* nC, const EvapScratch& es, int t0, int eoff,
+                      const uint32_t* sStart, DevStatus* st, cudaStream_t s) {
+  const int nw = (int)ev_max_windows(nP);
+  k_evap_wsum<<<nw, 256, 0, s>>>(es.thr, nC, t0, es.wsum);
+  k_evap_band<<<1, 1024, 0, s>>>(es.wsum, nC, t0, es.L, st);
+  k_evap_table<<<nw, 1024, 0, s>>>(es.thr, nC, t0, sStart, es.L, st, es.b, es.table);
+  k_evap_chain<<<1, 32, 0, s>>>(nC, t0, es.L, es.table, es.b, es.thr, sStart, es.Ew, st);
+  k_evap_emit<<<(nw + 3) / 4, 128, 0, s>>>(nC, t0, es.b, es.thr, es.Ew, list, eoff, es.ejP, es.ejS, st);
+}
+void launch_evap_apply(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, const EvapScratch& es,
+                       int nEj, cudaStream_t s) {
+  if (nEj > 0) k_evap_apply<<<grid_for(nEj, 256), 256, 0, s>>>(d, g, P, freezeT, es.ejP, es.ejS, nEj);
 }
 
 // ------------------------------------------------------------ phase changes

@@ -121,6 +121,9 @@ struct DevStatus {
   int sorIters, pad2;
   double relres;
   double rr, bb;
+  unsigned long long evIrr;   // evaporation pass: (ejection << 32 | candidate) of the first irregular kick
+  int evNEj, evNC, evKeff;    // ejections in the pass, candidates, tabulated band width
+  unsigned int evSEnd, evSStart, pad3;   // stream after the pass; start state of a restarted pass
 };
 
 struct GridDev {

@@ -56,10 +56,21 @@ void launch_stir_gaussian(const PartsDev& P, double pcx, double pcy, double pcz,
 // ---- ws_frame.cu
 void launch_heat(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t, const HeatParams& hp,
                  double dt, int* cnt, double* sumT, double* change, cudaStream_t s);
-void launch_evaporation(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
-                        uint8_t* cand, int* blockCounts, int* list, int* nC, uint32_t* evS, void* scratch, int cap,
-                        DevStatus* st, cudaStream_t s);
+// Evaporation (exact _evS stream): prepare (flags, compaction, thresholds) once,
+// then passes over the candidates from t0 until no irregular kick is reported.
+struct EvapScratch {
+  long long* thr; uint32_t* b; int* ejP; uint32_t* ejS;
+  double* wsum; int* L; int* Ew; unsigned short* table;
+};
 size_t evaporation_scratch_bytes(int capacity);   // <= contacts_scratch_bytes: the two share one buffer
+EvapScratch evap_carve(void* base, int capacity);
+void launch_evap_prepare(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, double rate, double dt,
+                         uint8_t* cand, int* blockCounts, int* list, int* nC, const EvapScratch& es, cudaStream_t s);
+void launch_evap_pass(int nP, const int* list, const int* nC, const EvapScratch& es, int t0, int eoff,
+                      const uint32_t* sStart, DevStatus* st, cudaStream_t s);
+void launch_evap_apply(const Dims& d, const GridDev& g, const PartsDev& P, double freezeT, const EvapScratch& es,
+                       int nEj, cudaStream_t s);
+uint32_t evap_kick_end(uint32_t s);
 void launch_phase(const Dims& d, const GridDev& g, const PartsDev& P, const PhaseParams& pp, int* cnt, cudaStream_t s);
 void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                          double oceanR, double coreR, double atmosphereH, cudaStream_t s);
