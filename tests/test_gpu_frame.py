@@ -67,6 +67,48 @@ def test_evaporation_parity():
         assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
 
 
+def _lcg_back(x, n):
+    """The _evS state n draws before x (the generator is a bijection mod 2^32)."""
+    a_inv = pow(1664525, -1, 2**32)
+    for _ in range(n):
+        x = (a_inv * (x - 1013904223)) % 2**32
+    return x
+
+
+@pytest.mark.parametrize("where", ["first", "second_window"])
+def test_evaporation_irregular_kick(where):
+    """A kick whose Box-Muller u1 draw is below 1e-9 takes an extra draw and
+    shifts every later stream position (js/solver.js:3118-3125). With every
+    candidate ejecting (prob capped at 1), candidate t decides on draw 7t + 1
+    and draws its first u1 at 7t + 2; the start state is set so that this u1
+    state is 3, i.e. u1 = 7e-10, at the first candidate or one in the second
+    window of 4096 candidates."""
+    def hot_state():
+        o = _state64()
+        o.set(sunActivity=2.0, evapIntensity=1.0)
+        nP = o.nP
+        o.pT[:nP] = np.random.default_rng(9).uniform(0.9, 1.0, nP).astype(np.float32)
+        return o
+    probe = hot_state()
+    probe.stage("update_evaporation", 1 / 12)
+    nC = probe.scalars.evapCount
+    t = 0 if where == "first" else 4096 + 17
+    if t >= nC:
+        pytest.skip("fewer candidates than the second window needs")
+    o = hot_state()
+    o.set_scalars(evS=_lcg_back(3, 7 * t + 2))
+    nP = o.nP
+    fs = to_device(o, with_grid=True)
+    o.stage("update_evaporation", 1 / 12)
+    fs.stage("EVAPORATION", 1 / 12)
+    so, sg = o.scalars, fs.scalars
+    assert so.evapCount == nC and sg.evapCount == nC
+    assert sg.evS == so.evS
+    assert np.array_equal(fs.pflag, o.pflag[:nP])
+    for k in ("pvx", "pvy", "pvz"):
+        assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
+
+
 def test_phase_parity():
     o = _state64()
     nP = o.nP
