@@ -20,7 +20,7 @@ __global__ void k_heat_shadow(Dims d, GridDev g, PartsDev P, TerrainDev t, HeatP
   double stpU = dx / dwl; int above = 0;
   for (int stU = 1; stU <= 4; stU++) {
     double qx = PX + dwx * stpU * stU, qy = PY + dwy * stpU * stU, qz = PZ + dwz * stpU * stU;
-    int qi = jtrunc(qx / dx), qj = jtrunc(qy / dx), qk = jtrunc(qz / dx);
+    int qi = jtrunc(over_dx(d, qx)), qj = jtrunc(over_dx(d, qy)), qk = jtrunc(over_dx(d, qz));
     if (qi < 0 || qj < 0 || qk < 0 || qi >= nx || qj >= ny || qk >= nz) break;
     if (type[((long long)qk * ny + qj) * nx + qi] != WS_FLUID) break;
     above++;
@@ -44,9 +44,9 @@ __global__ void k_heat_shadow(Dims d, GridDev g, PartsDev P, TerrainDev t, HeatP
             mx += dxn * stp; my += dyn * stp; mz += dzn * stp;
             double rex = mx - cx, rey = my - cy, rez = mz - cz;
             if (rex * rex + rey * rey + rez * rez > esc2) break;
-            int ivx = jtrunc(mx / t.dv); if (ivx < 0 || ivx >= t.n) break;
-            int ivy = jtrunc(my / t.dv); if (ivy < 0 || ivy >= t.n) break;
-            int ivz = jtrunc(mz / t.dv); if (ivz < 0 || ivz >= t.n) break;
+            int ivx = jtrunc(over_dv(t, mx)); if (ivx < 0 || ivx >= t.n) break;
+            int ivy = jtrunc(over_dv(t, my)); if (ivy < 0 || ivy >= t.n) break;
+            int ivz = jtrunc(over_dv(t, mz)); if (ivz < 0 || ivz >= t.n) break;
             if (t.solid[((long long)ivz * t.n + ivy) * t.n + ivx]) { lit = 0; break; }
           }
         }
@@ -59,7 +59,7 @@ __global__ void k_heat_shadow(Dims d, GridDev g, PartsDev P, TerrainDev t, HeatP
         long long sj = nx + 1, sk = (long long)(ny + 1) * sj;
         for (int st = 0; st < 6 && st * half < 0.55; st++) {
           sx += dxn * half; sy += dyn * half; sz += dzn * half;
-          int i0 = jtrunc(sx / dx), j0 = jtrunc(sy / dx), k0 = jtrunc(sz / dx);
+          int i0 = jtrunc(over_dx(d, sx)), j0 = jtrunc(over_dx(d, sy)), k0 = jtrunc(over_dx(d, sz));
           if (i0 < 0 || j0 < 0 || k0 < 0 || i0 >= nx || j0 >= ny || k0 >= nz) break;
           double vv = g.dens[k0 * sk + j0 * sj + i0];
           od += vv * half * 1.1;
@@ -95,9 +95,9 @@ __global__ void k_heat_shadow(Dims d, GridDev g, PartsDev P, TerrainDev t, HeatP
 // cell, then each cell gathers its six edge energies in the reference's
 // accumulation order, then each particle applies its cell's update.
 __device__ __forceinline__ long long heat_cell(const Dims& d, double x, double y, double z) {
-  int gx = jtrunc(x / d.dx); if (gx < 0) gx = 0; else if (gx >= d.nx) gx = d.nx - 1;
-  int gy = jtrunc(y / d.dx); if (gy < 0) gy = 0; else if (gy >= d.ny) gy = d.ny - 1;
-  int gz = jtrunc(z / d.dx); if (gz < 0) gz = 0; else if (gz >= d.nz) gz = d.nz - 1;
+  int gx = jtrunc(over_dx(d, x)); if (gx < 0) gx = 0; else if (gx >= d.nx) gx = d.nx - 1;
+  int gy = jtrunc(over_dx(d, y)); if (gy < 0) gy = 0; else if (gy >= d.ny) gy = d.ny - 1;
+  int gz = jtrunc(over_dx(d, z)); if (gz < 0) gz = 0; else if (gz >= d.nz) gz = d.nz - 1;
   return ((long long)gz * d.ny + gy) * d.nx + gx;
 }
 __global__ void k_heat_bin(Dims d, PartsDev P, int* __restrict__ cnt, double* __restrict__ sumT) {
@@ -193,14 +193,14 @@ __device__ __forceinline__ bool evap_candidate(const Dims& d, const GridDev& g, 
   double T = P.pT[p];
   if (T <= freezeT) return false;
   double PX = P.px[p], PY = P.py[p], PZ = P.pz[p];
-  int i = jtrunc(PX / d.dx), j = jtrunc(PY / d.dx), k = jtrunc(PZ / d.dx);
+  int i = jtrunc(over_dx(d, PX)), j = jtrunc(over_dx(d, PY)), k = jtrunc(over_dx(d, PZ));
   if (i < 1) i = 1; else if (i > d.nx - 2) i = d.nx - 2;
   if (j < 1) j = 1; else if (j > d.ny - 2) j = d.ny - 2;
   if (k < 1) k = 1; else if (k > d.nz - 2) k = d.nz - 2;
   if (g.type[((long long)k * d.ny + j) * d.nx + i] != WS_FLUID) return false;
   double ex = PX - d.cx, ey = PY - d.cy, ez = PZ - d.cz;
   double el = sqrt(ex * ex + ey * ey + ez * ez); if (el == 0) el = 1e-9;
-  int ui = jtrunc((PX + ex / el * d.dx) / d.dx), uj = jtrunc((PY + ey / el * d.dx) / d.dx), uk = jtrunc((PZ + ez / el * d.dx) / d.dx);
+  int ui = jtrunc(over_dx(d, PX + ex / el * d.dx)), uj = jtrunc(over_dx(d, PY + ey / el * d.dx)), uk = jtrunc(over_dx(d, PZ + ez / el * d.dx));
   if (ui < 0 || uj < 0 || uk < 0 || ui >= d.nx || uj >= d.ny || uk >= d.nz) return false;
   if (g.type[((long long)uk * d.ny + uj) * d.nx + ui] == WS_FLUID) return false;
   ci = i; cj = j; ck = k;
@@ -478,7 +478,7 @@ void launch_evap_apply(const Dims& d, const GridDev& g, const PartsDev& P, doubl
 // _updatePhaseChanges, js/solver.js:3152-3281: steam counts per cell
 // (integer atomics, exact), then independent per-particle transitions.
 __device__ __forceinline__ long long clamp_cell(const Dims& d, double x, double y, double z, int& i, int& j, int& k) {
-  i = jtrunc(x / d.dx); j = jtrunc(y / d.dx); k = jtrunc(z / d.dx);
+  i = jtrunc(over_dx(d, x)); j = jtrunc(over_dx(d, y)); k = jtrunc(over_dx(d, z));
   if (i < 0) i = 0; else if (i >= d.nx) i = d.nx - 1;
   if (j < 0) j = 0; else if (j >= d.ny) j = d.ny - 1;
   if (k < 0) k = 0; else if (k >= d.nz) k = d.nz - 1;
@@ -529,7 +529,7 @@ __global__ void k_phase_update(Dims d, GridDev g, PartsDev P, PhaseParams pp, co
       } else if (T <= pp.cloudT) {
         double rx = (double)P.px[p] - d.cx, ry = (double)P.py[p] - d.cy, rz = (double)P.pz[p] - d.cz;
         if (sqrt(rx * rx + ry * ry + rz * rz) >= pp.cloudBase) {
-          i = jtrunc(P.px[p] / d.dx); j = jtrunc(P.py[p] / d.dx); k = jtrunc(P.pz[p] / d.dx);
+          i = jtrunc(over_dx(d, P.px[p])); j = jtrunc(over_dx(d, P.py[p])); k = jtrunc(over_dx(d, P.pz[p]));
           int i0 = i > 0 ? i - 1 : 0, i1 = i < nx - 1 ? i + 1 : nx - 1;
           int j0 = j > 0 ? j - 1 : 0, j1 = j < ny - 1 ? j + 1 : ny - 1;
           int k0 = k > 0 ? k - 1 : 0, k1 = k < nz - 1 ? k + 1 : nz - 1;
@@ -653,7 +653,7 @@ __global__ void k_splat(Dims d, GridDev g, PartsDev P, double spacing) {
   double dx = d.dx, r = 1.6 * spacing, r2 = r * r;
   long long sj = d.nx + 1, sk = (long long)(d.ny + 1) * sj;
   double X = P.px[p], Y = P.py[p], Z = P.pz[p];
-  double fi = floor(X / dx), fj = floor(Y / dx), fk = floor(Z / dx);
+  double fi = floor(over_dx(d, X)), fj = floor(over_dx(d, Y)), fk = floor(over_dx(d, Z));
   int i0 = fi < 0 ? 0 : (fi > d.nx - 1 ? d.nx - 1 : (int)fi);
   int j0 = fj < 0 ? 0 : (fj > d.ny - 1 ? d.ny - 1 : (int)fj);
   int k0 = fk < 0 ? 0 : (fk > d.nz - 1 ? d.nz - 1 : (int)fk);

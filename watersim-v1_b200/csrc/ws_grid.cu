@@ -457,9 +457,11 @@ __device__ __forceinline__ float ccz(const Dims& d, const float* w, int i, int j
   const long long c = ((long long)k * d.ny + j) * d.nx + i, nxy = (long long)d.nx * d.ny;
   return (float)(0.5 * ((double)w[c] + (double)w[c + nxy]));
 }
+// Omega is read only at fluid cells: k_vort_force reads omg and om* at a fluid
+// cell, and omg at its six neighbours only when all six are fluid.
 __global__ void k_vort_omega(Dims d, GridDev g) {
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c >= d.nCells) return;
+  if (c >= d.nCells || g.type[c] != WS_FLUID) return;
   int nx = d.nx, ny = d.ny, nz = d.nz;
   int i, j, k; decode_cell(d, c, i, j, k);
   const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;

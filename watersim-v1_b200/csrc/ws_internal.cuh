@@ -79,6 +79,7 @@ struct TerrainDev {
   const uint8_t* __restrict__ solid;
   const float* __restrict__ R;
 };
+__device__ __forceinline__ double over_dv(const TerrainDev& t, double v) { return t.dvPow2 ? v * t.rdv : v / t.dv; }
 
 struct PartsDev {
   float *px, *py, *pz, *pvx, *pvy, *pvz, *pT, *pAir, *pLight, *pWx, *pWy, *pWz, *pPh;
