@@ -155,6 +155,87 @@ def test_vapor_advection_exact_streams():
         assert np.max(np.abs(fs.download(k)[sel].astype(np.float64) - o.arr(k)[sel])) <= 1e-5 * W, k
 
 
+def _jacobi_vapor_contacts(o, rad):
+    """The device's vapour contact pass (js/solver.js:3345-3478 resolved from
+    one snapshot, Jacobi order) restated with a k-d tree: position and
+    velocity increments of every parcel, in FP64."""
+    from scipy.spatial import cKDTree
+    nP = o.nP
+    f = o.pflag[:nP]
+    X = np.stack([o.arr(k)[:nP].astype(np.float64) for k in ("px", "py", "pz")], 1)
+    V = np.stack([o.arr(k)[:nP].astype(np.float64) for k in ("pvx", "pvy", "pvz")], 1)
+    par = np.nonzero((f == 2) | (f == 3))[0]
+    dpos = np.zeros((nP, 3))
+    dvel = np.zeros((nP, 3))
+    tp = cKDTree(X[par])
+    pairs = np.array(sorted(tp.query_pairs(rad * 1.001)), dtype=np.int64).reshape(-1, 2)
+    a, b = par[pairs[:, 0]], par[pairs[:, 1]]
+    d = X[b] - X[a]
+    d2 = (d * d).sum(1)
+    keep = d2 < rad * rad
+    a, b, d, d2 = a[keep], b[keep], d[keep], d2[keep]
+    dd = np.sqrt(d2)
+    dd[dd == 0] = 1e-9
+    n = d / dd[:, None]
+    vrel = ((V[a] - V[b]) * n).sum(1)
+    dv = np.maximum(vrel, 0) + (rad - dd) * 2
+    half = (rad - dd) * 0.5
+    np.add.at(dpos, a, -n * half[:, None]); np.add.at(dpos, b, n * half[:, None])
+    np.add.at(dvel, a, -n * dv[:, None]); np.add.at(dvel, b, n * dv[:, None])
+    c = np.array([o.nx / 2, o.ny / 2, o.nz / 2], np.float64) * o.dx
+    band = o.scalars.oceanR - o.dx * 2
+    r2 = ((X - c) ** 2).sum(1)
+    liq = np.nonzero(((f == 0) & (r2 >= band * band)) | (f == 1) | (f == 4))[0]
+    tw = cKDTree(X[liq])
+    hits = tw.query_ball_tree(tp, rad * 1.001)
+    w = np.repeat(liq, [len(h) for h in hits])
+    bp = par[np.concatenate([np.asarray(h, np.int64) for h in hits])] if len(w) else np.zeros(0, np.int64)
+    d = X[bp] - X[w]
+    d2 = (d * d).sum(1)
+    keep = (d2 < rad * rad) & (d2 >= 1e-12)
+    w, bp, d, d2 = w[keep], bp[keep], d[keep], d2[keep]
+    dd = np.sqrt(d2)
+    n = d / dd[:, None]
+    vr = ((V[bp] - V[w]) * n).sum(1)
+    ov = rad - dd
+    dvl = ov * 2 - np.where(vr < 0, vr * 1.4, 0)
+    np.add.at(dpos, bp, n * ov[:, None])
+    np.add.at(dvel, bp, n * dvl[:, None])
+    return X, V, dpos, dvel, len(a), len(w)
+
+
+def test_vapor_contacts_jacobi():
+    """Vapour-vapour and liquid-vapour contacts of 6000 parcels placed in the
+    surface shell (steam and cloud), against a k-d tree restatement of the
+    device's snapshot order: the same contact set, increments summed in FP32
+    atomics on the device."""
+    o = _state64()
+    nP = o.nP
+    rng = np.random.default_rng(21)
+    c = o.nx / 2
+    R = o.scalars.oceanR
+    m = 6000
+    sel = rng.choice(nP, m, replace=False)
+    d = rng.normal(size=(m, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    r = R + rng.uniform(-0.6, 0.3, m)
+    o.px[sel] = c + d[:, 0] * r; o.py[sel] = c + d[:, 1] * r; o.pz[sel] = c + d[:, 2] * r
+    o.pvx[sel] = rng.normal(0, 0.5, m); o.pvy[sel] = rng.normal(0, 0.5, m); o.pvz[sel] = rng.normal(0, 0.5, m)
+    o.pflag[sel] = rng.choice([2, 3], m)
+    fs = to_device(o)
+    rad = o.scalars.spacing * 0.6
+    X, V, dpos, dvel, nvv, nvl = _jacobi_vapor_contacts(o, rad)
+    assert nvv > 20 and nvl > 200
+    fs.stage("VAPOR_COLLISIONS")
+    assert fs.scalars.vaporCount == int(np.count_nonzero(o.pflag[:nP] == 2))
+    gX = np.stack([fs.download(k).astype(np.float64) for k in ("px", "py", "pz")], 1)
+    gV = np.stack([fs.download(k).astype(np.float64) for k in ("pvx", "pvy", "pvz")], 1)
+    tol_x = 1e-5 + 1e-5 * np.abs(dpos).max()
+    tol_v = 1e-5 + 1e-5 * np.abs(dvel).max()
+    assert np.abs(gX - (X + dpos)).max() <= tol_x
+    assert np.abs(gV - (V + dvel)).max() <= tol_v
+
+
 def test_push_surface_parity():
     o = _state64()
     nP = o.nP

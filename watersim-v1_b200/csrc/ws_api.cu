@@ -905,14 +905,14 @@ static ws_status heat(ws_handle* h, double dt) {
 }
 static ws_status contact_scratch(ws_handle* h) {
   if (h->contactScratch) return WS_OK;
-  WS_TRY(cudaMalloc(&h->contactScratch, contacts_scratch_bytes(h->capacity)));
+  WS_TRY(cudaMalloc(&h->contactScratch, contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz)));
   return WS_OK;
 }
 static ws_status evaporation(ws_handle* h, double dt) {
   if (h->P.sunActivity <= 0 || h->P.evapIntensity <= 0) return WS_OK;
   double freezeT = std::max(h->P.meltT, h->P.snowT * 1.05);
   double rate = h->P.sunActivity * h->P.evapIntensity;
-  if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity)) return WS_ERR_STATE;
+  if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz)) return WS_ERR_STATE;
   ws_status s = contact_scratch(h); if (s) return s;
   uint32_t* evS = h->rng + 2;
   if (h->S.nP <= 0) { h->S.evapCount = 0; return WS_OK; }
@@ -975,7 +975,7 @@ static ws_status vapor_collisions(ws_handle* h) {
   double sunRel[3] = { h->P.sunPos[0] - h->d.cx, h->P.sunPos[1] - h->d.cy, h->P.sunPos[2] - h->d.cz };
   ws_status s0 = contact_scratch(h); if (s0) return s0;
   launch_vapor_collisions(h->d, parts_of(h), h->S.spacing, h->S.oceanR, h->P.spinOn, h->P.hasSun, sunRel,
-                          h->contactScratch, contacts_scratch_bytes(h->capacity), h->st, h->stream);
+                          h->contactScratch, contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz), h->st, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
   s = sync_status(h); if (s) return s;
   h->S.vaporCount = h->stHost->vaporCount; h->S.nightVaporCount = h->stHost->nightVapor;
@@ -983,7 +983,7 @@ static ws_status vapor_collisions(ws_handle* h) {
 }
 static ws_status ice_contacts(ws_handle* h) {
   ws_status s0 = contact_scratch(h); if (s0) return s0;
-  launch_ice_contacts(parts_of(h), h->S.spacing, h->contactScratch, contacts_scratch_bytes(h->capacity), h->stream);
+  launch_ice_contacts(parts_of(h), h->S.spacing, h->contactScratch, contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz), h->stream);
   return check_launch(h, 1);
 }
 

@@ -16,6 +16,7 @@ struct ContactScratch {
   int *idxA, *idxB, *blockCounts, *nV;
   uint32_t *keyA, *keyB;
   float *snap, *acc;       // 6 floats per contact particle (x, y, z, vx, vy, vz)
+  int *perm, *rowStart;    // parcels by grid row (j, k): snapshot index, first parcel of each row
   void* cubTemp;
   size_t cubBytes;
 };
@@ -27,11 +28,12 @@ static size_t cub_bytes(int cap) {
   return bytes;
 }
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-size_t contacts_scratch_bytes(int cap) {
+size_t contacts_scratch_bytes(int cap, int rows) {
   size_t nb = (size_t)(cap + 255) / 256 + 1;
-  return align256(4 * (size_t)cap) * 4 + align256(4 * nb) + 256 + align256(24 * (size_t)cap) * 2 + align256(cub_bytes(cap));
+  return align256(4 * (size_t)cap) * 5 + align256(4 * nb) + 256 + align256(24 * (size_t)cap) * 2 +
+         align256(4 * ((size_t)rows + 1)) + align256(cub_bytes(cap));
 }
-static ContactScratch carve(void* base, int cap) {
+static ContactScratch carve(void* base, int cap, int rows) {
   char* p = (char*)base; ContactScratch c;
   size_t nb = (size_t)(cap + 255) / 256 + 1;
   c.idxA = (int*)p; p += align256(4 * (size_t)cap);
@@ -42,6 +44,8 @@ static ContactScratch carve(void* base, int cap) {
   c.nV = (int*)p; p += 256;
   c.snap = (float*)p; p += align256(24 * (size_t)cap);
   c.acc = (float*)p; p += align256(24 * (size_t)cap);
+  c.perm = (int*)p; p += align256(4 * (size_t)cap);
+  c.rowStart = (int*)p; p += align256(4 * ((size_t)rows + 1));
   c.cubTemp = p; c.cubBytes = cub_bytes(cap);
   return c;
 }
@@ -95,9 +99,33 @@ __global__ void k_vv_pairs(const float* __restrict__ snap, int n, double rad, fl
     atomicAdd(&acc[6 * b + 3], (float)(nX * dv)); atomicAdd(&acc[6 * b + 4], (float)(nY * dv)); atomicAdd(&acc[6 * b + 5], (float)(nZ * dv));
   }
 }
-// liquid-vapour contacts (:3433-3478): only the parcel moves
-__global__ void k_vl_pairs(Dims d, PartsDev P, const float* __restrict__ snap, int n, double rad, double bandLo2,
-                           float* __restrict__ acc) {
+// Grid rows (j, k) of the snapshot's parcels. The snapshot is in x order and
+// the row sort is stable, so each row's parcels stay in x order.
+__global__ void k_row_keys(Dims d, const float* __restrict__ snap, int n, uint32_t* __restrict__ key,
+                           int* __restrict__ val) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int j = jtrunc(over_dx(d, snap[6 * i + 1])), k = jtrunc(over_dx(d, snap[6 * i + 2]));
+  j = j < 0 ? 0 : (j >= d.ny ? d.ny - 1 : j);
+  k = k < 0 ? 0 : (k >= d.nz ? d.nz - 1 : k);
+  key[i] = (uint32_t)(k * d.ny + j);
+  val[i] = i;
+}
+// rowStart[r] = first sorted parcel with row >= r, for r = 0 .. rows (rowStart[rows] = n)
+__global__ void k_row_starts(const uint32_t* __restrict__ key, int n, int rows, int* __restrict__ rowStart) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > rows) return;
+  int lo = 0, hi = n;
+  while (lo < hi) { int mid = (lo + hi) >> 1; if (key[mid] < (uint32_t)r) lo = mid + 1; else hi = mid; }
+  rowStart[r] = lo;
+}
+// liquid-vapour contacts (:3433-3478): only the parcel moves. The reference
+// tests every parcel of the x-sorted list within rad in x; the device tests
+// the same condition on the parcels of the grid rows that rad reaches in y
+// and z (a parcel outside them is farther than rad), so the contact set is
+// the same.
+__global__ void k_vl_pairs(Dims d, PartsDev P, const float* __restrict__ snap, const int* __restrict__ perm,
+                           const int* __restrict__ rowStart, double rad, double bandLo2, float* __restrict__ acc) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nP) return;
   int fw = P.pflag[p];
@@ -107,21 +135,30 @@ __global__ void k_vl_pairs(Dims d, PartsDev P, const float* __restrict__ snap, i
     double ex = wx - d.cx, ey = wy - d.cy, ez = wz - d.cz;
     if (ex * ex + ey * ey + ez * ez < bandLo2) return;
   }
-  int lo = 0, hi = n;
-  while (lo < hi) { int mid = (lo + hi) >> 1; if ((double)snap[6 * mid] < wx - rad) lo = mid + 1; else hi = mid; }
+  const double radq = rad + 1e-6 * d.dx;         // rows reached, widened past rounding
+  int j0 = jfloor_clamp(over_dx(d, wy - radq), 0, d.ny - 1), j1 = jfloor_clamp(over_dx(d, wy + radq), 0, d.ny - 1);
+  int k0 = jfloor_clamp(over_dx(d, wz - radq), 0, d.nz - 1), k1 = jfloor_clamp(over_dx(d, wz + radq), 0, d.nz - 1);
   double wvx = P.pvx[p], wvy = P.pvy[p], wvz = P.pvz[p], rad2 = rad * rad;
-  for (int b = lo; b < n; b++) {
-    const float* B = snap + 6 * b;
-    double ddx = (double)B[0] - wx;
-    if (ddx >= rad) break;
-    double ddy = (double)B[1] - wy, ddz = (double)B[2] - wz;
-    double dd2 = ddx * ddx + ddy * ddy + ddz * ddz;
-    if (dd2 >= rad2 || dd2 < 1e-12) continue;
-    double dd = sqrt(dd2), nX = ddx / dd, nY = ddy / dd, nZ = ddz / dd;
-    double vR = ((double)B[3] - wvx) * nX + ((double)B[4] - wvy) * nY + ((double)B[5] - wvz) * nZ;
-    double ov = rad - dd, dv = ov * 2 - (vR < 0 ? vR * 1.4 : 0);
-    atomicAdd(&acc[6 * b + 0], (float)(nX * ov)); atomicAdd(&acc[6 * b + 1], (float)(nY * ov)); atomicAdd(&acc[6 * b + 2], (float)(nZ * ov));
-    atomicAdd(&acc[6 * b + 3], (float)(nX * dv)); atomicAdd(&acc[6 * b + 4], (float)(nY * dv)); atomicAdd(&acc[6 * b + 5], (float)(nZ * dv));
+  for (int k = k0; k <= k1; k++) {
+    for (int j = j0; j <= j1; j++) {
+      const int r = k * d.ny + j;
+      const int m1 = rowStart[r + 1];
+      for (int m = rowStart[r]; m < m1; m++) {
+        const int b = perm[m];
+        const float* B = snap + 6 * b;
+        if ((double)B[0] < wx - rad) continue;
+        double ddx = (double)B[0] - wx;
+        if (ddx >= rad) break;                     // the row is in x order
+        double ddy = (double)B[1] - wy, ddz = (double)B[2] - wz;
+        double dd2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        if (dd2 >= rad2 || dd2 < 1e-12) continue;
+        double dd = sqrt(dd2), nX = ddx / dd, nY = ddy / dd, nZ = ddz / dd;
+        double vR = ((double)B[3] - wvx) * nX + ((double)B[4] - wvy) * nY + ((double)B[5] - wvz) * nZ;
+        double ov = rad - dd, dv = ov * 2 - (vR < 0 ? vR * 1.4 : 0);
+        atomicAdd(&acc[6 * b + 0], (float)(nX * ov)); atomicAdd(&acc[6 * b + 1], (float)(nY * ov)); atomicAdd(&acc[6 * b + 2], (float)(nZ * ov));
+        atomicAdd(&acc[6 * b + 3], (float)(nX * dv)); atomicAdd(&acc[6 * b + 4], (float)(nY * dv)); atomicAdd(&acc[6 * b + 5], (float)(nZ * dv));
+      }
+    }
   }
 }
 __global__ void k_apply(PartsDev P, const int* __restrict__ idx, int n, const float* __restrict__ acc) {
@@ -153,15 +190,22 @@ void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, d
   cudaMemsetAsync(&st->vaporCount, 0, 2 * sizeof(int), s);
   if (P.nP <= 0) return;
   k_vapor_census<<<grid_for(P.nP, 256), 256, 0, s>>>(d, P, hasSun, sunRel[0], sunRel[1], sunRel[2], st);
-  ContactScratch c = carve(scratch, P.nP > 0 ? P.nP : 1);
+  const int rows = d.ny * d.nz;
+  ContactScratch c = carve(scratch, P.nP > 0 ? P.nP : 1, rows);
   int hostN = 0;
   int n = sorted_list(P, 0, c, &hostN, s);
   if (n < 2) return;
   double rad = spacing * 0.6;
   k_snapshot<<<grid_for(n, 256), 256, 0, s>>>(P, c.idxB, n, c.snap, c.acc);
   k_vv_pairs<<<grid_for(n, 128), 128, 0, s>>>(c.snap, n, rad, c.acc);
+  int rowBits = 1;
+  while ((1ll << rowBits) < (long long)rows) rowBits++;
+  k_row_keys<<<grid_for(n, 256), 256, 0, s>>>(d, c.snap, n, c.keyA, c.idxA);
+  size_t bytes = c.cubBytes;
+  cub::DeviceRadixSort::SortPairs(c.cubTemp, bytes, c.keyA, c.keyB, c.idxA, c.perm, n, 0, rowBits, s);
+  k_row_starts<<<grid_for(rows + 1, 256), 256, 0, s>>>(c.keyB, n, rows, c.rowStart);
   double band = oceanR - d.dx * 2;
-  k_vl_pairs<<<grid_for(P.nP, 256), 256, 0, s>>>(d, P, c.snap, n, rad, band * band, c.acc);
+  k_vl_pairs<<<grid_for(P.nP, 256), 256, 0, s>>>(d, P, c.snap, c.perm, c.rowStart, rad, band * band, c.acc);
   k_apply<<<grid_for(n, 256), 256, 0, s>>>(P, c.idxB, n, c.acc);
 }
 
@@ -209,7 +253,7 @@ __global__ void k_ice_flags(const uint8_t* __restrict__ fl, int nP, uint8_t* __r
 void launch_ice_contacts(const PartsDev& P, double spacing, void* scratch, size_t scratchBytes, cudaStream_t s) {
   (void)scratchBytes;
   if (P.nP <= 1) return;
-  ContactScratch c = carve(scratch, P.nP);
+  ContactScratch c = carve(scratch, P.nP, 1);
   // ice list: compact pflag == 5 via a byte predicate in the snapshot buffer
   uint8_t* pred = (uint8_t*)c.acc;
   k_ice_flags<<<grid_for(P.nP, 256), 256, 0, s>>>(P.pflag, P.nP, pred);

@@ -114,4 +114,4 @@ void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, d
                              int hasSun, const double* sunRel, void* scratch, size_t scratchBytes,
                              DevStatus* st, cudaStream_t s);
 void launch_ice_contacts(const PartsDev& P, double spacing, void* scratch, size_t scratchBytes, cudaStream_t s);
-size_t contacts_scratch_bytes(int capacity);
+size_t contacts_scratch_bytes(int capacity, int rows);   // rows: ny * nz of the grid
