@@ -90,23 +90,39 @@ __global__ void __launch_bounds__(1024) k_sor_scan(const int* __restrict__ block
   }
   if (threadIdx.x == 0) { total[0] = w0[nw - 1]; total[1] = w1[nw - 1]; }
 }
-__global__ void k_sor_scatter(Dims d, const float* __restrict__ pw, const float* __restrict__ rhs,
-                              const uint8_t* __restrict__ diag8, const int* __restrict__ offs, SorLists L) {
-  __shared__ int wt0[32], wt1[32];
-  unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
-  int col = sor_colour(d, pw, c);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned m0 = __ballot_sync(0xffffffffu, col == 0), m1 = __ballot_sync(0xffffffffu, col == 1);
-  if (lane == 0) { wt0[wid] = __popc(m0); wt1[wid] = __popc(m1); }
-  __syncthreads();
-  if (col >= 0) {
-    unsigned m = col ? m1 : m0;
-    int rank = __popc(m & ((1u << lane) - 1u));
-    int off = offs[2 * blockIdx.x + col];
-    for (int w = 0; w < wid; w++) off += col ? wt1[w] : wt0[w];
-    int e = off + rank;
-    L.idx[col][e] = (int)c; L.rhs[col][e] = rhs[c]; L.pw[col][e] = pw[c]; L.dg[col][e] = diag8[c];
-    L.pos[c] = e;
+// Persistent over the 256-cell chunks the pressure setup counted (chunk b
+// holds cells 256 b .. 256 b + 255 and its list offsets are offs[2 b], offs[2 b
+// + 1]); the next chunk's colours and offsets are fetched before this chunk's
+// ranks are formed. Warp totals are double-buffered: one barrier per chunk.
+__global__ void __launch_bounds__(256) k_sor_scatter(Dims d, const float* __restrict__ pw, const float* __restrict__ rhs,
+                                                     const uint8_t* __restrict__ diag8, const int* __restrict__ offs,
+                                                     SorLists L, int nChunks) {
+  __shared__ int wt[2][2][8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int b = blockIdx.x;
+  unsigned c = (unsigned)b * 256u + threadIdx.x;
+  int col = b < nChunks ? sor_colour(d, pw, c) : -1;
+  int o0 = b < nChunks ? offs[2 * b] : 0, o1 = b < nChunks ? offs[2 * b + 1] : 0;
+  int buf = 0;
+  for (; b < nChunks; b += gridDim.x) {
+    const int bn = b + (int)gridDim.x;
+    const unsigned cn = (unsigned)bn * 256u + threadIdx.x;
+    const int coln = bn < nChunks ? sor_colour(d, pw, cn) : -1;
+    const int o0n = bn < nChunks ? offs[2 * bn] : 0, o1n = bn < nChunks ? offs[2 * bn + 1] : 0;
+    const unsigned m0 = __ballot_sync(0xffffffffu, col == 0), m1 = __ballot_sync(0xffffffffu, col == 1);
+    if (lane == 0) { wt[buf][0][wid] = __popc(m0); wt[buf][1][wid] = __popc(m1); }
+    __syncthreads();
+    if (col >= 0) {
+      const unsigned m = col ? m1 : m0;
+      int e = (col ? o1 : o0) + __popc(m & ((1u << lane) - 1u));
+      for (int w = 0; w < wid; w++) e += wt[buf][col][w];
+      (col ? L.idx[1] : L.idx[0])[e] = (int)c;      // selects, not a dynamic index into the parameter
+      (col ? L.rhs[1] : L.rhs[0])[e] = rhs[c];
+      (col ? L.pw[1] : L.pw[0])[e] = pw[c];
+      (col ? L.dg[1] : L.dg[0])[e] = diag8[c];
+      L.pos[c] = e;
+    }
+    c = cn; col = coln; o0 = o0n; o1 = o1n; buf ^= 1;
   }
 }
 // neighbour codes (-x, +x, -y, +y, -z, +z) for the cluster solve: the owner
@@ -120,9 +136,11 @@ __global__ void k_sor_codes(Dims d, const float* __restrict__ pw, SorLists L, in
   const int S = (nOther + C - 1) / C, Sown = (n + C - 1) / C;
   const long long nx = d.nx, nxy = (long long)d.nx * d.ny;
   const long long stride = (long long)gridDim.x * blockDim.x;
+  const int* __restrict__ idx = col ? L.idx[1] : L.idx[0];   // selects, not a dynamic index into the parameter
+  uint16_t* __restrict__ codes = col ? L.code[1] : L.code[0];
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 6LL * n; t += stride) {
     const int e = (int)(t / 6), q = (int)(t - (long long)e * 6);
-    const long long c = L.idx[col][e];
+    const long long c = idx[e];
     const long long nb = c + (q == 0 ? -1 : q == 1 ? 1 : q == 2 ? -nx : q == 3 ? nx : q == 4 ? -nxy : nxy);
     // a non-fluid neighbour reads the owner CTA's own zero slot (no remote traffic)
     uint16_t code = (uint16_t)(((e / Sown) << 12) | kSmax);
@@ -131,7 +149,7 @@ __global__ void k_sor_codes(Dims d, const float* __restrict__ pw, SorLists L, in
       const int r = e2 / S, slot = e2 - r * S;
       code = (uint16_t)((r << 12) | slot);
     }
-    L.code[col][t] = code;
+    codes[t] = code;
   }
 }
 
@@ -592,7 +610,7 @@ cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, co
   // the per-block colour counts come from the pressure setup (k_pressure_setup)
   int nb = (int)grid_for(d.nCells, 256);
   k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->blockOffs, S->L.count);
-  k_sor_scatter<<<nb, 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockOffs, S->L);
+  k_sor_scatter<<<std::min(nb, 148 * 8), 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockOffs, S->L, nb);
   cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
   int C = S->clusterSize;
   if (C) {
