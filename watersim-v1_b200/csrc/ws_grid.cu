@@ -92,15 +92,20 @@ void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_
 // ------------------------------------------------------------ 1. clear + raster
 // u..wW.fill(0) (js/solver.js:2569-2570) and cellType <- static types
 // (:865-871). Bytes: 8F (acc) + 2N.
+// 16-byte stores: two faces of the accumulator, sixteen cell types per
+// thread (both buffers are separate allocations, 256-byte aligned).
 __global__ void k_clear_raster(Dims d, GridDev g, DevStatus* st) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t < d.F) g.acc[t] = make_float2(0.f, 0.f);
-  if (t < d.nCells) g.type[t] = g.staticTypes[t];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long F2 = d.F >> 1, n16 = d.nCells >> 4;
+  if (t < F2) reinterpret_cast<float4*>(g.acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+  else if (t == F2 && (d.F & 1)) g.acc[d.F - 1] = make_float2(0.f, 0.f);
+  if (t < n16) reinterpret_cast<uint4*>(g.type)[t] = reinterpret_cast<const uint4*>(g.staticTypes)[t];
+  else if (t < n16 + (d.nCells & 15)) { const long long c = (n16 << 4) + (t - n16); g.type[c] = g.staticTypes[c]; }
   if (t == 0) { st->umaxBits = 0u; st->airborne = 0; st->nFluid = 0; }
 }
 void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s) {
-  long long n = d.F > d.nCells ? d.F : d.nCells;
-  k_clear_raster<<<grid_for(n, 256), 256, 0, s>>>(d, g, st);
+  const long long a = (d.F >> 1) + 1, b = (d.nCells >> 4) + 16;
+  k_clear_raster<<<grid_for(a > b ? a : b, 256), 256, 0, s>>>(d, g, st);
 }
 
 // ------------------------------------------------------------ 2. mark fluid
@@ -108,8 +113,9 @@ void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStr
 __global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nP) return;
-  if (P.pflag[p] != 0) return;
-  double X = P.px[p], Y = P.py[p], Z = P.pz[p];
+  const int fl = P.pflag[p];                     // issued with the position loads
+  const double X = P.px[p], Y = P.py[p], Z = P.pz[p];
+  if (fl != 0) return;
   double rx = X - d.cx, ry = Y - d.cy, rz = Z - d.cz;
   double radius2 = rx * rx + ry * ry + rz * rz;
   double skyAlt = 2 * d.dx > 0.3 ? 2 * d.dx : 0.3;
@@ -151,11 +157,14 @@ __device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc
 __global__ void k_p2g(Dims d, GridDev g, PartsDev P) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P.nP) return;
-  if (P.pflag[p] != 0) return;
-  double x = P.px[p], y = P.py[p], z = P.pz[p];
-  p2g_comp(d, g.acc, 0, x, y, z, P.pvx[p]);
-  p2g_comp(d, g.acc, 1, x, y, z, P.pvy[p]);
-  p2g_comp(d, g.acc, 2, x, y, z, P.pvz[p]);
+  // every load of the particle is issued before the flag test (one round trip)
+  const int fl = P.pflag[p];
+  const double x = P.px[p], y = P.py[p], z = P.pz[p];
+  const float vx = P.pvx[p], vy = P.pvy[p], vz = P.pvz[p];
+  if (fl != 0) return;
+  p2g_comp(d, g.acc, 0, x, y, z, vx);
+  p2g_comp(d, g.acc, 1, x, y, z, vy);
+  p2g_comp(d, g.acc, 2, x, y, z, vz);
 }
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s) {
   if (P.nP <= 0) return;
