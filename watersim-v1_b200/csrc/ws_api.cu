@@ -56,6 +56,8 @@ struct ws_handle {
   int* cellCnt = nullptr;
   double *cellSum = nullptr, *cellChange = nullptr;
   void* contactScratch = nullptr;       // allocated on first contact pass
+  void* mtScratch = nullptr;            // straddling-cell list of the marching tets, grown on demand
+  size_t mtScratchBytes = 0;
   void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
   // substep graph: the kernel sequence of one substep captured once and
   // replayed while its launch parameters stay the same
@@ -170,6 +172,7 @@ static void free_all(ws_handle* h) {
                    h->parts.pflag, h->parts.pcool, h->parts.pDepth };
   for (void* b : bufs) if (b) cudaFree(b);
   if (h->contactScratch) cudaFree(h->contactScratch);
+  if (h->mtScratch) cudaFree(h->mtScratch);
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->net) { h->net->destroy(); delete h->net; }
@@ -577,10 +580,23 @@ extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
 }
 
 // ------------------------------------------------------------ reductions
+static ws_status mt_scratch(ws_handle* h, long long nCells, void** out) {
+  const size_t need = mt_scratch_bytes(nCells);
+  if (need > h->mtScratchBytes) {
+    if (h->mtScratch) cudaFree(h->mtScratch);
+    h->mtScratch = nullptr; h->mtScratchBytes = 0;
+    WS_TRY(cudaMalloc(&h->mtScratch, need));
+    h->mtScratchBytes = need;
+  }
+  *out = h->mtScratch;
+  return WS_OK;
+}
 static ws_status mt_volume(ws_handle* h, double iso, double* vol, int64_t* cnt) {
   if ((long long)grid_for(h->d.nCells, 128) > h->partialsCap) return fail(h, WS_ERR_RANGE, "partials too small");
-  launch_mt_volume(h->d, h->dens, iso, h->partials, h->red, h->stream);
-  ws_status s = check_launch(h, 2); if (s) return s;
+  void* scr = nullptr;
+  ws_status s = mt_scratch(h, h->d.nCells, &scr); if (s) return s;
+  launch_mt_volume(h->d, h->dens, iso, h->partials, h->red, scr, h->stream);
+  s = check_launch(h, 6); if (s) return s;
   WS_TRY(cudaMemcpyAsync(h->redHost, h->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
   if (vol) *vol = std::fabs(h->redHost[0]);
@@ -1632,8 +1648,10 @@ extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
 static ws_status mt_build(ws_handle* h, const Dims& dd, const float* field, double iso, double2* partials, MeshBuf& mb,
                           int64_t* vertices, double* volume) {
   const long long nb = grid_for(dd.nCells, 128);
-  launch_mt_volume(dd, field, iso, partials, h->red, h->stream);
-  ws_status s = check_launch(h, 2); if (s) return s;
+  void* scr = nullptr;
+  ws_status s = mt_scratch(h, dd.nCells, &scr); if (s) return s;
+  launch_mt_volume(dd, field, iso, partials, h->red, scr, h->stream);
+  s = check_launch(h, 6); if (s) return s;
   WS_TRY(cudaMemcpyAsync(h->redHost, h->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
   const double vol = std::fabs(h->redHost[0]);
@@ -1653,7 +1671,7 @@ static ws_status mt_build(ws_handle* h, const Dims& dd, const float* field, doub
     WS_TRY(cudaMalloc(&mb.nrm, sizeof(float) * 3 * (size_t)cap));
     mb.cap = cap;
   }
-  launch_mt_mesh(dd, field, iso, partials, mb.offs, mb.cap, mb.pos, mb.nrm, h->stream);
+  launch_mt_mesh(dd, field, iso, partials, mb.offs, mb.cap, mb.pos, mb.nrm, scr, h->stream);
   if ((s = check_launch(h, 2))) return s;
   WS_TRY(cudaStreamSynchronize(h->stream));
   mb.verts = cnt;

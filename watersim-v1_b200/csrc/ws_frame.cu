@@ -762,31 +762,52 @@ __device__ double mt_cell(const float* __restrict__ dens, int nx, int ny, int nz
   }
   return vol;
 }
-// Block partial sums of the signed volume (FP64) and the vertex count.
-__global__ void __launch_bounds__(128, 8) k_mt_partial(Dims d, const float* __restrict__ dens, double iso, double2* __restrict__ partials) {
-  __shared__ double sv[32], sc[32];
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double vol = 0, cnt = 0;
-  if (c < d.nCells) {
-    int i, j, k; cell_ijk(d, c, i, j, k);
-    int v;
-    vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
-    cnt = v;
-  }
-  vol = warp_sum(vol); cnt = warp_sum(cnt);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { sv[wid] = vol; sc[wid] = cnt; }
-  __syncthreads();
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    vol = lane < nw ? sv[lane] : 0; cnt = lane < nw ? sc[lane] : 0;
+// Cells whose corners straddle iso (the only ones mt_cell emits triangles
+// for) are listed first, in index order, so the triangle work runs on full
+// warps: about 2% of the cells of an ocean planet's lattice.
+__global__ void k_mt_flags(Dims d, const float* __restrict__ dens, double iso, uint8_t* __restrict__ flag) {
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= d.nCells) return;
+  int i, j, k; cell_ijk(d, c, i, j, k);
+  const long long sj = d.nx + 1, sk = (long long)(d.ny + 1) * sj, b = k * sk + j * sj + i;
+  const float v[8] = { dens[b], dens[b + 1], dens[b + sj], dens[b + sj + 1],
+                       dens[b + sk], dens[b + sk + 1], dens[b + sk + sj], dens[b + sk + sj + 1] };
+  double mn = v[0], mx = v[0];
+#pragma unroll
+  for (int q = 1; q < 8; q++) { mn = fmin(mn, (double)v[q]); mx = fmax(mx, (double)v[q]); }
+  flag[c] = (mx < iso || mn > iso) ? 0 : 1;     // mt_cell's own early-out test
+}
+__device__ __forceinline__ int mt_chunks(const int* nList) { return (*nList + 127) >> 7; }
+// Per 128-entry chunk of the list: partial sums of the signed volume (FP64)
+// and the vertex count. Persistent over the chunks.
+__global__ void __launch_bounds__(128, 8) k_mt_partial(Dims d, const float* __restrict__ dens, double iso,
+                                                       const int* __restrict__ list, const int* __restrict__ nList,
+                                                       double2* __restrict__ partials) {
+  __shared__ double sv[4], sc[4];
+  const int n = *nList, nch = mt_chunks(nList);
+  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int e = ch * 128 + (int)threadIdx.x;
+    double vol = 0, cnt = 0;
+    if (e < n) {
+      int i, j, k; cell_ijk(d, list[e], i, j, k);
+      int v;
+      vol = mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
+      cnt = v;
+    }
     vol = warp_sum(vol); cnt = warp_sum(cnt);
-    if (lane == 0) partials[blockIdx.x] = make_double2(vol, cnt);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sv[wid] = vol; sc[wid] = cnt; }
+    __syncthreads();
+    if (threadIdx.x == 0) partials[ch] = make_double2(sv[0] + sv[1] + sv[2] + sv[3], sc[0] + sc[1] + sc[2] + sc[3]);
+    __syncthreads();                              // sv, sc are rewritten by the next chunk
   }
 }
-// Fixed-order final reduction of double2 partials into out[0..1].
-__global__ void k_reduce_pairs(const double2* __restrict__ partials, int n, double* __restrict__ out) {
+// Fixed-order final reduction of double2 partials into out[0..1]; nDev (when
+// given) holds a list length whose 128-entry chunks are the partials.
+__global__ void k_reduce_pairs(const double2* __restrict__ partials, int n, double* __restrict__ out,
+                               const int* __restrict__ nDev = nullptr) {
   __shared__ double sa[32], sb[32];
+  if (nDev) n = mt_chunks(nDev);
   double a = 0, b = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) { a += partials[i].x; b += partials[i].y; }
   a = warp_sum(a); b = warp_sum(b);
@@ -800,18 +821,34 @@ __global__ void k_reduce_pairs(const double2* __restrict__ partials, int n, doub
     if (lane == 0) { out[0] = a; out[1] = b; }
   }
 }
-void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s) {
-  int nb = (int)grid_for(d.nCells, 128);
-  k_mt_partial<<<nb, 128, 0, s>>>(d, dens, iso, partials);
-  k_reduce_pairs<<<1, 1024, 0, s>>>(partials, nb, out);
+size_t mt_scratch_bytes(long long nCells) {
+  return (size_t)nCells + 4 * (size_t)nCells + 4 * (size_t)((nCells + 255) / 256 + 1) + 64;
+}
+static void mt_carve(void* scratch, long long nCells, uint8_t*& flag, int*& list, int*& blockCounts, int*& nList) {
+  char* q = (char*)scratch;
+  list = (int*)q; q += 4 * (size_t)nCells;
+  blockCounts = (int*)q; q += 4 * (size_t)((nCells + 255) / 256 + 1);
+  nList = (int*)q; q += 64;
+  flag = (uint8_t*)q;
+}
+void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, void* scratch,
+                      cudaStream_t s) {
+  uint8_t* flag; int *list, *blockCounts, *nList;
+  mt_carve(scratch, d.nCells, flag, list, blockCounts, nList);
+  k_mt_flags<<<grid_for(d.nCells, 256), 256, 0, s>>>(d, dens, iso, flag);
+  launch_compact(flag, (int)d.nCells, 2, blockCounts, list, nList, s);
+  const int nb = (int)std::min<long long>(grid_for(d.nCells, 128), 148 * 8);
+  k_mt_partial<<<nb, 128, 0, s>>>(d, dens, iso, list, nList, partials);
+  k_reduce_pairs<<<1, 1024, 0, s>>>(partials, 0, out, nList);
 }
 
 // Mesh emission in the reference's order (cells in index order, then tets,
-// then case triangles): exclusive scan of the per-block vertex counts that
-// k_mt_partial left in partials[b].y, then each block places its cells'
-// vertices by a block scan of their counts.
-__global__ void k_mt_offsets(const double2* __restrict__ partials, int nb, long long* __restrict__ offs) {
+// then case triangles): exclusive scan of the per-chunk vertex counts that
+// k_mt_partial left in partials[ch].y, then each chunk of the straddling-cell
+// list places its cells' vertices by a block scan of their counts.
+__global__ void k_mt_offsets(const double2* __restrict__ partials, const int* __restrict__ nList, long long* __restrict__ offs) {
   __shared__ long long ws[32], carry;
+  const int nb = mt_chunks(nList);
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -834,32 +871,41 @@ __global__ void k_mt_offsets(const double2* __restrict__ partials, int nb, long 
     __syncthreads();
   }
 }
-__global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restrict__ dens, double iso, const long long* __restrict__ offs,
-                          long long maxVerts, float* __restrict__ pos, float* __restrict__ nrm) {
+__global__ void __launch_bounds__(128, 8) k_mt_emit(Dims d, const float* __restrict__ dens, double iso,
+                                                    const int* __restrict__ list, const int* __restrict__ nList,
+                                                    const long long* __restrict__ offs, long long maxVerts,
+                                                    float* __restrict__ pos, float* __restrict__ nrm) {
   __shared__ int ws[4];
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  int i = 0, j = 0, k = 0, v = 0;
-  if (c < d.nCells) {
-    cell_ijk(d, c, i, j, k);
-    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
-  }
-  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, x = v;
-  for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
-  if (lane == 31) ws[w] = x;
-  __syncthreads();
-  int before = 0;
-  for (int q = 0; q < w; q++) before += ws[q];
-  const long long base = offs[blockIdx.x] + before + x - v;
-  if (v > 0 && base + v <= maxVerts) {
-    int v2;
-    mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v2, pos, nrm, base);
+  const int n = *nList, nch = mt_chunks(nList);
+  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int e = ch * 128 + (int)threadIdx.x;
+    int i = 0, j = 0, k = 0, v = 0;
+    if (e < n) {
+      cell_ijk(d, list[e], i, j, k);
+      mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    int before = 0;
+    for (int q = 0; q < w; q++) before += ws[q];
+    const long long base = offs[ch] + before + x - v;
+    if (v > 0 && base + v <= maxVerts) {
+      int v2;
+      mt_cell(dens, d.nx, d.ny, d.nz, d.dx, d.dxPow2 != 0, 0.5 * d.rdx, iso, i, j, k, v2, pos, nrm, base);
+    }
+    __syncthreads();                              // ws is rewritten by the next chunk
   }
 }
 void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
-                    long long maxVerts, float* pos, float* nrm, cudaStream_t s) {
-  int nb = (int)grid_for(d.nCells, 128);
-  k_mt_offsets<<<1, 1024, 0, s>>>(partials, nb, offs);
-  k_mt_emit<<<nb, 128, 0, s>>>(d, dens, iso, offs, maxVerts, pos, nrm);
+                    long long maxVerts, float* pos, float* nrm, void* scratch, cudaStream_t s) {
+  uint8_t* flag; int *list, *blockCounts, *nList;
+  mt_carve(scratch, d.nCells, flag, list, blockCounts, nList);
+  const int nb = (int)std::min<long long>(grid_for(d.nCells, 128), 148 * 8);
+  k_mt_offsets<<<1, 1024, 0, s>>>(partials, nList, offs);
+  k_mt_emit<<<nb, 128, 0, s>>>(d, dens, iso, list, nList, offs, maxVerts, pos, nrm);
 }
 
 // ------------------------------------------------------------ particle reductions

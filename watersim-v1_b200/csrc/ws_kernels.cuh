@@ -77,11 +77,15 @@ void launch_push_surface(const Dims& d, const GridDev& g, const PartsDev& P, con
 void launch_splat(const Dims& d, const GridDev& g, const PartsDev& P, double spacing, cudaStream_t s);
 void launch_currents(const Dims& d, const PartsDev& P, const CurrField& F, double simTime, double strength,
                      double oceanR, double coreR, double dt, cudaStream_t s);
-void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, cudaStream_t s);
-// the marching-tets mesh after launch_mt_volume at the same iso (which leaves
-// the per-block vertex counts in partials): vertices in build order
+// scratch: mt_scratch_bytes(d.nCells) bytes (the straddling-cell list)
+size_t mt_scratch_bytes(long long nCells);
+void launch_mt_volume(const Dims& d, const float* dens, double iso, double2* partials, double* out, void* scratch,
+                      cudaStream_t s);
+// the marching-tets mesh after launch_mt_volume at the same iso and scratch
+// (which leave the cell list and its per-chunk vertex counts): vertices in
+// build order
 void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2* partials, long long* offs,
-                    long long maxVerts, float* pos, float* nrm, cudaStream_t s);
+                    long long maxVerts, float* pos, float* nrm, void* scratch, cudaStream_t s);
 // render-side particle prep: classify, bucket-sort far to near, emit the
 // draw list (ws_render.cu); counts land in the first five scratch words
 // balls (ws_balls.cu): moving-solid raster (after the static raster),
