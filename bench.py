@@ -347,7 +347,8 @@ def roofline(fs, ms_step, iters):
     #  P2G           25 B per particle in + 8 B per face accumulator
     #  G2P+advect    52 B per particle + 8 B per face (u and uO)
     #  faces pass 1  8 B acc + 9 B out per face; forces 12 B per face; project 8 B per face
-    sor_name = "k_sor_cluster" if s.sorPath == 2 else "k_sor_persistent"
+    # the path the timed solve took (its own diagnostics, read after it ran)
+    sor_name = "k_sor_cluster" if fs.scalars.sorPath == 2 else "k_sor_persistent"
     cand = {sor_name: (us_sor, 13.0 * nF * it),
             "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
             "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),
