@@ -341,23 +341,29 @@ __global__ void k_head_train(Level L, const int* tiles, const int* count, const 
 // FP32 master W[co][ci][27] -> the packed BF16 operand of the forward conv,
 // [ci/16][27][2][co][8], and of the backward-data conv (cin' = co, cout' =
 // ci, taps mirrored), [co/16][27][2][ci][8]
+// Packed B operands of k_conv3, per 16-channel input slice kk: for each of
+// the 9 in-plane taps g = 3 dy + dx, two K halves j (channels 8 j .. 8 j + 7),
+// and in each half the rows of the three z taps in the order dz = 2, 1, 0
+// (tap t = 9 dz + g), so the rows of consecutive z taps are contiguous along N.
 __global__ void k_pack(const float* __restrict__ W, int cin, int cout, bf16* __restrict__ fw, bf16* __restrict__ bw) {
   int n = 27 * cin * cout;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  {  // forward: i = ((((kk * 27 + t) * 2 + j) * cout + co) * 8 + e)
+  {  // forward: i = (((((kk * 9 + g) * 2 + j) * 3 + (2 - dz)) * cout + co) * 8 + e)
     int e = i & 7, r = i >> 3;
     int co = r % cout; r /= cout;
+    int dz = 2 - r % 3; r /= 3;
     int j = r & 1; r >>= 1;
-    int t = r % 27, kk = r / 27;
-    fw[i] = __float2bfloat16_rn(W[((size_t)co * cin + kk * 16 + j * 8 + e) * 27 + t]);
+    int g = r % 9, kk = r / 9;
+    fw[i] = __float2bfloat16_rn(W[((size_t)co * cin + kk * 16 + j * 8 + e) * 27 + 9 * dz + g]);
   }
-  {  // backward data: i = ((((kk * 27 + t) * 2 + j) * cin + ci) * 8 + e), co = 16 kk + 8 j + e
+  {  // backward data: the same layout over ci, co = 16 kk + 8 j + e, taps mirrored
     int e = i & 7, r = i >> 3;
     int ci = r % cin; r /= cin;
+    int dz = 2 - r % 3; r /= 3;
     int j = r & 1; r >>= 1;
-    int t = r % 27, kk = r / 27;
-    bw[i] = __float2bfloat16_rn(W[((size_t)(kk * 16 + j * 8 + e) * cin + ci) * 27 + (26 - t)]);
+    int g = r % 9, kk = r / 9;
+    bw[i] = __float2bfloat16_rn(W[((size_t)(kk * 16 + j * 8 + e) * cin + ci) * 27 + (26 - (9 * dz + g))]);
   }
 }
 // Adam (Kingma & Ba 2015) on the flat FP32 parameter vector; grad is the sum

@@ -177,6 +177,10 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   fence_after();
   const uint32_t tmem = s_tmem;
   constexpr uint32_t idesc = idesc_bf16_m128(COUT);
+  // N = 2 and 3 COUT (two or three z taps); with ZT = 2 at most two z taps meet one plane
+  constexpr uint32_t idesc2 = idesc_bf16_m128(2 * COUT);
+  constexpr uint32_t idesc3 = idesc_bf16_m128((ZT >= 3 ? 3 : 2) * COUT);
+  static_assert((ZT >= 3 ? 3 : 2) * COUT <= 256 && COUT % 16 == 0, "MMA N out of range");
   uint32_t phase = 0;
   bool pending = false;
 
@@ -196,19 +200,34 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
       __syncthreads();
       if (threadIdx.x == 0) {
         fence_after();
-        // taps outer, planes inner: consecutive MMAs go to different
-        // accumulators, so ZT of them are in flight instead of a chain of
-        // read-modify-writes of one accumulator. Descriptors are base
-        // descriptors plus 16-byte offsets in the start-address field.
-        const uint64_t ad0 = smem_desc(hbase, KSTR, HX * 16), bd0 = smem_desc(wbase, COUT * 16, 128);
-#pragma unroll 1
-        for (int t = 0; t < 27; t++) {
-          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint64_t bd = bd0 + (uint64_t)(t * 2 * COUT);
-          const uint64_t at = ad0 + (uint64_t)((dz * HY + dy) * HX + dx);
+        // Per in-plane tap g = (dy, dx), halo plane p feeds output planes
+        // p - dz for dz = 0..2: one MMA with the B rows of those z taps side
+        // by side along N (k_pack orders them dz = 2, 1, 0) writes the
+        // accumulators of planes p - dzhi .. p - dzlo, which are adjacent in
+        // tensor memory. Each A tile is then read once per (g, p) instead of
+        // once per (g, dz, z). The first tap group initialises every
+        // accumulator plane by plane (dz = 0 first), the later groups only
+        // accumulate. Descriptors are base descriptors plus 16-byte offsets
+        // in the start-address field.
+        const uint64_t ad0 = smem_desc(hbase, KSTR, HX * 16), bd0 = smem_desc(wbase, 3 * COUT * 16, 128);
+        constexpr int GB = 6 * COUT;                 // 16-byte units of one tap group (2 K halves x 3 z taps)
 #pragma unroll
-          for (int z = 0; z < ZT; z++)
-            mma_bf16(tmem + (uint32_t)(z * COUT), at + (uint64_t)(z * HY * HX), bd, idesc, (kk | t) != 0);
+        for (int z = 0; z < ZT; z++)
+#pragma unroll
+          for (int dz = 0; dz < 3; dz++)
+            mma_bf16(tmem + (uint32_t)(z * COUT), ad0 + (uint64_t)((z + dz) * HY * HX),
+                     bd0 + (uint64_t)((2 - dz) * COUT), idesc, (kk | dz) != 0);
+#pragma unroll 1
+        for (int g = 1; g < 9; g++) {
+          const int dy = g / 3, dx = g % 3;
+          const uint64_t ag = ad0 + (uint64_t)(dy * HX + dx), bg = bd0 + (uint64_t)(g * GB);
+#pragma unroll
+          for (int p = 0; p < ZT + 2; p++) {
+            const int dzlo = p > ZT - 1 ? p - (ZT - 1) : 0, dzhi = p < 2 ? p : 2;
+            const uint32_t id = dzhi - dzlo == 0 ? idesc : dzhi - dzlo == 1 ? idesc2 : idesc3;
+            mma_bf16(tmem + (uint32_t)((p - dzhi) * COUT), ag + (uint64_t)(p * HY * HX),
+                     bg + (uint64_t)((2 - dzhi) * COUT), id, 1u);
+          }
         }
         mma_commit(&mbar);
       }
