@@ -117,15 +117,16 @@ __device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, in
   }
   __syncthreads();
   const int cnx = (a.nx + 1) >> 1, cny = (a.ny + 1) >> 1;
-  for (int i = threadIdx.x; i < 2 * HV; i += blockDim.x) {
-    const int j = i & 1, hv = i >> 1;
+  // one voxel per thread and pass, both 8-channel chunks of the slice (the
+  // channel splits c0 are multiples of 16, so both come from one source)
+  for (int hv = threadIdx.x; hv < HV; hv += blockDim.x) {
     const int hx = hv % HX, t2 = hv / HX, hy = t2 % HY, hz = t2 / HY;
     const int gx = X0 - 1 + hx, gy = Y0 - 1 + hy, gz = Z0 - 1 + hz;
     const bf16* p = a.src1 ? a.src1 : a.src0;             // any valid address when nothing is read
     uint32_t n = 0;
     if (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.nx && gy < a.ny && gz < a.nz &&
         s_act[((gz / kTZ - tz0) * 3 + (gy / kTY - ty0)) * 3 + (gx / kTX - tx0)]) {
-      const int c = kk * 16 + j * 8;
+      const int c = kk * 16;
       if (c < a.c0) {
         p = a.up0 ? a.src0 + ((size_t)((gz >> 1) * cny + (gy >> 1)) * cnx + (gx >> 1)) * a.c0 + c
                   : a.src0 + ((size_t)(gz * a.ny + gy) * a.nx + gx) * a.c0 + c;
@@ -134,7 +135,8 @@ __device__ __forceinline__ void stage_halo(const ConvArgs& a, int X0, int Y0, in
       }
       n = 16;
     }
-    cp_async16(hbase + (uint32_t)(j * KSTR + hv * 16), p, n);
+    cp_async16(hbase + (uint32_t)(hv * 16), p, n);
+    cp_async16(hbase + (uint32_t)(KSTR + hv * 16), p + 8, n);
   }
 }
 template <int COUT>
@@ -257,22 +259,25 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
       const int q = warp & 3;                        // tensor-memory lane quarter of this warp
       const int m = q * 32 + lane;                   // accumulator row = voxel of the plane
       const int gx = cX + (m & 7), gy = cY + (m >> 3);
-      for (int z = warp >> 2; z < ZT; z += 2) {
-        const int gz = cZ + z;
-        const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
-        const size_t vox = ((size_t)gz * a.ny + gy) * a.nx + gx;
 #pragma unroll 1
-        for (int cg = 0; cg < COUT / 16; cg++) {
+      for (int cg = 0; cg < COUT / 16; cg++) {
+        const int c = cg * 16;
+        float bias[16];                              // this channel group's bias, once for all planes
+#pragma unroll
+        for (int i = 0; i < 16; i++) bias[i] = a.mode == 0 ? __ldg(a.bias + c + i) : 0.f;
+        for (int z = warp >> 2; z < ZT; z += 2) {
+          const int gz = cZ + z;
+          const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
+          const size_t vox = ((size_t)gz * a.ny + gy) * a.nx + gx;
           uint32_t r[16];
           tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(z * COUT + cg * 16), r);
           if (!in) continue;
           float v[16];
 #pragma unroll
           for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-          const int c = cg * 16;
           if (a.mode == 0) {
 #pragma unroll
-            for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + __ldg(a.bias + c + i), 0.f);
+            for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i] + bias[i], 0.f);
           } else if (a.mask) {
             const uint4* mp = reinterpret_cast<const uint4*>(a.mask + vox * COUT + c);
             uint4 mk[2] = { __ldg(mp), __ldg(mp + 1) };
