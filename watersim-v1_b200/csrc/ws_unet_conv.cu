@@ -466,7 +466,8 @@ size_t conv3_smem_bytes(int cout) {
   }
 }
 cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t s) {
-  if (((a.c0 + a.c1) & 15) || (a.c0 & 7) || (a.c1 & 7) || a.c0 + a.c1 <= 0 || (a.split & 15)) return cudaErrorInvalidValue;
+  // the halo staging takes both 8-channel chunks of a slice from one source: splits are multiples of 16
+  if (((a.c0 + a.c1) & 15) || (a.c0 & 15) || a.c0 + a.c1 <= 0 || (a.split & 15)) return cudaErrorInvalidValue;
   const int zt = conv3_zt(cout);
   if (!zt) return cudaErrorInvalidValue;
   // persistent: at most the CTAs the device holds at once, never more than the work items
