@@ -111,8 +111,7 @@ __global__ void k_residual0(Dims d, const float* __restrict__ q, const float* __
   if (c < d.nCells) {
     float r = 0.f;
     if (type[c] == WS_FLUID) {
-      unsigned cu = (unsigned)c, t = cu / (unsigned)d.nx;
-      int i = (int)(cu - t * (unsigned)d.nx), j = (int)(t % (unsigned)d.ny), k = (int)(t / (unsigned)d.ny);
+      int i, j, k; cell_ijk(d, c, i, j, k);
       long long nx = d.nx, nxy = (long long)d.nx * d.ny;
       double s = 0;
       if (i > 0) s += q[c - 1];
