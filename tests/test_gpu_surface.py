@@ -29,3 +29,9 @@ def test_surface_mesh_matches_oracle(name):
     vol2, pos2, _ = fs.surface_mesh(1.4)
     vref2, pref2, _ = mt_mesh_field(dens, o.nx, o.ny, o.nz, o.dx, 1.4)
     assert np.array_equal(pos2, pref2) and abs(vol2 - vref2) <= 1e-12 * vref2
+    # no straddling cell (iso above every corner, or below every corner): an empty mesh
+    for iso3 in (float(dens.max()) + 1.0, float(dens.min()) - 1.0):
+        vol3, pos3, nrm3 = fs.surface_mesh(iso3)
+        vref3, pref3, _ = mt_mesh_field(dens, o.nx, o.ny, o.nz, o.dx, iso3)
+        assert len(pos3) == len(pref3) == 0 and len(nrm3) == 0
+        assert vol3 == 0.0 and vref3 == 0.0

@@ -24,6 +24,8 @@ struct MeshBuf {
 struct ws_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;          // the SOR list build beside the learned warm start
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   Dims d{};
   ws_params P{};
   ws_scalars S{};
@@ -186,6 +188,9 @@ static void free_all(ws_handle* h) {
   if (h->rdrScratch) cudaFree(h->rdrScratch);
   if (h->stHost) cudaFreeHost(h->stHost);
   if (h->redHost) cudaFreeHost(h->redHost);
+  if (h->evFork) cudaEventDestroy(h->evFork);
+  if (h->evJoin) cudaEventDestroy(h->evJoin);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -207,7 +212,17 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaSetDevice"); delete h; return r; }
   e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaStreamCreate"); delete h; return r; }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    ws_status r = fail_cuda(h, e, "cudaStreamCreate");
+    if (h->evFork) cudaEventDestroy(h->evFork);
+    if (h->evJoin) cudaEventDestroy(h->evJoin);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h; return r;
+  }
   Dims& d = h->d;
   d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.dx = cfg->dx;
   d.W = d.nx * d.dx; d.H = d.ny * d.dx; d.D = d.nz * d.dx;
@@ -728,12 +743,21 @@ static ws_status stage_pressure(ws_handle* h) {
       return fail_cuda(h, e, "warm-start pair (before the solve)");
   }
   if (h->net && h->unetOn) {
+    // the colour lists on the side stream while the network predicts q (they do not read q)
+    WS_TRY(cudaEventRecord(h->evFork, h->stream));
+    WS_TRY(cudaStreamWaitEvent(h->side, h->evFork, 0));
+    if ((e = launch_sor_lists(h->sor, h->d, g, h->diag8, h->side)) != cudaSuccess) return fail_cuda(h, e, "SOR lists");
+    WS_TRY(cudaEventRecord(h->evJoin, h->side));
     if ((e = h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream)) != cudaSuccess)
       return fail_cuda(h, e, "learned warm start");
     h->launches += 23;
+    WS_TRY(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
+    e = launch_sor_run(h->sor, h->d, g, h->P.omega, iters, check, h->P.sorTol, &h->st->err, &dIters, &dRel, &dPath,
+                       h->stream);
+  } else {
+    e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
+                         &h->st->err, &dIters, &dRel, &dPath, h->stream);
   }
-  e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
-                                   &h->st->err, &dIters, &dRel, &dPath, h->stream);
   if (e != cudaSuccess) return fail_cuda(h, e, "SOR solve launch");
   s = check_launch(h, sor_solve_launches(h->sor)); if (s) return s;
   WS_TRY(cudaMemcpyAsync(&h->st->sorIters, dIters, sizeof(int), cudaMemcpyDeviceToDevice, h->stream));

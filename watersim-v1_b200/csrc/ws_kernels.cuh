@@ -106,6 +106,9 @@ void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* part
 // ---- ws_sor.cu
 cudaError_t sor_init(void** statePtr, long long nCells, int device);
 void sor_free(void* statePtr);
+cudaError_t launch_sor_lists(void* state, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s);
+cudaError_t launch_sor_run(void* state, const Dims& d, const GridDev& g, double omega, int iters, int check,
+                           double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s);
 cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
                              int iters, int check, double tol, int* err, int** outIters, double** outRel,
                              int** outPath, cudaStream_t s);

@@ -602,20 +602,31 @@ void sor_free(void* statePtr) {
 // Builds the colour lists from the pressure setup (pw, rhs, diag8) and runs
 // the whole solve. Results land in device memory (iterations, residual);
 // the caller reads them with its next status synchronisation.
-cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
-                             int iters, int check, double tol, int* err, int** outIters, double** outRel,
-                             int** outPath, cudaStream_t s) {
+// The colour lists (scan of the setup's block counts, scatter, neighbour
+// codes) and the barrier reset. They read the pressure setup's rhs, pw and
+// stencil bytes, never q, so they may run beside anything that only writes q
+// (the learned warm start).
+cudaError_t launch_sor_lists(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s) {
   SorState* S = (SorState*)statePtr;
-  *outPath = S->outPath;
   // the per-block colour counts come from the pressure setup (k_pressure_setup)
   int nb = (int)grid_for(d.nCells, 256);
   k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->blockOffs, S->L.count);
   k_sor_scatter<<<std::min(nb, 148 * 8), 256, 0, s>>>(d, g.pw, g.rhs, diag8, S->blockOffs, S->L, nb);
   cudaMemsetAsync(S->bar, 0, sizeof(GridBar), s);     // a solve that timed out leaves no stale arrivals
+  if (S->clusterSize)
+    k_sor_codes<<<dim3((unsigned)std::min<long long>(grid_for(6 * S->cap, 256), 148 * 8), 2), 256, 0, s>>>(d, g.pw,
+                                                                                                      S->L, S->clusterSize);
+  return cudaGetLastError();
+}
+// The solve on the lists of launch_sor_lists: cluster-resident when they fit
+// one cluster, else the grid-wide persistent kernel (each returns at once when
+// the other path applies).
+cudaError_t launch_sor_run(void* statePtr, const Dims& d, const GridDev& g, double omega, int iters, int check,
+                           double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s) {
+  SorState* S = (SorState*)statePtr;
+  *outPath = S->outPath;
   int C = S->clusterSize;
   if (C) {
-    k_sor_codes<<<dim3((unsigned)std::min<long long>(grid_for(6 * S->cap, 256), 148 * 8), 2), 256, 0, s>>>(d, g.pw,
-                                                                                                      S->L, C);
     ClusterArgs ca;
     ca.d = d; ca.q = g.q; ca.L = S->L; ca.om1 = 1 - omega; ca.iters = iters; ca.check = check; ca.tol = tol;
     ca.outIters = S->outIters; ca.outRel = S->outRel; ca.outPath = S->outPath;
@@ -637,4 +648,11 @@ cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, co
   cudaError_t e = cudaLaunchCooperativeKernel((void*)k_sor_persistent, dim3(S->grid), dim3(S->block), args, 0, s);
   *outIters = S->outIters; *outRel = S->outRel;
   return e;
+}
+cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                             int iters, int check, double tol, int* err, int** outIters, double** outRel,
+                             int** outPath, cudaStream_t s) {
+  cudaError_t e = launch_sor_lists(statePtr, d, g, diag8, s);
+  if (e != cudaSuccess) return e;
+  return launch_sor_run(statePtr, d, g, omega, iters, check, tol, err, outIters, outRel, outPath, s);
 }
