@@ -952,7 +952,8 @@ static ws_status evaporation(ws_handle* h, double dt) {
   if (h->P.sunActivity <= 0 || h->P.evapIntensity <= 0) return WS_OK;
   double freezeT = std::max(h->P.meltT, h->P.snowT * 1.05);
   double rate = h->P.sunActivity * h->P.evapIntensity;
-  if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz)) return WS_ERR_STATE;
+  if (evaporation_scratch_bytes(h->capacity) > contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz))
+    return fail(h, WS_ERR_STATE, "evaporation scratch exceeds the shared contact scratch");
   ws_status s = contact_scratch(h); if (s) return s;
   uint32_t* evS = h->rng + 2;
   if (h->S.nP <= 0) { h->S.evapCount = 0; return WS_OK; }
