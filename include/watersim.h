@@ -16,7 +16,11 @@
  *    the next call that synchronises.
  *  - Host pointers are owned by the caller and read or written only during
  *    the call. Device memory is owned by the handle.
- *  - One CUDA stream per handle; calls on one handle must be serialised by
+ *  - One CUDA stream per handle (ws_get_stream); with the learned warm start
+ *    on, the pressure stage forks the SOR list build onto a second, internal
+ *    stream and joins it back before the solve, so all of a call's work is
+ *    still ordered after earlier work on the handle's stream and before later
+ *    work on it. Calls on one handle must be serialised by
  *    the caller (a frame started by ws_step_async holds the handle until it
  *    is collected; other calls meanwhile return WS_ERR_BUSY). There is no
  *    global mutable state, so different handles may be used from different
