@@ -110,33 +110,46 @@ void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStr
 
 // ------------------------------------------------------------ 2. mark fluid
 // _markFluidCells, js/solver.js:945-1000 (sphere). Bytes: 13P + N.
-__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P.nP) return;
-  const int fl = P.pflag[p];                     // issued with the position loads
-  const double X = P.px[p], Y = P.py[p], Z = P.pz[p];
-  if (fl != 0) return;
+// the cell a grid-coupled particle marks, or -1 (not coupled, or it turns airborne: pflag 1)
+__device__ __forceinline__ long long mark_cell(const Dims& d, const GridDev& g, PartsDev& P, const TerrainDev& t,
+                                               double oceanR, double coreR, int p, int fl, double X, double Y,
+                                               double Z) {
+  if (fl != 0) return -1;
   double rx = X - d.cx, ry = Y - d.cy, rz = Z - d.cz;
   double radius2 = rx * rx + ry * ry + rz * rz;
   double skyAlt = 2 * d.dx > 0.3 ? 2 * d.dx : 0.3;
   if (radius2 > (oceanR + 0.3) * (oceanR + 0.3) &&
       sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > skyAlt &&
       !(t.has && rock_cell_at(d, g.staticTypes, X, Y, Z))) {
-    P.pflag[p] = 1; return;
+    P.pflag[p] = 1; return -1;
   }
   int i = jfloor_clamp(over_dx(d, X), 0, d.nx - 1);
   int j = jfloor_clamp(over_dx(d, Y), 0, d.ny - 1);
   int k = jfloor_clamp(over_dx(d, Z), 0, d.nz - 1);
   if (j >= d.ny - 2) {
-    if (sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > 0.3) { P.pflag[p] = 1; return; }
+    if (sqrt(radius2) - terrain_radius_at(t, coreR, X, Y, Z) > 0.3) { P.pflag[p] = 1; return -1; }
   }
-  long long idx = ((long long)k * d.ny + j) * d.nx + i;
-  if (g.type[idx] == WS_AIR) g.type[idx] = WS_FLUID;   // idempotent byte store
+  return ((long long)k * d.ny + j) * d.nx + i;
+}
+// Two particles per thread: both particles' loads, then both cells' type
+// loads, then the (idempotent) stores, so the two chains overlap.
+__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR) {
+  const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
+  if (p0 >= P.nP) return;
+  const bool has1 = p1 < P.nP;
+  const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
+  const double X0 = P.px[p0], Y0 = P.py[p0], Z0 = P.pz[p0];
+  const double X1 = has1 ? P.px[p1] : 0.0, Y1 = has1 ? P.py[p1] : 0.0, Z1 = has1 ? P.pz[p1] : 0.0;
+  const long long c0 = mark_cell(d, g, P, t, oceanR, coreR, p0, fl0, X0, Y0, Z0);
+  const long long c1 = mark_cell(d, g, P, t, oceanR, coreR, p1, fl1, X1, Y1, Z1);
+  const uint8_t t0 = c0 >= 0 ? g.type[c0] : (uint8_t)WS_SOLID, t1 = c1 >= 0 ? g.type[c1] : (uint8_t)WS_SOLID;
+  if (t0 == WS_AIR) g.type[c0] = WS_FLUID;
+  if (t1 == WS_AIR) g.type[c1] = WS_FLUID;
 }
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                        double oceanR, double coreR, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_mark_fluid<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR);
+  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR);
 }
 
 // ------------------------------------------------------------ 3. P2G scatter
