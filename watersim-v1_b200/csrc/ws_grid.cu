@@ -196,7 +196,7 @@ __device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc
   for (int q = 0; q < 8; q++)
     atomicAdd(&acc[o8[q]], make_float2((float)(wp[q] * v0) + (float)(wq[q] * v1), (float)wp[q] + (float)wq[q]));
 }
-__global__ void k_p2g(Dims d, GridDev g, PartsDev P) {
+__global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
   if (p0 >= P.nP) return;
   const bool has1 = p1 < P.nP;
