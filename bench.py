@@ -46,9 +46,16 @@ for p in (ROOT, PKG):
 
 WORKLOADS = {
     "planet128": dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000),
-    # the large planet: 256^3, radius 110, ocean 12 deep, ~16M particles (plain arm only)
+    # the large planet: 256^3, radius 110, ocean 12 deep, ~16M particles
     "planet256": dict(name="planet256", n=256, R=110.0, depth=12.0, seed=20260114, particles=16000000),
+    # the 64^3 planet with the thermal cycle on: radius 26, ocean 5 deep, 220k particles; whole
+    # 60 Hz frames (two substeps each, SOR to 1e-5, vorticity 0.05) make one bench step
+    "planet64": dict(name="planet64", n=64, R=26.0, depth=5.0, seed=20260114, particles=220000),
 }
+# the thermal cycle of the frame workloads: sun at three ocean radii on a 23.4-degree
+# axial tilt, sunActivity 0.6, evapIntensity 0.05, vorticity confinement 0.05
+THERMAL = dict(thermalOn=1, vorticity=0.05, sunActivity=0.6, evapIntensity=0.05)
+FRAME_PASSES = ("HEAT", "EVAPORATION", "VAPOR_COLLISIONS", "PHASE", "ICE_CONTACTS", "PUSH_SURFACE")
 WORKLOAD = WORKLOADS["planet128"]
 PARAMS = dict(pic=0.05, omega=1.7, maxSpeed=3.2, cfl=3.0, viscosity=5e-4, thermalOn=0,
               sorTol=1e-5, sorCheckEvery=10, sorMaxIters=5000, pressureIters=40)
@@ -56,7 +63,9 @@ DT = 0.01
 STIR_EVERY, STIR_SIGMA, STIR_PEAK = 50, 4.0, 2.0
 METRIC = "substeps/s @128^3/2M particles: learned warm-start vs plain SOR at equal \u2016\u2207\u00b7u\u2016"
 METRIC_PLAIN = "substeps/s @128^3/2M particles (plain red-black SOR to 1e-5 relative divergence residual)"
-E2E_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pflag")
+# the fields the JS drop-in's _pull reads back after every step (and uploads once)
+E2E_FIELDS = ("px", "py", "pz", "pvx", "pvy", "pvz", "pT", "pflag", "pLight", "pDepth")
+U8_FIELDS = ("pflag", "pcool", "pDepth")
 
 
 def _peaks():
@@ -203,7 +212,7 @@ def run_ours(args, rank, world, local_rank):
         fs.upload("q", qsave)
     value = args.steps * world / (ms / 1000.0)
     # ---- end to end through the public API with pinned host buffers
-    host = {k: torch.empty(nP, dtype=torch.uint8 if k == "pflag" else torch.float32).pin_memory().numpy()
+    host = {k: torch.empty(nP, dtype=torch.uint8 if k in U8_FIELDS else torch.float32).pin_memory().numpy()
             for k in E2E_FIELDS}
     fs.download_state(host, nP)
     e2e_steps = max(1, min(args.steps, 20))
@@ -236,22 +245,19 @@ def run_ours(args, rank, world, local_rank):
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)",
-               "config": {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles"
-                                      % (WORKLOAD["name"], WORKLOAD["n"], WORKLOAD["R"], WORKLOAD["depth"], nP),
-                          "particles": nP, "parallelism": "replicas x%d" % world,
-                          "arm": "learned warm start" if learned else "plain SOR",
-                          "sor": "red-black to 1e-5 (check every 10), mean iterations %.1f"
-                                 % ((learned or plain)["sor_iterations"]),
-                          "fluid_cells": fs.scalars.nFluid,
-                          "sor_path": {0: "none", 1: "grid-wide persistent", 2: "cluster-resident (DSMEM)"}[fs.scalars.sorPath],
-                          "particle_substeps_per_s": value * nP,
-                          "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(fs, nP),
-                          "surface_mesh": surface,
-                          "render_particles": render,
-                          "metaballs": metaballs,
-                          "fp64_field_errors": fp64,
-                          "balls": balls,
-                          **cfg_learned},
+               "config": workload_config(nP, world),
+               "details": {"arm": "learned warm start" if learned else "plain SOR",
+                           "sor": "red-black to 1e-5 (check every %d), mean iterations %.1f"
+                                  % (PARAMS["sorCheckEvery"], (learned or plain)["sor_iterations"]),
+                           "fluid_cells": fs.scalars.nFluid,
+                           "sor_path": SOR_PATHS.get(fs.scalars.sorPath, "unknown"),
+                           "particle_substeps_per_s": value * nP,
+                           "surface_mesh": surface,
+                           "render_particles": render,
+                           "metaballs": metaballs,
+                           "fp64_field_errors": fp64,
+                           "balls": balls,
+                           **cfg_learned},
                "e2e": {"value": e2e_steps * world / e2e_s, "unit": "substeps/s",
                        "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
                "gpu_launches": int(launches),
@@ -260,8 +266,20 @@ def run_ours(args, rank, world, local_rank):
     return out, fs
 
 
-def state_mb(fs, nP):
-    n = fs.nx
+SOR_PATHS = {0: "none", 1: "grid-wide persistent", 2: "cluster-resident (DSMEM)",
+             3: "temporal-blocked (all SMs, shared-memory regions)"}
+
+
+def workload_config(nP, world):
+    """The workload both arms run (identical dict on both arms' lines)."""
+    W = WORKLOAD
+    n = W["n"]
+    return {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles" % (W["name"], n, W["R"], W["depth"], nP),
+            "particles": nP, "parallelism": "replicas x%d" % world,
+            "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(n, nP)}
+
+
+def state_mb(n, nP):
     F = 3 * (n + 1) * n * n
     return int((nP * 55 + F * 21 + n ** 3 * 16) / 1e6)
 
@@ -359,7 +377,7 @@ def roofline(fs, ms_step, iters):
     us, nbytes = cand[name]
     achieved = nbytes / (us * 1e-6) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of each kernel
-    # on this 128^3 planet (watersim-v1_b200/profile_planet.py): the SOR
+    # on this 128^3 planet (bench.py --profile 3): the SOR
     # solve's lists are staged into shared memory once, so its traffic is a
     # small fraction of its algorithmic bytes
     captured = {"k_sor_cluster": 4428544.0, "k_p2g": 53253120.0, "k_g2p_advect": 66053376.0}
@@ -586,8 +604,15 @@ def cpu_baseline(fs, seconds=20.0):
                        "(C restatement of js/solver.js, lexicographic SOR) on 1 host core" % (done, W["n"], nP, el))}
 
 
-def run_reference(args, rank, world):
-    """Reference arm: the CPU algorithm of js/solver.js (oracle port), one core."""
+def frames_metric(n, nP):
+    return ("substeps/s @%d^3/%dk particles, thermal cycle on (whole 60 Hz frames, plain SOR to 1e-5)"
+            % (n, nP // 1000))
+
+
+def run_reference(args, rank, world, frames=False):
+    """Reference arm: the CPU algorithm of js/solver.js (oracle port), one
+    core, on the same workload, --steps timed steps after --warmup untimed
+    ones (substeps, or whole frames with the thermal cycle on)."""
     if rank != 0:
         return None
     from oracle.oracle import make_planet
@@ -596,32 +621,174 @@ def run_reference(args, rank, world):
     o.set(**PARAMS, sorRedBlack=0, viscJacobi=0, extrapJacobi=0)
     o.set_scalars(gRamp=1.5)
     nP = o.nP
-    warm = min(args.warmup, 1)
-    steps = max(1, min(args.steps, 3))
-    count = 0
-    for _ in range(warm):
-        if count % STIR_EVERY == 0:
+    if frames:
+        c = W["n"] / 2
+        R = o.scalars.oceanR * 3
+        tilt = math.radians(23.4)
+        o.set(**THERMAL, sunPos=[c + R * math.cos(tilt), c + R * math.sin(tilt), c])
+    count = [0]
+
+    def one():
+        if frames:
+            o.step(1 / 60)
+            return o.scalars.substepsLast
+        if count[0] % STIR_EVERY == 0:
             o.stir_gaussian(STIR_SIGMA, STIR_PEAK)
         o.substep(DT)
-        count += 1
+        count[0] += 1
+        return 1
+    for _ in range(args.warmup):
+        one()
     t0 = time.perf_counter()
-    for _ in range(steps):
-        if count % STIR_EVERY == 0:
-            o.stir_gaussian(STIR_SIGMA, STIR_PEAK)
-        o.substep(DT)
-        count += 1
+    subs = sum(one() for _ in range(args.steps))
     el = time.perf_counter() - t0
-    v = steps / el
-    sample = ("%d substep(s) of the %d^3 planet (%d particles) after %d warm-up; C restatement of "
-              "js/solver.js (reference order), 1 core — no JavaScript engine on the host" % (steps, W["n"], nP, warm))
-    return {"metric": METRIC, "value": v, "unit": "substeps/s", "n_gpus": world, "steps": steps,
-            "warmup": warm, "ms_per_step": 1000 * el / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic / f32 storage",
-            "data": "synthetic seeded planet", "impl": "reference",
-            "config": {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles"
-                                   % (W["name"], W["n"], W["R"], W["depth"], nP)},
+    v = subs / el
+    unit = "whole frame(s)" if frames else "whole substep(s)"
+    sample = ("%d %s of the %d^3 planet (%d particles) after %d warm-up; C restatement of js/solver.js "
+              "(reference order), 1 core: the reference's step is single-threaded; no JavaScript engine on the "
+              "host" % (args.steps, unit, W["n"], nP, args.warmup))
+    metric = frames_metric(W["n"], nP) if frames else (METRIC_PLAIN if args.no_learned else METRIC)
+    return {"metric": metric, "value": v, "unit": "substeps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 arithmetic / f32 storage",
+            "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)", "impl": "reference",
+            "config": workload_config(nP, world),
             "cpu_baseline": {"value": v, "unit": "substeps/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def thermal_on(fs):
+    """The thermal cycle of the frame workloads on this solver."""
+    c = fs.nx / 2
+    R = fs.scalars.oceanR * 3
+    tilt = math.radians(23.4)
+    fs.set_params(**THERMAL, sunPos=[c + R * math.cos(tilt), c + R * math.sin(tilt), c])
+
+
+def run_frames(args, rank, world, local_rank):
+    """Whole 60 Hz frames (step(1/60): substeps, contacts, phases, rescue,
+    and on tick frames the heat tick, evaporation and vapour contacts) with
+    the thermal cycle on. One bench step = one frame; value = substeps/s.
+    Frames are timed with CUDA events on the solver's stream (max over
+    ranks); each frame pass is then timed alone once."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    fs = make_solver(local_rank, rank)
+    thermal_on(fs)
+    for _ in range(args.warmup):
+        fs.step(1 / 60)
+    fs.synchronize()
+    st = torch.cuda.ExternalStream(fs.stream())
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.5)
+    ms, subs, evap = [], 0, []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fs.step(1 / 60)                  # synchronous: returns after the frame's counters are read
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        subs += fs.scalars.substepsLast
+        evap.append(fs.scalars.evapCount)
+    clk = clocks.stop()
+    total = sum(ms)
+    if world > 1:
+        total = reduce_max(total, "cuda")
+    passes = {}
+    for name in FRAME_PASSES:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        fs.stage(name, 1 / 25)
+        e1.record(st)
+        e1.synchronize()
+        passes[name] = round(e0.elapsed_time(e1), 3)
+    s = fs.scalars
+    srt = sorted(ms)
+    out = None
+    if rank == 0:
+        out = {"metric": frames_metric(WORKLOAD["n"], s.nP),
+               "value": subs * world / (total / 1000), "unit": "substeps/s", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic seeded planet (value-noise terrain, jittered lattice fill)",
+               "config": workload_config(s.nP, world),
+               "details": {"frames_per_s": args.steps * world / (total / 1000),
+                           "substeps_per_frame": subs / args.steps,
+                           "frame_ms": {"min": srt[0], "median": srt[len(srt) // 2], "max": srt[-1]},
+                           "evaporations_last_tick": evap[-1], "vapor": s.vaporCount,
+                           "sor_iterations_last": s.sorIters, "sor_path": SOR_PATHS.get(s.sorPath, "unknown"),
+                           "pass_ms": passes},
+               "gpu_launches": None, "clocks": clk}
+    return out, fs
+
+
+def run_profile(args, local_rank):
+    """A few substeps of the workload for capturing one kernel under a
+    profiler with few launches before it (no timing). With --learned-profile
+    two (input, converged q) pairs are recorded, one Adam step taken and the
+    warm start turned on, so the network's convolutions run every substep."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    fs = make_solver(local_rank)
+    if WORKLOAD["name"] == "planet64":
+        thermal_on(fs)
+    if args.learned_profile:
+        fs.unet_init(7)
+        fs.unet_collect(2)
+        fs._substep(DT)
+        fs._substep(DT)
+        fs.unet_collect(0)
+        fs.unet_train(1, 1, 1e-3, 1)
+        fs.unet_enable(1)
+    for _ in range(args.profile):
+        fs._substep(DT)
+    fs.synchronize()
+    s = fs.scalars
+    print(json.dumps({"profile_substeps": args.profile, "workload": WORKLOAD["name"], "learned": bool(args.learned_profile),
+                      "sor_iterations": s.sorIters, "fluid_cells": s.nFluid,
+                      "sor_path": SOR_PATHS.get(s.sorPath, "unknown")}))
+    fs.close()
+
+
+def run_render(args, local_rank):
+    """ws_render_particles (WaterScene.updateParticles, js/scene.js:1595-1922)
+    on seeded particles shaped like the 128^3 planet's: 1,856,640 particles
+    over a 128^3 box in cell order, liquid only (or all six flag classes with
+    --render-mix), the lit-planet scene in beads mode with the camera two box
+    widths out. Time per call (four kernels, count read-back, synchronisation)
+    and the algorithmic bytes per second (26 read per particle, 36 written
+    per drawn point)."""
+    import numpy as np
+    import torch
+    from fluid_solver import FluidSolver, render_opts
+    torch.cuda.set_device(local_rank)
+    n, W = 1856640, 128.0
+    r = np.random.default_rng(3)
+    px, py, pz = (r.uniform(0, W, n).astype(np.float32) for _ in range(3))
+    o = np.lexsort((px, py, pz))
+    flags = r.integers(0, 6, n) if args.render_mix else np.zeros(n)
+    parts = {"px": px[o], "py": py[o], "pz": pz[o], "pflag": flags.astype(np.uint8),
+             "pT": r.uniform(0, 1, n).astype(np.float32), "pLight": r.uniform(0, 1, n).astype(np.float32),
+             "pDepth": r.integers(0, 5, n).astype(np.uint8), "pPh": r.uniform(-3, 3, n).astype(np.float32)}
+    fs = FluidSolver(nx=128, ny=128, nz=128, dx=1.0, coreR=40, targetParticles=1000, capacity=n + 64,
+                     device=local_rank)
+    fs.set_scalars(nP=n)
+    fs.upload_state(parts, count=n)
+    opts = render_opts(beadsMode=1, cam=(0.5 * W, 0.5 * W, -2.0 * W), sunDir=(0.6, 0.0, 0.8))
+    for _ in range(max(3, args.warmup)):
+        fs.render_particles(opts, download=False)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        counts, pts = fs.render_particles(opts, download=False)
+    ms = (time.perf_counter() - t0) / args.steps * 1000
+    algo = 26 * n + 36 * pts
+    print(json.dumps({"render_particles": n, "points": pts, "counts": counts, "mix": bool(args.render_mix),
+                      "ms_per_call": ms, "algorithmic_bytes": algo, "achieved_gbs": algo / (ms * 1e6)}))
+    fs.close()
 
 
 def main():
@@ -636,7 +803,12 @@ def main():
     ap.add_argument("--pairs", type=int, default=2000, help="training pairs recorded from plain solves")
     ap.add_argument("--train-steps", type=int, default=1000, help="Adam steps of batch 4")
     ap.add_argument("--workload", default="planet128", choices=sorted(WORKLOADS),
-                    help="planet256 (256^3, ~16M particles) runs the plain arm only")
+                    help="planet64 runs whole thermal-cycle frames; planet256 the plain and learned arms at 256^3")
+    ap.add_argument("--frames", action="store_true", help="whole frames with the thermal cycle on (any workload)")
+    ap.add_argument("--profile", type=int, default=0, help="run this many substeps for a profiler capture and exit")
+    ap.add_argument("--learned-profile", action="store_true", help="--profile with the learned warm start on")
+    ap.add_argument("--render", action="store_true", help="time ws_render_particles alone and exit")
+    ap.add_argument("--render-mix", action="store_true", help="--render with all six flag classes")
     args = ap.parse_args()
     global WORKLOAD, METRIC_PLAIN
     WORKLOAD = WORKLOADS[args.workload]
@@ -644,24 +816,29 @@ def main():
         args.no_learned = True
         METRIC_PLAIN = ("substeps/s @%d^3/%dM particles (plain red-black SOR to 1e-5 relative divergence residual)"
                         % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000))
+    frames = args.frames or args.workload == "planet64"
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
-        out = run_reference(args, rank, world)
+        out = run_reference(args, rank, world, frames)
         if out is not None:
             print(json.dumps(out))
         return
+    if args.profile:
+        return run_profile(args, local_rank)
+    if args.render:
+        return run_render(args, local_rank)
     import torch
     import datetime
     if world > 1:
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    out, fs = run_ours(args, rank, world, local_rank)
+    out, fs = (run_frames if frames else run_ours)(args, rank, world, local_rank)
     if rank == 0:
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and not frames:
             out["cpu_baseline"] = cpu_baseline(fs, args.cpu_seconds)
         print(json.dumps(out))
     fs.close()

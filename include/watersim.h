@@ -356,8 +356,14 @@ ws_status ws_launch_count(ws_handle* h, int64_t* launches);        /* kernels th
  * (a cudaStream_t, or NULL). Calls no cudaMalloc/cudaFree: its scratch is a
  * fixed 128 KB device array in the library, so grids above 128^3 cells
  * (2,097,152) return WS_ERR_RANGE. All calls on a device share that array;
- * calls that overlap on the GPU race. The first call on a device looks the
- * array up (cudaGetSymbolAddress) and should come before any stream capture. */
+ * calls that overlap on the GPU race. Every call looks the array's address up
+ * on the current device (cudaGetSymbolAddress, which allocates nothing), in
+ * the runtime's current (primary) context, so a context re-created after
+ * cudaDeviceReset is handled; the first call on a device also loads the
+ * library's device code there and should come before any stream capture.
+ * Each launch is checked through its own return code (WS_ERR_CUDA when one
+ * fails); an earlier, unrelated error pending on the calling thread is
+ * neither cleared nor reported as this call's. */
 ws_status ws_residual_noalloc(int32_t nx, int32_t ny, int32_t nz, const float* q, const float* rhs,
                               const uint8_t* cellType, double* relres, void* stream);
 

@@ -340,3 +340,39 @@ def test_currents_parity():
     assert np.abs(o.arr("pvx")[:nP] - before).max() > 1e-3          # the pass acts
     for k in ("pvx", "pvy", "pvz"):
         assert rel_err(fs.download(k), o.arr(k)[:nP]) <= 1e-6, k
+
+
+def test_ice_contacts_parity():
+    """_iceContacts (js/solver.js:3290-3324) on 4000 snow grains dropped in
+    clumps at the sea surface, a third of them already stuck to the pack:
+    the device's segmented serial sweep reproduces the reference's in-place
+    sweep over the x-sorted list, so stuck flags and velocities are bit-exact."""
+    o = _state64()
+    nP = o.nP
+    rng = np.random.default_rng(31)
+    c = o.nx / 2
+    R = o.scalars.oceanR
+    m, clumps = 4000, 120
+    sel = rng.choice(nP, m, replace=False)
+    centres = rng.normal(size=(clumps, 3))
+    centres /= np.linalg.norm(centres, axis=1)[:, None]
+    centres = c + centres * (R + 0.5)
+    which = rng.integers(0, clumps, m)
+    pos = centres[which] + rng.normal(0, 0.6 * o.scalars.spacing, (m, 3))
+    for a, k in enumerate(("px", "py", "pz")):
+        o.arr(k)[sel] = pos[:, a]
+    for k in ("pvx", "pvy", "pvz"):
+        o.arr(k)[sel] = rng.normal(0, 0.4, m)
+    o.pflag[sel] = 5
+    o.pAir[sel] = np.where(rng.random(m) < 0.33, 1.0, rng.uniform(0, 0.9, m)).astype(np.float32)
+    fs = to_device(o)
+    before_air = o.pAir[:nP].copy()
+    before_v = o.arr("pvx")[:nP].copy()
+    o.stage("ice_contacts")
+    fs.stage("ICE_CONTACTS")
+    newly_stuck = np.count_nonzero((o.pAir[:nP] == 1) & (before_air != 1))
+    paired = np.count_nonzero((o.arr("pvx")[:nP] != before_v) & (o.pAir[:nP] != 1))
+    assert newly_stuck > 50 and paired > 50            # both rules fire
+    assert np.array_equal(fs.pAir, o.pAir[:nP])
+    for k in ("pvx", "pvy", "pvz"):
+        assert np.array_equal(fs.download(k), o.arr(k)[:nP]), k

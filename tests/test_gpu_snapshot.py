@@ -47,6 +47,11 @@ def test_snapshot_rejects_bad_blobs():
     b = _fresh(o)
     with pytest.raises(WsError):
         b.restore(blob[:-1])                           # truncated
+    # cut inside the knobs and scalars that follow the header: refused before
+    # they are read (the header alone is valid)
+    for cut in (100, 200, 400):
+        with pytest.raises(WsError):
+            b.restore(blob[:cut].copy())
     bad = blob.copy()
     bad[0] ^= 0xFF
     with pytest.raises(WsError):

@@ -46,3 +46,31 @@ def test_noalloc_residual_matches_handle():
                                out.data_ptr(), C.c_void_p(stream))
     assert rc == WS_ERR_RANGE
     fs.close()
+
+
+def test_noalloc_leaves_pending_error_alone():
+    """An earlier, unrelated CUDA error pending on the calling thread (here a
+    harmless cudaSetDevice(-1), which faults nothing) is neither reported as
+    this call's nor cleared: the call succeeds and the error is still there
+    for its owner to read."""
+    import torch
+    import fluid_solver
+    cudart = C.CDLL("libcudart.so.12")
+    q = torch.zeros(32 ** 3, dtype=torch.float32, device="cuda")
+    rhs = torch.ones(32 ** 3, dtype=torch.float32, device="cuda")
+    ct = torch.zeros(32 ** 3, dtype=torch.uint8, device="cuda")
+    ct.view(32, 32, 32)[8:24, 8:24, 8:24] = 1              # a fluid block: the residual of q = 0 is 1
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    L = fluid_solver.load_library()
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    assert cudart.cudaSetDevice(-1) != 0                   # leaves a pending, non-sticky error
+    pending = cudart.cudaPeekAtLastError()
+    assert pending != 0
+    rc = L.ws_residual_noalloc(32, 32, 32, q.data_ptr(), rhs.data_ptr(), ct.data_ptr(), out.data_ptr(),
+                               C.c_void_p(stream))
+    assert rc == 0
+    assert cudart.cudaPeekAtLastError() == pending         # still the caller's to read
+    assert cudart.cudaGetLastError() == pending            # which clears it
+    torch.cuda.synchronize()
+    assert abs(out.item() - 1.0) <= 1e-12

@@ -745,12 +745,22 @@ static ws_status stage_pressure(ws_handle* h) {
   if (h->net && h->unetOn) {
     // the colour lists on the side stream while the network predicts q (they do not read q)
     WS_TRY(cudaEventRecord(h->evFork, h->stream));
+    // From here on every exit joins the side stream back into the main one,
+    // so a capture in progress ends with no unjoined stream and reports the
+    // first error rather than an unjoined-capture one.
+    struct SideJoin {
+      ws_handle* h; bool armed;
+      ~SideJoin() {
+        if (armed && cudaEventRecord(h->evJoin, h->side) == cudaSuccess) cudaStreamWaitEvent(h->stream, h->evJoin, 0);
+      }
+    } join{ h, true };
     WS_TRY(cudaStreamWaitEvent(h->side, h->evFork, 0));
     if ((e = launch_sor_lists(h->sor, h->d, g, h->diag8, h->side)) != cudaSuccess) return fail_cuda(h, e, "SOR lists");
     WS_TRY(cudaEventRecord(h->evJoin, h->side));
     if ((e = h->net->predict(h->q, h->rhs, h->diag8, h->type, h->stream)) != cudaSuccess)
       return fail_cuda(h, e, "learned warm start");
     h->launches += 23;
+    join.armed = false;
     WS_TRY(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
     e = launch_sor_run(h->sor, h->d, g, h->P.omega, iters, check, h->P.sorTol, &h->st->err, &dIters, &dRel, &dPath,
                        h->stream);
@@ -1592,6 +1602,9 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
     return fail(h, WS_ERR_INVALID, "snapshot grid differs from this handle's");
   if (hd.nP < 0 || hd.nP > h->capacity) return fail(h, WS_ERR_RANGE, "snapshot holds more particles than the capacity");
   if (hd.terrainN < 0 || hd.terrainN > 4096) return fail(h, WS_ERR_INVALID, "bad terrain size");
+  // the knobs and scalars follow the header: a blob cut short before them is refused before they are read
+  if (size < (int64_t)(sizeof hd + sizeof(ws_params) + sizeof(ws_scalars)))
+    return fail(h, WS_ERR_INVALID, "snapshot size mismatch");
   ws_scalars S;
   std::memcpy(&S, (const unsigned char*)buf + sizeof hd + sizeof(ws_params), sizeof S);
   const int64_t nP = hd.nP, N = h->d.nCells, n3 = (int64_t)hd.terrainN * hd.terrainN * hd.terrainN;

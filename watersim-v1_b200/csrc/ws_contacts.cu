@@ -2,12 +2,16 @@
 // (js/solver.js:3345-3479) and _iceContacts (:3290-3324).
 //
 // The reference resolves pairs in place, one after another in sorted-x
-// order, so each pair sees the updates of the pairs before it. The device
-// pass resolves every pair from one snapshot of the state (Jacobi order)
-// and sums the equal-and-opposite impulses with atomics: pair momentum is
-// conserved exactly as in the reference, the per-particle result differs at
-// second order where one parcel touches several others in the same frame.
-// The vapour census (vaporCount, nightVaporCount) is exact.
+// order, so each pair sees the updates of the pairs before it.
+// - Vapour contacts: the device resolves every pair from one snapshot of the
+//   state (Jacobi order) and sums the equal-and-opposite impulses with
+//   atomics. Pair momentum is conserved exactly as in the reference; the
+//   per-particle result differs at second order where one parcel touches
+//   several others in the same frame. The vapour census (vaporCount,
+//   nightVaporCount) is exact.
+// - Ice contacts: exact. The sorted list is cut where neighbours are at
+//   least the contact radius apart in x; no pair crosses such a gap, so each
+//   segment is swept serially by one thread in the reference's order.
 // The x-sort uses CUB's device radix sort (a CUDA toolkit library).
 #include "ws_kernels.cuh"
 #include <cub/cub.cuh>
@@ -209,42 +213,49 @@ void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, d
   k_apply<<<grid_for(n, 256), 256, 0, s>>>(P, c.idxB, n, c.acc);
 }
 
-// ice pairs (:3304-3323): a free grain touching a stuck one sticks; two free
-// grains adopt their mean velocity (here: the mean over all free partners
-// from the snapshot, plus itself)
-__global__ void k_ice_pairs(PartsDev P, const int* __restrict__ idx, const float* __restrict__ snap, int n, double rad,
-                            float* __restrict__ acc) {
+// _iceContacts (:3290-3324), exact. The reference sweeps the x-sorted ice
+// list serially: pair (a, b) sees every update of the pairs before it. The
+// sweep of grain a only reaches grains b with px[b] - px[a] < rad, so a gap of
+// at least rad between neighbours in the sorted list cuts it into segments
+// no pair crosses. Each segment is swept by one thread in the reference's
+// order, with the reference's arithmetic, on the live particle arrays; the
+// segments touch disjoint particles, so their sweeps run in parallel and the
+// result is the serial sweep's, bit for bit.
+__global__ void k_ice_segments(const float* __restrict__ px, const int* __restrict__ idx, int n, double rad,
+                               uint8_t* __restrict__ segStart) {
   int a = blockIdx.x * blockDim.x + threadIdx.x;
   if (a >= n) return;
-  const float* A = snap + 6 * a;
-  bool stuckA = P.pAir[idx[a]] == 1.f;
-  double rad2 = rad * rad, mx = 0, my = 0, mz = 0; int nFree = 0; bool touchStuck = false;
-  for (int dir = -1; dir <= 1; dir += 2) {
-    for (int b = a + dir; b >= 0 && b < n; b += dir) {
-      const float* B = snap + 6 * b;
-      double ddx = (double)B[0] - A[0];
-      if (fabs(ddx) >= rad) break;
-      double ddy = (double)B[1] - A[1], ddz = (double)B[2] - A[2];
+  segStart[a] = a == 0 || (double)px[idx[a]] - (double)px[idx[a - 1]] >= rad;
+}
+__global__ void k_ice_sweep(PartsDev P, const int* __restrict__ idx, const uint8_t* __restrict__ segStart, int n,
+                            double rad) {
+  int s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s0 >= n || !segStart[s0]) return;
+  const double rad2 = rad * rad;
+  const float *px = P.px, *py = P.py, *pz = P.pz;
+  float *pvx = P.pvx, *pvy = P.pvy, *pvz = P.pvz, *pAir = P.pAir;
+  for (int a = s0; a < n && (a == s0 || !segStart[a]); a++) {
+    const int i = idx[a];
+    bool stuckI = pAir[i] == 1.f;
+    for (int b = a + 1; b < n; b++) {
+      const int j = idx[b];
+      if ((double)px[j] - (double)px[i] >= rad) break;
+      double ddx = (double)px[j] - (double)px[i], ddy = (double)py[j] - (double)py[i], ddz = (double)pz[j] - (double)pz[i];
       if (ddx * ddx + ddy * ddy + ddz * ddz >= rad2) continue;
-      bool stuckB = P.pAir[idx[b]] == 1.f;
-      if (stuckB) touchStuck = true;
-      else { mx += B[3]; my += B[4]; mz += B[5]; nFree++; }
+      const bool stuckJ = pAir[j] == 1.f;
+      if (stuckI && stuckJ) continue;
+      if (stuckJ) {                    // free i lands on the pack at j
+        pAir[i] = 1.f; pvx[i] = pvy[i] = pvz[i] = 0.f; stuckI = true;
+      } else if (stuckI) {             // free j lands on the pack at i
+        pAir[j] = 1.f; pvx[j] = pvy[j] = pvz[j] = 0.f;
+      } else {                         // two free grains: both take the mean velocity
+        const float mx = (float)(((double)pvx[i] + (double)pvx[j]) * 0.5);
+        const float my = (float)(((double)pvy[i] + (double)pvy[j]) * 0.5);
+        const float mz = (float)(((double)pvz[i] + (double)pvz[j]) * 0.5);
+        pvx[i] = pvx[j] = mx; pvy[i] = pvy[j] = my; pvz[i] = pvz[j] = mz;
+      }
     }
   }
-  acc[6 * a] = stuckA ? 1.f : 0.f;
-  if (stuckA) return;
-  if (touchStuck) { acc[6 * a + 1] = 2.f; return; }
-  acc[6 * a + 1] = nFree ? 1.f : 0.f;
-  acc[6 * a + 3] = (float)((A[3] + mx) / (nFree + 1)); acc[6 * a + 4] = (float)((A[4] + my) / (nFree + 1));
-  acc[6 * a + 5] = (float)((A[5] + mz) / (nFree + 1));
-}
-__global__ void k_ice_apply(PartsDev P, const int* __restrict__ idx, int n, const float* __restrict__ acc) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int p = idx[i];
-  if (acc[6 * i] == 1.f) return;
-  if (acc[6 * i + 1] == 2.f) { P.pAir[p] = 1.f; P.pvx[p] = P.pvy[p] = P.pvz[p] = 0.f; return; }
-  if (acc[6 * i + 1] == 1.f) { P.pvx[p] = acc[6 * i + 3]; P.pvy[p] = acc[6 * i + 4]; P.pvz[p] = acc[6 * i + 5]; }
 }
 __global__ void k_ice_flags(const uint8_t* __restrict__ fl, int nP, uint8_t* __restrict__ out) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -266,7 +277,7 @@ void launch_ice_contacts(const PartsDev& P, double spacing, void* scratch, size_
   k_keys<<<grid_for(n, 256), 256, 0, s>>>(c.idxA, c.nV, P.px, c.keyA);
   size_t bytes = c.cubBytes;
   cub::DeviceRadixSort::SortPairs(c.cubTemp, bytes, c.keyA, c.keyB, c.idxA, c.idxB, n, 0, 32, s);
-  k_snapshot<<<grid_for(n, 256), 256, 0, s>>>(P, c.idxB, n, c.snap, c.acc);
-  k_ice_pairs<<<grid_for(n, 128), 128, 0, s>>>(P, c.idxB, c.snap, n, spacing * 0.7, c.acc);
-  k_ice_apply<<<grid_for(n, 256), 256, 0, s>>>(P, c.idxB, n, c.acc);
+  uint8_t* segStart = (uint8_t*)c.acc;
+  k_ice_segments<<<grid_for(n, 256), 256, 0, s>>>(P.px, c.idxB, n, spacing * 0.7, segStart);
+  k_ice_sweep<<<grid_for(n, 128), 128, 0, s>>>(P, c.idxB, segStart, n, spacing * 0.7);
 }

@@ -17,12 +17,22 @@
 // on one device share the array: calls whose kernels overlap on the GPU (two
 // streams, two host threads) race and must be serialised by the caller.
 //
-// Set-up: the first call on each device, with that device current, looks the
-// array's device address up with cudaGetSymbolAddress (host code must not
-// pass the symbol itself to a kernel). Make that first call before any
-// stream capture.
+// Set-up: host code must not hand the array's name to a kernel (on the host it
+// names a stand-in, not device memory). Every call therefore looks up the
+// array's device address with cudaGetSymbolAddress on the current device and
+// checks the result. The lookup allocates nothing; repeating it on every call
+// keeps the address right when the caller's context is re-created (after
+// cudaDeviceReset the library's device code is loaded again, possibly at
+// another address). The first call on a device also loads the library's
+// device code there, so it should come before any stream capture. The
+// entry point uses the runtime's current (primary) context of the current
+// device.
+//
+// Errors: each of the two launches is checked through its own return code
+// (cudaLaunchKernel). The calling thread's pending CUDA error state is left
+// as it was: an earlier, unrelated error is neither cleared nor reported as
+// this call's.
 #include "ws_kernels.cuh"
-#include <atomic>
 
 #define WS_NOALLOC_BLOCK 256
 #define WS_NOALLOC_MAX_BLOCKS 8192
@@ -82,26 +92,21 @@ __global__ void k_noalloc_final(const double2* __restrict__ partials, int n, dou
   }
 }
 
-// device address of g_noalloc_partials, looked up once per device
-static std::atomic<double2*> s_scratch[256];
-
 extern "C" ws_status ws_residual_noalloc(int32_t nx, int32_t ny, int32_t nz, const float* q, const float* rhs,
                                          const uint8_t* cellType, double* relres, void* stream) {
   if (nx < 3 || ny < 3 || nz < 3 || !q || !rhs || !cellType || !relres) return WS_ERR_INVALID;
   long long cells = (long long)nx * ny * nz;
   if (cells > WS_NOALLOC_MAX_CELLS) return WS_ERR_RANGE;        // beyond the fixed scratch
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return WS_ERR_CUDA;
-  double2* scratch = s_scratch[dev].load(std::memory_order_acquire);
-  if (!scratch) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_partials) != cudaSuccess || !p) return WS_ERR_CUDA;
-    scratch = (double2*)p;
-    s_scratch[dev].store(scratch, std::memory_order_release);
-  }
+  void* sp = nullptr;
+  if (cudaGetSymbolAddress(&sp, g_noalloc_partials) != cudaSuccess || !sp) return WS_ERR_CUDA;
+  double2* scratch = (double2*)sp;
   cudaStream_t s = (cudaStream_t)stream;
   int nb = (int)((cells + WS_NOALLOC_BLOCK - 1) / WS_NOALLOC_BLOCK);
-  k_noalloc_partial<<<nb, WS_NOALLOC_BLOCK, 0, s>>>(nx, ny, nz, q, rhs, cellType, scratch);
-  k_noalloc_final<<<1, 1024, 0, s>>>(scratch, nb, relres);
-  return cudaGetLastError() == cudaSuccess ? WS_OK : WS_ERR_CUDA;
+  void* a1[] = { &nx, &ny, &nz, (void*)&q, (void*)&rhs, (void*)&cellType, &scratch };
+  if (cudaLaunchKernel((const void*)k_noalloc_partial, dim3(nb), dim3(WS_NOALLOC_BLOCK), a1, 0, s) != cudaSuccess)
+    return WS_ERR_CUDA;
+  void* a2[] = { &scratch, &nb, &relres };
+  if (cudaLaunchKernel((const void*)k_noalloc_final, dim3(1), dim3(1024), a2, 0, s) != cudaSuccess)
+    return WS_ERR_CUDA;
+  return WS_OK;
 }
