@@ -266,8 +266,10 @@ def run_ours(args, rank, world, local_rank):
     return out, fs
 
 
-SOR_PATHS = {0: "none", 1: "grid-wide persistent", 2: "cluster-resident (DSMEM)",
-             3: "temporal-blocked (all SMs, shared-memory regions)"}
+SOR_PATHS = {0: "none", 1: "grid-wide persistent (colour lists)", 2: "cluster-resident (DSMEM, colour lists)",
+             3: "temporal-blocked (every SM, shared-memory regions)",
+             4: "owned bricks in global memory (every SM, a grid barrier per half-sweep)"}
+SOR_KERNELS = {1: "k_sor_persistent", 2: "k_sor_cluster", 3: "k_sor_tb", 4: "k_sor_tb"}
 
 
 def workload_config(nP, world):
@@ -366,7 +368,7 @@ def roofline(fs, ms_step, iters):
     #  G2P+advect    52 B per particle + 8 B per face (u and uO)
     #  faces pass 1  8 B acc + 9 B out per face; forces 12 B per face; project 8 B per face
     # the path the timed solve took (its own diagnostics, read after it ran)
-    sor_name = "k_sor_cluster" if fs.scalars.sorPath == 2 else "k_sor_persistent"
+    sor_name = SOR_KERNELS.get(fs.scalars.sorPath, "k_sor_tb")
     cand = {sor_name: (us_sor, 13.0 * nF * it),
             "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
             "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),

@@ -107,7 +107,9 @@ typedef struct {
   int32_t nP, capacity;
   int32_t airborneCount, vaporCount, nightVaporCount, evapCount, substepsLast, nFluid;
   int32_t sorIters;        /* iterations run by the last solve */
-  int32_t sorPath;         /* 1 grid-wide persistent solve, 2 cluster-resident solve */
+  int32_t sorPath;         /* solve path of the last solve: 1 grid-wide colour lists, 2 cluster-resident
+                              colour lists, 3 temporal-blocked on every SM (shared-memory regions),
+                              4 owned bricks in global memory on every SM (regions too large) */
 } ws_scalars;
 
 /* Named fields — the typed arrays of FluidSolver (js/solver.js:94-129). */
@@ -330,6 +332,31 @@ ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy, double cz,
 ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, double vx, double vy,
                      double vz, double R, double dt);
 ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak);
+/* waveImpulse(dvx) (js/solver.js:3866-3892), sphere mode: a tide bulge in a
+ * random direction, every particle on that side pushed radially by
+ * dvx * pr^3 * (0.7 + 0.3 rnd) (pr the cosine to the bulge direction). The
+ * reference draws from Math.random(); here the draws come from the seeded
+ * stir stream (stirS): two for the direction, then draw p + 1 of the
+ * following stream for particle p (every particle takes one), so the call is
+ * reproducible; stirS advances by nP + 2 draws. */
+ws_status ws_wave_impulse(ws_handle* h, double dvx);
+/* dryLandFraction() (js/solver.js:3593-3623): the fraction of 1200
+ * golden-angle rays whose rock surface stands above sea level with no fluid
+ * cell on it, from the current cell types; 0 without terrain. */
+ws_status ws_dry_land_fraction(ws_handle* h, double* fraction);
+/* sampleVel(x, y, z) (js/solver.js:811-854) at n points: xyz holds n
+ * (x, y, z) host doubles, uvw receives n (u, v, w) host doubles, the
+ * trilinear MAC sample of the current face velocities. */
+ws_status ws_sample_vel(ws_handle* h, const double* xyz, int64_t n, double* uvw);
+/* terrainRadiusAt(x, y, z) (js/solver.js:512-535) at n points: the
+ * trilinear terrain radius field (coreR without terrain), n host doubles. */
+ws_status ws_terrain_radius_at(ws_handle* h, const double* xyz, int64_t n, double* radius);
+/* oceanPoint(minDepth) (js/solver.js:591-608): a point over an ocean column
+ * deeper than minDepth (0 -> 0.12), halfway between the terrain surface and
+ * sea level; the deepest of 64 tries otherwise. Draws from the seeded stir
+ * stream (two per try made) instead of Math.random(). WS_ERR_STATE without
+ * terrain. xyz receives three host doubles. */
+ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz);
 
 /* ---- timing / synchronisation helpers */
 /* Times `reps` back-to-back launches of one kernel group on the handle's
@@ -338,10 +365,19 @@ ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak);
  * as if the kernels ran). kernel: 0 one red-black SOR iteration (two
  * launches, reported per launch), 1 P2G scatter, 2 fused G2P + advection,
  * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection,
- * 6 one whole persistent SOR solve of pressureIters iterations (list build +
- * cooperative kernel, reported per solve). */
+ * 6 one whole SOR solve of pressureIters iterations on the default path
+ * (reported per solve), 7 the same solve on the colour-list path (cluster-
+ * resident or grid-wide, whichever the lists fit; list build included). */
 ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us_per_launch);
 ws_status ws_synchronize(ws_handle* h);
+/* Failure-detection check (no counterpart in the reference, whose solver
+ * has no device waits): one device thread waits for a status word that
+ * nothing ever sets, with the same bounded wait the pressure solve uses
+ * between its CTAs, limited to `polls` polls (1..1e8; about 1 us each). The
+ * wait runs out, latches the timeout bit, and the call returns
+ * WS_ERR_TIMEOUT exactly as a timed-out solve reports it; the handle and
+ * its CUDA context stay usable. */
+ws_status ws_probe_wait(ws_handle* h, int64_t polls);
 ws_status ws_get_stream(ws_handle* h, void** cuda_stream);
 ws_status ws_launch_count(ws_handle* h, int64_t* launches);        /* kernels this handle launched */
 

@@ -106,6 +106,8 @@ def _lib(fp64):
         "or_push_balls": (None, [vp]),
         "or_update_balls": (None, [vp, d]),
         "or_stir_gaussian": (None, [vp, d, d]),
+        "or_wave_impulse": (None, [vp, d]),
+        "or_ocean_point": (None, [vp, d, C.POINTER(C.c_double)]),
         "or_mt_volume_field": (d, [vp, i32, i32, i32, d, d, i64p]),
         "or_mt_mesh_field": (d, [vp, i32, i32, i32, d, d, vp, vp, C.c_int64, i64p]),
         "or_metaball_field": (i32, [i32, vp, vp, vp, vp, i32, d, d, d, d, vp,
@@ -297,6 +299,14 @@ class Oracle:
 
     def stir_gaussian(self, sigma, peak):
         self.L.or_stir_gaussian(self.h, sigma, peak)
+
+    def wave_impulse(self, dvx):
+        self.L.or_wave_impulse(self.h, dvx)
+
+    def ocean_point(self, min_depth=0.0):
+        out = (C.c_double * 3)()
+        self.L.or_ocean_point(self.h, min_depth, out)
+        return [out[0], out[1], out[2]]
 
     # balls: addBall (js/solver.js:3910); rows x y z vx vy vz r rho submerged
     def add_ball(self, x, y, z, r, rho):

@@ -2701,3 +2701,62 @@ void or_stir_gaussian(or_solver* s, double sigma, double peak) {
     s->pvz[p] = (st_t)(s->pvz[p] + a * tz);
   }
 }
+
+/* waveImpulse, js/solver.js:3866-3892 (sphere mode). The reference draws from
+ * Math.random(); this restatement draws from the seeded stir stream, in the
+ * order the library defines: theta, phi, then one draw per particle in index
+ * order, taken whether or not the particle is pushed. */
+void or_wave_impulse(or_solver* s, double dvx) {
+  uint32_t st = s->S.stirS;
+  st = lcg(st); double th = st / 4294967296.0 * M_PI * 2;
+  st = lcg(st); double ph = acos(2 * (st / 4294967296.0) - 1);
+  double dx = sin(ph) * cos(th), dy = cos(ph), dz = sin(ph) * sin(th);
+  double cx = s->cx, cy = s->cy, cz = s->cz;
+  for (int p = 0; p < s->S.nP; p++) {
+    st = lcg(st);
+    double ex = s->px[p] - cx, ey = s->py[p] - cy, ez = s->pz[p] - cz;
+    double er = sqrt(ex * ex + ey * ey + ez * ez);
+    if (er == 0 || isnan(er)) er = 1e-9;
+    double pr = (ex * dx + ey * dy + ez * dz) / er;
+    if (pr <= 0) continue;
+    double f = pr * pr * pr * (0.7 + st / 4294967296.0 * 0.3);
+    s->pvx[p] = (st_t)(s->pvx[p] + ex / er * dvx * f);
+    s->pvy[p] = (st_t)(s->pvy[p] + ey / er * dvx * f);
+    s->pvz[p] = (st_t)(s->pvz[p] + ez / er * dvx * f);
+  }
+  s->S.stirS = st;
+}
+
+/* oceanPoint, js/solver.js:591-608, drawing u1 and theta of each try from
+ * the seeded stir stream instead of Math.random(). */
+void or_ocean_point(or_solver* s, double minDepth, double out[3]) {
+  double need = minDepth ? minDepth : 0.12;
+  double cx = s->cx, cy = s->cy, cz = s->cz, oceanR = s->S.oceanR;
+  int found = 0;
+  double bestD = -1, best[3] = { 0, 0, 0 };
+  int haveBest = 0;
+  uint32_t st = s->S.stirS;
+  for (int att = 0; att < 64; att++) {
+    st = lcg(st); double u1 = st / 4294967296.0 * 2 - 1;
+    st = lcg(st); double th = st / 4294967296.0 * 6.2831853;
+    double sq = sqrt(1 - u1 * u1);
+    double dxn = sq * cos(th), dyn = u1, dzn = sq * sin(th);
+    double Rt = or_terrain_radius_at(s, cx + dxn * s->Rhi, cy + dyn * s->Rhi, cz + dzn * s->Rhi);
+    double dpt = oceanR - Rt;
+    if (dpt > need) {
+      double rm = (Rt + oceanR) * 0.5;
+      out[0] = cx + dxn * rm; out[1] = cy + dyn * rm; out[2] = cz + dzn * rm;
+      found = 1;
+      break;
+    }
+    if (dpt > bestD) {
+      bestD = dpt; haveBest = 1;
+      best[0] = cx + dxn * (Rt + oceanR) * 0.5; best[1] = cy + dyn * (Rt + oceanR) * 0.5;
+      best[2] = cz + dzn * (Rt + oceanR) * 0.5;
+    }
+  }
+  s->S.stirS = st;
+  if (found) return;
+  if (haveBest) { out[0] = best[0]; out[1] = best[1]; out[2] = best[2]; }
+  else { out[0] = cx; out[1] = cy + oceanR; out[2] = cz; }
+}

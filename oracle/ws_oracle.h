@@ -131,6 +131,8 @@ void   or_apply_impulse_sphere(or_solver*, double cx, double cy, double cz, doub
 void   or_stir_at(or_solver*, double cx, double cy, double cz, double vx, double vy,
                   double vz, double R, double dt);
 void   or_stir_gaussian(or_solver*, double sigma, double peak);
+void   or_wave_impulse(or_solver*, double dvx);
+void   or_ocean_point(or_solver*, double minDepth, double out[3]);
 /* standalone marching-tets volume over an external corner field (js/surface.js:66-177) */
 double or_mt_volume_field(const void* dens, int nx, int ny, int nz, double dx, double iso,
                           int64_t* triCount);

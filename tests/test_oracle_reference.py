@@ -264,3 +264,31 @@ def test_census_and_kinetic_energy():
     L, I, V = o.census()
     assert abs(I - 10 / nP) < 1e-15 and abs(V - 5 / nP) < 1e-15
     assert o.kinetic_energy() == 0.0
+
+
+def test_wave_impulse_and_ocean_point_semantics():
+    """waveImpulse (js/solver.js:3866-3892): only particles on the bulge side
+    move, each pushed radially outward; the seeded stream advances by nP + 2
+    draws. oceanPoint (:591-608): the point lies over the ocean, halfway between
+    the terrain surface and sea level along its ray."""
+    o = planet("planet32", **PLAIN32)
+    nP = o.nP
+    c = o.nx * o.dx / 2
+    X = np.stack([o.arr(k)[:nP].astype(np.float64) for k in ("px", "py", "pz")], 1) - c
+    s0 = o.scalars.stirS
+    o.wave_impulse(0.5)
+    V = np.stack([o.arr(k)[:nP].astype(np.float64) for k in ("pvx", "pvy", "pvz")], 1)
+    moved = np.any(V != 0, axis=1)
+    assert 0.2 < moved.mean() < 0.8                      # one hemisphere, less the pole-on rim
+    radial = np.sum(V[moved] * X[moved], 1) / np.linalg.norm(X[moved], axis=1)
+    speed = np.linalg.norm(V[moved], axis=1)
+    assert np.all(radial > 0) and np.allclose(radial, speed, rtol=1e-5)
+    s = s0
+    for _ in range(nP + 2):
+        s = (s * 1664525 + 1013904223) % 2**32
+    assert o.scalars.stirS == s
+    p = np.array(o.ocean_point(0.3))
+    r = np.linalg.norm(p - c)
+    Rt = o.terrain_radius_at(*(c + (p - c) / r * o.scalars.oceanR * 1.4))
+    assert r < o.scalars.oceanR
+    assert o.scalars.oceanR - Rt > 0.3

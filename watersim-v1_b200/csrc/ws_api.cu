@@ -59,6 +59,7 @@ struct ws_handle {
   double *cellSum = nullptr, *cellChange = nullptr;
   void* contactScratch = nullptr;       // allocated on first contact pass
   void* mtScratch = nullptr;            // straddling-cell list of the marching tets, grown on demand
+  double* queryBuf = nullptr;           // point queries (sampleVel, terrainRadiusAt), allocated on first use
   size_t mtScratchBytes = 0;
   void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
   // substep graph: the kernel sequence of one substep captured once and
@@ -175,6 +176,7 @@ static void free_all(ws_handle* h) {
   for (void* b : bufs) if (b) cudaFree(b);
   if (h->contactScratch) cudaFree(h->contactScratch);
   if (h->mtScratch) cudaFree(h->mtScratch);
+  if (h->queryBuf) cudaFree(h->queryBuf);
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->net) { h->net->destroy(); delete h->net; }
@@ -258,7 +260,7 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   AL(h->blockCounts, nb) AL(h->list, P) AL(h->listCount, 1) AL(h->cand, P)
   long long partN = std::max((long long)grid_for(N, 128) + 1, (long long)(3 * nb));
   AL(h->partials, partN)
-  if ((e = sor_init(&h->sor, N, cfg->device)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "SOR state"); free_all(h); delete h; return r; }
+  if ((e = sor_init(&h->sor, h->d, cfg->device)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "SOR state"); free_all(h); delete h; return r; }
   h->partialsCap = (int)partN;
 #undef AL
   if ((e = cudaMallocHost(&h->stHost, sizeof(DevStatus))) != cudaSuccess ||
@@ -312,7 +314,9 @@ static ws_status sync_status(ws_handle* h) {
     int ebits = h->stHost->err;
     cudaMemsetAsync(&h->st->err, 0, sizeof(int), h->stream);
     if (ebits & WS_DERR_TIMEOUT) return fail(h, WS_ERR_TIMEOUT, "a bounded device wait ran out");
-    return fail(h, WS_ERR_DEVICE, "device fault latched (NaN or index out of range)");
+    if (ebits & WS_DERR_NAN)
+      return fail(h, WS_ERR_DEVICE, "device fault latched: a particle with a NaN or infinite position or velocity");
+    return fail(h, WS_ERR_DEVICE, "device fault latched: a fluid particle outside the domain box (range)");
   }
   return WS_OK;
 }
@@ -708,7 +712,7 @@ static ws_status stage_mark(ws_handle* h) {
   return check_launch(h, 1);
 }
 static ws_status stage_p2g(ws_handle* h) {
-  launch_p2g(h->d, grid_of(h), parts_of(h), h->stream);
+  launch_p2g(h->d, grid_of(h), parts_of(h), h->st, h->stream);
   launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
   return check_launch(h, 2);
 }
@@ -762,8 +766,8 @@ static ws_status stage_pressure(ws_handle* h) {
     h->launches += 23;
     join.armed = false;
     WS_TRY(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
-    e = launch_sor_run(h->sor, h->d, g, h->P.omega, iters, check, h->P.sorTol, &h->st->err, &dIters, &dRel, &dPath,
-                       h->stream);
+    e = launch_sor_run(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol, &h->st->err, &dIters, &dRel,
+                       &dPath, h->stream);
   } else {
     e = launch_sor_solve(h->sor, h->d, g, h->diag8, h->P.omega, iters, check, h->P.sorTol,
                          &h->st->err, &dIters, &dRel, &dPath, h->stream);
@@ -1238,6 +1242,83 @@ extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, d
   ws_status s = check_launch(h, 1); if (s) return s;
   return sync_status(h);
 }
+// waveImpulse (js/solver.js:3866-3892), sphere mode, on the seeded stir
+// stream: theta and phi of the bulge direction, then one draw per particle.
+extern "C" ws_status ws_wave_impulse(ws_handle* h, double dvx) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || !std::isfinite(dvx)) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  uint32_t st = h->S.stirS;
+  st = lcg_next(st); const double th = st / 4294967296.0 * M_PI * 2;
+  st = lcg_next(st); const double ph = std::acos(2 * (st / 4294967296.0) - 1);
+  const double dir[3] = { std::sin(ph) * std::cos(th), std::cos(ph), std::sin(ph) * std::sin(th) };
+  launch_wave_impulse(h->d, parts_of(h), dir, st, dvx, h->stream);
+  h->S.stirS = lcg_jump(st, (uint32_t)h->S.nP);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  return sync_status(h);
+}
+// dryLandFraction (js/solver.js:3593-3623) of the current cell types; 0
+// without terrain, as the reference
+extern "C" ws_status ws_dry_land_fraction(ws_handle* h, double* out) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || !out) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->terr.has) { *out = 0; return WS_OK; }
+  int* dry = reinterpret_cast<int*>(h->red);
+  launch_dry_land(h->d, h->terr, h->type, h->S.oceanR, dry, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  int n = 0;
+  WS_TRY(cudaMemcpyAsync(&n, dry, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if ((s = sync_status(h))) return s;
+  *out = n / 1200.0;
+  return WS_OK;
+}
+// points: n (x, y, z) triples of host doubles -> n results; staged through
+// the handle's scratch in chunks of kQueryChunk points
+static const long long kQueryChunk = 1 << 16;
+static ws_status query_points(ws_handle* h, const double* xyz, int64_t n, double* out, int perPoint, int kind) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || n < 0 || (n > 0 && (!xyz || !out))) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  if (!h->queryBuf) WS_TRY(cudaMalloc(&h->queryBuf, sizeof(double) * 6 * kQueryChunk));
+  double* din = h->queryBuf;
+  double* dout = h->queryBuf + 3 * kQueryChunk;
+  for (long long b = 0; b < n; b += kQueryChunk) {
+    const long long m = std::min<long long>(kQueryChunk, n - b);
+    WS_TRY(cudaMemcpyAsync(din, xyz + 3 * b, sizeof(double) * 3 * m, cudaMemcpyHostToDevice, h->stream));
+    if (kind == 0) launch_sample_vel(h->d, h->vel, din, m, dout, h->stream);
+    else launch_terrain_radius(h->terr, h->S.coreR, din, m, dout, h->stream);
+    ws_status s = check_launch(h, 1); if (s) return s;
+    WS_TRY(cudaMemcpyAsync(out + perPoint * b, dout, sizeof(double) * perPoint * m, cudaMemcpyDeviceToHost, h->stream));
+  }
+  return sync_status(h);
+}
+// sampleVel (js/solver.js:811-854) at n points: u, v, w per point
+extern "C" ws_status ws_sample_vel(ws_handle* h, const double* xyz, int64_t n, double* uvw) {
+  return query_points(h, xyz, n, uvw, 3, 0);
+}
+// terrainRadiusAt (js/solver.js:512-535) at n points
+extern "C" ws_status ws_terrain_radius_at(ws_handle* h, const double* xyz, int64_t n, double* radius) {
+  return query_points(h, xyz, n, radius, 1, 1);
+}
+// oceanPoint (js/solver.js:591-608) on the seeded stir stream
+extern "C" ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || !xyz) return WS_ERR_INVALID;
+  if (!h->terr.has) return fail(h, WS_ERR_STATE, "oceanPoint needs terrain");
+  cudaSetDevice(h->device);
+  const double need = minDepth ? minDepth : 0.12;            // `minDepth || 0.12`
+  double* dout = reinterpret_cast<double*>(h->red);
+  launch_ocean_point(h->d, h->terr, h->S.coreR, h->S.oceanR, need, h->S.stirS, dout, h->stream);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  double r[4];
+  WS_TRY(cudaMemcpyAsync(r, dout, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+  if ((s = sync_status(h))) return s;
+  xyz[0] = r[0]; xyz[1] = r[1]; xyz[2] = r[2];
+  h->S.stirS = lcg_jump(h->S.stirS, 2u * (uint32_t)r[3]);
+  return WS_OK;
+}
+
 // Seeded Gaussian stir kick: the draw order (u1, theta, phi from stirS) and
 // the tangent construction are part of the workload definition.
 extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
@@ -1281,6 +1362,21 @@ extern "C" ws_status ws_launch_count(ws_handle* h, int64_t* n) {
   return WS_OK;
 }
 
+// One device thread waits, with the library's bounded wait, for a status
+// word that nothing sets (DevStatus::pad stays zero).
+__global__ void k_probe_wait(DevStatus* st, long long polls) {
+  bounded_wait_geq(reinterpret_cast<const unsigned*>(&st->pad), 1u, polls, &st->err);
+}
+extern "C" ws_status ws_probe_wait(ws_handle* h, int64_t polls) {
+  if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  if (!h || polls < 1 || polls > 100000000) return WS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  ws_status s = sync_status(h); if (s) return s;
+  k_probe_wait<<<1, 1, 0, h->stream>>>(h->st, (long long)polls);
+  s = check_launch(h, 1); if (s) return s;
+  return sync_status(h);
+}
+
 extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !us || reps < 1) return WS_ERR_INVALID;
@@ -1295,7 +1391,7 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
     switch (kernel) {
       case 0: launch_sor_color(h->d, g, 0, 1 - h->P.omega, h->stream);
               launch_sor_color(h->d, g, 1, 1 - h->P.omega, h->stream); perRep = 2; break;
-      case 1: launch_p2g(h->d, g, parts_of(h), h->stream); break;
+      case 1: launch_p2g(h->d, g, parts_of(h), h->st, h->stream); break;
       case 2: { AdvectParams ap = advect_params(h, h->S.dtLast > 0 ? h->S.dtLast : 0.01);
                 launch_g2p_advect(h->d, g, parts_of(h), h->terr, ap, h->st, h->stream); } break;
       case 3: launch_faces_normalize_bc(h->d, g, h->stream); break;
@@ -1306,6 +1402,11 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
                                                   &h->st->err, &di, &dr, &dp, h->stream);
                 if (e6 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e6, "SOR solve"); }
                 h->launches += sor_solve_launches(h->sor) - 1; } break;   // list build; timed per whole solve
+      case 7: { int* di; double* dr; int* dp;
+                cudaError_t e7 = launch_sor_solve_lists(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
+                                                        &h->st->err, &di, &dr, &dp, h->stream);
+                if (e7 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e7, "SOR solve"); }
+                h->launches += sor_list_solve_launches(h->sor) - 1; } break;
       default: cudaEventDestroy(e0); cudaEventDestroy(e1); return fail(h, WS_ERR_INVALID, "unknown kernel id");
     }
   }

@@ -196,7 +196,7 @@ __device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc
   for (int q = 0; q < 8; q++)
     atomicAdd(&acc[o8[q]], make_float2((float)(wp[q] * v0) + (float)(wq[q] * v1), (float)wp[q] + (float)wq[q]));
 }
-__global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P) {
+__global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, int* err) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
   if (p0 >= P.nP) return;
   const bool has1 = p1 < P.nP;
@@ -206,7 +206,9 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P) {
   const float u0 = P.pvx[p0], v0 = P.pvy[p0], w0 = P.pvz[p0];
   const double x1 = has1 ? P.px[p1] : 0.0, y1 = has1 ? P.py[p1] : 0.0, z1 = has1 ? P.pz[p1] : 0.0;
   const float u1 = has1 ? P.pvx[p1] : 0.f, v1 = has1 ? P.pvy[p1] : 0.f, w1 = has1 ? P.pvz[p1] : 0.f;
-  const bool a = fl0 == 0, b = fl1 == 0;
+  // a fluid particle with a non-finite state is left out of the grid and latched
+  const bool a = fl0 == 0 && particle_sound(d, x0, y0, z0, u0, v0, w0, err, true);
+  const bool b = fl1 == 0 && particle_sound(d, x1, y1, z1, u1, v1, w1, err, true);
   if (a && b) {
     p2g_pair(d, g.acc, 0, x0, y0, z0, u0, x1, y1, z1, u1);
     p2g_pair(d, g.acc, 1, x0, y0, z0, v0, x1, y1, z1, v1);
@@ -218,9 +220,9 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P) {
     p2g_comp(d, g.acc, 2, x, y, z, a ? w0 : w1);
   }
 }
-void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s) {
+void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_p2g<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P);
+  k_p2g<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, &st->err);
 }
 
 // Solid-adjacent interior face: the velocity of the solid cell beside it,

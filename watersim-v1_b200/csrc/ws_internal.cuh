@@ -26,9 +26,9 @@
 #define WS_SOLID 2
 
 // device error bits latched in DevStatus::err
-#define WS_DERR_NAN 1
-#define WS_DERR_RANGE 2
-#define WS_DERR_TIMEOUT 4
+#define WS_DERR_NAN 1        // a particle with a non-finite position or velocity (P2G, G2P/advection)
+#define WS_DERR_RANGE 2      // a fluid particle outside the domain box at P2G
+#define WS_DERR_TIMEOUT 4    // a bounded device wait ran out
 
 // Division by an invariant divisor for dividends below 2^31: q = n / d as a
 // multiply-high and a shift, m = ceil(2^(31 + l) / d) with l = ceil(log2 d)
@@ -142,6 +142,32 @@ struct GridDev {
 };
 
 // ---------------------------------------------------------------- helpers
+// Bounded wait of one thread until *flag >= target (acquire loads at GPU
+// scope). After `limit` polls it latches WS_DERR_TIMEOUT and returns false,
+// so a peer that never arrives ends the wait with an error, never a hang.
+__device__ __forceinline__ bool bounded_wait_geq(const unsigned* flag, unsigned target, long long limit, int* err) {
+  long long n = 0;
+  for (;;) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    if (v >= target) return true;
+    if (++n > limit) { atomicOr(err, WS_DERR_TIMEOUT); return false; }
+  }
+}
+// Fault latch of a particle a pass reads or writes: a non-finite position or
+// velocity latches WS_DERR_NAN; a position outside the box [0, W] x [0, H] x
+// [0, D] latches WS_DERR_RANGE (the reference's passes keep particles at
+// least 1.02 cells inside it, so only corrupt input gets there). Returns
+// whether the particle is sound. Faults are rare: one atomic per faulty particle.
+__device__ __forceinline__ bool particle_sound(const Dims& d, double x, double y, double z, double u, double v,
+                                               double w, int* err, bool checkRange) {
+  if (!(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(u) && isfinite(v) && isfinite(w))) {
+    atomicOr(err, WS_DERR_NAN);
+    return false;
+  }
+  if (checkRange && (x < 0 || y < 0 || z < 0 || x > d.W || y > d.H || z > d.D)) atomicOr(err, WS_DERR_RANGE);
+  return true;
+}
 __device__ __forceinline__ int jtrunc(double v) { return (int)v; }
 __device__ __forceinline__ int jfloor_clamp(double v, int a, int b) {
   double f = floor(v);

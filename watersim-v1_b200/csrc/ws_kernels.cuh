@@ -27,7 +27,7 @@ void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_
 void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s);
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                        double oceanR, double coreR, cudaStream_t s);
-void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, cudaStream_t s);
+void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s);
 void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s);
 void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s);
 void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, int* sorCounts,
@@ -103,18 +103,34 @@ size_t render_scratch_bytes(long long capacity);
 void launch_render_particles(const RenderCfg& c, const PartsDev& P, void* scratch, RenderOut o, cudaStream_t s);
 void launch_particle_reduce(const PartsDev& P, int mode, double mp, double* partials, double* out, cudaStream_t s);
 
-// ---- ws_sor.cu
-cudaError_t sor_init(void** statePtr, long long nCells, int device);
+// ---- ws_queries.cu
+void launch_wave_impulse(const Dims& d, const PartsDev& P, const double dir[3], uint32_t s0, double dvx, cudaStream_t s);
+void launch_dry_land(const Dims& d, const TerrainDev& t, const uint8_t* type, double oceanR, int* dry, cudaStream_t s);
+void launch_sample_vel(const Dims& d, const float* vel, const double* xyz, long long n, double* out, cudaStream_t s);
+void launch_terrain_radius(const TerrainDev& t, double coreR, const double* xyz, long long n, double* out,
+                           cudaStream_t s);
+void launch_ocean_point(const Dims& d, const TerrainDev& t, double coreR, double oceanR, double need, uint32_t s0,
+                        double* out, cudaStream_t s);
+
+// ---- ws_sor.cu (colour lists) and ws_sor_tb.cu (temporal blocking on every SM)
+cudaError_t sor_init(void** statePtr, const Dims& d, int device);
 void sor_free(void* statePtr);
+// the colour lists the list paths need (nothing when the temporal-blocked
+// solve is the default: it builds its own plan)
 cudaError_t launch_sor_lists(void* state, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s);
-cudaError_t launch_sor_run(void* state, const Dims& d, const GridDev& g, double omega, int iters, int check,
-                           double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s);
+cudaError_t launch_sor_run(void* state, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                           int iters, int check, double tol, int* err, int** outIters, double** outRel, int** outPath,
+                           cudaStream_t s);
 cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
                              int iters, int check, double tol, int* err, int** outIters, double** outRel,
                              int** outPath, cudaStream_t s);
+cudaError_t launch_sor_solve_lists(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                                   int iters, int check, double tol, int* err, int** outIters, double** outRel,
+                                   int** outPath, cudaStream_t s);
 // per-256-cell-block colour counts the pressure setup fills for the list build
 int* sor_block_counts(void* state);
 int sor_solve_launches(void* state);
+int sor_list_solve_launches(void* state);
 
 // ---- ws_contacts.cu
 void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,

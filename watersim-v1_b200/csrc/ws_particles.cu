@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
     if (fl != 2 && fl != 3) { P.pvx[p] = fvx; P.pvy[p] = fvy; P.pvz[p] = fvz; }
     if (writePos) { P.px[p] = (float)x; P.py[p] = (float)y; P.pz[p] = (float)z; }
     if (coolWrite) P.pcool[p] = (uint8_t)cool;
+    if (fl != 2 && fl != 3) particle_sound(d, x, y, z, fvx, fvy, fvz, &st->err, false);
   }
   // airborne count (G2P's airCount): exact integer sum
   int wsum = warp_sum(air);

@@ -532,12 +532,25 @@ struct SorState {
   int grid = 0, block = 1024;
   long long cap = 0;
   int clusterSize = 0;       // 0: cluster path unavailable on this device
+  void* tb = nullptr;        // temporal-blocked solve (ws_sor_tb.cu); null: the colour-list paths
 };
 
-cudaError_t sor_init(void** statePtr, long long nCells, int device) {
+// the temporal-blocked solve (ws_sor_tb.cu)
+cudaError_t sor_tb_init(void** statePtr, const Dims& d, int device);
+void sor_tb_free(void* statePtr);
+cudaError_t launch_sor_tb(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                          int iters, int check, double tol, int* err, int* outIters, double* outRel, int* outPath,
+                          cudaStream_t s);
+// grids up to this many cells solve on every SM with temporal blocking (at
+// 128^3 every region fits in shared memory); larger ones on the colour lists
+static const long long kTbMaxCells = 160LL * 160 * 160;
+
+cudaError_t sor_init(void** statePtr, const Dims& d, int device) {
   SorState* S = new SorState();
   *statePtr = S;
+  const long long nCells = d.nCells;
   cudaError_t e;
+  if (nCells <= kTbMaxCells && (e = sor_tb_init(&S->tb, d, device)) != cudaSuccess) return e;
   int smCount = 0, perSM = 0;
   cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sor_persistent, S->block, 0)) != cudaSuccess) return e;
@@ -588,10 +601,16 @@ cudaError_t sor_init(void** statePtr, long long nCells, int device) {
 
 int* sor_block_counts(void* statePtr) { return statePtr ? ((SorState*)statePtr)->blockCounts : nullptr; }
 // kernels one launch_sor_solve issues: scan, scatter, [codes, cluster solve,] grid solve
-int sor_solve_launches(void* statePtr) { return statePtr && ((SorState*)statePtr)->clusterSize ? 5 : 3; }
+int sor_solve_launches(void* statePtr) {
+  SorState* S = (SorState*)statePtr;
+  if (S && S->tb) return 1;
+  return S && S->clusterSize ? 5 : 3;
+}
+int sor_list_solve_launches(void* statePtr) { return statePtr && ((SorState*)statePtr)->clusterSize ? 5 : 3; }
 void sor_free(void* statePtr) {
   SorState* S = (SorState*)statePtr;
   if (!S) return;
+  sor_tb_free(S->tb);
   for (int c = 0; c < 2; c++) { cudaFree(S->L.idx[c]); cudaFree(S->L.rhs[c]); cudaFree(S->L.pw[c]); cudaFree(S->L.dg[c]); cudaFree(S->L.code[c]); }
   cudaFree(S->L.pos);
   cudaFree(S->L.count); cudaFree(S->blockCounts); cudaFree(S->blockOffs); cudaFree(S->bar); cudaFree(S->partials);
@@ -606,8 +625,13 @@ void sor_free(void* statePtr) {
 // codes) and the barrier reset. They read the pressure setup's rhs, pw and
 // stencil bytes, never q, so they may run beside anything that only writes q
 // (the learned warm start).
+static cudaError_t build_lists(SorState* S, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s);
 cudaError_t launch_sor_lists(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s) {
   SorState* S = (SorState*)statePtr;
+  if (S->tb) return cudaSuccess;          // the temporal-blocked solve builds its own plan
+  return build_lists(S, d, g, diag8, s);
+}
+static cudaError_t build_lists(SorState* S, const Dims& d, const GridDev& g, const uint8_t* diag8, cudaStream_t s) {
   // the per-block colour counts come from the pressure setup (k_pressure_setup)
   int nb = (int)grid_for(d.nCells, 256);
   k_sor_scan<<<1, 1024, 0, s>>>(S->blockCounts, nb, S->blockOffs, S->L.count);
@@ -621,9 +645,19 @@ cudaError_t launch_sor_lists(void* statePtr, const Dims& d, const GridDev& g, co
 // The solve on the lists of launch_sor_lists: cluster-resident when they fit
 // one cluster, else the grid-wide persistent kernel (each returns at once when
 // the other path applies).
-cudaError_t launch_sor_run(void* statePtr, const Dims& d, const GridDev& g, double omega, int iters, int check,
-                           double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s) {
+static cudaError_t run_lists(SorState* S, const Dims& d, const GridDev& g, double omega, int iters, int check,
+                             double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s);
+cudaError_t launch_sor_run(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                           int iters, int check, double tol, int* err, int** outIters, double** outRel, int** outPath,
+                           cudaStream_t s) {
   SorState* S = (SorState*)statePtr;
+  *outPath = S->outPath; *outIters = S->outIters; *outRel = S->outRel;
+  if (S->tb)
+    return launch_sor_tb(S->tb, d, g, diag8, omega, iters, check, tol, err, S->outIters, S->outRel, S->outPath, s);
+  return run_lists(S, d, g, omega, iters, check, tol, err, outIters, outRel, outPath, s);
+}
+static cudaError_t run_lists(SorState* S, const Dims& d, const GridDev& g, double omega, int iters, int check,
+                             double tol, int* err, int** outIters, double** outRel, int** outPath, cudaStream_t s) {
   *outPath = S->outPath;
   int C = S->clusterSize;
   if (C) {
@@ -654,5 +688,15 @@ cudaError_t launch_sor_solve(void* statePtr, const Dims& d, const GridDev& g, co
                              int** outPath, cudaStream_t s) {
   cudaError_t e = launch_sor_lists(statePtr, d, g, diag8, s);
   if (e != cudaSuccess) return e;
-  return launch_sor_run(statePtr, d, g, omega, iters, check, tol, err, outIters, outRel, outPath, s);
+  return launch_sor_run(statePtr, d, g, diag8, omega, iters, check, tol, err, outIters, outRel, outPath, s);
+}
+// the same solve on the colour lists (cluster-resident or grid-wide), whatever
+// the default path; for comparisons of the two paths
+cudaError_t launch_sor_solve_lists(void* statePtr, const Dims& d, const GridDev& g, const uint8_t* diag8, double omega,
+                                   int iters, int check, double tol, int* err, int** outIters, double** outRel,
+                                   int** outPath, cudaStream_t s) {
+  SorState* S = (SorState*)statePtr;
+  cudaError_t e = build_lists(S, d, g, diag8, s);
+  if (e != cudaSuccess) return e;
+  return run_lists(S, d, g, omega, iters, check, tol, err, outIters, outRel, outPath, s);
 }

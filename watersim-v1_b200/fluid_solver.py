@@ -154,7 +154,8 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_upload_field", "ws_download_field", "ws_field_info", "ws_set_nparticles", "ws_step",
            "ws_substep", "ws_stage", "ws_residual", "ws_mt_volume", "ws_autotune_iso", "ws_census",
            "ws_kinetic_energy", "ws_apply_impulse_sphere", "ws_stir_at", "ws_stir_gaussian",
-           "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel",
+           "ws_wave_impulse", "ws_dry_land_fraction", "ws_sample_vel", "ws_terrain_radius_at", "ws_ocean_point",
+           "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel", "ws_probe_wait",
            "ws_residual_noalloc", "ws_upload_state", "ws_download_state",
            "ws_unet_init", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
@@ -193,9 +194,14 @@ def load_library(path=None):
         "ws_kinetic_energy": [h, C.POINTER(C.c_double)],
         "ws_apply_impulse_sphere": [h, d, d, d, d, d, d, d],
         "ws_stir_at": [h, d, d, d, d, d, d, d, d], "ws_stir_gaussian": [h, d, d],
+        "ws_wave_impulse": [h, d], "ws_dry_land_fraction": [h, C.POINTER(C.c_double)],
+        "ws_sample_vel": [h, C.c_void_p, C.c_int64, C.c_void_p],
+        "ws_terrain_radius_at": [h, C.c_void_p, C.c_int64, C.c_void_p],
+        "ws_ocean_point": [h, d, C.POINTER(C.c_double)],
         "ws_synchronize": [h], "ws_get_stream": [h, C.POINTER(C.c_void_p)],
         "ws_launch_count": [h, C.POINTER(C.c_int64)],
         "ws_time_kernel": [h, i32, i32, C.POINTER(C.c_double)],
+        "ws_probe_wait": [h, C.c_int64],
         "ws_upload_state": [h, C.POINTER(WsHostArrays)], "ws_download_state": [h, C.POINTER(WsHostArrays)],
         "ws_unet_init": [h, u32], "ws_unet_collect": [h, i32], "ws_unet_enable": [h, i32],
         "ws_unet_train": [h, i32, i32, d, u32, C.POINTER(C.c_double)],
@@ -685,6 +691,41 @@ class FluidSolver:
     def stir_gaussian(self, sigma, peak):
         self._check(self._L.ws_stir_gaussian(self._h, float(sigma), float(peak)))
 
+    def waveImpulse(self, dvx):
+        """waveImpulse (js/solver.js:3866), draws from the seeded stir stream."""
+        self._check(self._L.ws_wave_impulse(self._h, float(dvx)))
+
+    def dryLandFraction(self):
+        v = C.c_double()
+        self._check(self._L.ws_dry_land_fraction(self._h, C.byref(v)))
+        return v.value
+
+    def sample_vel(self, points):
+        """sampleVel at an (n, 3) array of points -> (n, 3) float64."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        out = np.empty_like(pts)
+        self._check(self._L.ws_sample_vel(self._h, pts.ctypes.data, pts.shape[0], out.ctypes.data))
+        return out
+
+    def sampleVel(self, x, y, z):
+        return tuple(self.sample_vel([[x, y, z]])[0])
+
+    def terrain_radius_at(self, points):
+        """terrainRadiusAt at an (n, 3) array of points -> (n,) float64."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        out = np.empty(pts.shape[0], np.float64)
+        self._check(self._L.ws_terrain_radius_at(self._h, pts.ctypes.data, pts.shape[0], out.ctypes.data))
+        return out
+
+    def terrainRadiusAt(self, x, y, z):
+        return float(self.terrain_radius_at([[x, y, z]])[0])
+
+    def oceanPoint(self, minDepth=0.0):
+        """oceanPoint (js/solver.js:591), draws from the seeded stir stream."""
+        out = (C.c_double * 3)()
+        self._check(self._L.ws_ocean_point(self._h, float(minDepth), out))
+        return [out[0], out[1], out[2]]
+
     def synchronize(self):
         self._check(self._L.ws_synchronize(self._h))
 
@@ -697,6 +738,12 @@ class FluidSolver:
         n = C.c_int64()
         self._check(self._L.ws_launch_count(self._h, C.byref(n)))
         return n.value
+
+    def probe_wait(self, polls):
+        """One bounded device wait on a word nothing sets (ws_probe_wait):
+        raises WsError with WS_ERR_TIMEOUT when it runs out, as a timed-out
+        solve does; the handle stays usable."""
+        self._check(self._L.ws_probe_wait(self._h, int(polls)))
 
     def time_kernel(self, kernel, reps=20):
         """Mean microseconds per launch of one kernel group (ws_time_kernel)."""
