@@ -4,8 +4,9 @@
   particle out of the grid and latches the NaN bit; the next synchronising
   call returns WS_ERR_DEVICE. The handle stays usable: after a clean upload
   the next substep succeeds.
-* A fluid particle uploaded outside the domain box latches the range bit the
-  same way (the reference's own passes keep particles inside it).
+* A particle uploaded outside the domain box latches the range bit the same
+  way when the next substep reads the positions (the reference's own passes
+  keep every particle inside it).
 * A bounded device wait that runs out (ws_probe_wait: a status word nothing
   sets, the same bounded wait the pressure solve's CTAs use between them)
   returns WS_ERR_TIMEOUT; the context stays usable.

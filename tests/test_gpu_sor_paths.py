@@ -32,6 +32,7 @@ def _paths_bitwise(fs, iters):
     fs.set_params(sorTol=0.0, pressureIters=iters)
     _system(fs)
     q0 = fs.q.copy()
+    q0[fs.cellType != 1] = 0.0           # as the pressure setup leaves q off the fluid
     fs.stage("PRESSURE")
     path = fs.scalars.sorPath
     q_default = fs.q.copy()

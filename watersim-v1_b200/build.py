@@ -52,7 +52,8 @@ def build(verbose=False, force=False, jobs=8):
             _wait(procs.pop(0))
     for p in procs:
         _wait(p)
-    link = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+    # --no-undefined: a declaration left behind by a signature change fails here, not at load time
+    link = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-Xlinker", "--no-undefined"]
     if verbose:
         print(" ".join(link))
     r = subprocess.run(link, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)

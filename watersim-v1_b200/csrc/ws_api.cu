@@ -316,7 +316,7 @@ static ws_status sync_status(ws_handle* h) {
     if (ebits & WS_DERR_TIMEOUT) return fail(h, WS_ERR_TIMEOUT, "a bounded device wait ran out");
     if (ebits & WS_DERR_NAN)
       return fail(h, WS_ERR_DEVICE, "device fault latched: a particle with a NaN or infinite position or velocity");
-    return fail(h, WS_ERR_DEVICE, "device fault latched: a fluid particle outside the domain box (range)");
+    return fail(h, WS_ERR_DEVICE, "device fault latched: a particle outside the domain box (range)");
   }
   return WS_OK;
 }
@@ -708,7 +708,7 @@ static ws_status stage_clear_raster(ws_handle* h) {
   return check_launch(h, 1);
 }
 static ws_status stage_mark(ws_handle* h) {
-  launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->stream);
+  launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->st, h->stream);
   return check_launch(h, 1);
 }
 static ws_status stage_p2g(ws_handle* h) {

@@ -133,13 +133,17 @@ __device__ __forceinline__ long long mark_cell(const Dims& d, const GridDev& g, 
 }
 // Two particles per thread: both particles' loads, then both cells' type
 // loads, then the (idempotent) stores, so the two chains overlap.
-__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR) {
+__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR, int* err) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
   if (p0 >= P.nP) return;
   const bool has1 = p1 < P.nP;
   const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
   const double X0 = P.px[p0], Y0 = P.py[p0], Z0 = P.pz[p0];
   const double X1 = has1 ? P.px[p1] : 0.0, Y1 = has1 ? P.py[p1] : 0.0, Z1 = has1 ? P.pz[p1] : 0.0;
+  // the first pass of a substep to read the positions: every particle must
+  // be finite and inside the domain box (the reference's passes keep it there)
+  particle_sound(d, X0, Y0, Z0, 0.0, 0.0, 0.0, err, true);
+  if (has1) particle_sound(d, X1, Y1, Z1, 0.0, 0.0, 0.0, err, true);
   const long long c0 = mark_cell(d, g, P, t, oceanR, coreR, p0, fl0, X0, Y0, Z0);
   const long long c1 = mark_cell(d, g, P, t, oceanR, coreR, p1, fl1, X1, Y1, Z1);
   const uint8_t t0 = c0 >= 0 ? g.type[c0] : (uint8_t)WS_SOLID, t1 = c1 >= 0 ? g.type[c1] : (uint8_t)WS_SOLID;
@@ -147,9 +151,9 @@ __global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double
   if (t1 == WS_AIR) g.type[c1] = WS_FLUID;
 }
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
-                       double oceanR, double coreR, cudaStream_t s) {
+                       double oceanR, double coreR, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR);
+  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, &st->err);
 }
 
 // ------------------------------------------------------------ 3. P2G scatter
@@ -207,8 +211,8 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, i
   const double x1 = has1 ? P.px[p1] : 0.0, y1 = has1 ? P.py[p1] : 0.0, z1 = has1 ? P.pz[p1] : 0.0;
   const float u1 = has1 ? P.pvx[p1] : 0.f, v1 = has1 ? P.pvy[p1] : 0.f, w1 = has1 ? P.pvz[p1] : 0.f;
   // a fluid particle with a non-finite state is left out of the grid and latched
-  const bool a = fl0 == 0 && particle_sound(d, x0, y0, z0, u0, v0, w0, err, true);
-  const bool b = fl1 == 0 && particle_sound(d, x1, y1, z1, u1, v1, w1, err, true);
+  const bool a = fl0 == 0 && particle_sound(d, x0, y0, z0, u0, v0, w0, err, false);
+  const bool b = fl1 == 0 && particle_sound(d, x1, y1, z1, u1, v1, w1, err, false);
   if (a && b) {
     p2g_pair(d, g.acc, 0, x0, y0, z0, u0, x1, y1, z1, u1);
     p2g_pair(d, g.acc, 1, x0, y0, z0, v0, x1, y1, z1, v1);

@@ -27,7 +27,7 @@
 
 // device error bits latched in DevStatus::err
 #define WS_DERR_NAN 1        // a particle with a non-finite position or velocity (P2G, G2P/advection)
-#define WS_DERR_RANGE 2      // a fluid particle outside the domain box at P2G
+#define WS_DERR_RANGE 2      // a particle outside the domain box when a substep starts
 #define WS_DERR_TIMEOUT 4    // a bounded device wait ran out
 
 // Division by an invariant divisor for dividends below 2^31: q = n / d as a

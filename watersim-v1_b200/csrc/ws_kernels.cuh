@@ -26,7 +26,7 @@ void launch_static_types(const Dims& d, const TerrainDev& t, double coreR, uint8
 void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_t s);
 void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s);
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
-                       double oceanR, double coreR, cudaStream_t s);
+                       double oceanR, double coreR, DevStatus* st, cudaStream_t s);
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s);
 void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s);
 void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s);

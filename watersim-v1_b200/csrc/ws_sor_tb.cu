@@ -286,20 +286,28 @@ __device__ double2 owned_residual(const TbArgs& a, const TbSmem& S, int O, doubl
   return out;
 }
 
-// publish this CTA's partial for check number k, wait for all, sum in CTA
-// order; every CTA gets the same value. false when the wait timed out.
+// publish this CTA's partial for check number k, wait for all, sum in a
+// fixed order (lane l adds partials l, l + 32, ..., then a fixed butterfly);
+// every CTA gets the same value. false when the wait timed out.
 __device__ bool global_residual(const TbArgs& a, double2 part, int k, double* sRel, int* sAbort) {
+  const int P = gridDim.x;
+  double2* buf = a.resPart + (size_t)(k & 1) * P;
   if (threadIdx.x == 0) {
-    const int P = gridDim.x;
-    double2* buf = a.resPart + (size_t)(k & 1) * P;
     __stcg(&buf[blockIdx.x], part);
     __threadfence();
     atomicAdd(&a.ctl->resCount, 1u);
     if (!bounded_wait_geq(&a.ctl->resCount, (unsigned)P * (unsigned)(k + 1), kTbSpinLimit, a.err)) *sAbort = 1;
-    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
     double rr = 0, bb = 0;
-    for (int b = 0; b < P; b++) { double2 v = __ldcg(&buf[b]); rr += v.x; bb += v.y; }
-    *sRel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
+    if (!*(volatile int*)sAbort)
+      for (int b = threadIdx.x; b < P; b += 32) { const double2 v = __ldcg(&buf[b]); rr += v.x; bb += v.y; }
+    for (int o = 16; o > 0; o >>= 1) {
+      rr += __shfl_xor_sync(0xffffffffu, rr, o);
+      bb += __shfl_xor_sync(0xffffffffu, bb, o);
+    }
+    if (threadIdx.x == 0) *sRel = bb > 0 ? sqrt(rr) / sqrt(bb) : sqrt(rr);
   }
   __syncthreads();
   return *(volatile int*)sAbort == 0;
@@ -647,9 +655,8 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       it += m;
       epoch++;
       write_owned((epoch & 1u) ? a.q1 : a.q);
-      __threadfence();
       __syncthreads();
-      if (tid == 0) st_release(&a.ctl->flag[p], epoch);
+      if (tid == 0) { __threadfence(); st_release(&a.ctl->flag[p], epoch); }
       fresh = false;
       checked = false;
       const bool doCheck = a.check > 0 && it % a.check == 0;
