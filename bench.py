@@ -184,16 +184,32 @@ def run_ours(args, rank, world, local_rank):
         ms = e0.elapsed_time(e1)
         if world > 1:
             ms = reduce_max(ms, "cuda")
-        its = []                         # SOR iterations per substep, read back afterwards
-        for _ in range(min(20, args.steps)):
+        return ms, clocks, launches
+
+    def from_start():
+        """Back to the state both arms start from (the captured substep graph
+        survives: the restored terrain is the same)."""
+        fs.restore(start)
+        count[0] = count0
+
+    def iterations():
+        """SOR iterations of each timed substep: the same K substeps replayed
+        from the start state, read back one by one."""
+        from_start()
+        its = []
+        for _ in range(args.steps):
             one_step()
             its.append(fs.scalars.sorIters)
-        return ms, clocks, launches, its
+        return its
 
     for _ in range(args.warmup):
         one_step()
+    # Both arms are timed over the same K substeps from one saved state.
+    start, count0 = fs.snapshot(), count[0]
     # ---- plain SOR arm
-    ms, clocks, launches, iters0 = timed_region()
+    from_start()
+    ms, clocks, launches = timed_region()
+    iters0 = iterations()
     plain = {"substeps_per_s": args.steps * world / (ms / 1000.0), "ms_per_step": ms / args.steps,
              "sor_iterations": sum(iters0) / len(iters0), "clocks": clocks}
     ms_plain = ms
@@ -201,12 +217,15 @@ def run_ours(args, rank, world, local_rank):
     learned = None
     if not args.no_learned:
         learned = learned_arm(fs, one_step, args, world)
-        for _ in range(args.warmup):
-            one_step()
-        ms, clocks, launches, iters1 = timed_region()
+        from_start()
+        one_step()                       # captures the substep graph with the prediction in it
+        from_start()
+        ms, clocks, launches = timed_region()
+        iters1 = iterations()
         learned["sor_iterations"] = sum(iters1) / len(iters1)
         learned["substeps_per_s"] = args.steps * world / (ms / 1000.0)
         learned["ms_per_step"] = ms / args.steps
+        learned["same_start_as_plain"] = True
         qsave = fs.download("q")
         learned["inference_ms"] = fs.unet_time(0, 10)   # applies the prediction repeatedly: restore q after
         fs.upload("q", qsave)

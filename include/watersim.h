@@ -367,7 +367,9 @@ ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz);
  * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection,
  * 6 one whole SOR solve of pressureIters iterations on the default path
  * (reported per solve), 7 the same solve on the colour-list path (cluster-
- * resident or grid-wide, whichever the lists fit; list build included). */
+ * resident or grid-wide, whichever the lists fit; list build included),
+ * 8..11 passes 3, 4, 5 and the extrapolation over the active-brick list of
+ * the last substep, as a substep runs them. */
 ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us_per_launch);
 ws_status ws_synchronize(ws_handle* h);
 /* Failure-detection check (no counterpart in the reference, whose solver

@@ -62,6 +62,12 @@ struct ws_handle {
   double* queryBuf = nullptr;           // point queries (sampleVel, terrainRadiusAt), allocated on first use
   size_t mtScratchBytes = 0;
   void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
+  // the substep's face and cell passes run over the active 4^3 bricks
+  BrickSet bricks{};
+  int* brickIota = nullptr;             // 0 .. nB - 1, the input of the list compaction
+  void* brickCub = nullptr;             // compaction scratch
+  size_t brickCubBytes = 0;
+  bool tbSetup = false;                 // the pressure setup may run over bricks (the solve needs no block counts)
   // substep graph: the kernel sequence of one substep captured once and
   // replayed while its launch parameters stay the same
   cudaGraphExec_t gexec = nullptr;
@@ -137,7 +143,12 @@ static GridDev grid_of(ws_handle* h) {
   g.omx = h->vort + 4 * N; g.omy = h->vort + 5 * N; g.omz = h->vort + 6 * N;
   g.dens = h->dens;
   g.sv = h->sv;
+  g.seed = h->bricks.seed; g.nbx = h->bricks.nbx; g.nby = h->bricks.nby;
   return g;
+}
+// the next substep processes every brick (after a caller or a single stage wrote grid fields)
+static void force_full_pass(ws_handle* h) {
+  if (h->bricks.forceAll) cudaMemsetAsync(h->bricks.forceAll, 1, sizeof(int), h->stream);
 }
 static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; return P; }
 
@@ -177,6 +188,11 @@ static void free_all(ws_handle* h) {
   if (h->contactScratch) cudaFree(h->contactScratch);
   if (h->mtScratch) cudaFree(h->mtScratch);
   if (h->queryBuf) cudaFree(h->queryBuf);
+  {
+    void* bb[] = { h->bricks.seed, h->bricks.act, h->bricks.proc, h->bricks.list, h->bricks.count, h->bricks.forceAll,
+                   h->brickIota, h->brickCub };
+    for (void* b : bb) if (b) cudaFree(b);
+  }
   if (h->sor) sor_free(h->sor);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->net) { h->net->destroy(); delete h->net; }
@@ -262,6 +278,24 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   AL(h->partials, partN)
   if ((e = sor_init(&h->sor, h->d, cfg->device)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "SOR state"); free_all(h); delete h; return r; }
   h->partialsCap = (int)partN;
+  h->tbSetup = sor_uses_tb(h->sor);
+  {
+    BrickSet& B = h->bricks;
+    B.nbx = (d.nx + 3) / 4; B.nby = (d.ny + 3) / 4; B.nbz = (d.nz + 3) / 4;
+    const long long nB = (long long)B.nbx * B.nby * B.nbz;
+    AL(B.seed, nB) AL(B.act, nB) AL(B.proc, nB) AL(B.list, nB) AL(B.count, 1) AL(B.forceAll, 1) AL(h->brickIota, nB)
+    h->brickCubBytes = brick_list_scratch_bytes((int)nB);
+    if ((e = cudaMalloc(&h->brickCub, h->brickCubBytes)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
+    std::vector<int> iota((size_t)nB);
+    for (long long b = 0; b < nB; b++) iota[(size_t)b] = (int)b;
+    const int one = 1;
+    if ((e = cudaMemcpy(h->brickIota, iota.data(), sizeof(int) * nB, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(B.seed, 0, (size_t)nB)) != cudaSuccess || (e = cudaMemset(B.act, 0, (size_t)nB)) != cudaSuccess ||
+        (e = cudaMemset(B.count, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemcpy(B.forceAll, &one, sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
+      ws_status r = fail_cuda(h, e, "brick state"); free_all(h); delete h; return r;
+    }
+  }
 #undef AL
   if ((e = cudaMallocHost(&h->stHost, sizeof(DevStatus))) != cudaSuccess ||
       (e = cudaMallocHost(&h->redHost, sizeof(double) * 8)) != cudaSuccess) {
@@ -436,6 +470,7 @@ extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host,
   if (count < 0 || count > r.count) return fail(h, WS_ERR_RANGE, "count exceeds the field size");
   if (r.kind != 0) return fail(h, WS_ERR_INVALID, "derived field is read-only");
   WS_TRY(cudaMemcpyAsync(r.ptr, host, (size_t)count * r.elem, cudaMemcpyHostToDevice, h->stream));
+  if (f >= WS_F_CELLTYPE) force_full_pass(h);          // a grid field: rewrite every brick next substep
   WS_TRY(cudaStreamSynchronize(h->stream));
   if (f == WS_F_PFLAG && !h->vaporPossible && any_vapor_flag((const uint8_t*)host, count))
     h->vaporPossible = true;
@@ -490,17 +525,25 @@ extern "C" ws_status ws_download_state(ws_handle* h, const ws_host_arrays* a) {
 static ws_status terrain_to_device(ws_handle* h) {
   const wsterrain::Terrain& T = h->hostTerrain;
   long long n3 = (long long)T.n * T.n * T.n;
-  drop_graph(h);
-  if (h->tsolid) { cudaFree(h->tsolid); h->tsolid = nullptr; }
-  if (h->tR) { cudaFree(h->tR); h->tR = nullptr; }
-  WS_TRY(cudaMalloc(&h->tsolid, (size_t)n3));
-  WS_TRY(cudaMalloc(&h->tR, sizeof(float) * (size_t)n3));
+  // A terrain of the same lattice size reuses the device buffers; the captured
+  // substep graph, which holds the terrain by value, survives when nothing it
+  // holds changes (the case of a snapshot restored onto its own planet).
+  const bool reuse = h->tsolid && h->tR && h->terr.has && h->terr.n == T.n;
+  if (!reuse) {
+    drop_graph(h);
+    if (h->tsolid) { cudaFree(h->tsolid); h->tsolid = nullptr; }
+    if (h->tR) { cudaFree(h->tR); h->tR = nullptr; }
+    WS_TRY(cudaMalloc(&h->tsolid, (size_t)n3));
+    WS_TRY(cudaMalloc(&h->tR, sizeof(float) * (size_t)n3));
+  }
   WS_TRY(cudaMemcpyAsync(h->tsolid, T.solid.data(), (size_t)n3, cudaMemcpyHostToDevice, h->stream));
   WS_TRY(cudaMemcpyAsync(h->tR, T.R.data(), sizeof(float) * (size_t)n3, cudaMemcpyHostToDevice, h->stream));
+  const TerrainDev before = h->terr;
   TerrainDev& t = h->terr;
   t.n = T.n; t.has = 1; t.dv = T.dv; t.Rsl = T.Rsl; t.Rlo = T.Rlo; t.Rhi = T.Rhi;
   t.Rlo2 = T.Rlo * T.Rlo; t.Rhi2 = T.Rhi * T.Rhi; t.solid = h->tsolid; t.R = h->tR;
   t.rdv = 1.0 / T.dv; t.dvPow2 = is_pow2(T.dv) ? 1 : 0;
+  if (reuse && std::memcmp(&before, &t, sizeof(TerrainDev)) != 0) drop_graph(h);
   h->S.landFrac = T.landFrac;
   h->hasTerrain = true;
   launch_static_types(h->d, t, h->S.coreR, h->staticTypes, h->stream);
@@ -522,6 +565,7 @@ extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double sea
 extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !t || t->n < 2 || !t->solid || !t->R) return WS_ERR_INVALID;
+  force_full_pass(h);                            // the static cell types change
   wsterrain::Terrain& T = h->hostTerrain;
   long long n3 = (long long)t->n * t->n * t->n;
   T.n = t->n; T.dv = t->dv; T.Rsl = t->Rsl; T.Rlo = t->Rlo; T.Rhi = t->Rhi; T.landFrac = t->landFrac;
@@ -567,6 +611,7 @@ extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
   double R2 = h->S.coreR + depth;
   h->S.oceanR = R2;
   h->nBalls = 0;                                 // resetWater drops the balls (js/solver.js:612, 652)
+  force_full_pass(h);
   if (!h->hasTerrain) { ws_status s = ws_generate_terrain(h, h->S.terrainSeed, R2); if (s) return s; }
   wsterrain::FillOutput fo;
   wsterrain::fill(h->hostTerrain, fill_input(h, depth), fo);
@@ -703,17 +748,28 @@ static AdvectParams advect_params(ws_handle* h, double dt) {
   return a;
 }
 
-static ws_status stage_clear_raster(ws_handle* h) {
-  launch_clear_raster(h->d, grid_of(h), h->st, h->stream);
-  return check_launch(h, 1);
+// Stages take `bricks`: inside a whole substep the face and cell passes run
+// over the active-brick list; a stage called on its own runs over the whole
+// grid and forces the next substep to process every brick.
+static ws_status stage_clear_raster(ws_handle* h, bool bricks = false) {
+  launch_clear_raster(h->d, grid_of(h), h->st, !bricks, h->stream);
+  if (bricks) launch_clear_acc_bricks(h->d, grid_of(h), h->bricks, h->stream);
+  return check_launch(h, bricks ? 3 : 1);
 }
-static ws_status stage_mark(ws_handle* h) {
+static ws_status stage_mark(ws_handle* h, bool bricks = false) {
   launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->st, h->stream);
-  return check_launch(h, 1);
+  ws_status s = check_launch(h, 1); if (s) return s;
+  if (bricks) {
+    cudaError_t e = launch_brick_activity(h->bricks, h->brickIota, h->brickCub, h->brickCubBytes, h->stream);
+    if (e != cudaSuccess) return fail_cuda(h, e, "active bricks");
+    s = check_launch(h, 3); if (s) return s;
+  }
+  return WS_OK;
 }
-static ws_status stage_p2g(ws_handle* h) {
+static ws_status stage_p2g(ws_handle* h, bool bricks = false) {
   launch_p2g(h->d, grid_of(h), parts_of(h), h->st, h->stream);
-  launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
+  if (bricks) launch_faces_normalize_bc_bricks(h->d, grid_of(h), h->bricks, h->stream);
+  else launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
   return check_launch(h, 2);
 }
 // planet gravity ramp, js/solver.js:2656-2662: the applied scale of this
@@ -723,19 +779,22 @@ static double gravity_scale(ws_handle* h, double dt) {
   h->S.gRamp += dt;
   return gs > 0 ? gs * h->P.gravity : 0;
 }
-static ws_status stage_forces(ws_handle* h, double dt, double gsA) {
+static ws_status stage_forces(ws_handle* h, double dt, double gsA, bool bricks = false) {
   double nu = h->P.viscosity;
   double coef = std::min(nu * dt / (h->d.dx * h->d.dx), 0.24);
   int viscOn = nu > 1e-6;
-  launch_faces_forces(h->d, grid_of(h), coef, viscOn, dt, gsA, h->stream);
+  if (bricks) launch_faces_forces_bricks(h->d, grid_of(h), h->bricks, coef, viscOn, dt, gsA, h->stream);
+  else launch_faces_forces(h->d, grid_of(h), coef, viscOn, dt, gsA, h->stream);
   return check_launch(h, 1);
 }
 // _pressureSolve: setup (diag, rhs, q = 0 off the fluid) then the whole SOR
 // solve in one persistent cooperative launch (ws_sor.cu). Iteration count and
 // FP64 residual land in the status word and are read at the next sync.
-static ws_status stage_pressure(ws_handle* h) {
+static ws_status stage_pressure(ws_handle* h, bool bricks = false) {
   GridDev g = grid_of(h);
-  launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, sor_block_counts(h->sor), h->stream);
+  // the colour-list solves need the setup's per-block counts over the whole grid
+  if (bricks && h->tbSetup) launch_pressure_setup_bricks(h->d, g, h->diag8, h->P.omega, h->st, h->bricks, h->stream);
+  else launch_pressure_setup(h->d, g, h->diag8, h->P.omega, h->st, sor_block_counts(h->sor), h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
   bool tolMode = h->P.sorTol > 0;
   int iters = tolMode ? h->P.sorMaxIters : h->P.pressureIters;
@@ -795,8 +854,9 @@ static void pull_substep(ws_handle* h) {
   h->S.umax = (double)bits_to_float(h->stHost->umaxBits);
   h->S.airborneCount = h->stHost->airborne;
 }
-static ws_status stage_project(ws_handle* h, bool clampToo) {
-  launch_project(h->d, grid_of(h), clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
+static ws_status stage_project(ws_handle* h, bool clampToo, bool bricks = false) {
+  if (bricks) launch_project_bricks(h->d, grid_of(h), h->bricks, clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
+  else launch_project(h->d, grid_of(h), clampToo ? 1 : 0, h->P.maxSpeed, h->st, h->stream);
   return check_launch(h, 1);
 }
 static ws_status stage_vorticity(ws_handle* h, double dt) {
@@ -808,8 +868,9 @@ static ws_status stage_clamp(ws_handle* h) {
   launch_clamp_umax(h->d, grid_of(h), h->P.maxSpeed, h->st, h->stream);
   return check_launch(h, 1);
 }
-static ws_status stage_extrapolate(ws_handle* h) {
-  launch_extrapolate(h->d, grid_of(h), h->stream);
+static ws_status stage_extrapolate(ws_handle* h, bool bricks = false) {
+  if (bricks) launch_extrapolate_bricks(h->d, grid_of(h), h->bricks, h->stream);
+  else launch_extrapolate(h->d, grid_of(h), h->stream);
   return check_launch(h, 1);
 }
 static ws_status stage_g2p_advect(ws_handle* h, double dt) {
@@ -829,23 +890,23 @@ static ws_status stage_g2p_advect(ws_handle* h, double dt) {
 // without any host synchronisation (capturable into a CUDA graph)
 static ws_status enqueue_substep(ws_handle* h, double dt, double gsA) {
   ws_status s;
-  if ((s = stage_clear_raster(h))) return s;
+  if ((s = stage_clear_raster(h, true))) return s;
   if (h->sv && (h->nBalls || h->hadSolidVelocity)) {      // balls become moving solids
-    launch_ball_raster(h->d, h->type, h->sv, true, h->balls, h->nBalls, h->stream);
+    launch_ball_raster(h->d, h->type, h->sv, true, h->balls, h->nBalls, grid_of(h), h->stream);
     if ((s = check_launch(h, h->nBalls ? 1 : 0))) return s;
   }
-  if ((s = stage_mark(h))) return s;
+  if ((s = stage_mark(h, true))) return s;
   if (h->nBalls) {
     launch_ball_push(parts_of(h), h->balls, h->nBalls, h->stream);
     if ((s = check_launch(h, h->S.nP ? 1 : 0))) return s;
   }
-  if ((s = stage_p2g(h))) return s;
-  if ((s = stage_forces(h, dt, gsA))) return s;
-  if ((s = stage_pressure(h))) return s;
+  if ((s = stage_p2g(h, true))) return s;
+  if ((s = stage_forces(h, dt, gsA, true))) return s;
+  if ((s = stage_pressure(h, true))) return s;
   bool vort = h->P.vorticity > 0;
-  if ((s = stage_project(h, !vort))) return s;
+  if ((s = stage_project(h, !vort, true))) return s;
   if (vort) { if ((s = stage_vorticity(h, dt))) return s; if ((s = stage_clamp(h))) return s; }
-  if ((s = stage_extrapolate(h))) return s;
+  if ((s = stage_extrapolate(h, true))) return s;
   if ((s = stage_g2p_advect(h, dt))) return s;
   if (h->nBalls) {                                        // _advect's push, then _updateBalls
     launch_ball_push(parts_of(h), h->balls, h->nBalls, h->stream);
@@ -1129,6 +1190,7 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = WS_OK;
+  force_full_pass(h);                            // a stage alone runs over the whole grid
   switch (stage) {
     case WS_STAGE_CLEAR_RASTER: s = stage_clear_raster(h); break;
     case WS_STAGE_MARK_FLUID: s = stage_mark(h); break;
@@ -1381,6 +1443,7 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h || !us || reps < 1) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
+  force_full_pass(h);
   cudaEvent_t e0, e1;
   WS_TRY(cudaEventCreate(&e0));
   WS_TRY(cudaEventCreate(&e1));
@@ -1402,6 +1465,10 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
                                                   &h->st->err, &di, &dr, &dp, h->stream);
                 if (e6 != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, e6, "SOR solve"); }
                 h->launches += sor_solve_launches(h->sor) - 1; } break;   // list build; timed per whole solve
+      case 8: launch_faces_normalize_bc_bricks(h->d, g, h->bricks, h->stream); break;
+      case 9: launch_faces_forces_bricks(h->d, g, h->bricks, 5e-6, 1, 0.01, 9.81, h->stream); break;
+      case 10: launch_project_bricks(h->d, g, h->bricks, 1, h->P.maxSpeed, h->st, h->stream); break;
+      case 11: launch_extrapolate_bricks(h->d, g, h->bricks, h->stream); break;
       case 7: { int* di; double* dr; int* dp;
                 cudaError_t e7 = launch_sor_solve_lists(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
                                                         &h->st->err, &di, &dr, &dp, h->stream);
@@ -1692,6 +1759,7 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
   if (size < (int64_t)sizeof(SnapHeader)) return fail(h, WS_ERR_INVALID, "not a snapshot");
+  force_full_pass(h);                            // q and the terrain come back
   SnapHeader hd;
   std::memcpy(&hd, buf, sizeof hd);
   if (std::memcmp(hd.magic, kSnapMagic, 8) != 0 || (hd.version != 1 && hd.version != 2) ||

@@ -35,7 +35,7 @@ __device__ __forceinline__ int ceil_clamp(double v, int a, int b) {
 }
 
 __global__ void k_ball_raster(Dims d, uint8_t* __restrict__ type, float* __restrict__ sv, const double* __restrict__ balls,
-                              int nb) {
+                              int nb, GridDev g) {
   const long long N = d.nCells;
   for (int n = 0; n < nb; n++) {
     const double* b = balls + n * BWORDS;
@@ -55,6 +55,7 @@ __global__ void k_ball_raster(Dims d, uint8_t* __restrict__ type, float* __restr
         const long long ci = ((long long)k * d.ny + j) * d.nx + i;
         type[ci] = WS_SOLID;
         sv[ci] = (float)b[BVX]; sv[N + ci] = (float)b[BVY]; sv[2 * N + ci] = (float)b[BVZ];
+        seed_cell(g, i, j, k);                        // a moving solid keeps its faces active
       }
     }
     __syncthreads();                                  // a later ball overwrites a shared cell
@@ -343,9 +344,9 @@ __global__ void k_ball_contacts(double* __restrict__ balls, int nb) {
 }  // namespace
 
 void launch_ball_raster(const Dims& d, uint8_t* type, float* sv, bool clearSv, const double* balls, int nb,
-                        cudaStream_t s) {
+                        const GridDev& g, cudaStream_t s) {
   if (clearSv) cudaMemsetAsync(sv, 0, sizeof(float) * 3 * (size_t)d.nCells, s);
-  if (nb > 0) k_ball_raster<<<1, 256, 0, s>>>(d, type, sv, balls, nb);
+  if (nb > 0) k_ball_raster<<<1, 256, 0, s>>>(d, type, sv, balls, nb, g);
 }
 void launch_ball_push(const PartsDev& P, const double* balls, int nb, cudaStream_t s) {
   if (nb > 0 && P.nP > 0) k_ball_push<<<grid_for(P.nP, 256), 256, 0, s>>>(P, balls, nb);

@@ -4,6 +4,8 @@
 // HBM-bound streaming passes; their algorithmic bytes per element are listed
 // next to each launcher and used for the roofline report.
 #include "ws_kernels.cuh"
+#include <algorithm>
+#include <cub/cub.cuh>
 
 // ------------------------------------------------------------ face decoding
 struct FaceIJK { int comp, i, j, k; long long local; };
@@ -94,18 +96,20 @@ void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_
 // (:865-871). Bytes: 8F (acc) + 2N.
 // 16-byte stores: two faces of the accumulator, sixteen cell types per
 // thread (both buffers are separate allocations, 256-byte aligned).
-__global__ void k_clear_raster(Dims d, GridDev g, DevStatus* st) {
+__global__ void k_clear_raster(Dims d, GridDev g, DevStatus* st, int clearAcc) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long F2 = d.F >> 1, n16 = d.nCells >> 4;
-  if (t < F2) reinterpret_cast<float4*>(g.acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-  else if (t == F2 && (d.F & 1)) g.acc[d.F - 1] = make_float2(0.f, 0.f);
+  if (clearAcc) {
+    if (t < F2) reinterpret_cast<float4*>(g.acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    else if (t == F2 && (d.F & 1)) g.acc[d.F - 1] = make_float2(0.f, 0.f);
+  }
   if (t < n16) reinterpret_cast<uint4*>(g.type)[t] = reinterpret_cast<const uint4*>(g.staticTypes)[t];
   else if (t < n16 + (d.nCells & 15)) { const long long c = (n16 << 4) + (t - n16); g.type[c] = g.staticTypes[c]; }
   if (t == 0) { st->umaxBits = 0u; st->airborne = 0; st->nFluid = 0; }
 }
-void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s) {
-  const long long a = (d.F >> 1) + 1, b = (d.nCells >> 4) + 16;
-  k_clear_raster<<<grid_for(a > b ? a : b, 256), 256, 0, s>>>(d, g, st);
+void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, bool clearAcc, cudaStream_t s) {
+  const long long a = clearAcc ? (d.F >> 1) + 1 : 0, b = (d.nCells >> 4) + 16;
+  k_clear_raster<<<grid_for(a > b ? a : b, 256), 256, 0, s>>>(d, g, st, clearAcc ? 1 : 0);
 }
 
 // ------------------------------------------------------------ 2. mark fluid
@@ -144,6 +148,12 @@ __global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double
   // be finite and inside the domain box (the reference's passes keep it there)
   particle_sound(d, X0, Y0, Z0, 0.0, 0.0, 0.0, err, true);
   if (has1) particle_sound(d, X1, Y1, Z1, 0.0, 0.0, 0.0, err, true);
+  // the brick of every particle's cell seeds this substep's active bricks
+  seed_cell(g, jfloor_clamp(over_dx(d, X0), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y0), 0, d.ny - 1),
+            jfloor_clamp(over_dx(d, Z0), 0, d.nz - 1));
+  if (has1)
+    seed_cell(g, jfloor_clamp(over_dx(d, X1), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y1), 0, d.ny - 1),
+              jfloor_clamp(over_dx(d, Z1), 0, d.nz - 1));
   const long long c0 = mark_cell(d, g, P, t, oceanR, coreR, p0, fl0, X0, Y0, Z0);
   const long long c1 = mark_cell(d, g, P, t, oceanR, coreR, p1, fl1, X1, Y1, Z1);
   const uint8_t t0 = c0 >= 0 ? g.type[c0] : (uint8_t)WS_SOLID, t1 = c1 >= 0 ? g.type[c1] : (uint8_t)WS_SOLID;
@@ -242,13 +252,10 @@ __device__ __forceinline__ float solid_face_velocity(const Dims& d, const GridDe
 // _p2gNormalizeFace (:1109-1120) + _applyBC (:1130-1171)
 // + FLIP snapshot (:2579) + the extrapolation valid mark (:1578-1611).
 // Bytes: 8F read + 4F vel + 4F velO + 1F valid + 2 type reads per face.
-__global__ void k_faces_normalize_bc(Dims d, GridDev g) {
-  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (f >= d.F) return;
+__device__ __forceinline__ void face_normalize_bc(const Dims& d, const GridDev& g, long long f, const FaceIJK& F) {
   float2 a = g.acc[f];
   float u = a.x;
   if ((double)a.y > 1e-8) u = (float)((double)a.x / (double)a.y);
-  FaceIJK F = decode_face(d, f);
   long long cL = 0, cR = 0;
   bool solidAdj = face_cells(d, F, cL, cR);
   if (solidAdj) u = 0.f;                                   // domain boundary plane
@@ -256,6 +263,11 @@ __global__ void k_faces_normalize_bc(Dims d, GridDev g) {
   g.vel[f] = u;
   g.velO[f] = u;
   g.valid[f] = ((double)a.y > 1e-8 || solidAdj) ? 1 : 0;
+}
+__global__ void k_faces_normalize_bc(Dims d, GridDev g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  face_normalize_bc(d, g, f, decode_face(d, f));
 }
 void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s) {
   k_faces_normalize_bc<<<grid_for(d.F, 256), 256, 0, s>>>(d, g);
@@ -265,10 +277,8 @@ void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s) 
 // _viscosity (:1259-1304, Jacobi: neighbours from the snapshot, which equals
 // the post-BC field on entry), planet gravity (:1229-1256 with the ramp of
 // :2656-2662 applied by the caller in gs) and the BC again (:2598).
-__global__ void k_faces_forces(Dims d, GridDev g, double coef, int viscOn, double dt, double gs) {
-  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (f >= d.F) return;
-  FaceIJK F = decode_face(d, f);
+__device__ __forceinline__ void face_forces(const Dims& d, const GridDev& g, long long f, const FaceIJK& F, double coef,
+                                            int viscOn, double dt, double gs) {
   long long cL = 0, cR = 0;
   if (face_cells(d, F, cL, cR)) { g.vel[f] = 0.f; return; }
   int tL = g.type[cL], tR = g.type[cR];
@@ -297,6 +307,11 @@ __global__ void k_faces_forces(Dims d, GridDev g, double coef, int viscOn, doubl
   if (gs > 0 && (tL == WS_FLUID || tR == WS_FLUID)) u = (float)((double)u + (double)g.gvel[f] * dt * gs);
   g.vel[f] = u;
 }
+__global__ void k_faces_forces(Dims d, GridDev g, double coef, int viscOn, double dt, double gs) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  face_forces(d, g, f, decode_face(d, f), coef, viscOn, dt, gs);
+}
 void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s) {
   k_faces_forces<<<grid_for(d.F, 256), 256, 0, s>>>(d, g, coef, viscOn, dt, gs);
 }
@@ -308,33 +323,37 @@ void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscO
 // 256-cell block also counts its interior fluid cells per colour for the SOR
 // list build (sorCounts[2 b], [2 b + 1]; null skips) and adds its fluid
 // cells to the fluid count with one atomic.
+// one cell of the setup: returns whether it is fluid and its SOR colour (-1 off the lists)
+__device__ __forceinline__ bool cell_pressure_setup(const Dims& d, const GridDev& g, uint8_t* __restrict__ diag8,
+                                                    double omega, long long c, int i, int j, int k, int& col) {
+  col = -1;
+  const uint8_t* type = g.type;
+  if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; return false; }
+  int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
+  long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
+                       j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
+  int cnt = 0;
+#pragma unroll
+  for (int q = 0; q < 6; q++) if (nbr[q] >= 0 && type[nbr[q]] != WS_SOLID) cnt++;
+  const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
+  double div = ((double)u[((long long)k * ny + j) * (nx + 1) + i + 1] - (double)u[((long long)k * ny + j) * (nx + 1) + i] +
+                (double)v[((long long)k * (ny + 1) + j + 1) * nx + i] - (double)v[((long long)k * (ny + 1) + j) * nx + i] +
+                (double)w[((long long)(k + 1) * ny + j) * nx + i] - (double)w[((long long)k * ny + j) * nx + i]) / d.dx;
+  g.rhs[c] = (float)(-d.dx * d.dx * div);
+  g.pw[c] = (float)(cnt > 0 ? omega / (double)cnt : 0.0);
+  diag8[c] = (uint8_t)cnt;
+  // membership of the SOR colour lists: interior fluid cells (sor_colour)
+  if (i >= 1 && j >= 1 && k >= 1 && i + 2 <= nx && j + 2 <= ny && k + 2 <= nz) col = (i + j + k) & 1;
+  return true;
+}
 __global__ void __launch_bounds__(256) k_pressure_setup(Dims d, GridDev g, uint8_t* __restrict__ diag8, double omega,
                                                         DevStatus* st, int* __restrict__ sorCounts) {
   __shared__ int wc[3][8];                           // per warp: colour-0 and colour-1 list cells, fluid cells
   const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   int col = -1, fluid = 0;
   if (c < d.nCells) {
-    const uint8_t* type = g.type;
-    if (type[c] != WS_FLUID) { g.q[c] = 0.f; g.pw[c] = -1.f; diag8[c] = 0; }
-    else {
-      int nx = d.nx, ny = d.ny, nz = d.nz; long long nxy = (long long)nx * ny;
-      int i, j, k; decode_cell(d, c, i, j, k);
-      long long nbr[6] = { i > 0 ? c - 1 : -1, i < nx - 1 ? c + 1 : -1, j > 0 ? c - nx : -1,
-                           j < ny - 1 ? c + nx : -1, k > 0 ? c - nxy : -1, k < nz - 1 ? c + nxy : -1 };
-      int cnt = 0;
-#pragma unroll
-      for (int q = 0; q < 6; q++) if (nbr[q] >= 0 && type[nbr[q]] != WS_SOLID) cnt++;
-      const float* u = g.vel; const float* v = g.vel + d.uN; const float* w = g.vel + d.uN + d.vN;
-      double div = ((double)u[((long long)k * ny + j) * (nx + 1) + i + 1] - (double)u[((long long)k * ny + j) * (nx + 1) + i] +
-                    (double)v[((long long)k * (ny + 1) + j + 1) * nx + i] - (double)v[((long long)k * (ny + 1) + j) * nx + i] +
-                    (double)w[((long long)(k + 1) * ny + j) * nx + i] - (double)w[((long long)k * ny + j) * nx + i]) / d.dx;
-      g.rhs[c] = (float)(-d.dx * d.dx * div);
-      g.pw[c] = (float)(cnt > 0 ? omega / (double)cnt : 0.0);
-      diag8[c] = (uint8_t)cnt;
-      fluid = 1;
-      // membership of the SOR colour lists: interior fluid cells (sor_colour)
-      if (i >= 1 && j >= 1 && k >= 1 && i + 2 <= nx && j + 2 <= ny && k + 2 <= nz) col = (i + j + k) & 1;
-    }
+    int i, j, k; decode_cell(d, c, i, j, k);
+    fluid = cell_pressure_setup(d, g, diag8, omega, c, i, j, k, col) ? 1 : 0;
   }
   const unsigned full = 0xffffffffu;
   const unsigned m0 = __ballot_sync(full, col == 0), m1 = __ballot_sync(full, col == 1), mf = __ballot_sync(full, fluid);
@@ -470,23 +489,25 @@ __device__ __forceinline__ void umax_reduce(float a, DevStatus* st) {
     if (lane == 0 && bits) atomicMax(&st->umaxBits, bits);
   }
 }
+__device__ __forceinline__ float face_project(const Dims& d, const GridDev& g, long long f, const FaceIJK& F, int doClamp,
+                                              float vcap) {
+  float u = g.vel[f];
+  long long cL = 0, cR = 0;
+  if (!face_cells(d, F, cL, cR)) {
+    int tL = g.type[cL], tR = g.type[cR];
+    if (tL != WS_SOLID && tR != WS_SOLID) {
+      double pL = tL == WS_FLUID ? (double)g.q[cL] : 0.0, pR = tR == WS_FLUID ? (double)g.q[cR] : 0.0;
+      u = (float)((double)u - (pR - pL) * (1.0 / d.dx));
+    }
+  }
+  if (doClamp) { if (u > vcap) u = vcap; else if (u < -vcap) u = -vcap; }
+  g.vel[f] = u;
+  return u;
+}
 __global__ void k_project(Dims d, GridDev g, int doClamp, float vcap, DevStatus* st) {
   long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   float u = 0.f;
-  if (f < d.F) {
-    u = g.vel[f];
-    FaceIJK F = decode_face(d, f);
-    long long cL = 0, cR = 0;
-    if (!face_cells(d, F, cL, cR)) {
-      int tL = g.type[cL], tR = g.type[cR];
-      if (tL != WS_SOLID && tR != WS_SOLID) {
-        double pL = tL == WS_FLUID ? (double)g.q[cL] : 0.0, pR = tR == WS_FLUID ? (double)g.q[cR] : 0.0;
-        u = (float)((double)u - (pR - pL) * (1.0 / d.dx));
-      }
-    }
-    if (doClamp) { if (u > vcap) u = vcap; else if (u < -vcap) u = -vcap; }
-    g.vel[f] = u;
-  }
+  if (f < d.F) u = face_project(d, g, f, decode_face(d, f), doClamp, vcap);
   if (doClamp) umax_reduce(u, st);
 }
 void launch_project(const Dims& d, const GridDev& g, int doClamp, double maxSpeed, DevStatus* st, cudaStream_t s) {
@@ -594,12 +615,8 @@ void launch_vorticity(const Dims& d, const GridDev& g, double eps, double dt, cu
 // the mean of the neighbours (same component grid) that were valid before
 // the pass, summed in the reference's order -i, +i, -j, +j, -k, +k. Filled
 // faces are marked 2 so no thread reads a value written in this pass.
-__global__ void k_extrapolate(Dims d, GridDev g) {
-  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (f >= d.F) return;
+__device__ __forceinline__ void face_extrapolate(const Dims& d, const GridDev& g, long long f, const FaceIJK& F) {
   const uint8_t* valid = g.valid;
-  if (valid[f] != 0) return;
-  FaceIJK F = decode_face(d, f);
   int d0, d1, d2;
   if (F.comp == 0) { d0 = d.nx + 1; d1 = d.ny; d2 = d.nz; }
   else if (F.comp == 1) { d0 = d.nx; d1 = d.ny + 1; d2 = d.nz; }
@@ -615,8 +632,173 @@ __global__ void k_extrapolate(Dims d, GridDev g) {
   if (F.k < d2 - 1 && valid[f + sK] == 1) { sum += a[f + sK]; cnt++; }
   if (cnt > 0) { g.vel[f] = (float)(sum / cnt); g.valid[f] = 2; }
 }
+__global__ void k_extrapolate(Dims d, GridDev g) {
+  long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (f >= d.F) return;
+  if (g.valid[f] != 0) return;
+  face_extrapolate(d, g, f, decode_face(d, f));
+}
 void launch_extrapolate(const Dims& d, const GridDev& g, cudaStream_t s) {
   k_extrapolate<<<grid_for(d.F, 256), 256, 0, s>>>(d, g);
+}
+
+// ------------------------------------------------------------ active bricks
+// Faces and cells far from every particle and moving solid hold fixed values
+// (zero velocity, the static valid flags, q = 0 and pw = -1 off the fluid), so
+// a full pass over them rewrites what is already there. The substep therefore
+// runs its face and cell passes over a list of 4^3 bricks: those within one
+// brick of a particle's or moving solid's cell this substep (the reach of
+// P2G's stencils, the extrapolation layer and G2P's midpoint sample is under
+// four cells), plus those active in the previous substep, so a brick that
+// empties is rewritten once to the fixed values. A forced full pass (after a
+// caller wrote grid fields) processes every brick.
+__global__ void k_brick_activity(int nbx, int nby, int nbz, const uint8_t* __restrict__ seed, uint8_t* __restrict__ act,
+                                 uint8_t* __restrict__ proc, const int* __restrict__ forceAll) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nB = nbx * nby * nbz;
+  if (b >= nB) return;
+  const int bx = b % nbx, t = b / nbx, by = t % nby, bz = t / nby;
+  int a = 0;
+  for (int dz = -1; dz <= 1 && !a; dz++) {
+    const int z = bz + dz;
+    if (z < 0 || z >= nbz) continue;
+    for (int dy = -1; dy <= 1 && !a; dy++) {
+      const int y = by + dy;
+      if (y < 0 || y >= nby) continue;
+      const uint8_t* row = seed + ((long long)z * nby + y) * nbx;
+      for (int dx = -1; dx <= 1; dx++) {
+        const int x = bx + dx;
+        if (x >= 0 && x < nbx && row[x]) { a = 1; break; }
+      }
+    }
+  }
+  proc[b] = (uint8_t)(a | act[b] | (*forceAll != 0));
+  act[b] = (uint8_t)a;
+}
+size_t brick_list_scratch_bytes(int nB) {
+  size_t bytes = 0;
+  cub::DeviceSelect::Flagged(nullptr, bytes, (const int*)nullptr, (const uint8_t*)nullptr, (int*)nullptr, (int*)nullptr, nB);
+  return bytes;
+}
+// activity, the ordered brick list (CUB's flagged selection, a CUDA toolkit
+// library), then the seeds and the forced-pass flag cleared for the next substep
+cudaError_t launch_brick_activity(const BrickSet& B, const int* iota, void* scratch, size_t scratchBytes, cudaStream_t s) {
+  const int nB = B.nbx * B.nby * B.nbz;
+  k_brick_activity<<<grid_for(nB, 256), 256, 0, s>>>(B.nbx, B.nby, B.nbz, B.seed, B.act, B.proc, B.forceAll);
+  cudaError_t e = cub::DeviceSelect::Flagged(scratch, scratchBytes, iota, B.proc, B.list, B.count, nB, s);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(B.seed, 0, (size_t)nB, s)) != cudaSuccess) return e;
+  return cudaMemsetAsync(B.forceAll, 0, sizeof(int), s);
+}
+
+// The faces a brick owns: per component, the 64 faces whose lower cell lies
+// in the brick, and on the last brick along the component's axis the 16
+// faces of the domain's upper plane. Slot t in [0, 240).
+__device__ __forceinline__ bool brick_face(const Dims& d, const BrickSet& B, int b, int t, long long& f, FaceIJK& F) {
+  const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
+  const int comp = t / 80, s = t - comp * 80;
+  int la, lb, lc;
+  const bool upper = s >= 64;
+  if (!upper) { la = s & 3; lb = (s >> 2) & 3; lc = s >> 4; }
+  else { la = 0; lb = (s - 64) & 3; lc = (s - 64) >> 2; }
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  F.comp = comp;
+  if (comp == 0) {
+    if (upper && bx != B.nbx - 1) return false;
+    F.i = upper ? nx : bx * 4 + la; F.j = by * 4 + lb; F.k = bz * 4 + lc;
+    if ((!upper && F.i >= nx) || F.j >= ny || F.k >= nz) return false;
+    f = ((long long)F.k * ny + F.j) * (nx + 1) + F.i;
+  } else if (comp == 1) {
+    if (upper && by != B.nby - 1) return false;
+    F.j = upper ? ny : by * 4 + la; F.i = bx * 4 + lb; F.k = bz * 4 + lc;
+    if ((!upper && F.j >= ny) || F.i >= nx || F.k >= nz) return false;
+    f = d.uN + ((long long)F.k * (ny + 1) + F.j) * nx + F.i;
+  } else {
+    if (upper && bz != B.nbz - 1) return false;
+    F.k = upper ? nz : bz * 4 + la; F.i = bx * 4 + lb; F.j = by * 4 + lc;
+    if ((!upper && F.k >= nz) || F.i >= nx || F.j >= ny) return false;
+    f = d.uN + d.vN + ((long long)F.k * ny + F.j) * nx + F.i;
+  }
+  F.local = 0;
+  return true;
+}
+
+// one face pass over the brick list (persistent blocks, one brick per
+// iteration); op 0 normalise + BC, 1 forces, 2 project (+ clamp, umax),
+// 3 extrapolate, 4 clear the P2G accumulator
+struct FacePassArgs { double coef, dt, gs; int viscOn, doClamp; float vcap; };
+template <int OP>
+__global__ void __launch_bounds__(256) k_faces_bricks(Dims d, GridDev g, BrickSet B, FacePassArgs fa, DevStatus* st) {
+  const int n = *B.count;
+  float umax = 0.f;
+  for (int it = blockIdx.x; it < n; it += gridDim.x) {
+    const int b = B.list[it];
+    long long f; FaceIJK F;
+    if (threadIdx.x < 240 && brick_face(d, B, b, threadIdx.x, f, F)) {
+      if (OP == 0) face_normalize_bc(d, g, f, F);
+      else if (OP == 1) face_forces(d, g, f, F, fa.coef, fa.viscOn, fa.dt, fa.gs);
+      else if (OP == 2) umax = fmaxf(umax, fabsf(face_project(d, g, f, F, fa.doClamp, fa.vcap)));
+      else if (OP == 3) { if (g.valid[f] == 0) face_extrapolate(d, g, f, F); }
+      else g.acc[f] = make_float2(0.f, 0.f);
+    }
+  }
+  if (OP == 2 && fa.doClamp) umax_reduce(umax, st);
+}
+static unsigned brick_grid(const BrickSet& B) {
+  const int nB = B.nbx * B.nby * B.nbz;
+  return (unsigned)std::min(nB, 148 * 8);
+}
+void launch_faces_normalize_bc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s) {
+  k_faces_bricks<0><<<brick_grid(B), 256, 0, s>>>(d, g, B, FacePassArgs{}, nullptr);
+}
+void launch_faces_forces_bricks(const Dims& d, const GridDev& g, const BrickSet& B, double coef, int viscOn, double dt,
+                                double gs, cudaStream_t s) {
+  FacePassArgs fa{}; fa.coef = coef; fa.viscOn = viscOn; fa.dt = dt; fa.gs = gs;
+  k_faces_bricks<1><<<brick_grid(B), 256, 0, s>>>(d, g, B, fa, nullptr);
+}
+void launch_project_bricks(const Dims& d, const GridDev& g, const BrickSet& B, int doClamp, double maxSpeed,
+                           DevStatus* st, cudaStream_t s) {
+  FacePassArgs fa{}; fa.doClamp = doClamp; fa.vcap = (float)(maxSpeed * 1.1);
+  k_faces_bricks<2><<<brick_grid(B), 256, 0, s>>>(d, g, B, fa, st);
+}
+void launch_extrapolate_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s) {
+  k_faces_bricks<3><<<brick_grid(B), 256, 0, s>>>(d, g, B, FacePassArgs{}, nullptr);
+}
+// the accumulator of the bricks in the list (those the previous substep's
+// P2G may have written), or all of it after a forced full pass
+__global__ void k_clear_acc_all(Dims d, float2* acc, const int* __restrict__ forceAll) {
+  if (!*forceAll) return;
+  const long long F2 = d.F >> 1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t <= F2; t += (long long)gridDim.x * blockDim.x) {
+    if (t < F2) reinterpret_cast<float4*>(acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    else if (d.F & 1) acc[d.F - 1] = make_float2(0.f, 0.f);
+  }
+}
+void launch_clear_acc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s) {
+  k_clear_acc_all<<<148 * 8, 256, 0, s>>>(d, g.acc, B.forceAll);
+  k_faces_bricks<4><<<brick_grid(B), 256, 0, s>>>(d, g, B, FacePassArgs{}, nullptr);
+}
+// the pressure setup over the brick list: four bricks per 256-thread block
+__global__ void __launch_bounds__(256) k_pressure_setup_bricks(Dims d, GridDev g, uint8_t* __restrict__ diag8,
+                                                               double omega, DevStatus* st, BrickSet B) {
+  const int n = *B.count;
+  int fluid = 0;
+  for (int it = blockIdx.x * 4; it < n; it += gridDim.x * 4) {
+    const int e = it + (threadIdx.x >> 6);
+    if (e >= n) continue;
+    const int b = B.list[e], c = threadIdx.x & 63;
+    const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
+    const int i = bx * 4 + (c & 3), j = by * 4 + ((c >> 2) & 3), k = bz * 4 + (c >> 4);
+    if (i >= d.nx || j >= d.ny || k >= d.nz) continue;
+    int col;
+    if (cell_pressure_setup(d, g, diag8, omega, ((long long)k * d.ny + j) * d.nx + i, i, j, k, col)) fluid++;
+  }
+  fluid = warp_sum(fluid);
+  if ((threadIdx.x & 31) == 0 && fluid) atomicAdd(&st->nFluid, fluid);
+}
+void launch_pressure_setup_bricks(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st,
+                                  const BrickSet& B, cudaStream_t s) {
+  k_pressure_setup_bricks<<<brick_grid(B), 256, 0, s>>>(d, g, diag8, omega, st, B);
 }
 
 // ------------------------------------------------------------ field helpers

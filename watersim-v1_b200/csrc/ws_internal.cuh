@@ -139,7 +139,23 @@ struct GridDev {
   float *vfx, *vfy, *vfz, *omg, *omx, *omy, *omz;
   float* dens;
   const float* sv;          // solid velocity (3 x nCells: x, y, z) of moving solids, or null
+  uint8_t* seed;            // 4^3 bricks holding a particle or a moving solid this substep (or null)
+  int nbx, nby;             // bricks per axis (x, y) of the seed map
 };
+// The 4^3-brick work list of the substep's face and cell passes (ws_grid.cu)
+struct BrickSet {
+  int nbx, nby, nbz;
+  uint8_t* seed;            // bricks holding a particle or moving solid this substep
+  uint8_t* act;             // seeds dilated by one brick (kept for the next substep)
+  uint8_t* proc;            // this substep's work: act | last substep's act | forced
+  int* list;                // the bricks with proc set, in increasing order
+  int* count;
+  int* forceAll;            // device flag: process every brick once
+};
+// the seed brick of cell (i, j, k)
+__device__ __forceinline__ void seed_cell(const GridDev& g, int i, int j, int k) {
+  if (g.seed) g.seed[((k >> 2) * g.nby + (j >> 2)) * g.nbx + (i >> 2)] = 1;
+}
 
 // ---------------------------------------------------------------- helpers
 // Bounded wait of one thread until *flag >= target (acquire loads at GPU

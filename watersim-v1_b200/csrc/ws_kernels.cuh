@@ -24,7 +24,19 @@ struct PhaseParams {
 // ---- ws_grid.cu
 void launch_static_types(const Dims& d, const TerrainDev& t, double coreR, uint8_t* st, cudaStream_t s);
 void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_t s);
-void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, cudaStream_t s);
+void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, bool clearAcc, cudaStream_t s);
+// the substep's face and cell passes over the active-brick list (ws_grid.cu)
+size_t brick_list_scratch_bytes(int nB);
+cudaError_t launch_brick_activity(const BrickSet& B, const int* iota, void* scratch, size_t scratchBytes, cudaStream_t s);
+void launch_clear_acc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
+void launch_faces_normalize_bc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
+void launch_faces_forces_bricks(const Dims& d, const GridDev& g, const BrickSet& B, double coef, int viscOn, double dt,
+                                double gs, cudaStream_t s);
+void launch_project_bricks(const Dims& d, const GridDev& g, const BrickSet& B, int doClamp, double maxSpeed,
+                           DevStatus* st, cudaStream_t s);
+void launch_extrapolate_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
+void launch_pressure_setup_bricks(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st,
+                                  const BrickSet& B, cudaStream_t s);
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                        double oceanR, double coreR, DevStatus* st, cudaStream_t s);
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s);
@@ -91,7 +103,7 @@ void launch_mt_mesh(const Dims& d, const float* dens, double iso, const double2*
 // balls (ws_balls.cu): moving-solid raster (after the static raster),
 // particle push-out, and the per-substep histogram + integration
 void launch_ball_raster(const Dims& d, uint8_t* type, float* sv, bool clearSv, const double* balls, int nb,
-                        cudaStream_t s);
+                        const GridDev& g, cudaStream_t s);
 void launch_ball_push(const PartsDev& P, const double* balls, int nb, cudaStream_t s);
 void launch_ball_update(const Dims& d, const float* vel, const TerrainDev& t, const PartsDev& P, double* balls, int nb,
                         int* hist, float* surfY, const BallEnv& env, double dt, cudaStream_t s);
@@ -131,6 +143,8 @@ cudaError_t launch_sor_solve_lists(void* statePtr, const Dims& d, const GridDev&
 int* sor_block_counts(void* state);
 int sor_solve_launches(void* state);
 int sor_list_solve_launches(void* state);
+// whether the default solve is the temporal-blocked one (it needs no per-block colour counts)
+bool sor_uses_tb(void* state);
 
 // ---- ws_contacts.cu
 void launch_vapor_collisions(const Dims& d, const PartsDev& P, double spacing, double oceanR, int spinOn,

@@ -606,6 +606,7 @@ int sor_solve_launches(void* statePtr) {
   if (S && S->tb) return 1;
   return S && S->clusterSize ? 5 : 3;
 }
+bool sor_uses_tb(void* statePtr) { return statePtr && ((SorState*)statePtr)->tb; }
 int sor_list_solve_launches(void* statePtr) { return statePtr && ((SorState*)statePtr)->clusterSize ? 5 : 3; }
 void sor_free(void* statePtr) {
   SorState* S = (SorState*)statePtr;
