@@ -360,6 +360,25 @@ def learned_arm(fs, one_step, args, world=1):
             "probe_relres_predicted": sum(r[3] for r in rows) / n}
 
 
+def active_bricks(fs):
+    """4^3 bricks within one brick of a particle's cell (the substep's work
+    list, less the bricks kept for one substep after they empty)."""
+    import numpy as np
+    n = fs.nx
+    nb = (n + 3) // 4
+    nP = fs.scalars.nP
+    ijk = [np.clip(np.floor(fs.download(k, nP) / fs.dx).astype(np.int64), 0, n - 1) // 4 for k in ("px", "py", "pz")]
+    seed = np.zeros((nb, nb, nb), bool)
+    seed[ijk[2], ijk[1], ijk[0]] = True
+    act = np.zeros_like(seed)
+    p = np.pad(seed, 1)
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                act |= p[dz:dz + nb, dy:dy + nb, dx:dx + nb]
+    return int(act.sum())
+
+
 def roofline(fs, ms_step, iters):
     """Dominant kernel by measured time share per substep; achieved =
     algorithmic bytes per launch / live launch time (CUDA events on the
@@ -375,25 +394,31 @@ def roofline(fs, ms_step, iters):
     fs.pressureIters = it
     us_sor = fs.time_kernel(6, 5)                 # whole solve of `it` iterations
     fs.pressureIters = keep
+    # the face passes as the substep runs them: over the active-brick list of
+    # the last substep (ids 8-11); their bytes count the faces of those bricks
+    us_f1 = fs.time_kernel(8, 5)
+    us_f2 = fs.time_kernel(9, 5)
+    us_pr = fs.time_kernel(10, 5)
+    us_ex = fs.time_kernel(11, 5)
+    Fa = 192.0 * active_bricks(fs)
     us_p2g = fs.time_kernel(1, 5)
     us_g2p = fs.time_kernel(2, 5)
-    us_f1 = fs.time_kernel(3, 5)
-    us_f2 = fs.time_kernel(4, 5)
-    us_pr = fs.time_kernel(5, 5)
     step_us = ms_step * 1000
     # algorithmic bytes per launch (each input read once, each output written once):
     #  SOR solve     13 B per fluid cell per iteration (q read, rhs, stencil byte, q write)
     #  P2G           25 B per particle in + 8 B per face accumulator
     #  G2P+advect    52 B per particle + 8 B per face (u and uO)
-    #  faces pass 1  8 B acc + 9 B out per face; forces 12 B per face; project 8 B per face
+    #  faces pass 1  8 B acc + 9 B out per face; forces 12 B per face; project 8 B per face;
+    #                extrapolation 5 B per face (flag + value), all over the active bricks' faces
     # the path the timed solve took (its own diagnostics, read after it ran)
     sor_name = SOR_KERNELS.get(fs.scalars.sorPath, "k_sor_tb")
     cand = {sor_name: (us_sor, 13.0 * nF * it),
             "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
             "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),
-            "k_faces_normalize_bc": (us_f1, 17.0 * F),
-            "k_faces_forces": (us_f2, 12.0 * F),
-            "k_project": (us_pr, 8.0 * F)}
+            "k_faces_bricks<normalize_bc>": (us_f1, 17.0 * Fa),
+            "k_faces_bricks<forces>": (us_f2, 12.0 * Fa),
+            "k_faces_bricks<project>": (us_pr, 8.0 * Fa),
+            "k_faces_bricks<extrapolate>": (us_ex, 5.0 * Fa)}
     name = max(cand, key=lambda k: cand[k][0])
     us, nbytes = cand[name]
     achieved = nbytes / (us * 1e-6) / 1e9

@@ -53,6 +53,7 @@ constexpr int kTbThreads = 1024;
 constexpr int kRbMax = 256;                 // region bricks per CTA
 constexpr int kEMax = 4096;                 // update entries (d <= 3) per CTA
 constexpr int kLMax = 4096;                 // halo reload cells (1 <= d <= 4) per CTA
+constexpr int kOMax = 2048;                 // owned interior fluid cells per CTA
 constexpr int kHashSlots = 1024;            // open-addressing table of region bricks
 constexpr int kZero = kRbMax * 64;          // dense index of the always-zero cell
 constexpr long long kTbSpinLimit = 4000000LL;
@@ -99,6 +100,7 @@ struct TbSmem {
   int hkey[kHashSlots];
   short hval[kHashSlots];
   int rbLin[kRbMax];
+  short rbX[kRbMax], rbY[kRbMax], rbZ[kRbMax];   // brick coordinates of each slot
   short rbOwn[kRbMax];
   short rbNb[kRbMax][6];
   unsigned short eSelf[kEMax];
@@ -106,6 +108,7 @@ struct TbSmem {
   float eRhs[kEMax], ePw[kEMax];
   unsigned short lDense[kLMax];
   unsigned lGlob[kLMax];
+  unsigned oGlob[kOMax];                  // global index of each owned entry (buckets 0 and 4, in order)
   unsigned short deps[kMaxCtas];
   unsigned depMask[kMaxCtas / 32];
 };
@@ -180,23 +183,25 @@ __device__ __forceinline__ int dense_nb(const TbSmem& S, int x, int dir) {
 __device__ __forceinline__ bool dense_global(const TbArgs& a, const TbSmem& S, int x, unsigned& g, int& i, int& j,
                                              int& k) {
   const int s = x >> 6, c = x & 63;
-  const int lin = S.rbLin[s];
-  const int bx = lin % a.nbx, t = lin / a.nbx, by = t % a.nby, bz = t / a.nby;
-  i = bx * 4 + (c & 3); j = by * 4 + ((c >> 2) & 3); k = bz * 4 + (c >> 4);
+  i = S.rbX[s] * 4 + (c & 3); j = S.rbY[s] * 4 + ((c >> 2) & 3); k = S.rbZ[s] * 4 + (c >> 4);
   if (i >= a.d.nx || j >= a.d.ny || k >= a.d.nz) return false;
   g = ((unsigned)k * (unsigned)a.d.ny + (unsigned)j) * (unsigned)a.d.nx + (unsigned)i;
   return true;
 }
 
 __device__ __forceinline__ bool hash_insert(TbSmem& S, int key, int* nRegion, int* sOverflow, int fixedSlot,
-                                            short owner) {
+                                            short owner, int nbx, int nby) {
   unsigned h = ((unsigned)key * 2654435761u) >> 22;          // 10 bits
   for (int probe = 0; probe < kHashSlots; probe++, h = (h + 1) & (kHashSlots - 1)) {
     int prev = atomicCAS(&S.hkey[h], -1, key);
     if (prev == -1) {
       int slot = fixedSlot >= 0 ? fixedSlot : atomicAdd(nRegion, 1);
       S.hval[h] = (short)(slot < kRbMax ? slot : -1);
-      if (slot < kRbMax) { S.rbLin[slot] = key; S.rbOwn[slot] = owner; }
+      if (slot < kRbMax) {
+        S.rbLin[slot] = key; S.rbOwn[slot] = owner;
+        const int t = key / nbx;
+        S.rbX[slot] = (short)(key - t * nbx); S.rbY[slot] = (short)(t % nby); S.rbZ[slot] = (short)(t / nby);
+      }
       else *sOverflow = 1;
       return true;
     }
@@ -321,7 +326,7 @@ extern __shared__ __align__(16) unsigned char tb_smem_raw[];
 // The whole solve in one cooperative launch of one 1024-thread CTA per SM.
 __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   TbSmem& S = *reinterpret_cast<TbSmem*>(tb_smem_raw);
-  __shared__ int sAbort, sOverflow, nRegion, nReload, nDeps, sT0, sT1, sA;
+  __shared__ int sAbort, sOverflow, nRegion, nReload, nDeps, nCand, sT0, sT1, sA;
   __shared__ int bucket[8], bstart[8], bcur[8];
   __shared__ int2 sScan[33];
   __shared__ double2 sRed[32];
@@ -332,7 +337,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   const Dims& d = a.d;
   int it = 0, O = 0, R = 0, path = 3;
   double rel = -1;
-  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; nDeps = 0; }
+  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; nDeps = 0; nCand = 0; }
   if (tid < 8) bucket[tid] = 0;
   __syncthreads();
 
@@ -458,20 +463,20 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
     const int t0 = sT0;
     O = sT1 - sT0;
     if (!sOverflow) {
-      for (int s = tid; s < O; s += T) hash_insert(S, __ldcg(&a.actLin[t0 + s]), &nRegion, &sOverflow, s, (short)p);
+      for (int s = tid; s < O; s += T)
+        hash_insert(S, __ldcg(&a.actLin[t0 + s]), &nRegion, &sOverflow, s, (short)p, a.nbx, a.nby);
       __syncthreads();
       // the active bricks among the owned bricks' 26 neighbours that other CTAs own
       for (int item = tid; item < O * 26; item += T) {
         const int s = item / 26, n27 = item % 26 < 13 ? item % 26 : item % 26 + 1;
-        const int lin = S.rbLin[s];
-        const int bx = lin % a.nbx, tq = lin / a.nbx, by = tq % a.nby, bz = tq / a.nby;
+        const int bx = S.rbX[s], by = S.rbY[s], bz = S.rbZ[s];
         const int nx_ = bx + n27 % 3 - 1, ny_ = by + (n27 / 3) % 3 - 1, nz_ = bz + n27 / 9 - 1;
         if (nx_ < 0 || ny_ < 0 || nz_ < 0 || nx_ >= a.nbx || ny_ >= a.nby || nz_ >= a.nbz) continue;
         const int lin2 = (nz_ * a.nby + ny_) * a.nbx + nx_;
         const int ord = __ldcg(&a.brickOrd[lin2]);
         if (ord < 0) continue;
         const int ow = owner_of(__ldcg(&a.actWPre[ord]), P, NF);
-        if (ow != p) hash_insert(S, lin2, &nRegion, &sOverflow, -1, (short)ow);
+        if (ow != p) hash_insert(S, lin2, &nRegion, &sOverflow, -1, (short)ow, a.nbx, a.nby);
       }
       __syncthreads();
       if (tid == 0 && nRegion > kRbMax) sOverflow = 1;
@@ -481,8 +486,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
     // face neighbours of each region brick (slot, or -1: outside the region)
     for (int item = tid; item < R * 6; item += T) {
       const int s = item / 6, dir = item % 6;
-      const int lin = S.rbLin[s];
-      int bx = lin % a.nbx, tq = lin / a.nbx, by = tq % a.nby, bz = tq / a.nby;
+      int bx = S.rbX[s], by = S.rbY[s], bz = S.rbZ[s];
       if (dir == 0) bx--; else if (dir == 1) bx++; else if (dir == 2) by--; else if (dir == 3) by++;
       else if (dir == 4) bz--; else bz++;
       int slot = -1;
@@ -491,21 +495,77 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       S.rbNb[s][dir] = (short)slot;
     }
     // dense q of the region and the cell states: 0 owned, 255 halo (distance
-    // still unknown), 254 constant (no interior fluid: never updated)
-    for (int x = tid; x < R * 64; x += T) {
-      unsigned g; int i, j, k;
-      float qv = 0.f; uint8_t st = 254;
-      if (dense_global(a, S, x, g, i, j, k)) {
-        qv = __ldcg(a.q + g);
-        if (__ldcg(a.pw + g) >= 0.f && interior(d, i, j, k)) st = (x >> 6) < O ? 0 : 255;
+    // still unknown), 254 constant (no interior fluid: never updated). One
+    // thread per 4-cell brick row (float4 loads when rows are 16-byte
+    // aligned), four rows in flight per thread; the halo cells of unknown
+    // distance are listed for the distance rounds (in the entry area, unused yet).
+    unsigned short* cand = reinterpret_cast<unsigned short*>(&S.eNb[0][0]);
+    constexpr int kCandMax = kEMax * 6;
+    {
+      const bool vec = (d.nx & 3) == 0;
+      const int nRows = R * 16;
+      for (int r0 = 0; r0 < nRows; r0 += 4 * T) {
+        float qv[4][4], pv[4][4];
+        int rowOk[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int row = r0 + u * T + tid;
+          rowOk[u] = 0;
+#pragma unroll
+          for (int c = 0; c < 4; c++) { qv[u][c] = 0.f; pv[u][c] = -1.f; }
+          if (row >= nRows) continue;
+          const int sl = row >> 4, rr = row & 15;
+          const int j = S.rbY[sl] * 4 + (rr & 3), k = S.rbZ[sl] * 4 + (rr >> 2), i0 = S.rbX[sl] * 4;
+          if (j >= d.ny || k >= d.nz) continue;
+          rowOk[u] = 1;
+          const long long g0 = ((long long)k * d.ny + j) * d.nx + i0;
+          if (vec) {
+            const float4 q4 = __ldcg(reinterpret_cast<const float4*>(a.q + g0));
+            const float4 p4 = __ldcg(reinterpret_cast<const float4*>(a.pw + g0));
+            qv[u][0] = q4.x; qv[u][1] = q4.y; qv[u][2] = q4.z; qv[u][3] = q4.w;
+            pv[u][0] = p4.x; pv[u][1] = p4.y; pv[u][2] = p4.z; pv[u][3] = p4.w;
+          } else {
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+              if (i0 + c < d.nx) { qv[u][c] = __ldcg(a.q + g0 + c); pv[u][c] = __ldcg(a.pw + g0 + c); }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int row = r0 + u * T + tid;
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            bool isCand = false;
+            if (row < nRows) {
+              const int sl = row >> 4, rr = row & 15, x = row * 4 + c;
+              const int i = S.rbX[sl] * 4 + c, j = S.rbY[sl] * 4 + (rr & 3), k = S.rbZ[sl] * 4 + (rr >> 2);
+              uint8_t st = 254;
+              if (rowOk[u] && i < d.nx && pv[u][c] >= 0.f && interior(d, i, j, k)) st = sl < O ? 0 : 255;
+              S.q[x] = rowOk[u] && i < d.nx ? qv[u][c] : 0.f;
+              S.dist[x] = st;
+              isCand = st == 255;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, isCand);
+            int base = 0;
+            if (lane == 0 && m) base = atomicAdd(&nCand, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (isCand) {
+              const int pos = base + __popc(m & ((1u << lane) - 1u));
+              if (pos < kCandMax) cand[pos] = (unsigned short)(row * 4 + c);
+            }
+          }
+        }
       }
-      S.q[x] = qv; S.dist[x] = st;
     }
     if (tid == 0) S.q[kZero] = 0.f;
     __syncthreads();
+    if (tid == 0 && nCand > kCandMax) sOverflow = 1;
+    __syncthreads();
+    const int nC = sOverflow ? 0 : nCand;
     // distances 1..4 through the interior fluid cells
     for (int r = 1; r <= 4; r++) {
-      for (int x = tid; x < R * 64; x += T) {
+      for (int l = tid; l < nC; l += T) {
+        const int x = cand[l];
         if (S.dist[x] != 255) continue;
 #pragma unroll
         for (int dir = 0; dir < 6; dir++) {
@@ -515,15 +575,18 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
       __syncthreads();
     }
-    // update entries: cells with d <= 3, bucketed by (colour, d)
+    // update entries: cells with d <= 3, bucketed by (colour, d), and the
+    // halo cells reloaded after every epoch (1 <= d <= 4)
     for (int pass = 0; pass < 2; pass++) {
       for (int x0 = 0; x0 < R * 64; x0 += T) {
         const int x = x0 + tid;
         int b = -1;
+        bool rl = false;
         unsigned g = 0; int i = 0, j = 0, k = 0;
-        if (x < R * 64 && S.dist[x] <= 3) {
+        if (x < R * 64 && S.dist[x] <= 4) {
           dense_global(a, S, x, g, i, j, k);
-          b = ((i + j + k) & 1) * 4 + S.dist[x];
+          if (S.dist[x] <= 3) b = ((i + j + k) & 1) * 4 + S.dist[x];
+          rl = S.dist[x] >= 1;
         }
         const unsigned grp = __match_any_sync(0xffffffffu, b);
         const int leader = __ffs(grp) - 1;
@@ -545,23 +608,19 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
               S.eNb[pos][2] = (unsigned)nb[4] | ((unsigned)nb[5] << 16);
               S.eRhs[pos] = __ldcg(a.rhs + g);
               S.ePw[pos] = __ldcg(a.pw + g);
+              if (b == 0 || b == 4) {
+                const int o = b == 0 ? pos - bstart[0] : bucket[0] + pos - bstart[4];
+                if (o < kOMax) S.oGlob[o] = g;
+              }
             }
           }
-        }
-        // halo cells reloaded after every epoch: 1 <= d <= 4
-        if (pass == 1) {
-          const bool rl = x < R * 64 && S.dist[x] >= 1 && S.dist[x] <= 4;
           const unsigned m = __ballot_sync(0xffffffffu, rl);
-          int base = 0;
-          if (lane == 0 && m) base = atomicAdd(&nReload, __popc(m));
-          base = __shfl_sync(0xffffffffu, base, 0);
+          int rbase = 0;
+          if (lane == 0 && m) rbase = atomicAdd(&nReload, __popc(m));
+          rbase = __shfl_sync(0xffffffffu, rbase, 0);
           if (rl) {
-            const int pos = base + __popc(m & ((1u << lane) - 1u));
-            if (pos < kLMax) {
-              if (b < 0) dense_global(a, S, x, g, i, j, k);
-              S.lDense[pos] = (unsigned short)x;
-              S.lGlob[pos] = g;
-            }
+            const int rpos = rbase + __popc(m & ((1u << lane) - 1u));
+            if (rpos < kLMax) { S.lDense[rpos] = (unsigned short)x; S.lGlob[rpos] = g; }
           }
         }
       }
@@ -569,7 +628,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       if (pass == 0 && tid == 0) {
         int acc = 0;
         for (int b = 0; b < 8; b++) { bstart[b] = acc; bcur[b] = acc; acc += bucket[b]; }
-        if (acc > kEMax) sOverflow = 1;
+        if (acc > kEMax || bucket[0] + bucket[4] > kOMax) sOverflow = 1;
       }
       __syncthreads();
     }
@@ -613,18 +672,21 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
       __syncthreads();
       if (sAbort) return false;
+      // four loads in flight per thread before their stores
       const float* src = (target & 1u) ? a.q1 : a.q;
-      for (int l = tid; l < nReload; l += T) S.q[S.lDense[l]] = __ldcg(src + S.lGlob[l]);
+      for (int l0 = tid; l0 < nReload; l0 += 4 * T) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) { const int l = l0 + u * T; v[u] = l < nReload ? __ldcg(src + S.lGlob[l]) : 0.f; }
+#pragma unroll
+        for (int u = 0; u < 4; u++) { const int l = l0 + u * T; if (l < nReload) S.q[S.lDense[l]] = v[u]; }
+      }
       __syncthreads();
       return true;
     };
     auto write_owned = [&](float* dst) {
-      for (int e = tid; e < nOwn0 + nOwn1; e += T) {
-        const int x = S.eSelf[e < nOwn0 ? st0 + e : st1 + (e - nOwn0)];
-        unsigned g; int i, j, k;
-        dense_global(a, S, x, g, i, j, k);
-        __stcg(dst + g, S.q[x]);
-      }
+      for (int e = tid; e < nOwn0 + nOwn1; e += T)
+        __stcg(dst + S.oGlob[e], S.q[S.eSelf[e < nOwn0 ? st0 + e : st1 + (e - nOwn0)]]);
     };
     auto check_residual = [&]() -> bool {
       const double2 part = owned_residual(a, S, O, sRed);
