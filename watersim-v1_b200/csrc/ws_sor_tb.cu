@@ -8,13 +8,13 @@
 //
 // Region. A CTA keeps in shared memory its owned bricks plus every active
 // brick among their 26 neighbours, densely (64 q values per brick). The
-// interior fluid cells of the region are labelled with their distance d
-// from the owned cells in the fluid adjacency graph (d = 0 owned, 1..4
-// halo). A red-black half-sweep only propagates information one cell, so
-// after loading exact values for d <= 4, the CTA can run four half-sweeps
-// (two iterations) on its own: half-sweep t updates the cells with
-// d <= 4 - t, and after the fourth the owned cells hold exactly the values
-// of the global sweep. Each cell's update reads the same six neighbours in
+// interior fluid cells of the region are labelled with d, their L1 distance
+// in cells to the boxes of the owned bricks (d = 0 owned). d changes by at
+// most one between neighbouring cells, and a red-black half-sweep only
+// propagates information one cell, so after loading exact values for d <= 4,
+// the CTA can run four half-sweeps (two iterations) on its own: half-sweep t
+// updates the cells with d <= 4 - t, and after the fourth the owned cells
+// hold exactly the values of the global sweep. Each cell's update reads the same six neighbours in
 // the same order with the same arithmetic as the reference's sweep, so the
 // iterates are bitwise those of the plain red-black solve.
 //
@@ -96,13 +96,14 @@ struct TbArgs {
 // shared-memory layout (dynamic)
 struct TbSmem {
   float q[kRbMax * 64 + 4];               // dense region q; [kZero] = 0
-  uint8_t dist[kRbMax * 64];              // 0..4 distance, 254 constant, 255 unreached
+  uint8_t dist[kRbMax * 64];              // 0..4 distance d, 5 farther, 254 constant
   int hkey[kHashSlots];
   short hval[kHashSlots];
   int rbLin[kRbMax];
   short rbX[kRbMax], rbY[kRbMax], rbZ[kRbMax];   // brick coordinates of each slot
   short rbOwn[kRbMax];
   short rbNb[kRbMax][6];
+  unsigned rbOwnMask[kRbMax];             // which of the 27 bricks around a slot (itself included) this CTA owns
   unsigned short eSelf[kEMax];
   unsigned eNb[kEMax][3];                 // six neighbour dense indices, two per word
   float eRhs[kEMax], ePw[kEMax];
@@ -126,6 +127,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
@@ -299,7 +301,7 @@ __device__ bool global_residual(const TbArgs& a, double2 part, int k, double* sR
   double2* buf = a.resPart + (size_t)(k & 1) * P;
   if (threadIdx.x == 0) {
     __stcg(&buf[blockIdx.x], part);
-    __threadfence();
+    fence_acq_rel_gpu();
     atomicAdd(&a.ctl->resCount, 1u);
     if (!bounded_wait_geq(&a.ctl->resCount, (unsigned)P * (unsigned)(k + 1), kTbSpinLimit, a.err)) *sAbort = 1;
   }
@@ -326,7 +328,7 @@ extern __shared__ __align__(16) unsigned char tb_smem_raw[];
 // The whole solve in one cooperative launch of one 1024-thread CTA per SM.
 __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   TbSmem& S = *reinterpret_cast<TbSmem*>(tb_smem_raw);
-  __shared__ int sAbort, sOverflow, nRegion, nReload, nDeps, nCand, sT0, sT1, sA;
+  __shared__ int sAbort, sOverflow, nRegion, nReload, nDeps, sT0, sT1, sA;
   __shared__ int bucket[8], bstart[8], bcur[8];
   __shared__ int2 sScan[33];
   __shared__ double2 sRed[32];
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   const Dims& d = a.d;
   int it = 0, O = 0, R = 0, path = 3;
   double rel = -1;
-  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; nDeps = 0; nCand = 0; }
+  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; nDeps = 0; }
   if (tid < 8) bucket[tid] = 0;
   __syncthreads();
 
@@ -483,7 +485,8 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       __syncthreads();
     }
     R = sOverflow ? 0 : nRegion;
-    // face neighbours of each region brick (slot, or -1: outside the region)
+    // face neighbours of each region brick (slot, or -1: outside the region),
+    // and which of its 27 surrounding bricks this CTA owns
     for (int item = tid; item < R * 6; item += T) {
       const int s = item / 6, dir = item % 6;
       int bx = S.rbX[s], by = S.rbY[s], bz = S.rbZ[s];
@@ -494,13 +497,20 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
         slot = hash_find(S, (bz * a.nby + by) * a.nbx + bx);
       S.rbNb[s][dir] = (short)slot;
     }
-    // dense q of the region and the cell states: 0 owned, 255 halo (distance
-    // still unknown), 254 constant (no interior fluid: never updated). One
-    // thread per 4-cell brick row (float4 loads when rows are 16-byte
-    // aligned), four rows in flight per thread; the halo cells of unknown
-    // distance are listed for the distance rounds (in the entry area, unused yet).
-    unsigned short* cand = reinterpret_cast<unsigned short*>(&S.eNb[0][0]);
-    constexpr int kCandMax = kEMax * 6;
+    for (int s = tid; s < R; s += T) S.rbOwnMask[s] = 0;
+    __syncthreads();
+    for (int item = tid; item < (R - O) * 27; item += T) {
+      const int s = O + item / 27, n27 = item % 27;
+      const int bx = S.rbX[s] + n27 % 3 - 1, by = S.rbY[s] + (n27 / 3) % 3 - 1, bz = S.rbZ[s] + n27 / 9 - 1;
+      if (bx < 0 || by < 0 || bz < 0 || bx >= a.nbx || by >= a.nby || bz >= a.nbz) continue;
+      const int slot = hash_find(S, (bz * a.nby + by) * a.nbx + bx);
+      if (slot >= 0 && slot < O) atomicOr(&S.rbOwnMask[s], 1u << n27);
+    }
+    __syncthreads();
+    // dense q of the region and the cell states: 0..4 the distance d of an
+    // interior fluid cell (5: farther), 254 constant (no interior fluid:
+    // never updated). One thread per 4-cell brick row (float4 loads when rows
+    // are 16-byte aligned), four rows in flight per thread.
     {
       const bool vec = (d.nx & 3) == 0;
       const int nRows = R * 16;
@@ -533,48 +543,36 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const int row = r0 + u * T + tid;
+          if (row >= nRows) continue;
+          const int sl = row >> 4, rr = row & 15, cy = rr & 3, cz = rr >> 2;
+          const unsigned mask = sl < O ? 0u : S.rbOwnMask[sl];
 #pragma unroll
           for (int c = 0; c < 4; c++) {
-            bool isCand = false;
-            if (row < nRows) {
-              const int sl = row >> 4, rr = row & 15, x = row * 4 + c;
-              const int i = S.rbX[sl] * 4 + c, j = S.rbY[sl] * 4 + (rr & 3), k = S.rbZ[sl] * 4 + (rr >> 2);
-              uint8_t st = 254;
-              if (rowOk[u] && i < d.nx && pv[u][c] >= 0.f && interior(d, i, j, k)) st = sl < O ? 0 : 255;
-              S.q[x] = rowOk[u] && i < d.nx ? qv[u][c] : 0.f;
-              S.dist[x] = st;
-              isCand = st == 255;
+            const int x = row * 4 + c;
+            const int i = S.rbX[sl] * 4 + c, j = S.rbY[sl] * 4 + cy, k = S.rbZ[sl] * 4 + cz;
+            uint8_t st = 254;
+            if (rowOk[u] && i < d.nx && pv[u][c] >= 0.f && interior(d, i, j, k)) {
+              if (sl < O) st = 0;
+              else {
+                // L1 distance to the nearest owned brick box among the 26 around this one
+                int best = 5;
+                for (unsigned m = mask; m; m &= m - 1) {
+                  const int n27 = __ffs(m) - 1, ox = n27 % 3 - 1, oy = (n27 / 3) % 3 - 1, oz = n27 / 9 - 1;
+                  const int dd = (ox < 0 ? c + 1 : ox > 0 ? 4 - c : 0) + (oy < 0 ? cy + 1 : oy > 0 ? 4 - cy : 0) +
+                                 (oz < 0 ? cz + 1 : oz > 0 ? 4 - cz : 0);
+                  best = dd < best ? dd : best;
+                }
+                st = (uint8_t)best;
+              }
             }
-            const unsigned m = __ballot_sync(0xffffffffu, isCand);
-            int base = 0;
-            if (lane == 0 && m) base = atomicAdd(&nCand, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (isCand) {
-              const int pos = base + __popc(m & ((1u << lane) - 1u));
-              if (pos < kCandMax) cand[pos] = (unsigned short)(row * 4 + c);
-            }
+            S.q[x] = rowOk[u] && i < d.nx ? qv[u][c] : 0.f;
+            S.dist[x] = st;
           }
         }
       }
     }
     if (tid == 0) S.q[kZero] = 0.f;
     __syncthreads();
-    if (tid == 0 && nCand > kCandMax) sOverflow = 1;
-    __syncthreads();
-    const int nC = sOverflow ? 0 : nCand;
-    // distances 1..4 through the interior fluid cells
-    for (int r = 1; r <= 4; r++) {
-      for (int l = tid; l < nC; l += T) {
-        const int x = cand[l];
-        if (S.dist[x] != 255) continue;
-#pragma unroll
-        for (int dir = 0; dir < 6; dir++) {
-          const int y = dense_nb(S, x, dir);
-          if (y != kZero && S.dist[y] == r - 1) { S.dist[x] = (uint8_t)r; break; }
-        }
-      }
-      __syncthreads();
-    }
     // update entries: cells with d <= 3, bucketed by (colour, d), and the
     // halo cells reloaded after every epoch (1 <= d <= 4)
     for (int pass = 0; pass < 2; pass++) {
@@ -702,15 +700,30 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       for (int t = 1; t <= s; t++) {
         const int col = (t - 1) & 1, dmax = s - t;
         const int n = cum[col][dmax], base = col ? st1 : st0;
-        for (int e = tid; e < n; e += T) {
-          const int idx = base + e;
-          const unsigned w0 = S.eNb[idx][0], w1 = S.eNb[idx][1], w2 = S.eNb[idx][2];
+        // two updates per thread in flight where a thread has two entries
+        // (e and e + T are of one colour, so neither reads what the other
+        // writes); a thread with one entry reads nothing extra
+        for (int e = tid; e < n; e += 2 * T) {
+          const int i1 = base + e, e2 = e + T;
+          const unsigned a0 = S.eNb[i1][0], a1 = S.eNb[i1][1], a2 = S.eNb[i1][2];
           float v[6];
-          v[0] = S.q[w0 & 0xffffu]; v[1] = S.q[w0 >> 16];
-          v[2] = S.q[w1 & 0xffffu]; v[3] = S.q[w1 >> 16];
-          v[4] = S.q[w2 & 0xffffu]; v[5] = S.q[w2 >> 16];
-          const int x = S.eSelf[idx];
-          S.q[x] = relax(S.q[x], S.ePw[idx], S.eRhs[idx], v, om1);
+          v[0] = S.q[a0 & 0xffffu]; v[1] = S.q[a0 >> 16]; v[2] = S.q[a1 & 0xffffu];
+          v[3] = S.q[a1 >> 16]; v[4] = S.q[a2 & 0xffffu]; v[5] = S.q[a2 >> 16];
+          const int x1 = S.eSelf[i1];
+          if (e2 < n) {
+            const int i2 = base + e2;
+            const unsigned b0 = S.eNb[i2][0], b1 = S.eNb[i2][1], b2 = S.eNb[i2][2];
+            float u[6];
+            u[0] = S.q[b0 & 0xffffu]; u[1] = S.q[b0 >> 16]; u[2] = S.q[b1 & 0xffffu];
+            u[3] = S.q[b1 >> 16]; u[4] = S.q[b2 & 0xffffu]; u[5] = S.q[b2 >> 16];
+            const int x2 = S.eSelf[i2];
+            const float q1 = relax(S.q[x1], S.ePw[i1], S.eRhs[i1], v, om1);
+            const float q2 = relax(S.q[x2], S.ePw[i2], S.eRhs[i2], u, om1);
+            S.q[x1] = q1;
+            S.q[x2] = q2;
+          } else {
+            S.q[x1] = relax(S.q[x1], S.ePw[i1], S.eRhs[i1], v, om1);
+          }
         }
         __syncthreads();
       }
@@ -718,7 +731,9 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       epoch++;
       write_owned((epoch & 1u) ? a.q1 : a.q);
       __syncthreads();
-      if (tid == 0) { __threadfence(); st_release(&a.ctl->flag[p], epoch); }
+      // the CTA barrier orders every thread's stores before thread 0; its
+      // release fence at GPU scope carries them to the waiting neighbours
+      if (tid == 0) { fence_acq_rel_gpu(); st_release(&a.ctl->flag[p], epoch); }
       fresh = false;
       checked = false;
       const bool doCheck = a.check > 0 && it % a.check == 0;
