@@ -297,7 +297,16 @@ def workload_config(nP, world):
     n = W["n"]
     return {"workload": "%s: %d^3 MAC grid, R=%g, depth %g, %d particles" % (W["name"], n, W["R"], W["depth"], nP),
             "particles": nP, "parallelism": "replicas x%d" % world,
-            "l2": "state (~%d MB) larger than L2 (126 MB)" % state_mb(n, nP)}
+            "l2": ("state (~%d MB) larger than L2 (126 MB)" if not state_fits_l2(n, nP)
+                   else "state (~%d MB) fits in L2 (126 MB): a 256 MB buffer is written between timed steps")
+                  % state_mb(n, nP)}
+
+
+L2_BYTES = 126 * 1000 * 1000
+
+
+def state_fits_l2(n, nP):
+    return state_mb(n, nP) * 1e6 < L2_BYTES
 
 
 def state_mb(n, nP):
@@ -729,7 +738,14 @@ def run_frames(args, rank, world, local_rank):
     clocks.start()
     time.sleep(0.5)
     ms, subs, evap = [], 0, []
+    # a state that fits in L2 is evicted between timed frames by writing a
+    # buffer twice the L2 size on the solver's stream, outside the events
+    flush = (torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+             if state_fits_l2(WORKLOAD["n"], fs.scalars.nP) else None)
     for _ in range(args.steps):
+        if flush is not None:
+            with torch.cuda.stream(st):
+                flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(st)
