@@ -410,7 +410,11 @@ def roofline(fs, ms_step, iters):
     us_pr = fs.time_kernel(10, 5)
     us_ex = fs.time_kernel(11, 5)
     Fa = 192.0 * active_bricks(fs)
-    us_p2g = fs.time_kernel(1, 5)
+    # P2G as the substep runs it: the cell sort (count, prefix sum, scatter of
+    # particle ids) and the per-cell sums (id 12, every brick visited); the
+    # index-order scatter with one atomic per particle and face (id 1) beside it
+    us_p2g = fs.time_kernel(12, 5)
+    us_p2g_index = fs.time_kernel(1, 5)
     us_g2p = fs.time_kernel(2, 5)
     step_us = ms_step * 1000
     # algorithmic bytes per launch (each input read once, each output written once):
@@ -422,7 +426,7 @@ def roofline(fs, ms_step, iters):
     # the path the timed solve took (its own diagnostics, read after it ran)
     sor_name = SOR_KERNELS.get(fs.scalars.sorPath, "k_sor_tb")
     cand = {sor_name: (us_sor, 13.0 * nF * it),
-            "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
+            "p2g_sorted": (us_p2g, 25.0 * nP + 8.0 * F),
             "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),
             "k_faces_bricks<normalize_bc>": (us_f1, 17.0 * Fa),
             "k_faces_bricks<forces>": (us_f2, 12.0 * Fa),
@@ -432,18 +436,20 @@ def roofline(fs, ms_step, iters):
     us, nbytes = cand[name]
     achieved = nbytes / (us * 1e-6) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of each kernel
-    # on this 128^3 planet (bench.py --profile 3): the SOR
-    # solve's lists are staged into shared memory once, so its traffic is a
-    # small fraction of its algorithmic bytes
-    captured = {"k_sor_cluster": 4428544.0, "k_p2g": 53253120.0, "k_g2p_advect": 66053376.0}
-    traffic = captured.get(name) if WORKLOAD["name"] == "planet128" else None
+    # on this 128^3 planet: the temporal-blocked solve loads its system into
+    # shared memory once and iterates from there (halo exchanges hit L2), so
+    # its traffic hardly depends on the iteration count
+    captured = {"k_sor_tb": (16125696.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 150-iteration "
+                                         "solve of this planet (bench.py --profile 4 --learned-profile); the "
+                                         "system is read once, the iterations run from shared memory and L2"),
+                "k_g2p_advect": (66053376.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture at 128^3")}
+    traffic, note = captured.get(name, (None, None)) if WORKLOAD["name"] == "planet128" else (None, None)
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": kind, "traffic": traffic,
-            "traffic_note": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture at 128^3; the timed "
-                             "solve also includes the list build") if traffic else None,
+            "frac": achieved / peak, "peak_source": kind, "traffic": traffic, "traffic_note": note,
             "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": us / step_us,
             "others": {k: {"us_per_launch": v[0], "time_share": v[0] / step_us,
-                           "GB_s": v[1] / (v[0] * 1e-6) / 1e9} for k, v in cand.items()}}
+                           "GB_s": v[1] / (v[0] * 1e-6) / 1e9} for k, v in cand.items()},
+            "p2g_index_order_us": us_p2g_index}
 
 
 def surface_timing(fs, cpu=True):

@@ -74,7 +74,12 @@ typedef struct {
  *                checked every sorCheckEvery iterations, at most sorMaxIters;
  *                sorTol <= 0 runs pressureIters iterations like the reference;
  *   viscJacobi / extrapJacobi must be 1 (the device order of the two
- *                in-place passes of the reference). */
+ *                in-place passes of the reference);
+ *   p2gCellOrder 1 scatters P2G over the particles sorted by cell (a
+ *                counting sort by cell each substep, then one block per
+ *                4^3 brick summing in shared memory and one atomic per
+ *                touched face); 0 (default) in particle index order with
+ *                one atomic per particle and face, faster on B200. */
 typedef struct {
   int32_t substeps;
   int32_t pressureIters;
@@ -93,6 +98,7 @@ typedef struct {
   int32_t sorMaxIters;
   int32_t viscJacobi;
   int32_t extrapJacobi;
+  int32_t p2gCellOrder;
 } ws_params;
 
 /* Scalar state and counters of FluidSolver (js/solver.js:81-214, RNG states
@@ -363,13 +369,17 @@ ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz);
  * stream with CUDA events and returns the mean duration of one launch in
  * microseconds. Runs on the current state (timing only; the state advances
  * as if the kernels ran). kernel: 0 one red-black SOR iteration (two
- * launches, reported per launch), 1 P2G scatter, 2 fused G2P + advection,
+ * launches, reported per launch), 1 P2G scatter in particle index order (one
+ * atomic per particle and face; the substep uses 12), 2 fused G2P + advection,
  * 3 faces pass 1 (normalise + BC + snapshot), 4 forces pass, 5 projection,
  * 6 one whole SOR solve of pressureIters iterations on the default path
  * (reported per solve), 7 the same solve on the colour-list path (cluster-
  * resident or grid-wide, whichever the lists fit; list build included),
  * 8..11 passes 3, 4, 5 and the extrapolation over the active-brick list of
- * the last substep, as a substep runs them. */
+ * the last substep, as a substep runs them, 12 P2G in cell order from scratch
+ * (count per cell, prefix sum, particle ids scattered into cell order, per-
+ * cell sums with one atomic per touched face; every brick visited), reported
+ * per whole P2G. */
 ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us_per_launch);
 ws_status ws_synchronize(ws_handle* h);
 /* Failure-detection check (no counterpart in the reference, whose solver

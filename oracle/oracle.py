@@ -35,6 +35,7 @@ class OrParams(C.Structure):
         ("sorRedBlack", C.c_int32), ("sorCheckEvery", C.c_int32),
         ("sorTol", C.c_double), ("sorMaxIters", C.c_int32),
         ("viscJacobi", C.c_int32), ("extrapJacobi", C.c_int32),
+        ("p2gCellOrder", C.c_int32),
     ]
 
 

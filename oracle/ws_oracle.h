@@ -50,6 +50,7 @@ typedef struct {
   int32_t sorMaxIters;          /* cap in tolerance mode */
   int32_t viscJacobi;           /* 0 = in-place (reference), 1 = Jacobi */
   int32_t extrapJacobi;         /* 0 = in-place (reference), 1 = Jacobi */
+  int32_t p2gCellOrder;         /* accepted, no effect: the oracle's P2G is one serial sum */
 } or_params;
 
 typedef struct {

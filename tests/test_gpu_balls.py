@@ -69,8 +69,12 @@ def compare_balls(o, fs, pos_tol, vel_tol):
     assert np.max(np.abs(a[:, 8] - b[:, 8])) <= 1e-4
 
 
-def test_balls_one_substep():
+@pytest.mark.parametrize("cell_order", [0, 1])
+def test_balls_one_substep(cell_order):
+    """cell_order 1 also covers the cell-ordered P2G's direct path for the
+    particles a ball pushed out of the cell they were binned in."""
     o, fs = with_balls()
+    fs.set_params(p2gCellOrder=cell_order)
     o.substep(0.01)
     fs._substep(0.01)
     assert np.array_equal(fs.cellType, o.cellType)

@@ -37,10 +37,14 @@ def _compare_state(o, fs, label):
         assert e <= TOL, "%s %s rel err %.3g" % (label, k, e)
 
 
-def test_substep_parity_planet32():
+@pytest.mark.parametrize("cell_order", [0, 1])
+def test_substep_parity_planet32(cell_order):
+    """cell_order 1: P2G over the particles sorted by cell (counting sort,
+    shared-memory sums per brick) instead of particle index order."""
     o = planet("planet32", **PLAIN32)
     o.set_scalars(gRamp=1.5)
     fs = to_device(o)
+    fs.set_params(p2gCellOrder=cell_order)
     # rasterise: cell types bit-exact before any float work
     fs.stage("CLEAR_RASTER")
     fs.stage("MARK_FLUID")
@@ -50,6 +54,7 @@ def test_substep_parity_planet32():
     o2 = planet("planet32", **PLAIN32)
     o2.set_scalars(gRamp=1.5)
     fs2 = to_device(o2)
+    fs2.set_params(p2gCellOrder=cell_order)
     o2.substep(0.01)
     fs2._substep(0.01)
     assert np.array_equal(fs2.cellType, o2.cellType)
@@ -64,11 +69,13 @@ def test_substep_parity_planet32():
     assert fs2.scalars.airborneCount == o2.scalars.airborneCount
 
 
-def test_stagewise_planet32():
+@pytest.mark.parametrize("cell_order", [0, 1])
+def test_stagewise_planet32(cell_order):
     """Each stage from identical inputs: isolates which kernel drifts."""
     o = planet("planet32", **PLAIN32)
     o.set_scalars(gRamp=1.5)
     fs = to_device(o)
+    fs.set_params(p2gCellOrder=cell_order)
     dt = 0.01
     o.stage("clear_faces"); o.stage("rasterize_static"); o.stage("mark_fluid")
     fs.stage("CLEAR_RASTER"); fs.stage("MARK_FLUID")
@@ -89,11 +96,13 @@ def test_stagewise_planet32():
     assert rel_err(fs.rhs, o.rhs) <= 1e-6
 
 
-def test_multi_substep_planet32():
+@pytest.mark.parametrize("cell_order", [0, 1])
+def test_multi_substep_planet32(cell_order):
     """Ten substeps: errors stay at the FP32 rounding level."""
     o = planet("planet32", **PLAIN32)
     o.set_scalars(gRamp=1.5)
     fs = to_device(o)
+    fs.set_params(p2gCellOrder=cell_order)
     for _ in range(10):
         o.substep(0.01)
         fs._substep(0.01)

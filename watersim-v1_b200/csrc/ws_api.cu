@@ -67,6 +67,9 @@ struct ws_handle {
   int* brickIota = nullptr;             // 0 .. nB - 1, the input of the list compaction
   void* brickCub = nullptr;             // compaction scratch
   size_t brickCubBytes = 0;
+  CellSort csort{};                     // the particles sorted by cell for P2G
+  void* csortCub = nullptr;             // prefix-sum scratch
+  size_t csortCubBytes = 0;
   bool tbSetup = false;                 // the pressure setup may run over bricks (the solve needs no block counts)
   // substep graph: the kernel sequence of one substep captured once and
   // replayed while its launch parameters stay the same
@@ -149,6 +152,11 @@ static GridDev grid_of(ws_handle* h) {
 // the next substep processes every brick (after a caller or a single stage wrote grid fields)
 static void force_full_pass(ws_handle* h) {
   if (h->bricks.forceAll) cudaMemsetAsync(h->bricks.forceAll, 1, sizeof(int), h->stream);
+  // the cell counts start from zero again (an interrupted substep may have left some)
+  if (h->csort.count) {
+    const size_t nKeys = 64 * (size_t)h->bricks.nbx * h->bricks.nby * h->bricks.nbz;
+    cudaMemsetAsync(h->csort.count, 0, sizeof(int) * (nKeys + 1), h->stream);
+  }
 }
 static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; return P; }
 
@@ -173,7 +181,7 @@ extern "C" ws_status ws_default_params(ws_params* p) {
   p->meltT = 0.10 * 1.05; p->spinOn = 0; p->thermalOn = 1;
   // device order of the order-dependent passes
   p->sorRedBlack = 1; p->sorCheckEvery = 10; p->sorTol = 0; p->sorMaxIters = 10000;
-  p->viscJacobi = 1; p->extrapJacobi = 1;
+  p->viscJacobi = 1; p->extrapJacobi = 1; p->p2gCellOrder = 0;
   return WS_OK;
 }
 
@@ -190,7 +198,8 @@ static void free_all(ws_handle* h) {
   if (h->queryBuf) cudaFree(h->queryBuf);
   {
     void* bb[] = { h->bricks.seed, h->bricks.act, h->bricks.proc, h->bricks.list, h->bricks.count, h->bricks.forceAll,
-                   h->brickIota, h->brickCub };
+                   h->brickIota, h->brickCub, h->csort.count, h->csort.start, h->csort.pcell, h->csort.pslot,
+                   h->csort.perm, h->csortCub };
     for (void* b : bb) if (b) cudaFree(b);
   }
   if (h->sor) sor_free(h->sor);
@@ -286,6 +295,11 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
     AL(B.seed, nB) AL(B.act, nB) AL(B.proc, nB) AL(B.list, nB) AL(B.count, 1) AL(B.forceAll, 1) AL(h->brickIota, nB)
     h->brickCubBytes = brick_list_scratch_bytes((int)nB);
     if ((e = cudaMalloc(&h->brickCub, h->brickCubBytes)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
+    CellSort& cs = h->csort;
+    AL(cs.count, 64 * nB + 1) AL(cs.start, 64 * nB + 1) AL(cs.pcell, P) AL(cs.pslot, P) AL(cs.perm, P)
+    cs.cap = (int)P;
+    h->csortCubBytes = cell_sort_scratch_bytes(64 * nB);
+    if ((e = cudaMalloc(&h->csortCub, h->csortCubBytes)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
     std::vector<int> iota((size_t)nB);
     for (long long b = 0; b < nB; b++) iota[(size_t)b] = (int)b;
     const int one = 1;
@@ -756,8 +770,11 @@ static ws_status stage_clear_raster(ws_handle* h, bool bricks = false) {
   if (bricks) launch_clear_acc_bricks(h->d, grid_of(h), h->bricks, h->stream);
   return check_launch(h, bricks ? 3 : 1);
 }
+// bricks: the substep's own pipeline, where (with p2gCellOrder) the mark
+// pass also counts the particles per cell for the cell-ordered P2G
 static ws_status stage_mark(ws_handle* h, bool bricks = false) {
-  launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR, h->st, h->stream);
+  launch_mark_fluid(h->d, grid_of(h), parts_of(h), h->terr, h->S.oceanR, h->S.coreR,
+                    bricks && h->P.p2gCellOrder ? &h->csort : nullptr, h->st, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
   if (bricks) {
     cudaError_t e = launch_brick_activity(h->bricks, h->brickIota, h->brickCub, h->brickCubBytes, h->stream);
@@ -766,11 +783,21 @@ static ws_status stage_mark(ws_handle* h, bool bricks = false) {
   }
   return WS_OK;
 }
+// P2G in particle index order, or (p2gCellOrder) in cell order: with bricks
+// the mark pass counted and the brick list is current; the stage-wise call
+// counts here and visits every brick
 static ws_status stage_p2g(ws_handle* h, bool bricks = false) {
-  launch_p2g(h->d, grid_of(h), parts_of(h), h->st, h->stream);
+  int n = 1;
+  if (h->P.p2gCellOrder) {
+    n = launch_p2g_sorted(h->d, grid_of(h), parts_of(h), h->csort, h->bricks, bricks, h->csortCub, h->csortCubBytes,
+                          h->st, h->stream);
+    if (n < 0) return fail_cuda(h, cudaGetLastError(), "cell sort");
+  } else {
+    launch_p2g(h->d, grid_of(h), parts_of(h), h->st, h->stream);
+  }
   if (bricks) launch_faces_normalize_bc_bricks(h->d, grid_of(h), h->bricks, h->stream);
   else launch_faces_normalize_bc(h->d, grid_of(h), h->stream);
-  return check_launch(h, 2);
+  return check_launch(h, n + 1);
 }
 // planet gravity ramp, js/solver.js:2656-2662: the applied scale of this
 // substep (0 = no gravity), advancing the ramp timer
@@ -1469,6 +1496,10 @@ extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, 
       case 9: launch_faces_forces_bricks(h->d, g, h->bricks, 5e-6, 1, 0.01, 9.81, h->stream); break;
       case 10: launch_project_bricks(h->d, g, h->bricks, 1, h->P.maxSpeed, h->st, h->stream); break;
       case 11: launch_extrapolate_bricks(h->d, g, h->bricks, h->stream); break;
+      case 12: { const int n12 = launch_p2g_sorted(h->d, g, parts_of(h), h->csort, h->bricks, false, h->csortCub,
+                                                   h->csortCubBytes, h->st, h->stream);
+                 if (n12 < 0) { cudaEventDestroy(e0); cudaEventDestroy(e1); return fail_cuda(h, cudaGetLastError(), "cell sort"); }
+                 h->launches += n12 - 1; } break;
       case 7: { int* di; double* dr; int* dp;
                 cudaError_t e7 = launch_sor_solve_lists(h->sor, h->d, g, h->diag8, h->P.omega, h->P.pressureIters, 0, 0,
                                                         &h->st->err, &di, &dr, &dp, h->stream);

@@ -135,35 +135,69 @@ __device__ __forceinline__ long long mark_cell(const Dims& d, const GridDev& g, 
   }
   return ((long long)k * d.ny + j) * d.nx + i;
 }
+// Warp-aggregated increment of count[key] for every lane with key >= 0: the
+// lanes holding one key share a single atomic; each gets its own rank. All
+// 32 lanes of the warp call it (lanes without work pass -1).
+__device__ __forceinline__ int warp_rank_inc(int* count, int key) {
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader && key >= 0) base = atomicAdd(&count[key], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+// the sort key of cell (i, j, k): its 4^3 brick times 64 plus its place in the brick
+__device__ __forceinline__ int brick_key(const GridDev& g, int i, int j, int k) {
+  return ((((k >> 2) * g.nby + (j >> 2)) * g.nbx + (i >> 2)) << 6) | ((k & 3) << 4) | ((j & 3) << 2) | (i & 3);
+}
 // Two particles per thread: both particles' loads, then both cells' type
-// loads, then the (idempotent) stores, so the two chains overlap.
-__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR, int* err) {
+// loads, then the (idempotent) stores, so the two chains overlap. With a
+// cell sort (cs.count set) every particle that P2G will scatter (marked, with
+// a finite velocity) is also counted in its cell, and its rank recorded.
+__global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR, double coreR, CellSort cs,
+                             int* err) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
-  if (p0 >= P.nP) return;
-  const bool has1 = p1 < P.nP;
-  const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
-  const double X0 = P.px[p0], Y0 = P.py[p0], Z0 = P.pz[p0];
-  const double X1 = has1 ? P.px[p1] : 0.0, Y1 = has1 ? P.py[p1] : 0.0, Z1 = has1 ? P.pz[p1] : 0.0;
-  // the first pass of a substep to read the positions: every particle must
-  // be finite and inside the domain box (the reference's passes keep it there)
-  particle_sound(d, X0, Y0, Z0, 0.0, 0.0, 0.0, err, true);
-  if (has1) particle_sound(d, X1, Y1, Z1, 0.0, 0.0, 0.0, err, true);
-  // the brick of every particle's cell seeds this substep's active bricks
-  seed_cell(g, jfloor_clamp(over_dx(d, X0), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y0), 0, d.ny - 1),
-            jfloor_clamp(over_dx(d, Z0), 0, d.nz - 1));
-  if (has1)
-    seed_cell(g, jfloor_clamp(over_dx(d, X1), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y1), 0, d.ny - 1),
-              jfloor_clamp(over_dx(d, Z1), 0, d.nz - 1));
-  const long long c0 = mark_cell(d, g, P, t, oceanR, coreR, p0, fl0, X0, Y0, Z0);
-  const long long c1 = mark_cell(d, g, P, t, oceanR, coreR, p1, fl1, X1, Y1, Z1);
-  const uint8_t t0 = c0 >= 0 ? g.type[c0] : (uint8_t)WS_SOLID, t1 = c1 >= 0 ? g.type[c1] : (uint8_t)WS_SOLID;
-  if (t0 == WS_AIR) g.type[c0] = WS_FLUID;
-  if (t1 == WS_AIR) g.type[c1] = WS_FLUID;
+  const bool has0 = p0 < P.nP, has1 = p1 < P.nP;
+  long long c0 = -1, c1 = -1;
+  bool fin0 = false, fin1 = false;
+  if (has0) {
+    const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
+    const double X0 = P.px[p0], Y0 = P.py[p0], Z0 = P.pz[p0];
+    const double X1 = has1 ? P.px[p1] : 0.0, Y1 = has1 ? P.py[p1] : 0.0, Z1 = has1 ? P.pz[p1] : 0.0;
+    if (cs.count) {
+      fin0 = isfinite(P.pvx[p0]) && isfinite(P.pvy[p0]) && isfinite(P.pvz[p0]);
+      fin1 = has1 && isfinite(P.pvx[p1]) && isfinite(P.pvy[p1]) && isfinite(P.pvz[p1]);
+    }
+    // the first pass of a substep to read the positions: every particle must
+    // be finite and inside the domain box (the reference's passes keep it there)
+    particle_sound(d, X0, Y0, Z0, 0.0, 0.0, 0.0, err, true);
+    if (has1) particle_sound(d, X1, Y1, Z1, 0.0, 0.0, 0.0, err, true);
+    // the brick of every particle's cell seeds this substep's active bricks
+    seed_cell(g, jfloor_clamp(over_dx(d, X0), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y0), 0, d.ny - 1),
+              jfloor_clamp(over_dx(d, Z0), 0, d.nz - 1));
+    if (has1)
+      seed_cell(g, jfloor_clamp(over_dx(d, X1), 0, d.nx - 1), jfloor_clamp(over_dx(d, Y1), 0, d.ny - 1),
+                jfloor_clamp(over_dx(d, Z1), 0, d.nz - 1));
+    c0 = mark_cell(d, g, P, t, oceanR, coreR, p0, fl0, X0, Y0, Z0);
+    c1 = mark_cell(d, g, P, t, oceanR, coreR, p1, fl1, X1, Y1, Z1);
+    const uint8_t t0 = c0 >= 0 ? g.type[c0] : (uint8_t)WS_SOLID, t1 = c1 >= 0 ? g.type[c1] : (uint8_t)WS_SOLID;
+    if (t0 == WS_AIR) g.type[c0] = WS_FLUID;
+    if (t1 == WS_AIR) g.type[c1] = WS_FLUID;
+  }
+  if (!cs.count) return;                                // uniform over the launch
+  // a marked particle with a non-finite velocity stays off the grid and is latched
+  if ((c0 >= 0 && !fin0) || (c1 >= 0 && !fin1)) atomicOr(err, WS_DERR_NAN);
+  auto key_of = [&](long long c) { int i, j, k; cell_ijk(d, c, i, j, k); return brick_key(g, i, j, k); };
+  const int k0 = c0 >= 0 && fin0 ? key_of(c0) : -1, k1 = c1 >= 0 && fin1 ? key_of(c1) : -1;
+  const int r0 = warp_rank_inc(cs.count, k0), r1 = warp_rank_inc(cs.count, k1);
+  if (has0) { cs.pcell[p0] = k0; cs.pslot[p0] = r0; }
+  if (has1) { cs.pcell[p1] = k1; cs.pslot[p1] = r1; }
 }
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
-                       double oceanR, double coreR, DevStatus* st, cudaStream_t s) {
+                       double oceanR, double coreR, const CellSort* cs, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, &st->err);
+  CellSort none{};
+  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, cs ? *cs : none, &st->err);
 }
 
 // ------------------------------------------------------------ 3. P2G scatter
@@ -237,6 +271,159 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, i
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
   k_p2g<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, &st->err);
+}
+
+// ------------------------------------------------------------ 3b. P2G in cell order
+// The same scatter (_p2gInto, js/solver.js:1035-1105) over the particles
+// sorted by cell, brick-major: the key of cell (i, j, k) is its 4^3 brick
+// times 64 plus its place in the brick, so a brick's particles are one range
+// of the permutation. One block per brick adds every particle's eight FP32
+// (momentum, weight) terms per component into a shared-memory copy of the
+// faces the brick's particles can reach (red.shared.add.f32), then sends one
+// float2 atomic per touched face. Every FP32 term is the one k_p2g adds;
+// only the order of the FP32 sums differs. A particle whose stencil leaves
+// the brick's faces (a ball pushed it after the binning) adds its terms to
+// global memory directly.
+static unsigned brick_grid(const BrickSet& B);
+
+// The stage-wise P2G, without a mark pass that counted: the particles P2G
+// scatters (pflag 0, finite state) counted per cell, each with its rank.
+__global__ void k_bin_cells(Dims d, GridDev g, PartsDev P, CellSort cs, int* err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int key = -1;
+  if (p < P.nP && P.pflag[p] == 0) {
+    const double x = P.px[p], y = P.py[p], z = P.pz[p];
+    if (particle_sound(d, x, y, z, P.pvx[p], P.pvy[p], P.pvz[p], err, false))
+      key = brick_key(g, jfloor_clamp(over_dx(d, x), 0, d.nx - 1), jfloor_clamp(over_dx(d, y), 0, d.ny - 1),
+                      jfloor_clamp(over_dx(d, z), 0, d.nz - 1));
+  }
+  const int r = warp_rank_inc(cs.count, key);          // every lane of the warp takes part
+  if (p < P.nP) { cs.pcell[p] = key; cs.pslot[p] = r; }
+}
+// particle ids into their cells' ranges
+__global__ void k_cell_scatter(int nP, CellSort cs, int* err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nP) return;
+  const int c = cs.pcell[p];
+  if (c < 0) return;
+  const int at = cs.start[c] + cs.pslot[p];
+  if (at >= 0 && at < cs.cap) cs.perm[at] = p;
+  else atomicOr(err, WS_DERR_RANGE);
+}
+
+// Shared-memory faces of one brick: per component the faces of the brick's
+// cells widened by one along the two tangential axes (5 x 6 x 6 = 180), the
+// component's own axis keeping its upper face. Momentum sums first, then
+// the weights.
+constexpr int kBrickFaces = 180;
+// origin offset of component comp's face box from the brick's first cell, and its x and y extents
+__device__ __forceinline__ void brick_face_box(int comp, int& oi, int& oj, int& ok, int& ex, int& ey) {
+  oi = comp == 0 ? 0 : -1; oj = comp == 1 ? 0 : -1; ok = comp == 2 ? 0 : -1;
+  ex = comp == 0 ? 5 : 6; ey = comp == 1 ? 5 : 6;
+}
+// one particle's eight terms of component comp: into the brick's faces when
+// the whole stencil lies inside them, else straight to global memory
+__device__ __forceinline__ void p2g_brick_comp(const Dims& d, float2* __restrict__ acc, float* sm, int comp,
+                                               int fx, int fy, int fz, double x, double y, double z, double vel) {
+  int i0, j0, k0; double tx, ty, tz;
+  face_coords(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
+  const double s0 = 1 - tx, s1 = tx, t0 = 1 - ty, t1 = ty, r0 = 1 - tz, r1 = tz;
+  const double wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
+  const double w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
+  int oi, oj, ok, ex, ey;
+  brick_face_box(comp, oi, oj, ok, ex, ey);
+  const int ez = comp == 2 ? 5 : 6;
+  const int li = i0 - (fx + oi), lj = j0 - (fy + oj), lk = k0 - (fz + ok);
+  if ((unsigned)li < (unsigned)(ex - 1) && (unsigned)lj < (unsigned)(ey - 1) && (unsigned)lk < (unsigned)(ez - 1)) {
+    float* m = sm + comp * kBrickFaces;
+    float* w = m + 3 * kBrickFaces;
+    const int o = (lk * ey + lj) * ex + li, sj = ex, sk = ex * ey;
+    const int o8[8] = { o, o + 1, o + sj, o + sj + 1, o + sk, o + sk + 1, o + sk + sj, o + sk + sj + 1 };
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      atomicAdd(&m[o8[q]], (float)(w8[q] * vel));
+      atomicAdd(&w[o8[q]], (float)w8[q]);
+    }
+  } else {
+    long long idx, sj, sk;
+    face_strides(d, comp, i0, j0, k0, idx, sj, sk);
+    const long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj,
+                              idx + sk + sj + 1 };
+#pragma unroll
+    for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2((float)(w8[q] * vel), (float)w8[q]));
+  }
+}
+// One block per brick (the brick list, or every brick when allBricks). The
+// brick's particle range is cut into 32 lane chunks, so the 32 lanes of a
+// warp work on particles about a 32nd of the range apart, mostly in
+// different cells, and their shared-memory adds rarely meet on one address.
+__global__ void __launch_bounds__(256) k_p2g_bricks(Dims d, GridDev g, PartsDev P, CellSort cs, BrickSet B,
+                                                    int allBricks, int* err) {
+  __shared__ float sm[6 * kBrickFaces];
+  const int nB = allBricks ? B.nbx * B.nby * B.nbz : *B.count;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int e = blockIdx.x; e < nB; e += gridDim.x) {
+    const int b = allBricks ? e : B.list[e];
+    const int s0 = cs.start[b << 6], n = cs.start[(b << 6) + 64] - s0;
+    if (n <= 0) continue;                              // uniform over the block
+    if (threadIdx.x < 64) cs.count[(b << 6) + threadIdx.x] = 0;   // zero again for the next binning
+    if (s0 < 0 || s0 + n > cs.cap) { if (threadIdx.x == 0) atomicOr(err, WS_DERR_RANGE); continue; }
+    const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
+    const int fx = bx * 4, fy = by * 4, fz = bz * 4;
+    for (int t = threadIdx.x; t < 6 * kBrickFaces; t += blockDim.x) sm[t] = 0.f;
+    __syncthreads();
+    const int L = (n + 31) >> 5;                       // lane chunk
+    for (int a = warp; a < L; a += 8) {
+      const int at = lane * L + a;
+      if (at >= n) continue;
+      const int p = cs.perm[s0 + at];
+      const double x = P.px[p], y = P.py[p], z = P.pz[p];
+      const double u = P.pvx[p], v = P.pvy[p], w = P.pvz[p];
+      p2g_brick_comp(d, g.acc, sm, 0, fx, fy, fz, x, y, z, u);
+      p2g_brick_comp(d, g.acc, sm, 1, fx, fy, fz, x, y, z, v);
+      p2g_brick_comp(d, g.acc, sm, 2, fx, fy, fz, x, y, z, w);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 3 * kBrickFaces; t += blockDim.x) {
+      const float m = sm[t], wt = sm[t + 3 * kBrickFaces];
+      if (wt == 0.f && m == 0.f) continue;            // a face no stencil reached
+      const int comp = t / kBrickFaces, f = t - comp * kBrickFaces;
+      int oi, oj, ok, ex, ey;
+      brick_face_box(comp, oi, oj, ok, ex, ey);
+      const int li = f % ex, lj = (f / ex) % ey, lk = f / (ex * ey);
+      long long idx, sj, sk;
+      face_strides(d, comp, fx + oi + li, fy + oj + lj, fz + ok + lk, idx, sj, sk);
+      atomicAdd(&g.acc[idx], make_float2(m, wt));
+    }
+    __syncthreads();                                   // sm is cleared for the next brick
+  }
+}
+size_t cell_sort_scratch_bytes(long long nKeys) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int*)nullptr, (int*)nullptr, (int)(nKeys + 1));
+  return bytes;
+}
+// P2G in cell order. binned: the mark pass of this substep counted the
+// particles (k_mark_fluid with the cell sort) and the brick list is current;
+// otherwise the particles are counted here and every brick is visited.
+// Returns the number of kernel launches made (-1 on a launch error).
+int launch_p2g_sorted(const Dims& d, const GridDev& g, const PartsDev& P, const CellSort& cs, const BrickSet& B,
+                      bool binned, void* scratch, size_t scratchBytes, DevStatus* st, cudaStream_t s) {
+  if (P.nP <= 0) return 0;
+  const long long nKeys = 64LL * B.nbx * B.nby * B.nbz;
+  int launches = 0;
+  if (!binned) {
+    if (cudaMemsetAsync(cs.count, 0, sizeof(int) * (size_t)(nKeys + 1), s) != cudaSuccess) return -1;
+    k_bin_cells<<<grid_for(P.nP, 256), 256, 0, s>>>(d, g, P, cs, &st->err);
+    launches++;
+  }
+  // prefix sum over the keys (CUB's device scan, a CUDA toolkit library)
+  if (cub::DeviceScan::ExclusiveSum(scratch, scratchBytes, cs.count, cs.start, (int)(nKeys + 1), s) != cudaSuccess)
+    return -1;
+  launches += 2;
+  k_cell_scatter<<<grid_for(P.nP, 256), 256, 0, s>>>(P.nP, cs, &st->err);
+  k_p2g_bricks<<<brick_grid(B), 256, 0, s>>>(d, g, P, cs, B, binned ? 0 : 1, &st->err);
+  return launches + 2;
 }
 
 // Solid-adjacent interior face: the velocity of the solid cell beside it,

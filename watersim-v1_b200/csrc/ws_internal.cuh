@@ -152,6 +152,19 @@ struct BrickSet {
   int* count;
   int* forceAll;            // device flag: process every brick once
 };
+// Counting sort of the grid-coupled particles by cell, rebuilt every
+// substep: P2G then walks each cell's particles in a row. The particle
+// arrays themselves stay in index order (the serial random streams of the
+// later passes consume them in that order); only the permutation is sorted.
+struct CellSort {
+  int* count;       // particles per cell key (64 per 4^3 brick, + 1); all zero outside a bin..P2G window
+  int* start;       // exclusive prefix sum of count
+  int* pcell;       // per particle: the key of the cell it was binned in, or -1
+  int* pslot;       // per particle: its rank among that cell's particles
+  int* perm;        // particle ids in cell order
+  int cap;          // entries of pcell, pslot and perm (the particle capacity)
+};
+
 // the seed brick of cell (i, j, k)
 __device__ __forceinline__ void seed_cell(const GridDev& g, int i, int j, int k) {
   if (g.seed) g.seed[((k >> 2) * g.nby + (j >> 2)) * g.nbx + (i >> 2)] = 1;

@@ -37,9 +37,13 @@ void launch_project_bricks(const Dims& d, const GridDev& g, const BrickSet& B, i
 void launch_extrapolate_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
 void launch_pressure_setup_bricks(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st,
                                   const BrickSet& B, cudaStream_t s);
+// cs: count every particle P2G will scatter in its cell (null: mark only)
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
-                       double oceanR, double coreR, DevStatus* st, cudaStream_t s);
+                       double oceanR, double coreR, const CellSort* cs, DevStatus* st, cudaStream_t s);
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s);
+size_t cell_sort_scratch_bytes(long long nKeys);
+int launch_p2g_sorted(const Dims& d, const GridDev& g, const PartsDev& P, const CellSort& cs, const BrickSet& B,
+                      bool binned, void* scratch, size_t scratchBytes, DevStatus* st, cudaStream_t s);
 void launch_faces_normalize_bc(const Dims& d, const GridDev& g, cudaStream_t s);
 void launch_faces_forces(const Dims& d, const GridDev& g, double coef, int viscOn, double dt, double gs, cudaStream_t s);
 void launch_pressure_setup(const Dims& d, const GridDev& g, uint8_t* diag8, double omega, DevStatus* st, int* sorCounts,
