@@ -410,11 +410,12 @@ def roofline(fs, ms_step, iters):
     us_pr = fs.time_kernel(10, 5)
     us_ex = fs.time_kernel(11, 5)
     Fa = 192.0 * active_bricks(fs)
-    # P2G as the substep runs it: the cell sort (count, prefix sum, scatter of
-    # particle ids) and the per-cell sums (id 12, every brick visited); the
-    # index-order scatter with one atomic per particle and face (id 1) beside it
-    us_p2g = fs.time_kernel(12, 5)
-    us_p2g_index = fs.time_kernel(1, 5)
+    # P2G as the substep runs it by default: particle index order, one atomic
+    # per particle and face (id 1); the cell-ordered variant (id 12: counting
+    # sort, prefix sum, scatter of particle ids, shared-memory sums per brick,
+    # every brick visited) beside it
+    us_p2g = fs.time_kernel(1, 5)
+    us_p2g_cell = fs.time_kernel(12, 5)
     us_g2p = fs.time_kernel(2, 5)
     step_us = ms_step * 1000
     # algorithmic bytes per launch (each input read once, each output written once):
@@ -426,7 +427,7 @@ def roofline(fs, ms_step, iters):
     # the path the timed solve took (its own diagnostics, read after it ran)
     sor_name = SOR_KERNELS.get(fs.scalars.sorPath, "k_sor_tb")
     cand = {sor_name: (us_sor, 13.0 * nF * it),
-            "p2g_sorted": (us_p2g, 25.0 * nP + 8.0 * F),
+            "k_p2g": (us_p2g, 25.0 * nP + 8.0 * F),
             "k_g2p_advect": (us_g2p, 52.0 * nP + 8.0 * F),
             "k_faces_bricks<normalize_bc>": (us_f1, 17.0 * Fa),
             "k_faces_bricks<forces>": (us_f2, 12.0 * Fa),
@@ -449,7 +450,7 @@ def roofline(fs, ms_step, iters):
             "bytes_per_launch": nbytes, "us_per_launch": us, "time_share": us / step_us,
             "others": {k: {"us_per_launch": v[0], "time_share": v[0] / step_us,
                            "GB_s": v[1] / (v[0] * 1e-6) / 1e9} for k, v in cand.items()},
-            "p2g_index_order_us": us_p2g_index}
+            "p2g_cell_order_us": us_p2g_cell}
 
 
 def surface_timing(fs, cpu=True):
