@@ -45,9 +45,12 @@ for p in (ROOT, PKG):
         sys.path.insert(0, p)
 
 WORKLOADS = {
-    "planet128": dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000),
-    # the large planet: 256^3, radius 110, ocean 12 deep, ~16M particles
-    "planet256": dict(name="planet256", n=256, R=110.0, depth=12.0, seed=20260114, particles=16000000),
+    "planet128": dict(name="planet128", n=128, R=52.0, depth=8.0, seed=20260114, particles=2000000,
+                      levels=3, pairs=2000),
+    # the large planet: 256^3, radius 110, ocean 12 deep, ~16M particles; its
+    # warm start is the 4-level U-Net (16/32/64/128) trained on 1000 pairs
+    "planet256": dict(name="planet256", n=256, R=110.0, depth=12.0, seed=20260114, particles=16000000,
+                      levels=4, pairs=1000),
     # the 64^3 planet with the thermal cycle on: radius 26, ocean 5 deep, 220k particles; whole
     # 60 Hz frames (two substeps each, SOR to 1e-5, vorticity 0.05) make one bench step
     "planet64": dict(name="planet64", n=64, R=26.0, depth=5.0, seed=20260114, particles=220000),
@@ -318,7 +321,7 @@ def learned_arm(fs, one_step, args, world=1):
     """Record (input, converged q) pairs from the plain solves, train the
     U-Net on them, and measure what its prediction leaves for SOR on fresh
     pressure systems. Leaves the warm start enabled."""
-    fs.unet_init(7)
+    fs.unet_init(7, WORKLOAD.get("levels", 3))
     fs.unet_collect(args.pairs)
     t0 = time.perf_counter()
     for _ in range(args.pairs):
@@ -359,7 +362,9 @@ def learned_arm(fs, one_step, args, world=1):
     fs.sorCheckEvery = keep[0]
     fs.unet_enable(True)
     n = len(rows)
-    return {"pairs": args.pairs, "collect_s": collect_s, "train_steps": args.train_steps + 10, "batch": 4 * world,
+    info = fs.unet_info()
+    return {"levels": WORKLOAD.get("levels", 3), "pairs": info["pairs_stored"], "pairs_requested": args.pairs,
+            "collect_s": collect_s, "train_steps": args.train_steps + 10, "batch": 4 * world,
             "training": "data-parallel over %d ranks (gradients all-reduced)" % world if world > 1 else "one GPU",
             "lr": 1e-3, "train_s": train_s, "loss_first": loss0, "loss_last": loss1,
             "train_ms_per_sample": fs.unet_time(1, 3),
@@ -806,7 +811,7 @@ def run_profile(args, local_rank):
     if WORKLOAD["name"] == "planet64":
         thermal_on(fs)
     if args.learned_profile:
-        fs.unet_init(7)
+        fs.unet_init(7, WORKLOAD.get("levels", 3))
         fs.unet_collect(2)
         fs._substep(DT)
         fs._substep(DT)
@@ -869,8 +874,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="plain SOR arm only")
-    ap.add_argument("--pairs", type=int, default=2000, help="training pairs recorded from plain solves")
+    ap.add_argument("--pairs", type=int, default=None,
+                    help="training pairs recorded from plain solves (default: 2000 at 128^3, 1000 at 256^3)")
     ap.add_argument("--train-steps", type=int, default=1000, help="Adam steps of batch 4")
+    ap.add_argument("--levels", type=int, default=None, choices=[3, 4],
+                    help="U-Net depth (default: 3 at 128^3, 4 at 256^3)")
     ap.add_argument("--workload", default="planet128", choices=sorted(WORKLOADS),
                     help="planet64 runs whole thermal-cycle frames; planet256 the plain and learned arms at 256^3")
     ap.add_argument("--frames", action="store_true", help="whole frames with the thermal cycle on (any workload)")
@@ -879,12 +887,19 @@ def main():
     ap.add_argument("--render", action="store_true", help="time ws_render_particles alone and exit")
     ap.add_argument("--render-mix", action="store_true", help="--render with all six flag classes")
     args = ap.parse_args()
-    global WORKLOAD, METRIC_PLAIN
+    global WORKLOAD, METRIC, METRIC_PLAIN
     WORKLOAD = WORKLOADS[args.workload]
-    if args.workload != "planet128":
+    if args.pairs is None:
+        args.pairs = WORKLOAD.get("pairs", 2000)
+    if args.levels is not None:
+        WORKLOAD = dict(WORKLOAD, levels=args.levels)
+    if args.workload == "planet64":
         args.no_learned = True
+    if args.workload != "planet128":
         METRIC_PLAIN = ("substeps/s @%d^3/%dM particles (plain red-black SOR to 1e-5 relative divergence residual)"
                         % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000))
+        METRIC = ("substeps/s @%d^3/%dM particles: learned warm-start (%d-level U-Net) vs plain SOR at equal "
+                  "\u2016\u2207\u00b7u\u2016" % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000, WORKLOAD["levels"]))
     frames = args.frames or args.workload == "planet64"
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

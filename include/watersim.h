@@ -435,10 +435,18 @@ typedef struct {
   int32_t enabled, collecting;
 } ws_unet_info;
 /* allocate the network on first use and (re)initialise its weights (He
- * normal from seed, zero biases) and Adam state */
+ * normal from seed, zero biases) and Adam state; 3 levels (16/32/64) */
 ws_status ws_unet_init(ws_handle* h, uint32_t seed);
-/* capacity > 0: record one pair per solve into a ring of that many pairs
- * (about 9 bytes per cell each); 0: stop recording (pairs are kept) */
+/* the same with 3 or 4 levels (4: 16/32/64/128 channels, bottleneck at an
+ * eighth of the grid); a depth different from the current network's
+ * replaces it (its stored pairs included) */
+ws_status ws_unet_init_levels(ws_handle* h, uint32_t seed, int32_t levels);
+/* capacity > 0: record one pair per solve into a ring of that many pairs;
+ * 0: stop recording (pairs are kept). A pair keeps the active 8x16x8
+ * level-0 tiles only (9 bytes per voxel of those tiles): every tile fits
+ * when the grid has at most 2048 tiles, else a slot holds 1.5x the active
+ * tiles of the cell types at the first call, and a solve with more active
+ * tiles than that is not recorded. */
 ws_status ws_unet_collect(ws_handle* h, int32_t capacity);
 /* on != 0: every solve starts from the network's prediction */
 ws_status ws_unet_enable(ws_handle* h, int32_t on);

@@ -18,54 +18,66 @@ def lib():
             raise OSError("liboracle_unet.so not built; run make -C oracle")
         L = C.CDLL(path)
         vp, i32 = C.c_void_p, C.c_int32
-        L.un_num_params.restype = C.c_int64
-        L.un_num_params.argtypes = []
-        L.un_forward.restype = None
-        L.un_forward.argtypes = [i32, i32, i32, vp, vp, vp, i32, vp]
-        L.un_loss_grad.restype = C.c_double
-        L.un_loss_grad.argtypes = [i32, i32, i32, vp, vp, vp, vp, i32, vp]
+        L.un_num_params_levels.restype = C.c_int64
+        L.un_num_params_levels.argtypes = [i32]
+        L.un_forward_levels.restype = None
+        L.un_forward_levels.argtypes = [i32, i32, i32, i32, vp, vp, vp, i32, vp]
+        L.un_loss_grad_levels.restype = C.c_double
+        L.un_loss_grad_levels.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, i32, vp]
         _L = L
     return _L
 
 
-def num_params():
-    return int(lib().un_num_params())
+def num_params(levels=3):
+    return int(lib().un_num_params_levels(levels))
 
 
-def forward(dims, params, r0n, types, rounding=True):
+def forward(dims, params, r0n, types, rounding=True, levels=3):
     nx, ny, nz = dims
     params = np.ascontiguousarray(params, np.float32)
     r0n = np.ascontiguousarray(r0n, np.float32)
     types = np.ascontiguousarray(types, np.uint8)
     out = np.zeros(nx * ny * nz, np.float32)
-    lib().un_forward(nx, ny, nz, params.ctypes.data, r0n.ctypes.data, types.ctypes.data, 1 if rounding else 0,
-                     out.ctypes.data)
+    lib().un_forward_levels(nx, ny, nz, levels, params.ctypes.data, r0n.ctypes.data, types.ctypes.data,
+                            1 if rounding else 0, out.ctypes.data)
     return out
 
 
-def loss_grad(dims, params, r0n, types, target, rounding=True):
+def loss_grad(dims, params, r0n, types, target, rounding=True, levels=3):
     """(loss, grads) of one sample; target already divided by the gain."""
     nx, ny, nz = dims
     params = np.ascontiguousarray(params, np.float32)
     r0n = np.ascontiguousarray(r0n, np.float32)
     types = np.ascontiguousarray(types, np.uint8)
     target = np.ascontiguousarray(target, np.float32)
-    g = np.zeros(num_params(), np.float64)
-    loss = lib().un_loss_grad(nx, ny, nz, params.ctypes.data, r0n.ctypes.data, types.ctypes.data,
-                              target.ctypes.data, 1 if rounding else 0, g.ctypes.data)
+    g = np.zeros(num_params(levels), np.float64)
+    loss = lib().un_loss_grad_levels(nx, ny, nz, levels, params.ctypes.data, r0n.ctypes.data, types.ctypes.data,
+                                     target.ctypes.data, 1 if rounding else 0, g.ctypes.data)
     return loss, g
 
 
-# layer table of the network: name, level, upsampled input channels, skip/plain input channels, outputs
-LAYERS = [("e0a", 0, 0, 16, 16), ("e0b", 0, 0, 16, 16), ("e1a", 1, 0, 16, 32), ("e1b", 1, 0, 32, 32),
-          ("ba", 2, 0, 32, 64), ("bb", 2, 0, 64, 64), ("d1a", 1, 64, 32, 32), ("d1b", 1, 0, 32, 32),
-          ("d0a", 0, 32, 16, 16), ("d0b", 0, 0, 16, 16)]
+def layers(levels=3):
+    """Layer table (forward order): name, level, upsampled input channels,
+    skip/plain input channels, outputs."""
+    out = []
+    for l in range(levels - 1):
+        c = 16 << l
+        out += [("e%da" % l, l, 0, 16 if l == 0 else c // 2, c), ("e%db" % l, l, 0, c, c)]
+    cb = 16 << (levels - 1)
+    out += [("ba", levels - 1, 0, cb // 2, cb), ("bb", levels - 1, 0, cb, cb)]
+    for l in range(levels - 2, -1, -1):
+        c = 16 << l
+        out += [("d%da" % l, l, 2 * c, c, c), ("d%db" % l, l, 0, c, c)]
+    return out
 
 
-def slices():
+LAYERS = layers(3)
+
+
+def slices(levels=3):
     """name -> (weight slice, bias slice) in the flat parameter vector, plus 'head'."""
     out, n = {}, 0
-    for name, _lv, c0, c1, cout in LAYERS:
+    for name, _lv, c0, c1, cout in layers(levels):
         nw = 27 * (c0 + c1) * cout
         out[name] = (slice(n, n + nw), slice(n + nw, n + nw + cout))
         n += nw + cout

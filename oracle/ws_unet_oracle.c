@@ -16,8 +16,10 @@
  *  - conv3(x)[co] = relu(sum_t sum_ci x(v + off_t)[ci] W[co][ci][t] + b[co]),
  *    t = (dz * 3 + dy) * 3 + dx with offsets (dz-1, dy-1, dx-1);
  *  - pool = mean of the 8 children; up = nearest (the parent's value);
- *  - network: e0a, e0b | pool | e1a, e1b | pool | ba, bb | up, concat s1 |
- *    d1a, d1b | up, concat s0 | d0a, d0b | head out = wh . h + bh;
+ *  - network (3 levels): e0a, e0b | pool | e1a, e1b | pool | ba, bb | up,
+ *    concat s1 | d1a, d1b | up, concat s0 | d0a, d0b | head out = wh . h + bh;
+ *    with 4 levels e2a, e2b | pool sit before the bottleneck (now 64 -> 128
+ *    channels) and d2a, d2b (up, concat s2) after it; channels 16 << level;
  *  - loss = sum over fluid cells (out - t)^2 / nFluid.
  * round = 1 applies the GPU's BF16 rounding (round to nearest even) at the
  * same points: weights, input, every stored activation and every stored
@@ -32,14 +34,43 @@
 #define TX 8
 #define TY 16
 #define TZ 8
-#define NLAYERS 10
+#define MAXLEV 4
+#define MAXLAYERS (4 * (MAXLEV - 1) + 2)
 
 typedef struct { const char* name; int level, c0, c1, cout; } layer_t;
-static const layer_t LAYERS[NLAYERS] = {
-  {"e0a", 0, 0, 16, 16}, {"e0b", 0, 0, 16, 16}, {"e1a", 1, 0, 16, 32}, {"e1b", 1, 0, 32, 32},
-  {"ba", 2, 0, 32, 64},  {"bb", 2, 0, 64, 64},  {"d1a", 1, 64, 32, 32}, {"d1b", 1, 0, 32, 32},
-  {"d0a", 0, 32, 16, 16}, {"d0b", 0, 0, 16, 16},
-};
+/* the layers of the network in use (forward order): per level l below the
+ * bottleneck e<l>a, e<l>b; the bottleneck ba, bb; per level l from the
+ * bottleneck down d<l>a (upsampled input | skip), d<l>b */
+static layer_t LAYERS[MAXLAYERS];
+static int g_levels = 0, NLAYERS = 0;
+static void set_levels(int levels) {
+  static const char* encA[] = { "e0a", "e1a", "e2a" };
+  static const char* encB[] = { "e0b", "e1b", "e2b" };
+  static const char* decA[] = { "d0a", "d1a", "d2a" };
+  static const char* decB[] = { "d0b", "d1b", "d2b" };
+  int n = 0;
+  for (int l = 0; l + 1 < levels; l++) {
+    int c = 16 << l, cin = l == 0 ? 16 : 16 << (l - 1);
+    layer_t a = { encA[l], l, 0, cin, c }, b = { encB[l], l, 0, c, c };
+    LAYERS[n++] = a; LAYERS[n++] = b;
+  }
+  int cb = 16 << (levels - 1);
+  layer_t ba = { "ba", levels - 1, 0, cb / 2, cb }, bb = { "bb", levels - 1, 0, cb, cb };
+  LAYERS[n++] = ba; LAYERS[n++] = bb;
+  for (int l = levels - 2; l >= 0; l--) {
+    int c = 16 << l;
+    layer_t a = { decA[l], l, 2 * c, c, c }, b = { decB[l], l, 0, c, c };
+    LAYERS[n++] = a; LAYERS[n++] = b;
+  }
+  g_levels = levels; NLAYERS = n;
+}
+static int enc_a(int l) { return 2 * l; }
+static int enc_b(int l) { return 2 * l + 1; }
+static int bot_a(void) { return 2 * (g_levels - 1); }
+static int bot_b(void) { return 2 * (g_levels - 1) + 1; }
+static int dec_a(int l) { return 2 * (g_levels - 1) + 2 + 2 * (g_levels - 2 - l); }
+static int dec_b(int l) { return dec_a(l) + 1; }
+static int chan(int l) { return 16 << l; }
 
 typedef struct { int nx, ny, nz, ntx, nty, ntz; long nv; uint8_t* act; } lev_t;
 
@@ -56,7 +87,7 @@ static double rb(double x) {
   return (double)f;
 }
 
-static long woff_of[NLAYERS], boff_of[NLAYERS], head_off, nparams_total;
+static long woff_of[MAXLAYERS], boff_of[MAXLAYERS], head_off, nparams_total;
 static void layout(void) {
   long n = 0;
   for (int l = 0; l < NLAYERS; l++) {
@@ -66,7 +97,8 @@ static void layout(void) {
   head_off = n; n += 17;
   nparams_total = n;
 }
-int64_t un_num_params(void) { layout(); return nparams_total; }
+int64_t un_num_params_levels(int levels) { set_levels(levels); layout(); return nparams_total; }
+int64_t un_num_params(void) { return un_num_params_levels(3); }
 
 static int active(const lev_t* L, int x, int y, int z) {
   if (x < 0 || y < 0 || z < 0 || x >= L->nx || y >= L->ny || z >= L->nz) return 0;
@@ -195,15 +227,15 @@ static void pool_bwd_add(const lev_t* F, const lev_t* C, const double* dskip, co
 }
 
 typedef struct {
-  lev_t L[3];
-  double *x, *e0a, *s0, *p1, *e1a, *s1, *p2, *ba, *bb, *d1a, *d1b, *d0a, *h;
+  lev_t L[MAXLEV];
+  double *x, *ea[MAXLEV], *sk[MAXLEV], *pl[MAXLEV], *bA, *bB, *da[MAXLEV], *db[MAXLEV];
   double* W;      /* rounded weights (biases and head unrounded) */
   double* out;
   int nFluid;
 } net_t;
 
 static void build_levels(net_t* N, int nx, int ny, int nz, const uint8_t* types) {
-  for (int l = 0; l < 3; l++) {
+  for (int l = 0; l < g_levels; l++) {
     lev_t* L = &N->L[l];
     L->nx = nx; L->ny = ny; L->nz = nz;
     L->ntx = (nx + TX - 1) / TX; L->nty = (ny + TY - 1) / TY; L->ntz = (nz + TZ - 1) / TZ;
@@ -215,7 +247,7 @@ static void build_levels(net_t* N, int nx, int ny, int nz, const uint8_t* types)
   N->nFluid = 0;
   for (int z = 0; z < L0->nz; z++) for (int y = 0; y < L0->ny; y++) for (int x = 0; x < L0->nx; x++)
     if (types[vidx(L0, x, y, z)] == 1) { L0->act[((z / TZ) * L0->nty + y / TY) * L0->ntx + x / TX] = 1; N->nFluid++; }
-  for (int l = 1; l < 3; l++) {
+  for (int l = 1; l < g_levels; l++) {
     lev_t *L = &N->L[l], *F = &N->L[l - 1];
     for (int tz = 0; tz < L->ntz; tz++) for (int ty = 0; ty < L->nty; ty++) for (int tx = 0; tx < L->ntx; tx++) {
       int a = 0;
@@ -230,7 +262,8 @@ static void build_levels(net_t* N, int nx, int ny, int nz, const uint8_t* types)
 static double* zalloc(long n) { return (double*)calloc((size_t)n, sizeof(double)); }
 
 static void net_forward(net_t* N, const float* params, const float* r0n, const uint8_t* types) {
-  lev_t *L0 = &N->L[0], *L1 = &N->L[1], *L2 = &N->L[2];
+  lev_t* L0 = &N->L[0];
+  const int LB = g_levels - 1;
   layout();
   N->W = zalloc(nparams_total);
   for (long i = 0; i < nparams_total; i++) N->W[i] = params[i];
@@ -246,97 +279,126 @@ static void net_forward(net_t* N, const float* params, const float* r0n, const u
     N->x[v * 16 + 1] = types[v] == 1; N->x[v * 16 + 2] = types[v] == 2; N->x[v * 16 + 3] = types[v] == 0;
   }
 #define WL(l) (N->W + woff_of[l]), (N->W + boff_of[l])
-  N->e0a = zalloc(L0->nv * 16); conv_fwd(L0, L1, 0, WL(0), NULL, N->x, N->e0a);
-  N->s0 = zalloc(L0->nv * 16); conv_fwd(L0, L1, 1, WL(1), NULL, N->e0a, N->s0);
-  N->p1 = zalloc(L1->nv * 16); pool_fwd(L0, L1, N->s0, N->p1, 16);
-  N->e1a = zalloc(L1->nv * 32); conv_fwd(L1, L2, 2, WL(2), NULL, N->p1, N->e1a);
-  N->s1 = zalloc(L1->nv * 32); conv_fwd(L1, L2, 3, WL(3), NULL, N->e1a, N->s1);
-  N->p2 = zalloc(L2->nv * 32); pool_fwd(L1, L2, N->s1, N->p2, 32);
-  N->ba = zalloc(L2->nv * 64); conv_fwd(L2, NULL, 4, WL(4), NULL, N->p2, N->ba);
-  N->bb = zalloc(L2->nv * 64); conv_fwd(L2, NULL, 5, WL(5), NULL, N->ba, N->bb);
-  N->d1a = zalloc(L1->nv * 32); conv_fwd(L1, L2, 6, WL(6), N->bb, N->s1, N->d1a);
-  N->d1b = zalloc(L1->nv * 32); conv_fwd(L1, L2, 7, WL(7), NULL, N->d1a, N->d1b);
-  N->d0a = zalloc(L0->nv * 16); conv_fwd(L0, L1, 8, WL(8), N->d1b, N->s0, N->d0a);
-  N->h = zalloc(L0->nv * 16); conv_fwd(L0, L1, 9, WL(9), NULL, N->d0a, N->h);
+  const double* cur = N->x;
+  for (int l = 0; l < LB; l++) {
+    lev_t *L = &N->L[l], *C = &N->L[l + 1];
+    N->ea[l] = zalloc(L->nv * chan(l)); conv_fwd(L, C, enc_a(l), WL(enc_a(l)), NULL, cur, N->ea[l]);
+    N->sk[l] = zalloc(L->nv * chan(l)); conv_fwd(L, C, enc_b(l), WL(enc_b(l)), NULL, N->ea[l], N->sk[l]);
+    N->pl[l + 1] = zalloc(C->nv * chan(l)); pool_fwd(L, C, N->sk[l], N->pl[l + 1], chan(l));
+    cur = N->pl[l + 1];
+  }
+  lev_t* LBt = &N->L[LB];
+  N->bA = zalloc(LBt->nv * chan(LB)); conv_fwd(LBt, NULL, bot_a(), WL(bot_a()), NULL, cur, N->bA);
+  N->bB = zalloc(LBt->nv * chan(LB)); conv_fwd(LBt, NULL, bot_b(), WL(bot_b()), NULL, N->bA, N->bB);
+  const double* up = N->bB;
+  for (int l = LB - 1; l >= 0; l--) {
+    lev_t *L = &N->L[l], *C = &N->L[l + 1];
+    N->da[l] = zalloc(L->nv * chan(l)); conv_fwd(L, C, dec_a(l), WL(dec_a(l)), up, N->sk[l], N->da[l]);
+    N->db[l] = zalloc(L->nv * chan(l)); conv_fwd(L, C, dec_b(l), WL(dec_b(l)), NULL, N->da[l], N->db[l]);
+    up = N->db[l];
+  }
   N->out = zalloc(L0->nv);
   const double* hw = N->W + head_off;
+  const double* h = N->db[0];
   for (int z = 0; z < L0->nz; z++) for (int y = 0; y < L0->ny; y++) for (int x = 0; x < L0->nx; x++) {
     if (!active(L0, x, y, z)) continue;
     long v = vidx(L0, x, y, z);
     double o = hw[16];
-    for (int c = 0; c < 16; c++) o += hw[c] * N->h[v * 16 + c];
+    for (int c = 0; c < 16; c++) o += hw[c] * h[v * 16 + c];
     N->out[v] = o;
   }
 }
 static void net_free(net_t* N) {
-  double* b[] = { N->x, N->e0a, N->s0, N->p1, N->e1a, N->s1, N->p2, N->ba, N->bb, N->d1a, N->d1b, N->d0a, N->h,
-                  N->W, N->out };
-  for (unsigned i = 0; i < sizeof(b) / sizeof(b[0]); i++) free(b[i]);
-  for (int l = 0; l < 3; l++) free(N->L[l].act);
+  free(N->x); free(N->bA); free(N->bB); free(N->W); free(N->out);
+  for (int l = 0; l < MAXLEV; l++) { free(N->ea[l]); free(N->sk[l]); free(N->pl[l]); free(N->da[l]); free(N->db[l]); }
+  for (int l = 0; l < g_levels; l++) free(N->L[l].act);
 }
 
 /* network output (before the gain) at every cell, 0 outside active tiles */
-void un_forward(int nx, int ny, int nz, const float* params, const float* r0n, const uint8_t* types, int round,
-                float* out) {
+void un_forward_levels(int nx, int ny, int nz, int levels, const float* params, const float* r0n, const uint8_t* types,
+                       int round, float* out) {
   net_t N; memset(&N, 0, sizeof(N));
   g_round = round;
+  set_levels(levels);
   build_levels(&N, nx, ny, nz, types);
   net_forward(&N, params, r0n, types);
   for (long v = 0; v < N.L[0].nv; v++) out[v] = (float)N.out[v];
   net_free(&N);
 }
+void un_forward(int nx, int ny, int nz, const float* params, const float* r0n, const uint8_t* types, int round,
+                float* out) {
+  un_forward_levels(nx, ny, nz, 3, params, r0n, types, round, out);
+}
 
 /* loss over fluid cells against target (already divided by the gain) and
  * its gradient with respect to every parameter (flat, like the weights) */
-double un_loss_grad(int nx, int ny, int nz, const float* params, const float* r0n, const uint8_t* types,
-                    const float* target, int round, double* grads) {
+double un_loss_grad_levels(int nx, int ny, int nz, int levels, const float* params, const float* r0n,
+                           const uint8_t* types, const float* target, int round, double* grads) {
   net_t N; memset(&N, 0, sizeof(N));
   g_round = round;
+  set_levels(levels);
   build_levels(&N, nx, ny, nz, types);
   net_forward(&N, params, r0n, types);
-  lev_t *L0 = &N.L[0], *L1 = &N.L[1], *L2 = &N.L[2];
+  const int LB = g_levels - 1;
+  lev_t* L0 = &N.L[0];
   memset(grads, 0, sizeof(double) * nparams_total);
   const double* hw = N.W + head_off;
+  const double* h = N.db[0];
   double loss = 0;
   int nf = N.nFluid > 0 ? N.nFluid : 1;
-  double* gh = zalloc(L0->nv * 16);
+  double *gdb[MAXLEV] = { 0 }, *gda[MAXLEV] = { 0 }, *gup[MAXLEV] = { 0 }, *gsa[MAXLEV] = { 0 };
+  double *gp[MAXLEV] = { 0 }, *gs[MAXLEV] = { 0 }, *gea[MAXLEV] = { 0 };
+  gdb[0] = zalloc(L0->nv * 16);
   for (int z = 0; z < L0->nz; z++) for (int y = 0; y < L0->ny; y++) for (int x = 0; x < L0->nx; x++) {
     if (!active(L0, x, y, z)) continue;
     long v = vidx(L0, x, y, z);
     double dout = 0;
     if (types[v] == 1) { double diff = N.out[v] - target[v]; loss += diff * diff / nf; dout = 2 * diff / nf; }
     for (int c = 0; c < 16; c++) {
-      grads[head_off + c] += dout * N.h[v * 16 + c];
-      gh[v * 16 + c] = rb(N.h[v * 16 + c] > 0 ? dout * hw[c] : 0.0);
+      grads[head_off + c] += dout * h[v * 16 + c];
+      gdb[0][v * 16 + c] = rb(h[v * 16 + c] > 0 ? dout * hw[c] : 0.0);
     }
     grads[head_off + 16] += dout;
   }
 #define GL(l) (grads + woff_of[l]), (grads + boff_of[l])
-  double* gd0a = zalloc(L0->nv * 16);
-  conv_bwd(L0, L1, 9, N.W + woff_of[9], NULL, N.d0a, gh, GL(9), N.d0a, gd0a, NULL);
-  double *gup1 = zalloc(L0->nv * 32), *gs0a = zalloc(L0->nv * 16);
-  conv_bwd(L0, L1, 8, N.W + woff_of[8], N.d1b, N.s0, gd0a, GL(8), NULL, gup1, gs0a);
-  double* gd1b = zalloc(L1->nv * 32); up_bwd(L1, L0, gup1, N.d1b, gd1b, 32);
-  double* gd1a = zalloc(L1->nv * 32);
-  conv_bwd(L1, L2, 7, N.W + woff_of[7], NULL, N.d1a, gd1b, GL(7), N.d1a, gd1a, NULL);
-  double *gup2 = zalloc(L1->nv * 64), *gs1a = zalloc(L1->nv * 32);
-  conv_bwd(L1, L2, 6, N.W + woff_of[6], N.bb, N.s1, gd1a, GL(6), NULL, gup2, gs1a);
-  double* gbb = zalloc(L2->nv * 64); up_bwd(L2, L1, gup2, N.bb, gbb, 64);
-  double* gba = zalloc(L2->nv * 64);
-  conv_bwd(L2, NULL, 5, N.W + woff_of[5], NULL, N.ba, gbb, GL(5), N.ba, gba, NULL);
-  double* gp2 = zalloc(L2->nv * 32);
-  conv_bwd(L2, NULL, 4, N.W + woff_of[4], NULL, N.p2, gba, GL(4), NULL, gp2, NULL);
-  double* gs1 = zalloc(L1->nv * 32); pool_bwd_add(L1, L2, gs1a, gp2, N.s1, gs1, 32);
-  double* ge1a = zalloc(L1->nv * 32);
-  conv_bwd(L1, L2, 3, N.W + woff_of[3], NULL, N.e1a, gs1, GL(3), N.e1a, ge1a, NULL);
-  double* gp1 = zalloc(L1->nv * 16);
-  conv_bwd(L1, L2, 2, N.W + woff_of[2], NULL, N.p1, ge1a, GL(2), NULL, gp1, NULL);
-  double* gs0 = zalloc(L0->nv * 16); pool_bwd_add(L0, L1, gs0a, gp1, N.s0, gs0, 16);
-  double* ge0a = zalloc(L0->nv * 16);
-  conv_bwd(L0, L1, 1, N.W + woff_of[1], NULL, N.e0a, gs0, GL(1), N.e0a, ge0a, NULL);
-  conv_bwd(L0, L1, 0, N.W + woff_of[0], NULL, N.x, ge0a, GL(0), NULL, NULL, NULL);
-  double* fr[] = { gh, gd0a, gup1, gs0a, gd1b, gd1a, gup2, gs1a, gbb, gba, gp2, gs1, ge1a, gp1, gs0, ge0a };
-  for (unsigned i = 0; i < sizeof(fr) / sizeof(fr[0]); i++) free(fr[i]);
+#define WOF(l) (N.W + woff_of[l])
+  double *gbA = zalloc(N.L[LB].nv * chan(LB)), *gbB = zalloc(N.L[LB].nv * chan(LB));
+  /* decoder, from level 0 up */
+  for (int l = 0; l < LB; l++) {
+    lev_t *L = &N.L[l], *C = &N.L[l + 1];
+    gda[l] = zalloc(L->nv * chan(l));
+    conv_bwd(L, C, dec_b(l), WOF(dec_b(l)), NULL, N.da[l], gdb[l], GL(dec_b(l)), N.da[l], gda[l], NULL);
+    const double* upSrc = l + 1 < LB ? N.db[l + 1] : N.bB;
+    gup[l] = zalloc(L->nv * chan(l + 1)); gsa[l] = zalloc(L->nv * chan(l));
+    conv_bwd(L, C, dec_a(l), WOF(dec_a(l)), upSrc, N.sk[l], gda[l], GL(dec_a(l)), NULL, gup[l], gsa[l]);
+    double* tgt = gbB;
+    if (l + 1 < LB) { gdb[l + 1] = zalloc(C->nv * chan(l + 1)); tgt = gdb[l + 1]; }
+    up_bwd(C, L, gup[l], upSrc, tgt, chan(l + 1));
+  }
+  /* bottleneck */
+  lev_t* LBt = &N.L[LB];
+  conv_bwd(LBt, NULL, bot_b(), WOF(bot_b()), NULL, N.bA, gbB, GL(bot_b()), N.bA, gbA, NULL);
+  gp[LB] = zalloc(LBt->nv * chan(LB - 1));
+  conv_bwd(LBt, NULL, bot_a(), WOF(bot_a()), NULL, N.pl[LB], gbA, GL(bot_a()), NULL, gp[LB], NULL);
+  /* encoder, from the deepest level down */
+  for (int l = LB - 1; l >= 0; l--) {
+    lev_t *L = &N.L[l], *C = &N.L[l + 1];
+    gs[l] = zalloc(L->nv * chan(l)); pool_bwd_add(L, C, gsa[l], gp[l + 1], N.sk[l], gs[l], chan(l));
+    gea[l] = zalloc(L->nv * chan(l));
+    conv_bwd(L, C, enc_b(l), WOF(enc_b(l)), NULL, N.ea[l], gs[l], GL(enc_b(l)), N.ea[l], gea[l], NULL);
+    if (l > 0) {
+      gp[l] = zalloc(L->nv * chan(l - 1));
+      conv_bwd(L, C, enc_a(l), WOF(enc_a(l)), NULL, N.pl[l], gea[l], GL(enc_a(l)), NULL, gp[l], NULL);
+    } else {
+      conv_bwd(L, C, enc_a(0), WOF(enc_a(0)), NULL, N.x, gea[0], GL(enc_a(0)), NULL, NULL, NULL);
+    }
+  }
+  for (int l = 0; l < MAXLEV; l++) { free(gdb[l]); free(gda[l]); free(gup[l]); free(gsa[l]); free(gp[l]); free(gs[l]); free(gea[l]); }
+  free(gbA); free(gbB);
   net_free(&N);
   return loss;
+}
+double un_loss_grad(int nx, int ny, int nz, const float* params, const float* r0n, const uint8_t* types,
+                    const float* target, int round, double* grads) {
+  return un_loss_grad_levels(nx, ny, nz, 3, params, r0n, types, target, round, grads);
 }

@@ -17,6 +17,13 @@ from oracle import unet_oracle as U
 pytestmark = pytest.mark.gpu
 
 SOLVE = dict(sorTol=1e-5, sorCheckEvery=10, sorMaxIters=4000)
+# Per-layer gradient tolerance by network depth (relative L2). Each layer's
+# backward output is rounded to BF16 where it is stored, so the divergence
+# grows with the length of the backward path from the loss. On this 32^3
+# planet the 4-level bottleneck is a 4^3 level (64 voxels), so its gradients
+# sum few terms: measured 0.2-2% at 3 levels, 1-5% in the 4-level decoder
+# and 5-8% through the 4-level bottleneck and encoder, with no layer apart.
+GRAD_TOL = {3: 6e-2, 4: 1e-1}
 DIMS = (32, 32, 32)
 
 
@@ -24,11 +31,11 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def _solver(pairs, stir_every=0, seed=5):
+def _solver(pairs, stir_every=0, seed=5, levels=3):
     o = planet("planet32", **PLAIN32)
     fs = to_device(o)
     fs.set_params(**SOLVE)
-    fs.unet_init(seed)
+    fs.unet_init(seed, levels)
     fs.unet_collect(pairs)
     for i in range(pairs):
         if stir_every and i % stir_every == 0:
@@ -44,6 +51,13 @@ def two_pairs():
     return _solver(2)
 
 
+@pytest.fixture(scope="module")
+def two_pairs4():
+    """The 4-level network (16/32/64/128 channels; the 128- and 192-channel
+    convolutions and the two-pass 128-channel weight gradient)."""
+    return _solver(2, levels=4)
+
+
 def test_pair_contents(two_pairs):
     fs = two_pairs
     r0n, types, target = fs.unet_pair(1)
@@ -55,32 +69,48 @@ def test_pair_contents(two_pairs):
     assert np.abs(target[fl]).max() > 0
 
 
-def test_forward_matches_oracle(two_pairs):
-    fs = two_pairs
+def _forward_matches(fs, levels):
     w = fs.unet_weights()
+    assert w.size == U.num_params(levels)
     for p in range(2):
         r0n, types, target = fs.unet_pair(p)
         gpu = fs.unet_forward_pair(p)
-        cpu = U.forward(DIMS, w, r0n, types, rounding=True)
+        cpu = U.forward(DIMS, w, r0n, types, rounding=True, levels=levels)
         fl = types == 1
         assert np.all(gpu[cpu == 0] == 0)
         assert _rel(gpu[fl], cpu[fl]) < 3e-2, p
 
 
-def test_gradients_match_oracle(two_pairs):
-    fs = two_pairs
+def test_forward_matches_oracle(two_pairs):
+    _forward_matches(two_pairs, 3)
+
+
+def test_forward_matches_oracle_4levels(two_pairs4):
+    _forward_matches(two_pairs4, 4)
+
+
+def _gradients_match(fs, levels):
     w = fs.unet_weights()
     r0n, types, target = fs.unet_pair(1)
     fl = types == 1
     gain = float(np.sqrt(np.mean(target[fl].astype(np.float64) ** 2)))
     fs.unet_set_gain(gain)
     g_gpu, loss_gpu = fs.unet_grad_pair(1)
-    loss_cpu, g_cpu = U.loss_grad(DIMS, w, r0n, types, target / np.float32(gain), rounding=True)
+    loss_cpu, g_cpu = U.loss_grad(DIMS, w, r0n, types, target / np.float32(gain), rounding=True, levels=levels)
     assert abs(loss_gpu - loss_cpu) <= 2e-2 * loss_cpu
-    sl = U.slices()
-    for name, (ws, bs) in sl.items():
-        assert _rel(g_gpu[ws], g_cpu[ws]) < 6e-2, name + " weights"
-        assert _rel(g_gpu[bs], g_cpu[bs]) < 6e-2, name + " biases"
+    sl = U.slices(levels)
+    errs = {name: (_rel(g_gpu[ws], g_cpu[ws]), _rel(g_gpu[bs], g_cpu[bs])) for name, (ws, bs) in sl.items()}
+    print("levels %d gradient errors %s" % (levels, {k: (round(a, 4), round(b, 4)) for k, (a, b) in errs.items()}))
+    bad = {k: v for k, v in errs.items() if max(v) >= GRAD_TOL[levels]}
+    assert not bad, bad
+
+
+def test_gradients_match_oracle(two_pairs):
+    _gradients_match(two_pairs, 3)
+
+
+def test_gradients_match_oracle_4levels(two_pairs4):
+    _gradients_match(two_pairs4, 4)
 
 
 def test_trained_network_saves_iterations():

@@ -1525,27 +1525,34 @@ static ws_status net_ready(ws_handle* h) {
   cudaSetDevice(h->device);
   return sync_status(h);
 }
-extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) {
+extern "C" ws_status ws_unet_init_levels(ws_handle* h, uint32_t seed, int32_t levels) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   if (!h) return WS_ERR_INVALID;
+  if (levels < 3 || levels > unet::kMaxLevels) return fail(h, WS_ERR_INVALID, "levels must be 3 or 4");
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
+  if (h->net && h->net->levels != levels) {        // a different depth: a new network (its pairs go too)
+    h->unetOn = false; h->unetCollect = false;
+    h->net->destroy(); delete h->net; h->net = nullptr;
+    h->gsig.unet = -1;                             // recapture the substep graph
+  }
   if (!h->net) {
     h->net = new (std::nothrow) unet::Net();
     if (!h->net) return fail(h, WS_ERR_NOMEM, "warm-start network");
-    cudaError_t e = h->net->create(h->d);
+    cudaError_t e = h->net->create(h->d, levels);
     if (e != cudaSuccess) { h->net->destroy(); delete h->net; h->net = nullptr; return fail_cuda(h, e, "warm-start network buffers"); }
   }
   WS_TRY(h->net->init_weights(seed, h->stream));
   WS_TRY(cudaStreamSynchronize(h->stream));
   return WS_OK;
 }
+extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) { return ws_unet_init_levels(h, seed, 3); }
 extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   if (capacity < 0) return fail(h, WS_ERR_RANGE, "negative pair capacity");
   if (capacity > 0) {
-    cudaError_t e = h->net->reserve_pairs(capacity);
+    cudaError_t e = h->net->reserve_pairs(capacity, h->type, h->stream);
     if (e != cudaSuccess) return fail_cuda(h, e, "pair store");
   }
   h->unetCollect = capacity > 0;
@@ -1608,11 +1615,8 @@ extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uin
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
-  if (idx < 0 || idx >= std::min(n.pairsStored, n.pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
-  long long N = h->d.nCells;
-  if (r0n) WS_TRY(cudaMemcpy(r0n, n.pr0n + N * idx, sizeof(float) * N, cudaMemcpyDeviceToHost));
-  if (types) WS_TRY(cudaMemcpy(types, n.ptype + N * idx, (size_t)N, cudaMemcpyDeviceToHost));
-  if (target) WS_TRY(cudaMemcpy(target, n.ptarget + N * idx, sizeof(float) * N, cudaMemcpyDeviceToHost));
+  if (idx < 0 || idx >= n.stored()) return fail(h, WS_ERR_RANGE, "pair index");
+  WS_TRY(n.get_pair(idx, r0n, types, target, h->stream));
   return WS_OK;
 }
 extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint8_t* types, const float* target) {
@@ -1620,17 +1624,9 @@ extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
   if (!r0n || !types || !target) return WS_ERR_INVALID;
-  if (n.pairCap <= 0) { cudaError_t e = n.reserve_pairs(1); if (e != cudaSuccess) return fail_cuda(h, e, "pair store"); }
-  long long N = h->d.nCells;
-  int slot = n.pairsStored % n.pairCap;
-  double t2 = 0;
-  for (long long c = 0; c < N; c++) if (types[c] == 1) t2 += (double)target[c] * target[c];
-  double sc[2] = { 1.0, t2 };
-  WS_TRY(cudaMemcpy(n.pr0n + N * slot, r0n, sizeof(float) * N, cudaMemcpyHostToDevice));
-  WS_TRY(cudaMemcpy(n.ptype + N * slot, types, (size_t)N, cudaMemcpyHostToDevice));
-  WS_TRY(cudaMemcpy(n.ptarget + N * slot, target, sizeof(float) * N, cudaMemcpyHostToDevice));
-  WS_TRY(cudaMemcpy(n.pscal + 2 * slot, sc, sizeof(sc), cudaMemcpyHostToDevice));
-  n.pairsStored++;
+  cudaError_t e = n.put_pair(r0n, types, target, h->stream);
+  if (e == cudaErrorInvalidValue) return fail(h, WS_ERR_RANGE, "the pair has more active tiles than a pair slot holds");
+  if (e != cudaSuccess) return fail_cuda(h, e, "pair store");
   return WS_OK;
 }
 extern "C" ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out) {

@@ -10,6 +10,9 @@
 //   L1  d1a = conv(up(bb) | s1, 96->32)        d1b = conv(d1a, 32->32)
 //   L0  d0a = conv(up(d1b) | s0, 48->16)       h = conv(d0a, 16->16)
 //   out = wh . h + bh  (FP32 head), at fluid cells
+// With 4 levels an encoder pair e2a, e2b (32->64, 64->64) sits at L2, the
+// bottleneck ba, bb (64->128, 128->128) at L3 and a decoder pair d2a, d2b
+// (up(bb) | s2, 192->64; 64->64) at L2.
 // pool = 2x2x2 mean, up = nearest x2, | = channel concatenation.
 // Input x (16 channels, 4 used): r0 / sigma, fluid, solid, air, where r0 =
 // b - A q_prev is the residual of the previous pressure and sigma its RMS
@@ -59,11 +62,11 @@ __global__ void k_activity0(Level L, const uint8_t* __restrict__ type, uint8_t* 
   __syncthreads();
   if (threadIdx.x == 0) { act[t] = (uint8_t)s_any; if (s_cnt) atomicAdd(nFluid, s_cnt); }
 }
-struct Levels { Level l[kLevels]; uint8_t* act[kLevels]; int* tiles[kLevels]; int* count; };
+struct Levels { Level l[kMaxLevels]; uint8_t* act[kMaxLevels]; int* tiles[kMaxLevels]; int* count; int n; };
 // one CTA: coarser activity from the finer, then the compacted tile lists
 __global__ void k_tile_lists(Levels Ls) {
   __shared__ int wsum[32], carry;
-  for (int lv = 0; lv < kLevels; lv++) {
+  for (int lv = 0; lv < Ls.n; lv++) {
     const Level& L = Ls.l[lv];
     if (lv > 0) {
       const Level& F = Ls.l[lv - 1];
@@ -402,6 +405,43 @@ __global__ void k_scale_copy(const float* __restrict__ a, float* __restrict__ b,
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c < n) b[c] = a[c] * s;
 }
+// A pair slot holds, for each of its tiles k (tile id stiles[k]), the 1024
+// voxels of that level-0 tile in tile order (r = x + 8 (y + 16 z)).
+// pack: dense level-0 arrays -> slot, over the tile list of the current
+// activity (tiles, *count). With r0 / type null only the target is packed.
+__global__ void k_pair_pack(Level L, const int* __restrict__ tiles, const int* count, int tileCap,
+                            const float* __restrict__ r0, const uint8_t* __restrict__ type,
+                            const float* __restrict__ target, float* __restrict__ sr0, uint8_t* __restrict__ stype,
+                            float* __restrict__ starget, int* __restrict__ stiles) {
+  const int nT = *count;
+  if (nT > tileCap) return;                        // the slot is marked unusable by the host
+  const long long n = (long long)nT * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if ((i & 1023) == 0 && stiles) stiles[i >> 10] = tiles[i >> 10];
+    int X, Y, Z; long long v;
+    const bool in = tile_voxel(L, tiles, nT, i, X, Y, Z, v);
+    if (r0) sr0[i] = in ? r0[v] : 0.f;
+    if (type) stype[i] = in ? type[v] : (uint8_t)WS_AIR;
+    if (target) starget[i] = in ? target[v] : 0.f;
+  }
+}
+// unpack slot -> dense level-0 arrays at its tiles, and the level-0 activity
+__global__ void k_pair_unpack(Level L, const int* __restrict__ stiles, const int* __restrict__ meta,
+                              const float* __restrict__ sr0, const uint8_t* __restrict__ stype,
+                              const float* __restrict__ starget, float* __restrict__ r0, uint8_t* __restrict__ type,
+                              float* __restrict__ target, uint8_t* __restrict__ act0, int* fluidCount) {
+  const int nT = meta[0];
+  const long long n = (long long)nT * 1024;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    if ((i & 1023) == 0) act0[stiles[i >> 10]] = 1;
+    if (i == 0) *fluidCount = meta[1];
+    int X, Y, Z; long long v;
+    if (!tile_voxel(L, stiles, nT, i, X, Y, Z, v)) continue;
+    if (r0) r0[v] = sr0[i];
+    type[v] = stype[i];
+    if (target) target[v] = starget[i];
+  }
+}
 
 // ------------------------------------------------------------ host driver
 static inline unsigned grid1(long long n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -419,22 +459,38 @@ struct HostRng {
   }
 };
 
-const LayerSpec kLayers[kNumLayers] = {
-  // name, level, c0 (upsampled), c1, cout
-  {"e0a", 0, 0, 16, 16}, {"e0b", 0, 0, 16, 16},
-  {"e1a", 1, 0, 16, 32}, {"e1b", 1, 0, 32, 32},
-  {"ba", 2, 0, 32, 64},  {"bb", 2, 0, 64, 64},
-  {"d1a", 1, 64, 32, 32}, {"d1b", 1, 0, 32, 32},
-  {"d0a", 0, 32, 16, 16}, {"d0b", 0, 0, 16, 16},
-};
+int unet_layers(int levels, LayerSpec* out) {
+  static const char* encA[] = { "e0a", "e1a", "e2a" };
+  static const char* encB[] = { "e0b", "e1b", "e2b" };
+  static const char* decA[] = { "d0a", "d1a", "d2a" };
+  static const char* decB[] = { "d0b", "d1b", "d2b" };
+  int n = 0;
+  for (int l = 0; l + 1 < levels; l++) {
+    const int c = 16 << l, cin = l == 0 ? 16 : 16 << (l - 1);
+    out[n++] = { encA[l], l, 0, cin, c };
+    out[n++] = { encB[l], l, 0, c, c };
+  }
+  const int cb = 16 << (levels - 1);
+  out[n++] = { "ba", levels - 1, 0, cb / 2, cb };
+  out[n++] = { "bb", levels - 1, 0, cb, cb };
+  for (int l = levels - 2; l >= 0; l--) {
+    const int c = 16 << l;
+    out[n++] = { decA[l], l, 2 * c, c, c };
+    out[n++] = { decB[l], l, 0, c, c };
+  }
+  return n;
+}
 
-long long Net::layer_weights(int l) { return 27LL * (kLayers[l].c0 + kLayers[l].c1) * kLayers[l].cout; }
+long long Net::layer_weights(int l) const { return 27LL * (layers[l].c0 + layers[l].c1) * layers[l].cout; }
 
-cudaError_t Net::create(const Dims& d) {
+cudaError_t Net::create(const Dims& d, int nlev) {
   cudaError_t e;
+  if (nlev < 3 || nlev > kMaxLevels) return cudaErrorInvalidValue;
   dims = d;
+  levels = nlev;
+  nLayers = unet_layers(levels, layers);
   int nx = d.nx, ny = d.ny, nz = d.nz;
-  for (int l = 0; l < kLevels; l++) {
+  for (int l = 0; l < levels; l++) {
     Level& L = lv[l];
     L.nx = nx; L.ny = ny; L.nz = nz;
     L.ntx = (nx + kTX - 1) / kTX; L.nty = (ny + kTY - 1) / kTY; L.ntz = (nz + kTZ - 1) / kTZ;
@@ -445,66 +501,71 @@ cudaError_t Net::create(const Dims& d) {
     if ((e = cudaMalloc(&tiles[l], sizeof(int) * L.ntiles)) != cudaSuccess) return e;
     nx = (nx + 1) / 2; ny = (ny + 1) / 2; nz = (nz + 1) / 2;
   }
-  if ((e = cudaMalloc(&counts, sizeof(int) * 4)) != cudaSuccess) return e;   // 3 tile counts + fluid count
-  if ((e = cudaMemset(counts, 0, sizeof(int) * 4)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&counts, sizeof(int) * (kMaxLevels + 1))) != cudaSuccess) return e;   // tile counts + fluid count
+  if ((e = cudaMemset(counts, 0, sizeof(int) * (kMaxLevels + 1))) != cudaSuccess) return e;
   // parameters
   nparams = 0;
-  for (int l = 0; l < kNumLayers; l++) { woff[l] = nparams; nparams += layer_weights(l); boff[l] = nparams; nparams += kLayers[l].cout; }
+  for (int l = 0; l < nLayers; l++) { woff[l] = nparams; nparams += layer_weights(l); boff[l] = nparams; nparams += layers[l].cout; }
   headOff = nparams; nparams += 17;
   if ((e = cudaMalloc(&params, sizeof(float) * nparams)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&grads, sizeof(float) * nparams)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&adm, sizeof(float) * nparams)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&adv, sizeof(float) * nparams)) != cudaSuccess) return e;
-  for (int l = 0; l < kNumLayers; l++) {
+  for (int l = 0; l < nLayers; l++) {
     if ((e = cudaMalloc(&fw[l], sizeof(bf16) * layer_weights(l))) != cudaSuccess) return e;
     if ((e = cudaMalloc(&bw[l], sizeof(bf16) * layer_weights(l))) != cudaSuccess) return e;
   }
   // activations and gradients (NDHWC bf16, dense per level)
-  auto A = [&](bf16** p, int l, int ch) -> cudaError_t {
-    cudaError_t r = cudaMalloc(p, sizeof(bf16) * lv[l].nvox * ch);
-    if (r == cudaSuccess) r = cudaMemset(*p, 0, sizeof(bf16) * lv[l].nvox * ch);
+  auto A = [&](bf16** p, int l, int c) -> cudaError_t {
+    cudaError_t r = cudaMalloc(p, sizeof(bf16) * lv[l].nvox * c);
+    if (r == cudaSuccess) r = cudaMemset(*p, 0, sizeof(bf16) * lv[l].nvox * c);
     return r;
   };
-  bf16** acts[] = { &x, &e0a, &s0, &d0a, &h, &gh, &gd0a, &gs0a, &gs0, &ge0a };
-  for (bf16** p : acts) if ((e = A(p, 0, 16)) != cudaSuccess) return e;
-  if ((e = A(&gup1, 0, 32)) != cudaSuccess) return e;
-  bf16** l1_16[] = { &p1, &gp1 };
-  for (bf16** p : l1_16) if ((e = A(p, 1, 16)) != cudaSuccess) return e;
-  bf16** l1_32[] = { &e1a, &s1, &d1a, &d1b, &gd1b, &gd1a, &gs1a, &gs1, &ge1a };
-  for (bf16** p : l1_32) if ((e = A(p, 1, 32)) != cudaSuccess) return e;
-  if ((e = A(&gup2, 1, 64)) != cudaSuccess) return e;
-  if ((e = A(&p2, 2, 32)) != cudaSuccess) return e;
-  if ((e = A(&gp2, 2, 32)) != cudaSuccess) return e;
-  bf16** l2_64[] = { &ba, &bb, &gbb, &gba };
-  for (bf16** p : l2_64) if ((e = A(p, 2, 64)) != cudaSuccess) return e;
+  const int L1 = levels - 1;
+  if ((e = A(&x, 0, 16)) != cudaSuccess) return e;
+  for (int l = 0; l < L1; l++) {
+    bf16** same[] = { &ea[l], &sk[l], &da[l], &db[l], &gdb[l], &gda[l], &gsa[l], &gs[l], &gea[l] };
+    for (bf16** p : same) if ((e = A(p, l, ch(l))) != cudaSuccess) return e;
+    if ((e = A(&gup[l], l, ch(l + 1))) != cudaSuccess) return e;
+    if ((e = A(&pl[l + 1], l + 1, ch(l))) != cudaSuccess) return e;
+    if ((e = A(&gp[l + 1], l + 1, ch(l))) != cudaSuccess) return e;
+  }
+  bf16** bot[] = { &bA, &bB, &gbA, &gbB };
+  for (bf16** p : bot) if ((e = A(p, L1, ch(L1))) != cudaSuccess) return e;
   long long N = d.nCells;
   nPartials = (int)grid1(N, 256);
   if ((e = cudaMalloc(&partials, sizeof(double) * nPartials)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&scal, sizeof(double) * 8)) != cudaSuccess) return e;   // sigma, gain, loss, t2
   if ((e = cudaMemset(scal, 0, sizeof(double) * 8)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&r0n, sizeof(float) * N)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&qprev, sizeof(float) * N)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&tscaled, sizeof(float) * N)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&outbuf, sizeof(float) * N)) != cudaSuccess) return e;
+  float** fbufs[] = { &r0n, &qprev, &tscaled, &outbuf, &tbuf };
+  for (float** p : fbufs) {
+    if ((e = cudaMalloc(p, sizeof(float) * N)) != cudaSuccess) return e;
+    if ((e = cudaMemset(*p, 0, sizeof(float) * N)) != cudaSuccess) return e;
+  }
+  if ((e = cudaMalloc(&typebuf, (size_t)N)) != cudaSuccess) return e;
+  if ((e = cudaMemset(typebuf, 0, (size_t)N)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&err, sizeof(int))) != cudaSuccess) return e;
   if ((e = cudaMemset(err, 0, sizeof(int))) != cudaSuccess) return e;
   return conv3_init();
 }
 
 void Net::destroy() {
-  void* bufs[] = { counts, params, grads, adm, adv, x, e0a, s0, d0a, h, gh, gd0a, gs0a, gs0, ge0a, gup1, p1, gp1,
-                   e1a, s1, d1a, d1b, gd1b, gd1a, gs1a, gs1, ge1a, gup2, p2, gp2, ba, bb, gbb, gba,
-                   partials, scal, r0n, qprev, tscaled, outbuf, err, pr0n, ptype, ptarget, pscal };
+  void* bufs[] = { counts, params, grads, adm, adv, x, bA, bB, gbA, gbB, partials, scal, r0n, qprev, tscaled, outbuf,
+                   tbuf, typebuf, err, pr0n, ptype, ptarget, ptiles, pmeta, pscal };
   for (void* b : bufs) if (b) cudaFree(b);
-  for (int l = 0; l < kLevels; l++) { if (act[l]) cudaFree(act[l]); if (tiles[l]) cudaFree(tiles[l]); }
-  for (int l = 0; l < kNumLayers; l++) { if (fw[l]) cudaFree(fw[l]); if (bw[l]) cudaFree(bw[l]); }
+  for (int l = 0; l < kMaxLevels; l++) {
+    void* per[] = { act[l], tiles[l], ea[l], sk[l], pl[l], da[l], db[l], gdb[l], gda[l], gup[l], gsa[l], gp[l], gs[l],
+                    gea[l] };
+    for (void* b : per) if (b) cudaFree(b);
+  }
+  for (int l = 0; l < kMaxLayers; l++) { if (fw[l]) cudaFree(fw[l]); if (bw[l]) cudaFree(bw[l]); }
 }
 
 cudaError_t Net::init_weights(uint32_t seed, cudaStream_t s) {
   std::vector<float> P((size_t)nparams, 0.f);
   HostRng rng(seed);
-  for (int l = 0; l < kNumLayers; l++) {
-    int cin = kLayers[l].c0 + kLayers[l].c1;
+  for (int l = 0; l < nLayers; l++) {
+    int cin = layers[l].c0 + layers[l].c1;
     double sd = std::sqrt(2.0 / (27.0 * cin));
     for (long long i = 0; i < layer_weights(l); i++) P[(size_t)(woff[l] + i)] = (float)(sd * rng.normal());
   }
@@ -524,26 +585,30 @@ cudaError_t Net::set_weights(const float* host, cudaStream_t s) {
   return pack(s);
 }
 cudaError_t Net::pack(cudaStream_t s) {
-  for (int l = 0; l < kNumLayers; l++) {
+  for (int l = 0; l < nLayers; l++) {
     int n = (int)layer_weights(l);
-    k_pack<<<grid1(n, 256), 256, 0, s>>>(params + woff[l], kLayers[l].c0 + kLayers[l].c1, kLayers[l].cout, fw[l], bw[l]);
+    k_pack<<<grid1(n, 256), 256, 0, s>>>(params + woff[l], layers[l].c0 + layers[l].c1, layers[l].cout, fw[l], bw[l]);
   }
   return cudaGetLastError();
 }
 
-// tile activity of all levels from cell types; counts[3] = fluid cells
-cudaError_t Net::activity(const uint8_t* type, cudaStream_t s) {
-  cudaMemsetAsync(counts + 3, 0, sizeof(int), s);
-  k_activity0<<<lv[0].ntiles, 256, 0, s>>>(lv[0], type, act[0], counts + 3);
+// the coarser levels' activity and every level's tile list from act[0]
+cudaError_t Net::lists(cudaStream_t s) {
   Levels Ls;
-  for (int l = 0; l < kLevels; l++) { Ls.l[l] = lv[l]; Ls.act[l] = act[l]; Ls.tiles[l] = tiles[l]; }
-  Ls.count = counts;
+  for (int l = 0; l < levels; l++) { Ls.l[l] = lv[l]; Ls.act[l] = act[l]; Ls.tiles[l] = tiles[l]; }
+  Ls.count = counts; Ls.n = levels;
   k_tile_lists<<<1, 1024, 0, s>>>(Ls);
   return cudaGetLastError();
 }
+// tile activity of all levels from cell types; counts[kMaxLevels] = fluid cells
+cudaError_t Net::activity(const uint8_t* type, cudaStream_t s) {
+  cudaMemsetAsync(counts + kMaxLevels, 0, sizeof(int), s);
+  k_activity0<<<lv[0].ntiles, 256, 0, s>>>(lv[0], type, act[0], counts + kMaxLevels);
+  return lists(s);
+}
 
 cudaError_t Net::conv(int l, const bf16* src0, const bf16* src1, bf16* out, cudaStream_t s) {
-  const LayerSpec& S = kLayers[l];
+  const LayerSpec& S = layers[l];
   const Level& L = lv[S.level];
   ConvArgs a{};
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.ntx = L.ntx; a.nty = L.nty; a.ntz = L.ntz;
@@ -556,7 +621,7 @@ cudaError_t Net::conv(int l, const bf16* src0, const bf16* src1, bf16* out, cuda
 // backward data of layer l: dX = conv^T(dZ), optionally masked by (mask > 0)
 // or split into the upsampled part (out0) and the skip part (out1)
 cudaError_t Net::conv_bwd(int l, const bf16* dz, const bf16* mask, bf16* out0, bf16* out1, cudaStream_t s) {
-  const LayerSpec& S = kLayers[l];
+  const LayerSpec& S = layers[l];
   const Level& L = lv[S.level];
   ConvArgs a{};
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.ntx = L.ntx; a.nty = L.nty; a.ntz = L.ntz;
@@ -568,7 +633,7 @@ cudaError_t Net::conv_bwd(int l, const bf16* dz, const bf16* mask, bf16* out0, b
   return launch_conv3(a, cin, L.ntiles, s);
 }
 cudaError_t Net::dw(int l, const bf16* src0, const bf16* src1, const bf16* dz, cudaStream_t s) {
-  const LayerSpec& S = kLayers[l];
+  const LayerSpec& S = layers[l];
   const Level& L = lv[S.level];
   ConvArgs a{};
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.ntx = L.ntx; a.nty = L.nty; a.ntz = L.ntz;
@@ -578,87 +643,84 @@ cudaError_t Net::dw(int l, const bf16* src0, const bf16* src1, const bf16* dz, c
   return launch_dw_tc(a, dz, S.cout, grads + woff[l], grads + boff[l], L.ntiles * (cin / 16), s);
 }
 
-cudaError_t Net::pool(int fineLevel, const bf16* fine, bf16* coarse, int ch, cudaStream_t s) {
+cudaError_t Net::pool(int fineLevel, const bf16* fine, bf16* coarse, int c, cudaStream_t s) {
   const Level& C = lv[fineLevel + 1];
-  long long n = (long long)C.ntiles * 1024 * (ch / 8);
+  long long n = (long long)C.ntiles * 1024 * (c / 8);
   k_pool<<<gridv(n, 256), 256, 0, s>>>(C, tiles[fineLevel + 1], counts + fineLevel + 1, lv[fineLevel], act[fineLevel],
-                                       fine, coarse, ch);
+                                       fine, coarse, c);
   return cudaGetLastError();
 }
 
 // forward pass on the input already in x (activity and tile lists built)
 cudaError_t Net::forward(cudaStream_t s) {
   cudaError_t e;
-  if ((e = conv(0, nullptr, x, e0a, s)) != cudaSuccess) return e;
-  if ((e = conv(1, nullptr, e0a, s0, s)) != cudaSuccess) return e;
-  if ((e = pool(0, s0, p1, 16, s)) != cudaSuccess) return e;
-  if ((e = conv(2, nullptr, p1, e1a, s)) != cudaSuccess) return e;
-  if ((e = conv(3, nullptr, e1a, s1, s)) != cudaSuccess) return e;
-  if ((e = pool(1, s1, p2, 32, s)) != cudaSuccess) return e;
-  if ((e = conv(4, nullptr, p2, ba, s)) != cudaSuccess) return e;
-  if ((e = conv(5, nullptr, ba, bb, s)) != cudaSuccess) return e;
-  if ((e = conv(6, bb, s1, d1a, s)) != cudaSuccess) return e;
-  if ((e = conv(7, nullptr, d1a, d1b, s)) != cudaSuccess) return e;
-  if ((e = conv(8, d1b, s0, d0a, s)) != cudaSuccess) return e;
-  return conv(9, nullptr, d0a, h, s);
+  const bf16* cur = x;
+  for (int l = 0; l + 1 < levels; l++) {
+    if ((e = conv(enc_a(l), nullptr, cur, ea[l], s)) != cudaSuccess) return e;
+    if ((e = conv(enc_b(l), nullptr, ea[l], sk[l], s)) != cudaSuccess) return e;
+    if ((e = pool(l, sk[l], pl[l + 1], ch(l), s)) != cudaSuccess) return e;
+    cur = pl[l + 1];
+  }
+  if ((e = conv(bot_a(), nullptr, cur, bA, s)) != cudaSuccess) return e;
+  if ((e = conv(bot_b(), nullptr, bA, bB, s)) != cudaSuccess) return e;
+  const bf16* up = bB;
+  for (int l = levels - 2; l >= 0; l--) {
+    if ((e = conv(dec_a(l), up, sk[l], da[l], s)) != cudaSuccess) return e;
+    if ((e = conv(dec_b(l), nullptr, da[l], db[l], s)) != cudaSuccess) return e;
+    up = db[l];
+  }
+  return cudaSuccess;
 }
 
-// backward pass from the head gradient in gh; accumulates into grads
+// backward pass from the head gradient in gdb[0]; accumulates into grads
 cudaError_t Net::backward(cudaStream_t s) {
   cudaError_t e;
-  auto upb = [&](int coarseLevel, const bf16* dup, const bf16* a, bf16* out, int ch) {
+  auto upb = [&](int coarseLevel, const bf16* dup, const bf16* a, bf16* out, int c) {
     const Level& C = lv[coarseLevel];
-    long long n = (long long)C.ntiles * 1024 * (ch / 8);
+    long long n = (long long)C.ntiles * 1024 * (c / 8);
     k_up_bwd<<<gridv(n, 256), 256, 0, s>>>(C, tiles[coarseLevel], counts + coarseLevel, lv[coarseLevel - 1],
-                                           act[coarseLevel - 1], dup, a, out, ch);
+                                           act[coarseLevel - 1], dup, a, out, c);
     return cudaGetLastError();
   };
-  auto pba = [&](int fineLevel, const bf16* dskip, const bf16* dpool, const bf16* sAct, bf16* out, int ch) {
+  auto pba = [&](int fineLevel, const bf16* dskip, const bf16* dpool, const bf16* sAct, bf16* out, int c) {
     const Level& F = lv[fineLevel];
-    long long n = (long long)F.ntiles * 1024 * (ch / 8);
+    long long n = (long long)F.ntiles * 1024 * (c / 8);
     k_pool_bwd_add<<<gridv(n, 256), 256, 0, s>>>(F, tiles[fineLevel], counts + fineLevel, lv[fineLevel + 1],
-                                                 dskip, dpool, sAct, out, ch);
+                                                 dskip, dpool, sAct, out, c);
     return cudaGetLastError();
   };
-  if ((e = dw(9, nullptr, d0a, gh, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(9, gh, d0a, gd0a, nullptr, s)) != cudaSuccess) return e;
-  if ((e = dw(8, d1b, s0, gd0a, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(8, gd0a, nullptr, gup1, gs0a, s)) != cudaSuccess) return e;
-  if ((e = upb(1, gup1, d1b, gd1b, 32)) != cudaSuccess) return e;
-  if ((e = dw(7, nullptr, d1a, gd1b, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(7, gd1b, d1a, gd1a, nullptr, s)) != cudaSuccess) return e;
-  if ((e = dw(6, bb, s1, gd1a, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(6, gd1a, nullptr, gup2, gs1a, s)) != cudaSuccess) return e;
-  if ((e = upb(2, gup2, bb, gbb, 64)) != cudaSuccess) return e;
-  if ((e = dw(5, nullptr, ba, gbb, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(5, gbb, ba, gba, nullptr, s)) != cudaSuccess) return e;
-  if ((e = dw(4, nullptr, p2, gba, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(4, gba, nullptr, gp2, nullptr, s)) != cudaSuccess) return e;
-  if ((e = pba(1, gs1a, gp2, s1, gs1, 32)) != cudaSuccess) return e;
-  if ((e = dw(3, nullptr, e1a, gs1, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(3, gs1, e1a, ge1a, nullptr, s)) != cudaSuccess) return e;
-  if ((e = dw(2, nullptr, p1, ge1a, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(2, ge1a, nullptr, gp1, nullptr, s)) != cudaSuccess) return e;
-  if ((e = pba(0, gs0a, gp1, s0, gs0, 16)) != cudaSuccess) return e;
-  if ((e = dw(1, nullptr, e0a, gs0, s)) != cudaSuccess) return e;
-  if ((e = conv_bwd(1, gs0, e0a, ge0a, nullptr, s)) != cudaSuccess) return e;
-  return dw(0, nullptr, x, ge0a, s);
+  const int L1 = levels - 1;
+  // decoder, from level 0 up: d<l>b, then d<l>a and the gradient of what it upsampled
+  for (int l = 0; l < L1; l++) {
+    if ((e = dw(dec_b(l), nullptr, da[l], gdb[l], s)) != cudaSuccess) return e;
+    if ((e = conv_bwd(dec_b(l), gdb[l], da[l], gda[l], nullptr, s)) != cudaSuccess) return e;
+    const bf16* upSrc = l + 1 < L1 ? db[l + 1] : bB;
+    if ((e = dw(dec_a(l), upSrc, sk[l], gda[l], s)) != cudaSuccess) return e;
+    if ((e = conv_bwd(dec_a(l), gda[l], nullptr, gup[l], gsa[l], s)) != cudaSuccess) return e;
+    if ((e = upb(l + 1, gup[l], upSrc, l + 1 < L1 ? gdb[l + 1] : gbB, ch(l + 1))) != cudaSuccess) return e;
+  }
+  // bottleneck
+  if ((e = dw(bot_b(), nullptr, bA, gbB, s)) != cudaSuccess) return e;
+  if ((e = conv_bwd(bot_b(), gbB, bA, gbA, nullptr, s)) != cudaSuccess) return e;
+  if ((e = dw(bot_a(), nullptr, pl[L1], gbA, s)) != cudaSuccess) return e;
+  if ((e = conv_bwd(bot_a(), gbA, nullptr, gp[L1], nullptr, s)) != cudaSuccess) return e;
+  // encoder, from the deepest level down
+  for (int l = L1 - 1; l >= 0; l--) {
+    if ((e = pba(l, gsa[l], gp[l + 1], sk[l], gs[l], ch(l))) != cudaSuccess) return e;
+    if ((e = dw(enc_b(l), nullptr, ea[l], gs[l], s)) != cudaSuccess) return e;
+    if ((e = conv_bwd(enc_b(l), gs[l], ea[l], gea[l], nullptr, s)) != cudaSuccess) return e;
+    if ((e = dw(enc_a(l), nullptr, l == 0 ? x : pl[l], gea[l], s)) != cudaSuccess) return e;
+    if (l > 0 && (e = conv_bwd(enc_a(l), gea[l], nullptr, gp[l], nullptr, s)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
-// input from normalised residual + cell types; builds activity first
-cudaError_t Net::prepare(const float* r0nIn, const uint8_t* type, cudaStream_t s) {
-  cudaError_t e;
-  if ((e = activity(type, s)) != cudaSuccess) return e;
-  long long n = (long long)lv[0].ntiles * 1024;
-  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0nIn, type, x, nullptr);
-  return cudaGetLastError();
-}
 // r0 / sigma of the current pressure setup into dst, sigma into sig
 cudaError_t Net::residual(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type,
                           float* dst, double* sig, cudaStream_t s, bool scale) {
   long long N = dims.nCells;
   k_residual0<<<nPartials, 256, 0, s>>>(dims, q, rhs, diag8, type, dst, partials);
-  k_sigma<<<1, 1024, 0, s>>>(partials, nPartials, counts + 3, sig);
+  k_sigma<<<1, 1024, 0, s>>>(partials, nPartials, counts + kMaxLevels, sig);
   if (scale) k_scale<<<grid1(N, 256), 256, 0, s>>>(dst, N, sig);
   return cudaGetLastError();
 }
@@ -672,74 +734,116 @@ cudaError_t Net::predict(float* q, const float* rhs, const uint8_t* diag8, const
   long long n = (long long)lv[0].ntiles * 1024;
   k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, type, x, scal + 0);
   if ((e = forward(s)) != cudaSuccess) return e;
-  k_head_apply<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, type, scal + 0, scal + 1, q);
+  k_head_apply<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, db[0], params + headOff, type, scal + 0, scal + 1, q);
   return cudaGetLastError();
 }
 
 // ---- training pairs
-cudaError_t Net::reserve_pairs(int capacity) {
+// A slot holds tileCap level-0 tiles: every tile when the grid has at most
+// 2048 of them, else 1.5 x the active tiles of the current cell types (at
+// least 256). A pair with more active tiles is not stored (pairsDropped).
+cudaError_t Net::reserve_pairs(int capacity, const uint8_t* type, cudaStream_t s) {
   if (capacity <= pairCap) return cudaSuccess;
-  long long N = dims.nCells;
-  float *a = nullptr, *c = nullptr; uint8_t* b = nullptr; double* sc = nullptr;
   cudaError_t e;
-  if ((e = cudaMalloc(&a, sizeof(float) * N * capacity)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&b, (size_t)N * capacity)) != cudaSuccess) { cudaFree(a); return e; }
-  if ((e = cudaMalloc(&c, sizeof(float) * N * capacity)) != cudaSuccess) { cudaFree(a); cudaFree(b); return e; }
-  if ((e = cudaMalloc(&sc, sizeof(double) * 2 * capacity)) != cudaSuccess) { cudaFree(a); cudaFree(b); cudaFree(c); return e; }
+  int cap = lv[0].ntiles;
+  if (cap > 2048) {
+    if ((e = activity(type, s)) != cudaSuccess) return e;
+    int c0 = 0;
+    if ((e = cudaMemcpyAsync(&c0, counts, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    cap = std::min(lv[0].ntiles, std::max(256, c0 + c0 / 2));
+  }
+  if (tileCap > 0) cap = tileCap;                 // slots keep their size once made
+  const size_t V = (size_t)cap * 1024;
+  float *a = nullptr, *c = nullptr; uint8_t* b = nullptr; int *t = nullptr, *m = nullptr; double* sc = nullptr;
+  if ((e = cudaMalloc(&a, sizeof(float) * V * capacity)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&b, V * capacity)) != cudaSuccess) { cudaFree(a); return e; }
+  if ((e = cudaMalloc(&c, sizeof(float) * V * capacity)) != cudaSuccess) { cudaFree(a); cudaFree(b); return e; }
+  if ((e = cudaMalloc(&t, sizeof(int) * (size_t)cap * capacity)) != cudaSuccess) { cudaFree(a); cudaFree(b); cudaFree(c); return e; }
+  if ((e = cudaMalloc(&m, sizeof(int) * 2 * capacity)) != cudaSuccess) { cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(t); return e; }
+  if ((e = cudaMalloc(&sc, sizeof(double) * 2 * capacity)) != cudaSuccess) {
+    cudaFree(a); cudaFree(b); cudaFree(c); cudaFree(t); cudaFree(m); return e;
+  }
   cudaMemset(sc, 0, sizeof(double) * 2 * capacity);
-  if (pairCap > 0 && pairsStored > 0) {   // keep the stored pairs
-    int keep = std::min(pairsStored, pairCap);
-    cudaMemcpy(a, pr0n, sizeof(float) * N * keep, cudaMemcpyDeviceToDevice);
-    cudaMemcpy(b, ptype, (size_t)N * keep, cudaMemcpyDeviceToDevice);
-    cudaMemcpy(c, ptarget, sizeof(float) * N * keep, cudaMemcpyDeviceToDevice);
+  cudaMemset(m, 0, sizeof(int) * 2 * capacity);
+  if (pairCap > 0 && pairsStored > 0) {           // keep the stored pairs
+    const int keep = std::min(pairsStored, pairCap);
+    cudaMemcpy(a, pr0n, sizeof(float) * V * keep, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(b, ptype, V * keep, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(c, ptarget, sizeof(float) * V * keep, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(t, ptiles, sizeof(int) * (size_t)cap * keep, cudaMemcpyDeviceToDevice);
+    cudaMemcpy(m, pmeta, sizeof(int) * 2 * keep, cudaMemcpyDeviceToDevice);
     cudaMemcpy(sc, pscal, sizeof(double) * 2 * keep, cudaMemcpyDeviceToDevice);
   }
-  cudaFree(pr0n); cudaFree(ptype); cudaFree(ptarget); cudaFree(pscal);
-  pr0n = a; ptype = b; ptarget = c; pscal = sc; pairCap = capacity;
+  void* old[] = { pr0n, ptype, ptarget, ptiles, pmeta, pscal };
+  for (void* o : old) if (o) cudaFree(o);
+  pr0n = a; ptype = b; ptarget = c; ptiles = t; pmeta = m; pscal = sc; pairCap = capacity; tileCap = cap;
   return cudaSuccess;
 }
-// before the solve: slot <- (r0 / sigma, types), q_prev saved
+// before the solve: slot <- (r0 / sigma, types) over the active tiles, q_prev saved
 cudaError_t Net::collect_pre(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type, cudaStream_t s) {
   if (pairCap <= 0) return cudaSuccess;
-  long long N = dims.nCells;
-  int slot = pairsStored % pairCap;
+  const int slot = pairsStored % pairCap;
+  const size_t V = (size_t)tileCap * 1024;
   cudaError_t e;
   if ((e = activity(type, s)) != cudaSuccess) return e;
-  if ((e = residual(q, rhs, diag8, type, pr0n + N * slot, pscal + 2 * slot, s)) != cudaSuccess) return e;
-  cudaMemcpyAsync(ptype + N * slot, type, (size_t)N, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(qprev, q, sizeof(float) * N, cudaMemcpyDeviceToDevice, s);
+  if ((e = residual(q, rhs, diag8, type, r0n, pscal + 2 * slot, s)) != cudaSuccess) return e;
+  int c[2];                                        // active level-0 tiles, fluid cells
+  if ((e = cudaMemcpyAsync(&c[0], counts, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(&c[1], counts + kMaxLevels, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  if (c[0] > tileCap) { pendingSlot = -1; pairsDropped++; return cudaSuccess; }
+  k_pair_pack<<<gridv((long long)c[0] * 1024, 256), 256, 0, s>>>(lv[0], tiles[0], counts, tileCap, r0n, type, nullptr,
+                                                                pr0n + V * slot, ptype + V * slot, nullptr,
+                                                                ptiles + (size_t)tileCap * slot);
+  if ((e = cudaMemcpyAsync(pmeta + 2 * slot, c, sizeof(c), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;   // c lives on this frame
+  pendingSlot = slot;
+  cudaMemcpyAsync(typebuf, type, (size_t)dims.nCells, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(qprev, q, sizeof(float) * dims.nCells, cudaMemcpyDeviceToDevice, s);
   return cudaGetLastError();
 }
-// after the solve: target = (q - q_prev) / sigma
+// after the solve: target = (q - q_prev) / sigma over the slot's tiles
 cudaError_t Net::collect_post(const float* q, cudaStream_t s) {
-  if (pairCap <= 0) return cudaSuccess;
+  if (pairCap <= 0 || pendingSlot < 0) return cudaSuccess;
+  const int slot = pendingSlot;
+  const size_t V = (size_t)tileCap * 1024;
   long long N = dims.nCells;
-  int slot = pairsStored % pairCap;
   cudaMemsetAsync(pscal + 2 * slot + 1, 0, sizeof(double), s);
-  k_pair_target<<<grid1(N, 256), 256, 0, s>>>(N, q, qprev, ptype + N * slot, pscal + 2 * slot, ptarget + N * slot,
-                                             pscal + 2 * slot + 1);
+  k_pair_target<<<grid1(N, 256), 256, 0, s>>>(N, q, qprev, typebuf, pscal + 2 * slot, tbuf, pscal + 2 * slot + 1);
+  // the activity (and so tiles[0]) still describes the pre-solve types
+  k_pair_pack<<<gridv((long long)tileCap * 1024, 256), 256, 0, s>>>(lv[0], tiles[0], counts, tileCap, nullptr, nullptr,
+                                                                   tbuf, nullptr, nullptr, ptarget + V * slot, nullptr);
   pairsStored++;
+  pendingSlot = -1;
+  return cudaGetLastError();
+}
+// slot p -> the dense level-0 inputs (r0n, typebuf, tbuf) at its tiles, the activity and tile lists
+cudaError_t Net::unpack(int p, cudaStream_t s) {
+  const size_t V = (size_t)tileCap * 1024;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(act[0], 0, lv[0].ntiles, s)) != cudaSuccess) return e;
+  k_pair_unpack<<<gridv((long long)tileCap * 1024, 256), 256, 0, s>>>(lv[0], ptiles + (size_t)tileCap * p, pmeta + 2 * p,
+                                                                     pr0n + V * p, ptype + V * p, ptarget + V * p,
+                                                                     r0n, typebuf, tbuf, act[0], counts + kMaxLevels);
+  if ((e = lists(s)) != cudaSuccess) return e;
+  long long n = (long long)lv[0].ntiles * 1024;
+  k_input<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, r0n, typebuf, x, nullptr);
   return cudaGetLastError();
 }
 
 // gain G = RMS of the stored targets over fluid cells (set once, before the first training step)
 cudaError_t Net::set_gain_from_pairs(cudaStream_t s) {
-  int n = std::min(pairsStored, pairCap);
+  const int n = stored();
   if (n <= 0) return cudaErrorInvalidValue;
   std::vector<double> sc((size_t)2 * n);
+  std::vector<int> meta((size_t)2 * n);
   cudaError_t e = cudaMemcpyAsync(sc.data(), pscal, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(meta.data(), pmeta, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-  // fluid counts: per pair, from the activity pass (host loop over the pairs)
   double t2 = 0, cnt = 0;
-  long long N = dims.nCells;
-  for (int p = 0; p < n; p++) {
-    if ((e = activity(ptype + N * p, s)) != cudaSuccess) return e;
-    int c4[4];
-    if ((e = cudaMemcpyAsync(c4, counts, sizeof(int) * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    t2 += sc[(size_t)2 * p + 1]; cnt += c4[3];
-  }
+  for (int p = 0; p < n; p++) { t2 += sc[(size_t)2 * p + 1]; cnt += meta[(size_t)2 * p + 1]; }
   return set_gain(cnt > 0 && t2 > 0 ? std::sqrt(t2 / cnt) : 1.0, s);
 }
 
@@ -753,19 +857,19 @@ cudaError_t Net::set_gain(double g, cudaStream_t s) {
 cudaError_t Net::sample_grad(int p, cudaStream_t s) {
   long long N = dims.nCells;
   cudaError_t e;
-  if ((e = prepare(pr0n + N * p, ptype + N * p, s)) != cudaSuccess) return e;
+  if ((e = unpack(p, s)) != cudaSuccess) return e;
   if ((e = forward(s)) != cudaSuccess) return e;
-  k_scale_copy<<<grid1(N, 256), 256, 0, s>>>(ptarget + N * p, tscaled, N, (float)(1.0 / gain));
+  k_scale_copy<<<grid1(N, 256), 256, 0, s>>>(tbuf, tscaled, N, (float)(1.0 / gain));
   long long n = (long long)lv[0].ntiles * 1024;
-  k_head_train<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, ptype + N * p, tscaled,
-                                             counts + 3, gh, grads + headOff, scal + 2);
+  k_head_train<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, db[0], params + headOff, typebuf, tscaled,
+                                             counts + kMaxLevels, gdb[0], grads + headOff, scal + 2);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return backward(s);
 }
 // zero the gradients and the loss, then add the gradients of `samples`
 // pairs drawn with a seeded generator (no parameter update)
 cudaError_t Net::accumulate(int samples, uint32_t seed, cudaStream_t s) {
-  int n = std::min(pairsStored, pairCap);
+  const int n = stored();
   if (n <= 0 || samples < 0) return cudaErrorInvalidValue;
   cudaError_t e;
   if (!(gain > 0)) { if ((e = set_gain_from_pairs(s)) != cudaSuccess) return e; }
@@ -794,7 +898,7 @@ cudaError_t Net::loss_sum(double* out, cudaStream_t s) {
   return cudaStreamSynchronize(s);
 }
 cudaError_t Net::train(int steps, int batch, double lr, uint32_t seed, double* meanLoss, cudaStream_t s) {
-  int n = std::min(pairsStored, pairCap);
+  const int n = stored();
   if (n <= 0 || steps < 0 || batch < 1) return cudaErrorInvalidValue;
   cudaError_t e;
   if (!(gain > 0)) { if ((e = set_gain_from_pairs(s)) != cudaSuccess) return e; }
@@ -816,11 +920,11 @@ cudaError_t Net::train(int steps, int batch, double lr, uint32_t seed, double* m
 cudaError_t Net::forward_pair(int p, float* outHost, cudaStream_t s) {
   long long N = dims.nCells;
   cudaError_t e;
-  if ((e = prepare(pr0n + N * p, ptype + N * p, s)) != cudaSuccess) return e;
+  if ((e = unpack(p, s)) != cudaSuccess) return e;
   if ((e = forward(s)) != cudaSuccess) return e;
   cudaMemsetAsync(outbuf, 0, sizeof(float) * N, s);
   long long n = (long long)lv[0].ntiles * 1024;
-  k_head_out<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, h, params + headOff, outbuf);
+  k_head_out<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, db[0], params + headOff, outbuf);
   if ((e = cudaMemcpyAsync(outHost, outbuf, sizeof(float) * N, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   return cudaStreamSynchronize(s);
 }
@@ -833,6 +937,47 @@ cudaError_t Net::grad_pair(int p, float* gradHost, double* loss, cudaStream_t s)
   if ((e = cudaMemcpyAsync(gradHost, grads, sizeof(float) * nparams, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   if (loss && (e = cudaMemcpyAsync(loss, scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
   return cudaStreamSynchronize(s);
+}
+// dense copies of pair p: its tiles' voxels, zero (air) elsewhere
+cudaError_t Net::get_pair(int p, float* r0nHost, uint8_t* typeHost, float* targetHost, cudaStream_t s) {
+  const long long N = dims.nCells;
+  cudaError_t e;
+  cudaMemsetAsync(r0n, 0, sizeof(float) * N, s);
+  cudaMemsetAsync(typebuf, WS_AIR, (size_t)N, s);
+  cudaMemsetAsync(tbuf, 0, sizeof(float) * N, s);
+  if ((e = unpack(p, s)) != cudaSuccess) return e;
+  if (r0nHost && (e = cudaMemcpyAsync(r0nHost, r0n, sizeof(float) * N, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if (typeHost && (e = cudaMemcpyAsync(typeHost, typebuf, (size_t)N, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if (targetHost && (e = cudaMemcpyAsync(targetHost, tbuf, sizeof(float) * N, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  return cudaStreamSynchronize(s);
+}
+// a pair from dense host arrays (sigma 1): stored over the tiles its fluid cells make active
+cudaError_t Net::put_pair(const float* r0nHost, const uint8_t* typeHost, const float* targetHost, cudaStream_t s) {
+  const long long N = dims.nCells;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(r0n, r0nHost, sizeof(float) * N, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(typebuf, typeHost, (size_t)N, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(tbuf, targetHost, sizeof(float) * N, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if (pairCap <= 0 && (e = reserve_pairs(1, typebuf, s)) != cudaSuccess) return e;
+  const int slot = pairsStored % pairCap;
+  const size_t V = (size_t)tileCap * 1024;
+  if ((e = activity(typebuf, s)) != cudaSuccess) return e;
+  int c[2];
+  if ((e = cudaMemcpyAsync(&c[0], counts, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(&c[1], counts + kMaxLevels, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  if (c[0] > tileCap) return cudaErrorInvalidValue;
+  double t2 = 0;
+  for (long long i = 0; i < N; i++) if (typeHost[i] == WS_FLUID) t2 += (double)targetHost[i] * targetHost[i];
+  const double sc[2] = { 1.0, t2 };
+  k_pair_pack<<<gridv((long long)c[0] * 1024, 256), 256, 0, s>>>(lv[0], tiles[0], counts, tileCap, r0n, typebuf, tbuf,
+                                                                pr0n + V * slot, ptype + V * slot, ptarget + V * slot,
+                                                                ptiles + (size_t)tileCap * slot);
+  if ((e = cudaMemcpyAsync(pmeta + 2 * slot, c, sizeof(c), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(pscal + 2 * slot, sc, sizeof(sc), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  pairsStored++;
+  return cudaSuccess;
 }
 
 }  // namespace unet

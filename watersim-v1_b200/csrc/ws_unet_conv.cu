@@ -78,7 +78,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 
 template <int COUT> struct ConvShape {
-  static constexpr int ZT = COUT <= 32 ? 8 : COUT <= 64 ? 4 : 2;
+  static constexpr int ZT = COUT <= 32 ? 8 : COUT <= 64 ? 4 : COUT <= 128 ? 2 : 1;
   static constexpr int HX = kTX + 2, HY = kTY + 2, HZ = ZT + 2;
   static constexpr int HV = HX * HY * HZ;           // halo voxels
   static constexpr int KSTR = HV * 16;              // bytes of one 8-channel halo chunk
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
   // N = 2 and 3 COUT (two or three z taps); with ZT = 2 at most two z taps meet one plane
   constexpr uint32_t idesc2 = idesc_bf16_m128(2 * COUT);
   constexpr uint32_t idesc3 = idesc_bf16_m128((ZT >= 3 ? 3 : 2) * COUT);
-  static_assert((ZT >= 3 ? 3 : 2) * COUT <= 256 && COUT % 16 == 0, "MMA N out of range");
+  static_assert((ZT >= 3 ? 3 : ZT) * COUT <= 256 && COUT % 16 == 0, "MMA N out of range");
   uint32_t phase = 0;
   bool pending = false;
 
@@ -319,7 +319,9 @@ __global__ void __launch_bounds__(256) k_conv3(ConvArgs a) {
 // issued back to back (taps innermost: 27 independent accumulators of 16
 // columns) with descriptors formed by adding 16-byte offsets to two base
 // descriptors, and drained once per item.
-struct DwTcArgs { ConvArgs src; const bf16* dz; int cout; float* dw; float* db; };
+// one pass covers output channels coOff .. coOff + cout - 1 (cout <= 64) of a
+// dZ with dzStride channels per voxel
+struct DwTcArgs { ConvArgs src; const bf16* dz; int cout, dzStride, coOff; float* dw; float* db; };
 constexpr int kDzPlane = 128 * 16;                // bytes of one plane of one 8-channel chunk of dZ
 constexpr int kDzChunk = kTZ * kDzPlane;          // one 8-channel chunk of the tile's dZ
 constexpr int kDwTcSmem = 2 * ConvShape<16>::KSTR + 8 * kDzChunk;
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(256, 1) k_dw_tc(DwTcArgs A) {
       const int c = i / (kTZ * 128), r = i - c * (kTZ * 128), z = r >> 7, m = r & 127;
       const int gx = X0 + (m & 7), gy = Y0 + (m >> 3), gz = Z0 + z;
       const bool in = gx < a.nx && gy < a.ny && gz < a.nz;
-      const bf16* src = in ? A.dz + (((size_t)gz * a.ny + gy) * a.nx + gx) * cout + c * 8 : A.dz;
+      const bf16* src = in ? A.dz + (((size_t)gz * a.ny + gy) * a.nx + gx) * A.dzStride + A.coOff + c * 8 : A.dz;
       cp_async16(zbase + (uint32_t)(c * kDzChunk + z * kDzPlane + m * 16), src, in ? 16u : 0u);
     }
     cp_async_wait_all();
@@ -413,11 +415,11 @@ __global__ void __launch_bounds__(256, 1) k_dw_tc(DwTcArgs A) {
         if (co < cout) {
 #pragma unroll
           for (int i = 0; i < 16; i++)
-            atomicAdd(A.dw + ((size_t)co * cin + kk * 16 + i) * 27 + t, __uint_as_float(r[i]));
+            atomicAdd(A.dw + ((size_t)(A.coOff + co) * cin + kk * 16 + i) * 27 + t, __uint_as_float(r[i]));
         }
       }
     }
-    if (kk == 0 && (int)threadIdx.x < cout) atomicAdd(A.db + threadIdx.x, bsum);
+    if (kk == 0 && (int)threadIdx.x < cout) atomicAdd(A.db + A.coOff + threadIdx.x, bsum);
     fence_before();
     __syncthreads();                                 // accumulators and staged operands free for the next item
   }
@@ -430,13 +432,15 @@ __global__ void __launch_bounds__(256, 1) k_dw_tc(DwTcArgs A) {
 }
 cudaError_t launch_dw_tc(const ConvArgs& src, const bf16* dz, int cout, float* dw, float* db, int maxItems,
                          cudaStream_t s) {
-  if (((src.c0 + src.c1) & 15) || (cout & 7) || cout > 64) return cudaErrorInvalidValue;
+  if (((src.c0 + src.c1) & 15) || (cout & 7) || cout > 128) return cudaErrorInvalidValue;
   static int smCount = 0;
   if (!smCount) { int dev = 0; cudaGetDevice(&dev); cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev); }
-  DwTcArgs A{src, dz, cout, dw, db};
   const unsigned grid = (unsigned)std::min(maxItems, smCount);     // one CTA per SM: 512 TMEM columns each
   if (grid == 0) return cudaSuccess;
-  k_dw_tc<<<grid, 256, kDwTcSmem, s>>>(A);
+  for (int off = 0; off < cout; off += 64) {       // the A operand holds 64 output channels per pass
+    DwTcArgs A{src, dz, std::min(64, cout - off), cout, off, dw, db};
+    k_dw_tc<<<grid, 256, kDwTcSmem, s>>>(A);
+  }
   return cudaGetLastError();
 }
 
@@ -450,19 +454,23 @@ cudaError_t conv3_init() {
   if ((e = set_smem<48>()) != cudaSuccess) return e;
   if ((e = set_smem<64>()) != cudaSuccess) return e;
   if ((e = set_smem<96>()) != cudaSuccess) return e;
+  if ((e = set_smem<128>()) != cudaSuccess) return e;
+  if ((e = set_smem<192>()) != cudaSuccess) return e;
   // the weight-gradient kernel holds more than half an SM's shared memory: one CTA per SM
   return cudaFuncSetAttribute(k_dw_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kDwTcSmem);
 }
 int conv3_zt(int cout) {
   switch (cout) {
     case 16: return ConvShape<16>::ZT; case 32: return ConvShape<32>::ZT; case 48: return ConvShape<48>::ZT;
-    case 64: return ConvShape<64>::ZT; case 96: return ConvShape<96>::ZT; default: return 0;
+    case 64: return ConvShape<64>::ZT; case 96: return ConvShape<96>::ZT; case 128: return ConvShape<128>::ZT;
+    case 192: return ConvShape<192>::ZT; default: return 0;
   }
 }
 size_t conv3_smem_bytes(int cout) {
   switch (cout) {
     case 16: return ConvShape<16>::SMEM; case 32: return ConvShape<32>::SMEM; case 48: return ConvShape<48>::SMEM;
-    case 64: return ConvShape<64>::SMEM; case 96: return ConvShape<96>::SMEM; default: return 0;
+    case 64: return ConvShape<64>::SMEM; case 96: return ConvShape<96>::SMEM; case 128: return ConvShape<128>::SMEM;
+    case 192: return ConvShape<192>::SMEM; default: return 0;
   }
 }
 cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t s) {
@@ -485,6 +493,8 @@ cudaError_t launch_conv3(const ConvArgs& a, int cout, int maxTiles, cudaStream_t
     case 48: k_conv3<48><<<grid, 256, sm, s>>>(a); break;
     case 64: k_conv3<64><<<grid, 256, sm, s>>>(a); break;
     case 96: k_conv3<96><<<grid, 256, sm, s>>>(a); break;
+    case 128: k_conv3<128><<<grid, 256, sm, s>>>(a); break;
+    case 192: k_conv3<192><<<grid, 256, sm, s>>>(a); break;
   }
   return cudaGetLastError();
 }

@@ -158,7 +158,7 @@ SYMBOLS = ["ws_create", "ws_destroy", "ws_last_error", "ws_version", "ws_set_par
            "ws_wave_impulse", "ws_dry_land_fraction", "ws_sample_vel", "ws_terrain_radius_at", "ws_ocean_point",
            "ws_synchronize", "ws_get_stream", "ws_launch_count", "ws_time_kernel", "ws_probe_wait",
            "ws_residual_noalloc", "ws_upload_state", "ws_download_state",
-           "ws_unet_init", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
+           "ws_unet_init", "ws_unet_init_levels", "ws_unet_collect", "ws_unet_enable", "ws_unet_train", "ws_unet_get_info",
            "ws_unet_get_weights", "ws_unet_set_weights", "ws_unet_set_gain", "ws_unet_get_pair",
            "ws_unet_put_pair", "ws_unet_forward_pair", "ws_unet_grad_pair", "ws_unet_probe", "ws_unet_time",
            "ws_unet_accumulate", "ws_unet_grads", "ws_unet_apply", "ws_snapshot", "ws_restore",
@@ -204,7 +204,7 @@ def load_library(path=None):
         "ws_time_kernel": [h, i32, i32, C.POINTER(C.c_double)],
         "ws_probe_wait": [h, C.c_int64],
         "ws_upload_state": [h, C.POINTER(WsHostArrays)], "ws_download_state": [h, C.POINTER(WsHostArrays)],
-        "ws_unet_init": [h, u32], "ws_unet_collect": [h, i32], "ws_unet_enable": [h, i32],
+        "ws_unet_init": [h, u32], "ws_unet_init_levels": [h, u32, i32], "ws_unet_collect": [h, i32], "ws_unet_enable": [h, i32],
         "ws_unet_train": [h, i32, i32, d, u32, C.POINTER(C.c_double)],
         "ws_unet_get_info": [h, C.POINTER(WsUnetInfo)],
         "ws_unet_get_weights": [h, vp, i64], "ws_unet_set_weights": [h, vp, i64], "ws_unet_set_gain": [h, d],
@@ -450,8 +450,8 @@ class FluidSolver:
         self._check(self._L.ws_download_state(self._h, C.byref(a)))
 
     # ---- learned warm start of the pressure solve (no reference counterpart)
-    def unet_init(self, seed=1):
-        self._check(self._L.ws_unet_init(self._h, int(seed)))
+    def unet_init(self, seed=1, levels=3):
+        self._check(self._L.ws_unet_init_levels(self._h, int(seed), int(levels)))
 
     def unet_collect(self, capacity):
         self._check(self._L.ws_unet_collect(self._h, int(capacity)))
