@@ -750,6 +750,7 @@ def run_frames(args, rank, world, local_rank):
     clocks.start()
     time.sleep(0.5)
     ms, subs, evap = [], 0, []
+    launches = 0
     # a state that fits in L2 is evicted between timed frames by writing a
     # buffer twice the L2 size on the solver's stream, outside the events
     flush = (torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -760,9 +761,11 @@ def run_frames(args, rank, world, local_rank):
                 flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        l0 = fs.launch_count()
         e0.record(st)
         fs.step(1 / 60)                  # synchronous: returns after the frame's counters are read
         e1.record(st)
+        launches += fs.launch_count() - l0
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
         subs += fs.scalars.substepsLast
@@ -796,7 +799,7 @@ def run_frames(args, rank, world, local_rank):
                            "evaporations_last_tick": evap[-1], "vapor": s.vaporCount,
                            "sor_iterations_last": s.sorIters, "sor_path": SOR_PATHS.get(s.sorPath, "unknown"),
                            "pass_ms": passes},
-               "gpu_launches": None, "clocks": clk}
+               "gpu_launches": int(launches), "clocks": clk}
     return out, fs
 
 

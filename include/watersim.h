@@ -176,9 +176,17 @@ ws_status ws_set_nparticles(ws_handle* h, int32_t nP);
  *      frame (js/gpu/gpusim.js:568-650). field[f] is the host buffer of
  *      particle field f (WS_F_PX..WS_F_PDEPTH, element type as listed
  *      above) or NULL to skip it; count elements from element 0 move per
- *      field. All copies are queued on the handle's stream and the call
- *      returns after one synchronisation, so the buffers are only read (or
- *      written) during the call. Pinned buffers copy at full link speed. */
+ *      field. Pinned buffers copy at full link speed.
+ *      The fields no substep reads or writes (WS_F_PLIGHT, WS_F_PDEPTH,
+ *      WS_F_PPH, and WS_F_PT while no vapour parcel can exist) move on a
+ *      second stream beside the substeps: ws_upload_state returns once the
+ *      other fields are on the device and keeps reading those buffers until
+ *      the next call into the library other than ws_substep or
+ *      ws_download_state, so the caller leaves them unchanged until then;
+ *      ws_download_state copies them without waiting for the substeps when
+ *      only substeps ran since the last upload or download, and returns
+ *      with every buffer written. Every other entry point orders its work
+ *      after these copies. */
 #define WS_NUM_PARTICLE_FIELDS 16
 typedef struct {
   int64_t count;

@@ -26,6 +26,13 @@ struct ws_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;          // the SOR list build beside the learned warm start
   cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  // host copies of the particle fields no substep kernel reads or writes
+  // (ws_upload_state / ws_download_state) run on their own stream beside the
+  // substep; every other entry point joins them into the main stream first
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t evCopy = nullptr, evMain = nullptr;
+  bool copyPending = false;             // copies on copyStream not yet joined
+  bool mainTouched = true;              // main-stream work other than substeps since the last full sync
   Dims d{};
   ws_params P{};
   ws_scalars S{};
@@ -160,6 +167,22 @@ static void force_full_pass(ws_handle* h) {
 }
 static PartsDev parts_of(ws_handle* h) { PartsDev P = h->parts; P.nP = h->S.nP; return P; }
 
+// Fields no substep kernel reads or writes: the light and depth channels and
+// the phase, and the temperature while no vapour parcel can exist (only the
+// vapour pass reads it). Their copies may run beside the substep.
+static bool substep_free(const ws_handle* h, int f) {
+  return f == WS_F_PLIGHT || f == WS_F_PDEPTH || f == WS_F_PPH || (f == WS_F_PT && !h->vaporPossible);
+}
+// pending copies of substep-free fields into the main stream (every entry
+// point but ws_substep and the state copies calls it first)
+static void join_copies(ws_handle* h) {
+  if (!h) return;
+  if (h->copyPending && cudaEventRecord(h->evCopy, h->copyStream) == cudaSuccess)
+    cudaStreamWaitEvent(h->stream, h->evCopy, 0);
+  h->copyPending = false;
+  h->mainTouched = true;
+}
+
 extern "C" const char* ws_version(void) { return "watersim-b200 0.1 (sm_100a)"; }
 
 extern "C" const char* ws_last_error(const ws_handle* h) {
@@ -217,6 +240,9 @@ static void free_all(ws_handle* h) {
   if (h->redHost) cudaFreeHost(h->redHost);
   if (h->evFork) cudaEventDestroy(h->evFork);
   if (h->evJoin) cudaEventDestroy(h->evJoin);
+  if (h->evCopy) cudaEventDestroy(h->evCopy);
+  if (h->evMain) cudaEventDestroy(h->evMain);
+  if (h->copyStream) cudaStreamDestroy(h->copyStream);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
@@ -242,10 +268,16 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evCopy, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evMain, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     ws_status r = fail_cuda(h, e, "cudaStreamCreate");
     if (h->evFork) cudaEventDestroy(h->evFork);
     if (h->evJoin) cudaEventDestroy(h->evJoin);
+    if (h->evCopy) cudaEventDestroy(h->evCopy);
+    if (h->evMain) cudaEventDestroy(h->evMain);
+    if (h->copyStream) cudaStreamDestroy(h->copyStream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h; return r;
@@ -332,6 +364,7 @@ extern "C" ws_status ws_destroy(ws_handle* h) {
   collect_async(h);
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->copyStream) cudaStreamSynchronize(h->copyStream);
   free_all(h);
   delete h;
   return WS_OK;
@@ -380,6 +413,7 @@ static ws_status ensure_gravity(ws_handle* h) {
 
 extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !s) return WS_ERR_INVALID;
   ws_status st0 = sync_status(h); if (st0) return st0;
   uint32_t rng[4];
@@ -391,6 +425,7 @@ extern "C" ws_status ws_get_scalars(ws_handle* h, ws_scalars* s) {
 }
 extern "C" ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !s) return WS_ERR_INVALID;
   if (s->nP < 0 || s->nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
   int cap = h->capacity;
@@ -403,6 +438,7 @@ extern "C" ws_status ws_set_scalars(ws_handle* h, const ws_scalars* s) {
 }
 extern "C" ws_status ws_set_nparticles(ws_handle* h, int32_t nP) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   if (nP < 0 || nP > h->capacity) return fail(h, WS_ERR_RANGE, "nP exceeds the particle capacity");
   h->S.nP = nP;
@@ -478,6 +514,7 @@ extern "C" ws_status ws_field_info(const ws_handle* hc, ws_field f, int64_t* cou
 }
 extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host, int64_t count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || (!host && count)) return WS_ERR_INVALID;
   FieldRef r;
   if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
@@ -492,6 +529,7 @@ extern "C" ws_status ws_upload_field(ws_handle* h, ws_field f, const void* host,
 }
 extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int64_t count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || (!host && count)) return WS_ERR_INVALID;
   FieldRef r;
   if (!field_ref(h, f, r)) return fail(h, WS_ERR_INVALID, "unknown field");
@@ -511,21 +549,42 @@ extern "C" ws_status ws_download_field(ws_handle* h, ws_field f, void* host, int
 }
 
 // one queued copy per particle field, one synchronisation for all of them
+// Upload: the substep's fields on the main stream, which returns once they
+// are on the device; the substep-free fields on the copy stream, after any
+// main-stream work still reading them, left running beside the next
+// substeps. Download: the substep's fields after the main stream's work;
+// the substep-free fields, when only substeps ran since the last full sync,
+// straight away on the copy stream (no substep changes them); both streams
+// are synchronised before returning.
 static ws_status state_copy(ws_handle* h, const ws_host_arrays* a, bool up) {
   if (!h || !a) return WS_ERR_INVALID;
   if (a->count < 0 || a->count > h->capacity) return fail(h, WS_ERR_RANGE, "count exceeds the particle capacity");
+  if (up && a->field[WS_F_PFLAG] && !h->vaporPossible &&
+      any_vapor_flag((const uint8_t*)a->field[WS_F_PFLAG], a->count))
+    h->vaporPossible = true;
+  const bool beside = up || !h->mainTouched;
+  if (beside && h->mainTouched) {                 // copy stream after main-stream work that may use the fields
+    WS_TRY(cudaEventRecord(h->evMain, h->stream));
+    WS_TRY(cudaStreamWaitEvent(h->copyStream, h->evMain, 0));
+  }
   for (int f = 0; f < WS_NUM_PARTICLE_FIELDS; f++) {
     if (!a->field[f]) continue;
     FieldRef r;
     field_ref(h, (ws_field)f, r);
     size_t bytes = (size_t)a->count * r.elem;
-    if (up) WS_TRY(cudaMemcpyAsync(r.ptr, a->field[f], bytes, cudaMemcpyHostToDevice, h->stream));
-    else WS_TRY(cudaMemcpyAsync(a->field[f], r.ptr, bytes, cudaMemcpyDeviceToHost, h->stream));
+    cudaStream_t st = beside && substep_free(h, f) ? h->copyStream : h->stream;
+    if (up) WS_TRY(cudaMemcpyAsync(r.ptr, a->field[f], bytes, cudaMemcpyHostToDevice, st));
+    else WS_TRY(cudaMemcpyAsync(a->field[f], r.ptr, bytes, cudaMemcpyDeviceToHost, st));
   }
   WS_TRY(cudaStreamSynchronize(h->stream));
-  if (up && a->field[WS_F_PFLAG] && !h->vaporPossible &&
-      any_vapor_flag((const uint8_t*)a->field[WS_F_PFLAG], a->count))
-    h->vaporPossible = true;
+  if (up) {
+    h->copyPending = true;
+    h->mainTouched = false;
+  } else {
+    WS_TRY(cudaStreamSynchronize(h->copyStream));
+    h->copyPending = false;
+    h->mainTouched = false;
+  }
   return WS_OK;
 }
 extern "C" ws_status ws_upload_state(ws_handle* h, const ws_host_arrays* a) {
@@ -568,6 +627,7 @@ static ws_status terrain_to_device(ws_handle* h) {
 
 extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double seaLevel) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   wsterrain::GenInput in{seed, h->S.coreR, seaLevel, h->S.bumpiness, h->d.dx, h->d.cx, h->d.cy, h->d.cz, h->d.nx, h->stream};
   int r = wsterrain::generate(in, h->hostTerrain, h->err);
@@ -578,6 +638,7 @@ extern "C" ws_status ws_generate_terrain(ws_handle* h, uint32_t seed, double sea
 
 extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !t || t->n < 2 || !t->solid || !t->R) return WS_ERR_INVALID;
   force_full_pass(h);                            // the static cell types change
   wsterrain::Terrain& T = h->hostTerrain;
@@ -590,6 +651,7 @@ extern "C" ws_status ws_upload_terrain(ws_handle* h, const ws_terrain* t) {
 
 extern "C" ws_status ws_download_terrain(ws_handle* h, uint8_t* solid, float* R, double meta[4]) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
   const wsterrain::Terrain& T = h->hostTerrain;
@@ -610,6 +672,7 @@ static wsterrain::FillInput fill_input(ws_handle* h, double depth) {
 
 extern "C" ws_status ws_water_volume(ws_handle* h, double depth, double* volume) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !volume) return WS_ERR_INVALID;
   if (!h->hasTerrain) return fail(h, WS_ERR_STATE, "no terrain");
   *volume = wsterrain::water_volume(h->hostTerrain, fill_input(h, depth));
@@ -621,6 +684,7 @@ static ws_status splat_and_iso(ws_handle* h);
 // _resetWaterSphere, js/solver.js:651-731
 extern "C" ws_status ws_reset_water(ws_handle* h, double depth) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   double R2 = h->S.coreR + depth;
   h->S.oceanR = R2;
@@ -683,6 +747,7 @@ static ws_status mt_volume(ws_handle* h, double iso, double* vol, int64_t* cnt) 
 }
 extern "C" ws_status ws_mt_volume(ws_handle* h, double iso, double* volume, int64_t* vertexCount) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   return mt_volume(h, iso, volume, vertexCount);
 }
@@ -699,6 +764,7 @@ static ws_status autotune(ws_handle* h, double* iso) {
 }
 extern "C" ws_status ws_autotune_iso(ws_handle* h, double* iso) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !iso) return WS_ERR_INVALID;
   return autotune(h, iso);
 }
@@ -720,6 +786,7 @@ static ws_status particle_reduce(ws_handle* h, int mode, double mp, double out[3
 }
 extern "C" ws_status ws_kinetic_energy(ws_handle* h, double* ke) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !ke) return WS_ERR_INVALID;
   double o[3];
   ws_status s = particle_reduce(h, 0, 1000 * h->S.particleVolume, o); if (s) return s;
@@ -729,6 +796,7 @@ extern "C" ws_status ws_kinetic_energy(ws_handle* h, double* ke) {
 // earthCensus, js/main.js:176-186: counts are exact, fractions in FP64
 extern "C" ws_status ws_census(ws_handle* h, double fr[3]) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !fr) return WS_ERR_INVALID;
   double o[3];
   ws_status s = particle_reduce(h, 1, 0, o); if (s) return s;
@@ -738,6 +806,7 @@ extern "C" ws_status ws_census(ws_handle* h, double fr[3]) {
 }
 extern "C" ws_status ws_residual(ws_handle* h, double* relres) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !relres) return WS_ERR_INVALID;
   launch_residual(h->d, grid_of(h), h->diag8, h->partials, h->st, nullptr, h->stream);
   ws_status s = check_launch(h, 2); if (s) return s;
@@ -1169,6 +1238,7 @@ static ws_status step_frame(ws_handle* h, double dtFrame) {
 }
 extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !(dtFrame > 0)) return WS_ERR_INVALID;
   return step_frame(h, dtFrame);
 }
@@ -1214,6 +1284,7 @@ extern "C" ws_status ws_step_wait(ws_handle* h) {
 
 extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = WS_OK;
@@ -1277,6 +1348,7 @@ static ws_status ensure_balls(ws_handle* h) {
 }
 extern "C" ws_status ws_add_ball(ws_handle* h, double x, double y, double z, double r, double rho) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   if (!(r > 0) || !(rho > 0)) return fail(h, WS_ERR_INVALID, "ball radius and density must be positive");
   if (h->nBalls >= WS_MAX_BALLS) return fail(h, WS_ERR_RANGE, "too many balls");
@@ -1291,6 +1363,7 @@ extern "C" ws_status ws_add_ball(ws_handle* h, double x, double y, double z, dou
 }
 extern "C" ws_status ws_get_balls(ws_handle* h, ws_ball* out, int32_t max, int32_t* count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !count || (max > 0 && !out)) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1301,6 +1374,7 @@ extern "C" ws_status ws_get_balls(ws_handle* h, ws_ball* out, int32_t max, int32
 }
 extern "C" ws_status ws_set_balls(ws_handle* h, const ws_ball* in, int32_t count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || count < 0 || (count > 0 && !in)) return WS_ERR_INVALID;
   if (count > WS_MAX_BALLS) return fail(h, WS_ERR_RANGE, "too many balls");
   cudaSetDevice(h->device);
@@ -1318,6 +1392,7 @@ extern "C" ws_status ws_set_balls(ws_handle* h, const ws_ball* in, int32_t count
 extern "C" ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy, double cz, double R,
                                              double fx, double fy, double fz) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   launch_impulse_sphere(parts_of(h), cx, cy, cz, R, fx, fy, fz, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
@@ -1326,6 +1401,7 @@ extern "C" ws_status ws_apply_impulse_sphere(ws_handle* h, double cx, double cy,
 extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, double vx, double vy,
                                 double vz, double R, double dt) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   launch_stir_at(parts_of(h), cx, cy, cz, vx, vy, vz, R, dt, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
@@ -1335,6 +1411,7 @@ extern "C" ws_status ws_stir_at(ws_handle* h, double cx, double cy, double cz, d
 // stream: theta and phi of the bulge direction, then one draw per particle.
 extern "C" ws_status ws_wave_impulse(ws_handle* h, double dvx) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !std::isfinite(dvx)) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   uint32_t st = h->S.stirS;
@@ -1350,6 +1427,7 @@ extern "C" ws_status ws_wave_impulse(ws_handle* h, double dvx) {
 // without terrain, as the reference
 extern "C" ws_status ws_dry_land_fraction(ws_handle* h, double* out) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !out) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   if (!h->terr.has) { *out = 0; return WS_OK; }
@@ -1367,6 +1445,7 @@ extern "C" ws_status ws_dry_land_fraction(ws_handle* h, double* out) {
 static const long long kQueryChunk = 1 << 16;
 static ws_status query_points(ws_handle* h, const double* xyz, int64_t n, double* out, int perPoint, int kind) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || n < 0 || (n > 0 && (!xyz || !out))) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   if (!h->queryBuf) WS_TRY(cudaMalloc(&h->queryBuf, sizeof(double) * 6 * kQueryChunk));
@@ -1393,6 +1472,7 @@ extern "C" ws_status ws_terrain_radius_at(ws_handle* h, const double* xyz, int64
 // oceanPoint (js/solver.js:591-608) on the seeded stir stream
 extern "C" ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !xyz) return WS_ERR_INVALID;
   if (!h->terr.has) return fail(h, WS_ERR_STATE, "oceanPoint needs terrain");
   cudaSetDevice(h->device);
@@ -1412,6 +1492,7 @@ extern "C" ws_status ws_ocean_point(ws_handle* h, double minDepth, double* xyz) 
 // the tangent construction are part of the workload definition.
 extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !(sigma > 0)) return WS_ERR_INVALID;
   uint32_t st = h->S.stirS;
   st = lcg_next(st); double u1 = st / 4294967296.0 * 2 - 1;
@@ -1435,17 +1516,20 @@ extern "C" ws_status ws_stir_gaussian(ws_handle* h, double sigma, double peak) {
 
 extern "C" ws_status ws_synchronize(ws_handle* h) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   return sync_status(h);
 }
 extern "C" ws_status ws_get_stream(ws_handle* h, void** s) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !s) return WS_ERR_INVALID;
   *s = (void*)h->stream;
   return WS_OK;
 }
 extern "C" ws_status ws_launch_count(ws_handle* h, int64_t* n) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !n) return WS_ERR_INVALID;
   *n = h->launches;
   return WS_OK;
@@ -1458,6 +1542,7 @@ __global__ void k_probe_wait(DevStatus* st, long long polls) {
 }
 extern "C" ws_status ws_probe_wait(ws_handle* h, int64_t polls) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || polls < 1 || polls > 100000000) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1468,6 +1553,7 @@ extern "C" ws_status ws_probe_wait(ws_handle* h, int64_t polls) {
 
 extern "C" ws_status ws_time_kernel(ws_handle* h, int32_t kernel, int32_t reps, double* us) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !us || reps < 1) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   force_full_pass(h);
@@ -1527,6 +1613,7 @@ static ws_status net_ready(ws_handle* h) {
 }
 extern "C" ws_status ws_unet_init_levels(ws_handle* h, uint32_t seed, int32_t levels) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   if (levels < 3 || levels > unet::kMaxLevels) return fail(h, WS_ERR_INVALID, "levels must be 3 or 4");
   cudaSetDevice(h->device);
@@ -1549,6 +1636,7 @@ extern "C" ws_status ws_unet_init_levels(ws_handle* h, uint32_t seed, int32_t le
 extern "C" ws_status ws_unet_init(ws_handle* h, uint32_t seed) { return ws_unet_init_levels(h, seed, 3); }
 extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (capacity < 0) return fail(h, WS_ERR_RANGE, "negative pair capacity");
   if (capacity > 0) {
@@ -1560,6 +1648,7 @@ extern "C" ws_status ws_unet_collect(ws_handle* h, int32_t capacity) {
 }
 extern "C" ws_status ws_unet_enable(ws_handle* h, int32_t on) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (on && !(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain: train it or call ws_unet_set_gain");
   h->unetOn = on != 0;
@@ -1568,6 +1657,7 @@ extern "C" ws_status ws_unet_enable(ws_handle* h, int32_t on) {
 extern "C" ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, double lr, uint32_t seed,
                                    double* mean_loss) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
   if (steps < 0 || batch < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad training arguments");
@@ -1580,6 +1670,7 @@ extern "C" ws_status ws_unet_train(ws_handle* h, int32_t steps, int32_t batch, d
 }
 extern "C" ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !out) return WS_ERR_INVALID;
   std::memset(out, 0, sizeof(*out));
   if (!h->net) return WS_OK;
@@ -1591,6 +1682,7 @@ extern "C" ws_status ws_unet_get_info(ws_handle* h, ws_unet_info* out) {
 }
 extern "C" ws_status ws_unet_get_weights(ws_handle* h, float* host, int64_t count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
   WS_TRY(cudaMemcpy(host, h->net->params, sizeof(float) * count, cudaMemcpyDeviceToHost));
@@ -1598,6 +1690,7 @@ extern "C" ws_status ws_unet_get_weights(ws_handle* h, float* host, int64_t coun
 }
 extern "C" ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_t count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!host || count != h->net->nparams) return fail(h, WS_ERR_RANGE, "weight count mismatch");
   WS_TRY(h->net->set_weights(host, h->stream));
@@ -1606,6 +1699,7 @@ extern "C" ws_status ws_unet_set_weights(ws_handle* h, const float* host, int64_
 }
 extern "C" ws_status ws_unet_set_gain(ws_handle* h, double gain) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!(gain > 0)) return fail(h, WS_ERR_INVALID, "gain must be positive");
   WS_TRY(h->net->set_gain(gain, h->stream));
@@ -1613,6 +1707,7 @@ extern "C" ws_status ws_unet_set_gain(ws_handle* h, double gain) {
 }
 extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uint8_t* types, float* target) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
   if (idx < 0 || idx >= n.stored()) return fail(h, WS_ERR_RANGE, "pair index");
@@ -1621,6 +1716,7 @@ extern "C" ws_status ws_unet_get_pair(ws_handle* h, int32_t idx, float* r0n, uin
 }
 extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint8_t* types, const float* target) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   unet::Net& n = *h->net;
   if (!r0n || !types || !target) return WS_ERR_INVALID;
@@ -1631,6 +1727,7 @@ extern "C" ws_status ws_unet_put_pair(ws_handle* h, const float* r0n, const uint
 }
 extern "C" ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!out || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
   WS_TRY(h->net->forward_pair(idx, out, h->stream));
@@ -1638,6 +1735,7 @@ extern "C" ws_status ws_unet_forward_pair(ws_handle* h, int32_t idx, float* out)
 }
 extern "C" ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, double* loss) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!grads || idx < 0 || idx >= std::min(h->net->pairsStored, h->net->pairCap)) return fail(h, WS_ERR_RANGE, "pair index");
   WS_TRY(h->net->grad_pair(idx, grads, loss, h->stream));
@@ -1647,6 +1745,7 @@ extern "C" ws_status ws_unet_grad_pair(ws_handle* h, int32_t idx, float* grads, 
 // system of the current face velocities (call after the forces stage)
 extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* relres_pred) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!(h->net->gain > 0)) return fail(h, WS_ERR_STATE, "network has no output gain");
   GridDev g = grid_of(h);
@@ -1667,6 +1766,7 @@ extern "C" ws_status ws_unet_probe(ws_handle* h, double* relres_prev, double* re
 // (writes q), 1 one training step on a stored pair (batch 1, learning rate 0)
 extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, double* ms) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!ms || reps < 1 || what < 0 || what > 1) return WS_ERR_INVALID;
   if (what == 1 && h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
@@ -1692,6 +1792,7 @@ extern "C" ws_status ws_unet_time(ws_handle* h, int32_t what, int32_t reps, doub
 // all-reduce on its communicator), then every rank applies the same step
 extern "C" ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t seed, double* loss_sum) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (h->net->pairsStored <= 0) return fail(h, WS_ERR_STATE, "no training pairs stored");
   if (samples < 1) return fail(h, WS_ERR_INVALID, "samples must be positive");
@@ -1703,6 +1804,7 @@ extern "C" ws_status ws_unet_accumulate(ws_handle* h, int32_t samples, uint32_t 
 }
 extern "C" ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* count) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!device_ptr || !count) return WS_ERR_INVALID;
   *device_ptr = h->net->grads;
@@ -1711,6 +1813,7 @@ extern "C" ws_status ws_unet_grads(ws_handle* h, void** device_ptr, int64_t* cou
 }
 extern "C" ws_status ws_unet_apply(ws_handle* h, double lr, int32_t total_samples) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (total_samples < 1 || !(lr >= 0)) return fail(h, WS_ERR_INVALID, "bad learning rate or sample count");
   WS_TRY(h->net->apply(lr, total_samples, h->stream));
@@ -1742,6 +1845,7 @@ int64_t snap_bytes(const ws_handle* h, int terrainN) {
 
 extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !size) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1782,6 +1886,7 @@ extern "C" ws_status ws_snapshot(ws_handle* h, void* buf, int64_t capacity, int6
 
 extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !buf) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1837,6 +1942,7 @@ extern "C" ws_status ws_restore(ws_handle* h, const void* buf, int64_t size) {
 // network blob: header, gain, Adam step count, then params, Adam m and v (FP32)
 extern "C" ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int64_t* size) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!size) return WS_ERR_INVALID;
   const int64_t n = h->net->nparams, need = 8 + 8 + 8 + 8 + 3 * 4 * n;
@@ -1856,6 +1962,7 @@ extern "C" ws_status ws_unet_save(ws_handle* h, void* buf, int64_t capacity, int
 }
 extern "C" ws_status ws_unet_load(ws_handle* h, const void* buf, int64_t size) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   ws_status s = net_ready(h); if (s) return s;
   if (!buf) return WS_ERR_INVALID;
   const int64_t n = h->net->nparams;
@@ -1923,6 +2030,7 @@ static ws_status mesh_download(ws_handle* h, const MeshBuf& mb, float* pos, floa
 // the current density field (ws_stage SPLAT / splatDensity) at iso
 extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices, double* volume) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1931,11 +2039,13 @@ extern "C" ws_status ws_surface_mesh(ws_handle* h, double iso, int64_t* vertices
 }
 extern "C" ws_status ws_surface_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   return mesh_download(h, h->surf, pos, nrm, max_vertices);
 }
 extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
   *pos = h->surf.pos; *nrm = h->surf.nrm; *vertices = h->surf.verts;
   return WS_OK;
@@ -1948,6 +2058,7 @@ extern "C" ws_status ws_surface_device(ws_handle* h, const float** pos, const fl
 static double js_round(double x) { double r = std::floor(x); return (x - r >= 0.5) ? r + 1 : r; }
 extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detail, int64_t* vertices, double* volume) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -1985,17 +2096,20 @@ extern "C" ws_status ws_metaball_mesh(ws_handle* h, double tension, double detai
 }
 extern "C" ws_status ws_metaball_download(ws_handle* h, float* pos, float* nrm, int64_t max_vertices) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   return mesh_download(h, h->mball, pos, nrm, max_vertices);
 }
 extern "C" ws_status ws_metaball_device(ws_handle* h, const float** pos, const float** nrm, int64_t* vertices) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !pos || !nrm || !vertices) return WS_ERR_INVALID;
   *pos = h->mball.pos; *nrm = h->mball.nrm; *vertices = h->mball.verts;
   return WS_OK;
 }
 extern "C" ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capacity, int32_t* m) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   const long long corners = (long long)(h->mbM + 1) * (h->mbM + 1) * (h->mbM + 1);
   if (m) *m = h->mbM;
@@ -2011,6 +2125,7 @@ extern "C" ws_status ws_metaball_field(ws_handle* h, float* field, int64_t capac
 // 1783-1800), the per-particle work in ws_render.cu
 extern "C" ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, int32_t counts[5], int64_t* points) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !o) return WS_ERR_INVALID;
   cudaSetDevice(h->device);
   ws_status s = sync_status(h); if (s) return s;
@@ -2059,6 +2174,7 @@ extern "C" ws_status ws_render_particles(ws_handle* h, const ws_render_opts* o, 
 extern "C" ws_status ws_render_download(ws_handle* h, float* pos, float* col, float* alpha, float* size, float* sprite,
                                         int64_t max_points) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h) return WS_ERR_INVALID;
   if (max_points < h->rdrPoints) return fail(h, WS_ERR_RANGE, "buffers hold fewer points than the draw list");
   const size_t n = (size_t)h->rdrPoints;
@@ -2072,6 +2188,7 @@ extern "C" ws_status ws_render_download(ws_handle* h, float* pos, float* col, fl
 extern "C" ws_status ws_render_device(ws_handle* h, const float** pos, const float** col, const float** alpha,
                                       const float** size, const float** sprite, int64_t* points) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
+  join_copies(h);
   if (!h || !pos || !col || !alpha || !size || !sprite || !points) return WS_ERR_INVALID;
   *pos = h->rdr.pos; *col = h->rdr.col; *alpha = h->rdr.alpha; *size = h->rdr.size; *sprite = h->rdr.sprite;
   *points = h->rdrPoints;

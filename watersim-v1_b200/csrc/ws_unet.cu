@@ -105,16 +105,18 @@ __global__ void k_tile_lists(Levels Ls) {
 // ------------------------------------------------------------ input
 // r0 = b - A q at fluid cells (FP64; the residual of k_sor_persistent's
 // check), block partials of r0^2 -> sigma^2 = sum / nFluid
-__global__ void k_residual0(Dims d, const float* __restrict__ q, const float* __restrict__ rhs,
-                            const uint8_t* __restrict__ diag8, const uint8_t* __restrict__ type,
-                            float* __restrict__ r0, double* __restrict__ partials) {
+// over the voxels of the active level-0 tiles only (every fluid cell is in one)
+__global__ void k_residual0(Dims d, Level L, const int* tiles, const int* count, const float* __restrict__ q,
+                            const float* __restrict__ rhs, const uint8_t* __restrict__ diag8,
+                            const uint8_t* __restrict__ type, float* __restrict__ r0, double* __restrict__ partials) {
   __shared__ double ws[32];
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double rr = 0;
-  if (c < d.nCells) {
+  const long long nv = (long long)*count * 1024;
+  for (long long iv = blockIdx.x * (long long)blockDim.x + threadIdx.x; iv < nv; iv += (long long)gridDim.x * blockDim.x) {
+    int i, j, k; long long c;
+    if (!tile_voxel(L, tiles, *count, iv, i, j, k, c)) continue;
     float r = 0.f;
     if (type[c] == WS_FLUID) {
-      int i, j, k; cell_ijk(d, c, i, j, k);
       long long nx = d.nx, nxy = (long long)d.nx * d.ny;
       double s = 0;
       if (i > 0) s += q[c - 1];
@@ -124,7 +126,7 @@ __global__ void k_residual0(Dims d, const float* __restrict__ q, const float* __
       if (k > 0) s += q[c - nxy];
       if (k < d.nz - 1) s += q[c + nxy];
       double rd = (double)rhs[c] + s - (double)diag8[c] * (double)q[c];
-      rr = rd * rd;
+      rr += rd * rd;
       r = (float)rd;
     }
     r0[c] = r;
@@ -149,9 +151,12 @@ __global__ void k_sigma(const double* __restrict__ partials, int nb, const int* 
     *sigma = sg > 0 ? sg : 1.0;
   }
 }
-__global__ void k_scale(float* __restrict__ r0, long long n, const double* sigma) {
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c < n) r0[c] = (float)((double)r0[c] / *sigma);
+__global__ void k_scale(Level L, const int* tiles, const int* count, float* __restrict__ r0, const double* sigma) {
+  const long long nv = (long long)*count * 1024;
+  for (long long iv = blockIdx.x * (long long)blockDim.x + threadIdx.x; iv < nv; iv += (long long)gridDim.x * blockDim.x) {
+    int i, j, k; long long c;
+    if (tile_voxel(L, tiles, *count, iv, i, j, k, c)) r0[c] = (float)((double)r0[c] / *sigma);
+  }
 }
 // network input at the voxels of active level-0 tiles
 // r0n: the residual already divided by sigma, or (sigma non-null) the raw
@@ -718,10 +723,11 @@ cudaError_t Net::backward(cudaStream_t s) {
 // r0 / sigma of the current pressure setup into dst, sigma into sig
 cudaError_t Net::residual(const float* q, const float* rhs, const uint8_t* diag8, const uint8_t* type,
                           float* dst, double* sig, cudaStream_t s, bool scale) {
-  long long N = dims.nCells;
-  k_residual0<<<nPartials, 256, 0, s>>>(dims, q, rhs, diag8, type, dst, partials);
-  k_sigma<<<1, 1024, 0, s>>>(partials, nPartials, counts + kMaxLevels, sig);
-  if (scale) k_scale<<<grid1(N, 256), 256, 0, s>>>(dst, N, sig);
+  const long long n = (long long)lv[0].ntiles * 1024;
+  const unsigned nb = std::min<unsigned>(gridv(n, 256), (unsigned)nPartials);
+  k_residual0<<<nb, 256, 0, s>>>(dims, lv[0], tiles[0], counts, q, rhs, diag8, type, dst, partials);
+  k_sigma<<<1, 1024, 0, s>>>(partials, (int)nb, counts + kMaxLevels, sig);
+  if (scale) k_scale<<<gridv(n, 256), 256, 0, s>>>(lv[0], tiles[0], counts, dst, sig);
   return cudaGetLastError();
 }
 
