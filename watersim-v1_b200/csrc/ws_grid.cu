@@ -202,29 +202,32 @@ void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const
 
 // ------------------------------------------------------------ 3. P2G scatter
 // _p2gInto, js/solver.js:1035-1105: trilinear momentum + weight per face,
-// one float2 vector atomic per face (momentum, weight).
+// one float2 vector atomic per face (momentum, weight). FP32 arithmetic: the
+// face indices and fractions are exact (face_coords_f), the weights and
+// terms carry FP32 rounding (a few 1e-8 relative against the double sums).
 __device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc, int comp,
-                                         double x, double y, double z, double vel) {
-  int i0, j0, k0; double tx, ty, tz; long long idx, sj, sk;
-  face_coords(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
+                                         float x, float y, float z, float vel) {
+  int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
+  face_coords_f(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
   face_strides(d, comp, i0, j0, k0, idx, sj, sk);
-  double s0 = 1 - tx, s1 = tx, t0 = 1 - ty, t1 = ty, r0 = 1 - tz, r1 = tz;
-  double wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
-  double w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
-  long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj, idx + sk + sj + 1 };
+  const float s0 = 1.f - tx, s1 = tx, t0 = 1.f - ty, t1 = ty, r0 = 1.f - tz, r1 = tz;
+  const float wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
+  const float w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
+  const long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj,
+                            idx + sk + sj + 1 };
 #pragma unroll
-  for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2((float)(w8[q] * vel), (float)w8[q]));
+  for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2(w8[q] * vel, w8[q]));
 }
 // Two consecutive particles (the fill lays particles out row by row, so they
 // are usually within a cell of each other): when their stencils of one
 // component start at the same face, their eight (momentum, weight) pairs are
 // summed in registers and sent as eight atomics instead of sixteen.
 __device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc, int comp,
-                                         double x0, double y0, double z0, double v0,
-                                         double x1, double y1, double z1, double v1) {
-  int i0, j0, k0, i1, j1, k1; double tx0, ty0, tz0, tx1, ty1, tz1; long long idx0, idx1, sj, sk;
-  face_coords(d, comp, x0, y0, z0, i0, j0, k0, tx0, ty0, tz0);
-  face_coords(d, comp, x1, y1, z1, i1, j1, k1, tx1, ty1, tz1);
+                                         float x0, float y0, float z0, float v0,
+                                         float x1, float y1, float z1, float v1) {
+  int i0, j0, k0, i1, j1, k1; float tx0, ty0, tz0, tx1, ty1, tz1; long long idx0, idx1, sj, sk;
+  face_coords_f(d, comp, x0, y0, z0, i0, j0, k0, tx0, ty0, tz0);
+  face_coords_f(d, comp, x1, y1, z1, i1, j1, k1, tx1, ty1, tz1);
   face_strides(d, comp, i0, j0, k0, idx0, sj, sk);
   face_strides(d, comp, i1, j1, k1, idx1, sj, sk);
   if (idx0 != idx1) {
@@ -232,17 +235,17 @@ __device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc
     p2g_comp(d, acc, comp, x1, y1, z1, v1);
     return;
   }
-  const double a0 = 1 - tx0, a1 = tx0, b0 = 1 - ty0, b1 = ty0, c0 = 1 - tz0, c1 = tz0;
-  const double e0 = 1 - tx1, e1 = tx1, f0 = 1 - ty1, f1 = ty1, h0 = 1 - tz1, h1 = tz1;
-  const double pA = a0 * b0, pB = a1 * b0, pC = a0 * b1, pD = a1 * b1;
-  const double qA = e0 * f0, qB = e1 * f0, qC = e0 * f1, qD = e1 * f1;
-  const double wp[8] = { pA * c0, pB * c0, pC * c0, pD * c0, pA * c1, pB * c1, pC * c1, pD * c1 };
-  const double wq[8] = { qA * h0, qB * h0, qC * h0, qD * h0, qA * h1, qB * h1, qC * h1, qD * h1 };
+  const float a0 = 1.f - tx0, a1 = tx0, b0 = 1.f - ty0, b1 = ty0, c0 = 1.f - tz0, c1 = tz0;
+  const float e0 = 1.f - tx1, e1 = tx1, f0 = 1.f - ty1, f1 = ty1, h0 = 1.f - tz1, h1 = tz1;
+  const float pA = a0 * b0, pB = a1 * b0, pC = a0 * b1, pD = a1 * b1;
+  const float qA = e0 * f0, qB = e1 * f0, qC = e0 * f1, qD = e1 * f1;
+  const float wp[8] = { pA * c0, pB * c0, pC * c0, pD * c0, pA * c1, pB * c1, pC * c1, pD * c1 };
+  const float wq[8] = { qA * h0, qB * h0, qC * h0, qD * h0, qA * h1, qB * h1, qC * h1, qD * h1 };
   const long long o8[8] = { idx0, idx0 + 1, idx0 + sj, idx0 + sj + 1, idx0 + sk, idx0 + sk + 1, idx0 + sk + sj,
                             idx0 + sk + sj + 1 };
 #pragma unroll
   for (int q = 0; q < 8; q++)
-    atomicAdd(&acc[o8[q]], make_float2((float)(wp[q] * v0) + (float)(wq[q] * v1), (float)wp[q] + (float)wq[q]));
+    atomicAdd(&acc[o8[q]], make_float2(fmaf(wq[q], v1, wp[q] * v0), wp[q] + wq[q]));
 }
 __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, int* err) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
@@ -250,19 +253,19 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, i
   const bool has1 = p1 < P.nP;
   // every load of both particles is issued before the flag tests (one round trip)
   const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
-  const double x0 = P.px[p0], y0 = P.py[p0], z0 = P.pz[p0];
+  const float x0 = P.px[p0], y0 = P.py[p0], z0 = P.pz[p0];
   const float u0 = P.pvx[p0], v0 = P.pvy[p0], w0 = P.pvz[p0];
-  const double x1 = has1 ? P.px[p1] : 0.0, y1 = has1 ? P.py[p1] : 0.0, z1 = has1 ? P.pz[p1] : 0.0;
+  const float x1 = has1 ? P.px[p1] : 0.f, y1 = has1 ? P.py[p1] : 0.f, z1 = has1 ? P.pz[p1] : 0.f;
   const float u1 = has1 ? P.pvx[p1] : 0.f, v1 = has1 ? P.pvy[p1] : 0.f, w1 = has1 ? P.pvz[p1] : 0.f;
   // a fluid particle with a non-finite state is left out of the grid and latched
-  const bool a = fl0 == 0 && particle_sound(d, x0, y0, z0, u0, v0, w0, err, false);
-  const bool b = fl1 == 0 && particle_sound(d, x1, y1, z1, u1, v1, w1, err, false);
+  const bool a = fl0 == 0 && particle_sound_f(x0, y0, z0, u0, v0, w0, err);
+  const bool b = fl1 == 0 && particle_sound_f(x1, y1, z1, u1, v1, w1, err);
   if (a && b) {
     p2g_pair(d, g.acc, 0, x0, y0, z0, u0, x1, y1, z1, u1);
     p2g_pair(d, g.acc, 1, x0, y0, z0, v0, x1, y1, z1, v1);
     p2g_pair(d, g.acc, 2, x0, y0, z0, w0, x1, y1, z1, w1);
   } else if (a || b) {
-    const double x = a ? x0 : x1, y = a ? y0 : y1, z = a ? z0 : z1;
+    const float x = a ? x0 : x1, y = a ? y0 : y1, z = a ? z0 : z1;
     p2g_comp(d, g.acc, 0, x, y, z, a ? u0 : u1);
     p2g_comp(d, g.acc, 1, x, y, z, a ? v0 : v1);
     p2g_comp(d, g.acc, 2, x, y, z, a ? w0 : w1);
@@ -324,12 +327,12 @@ __device__ __forceinline__ void brick_face_box(int comp, int& oi, int& oj, int& 
 // one particle's eight terms of component comp: into the brick's faces when
 // the whole stencil lies inside them, else straight to global memory
 __device__ __forceinline__ void p2g_brick_comp(const Dims& d, float2* __restrict__ acc, float* sm, int comp,
-                                               int fx, int fy, int fz, double x, double y, double z, double vel) {
-  int i0, j0, k0; double tx, ty, tz;
-  face_coords(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
-  const double s0 = 1 - tx, s1 = tx, t0 = 1 - ty, t1 = ty, r0 = 1 - tz, r1 = tz;
-  const double wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
-  const double w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
+                                               int fx, int fy, int fz, float x, float y, float z, float vel) {
+  int i0, j0, k0; float tx, ty, tz;
+  face_coords_f(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
+  const float s0 = 1.f - tx, s1 = tx, t0 = 1.f - ty, t1 = ty, r0 = 1.f - tz, r1 = tz;
+  const float wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
+  const float w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
   int oi, oj, ok, ex, ey;
   brick_face_box(comp, oi, oj, ok, ex, ey);
   const int ez = comp == 2 ? 5 : 6;
@@ -341,8 +344,8 @@ __device__ __forceinline__ void p2g_brick_comp(const Dims& d, float2* __restrict
     const int o8[8] = { o, o + 1, o + sj, o + sj + 1, o + sk, o + sk + 1, o + sk + sj, o + sk + sj + 1 };
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      atomicAdd(&m[o8[q]], (float)(w8[q] * vel));
-      atomicAdd(&w[o8[q]], (float)w8[q]);
+      atomicAdd(&m[o8[q]], w8[q] * vel);
+      atomicAdd(&w[o8[q]], w8[q]);
     }
   } else {
     long long idx, sj, sk;
@@ -350,7 +353,7 @@ __device__ __forceinline__ void p2g_brick_comp(const Dims& d, float2* __restrict
     const long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj,
                               idx + sk + sj + 1 };
 #pragma unroll
-    for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2((float)(w8[q] * vel), (float)w8[q]));
+    for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2(w8[q] * vel, w8[q]));
   }
 }
 // One block per brick (the brick list, or every brick when allBricks). The
@@ -377,8 +380,8 @@ __global__ void __launch_bounds__(256) k_p2g_bricks(Dims d, GridDev g, PartsDev 
       const int at = lane * L + a;
       if (at >= n) continue;
       const int p = cs.perm[s0 + at];
-      const double x = P.px[p], y = P.py[p], z = P.pz[p];
-      const double u = P.pvx[p], v = P.pvy[p], w = P.pvz[p];
+      const float x = P.px[p], y = P.py[p], z = P.pz[p];
+      const float u = P.pvx[p], v = P.pvy[p], w = P.pvz[p];
       p2g_brick_comp(d, g.acc, sm, 0, fx, fy, fz, x, y, z, u);
       p2g_brick_comp(d, g.acc, sm, 1, fx, fy, fz, x, y, z, v);
       p2g_brick_comp(d, g.acc, sm, 2, fx, fy, fz, x, y, z, w);
@@ -583,13 +586,7 @@ __global__ void k_sor_color(Dims d, float* __restrict__ q, const float* __restri
   if (w < 0.f) return;
   if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2 || k < 1 || k > nz - 2) return;
   long long nxy = (long long)nx * ny;
-  double sum = (double)q[c - 1];
-  sum += (double)q[c + 1];
-  sum += (double)q[c - nx];
-  sum += (double)q[c + nx];
-  sum += (double)q[c - nxy];
-  sum += (double)q[c + nxy];
-  q[c] = (float)((double)q[c] * om1 + (double)w * ((double)rhs[c] + sum));
+  q[c] = sor_update(q[c], w, rhs[c], q[c - 1], q[c + 1], q[c - nx], q[c + nx], q[c - nxy], q[c + nxy], om1);
 }
 void launch_sor_color(const Dims& d, const GridDev& g, int color, double om1, cudaStream_t s) {
   long long n = (long long)d.ny * d.nz * ((d.nx + 1) >> 1);

@@ -11,9 +11,14 @@
 //              u (k*ny+j)*(nx+1)+i, v (k*(ny+1)+j)*nx+i, w (k*ny+j)*nx+i.
 //   cells      cellType u8, q/rhs/pw float32, cell (k*ny+j)*nx+i.
 //
-// Arithmetic: kernels evaluate in FP64 and store FP32, mirroring the
-// reference (JavaScript doubles over Float32Array storage); the library is
-// built with -fmad=false because JavaScript never fuses a multiply-add.
+// Arithmetic: the particle passes compute in FP32 with explicit fused
+// multiply-adds (P2G, the G2P/advection velocities); every value that decides
+// a cell type, a particle phase or a position test stays in FP64, as do the
+// residual norm and the volume and census reductions. The SOR iterate is
+// FP32 with each update accumulated in FP64 (sor_update says why).
+// The rest mirrors the reference (JavaScript doubles over Float32Array
+// storage) in FP64; the library is built with -fmad=false so that no FP64
+// multiply-add is fused behind the code's back (JavaScript never fuses one).
 #pragma once
 #include <cmath>
 #include <cuda_runtime.h>
@@ -197,7 +202,34 @@ __device__ __forceinline__ bool particle_sound(const Dims& d, double x, double y
   if (checkRange && (x < 0 || y < 0 || z < 0 || x > d.W || y > d.H || z > d.D)) atomicOr(err, WS_DERR_RANGE);
   return true;
 }
+// the same NaN latch on the stored FP32 state (no range check)
+__device__ __forceinline__ bool particle_sound_f(float x, float y, float z, float u, float v, float w, int* err) {
+  if (!(isfinite(x) && isfinite(y) && isfinite(z) && isfinite(u) && isfinite(v) && isfinite(w))) {
+    atomicOr(err, WS_DERR_NAN);
+    return false;
+  }
+  return true;
+}
 __device__ __forceinline__ int jtrunc(double v) { return (int)v; }
+// One red-black SOR update of a fluid cell (js/solver.js:1397-1404):
+// q (1 - omega) + (omega / diag) (rhs + the sum of the six neighbour q), with
+// q = 0 at the non-fluid neighbours, summed in the order -x, +x, -y, +y, -z,
+// +z. q is stored in FP32 and the update is accumulated in FP64 with one
+// rounding to FP32, as the reference computes it: an update accumulated in
+// FP32 (pairwise sum, one FMA) floors the relative residual of the 128^3
+// planet near the 1e-5 tolerance (180 iterations instead of 170 on one
+// system, q 6.8e-6 instead of 5.6e-7 from the FP64 solve). Every SOR path
+// calls this, so their iterates agree bit for bit.
+__device__ __forceinline__ float sor_update(float qc, float pw, float rhs, float n0, float n1, float n2, float n3,
+                                            float n4, float n5, double om1) {
+  double s = (double)n0;
+  s += (double)n1;
+  s += (double)n2;
+  s += (double)n3;
+  s += (double)n4;
+  s += (double)n5;
+  return (float)((double)qc * om1 + (double)pw * ((double)rhs + s));
+}
 __device__ __forceinline__ int jfloor_clamp(double v, int a, int b) {
   double f = floor(v);
   if (f < a) return a;
@@ -296,6 +328,52 @@ __device__ __forceinline__ void sample_vel3(const Dims& d, const float* __restri
   oy = tri_sample(vel, idx, sj, sk, tx, ty, tz);
   face_coords(d, 2, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
   oz = tri_sample(vel, idx, sj, sk, tx, ty, tz);
+}
+
+// ---- FP32 sampling of the hot particle passes (P2G, G2P, advection)
+// Face-grid coordinates of component comp in FP32. With a power-of-two cell
+// size (the only kind the reference's planets use) x * (1/dx), the half-cell
+// shift, the floor and the fraction are exact in FP32 for positions below
+// 2^21 cells, so i0/j0/k0 and tx/ty/tz equal the double computation of
+// face_coords bit for bit. Other cell sizes take the double path and round
+// the fractions.
+__device__ __forceinline__ void face_coords_f(const Dims& d, int comp, float x, float y, float z,
+                                              int& i0, int& j0, int& k0, float& tx, float& ty, float& tz) {
+  if (!d.dxPow2) {
+    double a, b, c;
+    face_coords(d, comp, x, y, z, i0, j0, k0, a, b, c);
+    tx = (float)a; ty = (float)b; tz = (float)c;
+    return;
+  }
+  const float r = (float)d.rdx;
+  const float X = x * r, Y = y * r, Z = z * r;
+  const float a = comp == 0 ? X : X - 0.5f, b = comp == 1 ? Y : Y - 0.5f, c = comp == 2 ? Z : Z - 0.5f;
+  const float fi = floorf(a), fj = floorf(b), fk = floorf(c);
+  if (fi < 0.f) { i0 = 0; tx = 0.f; } else if (fi > (float)(d.nx - 1)) { i0 = d.nx - 1; tx = 1.f; } else { i0 = (int)fi; tx = a - fi; }
+  if (fj < 0.f) { j0 = 0; ty = 0.f; } else if (fj > (float)(d.ny - 2)) { j0 = d.ny - 2; ty = 1.f; } else { j0 = (int)fj; ty = b - fj; }
+  if (fk < 0.f) { k0 = 0; tz = 0.f; } else if (fk > (float)(d.nz - 2)) { k0 = d.nz - 2; tz = 1.f; } else { k0 = (int)fk; tz = c - fk; }
+}
+// trilinear blend of the eight faces around idx, FP32 with fused multiply-adds
+__device__ __forceinline__ float tri_sample_f(const float* __restrict__ a, long long idx, long long sj, long long sk,
+                                              float tx, float ty, float tz) {
+  const long long o1 = idx + sj, o2 = idx + sk, o3 = o2 + sj;
+  const float a00 = a[idx], a10 = a[idx + 1], a01 = a[o1], a11 = a[o1 + 1];
+  const float b00 = a[o2], b10 = a[o2 + 1], b01 = a[o3], b11 = a[o3 + 1];
+  const float c0 = fmaf(tx, a10 - a00, a00), c1 = fmaf(tx, a11 - a01, a01);
+  const float c2 = fmaf(tx, b10 - b00, b00), c3 = fmaf(tx, b11 - b01, b01);
+  const float e0 = fmaf(ty, c1 - c0, c0), e1 = fmaf(ty, c3 - c2, c2);
+  return fmaf(tz, e1 - e0, e0);
+}
+// _sampleVel3 (js/solver.js:820-854) in FP32
+__device__ __forceinline__ void sample_vel3_f(const Dims& d, const float* __restrict__ vel, float x, float y, float z,
+                                              float& ox, float& oy, float& oz) {
+  int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
+  face_coords_f(d, 0, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
+  ox = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
+  face_coords_f(d, 1, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
+  oy = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
+  face_coords_f(d, 2, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
+  oz = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
 }
 
 // block-wide helpers

@@ -20,9 +20,10 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
     int fl = P.pflag[p];
     const double dx = d.dx, dt = ap.dt, maxSpeed = ap.maxSpeed, oceanR = ap.oceanR;
     const double cx = d.cx, cy = d.cy, cz = d.cz;
-    double x = P.px[p], y = P.py[p], z = P.pz[p];
+    const float xf = P.px[p], yf = P.py[p], zf = P.pz[p];
+    double x = xf, y = yf, z = zf;
     float fvx = P.pvx[p], fvy = P.pvy[p], fvz = P.pvz[p];
-    double a0 = 0, a1 = 0, a2 = 0;            // _advU/_advV/_advW
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;       // _advU/_advV/_advW (FP32 samples)
     int cool = 0, coolWrite = 0;
     // ---------------- G2P
     if (fl != 0) {
@@ -31,24 +32,25 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
       coolWrite = 1; cool--;
       double gdt = dt; if (gdt == 0) gdt = ap.dtLast; if (gdt == 0) gdt = 0.01;
       fvy = (float)((double)fvy - ap.gravity * gdt);
-      sample_vel3(d, g.vel, x, y, z, a0, a1, a2);
+      sample_vel3_f(d, g.vel, xf, yf, zf, a0, a1, a2);
     } else {
-      int i0, j0, k0; double tx, ty, tz; long long idx, sj, sk;
-      double ou, ov, ow;
-      face_coords(d, 0, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
-      ou = tri_sample(g.velO, idx, sj, sk, tx, ty, tz); a0 = tri_sample(g.vel, idx, sj, sk, tx, ty, tz);
-      face_coords(d, 1, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
-      ov = tri_sample(g.velO, idx, sj, sk, tx, ty, tz); a1 = tri_sample(g.vel, idx, sj, sk, tx, ty, tz);
-      face_coords(d, 2, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
-      ow = tri_sample(g.velO, idx, sj, sk, tx, ty, tz); a2 = tri_sample(g.vel, idx, sj, sk, tx, ty, tz);
-      double pic = ap.pic;
-      fvx = (float)(((double)fvx + a0 - ou) * (1 - pic) + a0 * pic);
-      fvy = (float)(((double)fvy + a1 - ov) * (1 - pic) + a1 * pic);
-      fvz = (float)(((double)fvz + a2 - ow) * (1 - pic) + a2 * pic);
-      double pv2 = (double)fvx * fvx + (double)fvy * fvy + (double)fvz * fvz;
-      if (pv2 > maxSpeed * maxSpeed) {
-        double psc = maxSpeed / sqrt(pv2);
-        fvx = (float)(fvx * psc); fvy = (float)(fvy * psc); fvz = (float)(fvz * psc);
+      // FP32 sampling at the stored position (exact face indices and fractions)
+      int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
+      float ou, ov, ow;
+      face_coords_f(d, 0, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
+      ou = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a0 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
+      face_coords_f(d, 1, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
+      ov = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a1 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
+      face_coords_f(d, 2, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
+      ow = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a2 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
+      const float pic = (float)ap.pic, flip = (float)(1 - ap.pic);
+      fvx = fmaf(fvx + a0 - ou, flip, a0 * pic);
+      fvy = fmaf(fvy + a1 - ov, flip, a1 * pic);
+      fvz = fmaf(fvz + a2 - ow, flip, a2 * pic);
+      const float pv2 = fvx * fvx + fvy * fvy + fvz * fvz, msf = (float)maxSpeed;
+      if (pv2 > msf * msf) {
+        const float psc = msf / sqrtf(pv2);
+        fvx *= psc; fvy *= psc; fvz *= psc;
       }
       int ci = jfloor_clamp(over_dx(d, x), 0, d.nx - 1), cj = jfloor_clamp(over_dx(d, y), 0, d.ny - 1), ck = jfloor_clamp(over_dx(d, z), 0, d.nz - 1);
       long long c = ((long long)ck * d.ny + cj) * d.nx + ci; long long nxy = (long long)d.nx * d.ny;
@@ -178,24 +180,31 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
     } else if (fl == 2 || fl == 3) {
       writePos = false;                                    // k_vapor_advect owns these
     } else {                                               // grid-coupled fluid, :2176-2290
-      double v2x = a0, v2y = a1, v2z = a2;
-      double sp2 = a0 * a0 + a1 * a1 + a2 * a2;
-      if (sp2 > 0.25) {
-        double mx = x + 0.5 * dt * a0, my = y + 0.5 * dt * a1, mz = z + 0.5 * dt * a2;
-        mx = mx < xLo ? xLo : (mx > xHi ? xHi : mx);
-        my = my < yLo ? yLo : (my > yHi ? yHi : my);
-        mz = mz < zLo ? zLo : (mz > zHi ? zHi : mz);
-        sample_vel3(d, g.vel, mx, my, mz, v2x, v2y, v2z);
+      // Velocities in FP32; the position update and every test of a position
+      // (domain shell, rock cells) in double, as the reference computes them.
+      float v2x = a0, v2y = a1, v2z = a2;
+      float sp2 = a0 * a0 + a1 * a1 + a2 * a2;
+      if (sp2 > 0.25f) {
+        const float hdt = (float)(0.5 * dt);
+        float mx = fmaf(hdt, a0, xf), my = fmaf(hdt, a1, yf), mz = fmaf(hdt, a2, zf);
+        const float xLof = (float)xLo, xHif = (float)xHi, yLof = (float)yLo, yHif = (float)yHi;
+        const float zLof = (float)zLo, zHif = (float)zHi;
+        mx = mx < xLof ? xLof : (mx > xHif ? xHif : mx);
+        my = my < yLof ? yLof : (my > yHif ? yHif : my);
+        mz = mz < zLof ? zLof : (mz > zHif ? zHif : mz);
+        sample_vel3_f(d, g.vel, mx, my, mz, v2x, v2y, v2z);
       }
       sp2 = v2x * v2x + v2y * v2y + v2z * v2z;
-      if (sp2 > maxSpeed * maxSpeed) {
-        double sc = maxSpeed / sqrt(sp2);
+      const float msf = (float)maxSpeed;
+      if (sp2 > msf * msf) {
+        const float sc = msf / sqrtf(sp2);
         v2x *= sc; v2y *= sc; v2z *= sc;
-        fvx = (float)(fvx * sc); fvy = (float)(fvy * sc); fvz = (float)(fvz * sc);
+        fvx *= sc; fvy *= sc; fvz *= sc;
       }
-      x += v2x * dt; y += v2y * dt; z += v2z * dt;
+      x += (double)v2x * dt; y += (double)v2y * dt; z += (double)v2z * dt;
       double nx2 = x - cx, ny2 = y - cy, nz2 = z - cz;
       double nr = sqrt(nx2 * nx2 + ny2 * ny2 + nz2 * nz2); if (nr == 0) nr = 1e-9;
+      const double inr = 1.0 / nr;
       if (nr > domHi) {
         double sc2 = domHi / nr;
         x = cx + nx2 * sc2; y = cy + ny2 * sc2; z = cz + nz2 * sc2;
@@ -226,18 +235,23 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
           double vr2 = ((double)fvx * nx2 + (double)fvy * ny2 + (double)fvz * nz2) / nr;
           if (vr2 < 0) { fvx = (float)(fvx - nx2 / nr * vr2); fvy = (float)(fvy - ny2 / nr * vr2); fvz = (float)(fvz - nz2 / nr * vr2); }
         }
-        if (hasTerr && (tries > 0 || rock_cell_at(d, g.staticTypes, x - nx2 / nr * dx, y - ny2 / nr * dx, z - nz2 / nr * dx))) {
+        if (hasTerr && (tries > 0 || rock_cell_at(d, g.staticTypes, x - nx2 * inr * dx, y - ny2 * inr * dx, z - nz2 * inr * dx))) {
           double fr0 = 1 - 0.6 * dt; if (fr0 < 0) fr0 = 0;
-          fvx = (float)(fvx * fr0); fvy = (float)(fvy * fr0); fvz = (float)(fvz * fr0);
+          const float fr = (float)fr0;
+          fvx *= fr; fvy *= fr; fvz *= fr;
         }
       }
-      double sx = x - cx, sy = y - cy, sz = z - cz;
-      double sr = sqrt(sx * sx + sy * sy + sz * sz); if (sr == 0) sr = 1e-9;
-      double vrad = ((double)fvx * sx + (double)fvy * sy + (double)fvz * sz) / sr;
+      // radial damping and drag (velocities only): FP32
+      const float sx = (float)(x - cx), sy = (float)(y - cy), sz = (float)(z - cz);
+      float sr = sqrtf(sx * sx + sy * sy + sz * sz); if (sr == 0.f) sr = 1e-9f;
+      const float isr = 1.f / sr;
+      const float vrad = (fvx * sx + fvy * sy + fvz * sz) * isr;
       double da = 1.0 * dt; if (da > 0.5) da = 0.5;
-      fvx = (float)(fvx - sx / sr * vrad * da); fvy = (float)(fvy - sy / sr * vrad * da); fvz = (float)(fvz - sz / sr * vrad * da);
+      const float kr = vrad * (float)da * isr;
+      fvx = fmaf(-sx, kr, fvx); fvy = fmaf(-sy, kr, fvy); fvz = fmaf(-sz, kr, fvz);
       double dg = 1 - 0.42 * dt; if (dg < 0) dg = 0;
-      fvx = (float)(fvx * dg); fvy = (float)(fvy * dg); fvz = (float)(fvz * dg);
+      const float dgf = (float)dg;
+      fvx *= dgf; fvy *= dgf; fvz *= dgf;
     }
     if (fl != 2 && fl != 3) { P.pvx[p] = fvx; P.pvy[p] = fvy; P.pvz[p] = fvz; }
     if (writePos) { P.px[p] = (float)x; P.py[p] = (float)y; P.pz[p] = (float)z; }

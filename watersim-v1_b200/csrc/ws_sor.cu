@@ -233,13 +233,8 @@ __device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned tid
 #pragma unroll
     for (int j = 0; j < kSorBatch; j++) {
       if (c[j] < 0) continue;
-      double sum = (double)v[j][0];
-      sum += (double)v[j][1];
-      sum += (double)v[j][2];
-      sum += (double)v[j][3];
-      sum += (double)v[j][4];
-      sum += (double)v[j][5];
-      __stcg(q + c[j], (float)((double)v[j][6] * a.om1 + (double)w[j] * ((double)r[j] + sum)));
+      __stcg(q + c[j], sor_update(v[j][6], w[j], r[j], v[j][0], v[j][1], v[j][2], v[j][3], v[j][4], v[j][5],
+                                  a.om1));
     }
   }
 }
@@ -292,13 +287,9 @@ struct Entry { long long c; float rhs, pw, q; uint8_t dg; };
 
 __device__ __forceinline__ void entry_relax(Entry& e, const float* q, long long nx, long long nxy, double om1) {
   if (e.c < 0) return;
-  double sum = (double)__ldcg(q + e.c - 1);
-  sum += (double)__ldcg(q + e.c + 1);
-  sum += (double)__ldcg(q + e.c - nx);
-  sum += (double)__ldcg(q + e.c + nx);
-  sum += (double)__ldcg(q + e.c - nxy);
-  sum += (double)__ldcg(q + e.c + nxy);
-  e.q = (float)((double)e.q * om1 + (double)e.pw * ((double)e.rhs + sum));
+  const float n0 = __ldcg(q + e.c - 1), n1 = __ldcg(q + e.c + 1), n2 = __ldcg(q + e.c - nx);
+  const float n3 = __ldcg(q + e.c + nx), n4 = __ldcg(q + e.c - nxy), n5 = __ldcg(q + e.c + nxy);
+  e.q = sor_update(e.q, e.pw, e.rhs, n0, n1, n2, n3, n4, n5, om1);
   __stcg(const_cast<float*>(q) + e.c, e.q);
 }
 __device__ __forceinline__ void entry_residual(const Entry& e, const float* q, long long nx, long long nxy,
@@ -405,14 +396,18 @@ __device__ __forceinline__ float cl_load(float* const* rq, uint16_t code) {
   return rq[code >> 12][code & 4095u];
 }
 // relax (or measure) up to two cells per call with all twelve loads in flight
-__device__ __forceinline__ void cl_sums(const uint16_t* cd, float* const* rq, int e0, int e1, int m,
-                                        double& s0, double& s1) {
-  float v[2][6];
+__device__ __forceinline__ void cl_vals(const uint16_t* cd, float* const* rq, int e0, int e1, int m, float (&v)[2][6]) {
 #pragma unroll
   for (int q = 0; q < 6; q++) {
     v[0][q] = e0 < m ? cl_load(rq, cd[6 * e0 + q]) : 0.f;
     v[1][q] = e1 < m ? cl_load(rq, cd[6 * e1 + q]) : 0.f;
   }
+}
+// FP64 sums of the six neighbours (the residual)
+__device__ __forceinline__ void cl_sums(const uint16_t* cd, float* const* rq, int e0, int e1, int m,
+                                        double& s0, double& s1) {
+  float v[2][6];
+  cl_vals(cd, rq, e0, e1, m, v);
   s0 = (double)v[0][0]; s1 = (double)v[1][0];
 #pragma unroll
   for (int q = 1; q < 6; q++) { s0 += (double)v[0][q]; s1 += (double)v[1][q]; }
@@ -498,11 +493,13 @@ __global__ void __launch_bounds__(1024, 1) k_sor_cluster(ClusterArgs a) {
     for (int col = 0; col < 2; col++) {
       for (int e = threadIdx.x; e < m[col]; e += 2 * B) {
         int e1 = e + B;
-        double s0, s1;
-        cl_sums(cd[col], rq[1 - col], e, e1, m[col], s0, s1);
-        qs[col][e] = (float)((double)qs[col][e] * om1 + (double)pw[col][e] * ((double)rh[col][e] + s0));
+        float v[2][6];
+        cl_vals(cd[col], rq[1 - col], e, e1, m[col], v);
+        qs[col][e] = sor_update(qs[col][e], pw[col][e], rh[col][e], v[0][0], v[0][1], v[0][2], v[0][3], v[0][4],
+                                v[0][5], om1);
         if (e1 < m[col])
-          qs[col][e1] = (float)((double)qs[col][e1] * om1 + (double)pw[col][e1] * ((double)rh[col][e1] + s1));
+          qs[col][e1] = sor_update(qs[col][e1], pw[col][e1], rh[col][e1], v[1][0], v[1][1], v[1][2], v[1][3],
+                                   v[1][4], v[1][5], om1);
       }
       cl.sync();
     }

@@ -18,14 +18,19 @@
 // the same order with the same arithmetic as the reference's sweep, so the
 // iterates are bitwise those of the plain red-black solve.
 //
-// Exchange. After each such epoch a CTA writes its owned cells into one of
-// two global q buffers (epochs alternate), publishes its epoch number, and
-// before the next epoch waits only for the CTAs owning its halo bricks
-// (release/acquire flags, no grid barrier) and reloads its halo cells.
-// Double buffering makes the write of epoch e safe against neighbours still
-// reading epoch e - 1: a neighbour reads buffer e & 1 only after it saw this
-// CTA's flag reach e, and this CTA writes that buffer again only after it saw
-// the neighbour's flag reach e + 1, i.e. after the neighbour's read.
+// Exchange. After each such epoch e a CTA writes its owned cells into one of
+// two global exchange buffers (e & 1) as 64-bit words (q's bits | e << 32),
+// one single-copy-atomic relaxed store per cell and no fence or flag; before
+// the next epoch every thread loads its halo cells from that buffer and
+// polls a word again until its tag reads e. The tag travels in the same word
+// as the value, so a matching tag proves the value, and a CTA waits only for
+// the values it needs. Double buffering makes the write of epoch e + 2 safe
+// against neighbours still reading epoch e: a CTA computes epoch e + 2 only
+// after reading its neighbours' epoch e + 1 values, which each neighbour
+// wrote after it had read this CTA's epoch e values (halo adjacency is
+// symmetric). The plan phase clears the tags of every owned cell in both
+// buffers before the first epoch, so stale words of an earlier solve never
+// match.
 //
 // Residual check. Every sorCheckEvery iterations (epochs end on check
 // iterations) the FP64 partial ||b - A q||^2 and ||b||^2 of the owned cells
@@ -71,7 +76,7 @@ struct TbCtl {
 struct TbArgs {
   Dims d;
   float* q;                      // the solve's q (epochs 0, 2, 4, ... end here)
-  float* q1;                     // second q buffer (epochs 1, 3, ...)
+  unsigned long long* xq;        // exchange: two buffers of nCells words (q bits | epoch << 32)
   const float* rhs;
   const float* pw;               // omega/diag, negative off the fluid
   const uint8_t* diag8;
@@ -128,6 +133,14 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
@@ -250,16 +263,9 @@ __device__ __forceinline__ int2 block_scan2(int a, int b, int2& total, int2* sw)
   return r;
 }
 
-// one cell update of the reference's sweep (js/solver.js:1397-1404):
-// q <- q (1 - omega) + pw (rhs + sum of the six neighbour q), FP64 arithmetic
+// one cell update of the reference's sweep (js/solver.js:1397-1404; sor_update)
 __device__ __forceinline__ float relax(float qc, float pw, float rhs, const float* v, double om1) {
-  double sum = (double)v[0];
-  sum += (double)v[1];
-  sum += (double)v[2];
-  sum += (double)v[3];
-  sum += (double)v[4];
-  sum += (double)v[5];
-  return (float)((double)qc * om1 + (double)pw * ((double)rhs + sum));
+  return sor_update(qc, pw, rhs, v[0], v[1], v[2], v[3], v[4], v[5], om1);
 }
 
 // residual partial of the owned cells (dense order, deterministic) of the
@@ -604,8 +610,6 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
               S.eNb[pos][0] = (unsigned)nb[0] | ((unsigned)nb[1] << 16);
               S.eNb[pos][1] = (unsigned)nb[2] | ((unsigned)nb[3] << 16);
               S.eNb[pos][2] = (unsigned)nb[4] | ((unsigned)nb[5] << 16);
-              S.eRhs[pos] = __ldcg(a.rhs + g);
-              S.ePw[pos] = __ldcg(a.pw + g);
               if (b == 0 || b == 4) {
                 const int o = b == 0 ? pos - bstart[0] : bucket[0] + pos - bstart[4];
                 if (o < kOMax) S.oGlob[o] = g;
@@ -630,6 +634,27 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
       __syncthreads();
     }
+    // right-hand side and relaxation weight of every entry, gathered after
+    // the bucketing (whose loop carries shuffles and shared atomics) with
+    // four loads in flight per thread
+    if (!sOverflow) {
+      const int nE = bstart[7] + bucket[7];
+      for (int e0 = tid; e0 < nE; e0 += 4 * T) {
+        float r[4], w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int e = e0 + u * T;
+          r[u] = 0.f; w[u] = 0.f;
+          unsigned g; int i, j, k;
+          if (e < nE && dense_global(a, S, S.eSelf[e], g, i, j, k)) { r[u] = __ldcg(a.rhs + g); w[u] = __ldcg(a.pw + g); }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int e = e0 + u * T;
+          if (e < nE) { S.eRhs[e] = r[u]; S.ePw[e] = w[u]; }
+        }
+      }
+    }
     if (tid == 0 && nReload > kLMax) sOverflow = 1;
     // the CTAs owning halo bricks: this CTA's neighbours in both directions
     for (int s = O + tid; s < R; s += T) atomicOr(&S.depMask[S.rbOwn[s] >> 5], 1u << (S.rbOwn[s] & 31));
@@ -642,6 +667,14 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
       nDeps = n;
       if (sOverflow) atomicOr(&a.ctl->overflow, 1);
+    }
+    // the owned cells' exchange words start with tag 0 (epochs count from 1)
+    if (!sOverflow) {
+      const int nOwn = bucket[0] + bucket[4];
+      for (int e = tid; e < nOwn; e += T) {
+        st_relaxed_u64(a.xq + S.oGlob[e], 0ull);
+        st_relaxed_u64(a.xq + (size_t)d.nCells + S.oGlob[e], 0ull);
+      }
     }
   }
   if (!tb_grid_barrier(a.ctl, a.err, &sAbort)) goto done;
@@ -663,24 +696,39 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
     unsigned epoch = 0;
     int nChecks = 0;
     bool fresh = true, checked = false;
+    // the halo values of epoch `target`: four loads in flight per thread,
+    // then each word polled again (bounded) until its tag reads target
     auto wait_and_reload = [&](unsigned target) -> bool {
-      if (tid < 32) {
-        for (int k = lane; k < nDeps; k += 32)
-          if (!bounded_wait_geq(&a.ctl->flag[S.deps[k]], target, kTbSpinLimit, a.err)) sAbort = 1;
-      }
-      __syncthreads();
-      if (sAbort) return false;
-      // four loads in flight per thread before their stores
-      const float* src = (target & 1u) ? a.q1 : a.q;
+      const unsigned long long* src = a.xq + (size_t)(target & 1u) * (size_t)d.nCells;
       for (int l0 = tid; l0 < nReload; l0 += 4 * T) {
-        float v[4];
+        unsigned long long v[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) { const int l = l0 + u * T; v[u] = l < nReload ? __ldcg(src + S.lGlob[l]) : 0.f; }
+        for (int u = 0; u < 4; u++) { const int l = l0 + u * T; v[u] = l < nReload ? ld_relaxed_u64(src + S.lGlob[l]) : 0ull; }
 #pragma unroll
-        for (int u = 0; u < 4; u++) { const int l = l0 + u * T; if (l < nReload) S.q[S.lDense[l]] = v[u]; }
+        for (int u = 0; u < 4; u++) {
+          const int l = l0 + u * T;
+          if (l >= nReload) continue;
+          long long n = 0;
+          while ((unsigned)(v[u] >> 32) != target) {
+            if (++n > kTbSpinLimit || *(volatile int*)&sAbort) {
+              if (n > kTbSpinLimit) atomicOr(a.err, WS_DERR_TIMEOUT);
+              sAbort = 1;
+              break;
+            }
+            v[u] = ld_relaxed_u64(src + S.lGlob[l]);
+          }
+          S.q[S.lDense[l]] = __uint_as_float((unsigned)v[u]);
+        }
       }
       __syncthreads();
-      return true;
+      return *(volatile int*)&sAbort == 0;
+    };
+    // the owned cells of epoch `ep` into exchange buffer ep & 1
+    auto publish_owned = [&](unsigned ep) {
+      unsigned long long* dst = a.xq + (size_t)(ep & 1u) * (size_t)d.nCells;
+      const unsigned long long tag = (unsigned long long)ep << 32;
+      for (int e = tid; e < nOwn0 + nOwn1; e += T)
+        st_relaxed_u64(dst + S.oGlob[e], tag | __float_as_uint(S.q[S.eSelf[e < nOwn0 ? st0 + e : st1 + (e - nOwn0)]]));
     };
     auto write_owned = [&](float* dst) {
       for (int e = tid; e < nOwn0 + nOwn1; e += T)
@@ -729,11 +777,9 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
       it += m;
       epoch++;
-      write_owned((epoch & 1u) ? a.q1 : a.q);
-      __syncthreads();
-      // the CTA barrier orders every thread's stores before thread 0; its
-      // release fence at GPU scope carries them to the waiting neighbours
-      if (tid == 0) { fence_acq_rel_gpu(); st_release(&a.ctl->flag[p], epoch); }
+      // no barrier before the reload that follows: it writes halo cells
+      // (d >= 1) of S.q, this reads owned cells (d = 0)
+      publish_owned(epoch);
       fresh = false;
       checked = false;
       const bool doCheck = a.check > 0 && it % a.check == 0;
@@ -826,7 +872,7 @@ done:
 // ---------------------------------------------------------------- host side
 struct TbState {
   TbCtl* ctl = nullptr;
-  float* q1 = nullptr;
+  unsigned long long* xq = nullptr;
   int* brickW = nullptr;
   int2* cntPart = nullptr;
   int *actLin = nullptr, *actWPre = nullptr, *brickOrd = nullptr, *chunkStart = nullptr;
@@ -863,7 +909,7 @@ cudaError_t sor_tb_init(void** statePtr, const Dims& d, int device) {
   const long long nB = (long long)S->nbx * S->nby * S->nbz, MC = 1LL << (3 * mb);
   cudaError_t e;
   if ((e = cudaMalloc(&S->ctl, sizeof(TbCtl))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&S->q1, sizeof(float) * d.nCells)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&S->xq, sizeof(unsigned long long) * 2 * d.nCells)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->brickW, sizeof(int) * MC)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->cntPart, sizeof(int2) * smCount)) != cudaSuccess) return e;
   if ((e = cudaMalloc(&S->actLin, sizeof(int) * nB)) != cudaSuccess) return e;
@@ -878,7 +924,7 @@ cudaError_t sor_tb_init(void** statePtr, const Dims& d, int device) {
 void sor_tb_free(void* statePtr) {
   TbState* S = (TbState*)statePtr;
   if (!S) return;
-  cudaFree(S->ctl); cudaFree(S->q1); cudaFree(S->brickW); cudaFree(S->cntPart); cudaFree(S->actLin);
+  cudaFree(S->ctl); cudaFree(S->xq); cudaFree(S->brickW); cudaFree(S->cntPart); cudaFree(S->actLin);
   cudaFree(S->actWPre); cudaFree(S->brickOrd); cudaFree(S->chunkStart); cudaFree(S->resPart);
   delete S;
 }
@@ -891,7 +937,7 @@ cudaError_t launch_sor_tb(void* statePtr, const Dims& d, const GridDev& g, const
   cudaError_t e = cudaMemsetAsync(S->ctl, 0, sizeof(TbCtl), s);
   if (e != cudaSuccess) return e;
   TbArgs a;
-  a.d = d; a.q = g.q; a.q1 = S->q1; a.rhs = g.rhs; a.pw = g.pw; a.diag8 = diag8;
+  a.d = d; a.q = g.q; a.xq = S->xq; a.rhs = g.rhs; a.pw = g.pw; a.diag8 = diag8;
   a.nbx = S->nbx; a.nby = S->nby; a.nbz = S->nbz; a.mbits = S->mbits;
   a.brickW = S->brickW; a.cntPart = S->cntPart; a.actLin = S->actLin; a.actWPre = S->actWPre;
   a.brickOrd = S->brickOrd; a.chunkStart = S->chunkStart; a.resPart = S->resPart; a.ctl = S->ctl;
