@@ -445,10 +445,11 @@ def roofline(fs, ms_step, iters):
     # on this 128^3 planet: the temporal-blocked solve loads its system into
     # shared memory once and iterates from there (halo exchanges hit L2), so
     # its traffic hardly depends on the iteration count
-    captured = {"k_sor_tb": (16125696.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 150-iteration "
-                                         "solve of this planet (bench.py --profile 4 --learned-profile); the "
-                                         "system is read once, the iterations run from shared memory and L2"),
-                "k_g2p_advect": (66053376.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture at 128^3")}
+    captured = {"k_sor_tb": (17864496.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 60-iteration "
+                                         "solve of this planet (bench.py --profile 3); the system is read once, "
+                                         "the iterations run from shared memory and L2"),
+                "k_p2g": (53146880.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture at 128^3"),
+                "k_g2p_advect": (65502208.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture at 128^3")}
     traffic, note = captured.get(name, (None, None)) if WORKLOAD["name"] == "planet128" else (None, None)
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": kind, "traffic": traffic, "traffic_note": note,

@@ -70,7 +70,6 @@ struct TbCtl {
   unsigned resCount;             // residual partials published so far (all checks)
   int overflow;                  // some region did not fit: every CTA takes the fallback
   int pad[12];
-  unsigned flag[kMaxCtas];       // last epoch each CTA published
 };
 
 struct TbArgs {
@@ -115,8 +114,6 @@ struct TbSmem {
   unsigned short lDense[kLMax];
   unsigned lGlob[kLMax];
   unsigned oGlob[kOMax];                  // global index of each owned entry (buckets 0 and 4, in order)
-  unsigned short deps[kMaxCtas];
-  unsigned depMask[kMaxCtas / 32];
 };
 
 __device__ __forceinline__ unsigned compact1by2(unsigned x) {
@@ -140,9 +137,6 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 }
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
 // bounded grid barrier on ctl->barCount/barGen; false when a wait timed out
@@ -334,7 +328,7 @@ extern __shared__ __align__(16) unsigned char tb_smem_raw[];
 // The whole solve in one cooperative launch of one 1024-thread CTA per SM.
 __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   TbSmem& S = *reinterpret_cast<TbSmem*>(tb_smem_raw);
-  __shared__ int sAbort, sOverflow, nRegion, nReload, nDeps, sT0, sT1, sA;
+  __shared__ int sAbort, sOverflow, nRegion, nReload, sT0, sT1, sA;
   __shared__ int bucket[8], bstart[8], bcur[8];
   __shared__ int2 sScan[33];
   __shared__ double2 sRed[32];
@@ -345,7 +339,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
   const Dims& d = a.d;
   int it = 0, O = 0, R = 0, path = 3;
   double rel = -1;
-  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; nDeps = 0; }
+  if (tid == 0) { sAbort = 0; sOverflow = 0; nRegion = 0; nReload = 0; }
   if (tid < 8) bucket[tid] = 0;
   __syncthreads();
 
@@ -466,7 +460,6 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       if (nRegion > kRbMax) sOverflow = 1;
     }
     for (int h = tid; h < kHashSlots; h += T) S.hkey[h] = -1;
-    for (int w = tid; w < kMaxCtas / 32; w += T) S.depMask[w] = 0;
     __syncthreads();
     const int t0 = sT0;
     O = sT1 - sT0;
@@ -656,18 +649,8 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
       }
     }
     if (tid == 0 && nReload > kLMax) sOverflow = 1;
-    // the CTAs owning halo bricks: this CTA's neighbours in both directions
-    for (int s = O + tid; s < R; s += T) atomicOr(&S.depMask[S.rbOwn[s] >> 5], 1u << (S.rbOwn[s] & 31));
     __syncthreads();
-    if (tid == 0) {
-      int n = 0;
-      for (int w = 0; w < (P + 31) / 32; w++) {
-        unsigned m = S.depMask[w];
-        while (m) { const int bit = __ffs(m) - 1; m &= m - 1; S.deps[n++] = (unsigned short)(w * 32 + bit); }
-      }
-      nDeps = n;
-      if (sOverflow) atomicOr(&a.ctl->overflow, 1);
-    }
+    if (tid == 0 && sOverflow) atomicOr(&a.ctl->overflow, 1);
     // the owned cells' exchange words start with tag 0 (epochs count from 1)
     if (!sOverflow) {
       const int nOwn = bucket[0] + bucket[4];
