@@ -205,47 +205,46 @@ void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const
 // one float2 vector atomic per face (momentum, weight). FP32 arithmetic: the
 // face indices and fractions are exact (face_coords_f), the weights and
 // terms carry FP32 rounding (a few 1e-8 relative against the double sums).
-__device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc, int comp,
-                                         float x, float y, float z, float vel) {
-  int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
-  face_coords_f(d, comp, x, y, z, i0, j0, k0, tx, ty, tz);
-  face_strides(d, comp, i0, j0, k0, idx, sj, sk);
+// one particle's eight (momentum, weight) terms of component comp
+__device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc, const Stencil3& S, int comp,
+                                         float vel) {
+  unsigned sj, sk;
+  face_strides32(d, comp, sj, sk);
+  const float tx = S.tx[comp], ty = S.ty[comp], tz = S.tz[comp];
   const float s0 = 1.f - tx, s1 = tx, t0 = 1.f - ty, t1 = ty, r0 = 1.f - tz, r1 = tz;
   const float wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
   const float w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
-  const long long o8[8] = { idx, idx + 1, idx + sj, idx + sj + 1, idx + sk, idx + sk + 1, idx + sk + sj,
-                            idx + sk + sj + 1 };
+  float2* p = acc + S.idx[comp];
+  const unsigned o8[8] = { 0u, 1u, sj, sj + 1, sk, sk + 1, sk + sj, sk + sj + 1 };
 #pragma unroll
-  for (int q = 0; q < 8; q++) atomicAdd(&acc[o8[q]], make_float2(w8[q] * vel, w8[q]));
+  for (int q = 0; q < 8; q++) atomicAdd(p + o8[q], make_float2(w8[q] * vel, w8[q]));
 }
 // Two consecutive particles (the fill lays particles out row by row, so they
 // are usually within a cell of each other): when their stencils of one
 // component start at the same face, their eight (momentum, weight) pairs are
 // summed in registers and sent as eight atomics instead of sixteen.
-__device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc, int comp,
-                                         float x0, float y0, float z0, float v0,
-                                         float x1, float y1, float z1, float v1) {
-  int i0, j0, k0, i1, j1, k1; float tx0, ty0, tz0, tx1, ty1, tz1; long long idx0, idx1, sj, sk;
-  face_coords_f(d, comp, x0, y0, z0, i0, j0, k0, tx0, ty0, tz0);
-  face_coords_f(d, comp, x1, y1, z1, i1, j1, k1, tx1, ty1, tz1);
-  face_strides(d, comp, i0, j0, k0, idx0, sj, sk);
-  face_strides(d, comp, i1, j1, k1, idx1, sj, sk);
-  if (idx0 != idx1) {
-    p2g_comp(d, acc, comp, x0, y0, z0, v0);
-    p2g_comp(d, acc, comp, x1, y1, z1, v1);
+__device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc, const Stencil3& S0,
+                                         const Stencil3& S1, int comp, float v0, float v1) {
+  if (S0.idx[comp] != S1.idx[comp]) {
+    p2g_comp(d, acc, S0, comp, v0);
+    p2g_comp(d, acc, S1, comp, v1);
     return;
   }
+  unsigned sj, sk;
+  face_strides32(d, comp, sj, sk);
+  const float tx0 = S0.tx[comp], ty0 = S0.ty[comp], tz0 = S0.tz[comp];
+  const float tx1 = S1.tx[comp], ty1 = S1.ty[comp], tz1 = S1.tz[comp];
   const float a0 = 1.f - tx0, a1 = tx0, b0 = 1.f - ty0, b1 = ty0, c0 = 1.f - tz0, c1 = tz0;
   const float e0 = 1.f - tx1, e1 = tx1, f0 = 1.f - ty1, f1 = ty1, h0 = 1.f - tz1, h1 = tz1;
   const float pA = a0 * b0, pB = a1 * b0, pC = a0 * b1, pD = a1 * b1;
   const float qA = e0 * f0, qB = e1 * f0, qC = e0 * f1, qD = e1 * f1;
   const float wp[8] = { pA * c0, pB * c0, pC * c0, pD * c0, pA * c1, pB * c1, pC * c1, pD * c1 };
   const float wq[8] = { qA * h0, qB * h0, qC * h0, qD * h0, qA * h1, qB * h1, qC * h1, qD * h1 };
-  const long long o8[8] = { idx0, idx0 + 1, idx0 + sj, idx0 + sj + 1, idx0 + sk, idx0 + sk + 1, idx0 + sk + sj,
-                            idx0 + sk + sj + 1 };
+  float2* p = acc + S0.idx[comp];
+  const unsigned o8[8] = { 0u, 1u, sj, sj + 1, sk, sk + 1, sk + sj, sk + sj + 1 };
 #pragma unroll
   for (int q = 0; q < 8; q++)
-    atomicAdd(&acc[o8[q]], make_float2(fmaf(wq[q], v1, wp[q] * v0), wp[q] + wq[q]));
+    atomicAdd(p + o8[q], make_float2(fmaf(wq[q], v1, wp[q] * v0), wp[q] + wq[q]));
 }
 __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, int* err) {
   const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
@@ -261,14 +260,18 @@ __global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, i
   const bool a = fl0 == 0 && particle_sound_f(x0, y0, z0, u0, v0, w0, err);
   const bool b = fl1 == 0 && particle_sound_f(x1, y1, z1, u1, v1, w1, err);
   if (a && b) {
-    p2g_pair(d, g.acc, 0, x0, y0, z0, u0, x1, y1, z1, u1);
-    p2g_pair(d, g.acc, 1, x0, y0, z0, v0, x1, y1, z1, v1);
-    p2g_pair(d, g.acc, 2, x0, y0, z0, w0, x1, y1, z1, w1);
+    Stencil3 S0, S1;
+    face_stencil3_f(d, x0, y0, z0, S0);
+    face_stencil3_f(d, x1, y1, z1, S1);
+    p2g_pair(d, g.acc, S0, S1, 0, u0, u1);
+    p2g_pair(d, g.acc, S0, S1, 1, v0, v1);
+    p2g_pair(d, g.acc, S0, S1, 2, w0, w1);
   } else if (a || b) {
-    const float x = a ? x0 : x1, y = a ? y0 : y1, z = a ? z0 : z1;
-    p2g_comp(d, g.acc, 0, x, y, z, a ? u0 : u1);
-    p2g_comp(d, g.acc, 1, x, y, z, a ? v0 : v1);
-    p2g_comp(d, g.acc, 2, x, y, z, a ? w0 : w1);
+    Stencil3 S;
+    face_stencil3_f(d, a ? x0 : x1, a ? y0 : y1, a ? z0 : z1, S);
+    p2g_comp(d, g.acc, S, 0, a ? u0 : u1);
+    p2g_comp(d, g.acc, S, 1, a ? v0 : v1);
+    p2g_comp(d, g.acc, S, 2, a ? w0 : w1);
   }
 }
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s) {
@@ -915,8 +918,11 @@ template <int OP>
 __global__ void __launch_bounds__(256) k_faces_bricks(Dims d, GridDev g, BrickSet B, FacePassArgs fa, DevStatus* st) {
   const int n = *B.count;
   float umax = 0.f;
+  int b = (int)blockIdx.x < n ? B.list[blockIdx.x] : 0;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
-    const int b = B.list[it];
+    // the next brick's id is loaded before this brick's faces are touched, so
+    // its round trip overlaps this brick's loads and stores
+    const int bNext = it + (int)gridDim.x < n ? B.list[it + gridDim.x] : 0;
     long long f; FaceIJK F;
     if (threadIdx.x < 240 && brick_face(d, B, b, threadIdx.x, f, F)) {
       if (OP == 0) face_normalize_bc(d, g, f, F);
@@ -925,6 +931,7 @@ __global__ void __launch_bounds__(256) k_faces_bricks(Dims d, GridDev g, BrickSe
       else if (OP == 3) { if (g.valid[f] == 0) face_extrapolate(d, g, f, F); }
       else g.acc[f] = make_float2(0.f, 0.f);
     }
+    b = bNext;
   }
   if (OP == 2 && fa.doClamp) umax_reduce(umax, st);
 }

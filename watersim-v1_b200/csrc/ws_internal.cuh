@@ -364,16 +364,78 @@ __device__ __forceinline__ float tri_sample_f(const float* __restrict__ a, long 
   const float e0 = fmaf(ty, c1 - c0, c0), e1 = fmaf(ty, c3 - c2, c2);
   return fmaf(tz, e1 - e0, e0);
 }
+// The stencils of all three components at one position, FP32, with 32-bit
+// face offsets (face counts stay below 2^32 for grids up to 1000^3). The
+// clamps of face_coords depend only on the axis (i in [0, nx - 1], j in
+// [0, ny - 2], k in [0, nz - 2]), and each component takes, per axis, either
+// the coordinate or the coordinate less half a cell; so six floors serve the
+// nine (index, fraction) pairs, bit for bit those of face_coords_f.
+struct Stencil3 {
+  unsigned idx[3];              // first face of each component's 2x2x2 stencil
+  float tx[3], ty[3], tz[3];
+};
+__device__ __forceinline__ void axis_floor_frac(float a, int hi, int& i0, float& t) {
+  const float f = floorf(a);
+  if (f < 0.f) { i0 = 0; t = 0.f; } else if (f > (float)hi) { i0 = hi; t = 1.f; } else { i0 = (int)f; t = a - f; }
+}
+// j and k strides of component comp, 32-bit
+__device__ __forceinline__ void face_strides32(const Dims& d, int comp, unsigned& sj, unsigned& sk) {
+  const unsigned nx = (unsigned)d.nx, ny = (unsigned)d.ny;
+  if (comp == 0) { sj = nx + 1; sk = ny * (nx + 1); }
+  else if (comp == 1) { sj = nx; sk = (ny + 1) * nx; }
+  else { sj = nx; sk = ny * nx; }
+}
+__device__ __forceinline__ void face_stencil3_f(const Dims& d, float x, float y, float z, Stencil3& S) {
+  const unsigned nx = (unsigned)d.nx, ny = (unsigned)d.ny, uN = (unsigned)d.uN, vN = (unsigned)d.vN;
+  if (!d.dxPow2) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int i0, j0, k0;
+      face_coords_f(d, c, x, y, z, i0, j0, k0, S.tx[c], S.ty[c], S.tz[c]);
+      S.idx[c] = c == 0 ? ((unsigned)k0 * ny + (unsigned)j0) * (nx + 1) + (unsigned)i0
+               : c == 1 ? uN + ((unsigned)k0 * (ny + 1) + (unsigned)j0) * nx + (unsigned)i0
+                        : uN + vN + ((unsigned)k0 * ny + (unsigned)j0) * nx + (unsigned)i0;
+    }
+    return;
+  }
+  const float r = (float)d.rdx;
+  const float X = x * r, Y = y * r, Z = z * r;
+  int iF, iH, jF, jH, kF, kH;
+  float txF, txH, tyF, tyH, tzF, tzH;
+  axis_floor_frac(X, d.nx - 1, iF, txF); axis_floor_frac(X - 0.5f, d.nx - 1, iH, txH);
+  axis_floor_frac(Y, d.ny - 2, jF, tyF); axis_floor_frac(Y - 0.5f, d.ny - 2, jH, tyH);
+  axis_floor_frac(Z, d.nz - 2, kF, tzF); axis_floor_frac(Z - 0.5f, d.nz - 2, kH, tzH);
+  S.idx[0] = ((unsigned)kH * ny + (unsigned)jH) * (nx + 1) + (unsigned)iF;
+  S.tx[0] = txF; S.ty[0] = tyH; S.tz[0] = tzH;
+  S.idx[1] = uN + ((unsigned)kH * (ny + 1) + (unsigned)jF) * nx + (unsigned)iH;
+  S.tx[1] = txH; S.ty[1] = tyF; S.tz[1] = tzH;
+  S.idx[2] = uN + vN + ((unsigned)kF * ny + (unsigned)jH) * nx + (unsigned)iH;
+  S.tx[2] = txH; S.ty[2] = tyH; S.tz[2] = tzF;
+}
+// trilinear blend of component comp's stencil in S (tri_sample_f with 32-bit offsets)
+__device__ __forceinline__ float stencil_sample(const Dims& d, const float* __restrict__ a, const Stencil3& S, int comp) {
+  unsigned sj, sk;
+  face_strides32(d, comp, sj, sk);
+  const float* p0 = a + S.idx[comp];
+  const float* p1 = p0 + sj;
+  const float* p2 = p0 + sk;
+  const float* p3 = p2 + sj;
+  const float a00 = p0[0], a10 = p0[1], a01 = p1[0], a11 = p1[1];
+  const float b00 = p2[0], b10 = p2[1], b01 = p3[0], b11 = p3[1];
+  const float tx = S.tx[comp], ty = S.ty[comp], tz = S.tz[comp];
+  const float c0 = fmaf(tx, a10 - a00, a00), c1 = fmaf(tx, a11 - a01, a01);
+  const float c2 = fmaf(tx, b10 - b00, b00), c3 = fmaf(tx, b11 - b01, b01);
+  const float e0 = fmaf(ty, c1 - c0, c0), e1 = fmaf(ty, c3 - c2, c2);
+  return fmaf(tz, e1 - e0, e0);
+}
 // _sampleVel3 (js/solver.js:820-854) in FP32
 __device__ __forceinline__ void sample_vel3_f(const Dims& d, const float* __restrict__ vel, float x, float y, float z,
                                               float& ox, float& oy, float& oz) {
-  int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
-  face_coords_f(d, 0, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
-  ox = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
-  face_coords_f(d, 1, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
-  oy = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
-  face_coords_f(d, 2, x, y, z, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
-  oz = tri_sample_f(vel, idx, sj, sk, tx, ty, tz);
+  Stencil3 S;
+  face_stencil3_f(d, x, y, z, S);
+  ox = stencil_sample(d, vel, S, 0);
+  oy = stencil_sample(d, vel, S, 1);
+  oz = stencil_sample(d, vel, S, 2);
 }
 
 // block-wide helpers

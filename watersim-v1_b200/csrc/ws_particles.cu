@@ -35,14 +35,11 @@ __global__ void __launch_bounds__(256, 4) k_g2p_advect(Dims d, GridDev g, PartsD
       sample_vel3_f(d, g.vel, xf, yf, zf, a0, a1, a2);
     } else {
       // FP32 sampling at the stored position (exact face indices and fractions)
-      int i0, j0, k0; float tx, ty, tz; long long idx, sj, sk;
-      float ou, ov, ow;
-      face_coords_f(d, 0, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 0, i0, j0, k0, idx, sj, sk);
-      ou = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a0 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
-      face_coords_f(d, 1, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 1, i0, j0, k0, idx, sj, sk);
-      ov = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a1 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
-      face_coords_f(d, 2, xf, yf, zf, i0, j0, k0, tx, ty, tz); face_strides(d, 2, i0, j0, k0, idx, sj, sk);
-      ow = tri_sample_f(g.velO, idx, sj, sk, tx, ty, tz); a2 = tri_sample_f(g.vel, idx, sj, sk, tx, ty, tz);
+      Stencil3 S;
+      face_stencil3_f(d, xf, yf, zf, S);
+      const float ou = stencil_sample(d, g.velO, S, 0), ov = stencil_sample(d, g.velO, S, 1);
+      const float ow = stencil_sample(d, g.velO, S, 2);
+      a0 = stencil_sample(d, g.vel, S, 0); a1 = stencil_sample(d, g.vel, S, 1); a2 = stencil_sample(d, g.vel, S, 2);
       const float pic = (float)ap.pic, flip = (float)(1 - ap.pic);
       fvx = fmaf(fvx + a0 - ou, flip, a0 * pic);
       fvy = fmaf(fvy + a1 - ov, flip, a1 * pic);
