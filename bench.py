@@ -903,7 +903,7 @@ def main():
         METRIC_PLAIN = ("substeps/s @%d^3/%dM particles (plain red-black SOR to 1e-5 relative divergence residual)"
                         % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000))
         METRIC = ("substeps/s @%d^3/%dM particles: learned warm-start (%d-level U-Net) vs plain SOR at equal "
-                  "\u2016\u2207\u00b7u\u2016" % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000, WORKLOAD["levels"]))
+                  "\u2016\u2207\u00b7u\u2016" % (WORKLOAD["n"], WORKLOAD["particles"] // 1000000, WORKLOAD.get("levels", 3)))
     frames = args.frames or args.workload == "planet64"
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

@@ -323,6 +323,7 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
   {
     BrickSet& B = h->bricks;
     B.nbx = (d.nx + 3) / 4; B.nby = (d.ny + 3) / 4; B.nbz = (d.nz + 3) / 4;
+    B.dnbx = fastdiv_make((unsigned)B.nbx); B.dnby = fastdiv_make((unsigned)B.nby);
     const long long nB = (long long)B.nbx * B.nby * B.nbz;
     AL(B.seed, nB) AL(B.act, nB) AL(B.proc, nB) AL(B.list, nB) AL(B.count, 1) AL(B.forceAll, 1) AL(h->brickIota, nB)
     h->brickCubBytes = brick_list_scratch_bytes((int)nB);

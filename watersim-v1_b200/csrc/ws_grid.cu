@@ -374,7 +374,8 @@ __global__ void __launch_bounds__(256) k_p2g_bricks(Dims d, GridDev g, PartsDev 
     if (n <= 0) continue;                              // uniform over the block
     if (threadIdx.x < 64) cs.count[(b << 6) + threadIdx.x] = 0;   // zero again for the next binning
     if (s0 < 0 || s0 + n > cs.cap) { if (threadIdx.x == 0) atomicOr(err, WS_DERR_RANGE); continue; }
-    const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
+    int bx, by, bz;
+    brick_coords(B, b, bx, by, bz);
     const int fx = bx * 4, fy = by * 4, fz = bz * 4;
     for (int t = threadIdx.x; t < 6 * kBrickFaces; t += blockDim.x) sm[t] = 0.f;
     __syncthreads();
@@ -810,13 +811,16 @@ __device__ __forceinline__ void face_extrapolate(const Dims& d, const GridDev& g
   else { d0 = d.nx; d1 = d.ny; d2 = d.nz + 1; }
   long long sK = (long long)d0 * d1;
   const float* a = g.vel;
+  // every in-range neighbour's flag and velocity in one round trip, then the
+  // sum over the originally valid ones in the fixed order -x, +x, -y, +y, -z, +z
+  const long long o[6] = { f - 1, f + 1, f - d0, f + d0, f - sK, f + sK };
+  const bool in[6] = { F.i > 0, F.i < d0 - 1, F.j > 0, F.j < d1 - 1, F.k > 0, F.k < d2 - 1 };
+  uint8_t vv[6]; float av[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) { vv[q] = in[q] ? valid[o[q]] : (uint8_t)0; av[q] = in[q] ? a[o[q]] : 0.f; }
   double sum = 0; int cnt = 0;
-  if (F.i > 0 && valid[f - 1] == 1) { sum += a[f - 1]; cnt++; }
-  if (F.i < d0 - 1 && valid[f + 1] == 1) { sum += a[f + 1]; cnt++; }
-  if (F.j > 0 && valid[f - d0] == 1) { sum += a[f - d0]; cnt++; }
-  if (F.j < d1 - 1 && valid[f + d0] == 1) { sum += a[f + d0]; cnt++; }
-  if (F.k > 0 && valid[f - sK] == 1) { sum += a[f - sK]; cnt++; }
-  if (F.k < d2 - 1 && valid[f + sK] == 1) { sum += a[f + sK]; cnt++; }
+#pragma unroll
+  for (int q = 0; q < 6; q++) if (vv[q] == 1) { sum += av[q]; cnt++; }
   if (cnt > 0) { g.vel[f] = (float)(sum / cnt); g.valid[f] = 2; }
 }
 __global__ void k_extrapolate(Dims d, GridDev g) {
@@ -880,14 +884,23 @@ cudaError_t launch_brick_activity(const BrickSet& B, const int* iota, void* scra
 
 // The faces a brick owns: per component, the 64 faces whose lower cell lies
 // in the brick, and on the last brick along the component's axis the 16
-// faces of the domain's upper plane. Slot t in [0, 240).
-__device__ __forceinline__ bool brick_face(const Dims& d, const BrickSet& B, int b, int t, long long& f, FaceIJK& F) {
-  const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
-  const int comp = t / 80, s = t - comp * 80;
-  int la, lb, lc;
-  const bool upper = s >= 64;
-  if (!upper) { la = s & 3; lb = (s >> 2) & 3; lc = s >> 4; }
-  else { la = 0; lb = (s - 64) & 3; lc = (s - 64) >> 2; }
+// faces of the domain's upper plane. Slot t in [0, 240): its component and
+// offsets in the brick are the same for every brick, so a thread decodes
+// them once (face_slot) and each brick adds only its coordinates.
+struct FaceSlot { int comp, la, lb, lc; bool upper; };
+__device__ __forceinline__ FaceSlot face_slot(int t) {
+  FaceSlot sl;
+  sl.comp = t >= 160 ? 2 : t >= 80 ? 1 : 0;
+  const int s = t - sl.comp * 80;
+  sl.upper = s >= 64;
+  if (!sl.upper) { sl.la = s & 3; sl.lb = (s >> 2) & 3; sl.lc = s >> 4; }
+  else { sl.la = 0; sl.lb = (s - 64) & 3; sl.lc = (s - 64) >> 2; }
+  return sl;
+}
+__device__ __forceinline__ bool brick_face(const Dims& d, const BrickSet& B, int bx, int by, int bz, const FaceSlot& sl,
+                                           long long& f, FaceIJK& F) {
+  const int comp = sl.comp, la = sl.la, lb = sl.lb, lc = sl.lc;
+  const bool upper = sl.upper;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   F.comp = comp;
   if (comp == 0) {
@@ -918,13 +931,16 @@ template <int OP>
 __global__ void __launch_bounds__(256) k_faces_bricks(Dims d, GridDev g, BrickSet B, FacePassArgs fa, DevStatus* st) {
   const int n = *B.count;
   float umax = 0.f;
+  const FaceSlot sl = face_slot(threadIdx.x < 240 ? (int)threadIdx.x : 0);
   int b = (int)blockIdx.x < n ? B.list[blockIdx.x] : 0;
   for (int it = blockIdx.x; it < n; it += gridDim.x) {
     // the next brick's id is loaded before this brick's faces are touched, so
     // its round trip overlaps this brick's loads and stores
     const int bNext = it + (int)gridDim.x < n ? B.list[it + gridDim.x] : 0;
     long long f; FaceIJK F;
-    if (threadIdx.x < 240 && brick_face(d, B, b, threadIdx.x, f, F)) {
+    int bx, by, bz;
+    brick_coords(B, b, bx, by, bz);
+    if (threadIdx.x < 240 && brick_face(d, B, bx, by, bz, sl, f, F)) {
       if (OP == 0) face_normalize_bc(d, g, f, F);
       else if (OP == 1) face_forces(d, g, f, F, fa.coef, fa.viscOn, fa.dt, fa.gs);
       else if (OP == 2) umax = fmaxf(umax, fabsf(face_project(d, g, f, F, fa.doClamp, fa.vcap)));
@@ -978,7 +994,8 @@ __global__ void __launch_bounds__(256) k_pressure_setup_bricks(Dims d, GridDev g
     const int e = it + (threadIdx.x >> 6);
     if (e >= n) continue;
     const int b = B.list[e], c = threadIdx.x & 63;
-    const int bx = b % B.nbx, r = b / B.nbx, by = r % B.nby, bz = r / B.nby;
+    int bx, by, bz;
+    brick_coords(B, b, bx, by, bz);
     const int i = bx * 4 + (c & 3), j = by * 4 + ((c >> 2) & 3), k = bz * 4 + (c >> 4);
     if (i >= d.nx || j >= d.ny || k >= d.nz) continue;
     int col;

@@ -156,7 +156,13 @@ struct BrickSet {
   int* list;                // the bricks with proc set, in increasing order
   int* count;
   int* forceAll;            // device flag: process every brick once
+  FastDiv dnbx, dnby;       // division by nbx and nby (brick coordinates of a linear brick index)
 };
+// (bx, by, bz) of linear brick b = (bz * nby + by) * nbx + bx
+__device__ __forceinline__ void brick_coords(const BrickSet& B, int b, int& bx, int& by, int& bz) {
+  const unsigned r = fastdiv((unsigned)b, B.dnbx), z = fastdiv(r, B.dnby);
+  bx = b - (int)(r * (unsigned)B.nbx); by = (int)(r - z * (unsigned)B.nby); bz = (int)z;
+}
 // Counting sort of the grid-coupled particles by cell, rebuilt every
 // substep: P2G then walks each cell's particles in a row. The particle
 // arrays themselves stay in index order (the serial random streams of the
