@@ -3,8 +3,9 @@
 //
 // Partition. The grid is cut into 4x4x4-cell bricks. Bricks holding a fluid
 // cell are taken in Morton order and split into one contiguous chunk per CTA
-// with equal counts of interior fluid cells, so each CTA owns a compact
-// patch of the ocean shell (about 700 cells at 128^3).
+// with equal shares of weight (interior fluid cells plus kBrickWeight per
+// brick), so each CTA owns a compact patch of the ocean shell (about 700
+// cells at 128^3).
 //
 // Region. A CTA keeps in shared memory its owned bricks plus every active
 // brick among their 26 neighbours, densely (64 q values per brick). The
@@ -63,6 +64,12 @@ constexpr int kHashSlots = 1024;            // open-addressing table of region b
 constexpr int kZero = kRbMax * 64;          // dense index of the always-zero cell
 constexpr long long kTbSpinLimit = 4000000LL;
 constexpr int kMaxCtas = 1024;
+// Chunk weight of an active brick: its interior fluid cells plus this much.
+// Equal shares of fluid alone gave CTAs 13-55 owned bricks at 128^3 (bricks
+// at the shell's edges hold few fluid cells), and the CTA with the most
+// bricks has the largest region, which every other CTA waits for at the end
+// of the plan; the per-brick term evens out the brick counts too.
+constexpr int kBrickWeight = 16;
 
 // device control block, zeroed before every solve
 struct TbCtl {
@@ -80,10 +87,10 @@ struct TbArgs {
   const float* pw;               // omega/diag, negative off the fluid
   const uint8_t* diag8;
   int nbx, nby, nbz, mbits;      // bricks per axis; Morton cube side 2^mbits
-  int* brickW;                   // per Morton code: interior fluid count | any-fluid << 8
+  int* brickW;                   // per Morton code: chunk weight (interior fluid + kBrickWeight) | any-fluid << 8
   int2* cntPart;                 // per CTA: (active bricks, interior fluid cells) of its Morton chunk
   int* actLin;                   // active brick t -> linear brick index
-  int* actWPre;                  // active brick t -> interior fluid cells before it
+  int* actWPre;                  // active brick t -> chunk weight before it
   int* brickOrd;                 // linear brick -> active ordinal, -1 inactive
   int* chunkStart;               // CTA -> first owned active brick ([P] = number of active bricks)
   double2* resPart;              // 2 x P residual partials
@@ -163,8 +170,8 @@ __device__ bool tb_grid_barrier(TbCtl* ctl, int* err, int* sAbort) {
   return *(volatile int*)sAbort == 0;
 }
 
-// the CTA that owns an active brick with `wpre` interior fluid cells before
-// it in Morton order (trailing bricks without interior fluid go to the last)
+// the CTA that owns an active brick with chunk weight `wpre` before
+// it in Morton order (NF: the total weight)
 __device__ __forceinline__ int owner_of(long long wpre, int P, long long NF) {
   if (NF <= 0) return 0;
   long long o = wpre * P / NF;
@@ -383,6 +390,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
         act |= __shfl_down_sync(0xffffffffu, act, o, 16);
       }
       if ((tid & 15) == 0 && m < c1) {
+        w += act * kBrickWeight;
         a.brickW[m] = w | (act << 8);
         actSum += act; wSum += w;
       }
