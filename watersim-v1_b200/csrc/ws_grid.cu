@@ -205,78 +205,95 @@ void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const
 // one float2 vector atomic per face (momentum, weight). FP32 arithmetic: the
 // face indices and fractions are exact (face_coords_f), the weights and
 // terms carry FP32 rounding (a few 1e-8 relative against the double sums).
-// one particle's eight (momentum, weight) terms of component comp
-__device__ __forceinline__ void p2g_comp(const Dims& d, float2* __restrict__ acc, const Stencil3& S, int comp,
-                                         float vel) {
+//
+// Runs of consecutive particles: each thread scatters four consecutive
+// particles (the fill's lattice runs along x about a third of a cell apart,
+// so three or four neighbours in index order usually share a stencil). Per
+// component, the particles' (momentum, weight) terms are summed in registers
+// while their stencils start at the same face, and each run sends one set of
+// eight float2 atomics.
+template <int COMP>
+__device__ __forceinline__ void p2g_run_comp(const Dims& d, float2* __restrict__ acc, const float (&x)[4],
+                                             const float (&y)[4], const float (&z)[4], const float (&v)[4],
+                                             unsigned okMask) {
   unsigned sj, sk;
-  face_strides32(d, comp, sj, sk);
-  const float tx = S.tx[comp], ty = S.ty[comp], tz = S.tz[comp];
-  const float s0 = 1.f - tx, s1 = tx, t0 = 1.f - ty, t1 = ty, r0 = 1.f - tz, r1 = tz;
-  const float wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
-  const float w8[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
-  float2* p = acc + S.idx[comp];
-  const unsigned o8[8] = { 0u, 1u, sj, sj + 1, sk, sk + 1, sk + sj, sk + sj + 1 };
-#pragma unroll
-  for (int q = 0; q < 8; q++) atomicAdd(p + o8[q], make_float2(w8[q] * vel, w8[q]));
-}
-// Two consecutive particles (the fill lays particles out row by row, so they
-// are usually within a cell of each other): when their stencils of one
-// component start at the same face, their eight (momentum, weight) pairs are
-// summed in registers and sent as eight atomics instead of sixteen.
-__device__ __forceinline__ void p2g_pair(const Dims& d, float2* __restrict__ acc, const Stencil3& S0,
-                                         const Stencil3& S1, int comp, float v0, float v1) {
-  if (S0.idx[comp] != S1.idx[comp]) {
-    p2g_comp(d, acc, S0, comp, v0);
-    p2g_comp(d, acc, S1, comp, v1);
-    return;
+  face_strides32(d, COMP, sj, sk);
+  const unsigned nx = (unsigned)d.nx, ny = (unsigned)d.ny, uN = (unsigned)d.uN, vN = (unsigned)d.vN;
+  float m8[8], w8[8];
+  unsigned cur = 0xffffffffu;
+#define WS_P2G_FLUSH                                                                         \
+  if (cur != 0xffffffffu) {                                                                  \
+    float2* p = acc + cur;                                                                   \
+    atomicAdd(p, make_float2(m8[0], w8[0]));                                                 \
+    atomicAdd(p + 1, make_float2(m8[1], w8[1]));                                             \
+    atomicAdd(p + sj, make_float2(m8[2], w8[2]));                                            \
+    atomicAdd(p + sj + 1, make_float2(m8[3], w8[3]));                                        \
+    atomicAdd(p + sk, make_float2(m8[4], w8[4]));                                            \
+    atomicAdd(p + sk + 1, make_float2(m8[5], w8[5]));                                        \
+    atomicAdd(p + sk + sj, make_float2(m8[6], w8[6]));                                       \
+    atomicAdd(p + sk + sj + 1, make_float2(m8[7], w8[7]));                                   \
   }
-  unsigned sj, sk;
-  face_strides32(d, comp, sj, sk);
-  const float tx0 = S0.tx[comp], ty0 = S0.ty[comp], tz0 = S0.tz[comp];
-  const float tx1 = S1.tx[comp], ty1 = S1.ty[comp], tz1 = S1.tz[comp];
-  const float a0 = 1.f - tx0, a1 = tx0, b0 = 1.f - ty0, b1 = ty0, c0 = 1.f - tz0, c1 = tz0;
-  const float e0 = 1.f - tx1, e1 = tx1, f0 = 1.f - ty1, f1 = ty1, h0 = 1.f - tz1, h1 = tz1;
-  const float pA = a0 * b0, pB = a1 * b0, pC = a0 * b1, pD = a1 * b1;
-  const float qA = e0 * f0, qB = e1 * f0, qC = e0 * f1, qD = e1 * f1;
-  const float wp[8] = { pA * c0, pB * c0, pC * c0, pD * c0, pA * c1, pB * c1, pC * c1, pD * c1 };
-  const float wq[8] = { qA * h0, qB * h0, qC * h0, qD * h0, qA * h1, qB * h1, qC * h1, qD * h1 };
-  float2* p = acc + S0.idx[comp];
-  const unsigned o8[8] = { 0u, 1u, sj, sj + 1, sk, sk + 1, sk + sj, sk + sj + 1 };
 #pragma unroll
-  for (int q = 0; q < 8; q++)
-    atomicAdd(p + o8[q], make_float2(fmaf(wq[q], v1, wp[q] * v0), wp[q] + wq[q]));
+  for (int r = 0; r < 4; r++) {
+    if (!((okMask >> r) & 1u)) continue;
+    int i0, j0, k0; float tx, ty, tz;
+    face_coords_f(d, COMP, x[r], y[r], z[r], i0, j0, k0, tx, ty, tz);
+    const unsigned idx = COMP == 0 ? ((unsigned)k0 * ny + (unsigned)j0) * (nx + 1) + (unsigned)i0
+                       : COMP == 1 ? uN + ((unsigned)k0 * (ny + 1) + (unsigned)j0) * nx + (unsigned)i0
+                                   : uN + vN + ((unsigned)k0 * ny + (unsigned)j0) * nx + (unsigned)i0;
+    const float s0 = 1.f - tx, s1 = tx, t0 = 1.f - ty, t1 = ty, r0 = 1.f - tz, r1 = tz;
+    const float wA = s0 * t0, wB = s1 * t0, wC = s0 * t1, wD = s1 * t1;
+    const float w[8] = { wA * r0, wB * r0, wC * r0, wD * r0, wA * r1, wB * r1, wC * r1, wD * r1 };
+    if (idx != cur) {
+      WS_P2G_FLUSH
+      cur = idx;
+#pragma unroll
+      for (int q = 0; q < 8; q++) { m8[q] = w[q] * v[r]; w8[q] = w[q]; }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; q++) { m8[q] = fmaf(w[q], v[r], m8[q]); w8[q] += w[q]; }
+    }
+  }
+  WS_P2G_FLUSH
+#undef WS_P2G_FLUSH
 }
-__global__ void __launch_bounds__(256, 4) k_p2g(Dims d, GridDev g, PartsDev P, int* err) {
-  const int p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x), p1 = p0 + 1;
+__global__ void __launch_bounds__(256, 4) k_p2g_runs(Dims d, GridDev g, PartsDev P, int* err) {
+  const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (p0 >= P.nP) return;
-  const bool has1 = p1 < P.nP;
-  // every load of both particles is issued before the flag tests (one round trip)
-  const int fl0 = P.pflag[p0], fl1 = has1 ? P.pflag[p1] : 1;
-  const float x0 = P.px[p0], y0 = P.py[p0], z0 = P.pz[p0];
-  const float u0 = P.pvx[p0], v0 = P.pvy[p0], w0 = P.pvz[p0];
-  const float x1 = has1 ? P.px[p1] : 0.f, y1 = has1 ? P.py[p1] : 0.f, z1 = has1 ? P.pz[p1] : 0.f;
-  const float u1 = has1 ? P.pvx[p1] : 0.f, v1 = has1 ? P.pvy[p1] : 0.f, w1 = has1 ? P.pvz[p1] : 0.f;
-  // a fluid particle with a non-finite state is left out of the grid and latched
-  const bool a = fl0 == 0 && particle_sound_f(x0, y0, z0, u0, v0, w0, err);
-  const bool b = fl1 == 0 && particle_sound_f(x1, y1, z1, u1, v1, w1, err);
-  if (a && b) {
-    Stencil3 S0, S1;
-    face_stencil3_f(d, x0, y0, z0, S0);
-    face_stencil3_f(d, x1, y1, z1, S1);
-    p2g_pair(d, g.acc, S0, S1, 0, u0, u1);
-    p2g_pair(d, g.acc, S0, S1, 1, v0, v1);
-    p2g_pair(d, g.acc, S0, S1, 2, w0, w1);
-  } else if (a || b) {
-    Stencil3 S;
-    face_stencil3_f(d, a ? x0 : x1, a ? y0 : y1, a ? z0 : z1, S);
-    p2g_comp(d, g.acc, S, 0, a ? u0 : u1);
-    p2g_comp(d, g.acc, S, 1, a ? v0 : v1);
-    p2g_comp(d, g.acc, S, 2, a ? w0 : w1);
+  float x[4], y[4], z[4], u[4], v[4], w[4];
+  int fl[4];
+  if (p0 + 3 < P.nP) {                                // the arrays are 16-byte aligned and p0 % 4 == 0
+    const float4 X = *reinterpret_cast<const float4*>(P.px + p0), Y = *reinterpret_cast<const float4*>(P.py + p0);
+    const float4 Z = *reinterpret_cast<const float4*>(P.pz + p0), U = *reinterpret_cast<const float4*>(P.pvx + p0);
+    const float4 V = *reinterpret_cast<const float4*>(P.pvy + p0), W = *reinterpret_cast<const float4*>(P.pvz + p0);
+    const uchar4 F = *reinterpret_cast<const uchar4*>(P.pflag + p0);
+    x[0] = X.x; x[1] = X.y; x[2] = X.z; x[3] = X.w; y[0] = Y.x; y[1] = Y.y; y[2] = Y.z; y[3] = Y.w;
+    z[0] = Z.x; z[1] = Z.y; z[2] = Z.z; z[3] = Z.w; u[0] = U.x; u[1] = U.y; u[2] = U.z; u[3] = U.w;
+    v[0] = V.x; v[1] = V.y; v[2] = V.z; v[3] = V.w; w[0] = W.x; w[1] = W.y; w[2] = W.z; w[3] = W.w;
+    fl[0] = F.x; fl[1] = F.y; fl[2] = F.z; fl[3] = F.w;
+  } else {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int p = p0 + r;
+      const bool has = p < P.nP;
+      x[r] = has ? P.px[p] : 0.f; y[r] = has ? P.py[p] : 0.f; z[r] = has ? P.pz[p] : 0.f;
+      u[r] = has ? P.pvx[p] : 0.f; v[r] = has ? P.pvy[p] : 0.f; w[r] = has ? P.pvz[p] : 0.f;
+      fl[r] = has ? P.pflag[p] : 1;
+    }
   }
+  // a fluid particle with a non-finite state is left out of the grid and latched
+  unsigned ok = 0;
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+    if (fl[r] == 0 && particle_sound_f(x[r], y[r], z[r], u[r], v[r], w[r], err)) ok |= 1u << r;
+  if (!ok) return;
+  p2g_run_comp<0>(d, g.acc, x, y, z, u, ok);
+  p2g_run_comp<1>(d, g.acc, x, y, z, v, ok);
+  p2g_run_comp<2>(d, g.acc, x, y, z, w, ok);
 }
 void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  k_p2g<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, &st->err);
+  k_p2g_runs<<<grid_for((P.nP + 3) / 4, 256), 256, 0, s>>>(d, g, P, &st->err);
 }
 
 // ------------------------------------------------------------ 3b. P2G in cell order
@@ -286,7 +303,7 @@ void launch_p2g(const Dims& d, const GridDev& g, const PartsDev& P, DevStatus* s
 // of the permutation. One block per brick adds every particle's eight FP32
 // (momentum, weight) terms per component into a shared-memory copy of the
 // faces the brick's particles can reach (red.shared.add.f32), then sends one
-// float2 atomic per touched face. Every FP32 term is the one k_p2g adds;
+// float2 atomic per touched face. Every FP32 term is the one k_p2g_runs adds;
 // only the order of the FP32 sums differs. A particle whose stencil leaves
 // the brick's faces (a ball pushed it after the binning) adds its terms to
 // global memory directly.
