@@ -13,8 +13,10 @@ step(1/60) runs two such substeps).
 Learned warm start (the metric's comparison): after the plain solver's
 timed run, the same planet keeps running while every solve stores its
 (input, converged pressure) pair (2000 pairs), the 3-level U-Net is trained
-on them with Adam (lr 1e-3, batch 4), and the same substep is timed again
-with every solve starting from the network's prediction. Both arms solve to
+on them with Adam (lr 1e-3, batch 4), its output scale is calibrated on
+eight fresh systems (1, 1/2 or 1/4 of the predicted correction, whichever
+leaves SOR the fewest iterations), and the same substep is timed again with
+every solve starting from the network's prediction. Both arms solve to
 the same 1e-5 relative residual. `value` is the learned arm's substeps/s;
 the plain arm's figure, SOR iterations of both, the residual left by the
 prediction and the training and inference times are reported beside it.
