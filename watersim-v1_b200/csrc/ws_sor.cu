@@ -154,7 +154,9 @@ __global__ void k_sor_codes(Dims d, const float* __restrict__ pw, SorLists L, in
 }
 
 // ---------------------------------------------------------------- grid barrier
-struct GridBar { unsigned count; unsigned gen; };
+// grid barrier counters, then (own cache lines) one half-sweep counter per CTA
+constexpr int kMaxSorCtas = 1024;
+struct GridBar { unsigned count; unsigned gen; unsigned pad[30]; unsigned flag[kMaxSorCtas]; };
 
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, unsigned nblocks, int* err) {
   __syncthreads();
@@ -198,6 +200,8 @@ struct SorArgs {
   double* outRel;
   int* outPath;
   int clusterCap;      // lists up to this size per colour were solved by k_sor_cluster
+  const int* offs;     // per 256-cell chunk b: its first list entry of colour 0 and 1 (offs[2 b], offs[2 b + 1])
+  int nChunks;
 };
 
 // One colour's half-sweep over the lists in global memory, three cells per
@@ -206,8 +210,8 @@ struct SorArgs {
 // round trip per batch instead of per cell. Cells of one colour never
 // neighbour each other, so the batch reads no value it writes.
 constexpr int kSorBatch = 3;
-__device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned tid, unsigned T) {
-  const unsigned n = (unsigned)a.L.count[col];
+__device__ __forceinline__ void sor_half(const SorArgs& a, int col, unsigned lo, unsigned hi) {
+  const unsigned n = hi, tid = lo + threadIdx.x, T = blockDim.x;
   const int* __restrict__ idx = a.L.idx[col];
   const float* __restrict__ rhs = a.L.rhs[col];
   const float* __restrict__ pw = a.L.pw[col];
@@ -316,32 +320,95 @@ __device__ __forceinline__ void block_partial(const SorArgs& a, double rr, doubl
   }
 }
 
+// release / acquire of the per-CTA half-sweep counters
+__device__ __forceinline__ void sor_publish(unsigned* flag, unsigned v) {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(flag), "r"(v) : "memory");
+}
+
 // The iteration loop, in two instantiations so that the register-resident
 // entries of the cached path are not live in the list-reading path.
+//
+// Cached path (each thread holds at most one cell per colour): a grid
+// barrier after every half-sweep. List path: CTA p sweeps the contiguous
+// range [ceil(p n / P), ceil((p + 1) n / P)) of each colour list (cells in
+// cell order, so a compact run of z-planes), and a half-sweep waits only for
+// the CTAs owning other-colour cells within one z-plane (nx ny cells) of its
+// range: those it reads, and those that read the cells it writes. Each CTA
+// publishes its count of finished half-sweeps (release) and polls its
+// neighbours' (acquire, bounded); the residual checks keep grid barriers.
 template <bool CACHED>
 __device__ __forceinline__ void persistent_loop(const SorArgs& a, unsigned tid, unsigned T) {
   const int n0 = a.L.count[0], n1 = a.L.count[1];
   const long long nx = a.d.nx, nxy = (long long)a.d.nx * a.d.ny;
+  __shared__ int sLo[2], sHi[2], sDl[2], sDh[2], sAbort;
   Entry e0, e1;
   e0.c = -1; e1.c = -1;
   if (CACHED) {
     if (tid < (unsigned)n0) { e0.c = a.L.idx[0][tid]; e0.rhs = a.L.rhs[0][tid]; e0.pw = a.L.pw[0][tid]; e0.dg = a.L.dg[0][tid]; e0.q = __ldcg(a.q + e0.c); }
     if (tid < (unsigned)n1) { e1.c = a.L.idx[1][tid]; e1.rhs = a.L.rhs[1][tid]; e1.pw = a.L.pw[1][tid]; e1.dg = a.L.dg[1][tid]; e1.q = __ldcg(a.q + e1.c); }
+  } else {
+    if (threadIdx.x == 0) {
+      const long long P = gridDim.x, p = blockIdx.x;
+      sAbort = 0;
+      for (int c = 0; c < 2; c++) {
+        const long long n = c ? n1 : n0, no = c ? n0 : n1;
+        const int lo = (int)((p * n + P - 1) / P), hi = (int)(((p + 1) * n + P - 1) / P);
+        sLo[c] = lo; sHi[c] = hi;
+        int dl = (int)p, dh = (int)p;
+        if (hi > lo && no > 0) {
+          const long long cLo = (long long)(c ? a.L.idx[1] : a.L.idx[0])[lo] - nxy;
+          const long long cHi = (long long)(c ? a.L.idx[1] : a.L.idx[0])[hi - 1] + nxy;
+          const int bLo = cLo < 0 ? 0 : (int)(cLo / 256);
+          const int bHi = (int)std::min<long long>(a.nChunks - 1, cHi / 256);
+          const long long eLo = a.offs[2 * bLo + (1 - c)];
+          const long long eHi = bHi + 1 < a.nChunks ? a.offs[2 * (bHi + 1) + (1 - c)] : no;   // exclusive
+          if (eHi > eLo) { dl = (int)(eLo * P / no); dh = (int)((eHi - 1) * P / no); }
+        }
+        sDl[c] = dl; sDh[c] = dh;
+      }
+    }
+    __syncthreads();
   }
   auto partial = [&]() {
     if (CACHED) { double rr = 0, bb = 0; entry_residual(e0, a.q, nx, nxy, rr, bb); entry_residual(e1, a.q, nx, nxy, rr, bb); block_partial(a, rr, bb); }
     else residual_block(a, tid, T);
   };
+  // list path: before a half-sweep of colour c, the neighbours of that colour
+  // have finished `done` half-sweeps
+  auto wait_deps = [&](int c, unsigned done) -> bool {
+    if (threadIdx.x < 32) {
+      for (int q = sDl[c] + (int)threadIdx.x; q <= sDh[c]; q += 32)
+        if (q != (int)blockIdx.x && !bounded_wait_geq(&a.bar->flag[q], done, kSpinLimit, a.err)) sAbort = 1;
+    }
+    __syncthreads();
+    return *(volatile int*)&sAbort == 0;
+  };
+  auto finish_half = [&](unsigned done) {
+    __syncthreads();                       // every thread's stores before thread 0's release
+    if (threadIdx.x == 0) sor_publish(&a.bar->flag[blockIdx.x], done);
+  };
   int it = 0;
   bool ok = true;
   double rel = -1;
+  unsigned done = 0;
   for (it = 0; it < a.iters && ok; ) {
-    if (CACHED) entry_relax(e0, a.q, nx, nxy, a.om1); else sor_half(a, 0, tid, T);
-    if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
-    if (CACHED) entry_relax(e1, a.q, nx, nxy, a.om1); else sor_half(a, 1, tid, T);
-    if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+    if (CACHED) {
+      entry_relax(e0, a.q, nx, nxy, a.om1);
+      if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+      entry_relax(e1, a.q, nx, nxy, a.om1);
+      if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
+    } else {
+      if (done > 0 && !(ok = wait_deps(0, done))) break;
+      sor_half(a, 0, (unsigned)sLo[0], (unsigned)sHi[0]);
+      finish_half(++done);
+      if (!(ok = wait_deps(1, done))) break;
+      sor_half(a, 1, (unsigned)sLo[1], (unsigned)sHi[1]);
+      finish_half(++done);
+    }
     it++;
     if (a.check > 0 && it % a.check == 0) {
+      if (!CACHED && !(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;   // every half-sweep finished
       partial();
       if (!(ok = grid_barrier(a.bar, gridDim.x, a.err))) break;
       rel = residual_total(a);
@@ -350,8 +417,9 @@ __device__ __forceinline__ void persistent_loop(const SorArgs& a, unsigned tid, 
     }
   }
   if (ok) {
-    partial();
-    ok = grid_barrier(a.bar, gridDim.x, a.err);
+    if (!CACHED) ok = grid_barrier(a.bar, gridDim.x, a.err);
+    if (ok) partial();
+    if (ok) ok = grid_barrier(a.bar, gridDim.x, a.err);
     if (ok) rel = residual_total(a);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) { *a.outIters = it; *a.outRel = rel; *a.outPath = 1; }
@@ -552,7 +620,7 @@ cudaError_t sor_init(void** statePtr, const Dims& d, int device) {
   cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device);
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_sor_persistent, S->block, 0)) != cudaSuccess) return e;
   if (perSM < 1) return cudaErrorLaunchOutOfResources;
-  S->grid = smCount * (perSM > 1 ? 1 : perSM);
+  S->grid = std::min(kMaxSorCtas, smCount * (perSM > 1 ? 1 : perSM));
   long long half = nCells / 2 + 2;
   S->cap = half;
   for (int c = 0; c < 2; c++) {
@@ -676,6 +744,7 @@ static cudaError_t run_lists(SorState* S, const Dims& d, const GridDev& g, doubl
   a.bar = S->bar; a.partials = S->partials; a.err = err; a.outIters = S->outIters; a.outRel = S->outRel;
   a.outPath = S->outPath;
   a.clusterCap = C ? C * kSmax : -1;
+  a.offs = S->blockOffs; a.nChunks = (int)grid_for(d.nCells, 256);
   void* args[] = { &a };
   cudaError_t e = cudaLaunchCooperativeKernel((void*)k_sor_persistent, dim3(S->grid), dim3(S->block), args, 0, s);
   *outIters = S->outIters; *outRel = S->outRel;
