@@ -518,9 +518,14 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
     // interior fluid cell (5: farther), 254 constant (no interior fluid:
     // never updated). One thread per 4-cell brick row (float4 loads when rows
     // are 16-byte aligned), four rows in flight per thread.
+    // Update entries are counted per bucket (colour, d <= 3) here, two
+    // 8-bit counters per byte lane of two words per thread (at most 16 cells
+    // per bucket and pass, since R * 16 rows <= 4 T), so the bucketing below
+    // needs a single pass.
     {
       const bool vec = (d.nx & 3) == 0;
       const int nRows = R * 16;
+      unsigned cnt0 = 0u, cnt1 = 0u;         // buckets 0-3 and 4-7, one byte each
       for (int r0 = 0; r0 < nRows; r0 += 4 * T) {
         float qv[4][4], pv[4][4];
         int rowOk[4];
@@ -571,18 +576,33 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
                 }
                 st = (uint8_t)best;
               }
+              if (st <= 3) {
+                const unsigned inc = 1u << (8 * st);
+                if ((i + j + k) & 1) cnt1 += inc; else cnt0 += inc;
+              }
             }
             S.q[x] = rowOk[u] && i < d.nx ? qv[u][c] : 0.f;
             S.dist[x] = st;
           }
         }
       }
+#pragma unroll
+      for (int b = 0; b < 8; b++) {
+        const int v = warp_sum((int)(((b < 4 ? cnt0 : cnt1) >> (8 * (b & 3))) & 0xffu));
+        if (lane == 0 && v) atomicAdd(&bucket[b], v);
+      }
     }
     if (tid == 0) S.q[kZero] = 0.f;
     __syncthreads();
+    if (tid == 0) {
+      int acc = 0;
+      for (int b = 0; b < 8; b++) { bstart[b] = acc; bcur[b] = acc; acc += bucket[b]; }
+      if (acc > kEMax || bucket[0] + bucket[4] > kOMax) sOverflow = 1;
+    }
+    __syncthreads();
     // update entries: cells with d <= 3, bucketed by (colour, d), and the
     // halo cells reloaded after every epoch (1 <= d <= 4)
-    for (int pass = 0; pass < 2; pass++) {
+    {
       for (int x0 = 0; x0 < R * 64; x0 += T) {
         const int x = x0 + tid;
         int b = -1;
@@ -595,9 +615,7 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
         }
         const unsigned grp = __match_any_sync(0xffffffffu, b);
         const int leader = __ffs(grp) - 1;
-        if (pass == 0) {
-          if (b >= 0 && lane == leader) atomicAdd(&bucket[b], __popc(grp));
-        } else {
+        {
           int base = 0;
           if (b >= 0 && lane == leader) base = atomicAdd(&bcur[b], __popc(grp));
           base = __shfl_sync(0xffffffffu, base, leader);
@@ -626,12 +644,6 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
             if (rpos < kLMax) { S.lDense[rpos] = (unsigned short)x; S.lGlob[rpos] = g; }
           }
         }
-      }
-      __syncthreads();
-      if (pass == 0 && tid == 0) {
-        int acc = 0;
-        for (int b = 0; b < 8; b++) { bstart[b] = acc; bcur[b] = acc; acc += bucket[b]; }
-        if (acc > kEMax || bucket[0] + bucket[4] > kOMax) sOverflow = 1;
       }
       __syncthreads();
     }
