@@ -71,9 +71,6 @@ struct ws_handle {
   void* sor = nullptr;                  // persistent SOR solver state (ws_sor.cu)
   // the substep's face and cell passes run over the active 4^3 bricks
   BrickSet bricks{};
-  int* brickIota = nullptr;             // 0 .. nB - 1, the input of the list compaction
-  void* brickCub = nullptr;             // compaction scratch
-  size_t brickCubBytes = 0;
   CellSort csort{};                     // the particles sorted by cell for P2G
   void* csortCub = nullptr;             // prefix-sum scratch
   size_t csortCubBytes = 0;
@@ -221,7 +218,7 @@ static void free_all(ws_handle* h) {
   if (h->queryBuf) cudaFree(h->queryBuf);
   {
     void* bb[] = { h->bricks.seed, h->bricks.act, h->bricks.proc, h->bricks.list, h->bricks.count, h->bricks.forceAll,
-                   h->brickIota, h->brickCub, h->csort.count, h->csort.start, h->csort.pcell, h->csort.pslot,
+                   h->csort.count, h->csort.start, h->csort.pcell, h->csort.pslot,
                    h->csort.perm, h->csortCub };
     for (void* b : bb) if (b) cudaFree(b);
   }
@@ -325,19 +322,14 @@ extern "C" ws_status ws_create(const ws_config* cfg, ws_handle** out) {
     B.nbx = (d.nx + 3) / 4; B.nby = (d.ny + 3) / 4; B.nbz = (d.nz + 3) / 4;
     B.dnbx = fastdiv_make((unsigned)B.nbx); B.dnby = fastdiv_make((unsigned)B.nby);
     const long long nB = (long long)B.nbx * B.nby * B.nbz;
-    AL(B.seed, nB) AL(B.act, nB) AL(B.proc, nB) AL(B.list, nB) AL(B.count, 1) AL(B.forceAll, 1) AL(h->brickIota, nB)
-    h->brickCubBytes = brick_list_scratch_bytes((int)nB);
-    if ((e = cudaMalloc(&h->brickCub, h->brickCubBytes)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
+    AL(B.seed, nB) AL(B.act, nB) AL(B.proc, nB) AL(B.list, nB) AL(B.count, 1) AL(B.forceAll, 1)
     CellSort& cs = h->csort;
     AL(cs.count, 64 * nB + 1) AL(cs.start, 64 * nB + 1) AL(cs.pcell, P) AL(cs.pslot, P) AL(cs.perm, P)
     cs.cap = (int)P;
     h->csortCubBytes = cell_sort_scratch_bytes(64 * nB);
     if ((e = cudaMalloc(&h->csortCub, h->csortCubBytes)) != cudaSuccess) { ws_status r = fail_cuda(h, e, "cudaMalloc"); free_all(h); delete h; return r; }
-    std::vector<int> iota((size_t)nB);
-    for (long long b = 0; b < nB; b++) iota[(size_t)b] = (int)b;
     const int one = 1;
-    if ((e = cudaMemcpy(h->brickIota, iota.data(), sizeof(int) * nB, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(B.seed, 0, (size_t)nB)) != cudaSuccess || (e = cudaMemset(B.act, 0, (size_t)nB)) != cudaSuccess ||
+    if ((e = cudaMemset(B.seed, 0, (size_t)nB)) != cudaSuccess || (e = cudaMemset(B.act, 0, (size_t)nB)) != cudaSuccess ||
         (e = cudaMemset(B.count, 0, sizeof(int))) != cudaSuccess ||
         (e = cudaMemcpy(B.forceAll, &one, sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
       ws_status r = fail_cuda(h, e, "brick state"); free_all(h); delete h; return r;
@@ -847,9 +839,9 @@ static ws_status stage_mark(ws_handle* h, bool bricks = false) {
                     bricks && h->P.p2gCellOrder ? &h->csort : nullptr, h->st, h->stream);
   ws_status s = check_launch(h, 1); if (s) return s;
   if (bricks) {
-    cudaError_t e = launch_brick_activity(h->bricks, h->brickIota, h->brickCub, h->brickCubBytes, h->stream);
+    cudaError_t e = launch_brick_activity(h->bricks, h->stream);
     if (e != cudaSuccess) return fail_cuda(h, e, "active bricks");
-    s = check_launch(h, 3); if (s) return s;
+    s = check_launch(h, 1); if (s) return s;
   }
   return WS_OK;
 }

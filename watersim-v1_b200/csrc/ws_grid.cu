@@ -861,40 +861,48 @@ void launch_extrapolate(const Dims& d, const GridDev& g, cudaStream_t s) {
 // empties is rewritten once to the fixed values. A forced full pass (after a
 // caller wrote grid fields) processes every brick.
 __global__ void k_brick_activity(int nbx, int nby, int nbz, const uint8_t* __restrict__ seed, uint8_t* __restrict__ act,
-                                 uint8_t* __restrict__ proc, const int* __restrict__ forceAll) {
+                                 uint8_t* __restrict__ proc, const int* __restrict__ forceAll, int* __restrict__ list,
+                                 int* __restrict__ count) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int nB = nbx * nby * nbz;
-  if (b >= nB) return;
-  const int bx = b % nbx, t = b / nbx, by = t % nby, bz = t / nby;
-  int a = 0;
-  for (int dz = -1; dz <= 1 && !a; dz++) {
-    const int z = bz + dz;
-    if (z < 0 || z >= nbz) continue;
-    for (int dy = -1; dy <= 1 && !a; dy++) {
-      const int y = by + dy;
-      if (y < 0 || y >= nby) continue;
-      const uint8_t* row = seed + ((long long)z * nby + y) * nbx;
-      for (int dx = -1; dx <= 1; dx++) {
-        const int x = bx + dx;
-        if (x >= 0 && x < nbx && row[x]) { a = 1; break; }
+  int p = 0;
+  if (b < nB) {
+    const int bx = b % nbx, t = b / nbx, by = t % nby, bz = t / nby;
+    int a = 0;
+    for (int dz = -1; dz <= 1 && !a; dz++) {
+      const int z = bz + dz;
+      if (z < 0 || z >= nbz) continue;
+      for (int dy = -1; dy <= 1 && !a; dy++) {
+        const int y = by + dy;
+        if (y < 0 || y >= nby) continue;
+        const uint8_t* row = seed + ((long long)z * nby + y) * nbx;
+        for (int dx = -1; dx <= 1; dx++) {
+          const int x = bx + dx;
+          if (x >= 0 && x < nbx && row[x]) { a = 1; break; }
+        }
       }
     }
+    p = a | act[b] | (*forceAll != 0);
+    proc[b] = (uint8_t)p;
+    act[b] = (uint8_t)a;
   }
-  proc[b] = (uint8_t)(a | act[b] | (*forceAll != 0));
-  act[b] = (uint8_t)a;
+  // the work list: one atomic per warp (the passes over it do not depend on its order)
+  const unsigned m = __ballot_sync(0xffffffffu, p != 0);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (p) list[base + __popc(m & ((1u << lane) - 1u))] = b;
 }
-size_t brick_list_scratch_bytes(int nB) {
-  size_t bytes = 0;
-  cub::DeviceSelect::Flagged(nullptr, bytes, (const int*)nullptr, (const uint8_t*)nullptr, (int*)nullptr, (int*)nullptr, nB);
-  return bytes;
-}
-// activity, the ordered brick list (CUB's flagged selection, a CUDA toolkit
-// library), then the seeds and the forced-pass flag cleared for the next substep
-cudaError_t launch_brick_activity(const BrickSet& B, const int* iota, void* scratch, size_t scratchBytes, cudaStream_t s) {
+// the count reset, activity and work list, then the seeds and the
+// forced-pass flag cleared for the next substep
+cudaError_t launch_brick_activity(const BrickSet& B, cudaStream_t s) {
   const int nB = B.nbx * B.nby * B.nbz;
-  k_brick_activity<<<grid_for(nB, 256), 256, 0, s>>>(B.nbx, B.nby, B.nbz, B.seed, B.act, B.proc, B.forceAll);
-  cudaError_t e = cub::DeviceSelect::Flagged(scratch, scratchBytes, iota, B.proc, B.list, B.count, nB, s);
+  cudaError_t e = cudaMemsetAsync(B.count, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
+  k_brick_activity<<<grid_for(nB, 256), 256, 0, s>>>(B.nbx, B.nby, B.nbz, B.seed, B.act, B.proc, B.forceAll, B.list,
+                                                      B.count);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(B.seed, 0, (size_t)nB, s)) != cudaSuccess) return e;
   return cudaMemsetAsync(B.forceAll, 0, sizeof(int), s);
 }

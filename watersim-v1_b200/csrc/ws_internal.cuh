@@ -153,7 +153,7 @@ struct BrickSet {
   uint8_t* seed;            // bricks holding a particle or moving solid this substep
   uint8_t* act;             // seeds dilated by one brick (kept for the next substep)
   uint8_t* proc;            // this substep's work: act | last substep's act | forced
-  int* list;                // the bricks with proc set, in increasing order
+  int* list;                // the bricks with proc set (in no particular order)
   int* count;
   int* forceAll;            // device flag: process every brick once
   FastDiv dnbx, dnby;       // division by nbx and nby (brick coordinates of a linear brick index)

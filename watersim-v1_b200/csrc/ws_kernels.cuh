@@ -26,8 +26,7 @@ void launch_static_types(const Dims& d, const TerrainDev& t, double coreR, uint8
 void launch_gravity_geometry(const Dims& d, double oceanR, float* g, cudaStream_t s);
 void launch_clear_raster(const Dims& d, const GridDev& g, DevStatus* st, bool clearAcc, cudaStream_t s);
 // the substep's face and cell passes over the active-brick list (ws_grid.cu)
-size_t brick_list_scratch_bytes(int nB);
-cudaError_t launch_brick_activity(const BrickSet& B, const int* iota, void* scratch, size_t scratchBytes, cudaStream_t s);
+cudaError_t launch_brick_activity(const BrickSet& B, cudaStream_t s);
 void launch_clear_acc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
 void launch_faces_normalize_bc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s);
 void launch_faces_forces_bricks(const Dims& d, const GridDev& g, const BrickSet& B, double coef, int viscOn, double dt,
