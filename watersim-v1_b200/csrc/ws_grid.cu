@@ -193,11 +193,64 @@ __global__ void k_mark_fluid(Dims d, GridDev g, PartsDev P, TerrainDev t, double
   if (has0) { cs.pcell[p0] = k0; cs.pslot[p0] = r0; }
   if (has1) { cs.pcell[p1] = k1; cs.pslot[p1] = r1; }
 }
+// Without the cell sort: four consecutive particles per thread (float4 and
+// uchar4 loads), the seed brick stored once per run of particles in one
+// brick, the cell types of all four loaded before any store, and a store
+// once per run of particles in one cell. Same marks as k_mark_fluid.
+__global__ void __launch_bounds__(256) k_mark_fluid_runs(Dims d, GridDev g, PartsDev P, TerrainDev t, double oceanR,
+                                                         double coreR, int* err) {
+  const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (p0 >= P.nP) return;
+  float xs[4], ys[4], zs[4];
+  int fl[4];
+  int nHave = 4;
+  if (p0 + 3 < P.nP) {                                // the arrays are 16-byte aligned and p0 % 4 == 0
+    const float4 X = *reinterpret_cast<const float4*>(P.px + p0), Y = *reinterpret_cast<const float4*>(P.py + p0);
+    const float4 Z = *reinterpret_cast<const float4*>(P.pz + p0);
+    const uchar4 F = *reinterpret_cast<const uchar4*>(P.pflag + p0);
+    xs[0] = X.x; xs[1] = X.y; xs[2] = X.z; xs[3] = X.w; ys[0] = Y.x; ys[1] = Y.y; ys[2] = Y.z; ys[3] = Y.w;
+    zs[0] = Z.x; zs[1] = Z.y; zs[2] = Z.z; zs[3] = Z.w; fl[0] = F.x; fl[1] = F.y; fl[2] = F.z; fl[3] = F.w;
+  } else {
+    nHave = P.nP - p0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const bool has = r < nHave;
+      xs[r] = has ? P.px[p0 + r] : 0.f; ys[r] = has ? P.py[p0 + r] : 0.f; zs[r] = has ? P.pz[p0 + r] : 0.f;
+      fl[r] = has ? P.pflag[p0 + r] : 1;
+    }
+  }
+  long long c[4];
+  int lastBrick = -1;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    c[r] = -1;
+    if (r >= nHave) continue;
+    const double X = xs[r], Y = ys[r], Z = zs[r];
+    // the first pass of a substep to read the positions: every particle must
+    // be finite and inside the domain box (the reference's passes keep it there)
+    particle_sound(d, X, Y, Z, 0.0, 0.0, 0.0, err, true);
+    // the brick of every particle's cell seeds this substep's active bricks
+    const int i = jfloor_clamp(over_dx(d, X), 0, d.nx - 1), j = jfloor_clamp(over_dx(d, Y), 0, d.ny - 1);
+    const int k = jfloor_clamp(over_dx(d, Z), 0, d.nz - 1);
+    const int sb = ((k >> 2) * g.nby + (j >> 2)) * g.nbx + (i >> 2);
+    if (g.seed && sb != lastBrick) { g.seed[sb] = 1; lastBrick = sb; }
+    c[r] = mark_cell(d, g, P, t, oceanR, coreR, p0 + r, fl[r], X, Y, Z);
+  }
+  uint8_t ty[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) ty[r] = c[r] >= 0 ? g.type[c[r]] : (uint8_t)WS_SOLID;
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+    if (ty[r] == WS_AIR && (r == 0 || c[r] != c[r - 1])) g.type[c[r]] = WS_FLUID;
+}
 void launch_mark_fluid(const Dims& d, const GridDev& g, const PartsDev& P, const TerrainDev& t,
                        double oceanR, double coreR, const CellSort* cs, DevStatus* st, cudaStream_t s) {
   if (P.nP <= 0) return;
-  CellSort none{};
-  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, cs ? *cs : none, &st->err);
+  if (!cs) {
+    k_mark_fluid_runs<<<grid_for((P.nP + 3) / 4, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, &st->err);
+    return;
+  }
+  k_mark_fluid<<<grid_for((P.nP + 1) / 2, 256), 256, 0, s>>>(d, g, P, t, oceanR, coreR, *cs, &st->err);
 }
 
 // ------------------------------------------------------------ 3. P2G scatter
