@@ -830,7 +830,7 @@ static AdvectParams advect_params(ws_handle* h, double dt) {
 static ws_status stage_clear_raster(ws_handle* h, bool bricks = false) {
   launch_clear_raster(h->d, grid_of(h), h->st, !bricks, h->stream);
   if (bricks) launch_clear_acc_bricks(h->d, grid_of(h), h->bricks, h->stream);
-  return check_launch(h, bricks ? 3 : 1);
+  return check_launch(h, bricks ? 2 : 1);
 }
 // bricks: the substep's own pipeline, where (with p2gCellOrder) the mark
 // pass also counts the particles per cell for the cell-ordered P2G
@@ -1181,10 +1181,12 @@ static ws_status vapor_collisions(ws_handle* h) {
   ws_status s0 = contact_scratch(h); if (s0) return s0;
   launch_vapor_collisions(h->d, parts_of(h), h->S.spacing, h->S.oceanR, h->P.spinOn, h->P.hasSun, sunRel,
                           h->contactScratch, contacts_scratch_bytes(h->capacity, h->d.ny * h->d.nz), h->st, h->stream);
-  ws_status s = check_launch(h, 1); if (s) return s;
-  s = sync_status(h); if (s) return s;
+  // the census lands in the status word; the caller reads it at its next
+  // synchronisation (no kernel after this in the frame writes it)
+  return check_launch(h, 1);
+}
+static void pull_vapor_census(ws_handle* h) {
   h->S.vaporCount = h->stHost->vaporCount; h->S.nightVaporCount = h->stHost->nightVapor;
-  return WS_OK;
 }
 static ws_status ice_contacts(ws_handle* h) {
   ws_status s0 = contact_scratch(h); if (s0) return s0;
@@ -1227,7 +1229,9 @@ static ws_status step_frame(ws_handle* h, double dtFrame) {
     if ((s = ice_contacts(h))) return s;
   }
   if ((s = push_surface(h))) return s;
-  return sync_status(h);
+  if ((s = sync_status(h))) return s;
+  if (h->P.thermalOn) pull_vapor_census(h);
+  return WS_OK;
 }
 extern "C" ws_status ws_step(ws_handle* h, double dtFrame) {
   if (h && h->asyncRunning.load(std::memory_order_acquire)) return WS_ERR_BUSY;
@@ -1320,7 +1324,9 @@ extern "C" ws_status ws_stage(ws_handle* h, int32_t stage, double dt) {
     default: return fail(h, WS_ERR_INVALID, "unknown stage");
   }
   if (s) return s;
-  return sync_status(h);
+  if ((s = sync_status(h))) return s;
+  if (stage == WS_STAGE_VAPOR_COLLISIONS) pull_vapor_census(h);
+  return WS_OK;
 }
 
 // ------------------------------------------------------------ balls

@@ -1007,6 +1007,14 @@ __device__ __forceinline__ bool brick_face(const Dims& d, const BrickSet& B, int
 struct FacePassArgs { double coef, dt, gs; int viscOn, doClamp; float vcap; };
 template <int OP>
 __global__ void __launch_bounds__(256) k_faces_bricks(Dims d, GridDev g, BrickSet B, FacePassArgs fa, DevStatus* st) {
+  if (OP == 4 && *B.forceAll) {                          // after a forced full pass: the whole accumulator
+    const long long F2 = d.F >> 1;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t <= F2; t += (long long)gridDim.x * blockDim.x) {
+      if (t < F2) reinterpret_cast<float4*>(g.acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+      else if (d.F & 1) g.acc[d.F - 1] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
   const int n = *B.count;
   float umax = 0.f;
   const FaceSlot sl = face_slot(threadIdx.x < 240 ? (int)threadIdx.x : 0);
@@ -1051,16 +1059,7 @@ void launch_extrapolate_bricks(const Dims& d, const GridDev& g, const BrickSet& 
 }
 // the accumulator of the bricks in the list (those the previous substep's
 // P2G may have written), or all of it after a forced full pass
-__global__ void k_clear_acc_all(Dims d, float2* acc, const int* __restrict__ forceAll) {
-  if (!*forceAll) return;
-  const long long F2 = d.F >> 1;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t <= F2; t += (long long)gridDim.x * blockDim.x) {
-    if (t < F2) reinterpret_cast<float4*>(acc)[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-    else if (d.F & 1) acc[d.F - 1] = make_float2(0.f, 0.f);
-  }
-}
 void launch_clear_acc_bricks(const Dims& d, const GridDev& g, const BrickSet& B, cudaStream_t s) {
-  k_clear_acc_all<<<148 * 8, 256, 0, s>>>(d, g.acc, B.forceAll);
   k_faces_bricks<4><<<brick_grid(B), 256, 0, s>>>(d, g, B, FacePassArgs{}, nullptr);
 }
 // the pressure setup over the brick list: four bricks per 256-thread block
