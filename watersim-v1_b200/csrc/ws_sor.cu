@@ -429,6 +429,10 @@ __global__ void __launch_bounds__(1024, 1) k_sor_persistent(SorArgs a) {
   const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n0 = a.L.count[0], n1 = a.L.count[1];
   if (n0 <= a.clusterCap && n1 <= a.clusterCap) return;      // the cluster solve ran
+  if (n0 + n1 == 0) {                  // no fluid cell: no sweep (js/solver.js:1330)
+    if (tid == 0) { *a.outIters = 0; *a.outRel = 0; *a.outPath = 1; }
+    return;
+  }
   // register-resident path when every thread owns at most one cell per colour
   if ((unsigned)n0 <= T && (unsigned)n1 <= T) persistent_loop<true>(a, tid, T);
   else persistent_loop<false>(a, tid, T);
@@ -488,6 +492,10 @@ __global__ void __launch_bounds__(1024, 1) k_sor_cluster(ClusterArgs a) {
   const int rank = (int)cl.block_rank();
   const int n0 = a.L.count[0], n1 = a.L.count[1];
   if (n0 > C * kSmax || n1 > C * kSmax) return;         // uniform: the grid solve takes it
+  if (n0 + n1 == 0) {                                    // no fluid cell: no sweep (js/solver.js:1330)
+    if (rank == 0 && threadIdx.x == 0) { *a.outIters = 0; *a.outRel = 0; *a.outPath = 2; }
+    return;
+  }
   const int S0 = (n0 + C - 1) / C, S1 = (n1 + C - 1) / C;
   const int QS = kSmax + 1;                              // slot kSmax holds 0.0f
   float* qs[2]; float* rh[2]; float* pw[2]; uint16_t* cd[2]; uint8_t* dg[2];

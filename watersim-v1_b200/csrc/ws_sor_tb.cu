@@ -454,6 +454,9 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_sor_tb(TbArgs a) {
     }
   }
   if (!tb_grid_barrier(a.ctl, a.err, &sAbort)) goto done;
+  // no fluid cell: the reference returns before its first sweep
+  // (js/solver.js:1330); every CTA read the same total, so all leave here
+  if (sA == 0) { rel = 0; goto done; }
 
   // ---- phase 2: this CTA's region
   {
