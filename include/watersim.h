@@ -143,7 +143,11 @@ typedef struct {
   const float* R;          /* n^3 */
 } ws_terrain;
 
-/* ---- lifetime: new FluidSolver(opts) (js/solver.js:45-216) */
+/* ---- lifetime: new FluidSolver(opts) (js/solver.js:45-216). The grid needs
+ *      at least 4 cells along each axis, dx > 0 and capacity >= 1
+ *      (WS_ERR_INVALID otherwise) and at most 2^29 cells (WS_ERR_RANGE); these
+ *      are checked before any device call. Every entry point answers a NULL
+ *      handle with WS_ERR_INVALID. */
 ws_status ws_create(const ws_config* cfg, ws_handle** out);
 ws_status ws_destroy(ws_handle* h);
 const char* ws_last_error(const ws_handle* h);

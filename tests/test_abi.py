@@ -50,3 +50,50 @@ def test_create_fails_cleanly_without_device(monkeypatch):
         assert e.code < 0
     else:
         raise AssertionError("ws_create must fail without a device")
+
+
+def _zero_args(fn):
+    import ctypes as C
+    args = []
+    for t in fn.argtypes or []:
+        if t in (C.c_double, C.c_float):
+            args.append(0.0)
+        elif t in (C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_int, C.c_uint8):
+            args.append(0)
+        else:
+            args.append(None)
+    return args
+
+
+def test_null_handle_rejected_everywhere():
+    """Every entry point that takes a handle (or an output pointer) answers a
+    NULL one with WS_ERR_INVALID before any device call; ws_last_error names it."""
+    L = fluid_solver.load_library()
+    for name in fluid_solver.SYMBOLS:
+        if name in ("ws_version", "ws_last_error"):
+            continue
+        fn = getattr(L, name)
+        assert fn(*_zero_args(fn)) == -1, name
+    assert L.ws_last_error(None) == b"null handle"
+
+
+def test_create_and_noalloc_validate_sizes_before_any_device_call():
+    import ctypes as C
+    L = fluid_solver.load_library()
+    h = C.c_void_p()
+
+    def create(nx, ny, nz, dx=1.0, cap=16):
+        cfg = fluid_solver.WsConfig(nx=nx, ny=ny, nz=nz, capacity=cap, dx=dx, coreR=1.0, bumpiness=0.3,
+                                    targetParticles=16.0, terrainSeed=1, device=0)
+        return L.ws_create(C.byref(cfg), C.byref(h))
+
+    assert create(3, 8, 8) == -1                     # below the 4-cell minimum
+    assert create(8, 8, 8, dx=0.0) == -1
+    assert create(8, 8, 8, cap=0) == -1
+    assert create(1024, 1024, 1024) == -7            # beyond 2^29 cells
+    buf = (C.c_float * 4)()
+    rel = C.c_double()
+    p = C.cast(buf, C.c_void_p)
+    assert L.ws_residual_noalloc(2, 8, 8, p, p, p, C.byref(rel), None) == -1
+    assert L.ws_residual_noalloc(8, 8, 8, None, p, p, C.byref(rel), None) == -1
+    assert L.ws_residual_noalloc(512, 512, 512, p, p, p, C.byref(rel), None) == -7
