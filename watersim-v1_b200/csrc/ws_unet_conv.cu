@@ -77,8 +77,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Output planes per work item: eight (a whole tile) up to 32 channels; two
+// from 48 to 128 channels, which run on the coarse levels, where a tile per
+// item would leave most SMs idle (the 32^3 level of a 128^3 grid has 32
+// tiles) and each CTA would walk four or more input slices in turn.
 template <int COUT> struct ConvShape {
-  static constexpr int ZT = COUT <= 32 ? 8 : COUT <= 64 ? 4 : COUT <= 128 ? 2 : 1;
+  static constexpr int ZT = COUT <= 32 ? 8 : COUT <= 128 ? 2 : 1;
   static constexpr int HX = kTX + 2, HY = kTY + 2, HZ = ZT + 2;
   static constexpr int HV = HX * HY * HZ;           // halo voxels
   static constexpr int KSTR = HV * 16;              // bytes of one 8-channel halo chunk
